@@ -1,0 +1,429 @@
+"""Benchmark: integral-direct J/K Fock builds of (H2O)_64 / STO-3G on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl dftk|reference]
+
+One step = one full FP64 direct J/K build (every Schwarz-surviving quartet,
+tau 1e-12, density cut 1e-14) of (H2O)_64 / STO-3G (448 basis functions,
+seeded 4x4x4 lattice, see dft_b200/geometry.py) at its converged RHF
+density, inputs resident in HBM.  The L2 (126 MB) is flushed between steps
+by writing a 256 MB buffer, outside the timed events.
+
+Reported besides the headline:
+  * e2e      the same build through the reference-facing call
+             shelled.fill_matrices(shells, P, P_a, P_b, J, K_a, K_b) with host
+             NumPy arrays (host->device densities and device->host J/K inside
+             the timed region);
+  * mixed    FP64 vs mixed FP32/FP64 incremental builds over the full SCF
+             (builds/s averaged over the build sequence) and |dE| in uEh;
+  * roofline the dominant class kernel's achieved FP64 rate from the fixed
+             flop accounting, against an FMA-loop peak measured here;
+  * cpu_baseline  the reference's integral kernel (oracle/_ref, host-compiled)
+             plus the restated contraction/digestion, timed on a sample of
+             screened quartets per class and extrapolated by class counts.
+
+With N > 1 (torchrun) every rank builds its own replica: weak scaling, no
+collective on the data path; the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "J/K Fock builds/s, (H2O)_64 STO-3G, mixed vs FP64 at |ΔE|≤1µEh; grad time"
+UNIT = "Fock builds/s"
+WORKLOAD = "(H2O)_64 STO-3G RHF, 448 basis functions, direct J/K FP64, Schwarz 1e-12"
+
+
+# ----------------------------------------------------------------- helpers
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            return json.load(fh)
+    return {}
+
+
+def fma_peak_tflops(torch, lib, precision=64):
+    """Measured FMA-pipe peak (TFLOP/s) from an 8-chain FMA loop on every SM."""
+    from dft_b200 import _lib
+
+    props = torch.cuda.get_device_properties(0)
+    blocks, threads, iters = props.multi_processor_count * 8, 256, 4096
+    sink = torch.empty(blocks * threads, dtype=torch.float64, device="cuda")
+    s = _lib.stream_handle()
+    for _ in range(2):
+        _lib.call("dftk_fma_burn", precision, blocks, threads, iters, _lib.ptr(sink), s)
+    torch.cuda.synchronize()
+    best = float("inf")
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _lib.call("dftk_fma_burn", precision, blocks, threads, iters, _lib.ptr(sink), s)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    flops = 2.0 * 8 * iters * blocks * threads
+    return flops / best / 1e12
+
+
+def setup_workload(torch, shape=(4, 4, 4)):
+    from dft_b200 import basis, geometry
+    from dft_b200.engine import IntegralEngine
+    from dft_b200.scf import scf_rhf
+
+    atoms, centers = geometry.water_cluster(shape)
+    shells = basis.build_shells(basis.load_basis(), atoms, centers)
+    eng = IntegralEngine(shells, tau_schwarz=1e-12)
+    S, T, V = eng.one_electron(atoms, centers)
+    H = T + V
+    enn = geometry.nuclear_repulsion(atoms, centers)
+    nocc = basis.n_electrons(atoms) // 2
+    return atoms, centers, shells, eng, S, H, enn, nocc
+
+
+# ------------------------------------------------------------ reference arm
+def cpu_reference_rate(eng_totals, shells, q_by_class, per_class, seed=0, kernel="reference"):
+    """Fock builds/s of the reference's CPU path, from timed per-class samples.
+
+    Samples `per_class[c]` Schwarz-surviving quartets of each class, digests
+    them with the reference's host-compiled eri_kernel (kernel="reference")
+    or the restated one ("port"), and extrapolates each class's time by its
+    quartet count.  Returns (builds_per_s, cores, sample description)."""
+    from oracle import oracle as orc
+
+    rng = np.random.default_rng(seed)
+    l = np.array([s["angular_momentum"] for s in shells])
+    ii, jj = np.tril_indices(len(shells))
+    pairs_by_class = [[], [], []]
+    for i, j in zip(ii, jj):
+        a, b = (i, j) if l[i] >= l[j] else (j, i)
+        pairs_by_class[l[a] + l[b]].append((i, j))
+    from dft_b200.engine import QCLASS_PAIRS
+
+    N = shells[-1]["ao_stop"]
+    A = rng.normal(size=(N, N))
+    P = (A + A.T) * 0.01
+    ref = orc.ref_lib() if kernel == "reference" else None
+    if kernel == "reference" and ref is None:
+        kernel = "port"
+    total_t = 0.0
+    desc = []
+    for c, (X, Y) in enumerate(QCLASS_PAIRS):
+        n = per_class[c]
+        if eng_totals[c] == 0 or n == 0:
+            continue
+        qx, qy = q_by_class[X], q_by_class[Y]
+        px, py = pairs_by_class[X], pairs_by_class[Y]
+        picks = []
+        tries = 0
+        while len(picks) < n and tries < 200 * n:
+            tries += 1
+            r = rng.integers(len(px))
+            k = rng.integers(len(py))
+            if X == Y and k > r:
+                r, k = k, r
+            if qx[r] * qy[k] >= 1e-12:
+                picks.append((*px[r], *py[k]))
+        quads = np.array(picks, dtype=np.int32)
+        t0 = time.perf_counter()
+        if kernel == "reference":
+            orc.direct_jk_reference_kernel(shells, quads, P, P / 2, P / 2, ref=ref)
+        else:
+            orc.direct_jk(shells, quads, P, P / 2, P / 2)
+        dt = time.perf_counter() - t0
+        total_t += dt / len(picks) * eng_totals[c]
+        desc.append(f"{len(picks)}")
+    cores = orc.lib().orc_num_threads()
+    sample = (f"{'/'.join(desc)} Schwarz-kept quartets per class (ss|ss)..(pp|pp) of (H2O)_64, "
+              f"timed with {cores} OpenMP threads, extrapolated by class counts {list(eng_totals)}")
+    return 1.0 / total_t, cores, sample, kernel
+
+
+def schwarz_by_reference_order(shells):
+    """Per pair-class Schwarz factors in the reference pair order (CPU oracle)."""
+    from oracle import oracle as orc
+
+    l = np.array([s["angular_momentum"] for s in shells])
+    ii, jj = np.tril_indices(len(shells))
+    diag = np.stack([ii, jj, ii, jj], axis=1).astype(np.int32)
+    vals, off = orc.eri_quartets(shells, diag)
+    q = np.sqrt(np.array([np.abs(vals[off[t]:off[t + 1]]).max() for t in range(len(ii))]))
+    pc = np.maximum(l[ii], l[jj]) + np.minimum(l[ii], l[jj])
+    return [q[pc == c] for c in range(3)]
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    from dft_b200 import basis, geometry
+    from dft_b200.engine import QCLASS_PAIRS, candidate_offsets
+
+    atoms, centers = geometry.water_cluster((4, 4, 4))
+    shells = basis.build_shells(basis.load_basis(), atoms, centers)
+    qs = schwarz_by_reference_order(shells)
+    qsorted = [np.sort(q)[::-1] for q in qs]
+    totals = [int(candidate_offsets(qsorted[X], qsorted[Y], X == Y, 1e-12)[-1]) for X, Y in QCLASS_PAIRS]
+    per_class = [4000, 4000, 2000, 2000, 800, 160]
+    for _ in range(max(0, args.warmup)):
+        cpu_reference_rate(totals, shells, qs, [max(1, n // 10) for n in per_class], seed=1)
+    rates = []
+    t0 = time.perf_counter()
+    for s in range(args.steps):
+        r, cores, sample, kind = cpu_reference_rate(totals, shells, qs, per_class, seed=100 + s)
+        rates.append(r)
+    wall = time.perf_counter() - t0
+    value = float(np.mean(rates))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "molecule": "(H2O)_64", "basis": "STO-3G", "n_basis": 448,
+                   "quartets_per_class": totals},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": wall,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- main arm
+def run_dftk_arm(args, rank, world, local_rank):
+    import torch
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+    from dft_b200 import _lib, shelled
+    from dft_b200.engine import FLOPS_PER_PRIM_QUARTET, QCLASS_NAMES
+    from dft_b200.scf import scf_rhf
+
+    atoms, centers, shells, eng, S, H, enn, nocc = setup_workload(torch)
+    # converged FP64 SCF (setup, untimed) gives the density of the timed builds
+    ref_scf = scf_rhf(eng, H, S, nocc, enn, incremental=True, mixed=False, count_quartets=False)
+    D = ref_scf.D_a
+    Dt = (2.0 * D).contiguous()
+    N = eng.n_ao
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    counts = torch.zeros(12, dtype=torch.int64, device="cuda")
+    J = torch.empty((N, N), dtype=torch.float64, device="cuda")
+    Ka = torch.empty((N, N), dtype=torch.float64, device="cuda")
+
+    def build():
+        eng.jk(Dt, D, tau=1e-14, out=(J, Ka, None))
+
+    for _ in range(max(args.warmup, 3)):
+        build()
+    torch.cuda.synchronize()
+    counts.zero_()
+    eng.jk(Dt, D, tau=1e-14, counts=counts)
+    torch.cuda.synchronize()
+    evaluated = counts[:6].tolist()
+    # per-class kernel times (events around each class launch inside dftk_jk)
+    lib = _lib.load()
+    _lib.call("dftk_jk_timing", 1)
+    class_ms = np.zeros(12)
+    n_timing = 3
+    for _ in range(n_timing):
+        flush.zero_()
+        build()
+        buf = (__import__("ctypes").c_float * 12)()
+        _lib.call("dftk_jk_timing_read", buf, 12)
+        class_ms += np.array(buf[:])
+    class_ms /= n_timing
+    _lib.call("dftk_jk_timing", 0)
+
+    # timed steps
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clocks:
+        for k in range(args.steps):
+            flush.zero_()
+            starts[k].record()
+            build()
+            stops[k].record()
+        torch.cuda.synchronize()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, stops)]
+    tot_ms = float(np.sum(step_ms))
+    if dist is not None:
+        t = torch.tensor([tot_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot_ms = float(t.item())
+        dist.barrier()
+    ms_per_step = tot_ms / args.steps
+    value = world * args.steps / (tot_ms / 1e3)
+
+    # e2e through the reference-facing call with host arrays
+    Dh = D.cpu().numpy()
+    Ph = (2.0 * Dh).copy()
+    Jh, Kah, Kbh = (np.zeros((N, N)) for _ in range(3))
+    for _ in range(2):
+        shelled.fill_matrices(shells, Ph, Dh, Dh, Jh, Kah, Kbh, tau=1e-14)
+    e2e_ms = []
+    for _ in range(max(2, min(args.steps, 5))):
+        Jh[:] = 0
+        Kah[:] = 0
+        Kbh[:] = 0
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        shelled.fill_matrices(shells, Ph, Dh, Dh, Jh, Kah, Kbh, tau=1e-14)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_value = world * 1e3 / float(np.mean(e2e_ms))
+
+    line = None
+    if rank == 0:
+        peaks = measured_peaks()
+        fp64_peak = fma_peak_tflops(torch, lib, 64)
+        fp32_peak = fma_peak_tflops(torch, lib, 32)
+        nprimq = eng.kmax * eng.kmax
+        class_flops = [FLOPS_PER_PRIM_QUARTET[c] * nprimq * evaluated[c] for c in range(6)]
+        dom = int(np.argmax(class_ms[:6]))
+        achieved = class_flops[dom] / (class_ms[dom] / 1e3) / 1e12
+        total_flops = sum(class_flops)
+        # mixed vs FP64 over a full incremental SCF (setup of the comparison, timed per build)
+        r64 = scf_rhf(eng, H, S, nocc, enn, incremental=True, mixed=False, count_quartets=True)
+        rmx = scf_rhf(eng, H, S, nocc, enn, incremental=True, mixed=True, count_quartets=True)
+        b64 = r64.fock_builds / r64.fock_seconds
+        bmx = rmx.fock_builds / rmx.fock_seconds
+        traffic = None
+        tpath = os.path.join(REPO, "profiles", "jk_traffic.json")
+        if os.path.exists(tpath):
+            with open(tpath) as fh:
+                tj = json.load(fh)
+            traffic = tj.get("per_launch_bytes", {}).get(QCLASS_NAMES[dom])
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            from dft_b200.engine import QCLASS_PAIRS
+
+            qs = schwarz_by_reference_order(shells)
+            rate, cores, sample, kind = cpu_reference_rate(eng.quartet_totals(), shells, qs,
+                                                           [6000, 6000, 3000, 3000, 1200, 240], seed=7)
+            cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "molecule": "(H2O)_64 4x4x4 lattice seed 0", "basis": "STO-3G",
+                       "n_basis": N, "tau_schwarz": 1e-12, "tau_density": 1e-14,
+                       "quartets_per_class": eng.quartet_totals(), "evaluated_per_class": evaluated,
+                       "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * N * N * 8,
+                    "d2h_bytes_per_step": 3 * N * N * 8, "call": "shelled.fill_matrices (host NumPy arrays)"},
+            "gpu_launches": args.steps * (2 + sum(1 for c in range(6) if eng.quartet_totals()[c] > 0)),
+            "roofline": {"bound": "fp64_fma", "kernel": f"k_jk<{dom},double> {QCLASS_NAMES[dom]}",
+                         "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
+                         "peak_source": "measured FP64 FMA loop (dftk_fma_burn) on this GPU",
+                         "traffic": traffic,
+                         "whole_build_tflops": total_flops / (ms_per_step / 1e3) / 1e12,
+                         "class_ms": {QCLASS_NAMES[c]: float(class_ms[c]) for c in range(6)},
+                         "fp32_peak_tflops": fp32_peak, "hbm_peak_gbs": peaks.get("hbm_gbs")},
+            "mixed": {"fp64_incremental_builds_per_s": b64, "mixed_incremental_builds_per_s": bmx,
+                      "speedup": bmx / b64, "scf_iterations_fp64": r64.iterations,
+                      "scf_iterations_mixed": rmx.iterations,
+                      "energy_fp64": r64.energy, "energy_mixed_final": rmx.energy,
+                      "delta_E_uEh_final": abs(rmx.energy - r64.energy) * 1e6,
+                      "delta_E_uEh_last_mixed_build": abs(rmx.energy_last_build - r64.energy) * 1e6,
+                      "quartets_fp64_fp32_mixed": rmx.counts},
+            "clocks": clocks.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="dftk", choices=["dftk", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference_arm(args, rank, world)
+    return run_dftk_arm(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,143 @@
+"""ctypes binding of libdftk.so (declared in include/dftk.h).
+
+The library is built in-tree (``dft_b200/libdftk.so``) by
+``dft_b200/csrc/build.py``.  There is no fallback: if the shared object is
+missing or a call fails, a :class:`DftkError` is raised.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdftk.so")
+
+N_QCLASS = 6
+N_PCLASS = 3
+JK_UHF = 1
+JK_MIXED = 2
+
+OK, ERR_ARG, ERR_CUDA, ERR_UNSUPPORTED, ERR_WORKSPACE, ERR_SIZE = range(6)
+
+# Exported symbols (every one declared in include/dftk.h).
+SYMBOLS = (
+    "dftk_version", "dftk_last_error", "dftk_init", "dftk_boys", "dftk_boys32",
+    "dftk_pair_data", "dftk_schwarz", "dftk_one_electron", "dftk_eri_blocks",
+    "dftk_jk_workspace_bytes", "dftk_jk", "dftk_nuclear_kernel", "dftk_eri_kernel",
+    "dftk_fma_burn", "dftk_jk_timing", "dftk_jk_timing_read",
+)
+
+
+class DftkError(RuntimeError):
+    """A libdftk call returned a non-zero status."""
+
+    def __init__(self, name: str, status: int, message: str):
+        super().__init__(f"{name} failed with status {status}: {message}")
+        self.status = status
+
+
+class Shells(ctypes.Structure):
+    _fields_ = [
+        ("n_shells", ctypes.c_int),
+        ("n_ao", ctypes.c_int),
+        ("xyz", ctypes.c_void_p),
+        ("l", ctypes.c_void_p),
+        ("nprim", ctypes.c_void_p),
+        ("prim_off", ctypes.c_void_p),
+        ("ao", ctypes.c_void_p),
+        ("prim_exp", ctypes.c_void_p),
+        ("prim_cn", ctypes.c_void_p),
+    ]
+
+
+class Pairs(ctypes.Structure):
+    _fields_ = [
+        ("n_pairs", ctypes.c_int),
+        ("kmax", ctypes.c_int),
+        ("ab", ctypes.c_void_p),
+        ("nprim", ctypes.c_void_p),
+        ("rec64", ctypes.c_void_p),
+        ("rec32", ctypes.c_void_p),
+        ("q", ctypes.c_void_p),
+    ]
+
+
+class Queue(ctypes.Structure):
+    _fields_ = [
+        ("n_rows", ctypes.c_longlong * N_QCLASS),
+        ("total", ctypes.c_longlong * N_QCLASS),
+        ("row_off", ctypes.c_void_p * N_QCLASS),
+    ]
+
+
+PairsArray = Pairs * N_PCLASS
+
+_lib: Optional[ctypes.CDLL] = None
+
+
+def load() -> ctypes.CDLL:
+    """Load libdftk.so (building it first when nvcc is present and it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        from .csrc import build as _build
+
+        try:
+            _build.build()
+        except Exception as exc:  # pragma: no cover - build environment specific
+            raise DftkError("load", -1, f"libdftk.so missing and build failed: {exc}") from exc
+    lib = ctypes.CDLL(LIB_PATH)
+    vp, i, ll, d, sz = ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_double, ctypes.c_size_t
+    sig = {
+        "dftk_version": ([], i),
+        "dftk_last_error": ([], ctypes.c_char_p),
+        "dftk_init": ([], i),
+        "dftk_boys": ([i, ll, vp, vp, vp], i),
+        "dftk_boys32": ([i, ll, vp, vp, vp], i),
+        "dftk_pair_data": ([ctypes.POINTER(Shells), i, ctypes.POINTER(Pairs), vp], i),
+        "dftk_schwarz": ([ctypes.POINTER(Shells), i, ctypes.POINTER(Pairs), vp], i),
+        "dftk_one_electron": ([ctypes.POINTER(Shells), i, vp, vp, vp, vp, vp, vp], i),
+        "dftk_eri_blocks": ([ctypes.POINTER(Shells), ctypes.POINTER(Pairs), ll, vp, vp, vp, vp], i),
+        "dftk_jk_workspace_bytes": ([i, i], sz),
+        "dftk_jk": ([ctypes.POINTER(Shells), ctypes.POINTER(Pairs), ctypes.POINTER(Queue), vp, vp, vp,
+                     vp, vp, vp, i, d, d, vp, sz, vp, vp], i),
+        "dftk_nuclear_kernel": ([vp] * 8 + [i, i, i] + [vp] * 9 + [vp], i),
+        "dftk_eri_kernel": ([i] + [vp] * 8 + [i] + [vp] * 8 + [vp, vp], i),
+        "dftk_fma_burn": ([i, i, i, i, vp, vp], i),
+        "dftk_jk_timing": ([i], i),
+        "dftk_jk_timing_read": ([vp, i], i),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+def call(name: str, *args) -> None:
+    lib = load()
+    st = getattr(lib, name)(*args)
+    if st != OK:
+        msg = lib.dftk_last_error()
+        raise DftkError(name, st, msg.decode() if msg else "")
+
+
+def stream_handle(stream=None) -> ctypes.c_void_p:
+    import torch
+
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def ptr(t) -> ctypes.c_void_p:
+    """Device pointer of a CUDA tensor (None -> NULL)."""
+    if t is None:
+        return ctypes.c_void_p(0)
+    if not t.is_cuda:
+        raise DftkError("ptr", ERR_ARG, "expected a CUDA tensor")
+    if not t.is_contiguous():
+        raise DftkError("ptr", ERR_ARG, "expected a contiguous tensor")
+    return ctypes.c_void_p(t.data_ptr())

@@ -1,0 +1,34 @@
+// Shared definitions for libdftk (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "dftk.h"
+
+#define DFTK_PI 3.14159265358979323846
+#define DFTK_FULL_MASK 0xffffffffu
+
+// sqrt(2 pi^{5/2}): split evenly between the bra and ket pair prefactors so
+// that (bra K)(ket K) rsqrt(p+q) = 2 pi^{5/2} / (p q sqrt(p+q)) K_AB K_CD.
+#define DFTK_SQRT_2PI52 5.9149671727956128778
+
+// Field indices of a primitive-pair record (see dftk_pairs_t).
+enum { F_PX = 0, F_PY, F_PZ, F_P, F_K, F_H, F_AX, F_AY, F_AZ, F_BX, F_BY, F_BZ };
+
+__host__ __device__ constexpr int pair_fields(int pc) { return pc == 0 ? 5 : (pc == 1 ? 9 : 12); }
+
+template <typename T> struct Math;
+template <> struct Math<double> {
+    __device__ __forceinline__ static double rsqrt(double x) { return ::rsqrt(x); }
+};
+template <> struct Math<float> {
+    __device__ __forceinline__ static float rsqrt(float x) { return ::rsqrtf(x); }
+};
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(DFTK_FULL_MASK, v, o);
+    return v;
+}

@@ -1,0 +1,414 @@
+// libdftk: C-ABI entry points (declared in include/dftk.h).
+//
+// One translation unit: the device tables (g_boys64/g_boys32) and all kernels
+// live here, so the library needs no relocatable device code.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "boys.cuh"
+#include "common.cuh"
+#include "generic.cuh"
+#include "jk.cuh"
+#include "onee.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+std::mutex g_init_mutex;
+bool g_init_done[128] = {false};
+std::vector<double> g_tab64;
+std::vector<float> g_tab32;
+
+int fail(int code, const char *what)
+{
+    g_last_error = what;
+    return code;
+}
+
+int fail_cuda(cudaError_t e, const char *where)
+{
+    g_last_error = std::string(where) + ": " + cudaGetErrorString(e);
+    return DFTK_ERR_CUDA;
+}
+
+#define DFTK_CUDA(call)                                                     \
+    do {                                                                    \
+        cudaError_t e_ = (call);                                            \
+        if (e_ != cudaSuccess) return fail_cuda(e_, #call);                 \
+    } while (0)
+
+#define DFTK_LAUNCHED(name)                                                 \
+    do {                                                                    \
+        cudaError_t e_ = cudaGetLastError();                                \
+        if (e_ != cudaSuccess) return fail_cuda(e_, name);                  \
+    } while (0)
+
+// F_m(T) = exp(-T) sum_i (2T)^i / ((2m+1)(2m+3)...(2m+2i+1)), all terms
+// positive, summed in long double until they stop contributing.
+long double boys_series_ld(int m, long double T)
+{
+    long double term = 1.0L / (2 * m + 1);
+    long double sum = term;
+    for (int i = 1; i < 2000; ++i) {
+        term *= 2.0L * T / (2 * m + 2 * i + 1);
+        sum += term;
+        if (term < sum * 1e-22L && i > T) break;
+    }
+    return expl(-T) * sum;
+}
+
+void build_tables()
+{
+    if (!g_tab64.empty()) return;
+    g_tab64.assign(DFTK_BOYS_ROWS * DFTK_BOYS_COLS, 0.0);
+    g_tab32.assign(DFTK_BOYS_ROWS * DFTK_BOYS_COLS, 0.0f);
+    for (int k = 0; k < DFTK_BOYS_ROWS; ++k) {
+        const double t64 = (double)k * 0.1;         // grid the FP64 evaluator rounds to
+        const float t32f = (float)k * 0.1f;         // grid the FP32 evaluator rounds to
+        const long double t32 = (long double)t32f;
+        for (int m = 0; m < DFTK_BOYS_EXPCOL; ++m) {
+            g_tab64[k * DFTK_BOYS_COLS + m] = (double)boys_series_ld(m, (long double)t64);
+            g_tab32[k * DFTK_BOYS_COLS + m] = (float)boys_series_ld(m, t32);
+        }
+        g_tab64[k * DFTK_BOYS_COLS + DFTK_BOYS_EXPCOL] = (double)expl(-(long double)t64);
+        g_tab32[k * DFTK_BOYS_COLS + DFTK_BOYS_EXPCOL] = (float)expl(-t32);
+    }
+}
+
+int ensure_init()
+{
+    int dev = 0;
+    DFTK_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 128) return fail(DFTK_ERR_ARG, "device index out of range");
+    std::lock_guard<std::mutex> lock(g_init_mutex);
+    if (g_init_done[dev]) return DFTK_OK;
+    build_tables();
+    DFTK_CUDA(cudaMemcpyToSymbol(g_boys64, g_tab64.data(), sizeof(double) * g_tab64.size()));
+    DFTK_CUDA(cudaMemcpyToSymbol(g_boys32, g_tab32.data(), sizeof(float) * g_tab32.size()));
+    g_init_done[dev] = true;
+    return DFTK_OK;
+}
+
+#define DFTK_INIT()                                                         \
+    do {                                                                    \
+        int s_ = ensure_init();                                             \
+        if (s_ != DFTK_OK) return s_;                                       \
+    } while (0)
+
+inline unsigned blocks_for(long long n, int threads)
+{
+    return (unsigned)((n + threads - 1) / threads);
+}
+
+// Workspace layout of dftk_jk: Y, Za, Zb (N*N doubles each), then Dsh (ns*ns floats).
+size_t ws_bytes(int ns, int n_ao)
+{
+    const size_t nn = (size_t)n_ao * n_ao;
+    size_t b = 3 * nn * sizeof(double);
+    b += (size_t)ns * ns * sizeof(float);
+    return (b + 255) & ~(size_t)255;
+}
+
+// Optional per-class event timing of dftk_jk (dftk_jk_timing).
+struct JkTiming {
+    bool enabled = false;
+    bool created = false;
+    bool launched[2 * DFTK_N_QCLASS] = {false};
+    cudaEvent_t start[2 * DFTK_N_QCLASS];
+    cudaEvent_t stop[2 * DFTK_N_QCLASS];
+};
+JkTiming g_timing;
+std::mutex g_timing_mutex;
+
+template <int C, typename T>
+int launch_jk_class(const JkParams &P, cudaStream_t s)
+{
+    const long long ncand = P.total[C];
+    const int slot = C + (sizeof(T) == 4 ? DFTK_N_QCLASS : 0);
+    if (g_timing.enabled) g_timing.launched[slot] = false;
+    if (ncand <= 0) return DFTK_OK;
+    const long long warps = ((ncand + 31) / 32) * EriClass<T, C, 0>::NSPLIT;
+    long long blocks = (warps * 32 + 127) / 128;
+    const long long cap = 148LL * 16;
+    if (blocks > cap) blocks = cap;
+    if (g_timing.enabled) DFTK_CUDA(cudaEventRecord(g_timing.start[slot], s));
+    k_jk<C, T><<<(unsigned)blocks, 128, 0, s>>>(P);
+    DFTK_LAUNCHED("k_jk");
+    if (g_timing.enabled) {
+        DFTK_CUDA(cudaEventRecord(g_timing.stop[slot], s));
+        g_timing.launched[slot] = true;
+    }
+    return DFTK_OK;
+}
+
+template <typename T>
+int launch_jk_all(const JkParams &P, cudaStream_t s)
+{
+    int st;
+    if ((st = launch_jk_class<0, T>(P, s))) return st;
+    if ((st = launch_jk_class<1, T>(P, s))) return st;
+    if ((st = launch_jk_class<2, T>(P, s))) return st;
+    if ((st = launch_jk_class<3, T>(P, s))) return st;
+    if ((st = launch_jk_class<4, T>(P, s))) return st;
+    if ((st = launch_jk_class<5, T>(P, s))) return st;
+    return DFTK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dftk_version(void) { return 100; }
+
+const char *dftk_last_error(void) { return g_last_error.c_str(); }
+
+int dftk_init(void)
+{
+    g_last_error.clear();
+    return ensure_init();
+}
+
+int dftk_boys(int mmax, long long n, const double *T, double *F, dftk_stream_t stream)
+{
+    if (mmax < 0 || mmax > 8 || n < 0 || (n > 0 && (!T || !F))) return fail(DFTK_ERR_ARG, "dftk_boys: bad arguments (mmax 0..8)");
+    DFTK_INIT();
+    if (n == 0) return DFTK_OK;
+    k_boys_test<<<blocks_for(n, 128), 128, 0, (cudaStream_t)stream>>>(mmax, n, T, F);
+    DFTK_LAUNCHED("k_boys_test");
+    return DFTK_OK;
+}
+
+int dftk_boys32(int mmax, long long n, const float *T, float *F, dftk_stream_t stream)
+{
+    if (mmax < 0 || mmax > 6 || n < 0 || (n > 0 && (!T || !F))) return fail(DFTK_ERR_ARG, "dftk_boys32: bad arguments (mmax 0..6)");
+    DFTK_INIT();
+    if (n == 0) return DFTK_OK;
+    k_boys32_test<<<blocks_for(n, 128), 128, 0, (cudaStream_t)stream>>>(mmax, n, T, F);
+    DFTK_LAUNCHED("k_boys32_test");
+    return DFTK_OK;
+}
+
+int dftk_pair_data(const dftk_shells_t *shells, int pair_class, dftk_pairs_t *pairs, dftk_stream_t stream)
+{
+    if (!shells || !pairs || pair_class < 0 || pair_class > 2) return fail(DFTK_ERR_ARG, "dftk_pair_data: bad arguments");
+    if (pairs->n_pairs < 0 || pairs->kmax <= 0) return fail(DFTK_ERR_ARG, "dftk_pair_data: bad pair counts");
+    DFTK_INIT();
+    const long long n = (long long)pairs->n_pairs * pairs->kmax;
+    if (n == 0) return DFTK_OK;
+    k_pair_data<<<blocks_for(n, 128), 128, 0, (cudaStream_t)stream>>>(*shells, *pairs, pair_fields(pair_class));
+    DFTK_LAUNCHED("k_pair_data");
+    return DFTK_OK;
+}
+
+int dftk_schwarz(const dftk_shells_t *shells, int pair_class, dftk_pairs_t *pairs, dftk_stream_t stream)
+{
+    if (!shells || !pairs || pair_class < 0 || pair_class > 2) return fail(DFTK_ERR_ARG, "dftk_schwarz: bad arguments");
+    DFTK_INIT();
+    const int n = pairs->n_pairs;
+    if (n == 0) return DFTK_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (pair_class == 0) k_schwarz<0><<<blocks_for(n, 64), 64, 0, s>>>(*pairs);
+    else if (pair_class == 1) k_schwarz<1><<<blocks_for(n, 64), 64, 0, s>>>(*pairs);
+    else k_schwarz<2><<<blocks_for(n, 64), 64, 0, s>>>(*pairs);
+    DFTK_LAUNCHED("k_schwarz");
+    return DFTK_OK;
+}
+
+int dftk_one_electron(const dftk_shells_t *shells, int n_atoms, const double *atom_xyz,
+                      const double *atom_z, double *S, double *T, double *V, dftk_stream_t stream)
+{
+    if (!shells || n_atoms < 0 || !S || !T || !V || (n_atoms > 0 && (!atom_xyz || !atom_z)))
+        return fail(DFTK_ERR_ARG, "dftk_one_electron: bad arguments");
+    DFTK_INIT();
+    const long long npair = (long long)shells->n_shells * (shells->n_shells + 1) / 2;
+    if (npair == 0) return DFTK_OK;
+    k_one_electron<<<blocks_for(npair, 64), 64, 0, (cudaStream_t)stream>>>(*shells, n_atoms, atom_xyz, atom_z, S, T, V);
+    DFTK_LAUNCHED("k_one_electron");
+    return DFTK_OK;
+}
+
+int dftk_eri_blocks(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N_PCLASS], long long n_quartets,
+                    const int *desc, const long long *out_off, double *out, dftk_stream_t stream)
+{
+    if (!shells || !pairs || n_quartets < 0 || (n_quartets > 0 && (!desc || !out_off || !out)))
+        return fail(DFTK_ERR_ARG, "dftk_eri_blocks: bad arguments");
+    DFTK_INIT();
+    if (n_quartets == 0) return DFTK_OK;
+    EmitParams P;
+    P.shell_ao = shells->ao;
+    P.shell_l = shells->l;
+    for (int k = 0; k < 3; ++k) {
+        P.ab[k] = pairs[k].ab;
+        P.np[k] = pairs[k].nprim;
+        P.rec64[k] = pairs[k].rec64;
+        P.n_pairs[k] = pairs[k].n_pairs;
+        P.kmax[k] = pairs[k].kmax;
+    }
+    P.nq = n_quartets;
+    P.desc = desc;
+    P.out_off = out_off;
+    P.out = out;
+    k_emit<<<blocks_for(n_quartets, 64), 64, 0, (cudaStream_t)stream>>>(P);
+    DFTK_LAUNCHED("k_emit");
+    return DFTK_OK;
+}
+
+size_t dftk_jk_workspace_bytes(int n_shells, int n_ao)
+{
+    if (n_shells < 0 || n_ao < 0) return 0;
+    return ws_bytes(n_shells, n_ao);
+}
+
+int dftk_jk(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N_PCLASS], const dftk_queue_t *queue,
+            const double *D, const double *D_a, const double *D_b, double *J, double *K_a, double *K_b,
+            int flags, double tau, double tau_fp32, void *workspace, size_t workspace_bytes,
+            long long *counts, dftk_stream_t stream)
+{
+    if (!shells || !pairs || !queue || !D || !D_a || !J || !K_a || !workspace)
+        return fail(DFTK_ERR_ARG, "dftk_jk: null argument");
+    const int uhf = (flags & DFTK_JK_UHF) != 0;
+    const int mixed = (flags & DFTK_JK_MIXED) != 0;
+    if (uhf && (!D_b || !K_b)) return fail(DFTK_ERR_ARG, "dftk_jk: UHF needs D_b and K_b");
+    if (!(tau >= 0.0) || (mixed && !(tau_fp32 >= tau))) return fail(DFTK_ERR_ARG, "dftk_jk: bad thresholds");
+    const int ns = shells->n_shells, N = shells->n_ao;
+    if (workspace_bytes < ws_bytes(ns, N)) return fail(DFTK_ERR_WORKSPACE, "dftk_jk: workspace too small");
+    DFTK_INIT();
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t nn = (size_t)N * N;
+    double *Y = (double *)workspace;
+    double *Za = Y + nn;
+    double *Zb = Za + nn;
+    float *Dsh = (float *)(Zb + nn);
+    DFTK_CUDA(cudaMemsetAsync(Y, 0, 3 * nn * sizeof(double), s));
+    if (ns > 0) {
+        k_dsh<<<blocks_for((long long)ns * ns, 128), 128, 0, s>>>(shells->ao, shells->l, ns, N, D, D_a,
+                                                                  uhf ? D_b : D_a, uhf, Dsh);
+        DFTK_LAUNCHED("k_dsh");
+    }
+    JkParams P;
+    memset(&P, 0, sizeof(P));
+    P.shell_ao = shells->ao;
+    P.N = N;
+    P.ns = ns;
+    for (int k = 0; k < 3; ++k) {
+        P.ab[k] = pairs[k].ab;
+        P.np[k] = pairs[k].nprim;
+        P.rec64[k] = pairs[k].rec64;
+        P.rec32[k] = pairs[k].rec32;
+        P.q[k] = pairs[k].q;
+        P.n_pairs[k] = pairs[k].n_pairs;
+        P.kmax[k] = pairs[k].kmax;
+    }
+    for (int c = 0; c < DFTK_N_QCLASS; ++c) {
+        P.n_rows[c] = queue->n_rows[c];
+        P.row_off[c] = queue->row_off[c];
+        P.total[c] = queue->n_rows[c] > 0 ? queue->total[c] : 0;
+        if (P.total[c] < 0) return fail(DFTK_ERR_ARG, "dftk_jk: negative candidate total");
+        if (P.total[c] > 0 && !queue->row_off[c]) return fail(DFTK_ERR_ARG, "dftk_jk: missing row offsets");
+    }
+    P.D = D;
+    P.Da = D_a;
+    P.Db = uhf ? D_b : D_a;
+    P.Y = Y;
+    P.Za = Za;
+    P.Zb = Zb;
+    P.Dsh = Dsh;
+    P.uhf = uhf;
+    int st;
+    P.tau_lo = tau;
+    P.tau_hi = INFINITY;
+    if (mixed) {
+        P.tau_lo = tau_fp32;
+        P.counts = counts;
+        if ((st = launch_jk_all<double>(P, s))) return st;
+        P.tau_lo = tau;
+        P.tau_hi = tau_fp32;
+        P.counts = counts ? counts + DFTK_N_QCLASS : nullptr;
+        if ((st = launch_jk_all<float>(P, s))) return st;
+    } else {
+        P.counts = counts;
+        if ((st = launch_jk_all<double>(P, s))) return st;
+    }
+    k_symmetrize<<<blocks_for((long long)nn, 256), 256, 0, s>>>(N, Y, Za, Zb, J, K_a, K_b, uhf);
+    DFTK_LAUNCHED("k_symmetrize");
+    return DFTK_OK;
+}
+
+int dftk_jk_timing(int enable)
+{
+    std::lock_guard<std::mutex> lock(g_timing_mutex);
+    if (enable && !g_timing.created) {
+        for (int k = 0; k < 2 * DFTK_N_QCLASS; ++k) {
+            DFTK_CUDA(cudaEventCreate(&g_timing.start[k]));
+            DFTK_CUDA(cudaEventCreate(&g_timing.stop[k]));
+        }
+        g_timing.created = true;
+    }
+    g_timing.enabled = enable != 0;
+    for (int k = 0; k < 2 * DFTK_N_QCLASS; ++k) g_timing.launched[k] = false;
+    return DFTK_OK;
+}
+
+int dftk_jk_timing_read(float *ms, int n)
+{
+    if (!ms || n < 2 * DFTK_N_QCLASS) return fail(DFTK_ERR_ARG, "dftk_jk_timing_read: need 12 floats");
+    std::lock_guard<std::mutex> lock(g_timing_mutex);
+    for (int k = 0; k < 2 * DFTK_N_QCLASS; ++k) {
+        ms[k] = 0.0f;
+        if (g_timing.created && g_timing.launched[k]) {
+            DFTK_CUDA(cudaEventSynchronize(g_timing.stop[k]));
+            DFTK_CUDA(cudaEventElapsedTime(&ms[k], g_timing.start[k], g_timing.stop[k]));
+        }
+    }
+    return DFTK_OK;
+}
+
+int dftk_nuclear_kernel(const double *exp_a, const double *exp_b, const double *cen_a, const double *cen_b,
+                        const int *pow_a, const int *pow_b, const int *atoms, const double *atom_centers,
+                        int num_atoms, int num_funcs_a, int num_funcs_b, double *V_output, double *Ex_output,
+                        double *Ey_output, double *Ez_output, double *p_output, double *P_output, int *nx_output,
+                        int *ny_output, int *nz_output, dftk_stream_t stream)
+{
+    if (num_funcs_a < 0 || num_funcs_b < 0 || num_atoms < 0) return fail(DFTK_ERR_ARG, "dftk_nuclear_kernel: negative size");
+    DFTK_INIT();
+    const long long n = (long long)num_funcs_a * num_funcs_b;
+    if (n == 0) return DFTK_OK;
+    k_nuclear_dropin<<<blocks_for(n, 128), 128, 0, (cudaStream_t)stream>>>(
+        exp_a, exp_b, cen_a, cen_b, pow_a, pow_b, atoms, atom_centers, num_atoms, num_funcs_a, num_funcs_b,
+        V_output, Ex_output, Ey_output, Ez_output, p_output, P_output, nx_output, ny_output, nz_output);
+    DFTK_LAUNCHED("k_nuclear_dropin");
+    return DFTK_OK;
+}
+
+int dftk_eri_kernel(int K_ab, const double *p_ab, const double *P_ab, const double *Exab, const double *Eyab,
+                    const double *Ezab, const int *nxab, const int *nyab, const int *nzab, int K_cd,
+                    const double *p_cd, const double *P_cd, const double *Excd, const double *Eycd,
+                    const double *Ezcd, const int *nxcd, const int *nycd, const int *nzcd, double *eri_output,
+                    dftk_stream_t stream)
+{
+    if (K_ab < 0 || K_cd < 0) return fail(DFTK_ERR_ARG, "dftk_eri_kernel: negative size");
+    DFTK_INIT();
+    const long long n = (long long)K_ab * K_cd;
+    if (n == 0) return DFTK_OK;
+    k_eri_dropin<<<blocks_for(n, 128), 128, 0, (cudaStream_t)stream>>>(
+        K_ab, p_ab, P_ab, Exab, Eyab, Ezab, nxab, nyab, nzab, K_cd, p_cd, P_cd, Excd, Eycd, Ezcd, nxcd, nycd,
+        nzcd, eri_output);
+    DFTK_LAUNCHED("k_eri_dropin");
+    return DFTK_OK;
+}
+
+int dftk_fma_burn(int precision, int blocks, int threads, int iters, double *sink, dftk_stream_t stream)
+{
+    if ((precision != 64 && precision != 32) || blocks <= 0 || threads <= 0 || threads > 1024 || iters < 0 || !sink)
+        return fail(DFTK_ERR_ARG, "dftk_fma_burn: bad arguments");
+    if (precision == 64) k_fma_burn<double><<<blocks, threads, 0, (cudaStream_t)stream>>>(iters, sink);
+    else k_fma_burn<float><<<blocks, threads, 0, (cudaStream_t)stream>>>(iters, sink);
+    DFTK_LAUNCHED("k_fma_burn");
+    return DFTK_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,260 @@
+"""Generate straight-line McMurchie-Davidson code for the s/p ERI classes.
+
+Writes ``eri_classes.cuh`` next to this file.  Run it after changing the
+class table; the generated header is committed so a build needs no Python.
+
+For every angular class (La Lb | Lc Ld) with La >= Lb, Lc >= Ld and
+La + Lb >= Lc + Ld (s = 0, p = 1) it emits one device function per
+ket-component split.  The function evaluates the contracted Cartesian block
+of one shell quartet from primitive-pair records:
+
+    (ab|cd) = sum_{ij} sum_{tuv} E^{ab}_{tuv}(i) sum_{kl}
+              sum_{tau nu phi} (-1)^{tau+nu+phi} E^{cd}_{tau nu phi}(kl) R_{t+tau,u+nu,v+phi}(i, kl)
+
+with the bra Hermite-to-Cartesian transform hoisted out of the ket primitive
+loop (W holds the ket-transformed, ket-primitive-summed Hermite integrals of
+one bra primitive).  Only non-zero Hermite coefficients are emitted.
+
+Primitive-pair record fields (SoA, ``base[(f * kmax + k) * stride + pair]``):
+    0 Px, 1 Py, 2 Pz, 3 p, 4 K (sqrt(2 pi^{5/2}) c_a c_b N_a N_b exp(-mu AB^2) / p),
+    5 h = 1/(2p), 6-8 PA = P - A, 9-11 PB = P - B.
+ss pairs use fields 0-4, ps pairs 0-8, pp pairs 0-11.
+"""
+from __future__ import annotations
+
+import itertools
+import os
+
+AX = "xyz"
+COMPS = {0: [(0, 0, 0)], 1: [(1, 0, 0), (0, 1, 0), (0, 0, 1)]}
+# (La, Lb, Lc, Ld, nsplit); nsplit > 1 splits the c components across threads
+CLASSES = [
+    (0, 0, 0, 0, 1),
+    (1, 0, 0, 0, 1),
+    (1, 0, 1, 0, 1),
+    (1, 1, 0, 0, 1),
+    (1, 1, 1, 0, 1),
+    (1, 1, 1, 1, 3),
+]
+PAIR_FIELDS = {0: 5, 1: 9, 2: 12}
+
+
+def e1d(side, a, b, axis):
+    """Non-zero 1-D Hermite coefficients {t: expr} for powers (a, b) on an axis."""
+    x = AX[axis]
+    if (a, b) == (0, 0):
+        return {0: None}
+    if (a, b) == (1, 0):
+        return {0: f"{side}A{x}", 1: f"{side}h"}
+    if (a, b) == (0, 1):
+        return {0: f"{side}B{x}", 1: f"{side}h"}
+    return {0: f"{side}E{x}0", 1: f"{side}E{x}1", 2: f"{side}h2"}
+
+
+def e3d(side, ca, cb, sign=False):
+    """List of ((t,u,v), sign, factors) for the product of three 1-D expansions."""
+    out = []
+    per_axis = [e1d(side, ca[k], cb[k], k) for k in range(3)]
+    for t, u, v in itertools.product(*[sorted(d) for d in per_axis]):
+        facs = [f for f in (per_axis[0][t], per_axis[1][u], per_axis[2][v]) if f is not None]
+        sg = -1 if (sign and (t + u + v) % 2) else 1
+        out.append(((t, u, v), sg, facs))
+    return out
+
+
+def herm(L):
+    return [(t, u, v) for t in range(L + 1) for u in range(L + 1) for v in range(L + 1) if t + u + v <= L]
+
+
+def rname(t, u, v, n):
+    return f"R{t}{u}{v}_{n}"
+
+
+def r_program(needed, L):
+    """Emit R^{(n)}_{tuv} definitions closing `needed` under the MD recursion."""
+    need = set()
+
+    def add(t, u, v, n):
+        if (t, u, v, n) in need:
+            return
+        need.add((t, u, v, n))
+        if t > 0:
+            add(t - 1, u, v, n + 1)
+            if t > 1:
+                add(t - 2, u, v, n + 1)
+        elif u > 0:
+            add(t, u - 1, v, n + 1)
+            if u > 1:
+                add(t, u - 2, v, n + 1)
+        elif v > 0:
+            add(t, u, v - 1, n + 1)
+            if v > 1:
+                add(t, u, v - 2, n + 1)
+
+    for t, u, v in needed:
+        add(t, u, v, 0)
+    lines = []
+    base_n = sorted(n for (t, u, v, n) in need if t + u + v == 0)
+    maxn = max(base_n)
+    lines.append("T cpow = pre;")
+    for n in range(maxn + 1):
+        if n > 0:
+            lines.append("cpow *= m2rho;")
+        if n in base_n:
+            lines.append(f"const T {rname(0, 0, 0, n)} = cpow * F[{n}];")
+    for (t, u, v, n) in sorted(need, key=lambda k: (k[0] + k[1] + k[2], -k[3], k)):
+        if t + u + v == 0:
+            continue
+        if t > 0:
+            e = f"X * {rname(t - 1, u, v, n + 1)}"
+            if t > 1:
+                e += f" + T({t - 1}) * {rname(t - 2, u, v, n + 1)}"
+        elif u > 0:
+            e = f"Y * {rname(t, u - 1, v, n + 1)}"
+            if u > 1:
+                e += f" + T({u - 1}) * {rname(t, u - 2, v, n + 1)}"
+        else:
+            e = f"Z * {rname(t, u, v - 1, n + 1)}"
+            if v > 1:
+                e += f" + T({v - 1}) * {rname(t, u, v - 2, n + 1)}"
+        lines.append(f"const T {rname(t, u, v, n)} = {e};")
+    return lines
+
+
+def prod(facs):
+    return " * ".join(facs) if facs else "T(1)"
+
+
+def side_loads(side, pc, var, idx):
+    """Load the fields of one primitive pair record."""
+    names = ["Px", "Py", "Pz", "p", "K", "h", "Ax", "Ay", "Az", "Bx", "By", "Bz"]
+    n = PAIR_FIELDS[pc]
+    out = []
+    for f in range(n):
+        out.append(f"const T {side}{names[f]} = {var}[({f} * {var}_kmax + {idx}) * {var}_stride + {var}_row];")
+    return out
+
+
+def side_pre(side, pc):
+    lines = []
+    if pc == 2:
+        for x in AX:
+            lines.append(f"const T {side}E{x}0 = {side}A{x} * {side}B{x} + {side}h;")
+            lines.append(f"const T {side}E{x}1 = {side}h * ({side}A{x} + {side}B{x});")
+        lines.append(f"const T {side}h2 = {side}h * {side}h;")
+    return lines
+
+
+def gen_class(cid, la, lb, lc, ld, nsplit, split):
+    pa, pk = la + lb, lc + ld
+    L = pa + pk
+    A, B, C, D = COMPS[la], COMPS[lb], COMPS[lc], COMPS[ld]
+    cds = [(ic, id_) for ic in range(len(C)) for id_ in range(len(D))]
+    if nsplit > 1:
+        cds = [(ic, id_) for (ic, id_) in cds if ic == split]
+    abs_ = [(ia, ib) for ia in range(len(A)) for ib in range(len(B))]
+    hb = herm(pa)
+    # ket expansions per local cd
+    ket_terms = {m: e3d("k", C[ic], D[id_], sign=True) for m, (ic, id_) in enumerate(cds)}
+    bra_terms = {n: e3d("b", A[ia], B[ib]) for n, (ia, ib) in enumerate(abs_)}
+    needed = set()
+    for m, terms in ket_terms.items():
+        for (tk, uk, vk), _, _ in terms:
+            for (tb, ub, vb) in hb:
+                needed.add((tb + tk, ub + uk, vb + vk))
+    body = []
+    w = lambda m, h: f"W{m}_{h[0]}{h[1]}{h[2]}"
+    body.append("#pragma unroll 1")
+    body.append("for (int i = 0; i < bra_n; ++i) {")
+    body += ["  " + s for s in side_loads("b", pa, "bra", "i")]
+    body += ["  " + s for s in side_pre("b", pa)]
+    for m in range(len(cds)):
+        body.append("  T " + ", ".join(f"{w(m, h)} = T(0)" for h in hb) + ";")
+    body.append("  #pragma unroll 1")
+    body.append("  for (int j = 0; j < ket_n; ++j) {")
+    inner = []
+    inner += side_loads("k", pk, "ket", "j")
+    inner += side_pre("k", pk)
+    inner.append("const T s = bp + kp;")
+    inner.append("const T rs = Math<T>::rsqrt(s);")
+    inner.append("const T rho = bp * kp * (rs * rs);")
+    inner.append("const T X = bPx - kPx, Y = bPy - kPy, Z = bPz - kPz;")
+    inner.append("const T pre = bK * kK * rs;")
+    inner.append("const T m2rho = T(-2) * rho;")
+    inner.append(f"T F[{L + 1}];")
+    inner.append(f"Boys<T, {L}>::eval(rho * (X * X + Y * Y + Z * Z), F);")
+    inner += r_program(sorted(needed), L)
+    # ket coefficients, then W accumulation
+    for m, terms in ket_terms.items():
+        for (tk, uk, vk), sg, facs in terms:
+            cname = f"kc{m}_{tk}{uk}{vk}"
+            if facs:
+                expr = prod(facs)
+                inner.append(f"const T {cname} = {'-' if sg < 0 else ''}{expr};")
+            for (tb, ub, vb) in hb:
+                r = rname(tb + tk, ub + uk, vb + vk, 0)
+                tgt = w(m, (tb, ub, vb))
+                if facs:
+                    inner.append(f"{tgt} = fma({cname}, {r}, {tgt});")
+                else:
+                    op = "-=" if sg < 0 else "+="
+                    inner.append(f"{tgt} {op} {r};")
+    body += ["    " + s for s in inner]
+    body.append("  }")
+    # bra transform
+    for n, terms in bra_terms.items():
+        for m in range(len(cds)):
+            acc = f"I[{n * len(cds) + m}]"
+            for (tb, ub, vb), _, facs in terms:
+                src = w(m, (tb, ub, vb))
+                if facs:
+                    body.append(f"  {acc} = fma({prod(facs)}, {src}, {acc});")
+                else:
+                    body.append(f"  {acc} += {src};")
+    body.append("}")
+    nloc = len(abs_) * len(cds)
+    cd_c = ", ".join(str(ic) for ic, _ in cds)
+    cd_d = ", ".join(str(id_) for _, id_ in cds)
+    head = [
+        f"// class {cid}: ({'sp'[la]}{'sp'[lb]}|{'sp'[lc]}{'sp'[ld]}), split {split} of {nsplit}",
+        "template <typename T>",
+        f"struct EriClass<T, {cid}, {split}> {{",
+        f"  static constexpr int LA = {la}, LB = {lb}, LC = {lc}, LD = {ld}, L = {L};",
+        f"  static constexpr int NA = {len(A)}, NB = {len(B)}, NC = {len(C)}, ND = {len(D)};",
+        f"  static constexpr int NSPLIT = {nsplit}, NCD = {len(cds)}, NI = {nloc};",
+        f"  static constexpr int BRA_CLASS = {pa}, KET_CLASS = {pk};",
+        f"  __device__ static constexpr int cd_c(int m) {{ constexpr int v[] = {{{cd_c}}}; return v[m]; }}",
+        f"  __device__ static constexpr int cd_d(int m) {{ constexpr int v[] = {{{cd_d}}}; return v[m]; }}",
+        "  __device__ __forceinline__ static void run(",
+        "      const T* __restrict__ bra, long long bra_stride, int bra_kmax, int bra_row, int bra_n,",
+        "      const T* __restrict__ ket, long long ket_stride, int ket_kmax, int ket_row, int ket_n,",
+        "      T (&I)[NI]) {",
+        f"    #pragma unroll",
+        f"    for (int q = 0; q < NI; ++q) I[q] = T(0);",
+    ]
+    tail = ["  }", "};", ""]
+    return head + ["    " + s for s in body] + tail
+
+
+def main():
+    out = [
+        "// GENERATED by gen_eri.py -- do not edit by hand.",
+        "// Straight-line McMurchie-Davidson bodies for the s/p ERI classes.",
+        "#pragma once",
+        "",
+        "template <typename T, int C, int S> struct EriClass;",
+        "",
+        f"#define DFTK_N_CLASSES {len(CLASSES)}",
+        "",
+    ]
+    for cid, (la, lb, lc, ld, ns) in enumerate(CLASSES):
+        for s in range(ns):
+            out += gen_class(cid, la, lb, lc, ld, ns, s)
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "eri_classes.cuh")
+    with open(path, "w") as fh:
+        fh.write("\n".join(out) + "\n")
+    print(path)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,424 @@
+// Pair data, Schwarz factors, integral-direct J/K and ERI-block kernels.
+#pragma once
+
+#include "boys.cuh"
+#include "common.cuh"
+#include "eri_classes.cuh"
+
+// ----------------------------------------------------------------- pair data
+// One thread per (primitive slot k, pair); pair index fastest so the SoA
+// record writes are coalesced.  Replaces the per-pair nuclear_kernel launch
+// and pair_cache dict (shelled.py:1000-1059) for the ERI path.
+__global__ void k_pair_data(const dftk_shells_t sh, const dftk_pairs_t pr, int nfields)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = pr.n_pairs;
+    if (t >= (long long)n * pr.kmax) return;
+    const int pair = (int)(t % n);
+    const int k = (int)(t / n);
+    const int a = pr.ab[2 * pair], b = pr.ab[2 * pair + 1];
+    const int na = sh.nprim[a], nb = sh.nprim[b];
+    if (k == 0) pr.nprim[pair] = na * nb;
+    double f[12];
+#pragma unroll
+    for (int i = 0; i < 12; ++i) f[i] = 0.0;
+    if (k < na * nb) {
+        const int ia = k / nb, ib = k % nb;
+        const double al = sh.prim_exp[sh.prim_off[a] + ia];
+        const double be = sh.prim_exp[sh.prim_off[b] + ib];
+        const double ca = sh.prim_cn[sh.prim_off[a] + ia];
+        const double cb = sh.prim_cn[sh.prim_off[b] + ib];
+        const double Ax = sh.xyz[3 * a], Ay = sh.xyz[3 * a + 1], Az = sh.xyz[3 * a + 2];
+        const double Bx = sh.xyz[3 * b], By = sh.xyz[3 * b + 1], Bz = sh.xyz[3 * b + 2];
+        const double p = al + be;
+        const double ip = 1.0 / p;
+        const double Px = (al * Ax + be * Bx) * ip;
+        const double Py = (al * Ay + be * By) * ip;
+        const double Pz = (al * Az + be * Bz) * ip;
+        const double ab2 = (Ax - Bx) * (Ax - Bx) + (Ay - By) * (Ay - By) + (Az - Bz) * (Az - Bz);
+        f[F_PX] = Px; f[F_PY] = Py; f[F_PZ] = Pz; f[F_P] = p;
+        f[F_K] = DFTK_SQRT_2PI52 * ca * cb * exp(-al * be * ip * ab2) * ip;
+        f[F_H] = 0.5 * ip;
+        f[F_AX] = Px - Ax; f[F_AY] = Py - Ay; f[F_AZ] = Pz - Az;
+        f[F_BX] = Px - Bx; f[F_BY] = Py - By; f[F_BZ] = Pz - Bz;
+    }
+    for (int i = 0; i < nfields; ++i) {
+        const long long o = ((long long)i * pr.kmax + k) * n + pair;
+        pr.rec64[o] = f[i];
+        pr.rec32[o] = (float)f[i];
+    }
+}
+
+// ------------------------------------------------------------------ helpers
+template <int C, typename T, int S>
+__device__ __forceinline__ void eri_run(const T *bra, int bra_n_pairs, int bra_kmax, int bra_row,
+                                        int bra_np, const T *ket, int ket_n_pairs, int ket_kmax,
+                                        int ket_row, int ket_np, T (&I)[EriClass<T, C, S>::NI])
+{
+    EriClass<T, C, S>::run(bra, bra_n_pairs, bra_kmax, bra_row, bra_np, ket, ket_n_pairs, ket_kmax,
+                           ket_row, ket_np, I);
+}
+
+// Diagonal class of a pair class: ss -> (ss|ss), ps -> (ps|ps), pp -> (pp|pp).
+template <int PC> struct DiagClass { static constexpr int C = PC == 0 ? 0 : (PC == 1 ? 2 : 5); };
+
+template <int C, int S>
+__device__ __forceinline__ double diag_max(const dftk_pairs_t &pr, int pair)
+{
+    double I[EriClass<double, C, S>::NI];
+    const int np = pr.nprim[pair];
+    eri_run<C, double, S>(pr.rec64, pr.n_pairs, pr.kmax, pair, np, pr.rec64, pr.n_pairs, pr.kmax,
+                          pair, np, I);
+    double m = 0.0;
+#pragma unroll
+    for (int q = 0; q < EriClass<double, C, S>::NI; ++q) m = fmax(m, fabs(I[q]));
+    return m;
+}
+
+// Schwarz factor Q_ab = sqrt(max |(ab|ab)|), one thread per pair.
+template <int PC>
+__global__ void k_schwarz(const dftk_pairs_t pr)
+{
+    const int pair = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pair >= pr.n_pairs) return;
+    constexpr int C = DiagClass<PC>::C;
+    double m = diag_max<C, 0>(pr, pair);
+    if constexpr (EriClass<double, C, 0>::NSPLIT > 1) {
+        m = fmax(m, diag_max<C, 1>(pr, pair));
+        m = fmax(m, diag_max<C, 2>(pr, pair));
+    }
+    pr.q[pair] = sqrt(m);
+}
+
+// ------------------------------------------------------------------- J / K
+struct JkParams {
+    const int *shell_ao;
+    int N, ns;
+    const int *ab[3];
+    const int *np[3];
+    const double *rec64[3];
+    const float *rec32[3];
+    const double *q[3];
+    int n_pairs[3];
+    int kmax[3];
+    long long n_rows[DFTK_N_QCLASS];
+    long long total[DFTK_N_QCLASS];
+    const long long *row_off[DFTK_N_QCLASS];
+    const double *D, *Da, *Db;
+    double *Y, *Za, *Zb;
+    const float *Dsh;
+    int uhf;
+    double tau_lo, tau_hi;  // quartet processed if tau_lo <= bound < tau_hi
+    long long *counts;
+};
+
+// largest r in [0, n_rows) with off[r] <= cand
+__device__ __forceinline__ int find_row(const long long *off, long long n_rows, long long cand)
+{
+    long long lo = 0, hi = n_rows - 1;
+    while (lo < hi) {
+        const long long mid = (lo + hi + 1) >> 1;
+        if (__ldg(off + mid) <= cand) lo = mid; else hi = mid - 1;
+    }
+    return (int)lo;
+}
+
+// Shell-block maxima of |D| (and |D_a|, |D_b| for UHF): Dsh[x * ns + y].
+__global__ void k_dsh(const int *shell_ao, const int *shell_l, int ns, int N, const double *D,
+                      const double *Da, const double *Db, int uhf, float *Dsh)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ns * ns) return;
+    const int x = t / ns, y = t % ns;
+    const int ox = shell_ao[x], oy = shell_ao[y];
+    const int nx = (shell_l[x] + 1) * (shell_l[x] + 2) / 2, ny = (shell_l[y] + 1) * (shell_l[y] + 2) / 2;
+    double m = 0.0;
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j) {
+            const long long o = (long long)(ox + i) * N + oy + j;
+            m = fmax(m, fabs(D[o]));
+            m = fmax(m, fabs(Da[o]));
+            if (uhf) m = fmax(m, fabs(Db[o]));
+        }
+    Dsh[t] = (float)m;
+}
+
+// Digest one contracted block into the half-accumulators Y (J) and Z (K):
+//   Y_ab += 2/w sum_cd I D_cd,  Y_cd += 2/w sum_ab I D_ab,
+//   Z_ac += 1/w sum_bd I D_bd,  Z_ad += 1/w sum_bc I D_bc,
+//   Z_bc += 1/w sum_ad I D_ad,  Z_bd += 1/w sum_ac I D_ac,
+// w = 2^{[a=b]+[c=d]+[ab=cd]}; J = Y + Y^T and K = Z + Z^T afterwards give the
+// eight orientations of fill_matrices (shelled.py:791-859) with its weights.
+template <int C, typename T, int S>
+__device__ __forceinline__ void digest(const JkParams &P, bool valid, bool uniform_bra, int a, int b,
+                                       int c, int d, double w, const T (&I)[EriClass<T, C, S>::NI])
+{
+    using E = EriClass<T, C, S>;
+    constexpr int NA = E::NA, NB = E::NB, NC = E::NC, ND = E::ND, NCD = E::NCD;
+    const int N = P.N;
+    const int oa = P.shell_ao[a], ob = P.shell_ao[b], oc = P.shell_ao[c], od = P.shell_ao[d];
+    const double fJ = valid ? 2.0 / w : 0.0;
+    const double fK = valid ? 1.0 / w : 0.0;
+    double v[E::NI];
+#pragma unroll
+    for (int q = 0; q < E::NI; ++q) v[q] = valid ? (double)I[q] : 0.0;
+    const double *D = P.D;
+    // Y_cd
+#pragma unroll
+    for (int m = 0; m < NCD; ++m) {
+        double s = 0.0;
+#pragma unroll
+        for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+            for (int ib = 0; ib < NB; ++ib)
+                s = fma(v[(ia * NB + ib) * NCD + m], __ldg(D + (long long)(oa + ia) * N + ob + ib), s);
+        if (valid) atomicAdd(P.Y + (long long)(oc + E::cd_c(m)) * N + od + E::cd_d(m), fJ * s);
+    }
+    // Y_ab
+#pragma unroll
+    for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+        for (int ib = 0; ib < NB; ++ib) {
+            double s = 0.0;
+#pragma unroll
+            for (int m = 0; m < NCD; ++m)
+                s = fma(v[(ia * NB + ib) * NCD + m],
+                        __ldg(D + (long long)(oc + E::cd_c(m)) * N + od + E::cd_d(m)), s);
+            s *= fJ;
+            if (uniform_bra) {
+                s = warp_sum(s);
+                if ((threadIdx.x & 31) == 0) atomicAdd(P.Y + (long long)(oa + ia) * N + ob + ib, s);
+            } else if (valid) {
+                atomicAdd(P.Y + (long long)(oa + ia) * N + ob + ib, s);
+            }
+        }
+    // K, one or two spins
+    for (int spin = 0; spin < (P.uhf ? 2 : 1); ++spin) {
+        const double *Ds = spin ? P.Db : P.Da;
+        double *Z = spin ? P.Zb : P.Za;
+        double zac[NA][NC], zad[NA][ND], zbc[NB][NC], zbd[NB][ND];
+#pragma unroll
+        for (int i = 0; i < NA; ++i) {
+#pragma unroll
+            for (int j = 0; j < NC; ++j) zac[i][j] = 0.0;
+#pragma unroll
+            for (int j = 0; j < ND; ++j) zad[i][j] = 0.0;
+        }
+#pragma unroll
+        for (int i = 0; i < NB; ++i) {
+#pragma unroll
+            for (int j = 0; j < NC; ++j) zbc[i][j] = 0.0;
+#pragma unroll
+            for (int j = 0; j < ND; ++j) zbd[i][j] = 0.0;
+        }
+#pragma unroll
+        for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+            for (int ib = 0; ib < NB; ++ib)
+#pragma unroll
+                for (int m = 0; m < NCD; ++m) {
+                    const int cc = E::cd_c(m), dd = E::cd_d(m);
+                    const double val = v[(ia * NB + ib) * NCD + m] * fK;
+                    zac[ia][cc] = fma(val, __ldg(Ds + (long long)(ob + ib) * N + od + dd), zac[ia][cc]);
+                    zad[ia][dd] = fma(val, __ldg(Ds + (long long)(ob + ib) * N + oc + cc), zad[ia][dd]);
+                    zbc[ib][cc] = fma(val, __ldg(Ds + (long long)(oa + ia) * N + od + dd), zbc[ib][cc]);
+                    zbd[ib][dd] = fma(val, __ldg(Ds + (long long)(oa + ia) * N + oc + cc), zbd[ib][dd]);
+                }
+        if (valid) {
+#pragma unroll
+            for (int ia = 0; ia < NA; ++ia) {
+#pragma unroll
+                for (int cc = 0; cc < NC; ++cc)
+                    if (E::NSPLIT == 1 || cc == S)
+                        atomicAdd(Z + (long long)(oa + ia) * N + oc + cc, zac[ia][cc]);
+#pragma unroll
+                for (int dd = 0; dd < ND; ++dd) atomicAdd(Z + (long long)(oa + ia) * N + od + dd, zad[ia][dd]);
+            }
+#pragma unroll
+            for (int ib = 0; ib < NB; ++ib) {
+#pragma unroll
+                for (int cc = 0; cc < NC; ++cc)
+                    if (E::NSPLIT == 1 || cc == S)
+                        atomicAdd(Z + (long long)(ob + ib) * N + oc + cc, zbc[ib][cc]);
+#pragma unroll
+                for (int dd = 0; dd < ND; ++dd) atomicAdd(Z + (long long)(ob + ib) * N + od + dd, zbd[ib][dd]);
+            }
+        }
+    }
+}
+
+template <int C, typename T> struct RecOf;
+template <int C> struct RecOf<C, double> {
+    __device__ static const double *get(const JkParams &P, int pc) { return P.rec64[pc]; }
+};
+template <int C> struct RecOf<C, float> {
+    __device__ static const float *get(const JkParams &P, int pc) { return P.rec32[pc]; }
+};
+
+template <int C, typename T, int S>
+__device__ __forceinline__ void jk_one(const JkParams &P, bool valid, int row, int ket)
+{
+    using E = EriClass<T, C, S>;
+    constexpr int X = E::BRA_CLASS, Yc = E::KET_CLASS;
+    const int *abX = P.ab[X];
+    const int *abY = P.ab[Yc];
+    const int a = valid ? abX[2 * row] : 0, b = valid ? abX[2 * row + 1] : 0;
+    const int c = valid ? abY[2 * ket] : 0, d = valid ? abY[2 * ket + 1] : 0;
+    // warp-uniform bra pair lets the Y_ab reduction happen in registers
+    const int lead = __ffs(__ballot_sync(DFTK_FULL_MASK, valid)) - 1;
+    const int row0 = __shfl_sync(DFTK_FULL_MASK, row, lead < 0 ? 0 : lead);
+    const bool uniform = __all_sync(DFTK_FULL_MASK, !valid || row == row0);
+    T I[E::NI];
+    if (valid) {
+        eri_run<C, T, S>(RecOf<C, T>::get(P, X), P.n_pairs[X], P.kmax[X], row, P.np[X][row],
+                         RecOf<C, T>::get(P, Yc), P.n_pairs[Yc], P.kmax[Yc], ket, P.np[Yc][ket], I);
+    } else {
+#pragma unroll
+        for (int q = 0; q < E::NI; ++q) I[q] = T(0);
+    }
+    const int ew = (a == b) + (c == d) + ((X == Yc) && (row == ket));
+    digest<C, T, S>(P, valid, uniform, a, b, c, d, (double)(1 << ew), I);
+}
+
+// One warp per 32 consecutive candidates of class C (and one split of the
+// c components for the split classes); quartets whose density-weighted
+// Schwarz bound falls outside [tau_lo, tau_hi) are skipped.
+template <int C, typename T>
+__global__ void __launch_bounds__(128) k_jk(const JkParams P)
+{
+    using E0 = EriClass<T, C, 0>;
+    constexpr int NS = E0::NSPLIT;
+    constexpr int X = E0::BRA_CLASS, Yc = E0::KET_CLASS;
+    const long long ncand = P.total[C];
+    const long long nwork = ((ncand + 31) >> 5) * NS;
+    const int lane = threadIdx.x & 31;
+    const long long wstride = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; gw < nwork; gw += wstride) {
+        const int split = (int)(gw % NS);
+        const long long cand = (gw / NS) * 32 + lane;
+        bool valid = cand < ncand;
+        int row = 0, ket = 0;
+        if (valid) {
+            row = find_row(P.row_off[C], P.n_rows[C], cand);
+            ket = (int)(cand - __ldg(P.row_off[C] + row));
+            const int a = P.ab[X][2 * row], b = P.ab[X][2 * row + 1];
+            const int c = P.ab[Yc][2 * ket], d = P.ab[Yc][2 * ket + 1];
+            const int ns = P.ns;
+            float dm = fmaxf(fmaxf(__ldg(P.Dsh + a * ns + b), __ldg(P.Dsh + c * ns + d)),
+                             fmaxf(fmaxf(__ldg(P.Dsh + a * ns + c), __ldg(P.Dsh + a * ns + d)),
+                                   fmaxf(__ldg(P.Dsh + b * ns + c), __ldg(P.Dsh + b * ns + d))));
+            const double bound = __ldg(P.q[X] + row) * __ldg(P.q[Yc] + ket) * (double)dm;
+            valid = bound >= P.tau_lo && bound < P.tau_hi;
+        }
+        if (P.counts && split == 0) {
+            const unsigned bal = __ballot_sync(DFTK_FULL_MASK, valid);
+            if (lane == 0 && bal) atomicAdd((unsigned long long *)(P.counts + C), (unsigned long long)__popc(bal));
+        }
+        if (!__any_sync(DFTK_FULL_MASK, valid)) continue;
+        if constexpr (NS == 1) {
+            jk_one<C, T, 0>(P, valid, row, ket);
+        } else {
+            if (split == 0) jk_one<C, T, 0>(P, valid, row, ket);
+            else if (split == 1) jk_one<C, T, 1>(P, valid, row, ket);
+            else jk_one<C, T, 2>(P, valid, row, ket);
+        }
+    }
+}
+
+// J = Y + Y^T, K = Z + Z^T
+__global__ void k_symmetrize(int N, const double *Y, const double *Za, const double *Zb, double *J,
+                             double *Ka, double *Kb, int uhf)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)N * N) return;
+    const int i = (int)(t / N), j = (int)(t % N);
+    const long long tt = (long long)j * N + i;
+    J[t] = Y[t] + Y[tt];
+    Ka[t] = Za[t] + Za[tt];
+    if (uhf) Kb[t] = Zb[t] + Zb[tt];
+}
+
+// ------------------------------------------------------------- ERI blocks
+struct EmitParams {
+    const int *shell_ao;
+    const int *shell_l;
+    const int *ab[3];
+    const int *np[3];
+    const double *rec64[3];
+    int n_pairs[3];
+    int kmax[3];
+    long long nq;
+    const int *desc;
+    const long long *out_off;
+    double *out;
+};
+
+__device__ __forceinline__ int ncomp(int l) { return (l + 1) * (l + 2) / 2; }
+
+template <int C, int S>
+__device__ __forceinline__ void emit_split(const EmitParams &P, int row, int ket, int flags,
+                                           const int (&slot)[4], const int (&stride)[4], double *out)
+{
+    using E = EriClass<double, C, S>;
+    constexpr int X = E::BRA_CLASS, Yc = E::KET_CLASS;
+    double I[E::NI];
+    eri_run<C, double, S>(P.rec64[X], P.n_pairs[X], P.kmax[X], row, P.np[X][row], P.rec64[Yc],
+                          P.n_pairs[Yc], P.kmax[Yc], ket, P.np[Yc][ket], I);
+#pragma unroll
+    for (int ia = 0; ia < E::NA; ++ia)
+#pragma unroll
+        for (int ib = 0; ib < E::NB; ++ib)
+#pragma unroll
+            for (int m = 0; m < E::NCD; ++m) {
+                const int comp[4] = {ia, ib, E::cd_c(m), E::cd_d(m)};
+                long long o = 0;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) o += (long long)comp[k] * stride[slot[k]];
+                out[o] = I[(ia * E::NB + ib) * E::NCD + m];
+            }
+}
+
+template <int C>
+__device__ __forceinline__ void emit_class(const EmitParams &P, int row, int ket, int flags,
+                                           const int (&slot)[4], const int (&stride)[4], double *out)
+{
+    emit_split<C, 0>(P, row, ket, flags, slot, stride, out);
+    if constexpr (EriClass<double, C, 0>::NSPLIT > 1) {
+        emit_split<C, 1>(P, row, ket, flags, slot, stride, out);
+        emit_split<C, 2>(P, row, ket, flags, slot, stride, out);
+    }
+}
+
+__global__ void k_emit(const EmitParams P)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= P.nq) return;
+    const int C = P.desc[4 * t], row = P.desc[4 * t + 1], ket = P.desc[4 * t + 2], flags = P.desc[4 * t + 3];
+    constexpr int bra_pc[6] = {0, 1, 1, 2, 2, 2};
+    constexpr int ket_pc[6] = {0, 0, 1, 0, 1, 2};
+    const int X = bra_pc[C], Yc = ket_pc[C];
+    // my (a', b', c', d') -> reference slots
+    int slot[4];
+    const int bra0 = (flags & 4) ? 2 : 0, ket0 = (flags & 4) ? 0 : 2;
+    slot[0] = bra0 + ((flags & 1) ? 1 : 0);
+    slot[1] = bra0 + ((flags & 1) ? 0 : 1);
+    slot[2] = ket0 + ((flags & 2) ? 1 : 0);
+    slot[3] = ket0 + ((flags & 2) ? 0 : 1);
+    const int sh[4] = {P.ab[X][2 * row], P.ab[X][2 * row + 1], P.ab[Yc][2 * ket], P.ab[Yc][2 * ket + 1]};
+    int nref[4];
+    for (int k = 0; k < 4; ++k) nref[slot[k]] = ncomp(P.shell_l[sh[k]]);
+    int stride[4];
+    stride[3] = 1;
+    stride[2] = nref[3];
+    stride[1] = nref[3] * nref[2];
+    stride[0] = nref[3] * nref[2] * nref[1];
+    double *out = P.out + P.out_off[t];
+    switch (C) {
+    case 0: emit_class<0>(P, row, ket, flags, slot, stride, out); break;
+    case 1: emit_class<1>(P, row, ket, flags, slot, stride, out); break;
+    case 2: emit_class<2>(P, row, ket, flags, slot, stride, out); break;
+    case 3: emit_class<3>(P, row, ket, flags, slot, stride, out); break;
+    case 4: emit_class<4>(P, row, ket, flags, slot, stride, out); break;
+    default: emit_class<5>(P, row, ket, flags, slot, stride, out); break;
+    }
+}

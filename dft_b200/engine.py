@@ -1,0 +1,282 @@
+"""Device-resident integral data of one molecule and the calls on it.
+
+An :class:`IntegralEngine` owns, on one CUDA device:
+
+* the shell arrays (centres, momenta, primitive exponents and
+  coefficient x normalisation products),
+* every shell pair (i >= j, the reference's ``pair_list``, shelled.py:962-964)
+  in canonical orientation l_a >= l_b, split into the pair classes ss/ps/pp and
+  sorted by descending Schwarz factor, with SoA primitive-pair records,
+* the candidate-quartet queue: per quartet class, bra row r pairs with the
+  ket prefix whose Schwarz product clears ``tau_schwarz``,
+* the J/K workspace.
+
+PyTorch only provides the device buffers and the stream; all arithmetic is in
+``libdftk.so``.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+import torch
+
+from . import _lib, basis as _basis
+
+# quartet class of (bra pair class, ket pair class), bra class >= ket class
+QCLASS_OF = {(0, 0): 0, (1, 0): 1, (1, 1): 2, (2, 0): 3, (2, 1): 4, (2, 2): 5}
+QCLASS_PAIRS = [(0, 0), (1, 0), (1, 1), (2, 0), (2, 1), (2, 2)]
+QCLASS_NAMES = ["(ss|ss)", "(ps|ss)", "(ps|ps)", "(pp|ss)", "(pp|ps)", "(pp|pp)"]
+PAIR_FIELDS = {0: 5, 1: 9, 2: 12}
+# Fixed flop accounting per evaluated primitive quartet, by class (ss|ss)..(pp|pp):
+# 2 x (R-recursion FMAs + ket Hermite contraction + bra contraction) + 40 + 3L.
+FLOPS_PER_PRIM_QUARTET = [44, 66, 145, 147, 410, 1402]
+
+
+def candidate_offsets(q_bra: np.ndarray, q_ket: np.ndarray, same_class: bool, tau: float) -> np.ndarray:
+    """Row offsets of the candidate-quartet space of one quartet class.
+
+    Both Schwarz-factor arrays are sorted in descending order, so bra row r
+    keeps the ket prefix k < count_r with q_ket[k] >= tau / q_bra[r]; for
+    bra class == ket class the prefix also stops at k <= r so each unique
+    quartet appears once.  Returns int64 offsets of length n_rows + 1."""
+    nrows = q_bra.size
+    if nrows == 0 or q_ket.size == 0:
+        return np.zeros(nrows + 1, dtype=np.int64)
+    with np.errstate(divide="ignore"):
+        thr = np.where(q_bra > 0, tau / np.where(q_bra > 0, q_bra, 1.0), np.inf)
+    cnt = np.searchsorted(-q_ket, -thr, side="right").astype(np.int64)
+    if same_class:
+        cnt = np.minimum(cnt, np.arange(1, nrows + 1))
+    return np.concatenate([[0], np.cumsum(cnt)]).astype(np.int64)
+
+
+def _dev(device) -> torch.device:
+    if device is None:
+        if not torch.cuda.is_available():
+            raise _lib.DftkError("engine", _lib.ERR_CUDA, "no CUDA device: the integral engine has no CPU path")
+        return torch.device("cuda", torch.cuda.current_device())
+    return torch.device(device)
+
+
+class IntegralEngine:
+    def __init__(self, shells: List[Dict], tau_schwarz: float = 1e-12, device=None):
+        _basis.check_supported(shells)
+        _lib.load()
+        self.device = _dev(device)
+        self.shells = shells
+        self.ns = len(shells)
+        self.n_ao = int(shells[-1]["ao_stop"]) if shells else 0
+        self.tau_schwarz = float(tau_schwarz)
+        self.l = np.array([s["angular_momentum"] for s in shells], dtype=np.int32)
+        self.nao_sh = np.array([s["n_ao"] for s in shells], dtype=np.int64)
+        with torch.cuda.device(self.device):
+            _lib.call("dftk_init")
+            self._upload_shells()
+            self._build_pairs()
+            self._build_queue()
+            nbytes = _lib.load().dftk_jk_workspace_bytes(self.ns, self.n_ao)
+            self.workspace = torch.empty(int(nbytes), dtype=torch.uint8, device=self.device)
+            self.workspace_bytes = int(nbytes)
+
+    # ------------------------------------------------------------------ setup
+    def _t(self, arr, dtype):
+        return torch.as_tensor(np.ascontiguousarray(arr), dtype=dtype).to(self.device)
+
+    def _upload_shells(self):
+        sh = self.shells
+        nprim = np.array([s["n_exponents"] for s in sh], dtype=np.int32)
+        prim_off = np.concatenate([[0], np.cumsum(nprim)[:-1]]).astype(np.int32)
+        exps = np.concatenate([s["exponents"] for s in sh]) if sh else np.zeros(0)
+        # coefficient x primitive normalisation; for s and p shells the norm of
+        # every component is the same, so the first component's values serve.
+        cn = np.concatenate([s["coefficients"][0] * s["normalization"][: s["n_exponents"]] for s in sh]) \
+            if sh else np.zeros(0)
+        self.kmax = int(max(1, (nprim.max() if sh else 1) ** 2))
+        self.d_xyz = self._t(np.array([s["atom_pos"] for s in sh], dtype=np.float64).reshape(-1), torch.float64)
+        self.d_l = self._t(self.l, torch.int32)
+        self.d_nprim = self._t(nprim, torch.int32)
+        self.d_prim_off = self._t(prim_off, torch.int32)
+        self.d_ao = self._t(np.array([s["ao_start"] for s in sh], dtype=np.int32), torch.int32)
+        self.d_exp = self._t(exps.astype(np.float64), torch.float64)
+        self.d_cn = self._t(cn.astype(np.float64), torch.float64)
+        self.c_shells = _lib.Shells(
+            self.ns, self.n_ao, _lib.ptr(self.d_xyz).value, _lib.ptr(self.d_l).value, _lib.ptr(self.d_nprim).value,
+            _lib.ptr(self.d_prim_off).value, _lib.ptr(self.d_ao).value, _lib.ptr(self.d_exp).value,
+            _lib.ptr(self.d_cn).value)
+
+    def _alloc_class(self, pc: int, ab: np.ndarray):
+        n = ab.shape[0]
+        nf = PAIR_FIELDS[pc]
+        bufs = {
+            "ab": self._t(ab.reshape(-1).astype(np.int32), torch.int32) if n else torch.zeros(2, dtype=torch.int32, device=self.device),
+            "nprim": torch.zeros(max(n, 1), dtype=torch.int32, device=self.device),
+            "rec64": torch.zeros(max(nf * self.kmax * n, 1), dtype=torch.float64, device=self.device),
+            "rec32": torch.zeros(max(nf * self.kmax * n, 1), dtype=torch.float32, device=self.device),
+            "q": torch.zeros(max(n, 1), dtype=torch.float64, device=self.device),
+        }
+        st = _lib.Pairs(n, self.kmax, _lib.ptr(bufs["ab"]).value, _lib.ptr(bufs["nprim"]).value,
+                        _lib.ptr(bufs["rec64"]).value, _lib.ptr(bufs["rec32"]).value, _lib.ptr(bufs["q"]).value)
+        return bufs, st
+
+    def _build_pairs(self):
+        ns = self.ns
+        ii, jj = np.tril_indices(ns)  # reference pair_list order: (i, j), j <= i
+        ii = ii.astype(np.int64)
+        jj = jj.astype(np.int64)
+        swap = self.l[ii] < self.l[jj]
+        a = np.where(swap, jj, ii)
+        b = np.where(swap, ii, jj)
+        pclass = self.l[a] + self.l[b]
+        stream = _lib.stream_handle()
+        self.pair_bufs, self.c_pairs_list = [], []
+        ref_class = np.zeros(ii.size, dtype=np.int32)
+        ref_row = np.zeros(ii.size, dtype=np.int64)
+        self.q_sorted = []
+        for pc in range(3):
+            sel = np.nonzero(pclass == pc)[0]
+            ab = np.stack([a[sel], b[sel]], axis=1)
+            bufs, st = self._alloc_class(pc, ab)
+            if ab.shape[0]:
+                _lib.call("dftk_pair_data", ctypes.byref(self.c_shells), pc, ctypes.byref(st), stream)
+                _lib.call("dftk_schwarz", ctypes.byref(self.c_shells), pc, ctypes.byref(st), stream)
+                q = bufs["q"][: ab.shape[0]].cpu().numpy()
+                order = np.argsort(-q, kind="stable")
+                ab = ab[order]
+                sel = sel[order]
+                bufs, st = self._alloc_class(pc, ab)
+                _lib.call("dftk_pair_data", ctypes.byref(self.c_shells), pc, ctypes.byref(st), stream)
+                bufs["q"][: ab.shape[0]] = torch.as_tensor(q[order], dtype=torch.float64, device=self.device)
+                self.q_sorted.append(q[order])
+            else:
+                self.q_sorted.append(np.zeros(0))
+            ref_class[sel] = pc
+            ref_row[sel] = np.arange(sel.size)
+            self.pair_bufs.append(bufs)
+            self.c_pairs_list.append(st)
+        self.c_pairs = _lib.PairsArray(*self.c_pairs_list)
+        # reference pair index i(i+1)/2 + j -> (class, sorted row, stored as (j, i))
+        self.ref_pair_class = ref_class
+        self.ref_pair_row = ref_row
+        self.ref_pair_swap = swap
+        self.n_pairs = [int(x.shape[0]) for x in self.q_sorted]
+
+    def _build_queue(self):
+        self.row_off = []
+        self.totals = []
+        q = _lib.Queue()
+        for c, (X, Y) in enumerate(QCLASS_PAIRS):
+            qx, qy = self.q_sorted[X], self.q_sorted[Y]
+            nrows = qx.size
+            off = candidate_offsets(qx, qy, X == Y, self.tau_schwarz)
+            d_off = self._t(off, torch.int64)
+            self.row_off.append(d_off)
+            self.totals.append(int(off[-1]))
+            q.n_rows[c] = nrows if off[-1] > 0 else 0
+            q.total[c] = int(off[-1])
+            q.row_off[c] = _lib.ptr(d_off).value
+        self.c_queue = q
+
+    # ---------------------------------------------------------------- queries
+    def quartet_totals(self) -> List[int]:
+        """Schwarz-surviving unique quartets per class (ss|ss)..(pp|pp)."""
+        return list(self.totals)
+
+    def schwarz_flops(self, counts: Sequence[int]) -> float:
+        """Fixed-accounting flops of evaluating `counts` contracted quartets per class."""
+        nprim_q = self.kmax * self.kmax
+        return float(sum(FLOPS_PER_PRIM_QUARTET[c] * nprim_q * counts[c] for c in range(6)))
+
+    # ---------------------------------------------------------------- compute
+    def one_electron(self, atoms: Sequence[str], centers) -> Tuple[torch.Tensor, torch.Tensor, torch.Tensor]:
+        """S, T, V as N x N float64 CUDA tensors."""
+        N = self.n_ao
+        xyz = torch.as_tensor(np.asarray(centers, dtype=np.float64).reshape(-1), device=self.device)
+        z = torch.as_tensor(np.array([float(int(a)) for a in atoms]), dtype=torch.float64, device=self.device)
+        S, T, V = (torch.empty((N, N), dtype=torch.float64, device=self.device) for _ in range(3))
+        _lib.call("dftk_one_electron", ctypes.byref(self.c_shells), len(atoms), _lib.ptr(xyz), _lib.ptr(z),
+                  _lib.ptr(S), _lib.ptr(T), _lib.ptr(V), _lib.stream_handle())
+        return S, T, V
+
+    def jk(self, D: torch.Tensor, D_a: Optional[torch.Tensor] = None, D_b: Optional[torch.Tensor] = None,
+           uhf: bool = False, mixed: bool = False, tau: float = 1e-14, tau_fp32: float = 1e-6,
+           out=None, counts: Optional[torch.Tensor] = None):
+        """Direct J, K_a (, K_b) for densities on the device.
+
+        D is the density J is built from (the reference's P = P_a + P_b);
+        K_a uses D_a (defaults to D / 2, the RHF alpha density) and, with
+        ``uhf``, K_b uses D_b.  Returns (J, K_a, K_b) with K_b = K_a unless uhf.
+        """
+        N = self.n_ao
+        dev = self.device
+        D = self._square(D)
+        D_a = self._square(D_a) if D_a is not None else (0.5 * D).contiguous()
+        if uhf:
+            if D_b is None:
+                raise _lib.DftkError("jk", _lib.ERR_ARG, "uhf needs D_b")
+            D_b = self._square(D_b)
+        if out is None:
+            J = torch.empty((N, N), dtype=torch.float64, device=dev)
+            Ka = torch.empty((N, N), dtype=torch.float64, device=dev)
+            Kb = torch.empty((N, N), dtype=torch.float64, device=dev) if uhf else None
+        else:
+            J, Ka, Kb = out
+        flags = (_lib.JK_UHF if uhf else 0) | (_lib.JK_MIXED if mixed else 0)
+        _lib.call("dftk_jk", ctypes.byref(self.c_shells), self.c_pairs, ctypes.byref(self.c_queue),
+                  _lib.ptr(D), _lib.ptr(D_a), _lib.ptr(D_b if uhf else None), _lib.ptr(J), _lib.ptr(Ka),
+                  _lib.ptr(Kb if uhf else None), flags, float(tau), float(tau_fp32 if mixed else tau),
+                  _lib.ptr(self.workspace), self.workspace_bytes, _lib.ptr(counts), _lib.stream_handle())
+        return J, Ka, (Kb if uhf else Ka)
+
+    def _square(self, M) -> torch.Tensor:
+        if not isinstance(M, torch.Tensor):
+            M = torch.as_tensor(np.asarray(M, dtype=np.float64))
+        M = M.to(device=self.device, dtype=torch.float64).contiguous()
+        if M.shape != (self.n_ao, self.n_ao):
+            raise _lib.DftkError("jk", _lib.ERR_ARG, f"density shape {tuple(M.shape)} != ({self.n_ao}, {self.n_ao})")
+        return M
+
+    def quartet_descriptors(self, quads: np.ndarray):
+        """Map reference quartets (a, b, c, d) to dftk_eri_blocks descriptors and offsets."""
+        quads = np.asarray(quads, dtype=np.int64).reshape(-1, 4)
+        a, b, c, d = quads.T
+
+        def pair_info(x, y):
+            i = np.maximum(x, y)
+            j = np.minimum(x, y)
+            idx = i * (i + 1) // 2 + j
+            pc = self.ref_pair_class[idx]
+            row = self.ref_pair_row[idx]
+            # canonical first shell: i unless swapped to (j, i)
+            first = np.where(self.ref_pair_swap[idx], j, i)
+            flip = (first != x).astype(np.int32)
+            return pc, row, flip
+
+        pc1, r1, f1 = pair_info(a, b)
+        pc2, r2, f2 = pair_info(c, d)
+        exch = pc1 < pc2
+        X = np.where(exch, pc2, pc1)
+        Y = np.where(exch, pc1, pc2)
+        rb = np.where(exch, r2, r1)
+        rk = np.where(exch, r1, r2)
+        fb = np.where(exch, f2, f1)
+        fk = np.where(exch, f1, f2)
+        qc = np.array([QCLASS_OF[(int(x), int(y))] for x, y in zip(X, Y)], dtype=np.int32) if quads.shape[0] else \
+            np.zeros(0, dtype=np.int32)
+        flags = fb | (fk << 1) | (exch.astype(np.int32) << 2)
+        desc = np.stack([qc, rb.astype(np.int32), rk.astype(np.int32), flags.astype(np.int32)], axis=1)
+        sizes = self.nao_sh[a] * self.nao_sh[b] * self.nao_sh[c] * self.nao_sh[d]
+        off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+        return desc.astype(np.int32), off
+
+    def eri_blocks(self, quads: np.ndarray) -> Tuple[torch.Tensor, np.ndarray]:
+        """Contracted ERI blocks of reference quartets, flat in calc_eri layout."""
+        desc, off = self.quartet_descriptors(quads)
+        d_desc = self._t(desc.reshape(-1), torch.int32)
+        d_off = self._t(off[:-1], torch.int64)
+        out = torch.zeros(int(off[-1]), dtype=torch.float64, device=self.device)
+        if desc.shape[0]:
+            _lib.call("dftk_eri_blocks", ctypes.byref(self.c_shells), self.c_pairs, desc.shape[0],
+                      _lib.ptr(d_desc), _lib.ptr(d_off), _lib.ptr(out), _lib.stream_handle())
+        return out, off

@@ -1,0 +1,239 @@
+"""SCF drivers on the GPU, consuming the integral-direct J/K build.
+
+* :func:`scf_reference` follows the reference's UHF loop (shelled.py:1079-1293):
+  core-Hamiltonian guess, damping from rate 0.4 (divided by 1.1 after four
+  strikes), DIIS on FPS - SPF with a 10-deep history once |dE| < 1e-3,
+  convergence at |dE| < etol and max|dP| < ptol, then one rebuild with the
+  last density.  The Cartesian-to-spherical transform is the identity for s
+  and p shells (shelled.py:878-920), which are all the kernels take.
+* :func:`scf_rhf` is the closed-shell driver the benchmarks use: Pulay DIIS
+  with 8 vectors, convergence at |dE| < 1e-10 and RMS(dD) < 1e-8, and an
+  incremental Fock build F_k = F_{k-1} + G(D_k - D_{k-1}) with optional mixed
+  precision (quartets whose Schwarz bound times |dD| is below tau_fp32 run in
+  FP32, accumulation in FP64).  Full FP64 rebuilds every ``rebuild_every``
+  iterations and at convergence bound the drift of the incremental sum.
+
+Dense linear algebra (eigh via cuSOLVER, DIIS solves) runs in torch float64
+on the same device; it is O(N^3) with N <= a few hundred, far below the J/K
+cost.
+"""
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import torch
+
+from .engine import IntegralEngine
+
+
+@dataclass
+class SCFResult:
+    energy: float
+    converged: bool
+    iterations: int
+    D_a: torch.Tensor
+    D_b: torch.Tensor
+    C_a: torch.Tensor
+    eps_a: torch.Tensor
+    F_a: torch.Tensor
+    fock_builds: int
+    fock_seconds: float
+    energy_history: List[float] = field(default_factory=list)
+    energy_last_build: Optional[float] = None  # energy from the last (incremental/mixed) Fock build
+    counts: Optional[List[int]] = None
+
+
+def orthogonalizer(S: torch.Tensor) -> torch.Tensor:
+    """X = U s^{-1/2} U^T (shelled.py:1083-1088)."""
+    w, U = torch.linalg.eigh(S)
+    return (U * w.rsqrt()) @ U.T
+
+
+def _occupied_density(C: torch.Tensor, n: int) -> torch.Tensor:
+    Co = C[:, :n]
+    return Co @ Co.T
+
+
+def scf_reference(engine: IntegralEngine, H: torch.Tensor, S: torch.Tensor, n_alpha: int, n_beta: int,
+                  e_nn: float, etol: float = 1e-8, ptol: float = 1e-6, max_iter: int = 500,
+                  history: int = 10, tau: float = 0.0) -> SCFResult:
+    dev = engine.device
+    H = H.to(dev, torch.float64)
+    S = S.to(dev, torch.float64)
+    N = H.shape[0]
+    X = orthogonalizer(S)
+    _, Cp = torch.linalg.eigh(X.T @ H @ X)
+    C = X @ Cp
+    P_a = _occupied_density(C, n_alpha)
+    P_b = _occupied_density(C, n_beta)
+    hist = {k: torch.zeros((history, N, N), dtype=torch.float64, device=dev)
+            for k in ("Fa", "Fb", "Ra", "Rb")}
+    E_total, prev_dE, prev_dP = None, float("inf"), float("inf")
+    rate, strikes, use_diis, count = 0.4, 0, False, 0
+    builds, tb = 0, 0.0
+    energies = []
+
+    def build(P, Pa, Pb):
+        nonlocal builds, tb
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        J, Ka, Kb = engine.jk(P, Pa, Pb, uhf=True, tau=tau)
+        torch.cuda.synchronize(dev)
+        tb += time.perf_counter() - t0
+        builds += 1
+        return J, Ka, Kb
+
+    while True:
+        if count > max_iter:
+            raise RuntimeError(f"SCF did not converge in {max_iter} iterations")
+        P = P_a + P_b
+        J, Ka, Kb = build(P, P_a, P_b)
+        Fa, Fb = H + J - Ka, H + J - Kb
+        for key, val in (("Fa", Fa), ("Fb", Fb), ("Ra", Fa @ P_a @ S - S @ P_a @ Fa),
+                         ("Rb", Fb @ P_b @ S - S @ P_b @ Fb)):
+            hist[key] = torch.roll(hist[key], 1, dims=0)
+            hist[key][0] = val
+        if use_diis:
+            B = (torch.einsum("iab,jab->ij", hist["Ra"], hist["Ra"]) +
+                 torch.einsum("iab,jab->ij", hist["Rb"], hist["Rb"]))
+            lim = min(count + 1, history)
+            c = torch.linalg.solve(B[:lim, :lim], torch.ones(lim, dtype=torch.float64, device=dev))
+            c = c / c.sum()
+            Fa = torch.einsum("i,iab->ab", c, hist["Fa"][:lim])
+            Fb = torch.einsum("i,iab->ab", c, hist["Fb"][:lim])
+        E_new = float(0.5 * torch.sum(P * H + P_a * Fa + P_b * Fb)) + e_nn
+        energies.append(E_new)
+        dE = float("inf") if E_total is None else abs(E_new - E_total)
+        _, Ca = torch.linalg.eigh(X.T @ Fa @ X)
+        _, Cb = torch.linalg.eigh(X.T @ Fb @ X)
+        Ca, Cb = X @ Ca, X @ Cb
+        Pa_new = rate * _occupied_density(Ca, n_alpha) + (1 - rate) * P_a
+        Pb_new = rate * _occupied_density(Cb, n_beta) + (1 - rate) * P_b
+        dP = float(torch.max(torch.maximum((Pa_new - P_a).abs(), (Pb_new - P_b).abs())))
+        if (dE > prev_dE or dP > prev_dP) and not use_diis:
+            if strikes == 3:
+                rate /= 1.1
+                strikes = 0
+            else:
+                strikes += 1
+        if dE < 1e-3:
+            use_diis = True
+        if dE < etol and dP < ptol:
+            J, Ka, Kb = build(P, P_a, P_b)
+            Fa, Fb = H + J - Ka, H + J - Kb
+            E_fin = float(0.5 * torch.sum(P * H + P_a * Fa + P_b * Fb)) + e_nn
+            w, Cp = torch.linalg.eigh(X.T @ Fa @ X)
+            return SCFResult(E_fin, True, count, P_a, P_b, X @ Cp, w, Fa, builds, tb, energies)
+        E_total, prev_dE, prev_dP = E_new, dE, dP
+        P_a, P_b = Pa_new, Pb_new
+        count += 1
+
+
+class _Diis:
+    def __init__(self, size: int):
+        self.size = size
+        self.F: List[torch.Tensor] = []
+        self.E: List[torch.Tensor] = []
+
+    def push(self, F: torch.Tensor, err: torch.Tensor):
+        self.F.append(F)
+        self.E.append(err)
+        if len(self.F) > self.size:
+            self.F.pop(0)
+            self.E.pop(0)
+
+    def extrapolate(self) -> torch.Tensor:
+        n = len(self.F)
+        if n < 2:
+            return self.F[-1]
+        dev = self.F[0].device
+        B = torch.empty((n + 1, n + 1), dtype=torch.float64, device=dev)
+        E = torch.stack(self.E).reshape(n, -1)
+        B[:n, :n] = E @ E.T
+        B[n, :n] = -1.0
+        B[:n, n] = -1.0
+        B[n, n] = 0.0
+        rhs = torch.zeros(n + 1, dtype=torch.float64, device=dev)
+        rhs[n] = -1.0
+        try:
+            c = torch.linalg.solve(B, rhs)[:n]
+        except RuntimeError:
+            return self.F[-1]
+        return torch.einsum("i,iab->ab", c, torch.stack(self.F))
+
+
+def scf_rhf(engine: IntegralEngine, H: torch.Tensor, S: torch.Tensor, n_occ: int, e_nn: float,
+            diis: int = 8, etol: float = 1e-10, dtol: float = 1e-8, max_iter: int = 200,
+            incremental: bool = True, mixed: bool = False, tau: float = 1e-12, tau_fp32: float = 1e-6,
+            rebuild_every: int = 12, final_rebuild: bool = True, count_quartets: bool = False,
+            D_guess: Optional[torch.Tensor] = None, callback=None) -> SCFResult:
+    dev = engine.device
+    H = H.to(dev, torch.float64)
+    S = S.to(dev, torch.float64)
+    X = orthogonalizer(S)
+    if D_guess is None:
+        _, Cp = torch.linalg.eigh(X.T @ H @ X)
+        D = _occupied_density(X @ Cp, n_occ)
+    else:
+        D = D_guess.to(dev, torch.float64)
+    acc = _Diis(diis)
+    G = None           # accumulated two-electron Fock part J - K for D_ref
+    D_ref = None       # density G corresponds to
+    E_prev = None
+    builds, tb = 0, 0.0
+    energies: List[float] = []
+    counts_t = torch.zeros(12, dtype=torch.int64, device=dev) if count_quartets else None
+    since_full = 0
+    E_last = None
+    for it in range(max_iter + 1):
+        full = (G is None) or (not incremental) or since_full >= rebuild_every
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        if full:
+            J, K, _ = engine.jk(2.0 * D, D, tau=min(tau, 1e-14), counts=counts_t)
+            G = J - K
+            since_full = 0
+        else:
+            dD = D - D_ref
+            J, K, _ = engine.jk(2.0 * dD, dD, mixed=mixed, tau=tau, tau_fp32=tau_fp32, counts=counts_t)
+            G = G + (J - K)
+            since_full += 1
+        torch.cuda.synchronize(dev)
+        tb += time.perf_counter() - t0
+        builds += 1
+        D_ref = D
+        F = H + G
+        E = float(torch.sum(D * (H + F))) + e_nn
+        E_last = E
+        energies.append(E)
+        err = X.T @ (F @ D @ S - S @ D @ F) @ X
+        acc.push(F, err)
+        Fx = acc.extrapolate()
+        w, Cp = torch.linalg.eigh(X.T @ Fx @ X)
+        C = X @ Cp
+        D_new = _occupied_density(C, n_occ)
+        dE = float("inf") if E_prev is None else abs(E - E_prev)
+        rms = float(torch.sqrt(torch.mean((D_new - D) ** 2)))
+        if callback is not None:
+            callback(it, E, dE, rms, D)
+        if dE < etol and rms < dtol:
+            e_last_build = E
+            if final_rebuild:
+                torch.cuda.synchronize(dev)
+                t0 = time.perf_counter()
+                J, K, _ = engine.jk(2.0 * D, D, tau=min(tau, 1e-14))
+                torch.cuda.synchronize(dev)
+                tb += time.perf_counter() - t0
+                builds += 1
+                F = H + J - K
+                E = float(torch.sum(D * (H + F))) + e_nn
+                w, Cp = torch.linalg.eigh(X.T @ F @ X)
+                C = X @ Cp
+            return SCFResult(E, True, it, D, D, C, w, F, builds, tb, energies, e_last_build,
+                             counts_t.tolist() if counts_t is not None else None)
+        E_prev = E
+        D = D_new
+    return SCFResult(E_last, False, max_iter, D, D, C, w, F, builds, tb, energies, E_last,
+                     counts_t.tolist() if counts_t is not None else None)

@@ -1,0 +1,185 @@
+/*
+ * dftk.h -- C-ABI of libdftk.so, the B200 (sm_100a) Gaussian-integral and
+ * Fock-build library.
+ *
+ * Every entry point returns an int status (DFTK_OK = 0); dftk_last_error()
+ * gives a message for the calling host thread.  All array arguments are
+ * DEVICE pointers owned by the caller unless stated otherwise; nothing here
+ * allocates device memory except dftk_init's one-off constant tables.  Work is
+ * issued on the given stream (NULL = legacy default stream) and is
+ * asynchronous unless stated otherwise.
+ *
+ * Reference interfaces replaced (yegor-gondhal/DFT, shelled.py):
+ *   dftk_nuclear_kernel   <- RawKernel nuclear_kernel         shelled.py:350-450 (launch :1015)
+ *   dftk_eri_kernel       <- RawKernel eri_kernel             shelled.py:452-532 (launch :642)
+ *   dftk_boys             <- device boys()/taylor()           shelled.py:174-211
+ *   dftk_pair_data        <- per-pair nuclear_kernel launch + pair_cache   shelled.py:1000-1059
+ *   dftk_one_electron     <- overlap/T_raw/V block loop       shelled.py:961-1069
+ *   dftk_schwarz          <- (absent in the reference: screening bounds)
+ *   dftk_eri_blocks       <- calc_eri quartet blocks          shelled.py:596-700
+ *   dftk_jk               <- fill_matrices                    shelled.py:770-877
+ */
+#ifndef DFTK_H
+#define DFTK_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* cudaStream_t-compatible opaque stream handle */
+typedef struct CUstream_st *dftk_stream_t;
+
+enum {
+    DFTK_OK = 0,
+    DFTK_ERR_ARG = 1,          /* bad argument (null pointer, negative size, ...) */
+    DFTK_ERR_CUDA = 2,         /* a CUDA runtime call or launch failed */
+    DFTK_ERR_UNSUPPORTED = 3,  /* basis feature outside what the kernels handle */
+    DFTK_ERR_WORKSPACE = 4,    /* workspace too small */
+    DFTK_ERR_SIZE = 5          /* size beyond a fixed maximum */
+};
+
+/* dftk_jk flags */
+#define DFTK_JK_UHF 1          /* K_a from D_a and K_b from D_b; else K_b untouched and D_b unused */
+#define DFTK_JK_MIXED 2        /* FP32 for quartets with Q_ab Q_cd Dmax < tau_fp32 */
+
+/* Quartet classes, in the order dftk_jk and dftk_queue_t use them:
+ * 0 (ss|ss), 1 (ps|ss), 2 (ps|ps), 3 (pp|ss), 4 (pp|ps), 5 (pp|pp). */
+#define DFTK_N_QCLASS 6
+#define DFTK_N_PCLASS 3
+
+/* Shells of one molecule (device arrays).  l <= 1 (s, p) for the ERI and J/K
+ * kernels, one contraction per shell (the reference splits sp shells,
+ * shelled.py:66-75). */
+typedef struct {
+    int n_shells;
+    int n_ao;
+    const double *xyz;      /* [3 * n_shells] centre of each shell, bohr */
+    const int *l;           /* [n_shells] angular momentum */
+    const int *nprim;       /* [n_shells] primitives */
+    const int *prim_off;    /* [n_shells] first primitive in prim_exp/prim_cn */
+    const int *ao;          /* [n_shells] first AO (reference ao_start) */
+    const double *prim_exp; /* [total primitives] exponents */
+    const double *prim_cn;  /* [total primitives] coefficient x primitive norm (normal(), shelled.py:95-101) */
+} dftk_shells_t;
+
+/* Shell pairs of one pair class (0 ss, 1 ps, 2 pp) with l_a >= l_b, and their
+ * primitive-pair records in SoA layout rec[(field * kmax + k) * n_pairs + pair]
+ * (fields: P x/y/z, p, K, 1/(2p), PA x/y/z, PB x/y/z; ss uses 5, ps 9, pp 12). */
+typedef struct {
+    int n_pairs;
+    int kmax;               /* primitive-pair slots per pair (max nprim_a * nprim_b) */
+    const int *ab;          /* [2 * n_pairs] shells (a, b) */
+    int *nprim;             /* [n_pairs] primitive pairs in use (written by dftk_pair_data) */
+    double *rec64;          /* [nfields * kmax * n_pairs] (written by dftk_pair_data) */
+    float *rec32;           /* same, FP32 copy for the mixed path */
+    double *q;              /* [n_pairs] Schwarz factor sqrt(max|(ab|ab)|) (written by dftk_schwarz) */
+} dftk_pairs_t;
+
+/* Candidate quartets of each class: bra pair `row` of the bra pair class pairs
+ * with ket pairs 0 .. (row_off[row+1] - row_off[row] - 1) of the ket class,
+ * both classes sorted by descending Schwarz factor (so the Schwarz-surviving
+ * kets of a row form a prefix).  For bra class == ket class the prefix stops
+ * at the row itself, which enumerates each unique quartet once. */
+typedef struct {
+    long long n_rows[DFTK_N_QCLASS];
+    long long total[DFTK_N_QCLASS];           /* host copy of row_off[n_rows] */
+    const long long *row_off[DFTK_N_QCLASS];  /* device [n_rows + 1] */
+} dftk_queue_t;
+
+/* library version (integer, 100 * major + minor) */
+int dftk_version(void);
+
+/* message of the last failing call on this host thread ("" if none) */
+const char *dftk_last_error(void);
+
+/* Load the Boys tables on the current device.  Called implicitly by every
+ * compute entry point; call it once yourself before any stream capture. */
+int dftk_init(void);
+
+/* F_0..F_mmax(T) for n arguments: F[i * (mmax + 1) + m] (boys/taylor,
+ * shelled.py:174-211).  precision 64 or 32 (32 reads T32/F32 instead). */
+int dftk_boys(int mmax, long long n, const double *T, double *F, dftk_stream_t stream);
+int dftk_boys32(int mmax, long long n, const float *T, float *F, dftk_stream_t stream);
+
+/* Primitive-pair records of every pair in `pairs` (the pair part of
+ * nuclear_kernel and pair_cache, shelled.py:1000-1059). */
+int dftk_pair_data(const dftk_shells_t *shells, int pair_class, dftk_pairs_t *pairs,
+                   dftk_stream_t stream);
+
+/* Schwarz factors pairs->q from the diagonal quartets (ab|ab). */
+int dftk_schwarz(const dftk_shells_t *shells, int pair_class, dftk_pairs_t *pairs,
+                 dftk_stream_t stream);
+
+/* Contracted Cartesian S, T, V (N x N, row-major) over all shell pairs
+ * (shelled.py:961-1069); atom_z are the nuclear charges as doubles. */
+int dftk_one_electron(const dftk_shells_t *shells, int n_atoms, const double *atom_xyz,
+                      const double *atom_z, double *S, double *T, double *V,
+                      dftk_stream_t stream);
+
+/* Contracted ERI blocks of explicit quartets (debug / parity path of calc_eri,
+ * shelled.py:640-691).  desc[4 * t] = {quartet class, bra row, ket row, flags}
+ * with flags bit0 = bra pair stored as (b, a), bit1 = ket pair stored as
+ * (d, c), bit2 = bra and ket exchanged, all relative to the reference quartet
+ * (a, b, c, d); block t is written at out + out_off[t] in the reference's
+ * (n_ao_a, n_ao_b, n_ao_c, n_ao_d) row-major layout. */
+int dftk_eri_blocks(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N_PCLASS],
+                    long long n_quartets, const int *desc, const long long *out_off,
+                    double *out, dftk_stream_t stream);
+
+/* Workspace bytes dftk_jk needs for n_shells shells and n_ao AOs. */
+size_t dftk_jk_workspace_bytes(int n_shells, int n_ao);
+
+/* Integral-direct J and K (fill_matrices, shelled.py:770-877, without stored
+ * ERIs): J = (mu nu|la si) D_la,si and K_s = (mu la|nu si) Ds_la,si over the
+ * unique Schwarz-surviving quartets of `queue` whose bound
+ * Q_ab Q_cd max|D block| >= tau.  J, K_a (and K_b with DFTK_JK_UHF) are
+ * overwritten, N x N row-major, symmetric.  With DFTK_JK_MIXED the quartets
+ * with bound < tau_fp32 run in FP32 (accumulation stays FP64).
+ * counts (optional device array of 2 * DFTK_N_QCLASS long long, zeroed by
+ * the caller) receives the quartets evaluated per class in FP64 then FP32. */
+int dftk_jk(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N_PCLASS],
+            const dftk_queue_t *queue, const double *D, const double *D_a, const double *D_b,
+            double *J, double *K_a, double *K_b, int flags, double tau, double tau_fp32,
+            void *workspace, size_t workspace_bytes, long long *counts, dftk_stream_t stream);
+
+/* Profiling aid: with timing enabled, later dftk_jk calls record CUDA events
+ * around each class kernel on their stream.  dftk_jk_timing_read waits for
+ * the last recorded call and writes ms[2 * DFTK_N_QCLASS] (FP64 launches,
+ * then FP32 launches; 0 where a class did not launch). */
+int dftk_jk_timing(int enable);
+int dftk_jk_timing_read(float *ms, int n);
+
+/* Drop-in for the reference's nuclear_kernel (same arguments and output
+ * layout, shelled.py:350-371): one thread per primitive-component pair,
+ * E arrays with 7 slots per pair, num_atoms nuclei with integer charges. */
+int dftk_nuclear_kernel(const double *exp_a, const double *exp_b, const double *cen_a,
+                        const double *cen_b, const int *pow_a, const int *pow_b,
+                        const int *atoms, const double *atom_centers, int num_atoms,
+                        int num_funcs_a, int num_funcs_b, double *V_output, double *Ex_output,
+                        double *Ey_output, double *Ez_output, double *p_output,
+                        double *P_output, int *nx_output, int *ny_output, int *nz_output,
+                        dftk_stream_t stream);
+
+/* Drop-in for the reference's eri_kernel (same arguments and output layout,
+ * shelled.py:452-473): eri_output[i * K_cd + j] for primitive pair records
+ * i of ab and j of cd. */
+int dftk_eri_kernel(int K_ab, const double *p_ab, const double *P_ab, const double *Exab,
+                    const double *Eyab, const double *Ezab, const int *nxab, const int *nyab,
+                    const int *nzab, int K_cd, const double *p_cd, const double *P_cd,
+                    const double *Excd, const double *Eycd, const double *Ezcd,
+                    const int *nxcd, const int *nycd, const int *nzcd, double *eri_output,
+                    dftk_stream_t stream);
+
+/* FMA-pipe microbenchmark used to measure the FP64/FP32 roofline denominator:
+ * `iters` dependent-chain-free FMAs per thread (8 chains), result in sink[]
+ * (blocks * threads doubles).  precision 64 or 32. */
+int dftk_fma_burn(int precision, int blocks, int threads, int iters, double *sink,
+                  dftk_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DFTK_H */

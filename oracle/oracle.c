@@ -339,11 +339,34 @@ static void orc_pair_free(OrcPair *pr)
 /* Contracted Cartesian block of the shell quartet (ab|cd), layout
  * (n_ao_a, n_ao_b, n_ao_c, n_ao_d) with AO = contraction * n_comp + component
  * (calc_eri, shelled.py:640-691: eri_kernel, normalisation, einsum). */
+/* Signature of the reference's host-compiled eri_kernel launch loop
+ * (oracle/_ref ref_run_eri_kernel): primitive ERIs from two pair records. */
+typedef void (*orc_ref_eri_fn)(long long, int, const double *, const double *, const double *,
+                               const double *, const double *, const int *, const int *,
+                               const int *, int, const double *, const double *, const double *,
+                               const double *, const double *, const int *, const int *,
+                               const int *, double *);
+
+static void orc_quartet_block_fn(const OrcShells *S, const OrcPair *ab, const OrcPair *cd,
+                                 int a, int b, int c, int d, double *prim, double *out,
+                                 orc_ref_eri_fn fn);
+
 static void orc_quartet_block(const OrcShells *S, const OrcPair *ab, const OrcPair *cd,
                               int a, int b, int c, int d, double *prim, double *out)
 {
-    orc_eri_prims(ab->K, ab->p, ab->P, ab->Ex, ab->Ey, ab->Ez, ab->nx, ab->ny, ab->nz, cd->K,
-                  cd->p, cd->P, cd->Ex, cd->Ey, cd->Ez, cd->nx, cd->ny, cd->nz, prim);
+    orc_quartet_block_fn(S, ab, cd, a, b, c, d, prim, out, NULL);
+}
+
+static void orc_quartet_block_fn(const OrcShells *S, const OrcPair *ab, const OrcPair *cd,
+                                 int a, int b, int c, int d, double *prim, double *out,
+                                 orc_ref_eri_fn fn)
+{
+    if (fn)
+        fn((long long)ab->K * cd->K, ab->K, ab->p, ab->P, ab->Ex, ab->Ey, ab->Ez, ab->nx, ab->ny,
+           ab->nz, cd->K, cd->p, cd->P, cd->Ex, cd->Ey, cd->Ez, cd->nx, cd->ny, cd->nz, prim);
+    else
+        orc_eri_prims(ab->K, ab->p, ab->P, ab->Ex, ab->Ey, ab->Ez, ab->nx, ab->ny, ab->nz, cd->K,
+                      cd->p, cd->P, cd->Ex, cd->Ey, cd->Ez, cd->nx, cd->ny, cd->nz, prim);
     int cmp[4] = {orc_ncomp(S->l[a]), orc_ncomp(S->l[b]), orc_ncomp(S->l[c]), orc_ncomp(S->l[d])};
     int ne[4] = {S->nexp[a], S->nexp[b], S->nexp[c], S->nexp[d]};
     int nc[4] = {S->ncontr[a], S->ncontr[b], S->ncontr[c], S->ncontr[d]};
@@ -489,11 +512,29 @@ void orc_fill_matrices(int ns, const double *center, const int *l, const int *ne
 /* Integral-direct J/K over a quartet list: the reference's calc_eri quartet
  * block (shelled.py:640-691) digested at once by fill_matrices' rule
  * (shelled.py:826-859), without storing the integrals. */
+void orc_direct_jk_fn(int ns, const double *center, const int *l, const int *nexp,
+                      const int *ncontr, const int *exp_off, const int *coef_off, const int *ao,
+                      const double *exps, const double *coefs, long nq, const int *quads, int N,
+                      const double *P, const double *Pa, const double *Pb, double *J, double *Ka,
+                      double *Kb, orc_ref_eri_fn fn);
+
 void orc_direct_jk(int ns, const double *center, const int *l, const int *nexp,
                    const int *ncontr, const int *exp_off, const int *coef_off, const int *ao,
                    const double *exps, const double *coefs, long nq, const int *quads, int N,
                    const double *P, const double *Pa, const double *Pb, double *J, double *Ka,
                    double *Kb)
+{
+    orc_direct_jk_fn(ns, center, l, nexp, ncontr, exp_off, coef_off, ao, exps, coefs, nq, quads, N,
+                     P, Pa, Pb, J, Ka, Kb, NULL);
+}
+
+/* Same, with the primitive ERIs from `fn` (the reference's own eri_kernel
+ * compiled as host code) when it is not NULL. */
+void orc_direct_jk_fn(int ns, const double *center, const int *l, const int *nexp,
+                      const int *ncontr, const int *exp_off, const int *coef_off, const int *ao,
+                      const double *exps, const double *coefs, long nq, const int *quads, int N,
+                      const double *P, const double *Pa, const double *Pb, double *J, double *Ka,
+                      double *Kb, orc_ref_eri_fn fn)
 {
     OrcShells S = orc_shells(ns, center, l, nexp, ncontr, exp_off, coef_off, ao, exps, coefs);
     long NN = (long)N * N;
@@ -517,7 +558,7 @@ void orc_direct_jk(int ns, const double *center, const int *l, const int *nexp,
             OrcPair ab, cd;
             orc_pair_build(&S, q[0], q[1], &ab);
             orc_pair_build(&S, q[2], q[3], &cd);
-            orc_quartet_block(&S, &ab, &cd, q[0], q[1], q[2], q[3], prim, blk);
+            orc_quartet_block_fn(&S, &ab, &cd, q[0], q[1], q[2], q[3], prim, blk, fn);
             orc_digest_one(&S, q, blk, N, P, Pa, Pb, aj, aj + NN, aj + 2 * NN);
             orc_pair_free(&ab);
             orc_pair_free(&cd);

@@ -234,6 +234,24 @@ def direct_jk(shells, quads, P, P_a, P_b):
     return J, Ka, Kb
 
 
+def direct_jk_reference_kernel(shells, quads, P, P_a, P_b, ref=None):
+    """direct_jk with the primitive ERIs from the reference's own eri_kernel
+    (oracle/_ref), contraction and digestion from the restatement."""
+    ref = ref if ref is not None else ref_lib()
+    if ref is None:
+        raise RuntimeError("oracle/_ref/libref.so not built")
+    sa = ShellArrays(shells)
+    N = sa.N
+    J, Ka, Kb = (np.zeros((N, N)) for _ in range(3))
+    P, P_a, P_b = (np.ascontiguousarray(x, dtype=np.float64) for x in (P, P_a, P_b))
+    quads = np.ascontiguousarray(quads, dtype=np.int32)
+    fn = ctypes.cast(ref.ref_run_eri_kernel, ctypes.c_void_p)
+    lib().orc_direct_jk_fn.restype = None
+    lib().orc_direct_jk_fn(*sa.args(), ctypes.c_long(quads.shape[0]), _p(quads), ctypes.c_int(N),
+                           _p(P), _p(P_a), _p(P_b), _p(J), _p(Ka), _p(Kb), fn)
+    return J, Ka, Kb
+
+
 def full_eri_tensor(shells: List[Dict]) -> np.ndarray:
     """Dense (N,N,N,N) ERI tensor from the unique quartets (small N only)."""
     quads = quartet_list(len(shells))

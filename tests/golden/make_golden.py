@@ -248,8 +248,7 @@ def case_h2o64(out_dir, n_subsets=12, subset_pairs=24, seed=1234):
     res = {"atoms": np.array(atoms), "centers": centers,
            "sample_quads": np.array(all_quads, dtype=np.int32),
            "sample_offsets": np.array(offsets, dtype=np.int64),
-           "sample_values": np.concatenate(all_vals),
-           "E_NN": float(ns["E_NN"])}
+           "sample_values": np.concatenate(all_vals)}
     for k in ("overlaps", "T_matrix", "V_matrix"):
         m = np.asarray(ns[k])
         res[k + "_diag"] = np.diag(m).copy()

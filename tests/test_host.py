@@ -1,0 +1,152 @@
+"""Host logic and the C-ABI boundary, without a GPU."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from dft_b200 import _lib, basis, geometry, shelled
+from dft_b200.engine import QCLASS_PAIRS, candidate_offsets
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_shells_match_oracle(oracle_mod):
+    atoms, centers = geometry.alkane(10)
+    mine = basis.build_shells(basis.load_basis(), atoms, centers)
+    ref = oracle_mod.build_shells(oracle_mod.load_basis(basis.STO3G_PATH), atoms, centers)
+    assert len(mine) == len(ref) == 52
+    for a, b in zip(mine, ref):
+        for k in ("angular_momentum", "n_components", "n_contractions", "n_ao", "n_exponents", "ao_start",
+                  "ao_stop", "atom_idx"):
+            assert a[k] == b[k], k
+        np.testing.assert_allclose(a["normalization"], b["normalization"], rtol=1e-15)
+        np.testing.assert_array_equal(a["components"], b["components"])
+    assert mine[-1]["ao_stop"] == 72
+
+
+def test_basis_file_matches_reference_format():
+    data = basis.load_basis()
+    assert set(data) >= {str(z) for z in range(1, 55)}
+    o = data["8"]
+    assert o[0][0] == [0] and o[1][0] == [0, 1] and len(o[1][2]) == 2
+
+
+def test_combinations_order():
+    assert basis.combinations(1) == [[1, 0, 0], [0, 1, 0], [0, 0, 1]]
+    assert basis.combinations(2) == [[2, 0, 0], [1, 1, 0], [0, 2, 0], [1, 0, 1], [0, 1, 1], [0, 0, 2]]
+
+
+def test_unsupported_basis_is_rejected():
+    shells = basis.build_shells(basis.load_basis(), ["21"], np.zeros((1, 3)))  # Sc has d shells
+    with pytest.raises(basis.UnsupportedBasis):
+        basis.check_supported(shells)
+
+
+def test_geometry_alkane():
+    atoms, c = geometry.alkane(10)
+    assert atoms.count("6") == 10 and atoms.count("1") == 22
+    d = np.linalg.norm(c[:, None] - c[None], axis=-1)
+    cc = d[:10, :10][np.triu_indices(10, 1)]
+    bond = 1.54 * geometry.ANGSTROM_TO_BOHR
+    assert np.sum(np.isclose(cc, bond, atol=1e-9)) == 9
+    ch = d[:10, 10:]
+    assert np.allclose(np.sort(ch, axis=0)[0], 1.09 * geometry.ANGSTROM_TO_BOHR)
+    # every C-C-C and H-C-H angle is tetrahedral
+    for k in range(1, 9):
+        u, v = c[k - 1] - c[k], c[k + 1] - c[k]
+        assert np.isclose(np.dot(u, v) / np.linalg.norm(u) / np.linalg.norm(v), -1 / 3)
+    # the chain is planar (all carbons at z = 0)
+    assert np.allclose(c[:10, 2], 0)
+
+
+def test_geometry_clusters_deterministic():
+    a1, c1 = geometry.water_cluster((4, 4, 4))
+    a2, c2 = geometry.water_cluster((4, 4, 4))
+    assert len(a1) == 192
+    np.testing.assert_array_equal(c1, c2)
+    # monomer O-H bond lengths preserved up to the +-0.3 bohr jitter
+    oh = np.linalg.norm(c1[1::3] - c1[0::3], axis=1)
+    assert np.all(np.abs(oh - 1.8089) < 0.3 * np.sqrt(3) * 2 + 1e-9)
+    batch = geometry.water_cluster_batch(16, 24, seed=3)
+    assert len(batch) == 16
+    for atoms, cen in batch:
+        assert 3 <= len(atoms) <= 72 and cen.shape == (len(atoms), 3)
+
+
+def test_quartet_order_matches_reference(golden_h2o):
+    n = 5
+    pl = [(i, j) for i in range(n) for j in range(i + 1)]
+    q = shelled.quartet_list(pl)
+    np.testing.assert_array_equal(q, golden_h2o["eri_quads"])
+
+
+def test_process_eri_matches_reference(golden_h2o):
+    g = golden_h2o
+    eri = {"eri_values": np.arange(int(g["eri_indices"][-1, 1]), dtype=np.float64),
+           "eri_indices": g["eri_indices"], "eri_quads": g["eri_quads"], "eri_quads_shapes": g["eri_quads_shapes"]}
+    res = shelled.process_eri(eri)
+    np.testing.assert_array_equal(res["processed_eri_quads"], g["processed_eri_quads"])
+    np.testing.assert_array_equal(res["processed_eri_indices"], g["processed_eri_indices"])
+    np.testing.assert_array_equal(res["block_idxs"], g["block_idxs"])
+    np.testing.assert_array_equal(res["chunked_quad_shape"], g["chunked_quad_shape"])
+    assert g["block_idxs"].shape[0] == 13
+
+
+def test_candidate_counts_c10h22(oracle_mod, golden_c10h22):
+    """Schwarz-surviving unique quartets per class for C10H22 (tau = 1e-12)
+    from the oracle's diagonal integrals, against a brute-force count."""
+    g = golden_c10h22
+    atoms, centers = [str(a) for a in g["atoms"]], g["centers"]
+    sh = oracle_mod.build_shells(oracle_mod.load_basis(basis.STO3G_PATH), atoms, centers)
+    l = np.array([s["angular_momentum"] for s in sh])
+    ii, jj = np.tril_indices(len(sh))
+    diag = np.stack([ii, jj, ii, jj], axis=1).astype(np.int32)
+    vals, off = oracle_mod.eri_quartets(sh, diag)
+    q = np.array([np.sqrt(np.abs(vals[off[t]:off[t + 1]]).max()) for t in range(len(ii))])
+    pc = l[ii] + l[jj]
+    qs = [np.sort(q[pc == c])[::-1] for c in range(3)]
+    counts = []
+    for X, Y in QCLASS_PAIRS:
+        off_ = candidate_offsets(qs[X], qs[Y], X == Y, 1e-12)
+        counts.append(int(off_[-1]))
+    # brute force over unique pairs of pairs
+    brute = [0] * 6
+    from dft_b200.engine import QCLASS_OF
+    for X in range(3):
+        for Y in range(X + 1):
+            prod = np.outer(qs[X], qs[Y]) >= 1e-12
+            if X == Y:
+                prod = np.tril(prod)
+            brute[QCLASS_OF[(X, Y)]] = int(prod.sum())
+    assert counts == brute
+    assert sum(counts) <= 950131
+
+
+def test_header_symbols_exported():
+    """libdftk.so loads without a GPU and exports every symbol include/dftk.h declares."""
+    header = open(os.path.join(REPO, "include", "dftk.h")).read()
+    declared = set(re.findall(r"\b(dftk_\w+)\s*\(", header))
+    assert declared == set(_lib.SYMBOLS)
+    lib = _lib.load()
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert lib.dftk_version() == 100
+
+
+def test_cabi_argument_errors_without_gpu():
+    """Argument validation happens before any CUDA call and reports through
+    the status code and dftk_last_error()."""
+    lib = _lib.load()
+    st = lib.dftk_jk(None, None, None, None, None, None, None, None, None, 0, 0.0, 0.0, None, 0, None, None)
+    assert st == _lib.ERR_ARG
+    assert b"null" in lib.dftk_last_error()
+    st = lib.dftk_boys(-1, 4, None, None, None)
+    assert st == _lib.ERR_ARG
+    st = lib.dftk_fma_burn(16, 1, 32, 1, None, None)
+    assert st == _lib.ERR_ARG
+    assert lib.dftk_jk_workspace_bytes(10, 20) >= 3 * 20 * 20 * 8
+    with pytest.raises(_lib.DftkError) as ei:
+        _lib.call("dftk_boys", 99, 1, None, None, None)
+    assert ei.value.status == _lib.ERR_ARG
