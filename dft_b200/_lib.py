@@ -11,7 +11,8 @@ import os
 from typing import Optional
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libdftk.so")
+# DFTK_LIB selects another build of the same library (e.g. a tuning variant)
+LIB_PATH = os.environ.get("DFTK_LIB") or os.path.join(HERE, "libdftk.so")
 
 N_QCLASS = 6
 N_PCLASS = 3

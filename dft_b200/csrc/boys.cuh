@@ -2,57 +2,64 @@
 //
 // Method (McMurchie & Davidson, J. Comput. Phys. 26, 218 (1978), sec. 4;
 // the tabulated-Taylor scheme used by most MD codes):
-//   T < 36: F_L(T) = sum_{j=0}^{6} F_{L+j}(T_k) (T_k - T)^j / j!  around the
+//   T < 50: F_L(T) = sum_{j=0}^{7} F_{L+j}(T_k) (T_k - T)^j / j!  around the
 //           nearest grid point T_k = k / 10 (|T_k - T| <= 0.05, truncation
-//           ~1e-15 relative), exp(-T) = exp(-T_k) exp(T_k - T) with a 7-term
-//           Taylor series, then the downward recursion
-//           F_m = (2T F_{m+1} + exp(-T)) / (2m + 1), which is stable.
-//   T >= 36: F_0 = sqrt(pi / T) / 2 (erfc(6) < 2e-17), upward recursion
-//           F_{m+1} = ((2m + 1) F_m - exp(-T)) / (2T), stable for T > m.
-// The table holds F_0..F_14 and exp(-T_k) for T_k = 0, 0.1, ..., 36; it is
-// computed on the host in long double from the all-positive series
+//           < 2e-15 relative).  The table stores, per order L, the eight
+//           coefficients F_{L+j}(T_k) / j! of one grid point contiguously, so
+//           the polynomial is a plain FMA Horner chain fed by 128-bit loads.
+//           exp(-T) = exp(-T_k) exp(T_k - T) with a 7-term Taylor series,
+//           then the downward recursion F_m = (2T F_{m+1} + exp(-T)) / (2m+1),
+//           which is stable.
+//   T >= 50: F_0 = sqrt(pi / T) / 2 (erfc(7) < 5e-23) and the upward
+//           recursion F_{m+1} = (2m + 1) F_m / (2T); the exp(-T) < 2e-22 term
+//           it drops changes F_m by < 2e-14 relative for m <= 7.
+// Tables: orders L = 0..8, grid points T_k = 0, 0.1, ..., 50, computed on the
+// host in long double from the all-positive series
 // F_m(T) = exp(-T) sum_i (2T)^i / ((2m+1)(2m+3)...(2m+2i+1)).
-// FP32 uses the same scheme with 5 Taylor terms and a float table built at
-// the float grid points.
+// FP32 uses the same scheme with the first five coefficients of a float table
+// built at the float grid points, and a 5-term exp series.
 #pragma once
 
 #include "common.cuh"
 
-#define DFTK_BOYS_ROWS 361
-#define DFTK_BOYS_COLS 16
-#define DFTK_BOYS_EXPCOL 15
-#define DFTK_BOYS_TMAX 36.0
+#define DFTK_BOYS_ROWS 501
+#define DFTK_BOYS_NL 9         // orders 0..8
+#define DFTK_BOYS_W 8          // coefficients per grid point
+#define DFTK_BOYS_TMAX 50.0
 
-__device__ double g_boys64[DFTK_BOYS_ROWS * DFTK_BOYS_COLS];
-__device__ float g_boys32[DFTK_BOYS_ROWS * DFTK_BOYS_COLS];
+__device__ double g_boys64[DFTK_BOYS_NL * DFTK_BOYS_ROWS * DFTK_BOYS_W];
+__device__ double g_bexp64[DFTK_BOYS_ROWS];
+__device__ float g_boys32[DFTK_BOYS_NL * DFTK_BOYS_ROWS * DFTK_BOYS_W];
+__device__ float g_bexp32[DFTK_BOYS_ROWS];
 
 template <typename T, int L> struct Boys;
 
 template <int L> struct Boys<double, L> {
-    static_assert(L + 6 < DFTK_BOYS_EXPCOL, "Boys table too narrow");
+    static_assert(L < DFTK_BOYS_NL, "Boys order beyond the table");
     __device__ __forceinline__ static void eval(double x, double *F)
     {
         if (x < DFTK_BOYS_TMAX) {
-            const int k = __double2int_rn(x * 10.0);
+            const int k = max(__double2int_rn(x * 10.0), 0);
             const double d = (double)k * 0.1 - x;
-            const double *row = g_boys64 + k * DFTK_BOYS_COLS;
-            double f = __ldg(row + L + 6);
-            f = fma(f, d * (1.0 / 6.0), __ldg(row + L + 5));
-            f = fma(f, d * 0.2, __ldg(row + L + 4));
-            f = fma(f, d * 0.25, __ldg(row + L + 3));
-            f = fma(f, d * (1.0 / 3.0), __ldg(row + L + 2));
-            f = fma(f, d * 0.5, __ldg(row + L + 1));
-            f = fma(f, d, __ldg(row + L));
-            F[L] = f;
+            const double2 *row = reinterpret_cast<const double2 *>(
+                g_boys64 + ((size_t)L * DFTK_BOYS_ROWS + k) * DFTK_BOYS_W);
+            const double2 c01 = __ldg(row), c23 = __ldg(row + 1), c45 = __ldg(row + 2), c67 = __ldg(row + 3);
+            double f = fma(c67.y, d, c67.x);
+            f = fma(f, d, c45.y);
+            f = fma(f, d, c45.x);
+            f = fma(f, d, c23.y);
+            f = fma(f, d, c23.x);
+            f = fma(f, d, c01.y);
+            F[L] = fma(f, d, c01.x);
             if (L > 0) {
-                double e = fma(d, 1.0 / 7.0, 1.0);
-                e = fma(d * (1.0 / 6.0), e, 1.0);
-                e = fma(d * 0.2, e, 1.0);
-                e = fma(d * 0.25, e, 1.0);
-                e = fma(d * (1.0 / 3.0), e, 1.0);
-                e = fma(d * 0.5, e, 1.0);
-                e = fma(d, e, 1.0);
-                e *= __ldg(row + DFTK_BOYS_EXPCOL);
+                double e = fma(d, 1.0 / 5040.0, 1.0 / 720.0);
+                e = fma(e, d, 1.0 / 120.0);
+                e = fma(e, d, 1.0 / 24.0);
+                e = fma(e, d, 1.0 / 6.0);
+                e = fma(e, d, 0.5);
+                e = fma(e, d, 1.0);
+                e = fma(e, d, 1.0);
+                e *= __ldg(g_bexp64 + k);
                 const double x2 = x + x;
 #pragma unroll
                 for (int m = L - 1; m >= 0; --m) F[m] = fma(x2, F[m + 1], e) * (1.0 / (2 * m + 1));
@@ -60,36 +67,34 @@ template <int L> struct Boys<double, L> {
         } else {
             const double rs = ::rsqrt(x);
             F[0] = 0.88622692545275801365 * rs;
-            if (L > 0) {
-                const double e = ::exp(-x);
-                const double h = 0.5 * rs * rs;
+            const double h = 0.5 * rs * rs;
 #pragma unroll
-                for (int m = 0; m < L; ++m) F[m + 1] = fma((double)(2 * m + 1), F[m], -e) * h;
-            }
+            for (int m = 0; m < L; ++m) F[m + 1] = ((double)(2 * m + 1) * h) * F[m];
         }
     }
 };
 
 template <int L> struct Boys<float, L> {
-    static_assert(L + 4 < DFTK_BOYS_EXPCOL, "Boys table too narrow");
+    static_assert(L < DFTK_BOYS_NL, "Boys order beyond the table");
     __device__ __forceinline__ static void eval(float x, float *F)
     {
         if (x < (float)DFTK_BOYS_TMAX) {
-            const int k = __float2int_rn(x * 10.0f);
+            const int k = max(__float2int_rn(x * 10.0f), 0);
             const float d = (float)k * 0.1f - x;
-            const float *row = g_boys32 + k * DFTK_BOYS_COLS;
-            float f = __ldg(row + L + 4);
-            f = fmaf(f, d * 0.25f, __ldg(row + L + 3));
-            f = fmaf(f, d * (1.0f / 3.0f), __ldg(row + L + 2));
-            f = fmaf(f, d * 0.5f, __ldg(row + L + 1));
-            f = fmaf(f, d, __ldg(row + L));
-            F[L] = f;
+            const float4 *row = reinterpret_cast<const float4 *>(
+                g_boys32 + ((size_t)L * DFTK_BOYS_ROWS + k) * DFTK_BOYS_W);
+            const float4 c0 = __ldg(row);
+            const float c4 = __ldg(reinterpret_cast<const float *>(row + 1));
+            float f = fmaf(c4, d, c0.w);
+            f = fmaf(f, d, c0.z);
+            f = fmaf(f, d, c0.y);
+            F[L] = fmaf(f, d, c0.x);
             if (L > 0) {
-                float e = fmaf(d, 0.25f, 1.0f);
-                e = fmaf(d * (1.0f / 3.0f), e, 1.0f);
-                e = fmaf(d * 0.5f, e, 1.0f);
-                e = fmaf(d, e, 1.0f);
-                e *= __ldg(row + DFTK_BOYS_EXPCOL);
+                float e = fmaf(d, 1.0f / 24.0f, 1.0f / 6.0f);
+                e = fmaf(e, d, 0.5f);
+                e = fmaf(e, d, 1.0f);
+                e = fmaf(e, d, 1.0f);
+                e *= __ldg(g_bexp32 + k);
                 const float x2 = x + x;
 #pragma unroll
                 for (int m = L - 1; m >= 0; --m) F[m] = fmaf(x2, F[m + 1], e) * (1.0f / (2 * m + 1));
@@ -97,37 +102,32 @@ template <int L> struct Boys<float, L> {
         } else {
             const float rs = ::rsqrtf(x);
             F[0] = 0.886226925f * rs;
-            if (L > 0) {
-                const float e = __expf(-x);
-                const float h = 0.5f * rs * rs;
+            const float h = 0.5f * rs * rs;
 #pragma unroll
-                for (int m = 0; m < L; ++m) F[m + 1] = fmaf((float)(2 * m + 1), F[m], -e) * h;
-            }
+            for (int m = 0; m < L; ++m) F[m + 1] = ((float)(2 * m + 1) * h) * F[m];
         }
     }
 };
 
-// Runtime-order Boys (orders up to 14) for the generic drop-in kernels and the
-// one-electron kernel: same scheme, loop instead of unrolled code.
+// Runtime-order Boys (orders 0..8) for the generic drop-in kernels and the
+// one-electron kernel: same scheme and tables, order chosen at run time.
 __device__ __forceinline__ void boys_runtime(int L, double x, double *F)
 {
     if (x < DFTK_BOYS_TMAX) {
-        const int k = __double2int_rn(x * 10.0);
+        const int k = max(__double2int_rn(x * 10.0), 0);
         const double d = (double)k * 0.1 - x;
-        const double *row = g_boys64 + k * DFTK_BOYS_COLS;
-        const int top = L + 6 < DFTK_BOYS_EXPCOL ? 6 : DFTK_BOYS_EXPCOL - 1 - L;
-        double f = __ldg(row + L + top);
-        for (int j = top; j >= 1; --j) f = fma(f, d / j, __ldg(row + L + j - 1));
+        const double *row = g_boys64 + ((size_t)L * DFTK_BOYS_ROWS + k) * DFTK_BOYS_W;
+        double f = __ldg(row + 7);
+        for (int j = 6; j >= 0; --j) f = fma(f, d, __ldg(row + j));
         F[L] = f;
         double e = 1.0;
         for (int j = 7; j >= 1; --j) e = fma(d / j, e, 1.0);
-        e *= __ldg(row + DFTK_BOYS_EXPCOL);
+        e *= __ldg(g_bexp64 + k);
         for (int m = L - 1; m >= 0; --m) F[m] = (2.0 * x * F[m + 1] + e) / (2 * m + 1);
     } else {
         const double rs = ::rsqrt(x);
         F[0] = 0.88622692545275801365 * rs;
-        const double e = ::exp(-x);
         const double h = 0.5 * rs * rs;
-        for (int m = 0; m < L; ++m) F[m + 1] = ((2 * m + 1) * F[m] - e) * h;
+        for (int m = 0; m < L; ++m) F[m + 1] = (2 * m + 1) * h * F[m];
     }
 }

@@ -61,21 +61,36 @@ long double boys_series_ld(int m, long double T)
     return expl(-T) * sum;
 }
 
+std::vector<double> g_exp64;
+std::vector<float> g_exp32;
+
+// Per-order Taylor coefficients F_{L+j}(T_k) / j! (see boys.cuh).
 void build_tables()
 {
     if (!g_tab64.empty()) return;
-    g_tab64.assign(DFTK_BOYS_ROWS * DFTK_BOYS_COLS, 0.0);
-    g_tab32.assign(DFTK_BOYS_ROWS * DFTK_BOYS_COLS, 0.0f);
-    for (int k = 0; k < DFTK_BOYS_ROWS; ++k) {
-        const double t64 = (double)k * 0.1;         // grid the FP64 evaluator rounds to
-        const float t32f = (float)k * 0.1f;         // grid the FP32 evaluator rounds to
-        const long double t32 = (long double)t32f;
-        for (int m = 0; m < DFTK_BOYS_EXPCOL; ++m) {
-            g_tab64[k * DFTK_BOYS_COLS + m] = (double)boys_series_ld(m, (long double)t64);
-            g_tab32[k * DFTK_BOYS_COLS + m] = (float)boys_series_ld(m, t32);
+    const int R = DFTK_BOYS_ROWS, W = DFTK_BOYS_W, NL = DFTK_BOYS_NL;
+    g_tab64.assign((size_t)NL * R * W, 0.0);
+    g_tab32.assign((size_t)NL * R * W, 0.0f);
+    g_exp64.assign(R, 0.0);
+    g_exp32.assign(R, 0.0f);
+    std::vector<long double> F64(NL + W), F32(NL + W);
+    for (int k = 0; k < R; ++k) {
+        const long double t64 = (long double)((double)k * 0.1);  // grid the FP64 evaluator rounds to
+        const long double t32 = (long double)((float)k * 0.1f);  // grid the FP32 evaluator rounds to
+        for (int m = 0; m < NL + W; ++m) {
+            F64[m] = boys_series_ld(m, t64);
+            F32[m] = boys_series_ld(m, t32);
         }
-        g_tab64[k * DFTK_BOYS_COLS + DFTK_BOYS_EXPCOL] = (double)expl(-(long double)t64);
-        g_tab32[k * DFTK_BOYS_COLS + DFTK_BOYS_EXPCOL] = (float)expl(-t32);
+        for (int L = 0; L < NL; ++L) {
+            long double fact = 1.0L;
+            for (int j = 0; j < W; ++j) {
+                if (j > 0) fact *= j;
+                g_tab64[((size_t)L * R + k) * W + j] = (double)(F64[L + j] / fact);
+                g_tab32[((size_t)L * R + k) * W + j] = (float)(F32[L + j] / fact);
+            }
+        }
+        g_exp64[k] = (double)expl(-t64);
+        g_exp32[k] = (float)expl(-t32);
     }
 }
 
@@ -89,6 +104,8 @@ int ensure_init()
     build_tables();
     DFTK_CUDA(cudaMemcpyToSymbol(g_boys64, g_tab64.data(), sizeof(double) * g_tab64.size()));
     DFTK_CUDA(cudaMemcpyToSymbol(g_boys32, g_tab32.data(), sizeof(float) * g_tab32.size()));
+    DFTK_CUDA(cudaMemcpyToSymbol(g_bexp64, g_exp64.data(), sizeof(double) * g_exp64.size()));
+    DFTK_CUDA(cudaMemcpyToSymbol(g_bexp32, g_exp32.data(), sizeof(float) * g_exp32.size()));
     g_init_done[dev] = true;
     return DFTK_OK;
 }
@@ -184,7 +201,7 @@ int dftk_boys(int mmax, long long n, const double *T, double *F, dftk_stream_t s
 
 int dftk_boys32(int mmax, long long n, const float *T, float *F, dftk_stream_t stream)
 {
-    if (mmax < 0 || mmax > 6 || n < 0 || (n > 0 && (!T || !F))) return fail(DFTK_ERR_ARG, "dftk_boys32: bad arguments (mmax 0..6)");
+    if (mmax < 0 || mmax > 8 || n < 0 || (n > 0 && (!T || !F))) return fail(DFTK_ERR_ARG, "dftk_boys32: bad arguments (mmax 0..8)");
     DFTK_INIT();
     if (n == 0) return DFTK_OK;
     k_boys32_test<<<blocks_for(n, 128), 128, 0, (cudaStream_t)stream>>>(mmax, n, T, F);
@@ -245,6 +262,7 @@ int dftk_eri_blocks(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N
         P.ab[k] = pairs[k].ab;
         P.np[k] = pairs[k].nprim;
         P.rec64[k] = pairs[k].rec64;
+        P.rec32[k] = pairs[k].rec32;
         P.n_pairs[k] = pairs[k].n_pairs;
         P.kmax[k] = pairs[k].kmax;
     }

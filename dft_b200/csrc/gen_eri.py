@@ -11,9 +11,10 @@ of one shell quartet from primitive-pair records:
     (ab|cd) = sum_{ij} sum_{tuv} E^{ab}_{tuv}(i) sum_{kl}
               sum_{tau nu phi} (-1)^{tau+nu+phi} E^{cd}_{tau nu phi}(kl) R_{t+tau,u+nu,v+phi}(i, kl)
 
-with the bra Hermite-to-Cartesian transform hoisted out of the ket primitive
-loop (W holds the ket-transformed, ket-primitive-summed Hermite integrals of
-one bra primitive).  Only non-zero Hermite coefficients are emitted.
+with the Hermite-to-Cartesian transform of the outer-loop side hoisted out
+of the inner primitive loop (W/V hold the inner-side-transformed,
+inner-primitive-summed Hermite integrals of one outer primitive).  Only
+non-zero Hermite coefficients are emitted.
 
 Primitive-pair record fields (SoA, ``base[(f * kmax + k) * stride + pair]``):
     0 Px, 1 Py, 2 Pz, 3 p, 4 K (sqrt(2 pi^{5/2}) c_a c_b N_a N_b exp(-mu AB^2) / p),
@@ -27,14 +28,17 @@ import os
 
 AX = "xyz"
 COMPS = {0: [(0, 0, 0)], 1: [(1, 0, 0), (0, 1, 0), (0, 0, 1)]}
-# (La, Lb, Lc, Ld, nsplit); nsplit > 1 splits the c components across threads
+# (La, Lb, Lc, Ld, nsplit, loop order); nsplit > 1 splits the c components
+# across threads.  'ket' order keeps each thread's ket records in the outer
+# loop (read once per quartet, the bra records re-read as warp broadcasts);
+# it costs no extra FMAs where the bra and ket transforms are equally cheap.
 CLASSES = [
-    (0, 0, 0, 0, 1),
-    (1, 0, 0, 0, 1),
-    (1, 0, 1, 0, 1),
-    (1, 1, 0, 0, 1),
-    (1, 1, 1, 0, 1),
-    (1, 1, 1, 1, 3),
+    (0, 0, 0, 0, 1, "ket"),
+    (1, 0, 0, 0, 1, "ket"),
+    (1, 0, 1, 0, 1, "ket"),
+    (1, 1, 0, 0, 1, "bra"),
+    (1, 1, 1, 0, 1, "bra"),
+    (1, 1, 1, 1, 3, "bra"),
 ]
 PAIR_FIELDS = {0: 5, 1: 9, 2: 12}
 
@@ -145,7 +149,10 @@ def side_pre(side, pc):
     return lines
 
 
-def gen_class(cid, la, lb, lc, ld, nsplit, split):
+def gen_class(cid, la, lb, lc, ld, nsplit, split, order):
+    """order 'bra': bra primitive loop outside, the ket transform per primitive
+    quartet and the bra transform hoisted; order 'ket': the mirror image (ket
+    records loaded once per quartet, bra records re-read as warp-broadcast)."""
     pa, pk = la + lb, lc + ld
     L = pa + pk
     A, B, C, D = COMPS[la], COMPS[lb], COMPS[lc], COMPS[ld]
@@ -153,70 +160,95 @@ def gen_class(cid, la, lb, lc, ld, nsplit, split):
     if nsplit > 1:
         cds = [(ic, id_) for (ic, id_) in cds if ic == split]
     abs_ = [(ia, ib) for ia in range(len(A)) for ib in range(len(B))]
-    hb = herm(pa)
-    # ket expansions per local cd
     ket_terms = {m: e3d("k", C[ic], D[id_], sign=True) for m, (ic, id_) in enumerate(cds)}
     bra_terms = {n: e3d("b", A[ia], B[ib]) for n, (ia, ib) in enumerate(abs_)}
+    hb, hk = herm(pa), herm(pk)
     needed = set()
     for m, terms in ket_terms.items():
         for (tk, uk, vk), _, _ in terms:
             for (tb, ub, vb) in hb:
                 needed.add((tb + tk, ub + uk, vb + vk))
-    body = []
-    w = lambda m, h: f"W{m}_{h[0]}{h[1]}{h[2]}"
-    body.append("#pragma unroll 1")
-    body.append("for (int i = 0; i < bra_n; ++i) {")
-    body += ["  " + s for s in side_loads("b", pa, "bra", "i")]
-    body += ["  " + s for s in side_pre("b", pa)]
-    for m in range(len(cds)):
-        body.append("  T " + ", ".join(f"{w(m, h)} = T(0)" for h in hb) + ";")
-    body.append("  #pragma unroll 1")
-    body.append("  for (int j = 0; j < ket_n; ++j) {")
-    inner = []
-    inner += side_loads("k", pk, "ket", "j")
-    inner += side_pre("k", pk)
-    inner.append("const T s = bp + kp;")
-    inner.append("const T rs = Math<T>::rsqrt(s);")
-    inner.append("const T rho = bp * kp * (rs * rs);")
-    inner.append("const T X = bPx - kPx, Y = bPy - kPy, Z = bPz - kPz;")
-    inner.append("const T pre = bK * kK * rs;")
-    inner.append("const T m2rho = T(-2) * rho;")
-    inner.append(f"T F[{L + 1}];")
-    inner.append(f"Boys<T, {L}>::eval(rho * (X * X + Y * Y + Z * Z), F);")
-    inner += r_program(sorted(needed), L)
-    # ket coefficients, then W accumulation
-    for m, terms in ket_terms.items():
-        for (tk, uk, vk), sg, facs in terms:
-            cname = f"kc{m}_{tk}{uk}{vk}"
-            if facs:
-                expr = prod(facs)
-                inner.append(f"const T {cname} = {'-' if sg < 0 else ''}{expr};")
-            for (tb, ub, vb) in hb:
-                r = rname(tb + tk, ub + uk, vb + vk, 0)
-                tgt = w(m, (tb, ub, vb))
-                if facs:
-                    inner.append(f"{tgt} = fma({cname}, {r}, {tgt});")
-                else:
-                    op = "-=" if sg < 0 else "+="
-                    inner.append(f"{tgt} {op} {r};")
-    body += ["    " + s for s in inner]
-    body.append("  }")
-    # bra transform
-    for n, terms in bra_terms.items():
-        for m in range(len(cds)):
-            acc = f"I[{n * len(cds) + m}]"
-            for (tb, ub, vb), _, facs in terms:
-                src = w(m, (tb, ub, vb))
-                if facs:
-                    body.append(f"  {acc} = fma({prod(facs)}, {src}, {acc});")
-                else:
-                    body.append(f"  {acc} += {src};")
-    body.append("}")
     nloc = len(abs_) * len(cds)
+    core = [
+        "const T s = bp + kp;",
+        "const T rs = Math<T>::rsqrt(s);",
+        "const T rho = bp * kp * (rs * rs);",
+        "const T X = bPx - kPx, Y = bPy - kPy, Z = bPz - kPz;",
+        "const T pre = bK * kK * rs;",
+    ]
+    if L > 0:
+        core.append("const T m2rho = T(-2) * rho;")
+    core.append(f"T F[{L + 1}];")
+    core.append(f"Boys<T, {L}>::eval(rho * (X * X + Y * Y + Z * Z), F);")
+    core += r_program(sorted(needed), L)
+    body = []
+    if order == "bra":
+        w = lambda m, h: f"W{m}_{h[0]}{h[1]}{h[2]}"
+        body.append("#pragma unroll 1")
+        body.append("for (int i = 0; i < bra_n; ++i) {")
+        body += ["  " + x for x in side_loads("b", pa, "bra", "i") + side_pre("b", pa)]
+        for m in range(len(cds)):
+            body.append("  T " + ", ".join(f"{w(m, h)} = T(0)" for h in hb) + ";")
+        body.append("  #pragma unroll 1")
+        body.append("  for (int j = 0; j < ket_n; ++j) {")
+        inner = side_loads("k", pk, "ket", "j") + side_pre("k", pk) + list(core)
+        for m, terms in ket_terms.items():
+            for (tk, uk, vk), sg, facs in terms:
+                cname = f"kc{m}_{tk}{uk}{vk}"
+                if facs:
+                    inner.append(f"const T {cname} = {'-' if sg < 0 else ''}{prod(facs)};")
+                for (tb, ub, vb) in hb:
+                    r = rname(tb + tk, ub + uk, vb + vk, 0)
+                    tgt = w(m, (tb, ub, vb))
+                    if facs:
+                        inner.append(f"{tgt} = fma({cname}, {r}, {tgt});")
+                    else:
+                        inner.append(f"{tgt} {'-=' if sg < 0 else '+='} {r};")
+        body += ["    " + x for x in inner]
+        body.append("  }")
+        for n, terms in bra_terms.items():
+            for m in range(len(cds)):
+                acc = f"I[{n * len(cds) + m}]"
+                for (tb, ub, vb), _, facs in terms:
+                    src = w(m, (tb, ub, vb))
+                    body.append(f"  {acc} = fma({prod(facs)}, {src}, {acc});" if facs else f"  {acc} += {src};")
+        body.append("}")
+    else:
+        w = lambda n, h: f"V{n}_{h[0]}{h[1]}{h[2]}"
+        body.append("#pragma unroll 1")
+        body.append("for (int j = 0; j < ket_n; ++j) {")
+        body += ["  " + x for x in side_loads("k", pk, "ket", "j") + side_pre("k", pk)]
+        for n in range(len(abs_)):
+            body.append("  T " + ", ".join(f"{w(n, h)} = T(0)" for h in hk) + ";")
+        body.append("  #pragma unroll 1")
+        body.append("  for (int i = 0; i < bra_n; ++i) {")
+        inner = side_loads("b", pa, "bra", "i") + side_pre("b", pa) + list(core)
+        for n, terms in bra_terms.items():
+            for (tb, ub, vb), _, facs in terms:
+                cname = f"bc{n}_{tb}{ub}{vb}"
+                if facs:
+                    inner.append(f"const T {cname} = {prod(facs)};")
+                for (tk, uk, vk) in hk:
+                    r = rname(tb + tk, ub + uk, vb + vk, 0)
+                    tgt = w(n, (tk, uk, vk))
+                    inner.append(f"{tgt} = fma({cname}, {r}, {tgt});" if facs else f"{tgt} += {r};")
+        body += ["    " + x for x in inner]
+        body.append("  }")
+        # ket transform with the (-1)^{tau+nu+phi} sign
+        for m, terms in ket_terms.items():
+            for n in range(len(abs_)):
+                acc = f"I[{n * len(cds) + m}]"
+                for (tk, uk, vk), sg, facs in terms:
+                    src = w(n, (tk, uk, vk))
+                    if facs:
+                        body.append(f"  {acc} = fma({'-' if sg < 0 else ''}{prod(facs)}, {src}, {acc});")
+                    else:
+                        body.append(f"  {acc} {'-=' if sg < 0 else '+='} {src};")
+        body.append("}")
     cd_c = ", ".join(str(ic) for ic, _ in cds)
     cd_d = ", ".join(str(id_) for _, id_ in cds)
     head = [
-        f"// class {cid}: ({'sp'[la]}{'sp'[lb]}|{'sp'[lc]}{'sp'[ld]}), split {split} of {nsplit}",
+        f"// class {cid}: ({'sp'[la]}{'sp'[lb]}|{'sp'[lc]}{'sp'[ld]}), split {split} of {nsplit}, {order} primitives outside",
         "template <typename T>",
         f"struct EriClass<T, {cid}, {split}> {{",
         f"  static constexpr int LA = {la}, LB = {lb}, LC = {lc}, LD = {ld}, L = {L};",
@@ -229,11 +261,11 @@ def gen_class(cid, la, lb, lc, ld, nsplit, split):
         "      const T* __restrict__ bra, long long bra_stride, int bra_kmax, int bra_row, int bra_n,",
         "      const T* __restrict__ ket, long long ket_stride, int ket_kmax, int ket_row, int ket_n,",
         "      T (&I)[NI]) {",
-        f"    #pragma unroll",
-        f"    for (int q = 0; q < NI; ++q) I[q] = T(0);",
+        "    #pragma unroll",
+        "    for (int q = 0; q < NI; ++q) I[q] = T(0);",
     ]
     tail = ["  }", "};", ""]
-    return head + ["    " + s for s in body] + tail
+    return head + ["    " + x for x in body] + tail
 
 
 def main():
@@ -247,9 +279,9 @@ def main():
         f"#define DFTK_N_CLASSES {len(CLASSES)}",
         "",
     ]
-    for cid, (la, lb, lc, ld, ns) in enumerate(CLASSES):
+    for cid, (la, lb, lc, ld, ns, order) in enumerate(CLASSES):
         for s in range(ns):
-            out += gen_class(cid, la, lb, lc, ld, ns, s)
+            out += gen_class(cid, la, lb, lc, ld, ns, s, order)
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "eri_classes.cuh")
     with open(path, "w") as fh:
         fh.write("\n".join(out) + "\n")

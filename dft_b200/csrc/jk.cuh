@@ -262,12 +262,16 @@ __device__ __forceinline__ void jk_one(const JkParams &P, bool valid, int row, i
     constexpr int X = E::BRA_CLASS, Yc = E::KET_CLASS;
     const int *abX = P.ab[X];
     const int *abY = P.ab[Yc];
-    const int a = valid ? abX[2 * row] : 0, b = valid ? abX[2 * row + 1] : 0;
-    const int c = valid ? abY[2 * ket] : 0, d = valid ? abY[2 * ket + 1] : 0;
-    // warp-uniform bra pair lets the Y_ab reduction happen in registers
+    // warp-uniform bra pair lets the Y_ab reduction happen in registers; the
+    // caller guarantees at least one valid lane
     const int lead = __ffs(__ballot_sync(DFTK_FULL_MASK, valid)) - 1;
     const int row0 = __shfl_sync(DFTK_FULL_MASK, row, lead < 0 ? 0 : lead);
     const bool uniform = __all_sync(DFTK_FULL_MASK, !valid || row == row0);
+    // screened-out lanes take the bra shells of the warp's lead row: lane 0
+    // writes the reduced Y_ab block with its own a, b even when it is invalid
+    const int brow = valid ? row : row0;
+    const int a = abX[2 * brow], b = abX[2 * brow + 1];
+    const int c = valid ? abY[2 * ket] : 0, d = valid ? abY[2 * ket + 1] : 0;
     T I[E::NI];
     if (valid) {
         eri_run<C, T, S>(RecOf<C, T>::get(P, X), P.n_pairs[X], P.kmax[X], row, P.np[X][row],
@@ -345,6 +349,7 @@ struct EmitParams {
     const int *ab[3];
     const int *np[3];
     const double *rec64[3];
+    const float *rec32[3];
     int n_pairs[3];
     int kmax[3];
     long long nq;
@@ -355,15 +360,23 @@ struct EmitParams {
 
 __device__ __forceinline__ int ncomp(int l) { return (l + 1) * (l + 2) / 2; }
 
-template <int C, int S>
-__device__ __forceinline__ void emit_split(const EmitParams &P, int row, int ket, int flags,
-                                           const int (&slot)[4], const int (&stride)[4], double *out)
+template <typename T> struct EmitRec;
+template <> struct EmitRec<double> {
+    __device__ static const double *get(const EmitParams &P, int pc) { return P.rec64[pc]; }
+};
+template <> struct EmitRec<float> {
+    __device__ static const float *get(const EmitParams &P, int pc) { return P.rec32[pc]; }
+};
+
+template <int C, typename T, int S>
+__device__ __forceinline__ void emit_split(const EmitParams &P, int row, int ket, const int (&slot)[4],
+                                           const int (&stride)[4], double *out)
 {
-    using E = EriClass<double, C, S>;
+    using E = EriClass<T, C, S>;
     constexpr int X = E::BRA_CLASS, Yc = E::KET_CLASS;
-    double I[E::NI];
-    eri_run<C, double, S>(P.rec64[X], P.n_pairs[X], P.kmax[X], row, P.np[X][row], P.rec64[Yc],
-                          P.n_pairs[Yc], P.kmax[Yc], ket, P.np[Yc][ket], I);
+    T I[E::NI];
+    eri_run<C, T, S>(EmitRec<T>::get(P, X), P.n_pairs[X], P.kmax[X], row, P.np[X][row], EmitRec<T>::get(P, Yc),
+                     P.n_pairs[Yc], P.kmax[Yc], ket, P.np[Yc][ket], I);
 #pragma unroll
     for (int ia = 0; ia < E::NA; ++ia)
 #pragma unroll
@@ -374,29 +387,46 @@ __device__ __forceinline__ void emit_split(const EmitParams &P, int row, int ket
                 long long o = 0;
 #pragma unroll
                 for (int k = 0; k < 4; ++k) o += (long long)comp[k] * stride[slot[k]];
-                out[o] = I[(ia * E::NB + ib) * E::NCD + m];
+                out[o] = (double)I[(ia * E::NB + ib) * E::NCD + m];
             }
 }
 
-template <int C>
-__device__ __forceinline__ void emit_class(const EmitParams &P, int row, int ket, int flags,
-                                           const int (&slot)[4], const int (&stride)[4], double *out)
+template <int C, typename T>
+__device__ __forceinline__ void emit_class(const EmitParams &P, int row, int ket, const int (&slot)[4],
+                                           const int (&stride)[4], double *out)
 {
-    emit_split<C, 0>(P, row, ket, flags, slot, stride, out);
-    if constexpr (EriClass<double, C, 0>::NSPLIT > 1) {
-        emit_split<C, 1>(P, row, ket, flags, slot, stride, out);
-        emit_split<C, 2>(P, row, ket, flags, slot, stride, out);
+    emit_split<C, T, 0>(P, row, ket, slot, stride, out);
+    if constexpr (EriClass<T, C, 0>::NSPLIT > 1) {
+        emit_split<C, T, 1>(P, row, ket, slot, stride, out);
+        emit_split<C, T, 2>(P, row, ket, slot, stride, out);
     }
 }
 
+template <typename T>
+__device__ __forceinline__ void emit_any(int C, const EmitParams &P, int row, int ket, const int (&slot)[4],
+                                         const int (&stride)[4], double *out)
+{
+    switch (C) {
+    case 0: emit_class<0, T>(P, row, ket, slot, stride, out); break;
+    case 1: emit_class<1, T>(P, row, ket, slot, stride, out); break;
+    case 2: emit_class<2, T>(P, row, ket, slot, stride, out); break;
+    case 3: emit_class<3, T>(P, row, ket, slot, stride, out); break;
+    case 4: emit_class<4, T>(P, row, ket, slot, stride, out); break;
+    default: emit_class<5, T>(P, row, ket, slot, stride, out); break;
+    }
+}
+
+// One thread per quartet; desc flags bit 3 selects the FP32 evaluation.
 __global__ void k_emit(const EmitParams P)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= P.nq) return;
     const int C = P.desc[4 * t], row = P.desc[4 * t + 1], ket = P.desc[4 * t + 2], flags = P.desc[4 * t + 3];
+    if (C < 0 || C >= DFTK_N_QCLASS) return;
     constexpr int bra_pc[6] = {0, 1, 1, 2, 2, 2};
     constexpr int ket_pc[6] = {0, 0, 1, 0, 1, 2};
     const int X = bra_pc[C], Yc = ket_pc[C];
+    if (row < 0 || row >= P.n_pairs[X] || ket < 0 || ket >= P.n_pairs[Yc]) return;
     // my (a', b', c', d') -> reference slots
     int slot[4];
     const int bra0 = (flags & 4) ? 2 : 0, ket0 = (flags & 4) ? 0 : 2;
@@ -413,12 +443,6 @@ __global__ void k_emit(const EmitParams P)
     stride[1] = nref[3] * nref[2];
     stride[0] = nref[3] * nref[2] * nref[1];
     double *out = P.out + P.out_off[t];
-    switch (C) {
-    case 0: emit_class<0>(P, row, ket, flags, slot, stride, out); break;
-    case 1: emit_class<1>(P, row, ket, flags, slot, stride, out); break;
-    case 2: emit_class<2>(P, row, ket, flags, slot, stride, out); break;
-    case 3: emit_class<3>(P, row, ket, flags, slot, stride, out); break;
-    case 4: emit_class<4>(P, row, ket, flags, slot, stride, out); break;
-    default: emit_class<5>(P, row, ket, flags, slot, stride, out); break;
-    }
+    if (flags & 8) emit_any<float>(C, P, row, ket, slot, stride, out);
+    else emit_any<double>(C, P, row, ket, slot, stride, out);
 }

@@ -26,6 +26,7 @@ __global__ void k_one_electron(const dftk_shells_t sh, int n_atoms, const double
     while ((long long)(i + 1) * (i + 2) / 2 <= t) ++i;
     const int j = (int)(t - (long long)i * (i + 1) / 2);
     const int la = sh.l[i], lb = sh.l[j];
+    if (la > 1 || lb > 1 || la < 0 || lb < 0) return;  // s and p only; blocks left untouched
     const int ca = (la + 1) * (la + 2) / 2, cb = (lb + 1) * (lb + 2) / 2;
     const int N = sh.n_ao;
     const double A[3] = {sh.xyz[3 * i], sh.xyz[3 * i + 1], sh.xyz[3 * i + 2]};
@@ -121,8 +122,13 @@ __global__ void k_nuclear_dropin(const double *exp_a, const double *exp_b, const
     const double al = exp_a[a], be = exp_b[b];
     double E[3][16];
     int len[3];
+    bool ok = true;
     for (int x = 0; x < 3; ++x) {
         const int la = pow_a[3 * a + x], lb = pow_b[3 * b + x];
+        ok = ok && la >= 0 && lb >= 0 && la + lb < DFTK_E_SLOTS;
+    }
+    for (int x = 0; x < 3; ++x) {
+        const int la = ok ? pow_a[3 * a + x] : 0, lb = ok ? pow_b[3 * b + x] : 0;
         herm_E1d(al, be, cen_a[x], cen_b[x], la, lb, E[x]);
         len[x] = la + lb + 1;
         for (int t = len[x]; t < 16; ++t) E[x][t] = 0.0;
@@ -133,7 +139,7 @@ __global__ void k_nuclear_dropin(const double *exp_a, const double *exp_b, const
     const double Pz = (al * cen_a[2] + be * cen_b[2]) / p;
     const int L = len[0] + len[1] + len[2] - 3;
     double value = 0.0;
-    if (L <= DFTK_GENERIC_LMAX) {
+    if (ok && L <= DFTK_GENERIC_LMAX) {
         constexpr int D = DFTK_GENERIC_LMAX + 1;
         for (int c = 0; c < num_atoms; ++c) {
             double R[D * D * D];
@@ -176,9 +182,13 @@ __global__ void k_eri_dropin(int K_ab, const double *p_ab, const double *P_ab, c
     const double *Ei[3] = {Exab + DFTK_E_SLOTS * i, Eyab + DFTK_E_SLOTS * i, Ezab + DFTK_E_SLOTS * i};
     const double *Ej[3] = {Excd + DFTK_E_SLOTS * j, Eycd + DFTK_E_SLOTS * j, Ezcd + DFTK_E_SLOTS * j};
     int len[3];
-    for (int x = 0; x < 3; ++x) len[x] = ni[x] + nj[x] - 1;
+    bool ok = true;
+    for (int x = 0; x < 3; ++x) {
+        len[x] = ni[x] + nj[x] - 1;
+        ok = ok && ni[x] >= 1 && nj[x] >= 1 && ni[x] <= DFTK_E_SLOTS && nj[x] <= DFTK_E_SLOTS;
+    }
     const int L = len[0] + len[1] + len[2] - 3;
-    if (L > DFTK_GENERIC_LMAX) {
+    if (!ok || L > DFTK_GENERIC_LMAX) {
         out[q] = __longlong_as_double(0x7ff8000000000000ULL);
         return;
     }
@@ -266,6 +276,8 @@ __global__ void k_boys32_test(int mmax, long long n, const float *T, float *F)
     case 3: boys32_store<3>(T[t], o); break;
     case 4: boys32_store<4>(T[t], o); break;
     case 5: boys32_store<5>(T[t], o); break;
-    default: boys32_store<6>(T[t], o); break;
+    case 6: boys32_store<6>(T[t], o); break;
+    case 7: boys32_store<7>(T[t], o); break;
+    default: boys32_store<8>(T[t], o); break;
     }
 }

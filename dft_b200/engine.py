@@ -270,9 +270,12 @@ class IntegralEngine:
         off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
         return desc.astype(np.int32), off
 
-    def eri_blocks(self, quads: np.ndarray) -> Tuple[torch.Tensor, np.ndarray]:
-        """Contracted ERI blocks of reference quartets, flat in calc_eri layout."""
+    def eri_blocks(self, quads: np.ndarray, fp32: bool = False) -> Tuple[torch.Tensor, np.ndarray]:
+        """Contracted ERI blocks of reference quartets, flat in calc_eri layout
+        (fp32=True evaluates with the mixed path's FP32 kernels)."""
         desc, off = self.quartet_descriptors(quads)
+        if fp32:
+            desc[:, 3] |= 8
         d_desc = self._t(desc.reshape(-1), torch.int32)
         d_off = self._t(off[:-1], torch.int64)
         out = torch.zeros(int(off[-1]), dtype=torch.float64, device=self.device)

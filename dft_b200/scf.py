@@ -11,7 +11,9 @@
   incremental Fock build F_k = F_{k-1} + G(D_k - D_{k-1}) with optional mixed
   precision (quartets whose Schwarz bound times |dD| is below tau_fp32 run in
   FP32, accumulation in FP64).  Full FP64 rebuilds every ``rebuild_every``
-  iterations and at convergence bound the drift of the incremental sum.
+  iterations, and for every iteration once RMS(dD) < ``finish_factor`` x
+  dtol, bound the drift of the incremental sum, so convergence is always
+  judged on a full FP64 Fock matrix.
 
 Dense linear algebra (eigh via cuSOLVER, DIIS solves) runs in torch float64
 on the same device; it is O(N^3) with N <= a few hundred, far below the J/K
@@ -41,7 +43,7 @@ class SCFResult:
     fock_builds: int
     fock_seconds: float
     energy_history: List[float] = field(default_factory=list)
-    energy_last_build: Optional[float] = None  # energy from the last (incremental/mixed) Fock build
+    energy_last_build: Optional[float] = None  # energy of the last incremental (FP64 or mixed) Fock build
     counts: Optional[List[int]] = None
 
 
@@ -145,29 +147,35 @@ class _Diis:
             self.E.pop(0)
 
     def extrapolate(self) -> torch.Tensor:
+        """Pulay extrapolation.  The bordered system [[B, -1], [-1, 0]] is
+        solved through its eigen-decomposition with eigenvalues below 1e-14 of
+        the largest dropped, so nearly dependent error vectors (late
+        iterations) cannot blow the coefficients up."""
         n = len(self.F)
         if n < 2:
             return self.F[-1]
         dev = self.F[0].device
-        B = torch.empty((n + 1, n + 1), dtype=torch.float64, device=dev)
         E = torch.stack(self.E).reshape(n, -1)
-        B[:n, :n] = E @ E.T
+        Bm = E @ E.T
+        scale = Bm.diagonal().max().clamp_min(1e-300)
+        B = torch.zeros((n + 1, n + 1), dtype=torch.float64, device=dev)
+        B[:n, :n] = Bm / scale
         B[n, :n] = -1.0
         B[:n, n] = -1.0
-        B[n, n] = 0.0
         rhs = torch.zeros(n + 1, dtype=torch.float64, device=dev)
         rhs[n] = -1.0
-        try:
-            c = torch.linalg.solve(B, rhs)[:n]
-        except RuntimeError:
-            return self.F[-1]
+        w, v = torch.linalg.eigh(B)
+        keep = w.abs() > 1e-14 * w.abs().max()
+        c = v[:, keep] @ ((v[:, keep].T @ rhs) / w[keep])
+        c = c[:n]
         return torch.einsum("i,iab->ab", c, torch.stack(self.F))
 
 
 def scf_rhf(engine: IntegralEngine, H: torch.Tensor, S: torch.Tensor, n_occ: int, e_nn: float,
             diis: int = 8, etol: float = 1e-10, dtol: float = 1e-8, max_iter: int = 200,
             incremental: bool = True, mixed: bool = False, tau: float = 1e-12, tau_fp32: float = 1e-6,
-            rebuild_every: int = 12, final_rebuild: bool = True, count_quartets: bool = False,
+            rebuild_every: int = 12, count_quartets: bool = False,
+            finish_factor: float = 100.0,
             D_guess: Optional[torch.Tensor] = None, callback=None) -> SCFResult:
     dev = engine.device
     H = H.to(dev, torch.float64)
@@ -187,10 +195,13 @@ def scf_rhf(engine: IntegralEngine, H: torch.Tensor, S: torch.Tensor, n_occ: int
     counts_t = torch.zeros(12, dtype=torch.int64, device=dev) if count_quartets else None
     since_full = 0
     E_last = None
+    e_last_incremental = None
+    finishing = False  # density nearly converged: full FP64 builds from here on
     for it in range(max_iter + 1):
-        full = (G is None) or (not incremental) or since_full >= rebuild_every
+        full = (G is None) or (not incremental) or since_full >= rebuild_every or finishing
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
+        incremental_build = False
         if full:
             J, K, _ = engine.jk(2.0 * D, D, tau=min(tau, 1e-14), counts=counts_t)
             G = J - K
@@ -200,6 +211,7 @@ def scf_rhf(engine: IntegralEngine, H: torch.Tensor, S: torch.Tensor, n_occ: int
             J, K, _ = engine.jk(2.0 * dD, dD, mixed=mixed, tau=tau, tau_fp32=tau_fp32, counts=counts_t)
             G = G + (J - K)
             since_full += 1
+            incremental_build = True
         torch.cuda.synchronize(dev)
         tb += time.perf_counter() - t0
         builds += 1
@@ -216,21 +228,20 @@ def scf_rhf(engine: IntegralEngine, H: torch.Tensor, S: torch.Tensor, n_occ: int
         D_new = _occupied_density(C, n_occ)
         dE = float("inf") if E_prev is None else abs(E - E_prev)
         rms = float(torch.sqrt(torch.mean((D_new - D) ** 2)))
+        if incremental_build:
+            e_last_incremental = E
         if callback is not None:
             callback(it, E, dE, rms, D)
-        if dE < etol and rms < dtol:
-            e_last_build = E
-            if final_rebuild:
-                torch.cuda.synchronize(dev)
-                t0 = time.perf_counter()
-                J, K, _ = engine.jk(2.0 * D, D, tau=min(tau, 1e-14))
-                torch.cuda.synchronize(dev)
-                tb += time.perf_counter() - t0
-                builds += 1
-                F = H + J - K
-                E = float(torch.sum(D * (H + F))) + e_nn
-                w, Cp = torch.linalg.eigh(X.T @ F @ X)
-                C = X @ Cp
+        # Incremental sums carry the contributions screening dropped (each below
+        # tau, ~1e8 of them): near convergence switch to full FP64 builds so the
+        # 1e-10 energy criterion is tested on a consistent Fock matrix.
+        if incremental and rms < finish_factor * dtol:
+            finishing = True
+        if dE < etol and rms < dtol and (not incremental or not incremental_build):
+            e_last_build = e_last_incremental if e_last_incremental is not None else E
+            # F is a full FP64 build at D here, so E needs no extra rebuild
+            w, Cp = torch.linalg.eigh(X.T @ F @ X)
+            C = X @ Cp
             return SCFResult(E, True, it, D, D, C, w, F, builds, tb, energies, e_last_build,
                              counts_t.tolist() if counts_t is not None else None)
         E_prev = E

@@ -99,7 +99,8 @@ const char *dftk_last_error(void);
 int dftk_init(void);
 
 /* F_0..F_mmax(T) for n arguments: F[i * (mmax + 1) + m] (boys/taylor,
- * shelled.py:174-211).  precision 64 or 32 (32 reads T32/F32 instead). */
+ * shelled.py:174-211), through the evaluators the ERI kernels use:
+ * mmax 0..8 in FP64 and (dftk_boys32) FP32. */
 int dftk_boys(int mmax, long long n, const double *T, double *F, dftk_stream_t stream);
 int dftk_boys32(int mmax, long long n, const float *T, float *F, dftk_stream_t stream);
 
@@ -122,8 +123,10 @@ int dftk_one_electron(const dftk_shells_t *shells, int n_atoms, const double *at
  * shelled.py:640-691).  desc[4 * t] = {quartet class, bra row, ket row, flags}
  * with flags bit0 = bra pair stored as (b, a), bit1 = ket pair stored as
  * (d, c), bit2 = bra and ket exchanged, all relative to the reference quartet
- * (a, b, c, d); block t is written at out + out_off[t] in the reference's
- * (n_ao_a, n_ao_b, n_ao_c, n_ao_d) row-major layout. */
+ * (a, b, c, d), and bit3 = evaluate with the FP32 kernels (the mixed path);
+ * block t is written at out + out_off[t] in the reference's
+ * (n_ao_a, n_ao_b, n_ao_c, n_ao_d) row-major layout.  Descriptors out of
+ * range are skipped (their block is left untouched). */
 int dftk_eri_blocks(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N_PCLASS],
                     long long n_quartets, const int *desc, const long long *out_off,
                     double *out, dftk_stream_t stream);
