@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.dirname(HERE)
 REPO = os.path.dirname(PKG)
 LIB = os.path.join(PKG, "libdftk.so")
-SOURCES = ["dftk.cu"]
+SOURCES = ["dftk.cu", "jk_noalloc.cu"]
 HEADERS = ["common.cuh", "boys.cuh", "eri_classes.cuh", "jk.cuh", "generic.cuh", "onee.cuh"]
 
 NVCC_FLAGS = [

@@ -177,6 +177,13 @@ int launch_jk_all(const JkParams &P, cudaStream_t s)
 
 }  // namespace
 
+// Lets the other translation units of the library report errors through
+// dftk_last_error(); hidden, not part of the C-ABI.
+extern "C" __attribute__((visibility("hidden"))) void dftk_internal_set_error(const char *msg)
+{
+    g_last_error = msg ? msg : "";
+}
+
 extern "C" {
 
 int dftk_version(void) { return 100; }

@@ -147,6 +147,19 @@ int dftk_jk(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N_PCLASS]
             double *J, double *K_a, double *K_b, int flags, double tau, double tau_fp32,
             void *workspace, size_t workspace_bytes, long long *counts, dftk_stream_t stream);
 
+/* dftk_jk for callers that cannot allocate device memory (no counterpart in
+ * the reference).  Same arguments as dftk_jk without the workspace: the
+ * scratch is a fixed device array inside the library (about 7 MB, held on
+ * every GPU that loads the library until exit), so the molecule may have at
+ * most 512 basis functions and 512 shells (DFTK_ERR_SIZE otherwise).  All
+ * calls share that array: calls that overlap on the GPU race, so keep them on
+ * one stream.  The first call on a device looks up the array's address with
+ * that device current; make it before any stream capture. */
+int dftk_jk_noalloc(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N_PCLASS],
+                    const dftk_queue_t *queue, const double *D, const double *D_a,
+                    const double *D_b, double *J, double *K_a, double *K_b, int flags,
+                    double tau, double tau_fp32, long long *counts, dftk_stream_t stream);
+
 /* Profiling aid: with timing enabled, later dftk_jk calls record CUDA events
  * around each class kernel on their stream.  dftk_jk_timing_read waits for
  * the last recorded call and writes ms[2 * DFTK_N_QCLASS] (FP64 launches,
