@@ -276,7 +276,7 @@ def run_dftk_arm(args, rank, world, local_rank):
     Dt = (2.0 * D).contiguous()
     N = eng.n_ao
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
-    counts = torch.zeros(12, dtype=torch.int64, device="cuda")
+    counts = torch.zeros(24, dtype=torch.int64, device="cuda")
     J = torch.empty((N, N), dtype=torch.float64, device="cuda")
     Ka = torch.empty((N, N), dtype=torch.float64, device="cuda")
 
@@ -289,7 +289,8 @@ def run_dftk_arm(args, rank, world, local_rank):
     counts.zero_()
     eng.jk(Dt, D, tau=1e-14, counts=counts)
     torch.cuda.synchronize()
-    evaluated = counts[:6].tolist()
+    evaluated = counts[:6].tolist()          # shell quartets per class
+    prim_evaluated = counts[12:18].tolist()  # primitive quartets per class (after primitive screening)
     # per-class kernel times (events around each class launch inside dftk_jk)
     lib = _lib.load()
     _lib.call("dftk_jk_timing", 1)
@@ -350,8 +351,7 @@ def run_dftk_arm(args, rank, world, local_rank):
         peaks = measured_peaks()
         fp64_peak = fma_peak_tflops(torch, lib, 64)
         fp32_peak = fma_peak_tflops(torch, lib, 32)
-        nprimq = eng.kmax * eng.kmax
-        class_flops = [FLOPS_PER_PRIM_QUARTET[c] * nprimq * evaluated[c] for c in range(6)]
+        class_flops = [FLOPS_PER_PRIM_QUARTET[c] * prim_evaluated[c] for c in range(6)]
         dom = int(np.argmax(class_ms[:6]))
         achieved = class_flops[dom] / (class_ms[dom] / 1e3) / 1e12
         total_flops = sum(class_flops)
@@ -381,6 +381,7 @@ def run_dftk_arm(args, rank, world, local_rank):
             "config": {"workload": WORKLOAD, "molecule": "(H2O)_64 4x4x4 lattice seed 0", "basis": "STO-3G",
                        "n_basis": N, "tau_schwarz": 1e-12, "tau_density": 1e-14,
                        "quartets_per_class": eng.quartet_totals(), "evaluated_per_class": evaluated,
+                       "primitive_quartets_per_class": prim_evaluated, "tau_prim": eng.tau_prim,
                        "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * N * N * 8,
                     "d2h_bytes_per_step": 3 * N * N * 8, "call": "shelled.fill_matrices (host NumPy arrays)"},

@@ -25,7 +25,7 @@ OK, ERR_ARG, ERR_CUDA, ERR_UNSUPPORTED, ERR_WORKSPACE, ERR_SIZE = range(6)
 SYMBOLS = (
     "dftk_version", "dftk_last_error", "dftk_init", "dftk_boys", "dftk_boys32",
     "dftk_pair_data", "dftk_schwarz", "dftk_one_electron", "dftk_eri_blocks",
-    "dftk_jk_workspace_bytes", "dftk_jk", "dftk_nuclear_kernel", "dftk_eri_kernel",
+    "dftk_jk_workspace_bytes", "dftk_jk_workspace_bytes_queue", "dftk_jk", "dftk_nuclear_kernel", "dftk_eri_kernel",
     "dftk_fma_burn", "dftk_jk_timing", "dftk_jk_timing_read", "dftk_jk_noalloc",
 )
 
@@ -61,6 +61,7 @@ class Pairs(ctypes.Structure):
         ("rec64", ctypes.c_void_p),
         ("rec32", ctypes.c_void_p),
         ("q", ctypes.c_void_p),
+        ("qp", ctypes.c_void_p),
     ]
 
 
@@ -69,6 +70,7 @@ class Queue(ctypes.Structure):
         ("n_rows", ctypes.c_longlong * N_QCLASS),
         ("total", ctypes.c_longlong * N_QCLASS),
         ("row_off", ctypes.c_void_p * N_QCLASS),
+        ("tau_prim", ctypes.c_double),
     ]
 
 
@@ -102,6 +104,7 @@ def load() -> ctypes.CDLL:
         "dftk_one_electron": ([ctypes.POINTER(Shells), i, vp, vp, vp, vp, vp, vp], i),
         "dftk_eri_blocks": ([ctypes.POINTER(Shells), ctypes.POINTER(Pairs), ll, vp, vp, vp, vp], i),
         "dftk_jk_workspace_bytes": ([i, i], sz),
+        "dftk_jk_workspace_bytes_queue": ([i, i, ctypes.POINTER(Queue)], sz),
         "dftk_jk": ([ctypes.POINTER(Shells), ctypes.POINTER(Pairs), ctypes.POINTER(Queue), vp, vp, vp,
                      vp, vp, vp, i, d, d, vp, sz, vp, vp], i),
         "dftk_nuclear_kernel": ([vp] * 8 + [i, i, i] + [vp] * 9 + [vp], i),

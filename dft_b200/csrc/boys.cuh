@@ -39,8 +39,9 @@ template <int L> struct Boys<double, L> {
     __device__ __forceinline__ static void eval(double x, double *F)
     {
         if (x < DFTK_BOYS_TMAX) {
-            const int k = max(__double2int_rn(x * 10.0), 0);
-            const double d = (double)k * 0.1 - x;
+            const double shifted = fma(x, 10.0, DFTK_ROUND_MAGIC64);  // x >= 0
+            const int k = __double2loint(shifted);
+            const double d = (shifted - DFTK_ROUND_MAGIC64) * 0.1 - x;
             const double2 *row = reinterpret_cast<const double2 *>(
                 g_boys64 + ((size_t)L * DFTK_BOYS_ROWS + k) * DFTK_BOYS_W);
             const double2 c01 = __ldg(row), c23 = __ldg(row + 1), c45 = __ldg(row + 2), c67 = __ldg(row + 3);
@@ -65,7 +66,7 @@ template <int L> struct Boys<double, L> {
                 for (int m = L - 1; m >= 0; --m) F[m] = fma(x2, F[m + 1], e) * (1.0 / (2 * m + 1));
             }
         } else {
-            const double rs = ::rsqrt(x);
+            const double rs = Math<double>::rsqrt(x);
             F[0] = 0.88622692545275801365 * rs;
             const double h = 0.5 * rs * rs;
 #pragma unroll
@@ -79,8 +80,9 @@ template <int L> struct Boys<float, L> {
     __device__ __forceinline__ static void eval(float x, float *F)
     {
         if (x < (float)DFTK_BOYS_TMAX) {
-            const int k = max(__float2int_rn(x * 10.0f), 0);
-            const float d = (float)k * 0.1f - x;
+            const float shifted = fmaf(x, 10.0f, DFTK_ROUND_MAGIC32);  // x >= 0
+            const int k = __float_as_int(shifted) - 0x4B400000;
+            const float d = (shifted - DFTK_ROUND_MAGIC32) * 0.1f - x;
             const float4 *row = reinterpret_cast<const float4 *>(
                 g_boys32 + ((size_t)L * DFTK_BOYS_ROWS + k) * DFTK_BOYS_W);
             const float4 c0 = __ldg(row);

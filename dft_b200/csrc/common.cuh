@@ -18,13 +18,31 @@ enum { F_PX = 0, F_PY, F_PZ, F_P, F_K, F_H, F_AX, F_AY, F_AZ, F_BX, F_BY, F_BZ }
 
 __host__ __device__ constexpr int pair_fields(int pc) { return pc == 0 ? 5 : (pc == 1 ? 9 : 12); }
 
+// Inverse square root for the positive, normal, float-range arguments of the
+// integral kernels (p + q, and T beyond the Boys table): an FP32 estimate
+// refined by two Newton-Raphson steps r <- r (3 - x r^2) / 2, each of which
+// squares the relative error (2^-22 -> 2^-43 -> below double rounding).  No
+// special-case branches, unlike a general-purpose rsqrt.
 template <typename T> struct Math;
 template <> struct Math<double> {
-    __device__ __forceinline__ static double rsqrt(double x) { return ::rsqrt(x); }
+    __device__ __forceinline__ static double rsqrt(double x)
+    {
+        double r = (double)::rsqrtf((float)x);
+        const double h = 0.5 * x;
+        r = r * fma(-h * r, r, 1.5);
+        r = r * fma(-h * r, r, 1.5);
+        return r;
+    }
 };
 template <> struct Math<float> {
     __device__ __forceinline__ static float rsqrt(float x) { return ::rsqrtf(x); }
 };
+
+// Round-to-nearest of 0 <= v < 2^31 by adding 1.5 * 2^52: the sum's low
+// mantissa bits hold the integer, and subtracting the constant again gives it
+// as a double, so the table index needs no double<->int conversion.
+#define DFTK_ROUND_MAGIC64 6755399441055744.0
+#define DFTK_ROUND_MAGIC32 12582912.0f  // 1.5 * 2^23, bit pattern 0x4B400000
 
 __device__ __forceinline__ double warp_sum(double v)
 {

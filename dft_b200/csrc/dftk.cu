@@ -162,6 +162,63 @@ int launch_jk_class(const JkParams &P, cudaStream_t s)
     return DFTK_OK;
 }
 
+template <int C, typename T>
+int launch_jk_list_class(const JkParams &P, cudaStream_t s)
+{
+    const long long ncand = P.total[C];
+    const int slot = C + (sizeof(T) == 4 ? DFTK_N_QCLASS : 0);
+    if (g_timing.enabled) g_timing.launched[slot] = false;
+    if (ncand <= 0) return DFTK_OK;
+    const long long warps = ((ncand + 31) / 32) * EriClass<T, C, 0>::NSPLIT;
+    long long blocks = (warps * 32 + 127) / 128;
+    const long long cap = 148LL * 16;
+    if (blocks > cap) blocks = cap;
+    if (g_timing.enabled) DFTK_CUDA(cudaEventRecord(g_timing.start[slot], s));
+    k_jk_list<C, T><<<(unsigned)blocks, 128, 0, s>>>(P);
+    DFTK_LAUNCHED("k_jk_list");
+    if (g_timing.enabled) {
+        DFTK_CUDA(cudaEventRecord(g_timing.stop[slot], s));
+        g_timing.launched[slot] = true;
+    }
+    return DFTK_OK;
+}
+
+template <int C>
+int launch_select_class(const JkParams &P, cudaStream_t s)
+{
+    const long long ncand = P.total[C];
+    if (ncand <= 0) return DFTK_OK;
+    long long blocks = (ncand + SELECT_TILE - 1) / SELECT_TILE;
+    const long long cap = 148LL * 8;
+    if (blocks > cap) blocks = cap;
+    k_select<C><<<(unsigned)blocks, SELECT_THREADS, 0, s>>>(P);
+    DFTK_LAUNCHED("k_select");
+    return DFTK_OK;
+}
+
+template <typename T>
+int launch_jk_list_all(const JkParams &P, cudaStream_t s)
+{
+    int st;
+    if ((st = launch_jk_list_class<0, T>(P, s))) return st;
+    if ((st = launch_jk_list_class<1, T>(P, s))) return st;
+    if ((st = launch_jk_list_class<2, T>(P, s))) return st;
+    if ((st = launch_jk_list_class<3, T>(P, s))) return st;
+    if ((st = launch_jk_list_class<4, T>(P, s))) return st;
+    if ((st = launch_jk_list_class<5, T>(P, s))) return st;
+    return DFTK_OK;
+}
+
+// Workspace with room for the selection lists: the base layout, then the
+// 2 * DFTK_N_QCLASS list counters, then one int2 per candidate of every class.
+size_t ws_list_bytes(int ns, int n_ao, const dftk_queue_t *q)
+{
+    size_t b = ws_bytes(ns, n_ao) + 256;
+    for (int c = 0; c < DFTK_N_QCLASS; ++c)
+        if (q->n_rows[c] > 0 && q->total[c] > 0) b += (((size_t)q->total[c] * sizeof(int2)) + 255) & ~(size_t)255;
+    return b;
+}
+
 template <typename T>
 int launch_jk_all(const JkParams &P, cudaStream_t s)
 {
@@ -220,6 +277,8 @@ int dftk_pair_data(const dftk_shells_t *shells, int pair_class, dftk_pairs_t *pa
 {
     if (!shells || !pairs || pair_class < 0 || pair_class > 2) return fail(DFTK_ERR_ARG, "dftk_pair_data: bad arguments");
     if (pairs->n_pairs < 0 || pairs->kmax <= 0) return fail(DFTK_ERR_ARG, "dftk_pair_data: bad pair counts");
+    if ((long long)pairs->n_pairs * pairs->kmax * pair_fields(pair_class) >= (1LL << 31))
+        return fail(DFTK_ERR_SIZE, "dftk_pair_data: records exceed 2^31 elements (32-bit offsets)");
     DFTK_INIT();
     const long long n = (long long)pairs->n_pairs * pairs->kmax;
     if (n == 0) return DFTK_OK;
@@ -235,9 +294,12 @@ int dftk_schwarz(const dftk_shells_t *shells, int pair_class, dftk_pairs_t *pair
     const int n = pairs->n_pairs;
     if (n == 0) return DFTK_OK;
     cudaStream_t s = (cudaStream_t)stream;
-    if (pair_class == 0) k_schwarz<0><<<blocks_for(n, 64), 64, 0, s>>>(*pairs);
-    else if (pair_class == 1) k_schwarz<1><<<blocks_for(n, 64), 64, 0, s>>>(*pairs);
-    else k_schwarz<2><<<blocks_for(n, 64), 64, 0, s>>>(*pairs);
+    if (pairs->kmax > DFTK_MAX_KPAIR) return fail(DFTK_ERR_SIZE, "dftk_schwarz: more than 64 primitive pairs per pair");
+    if (!pairs->qp) return fail(DFTK_ERR_ARG, "dftk_schwarz: null qp");
+    const int nf = pair_fields(pair_class);
+    if (pair_class == 0) k_schwarz<0><<<blocks_for(n, 64), 64, 0, s>>>(*pairs, nf);
+    else if (pair_class == 1) k_schwarz<1><<<blocks_for(n, 64), 64, 0, s>>>(*pairs, nf);
+    else k_schwarz<2><<<blocks_for(n, 64), 64, 0, s>>>(*pairs, nf);
     DFTK_LAUNCHED("k_schwarz");
     return DFTK_OK;
 }
@@ -270,6 +332,7 @@ int dftk_eri_blocks(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N
         P.np[k] = pairs[k].nprim;
         P.rec64[k] = pairs[k].rec64;
         P.rec32[k] = pairs[k].rec32;
+        P.qp[k] = pairs[k].qp;
         P.n_pairs[k] = pairs[k].n_pairs;
         P.kmax[k] = pairs[k].kmax;
     }
@@ -286,6 +349,12 @@ size_t dftk_jk_workspace_bytes(int n_shells, int n_ao)
 {
     if (n_shells < 0 || n_ao < 0) return 0;
     return ws_bytes(n_shells, n_ao);
+}
+
+size_t dftk_jk_workspace_bytes_queue(int n_shells, int n_ao, const dftk_queue_t *queue)
+{
+    if (n_shells < 0 || n_ao < 0 || !queue) return 0;
+    return ws_list_bytes(n_shells, n_ao, queue);
 }
 
 int dftk_jk(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N_PCLASS], const dftk_queue_t *queue,
@@ -325,6 +394,7 @@ int dftk_jk(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N_PCLASS]
         P.rec64[k] = pairs[k].rec64;
         P.rec32[k] = pairs[k].rec32;
         P.q[k] = pairs[k].q;
+        P.qp[k] = pairs[k].qp;
         P.n_pairs[k] = pairs[k].n_pairs;
         P.kmax[k] = pairs[k].kmax;
     }
@@ -335,6 +405,7 @@ int dftk_jk(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N_PCLASS]
         if (P.total[c] < 0) return fail(DFTK_ERR_ARG, "dftk_jk: negative candidate total");
         if (P.total[c] > 0 && !queue->row_off[c]) return fail(DFTK_ERR_ARG, "dftk_jk: missing row offsets");
     }
+    P.tau_prim = (float)queue->tau_prim;
     P.D = D;
     P.Da = D_a;
     P.Db = uhf ? D_b : D_a;
@@ -344,6 +415,34 @@ int dftk_jk(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N_PCLASS]
     P.Dsh = Dsh;
     P.uhf = uhf;
     int st;
+    if (workspace_bytes >= ws_list_bytes(ns, N, queue)) {
+        // selection pass + list-driven class kernels
+        unsigned char *cur = (unsigned char *)workspace + ws_bytes(ns, N);
+        P.heads = (unsigned long long *)cur;
+        cur += 256;
+        for (int c = 0; c < DFTK_N_QCLASS; ++c) {
+            P.list[c] = (int2 *)cur;
+            if (P.total[c] > 0) cur += (((size_t)P.total[c] * sizeof(int2)) + 255) & ~(size_t)255;
+        }
+        DFTK_CUDA(cudaMemsetAsync(P.heads, 0, 2 * DFTK_N_QCLASS * sizeof(unsigned long long), s));
+        P.tau = tau;
+        P.tau32 = mixed ? tau_fp32 : tau;
+        P.counts = counts;
+        if ((st = launch_select_class<0>(P, s))) return st;
+        if ((st = launch_select_class<1>(P, s))) return st;
+        if ((st = launch_select_class<2>(P, s))) return st;
+        if ((st = launch_select_class<3>(P, s))) return st;
+        if ((st = launch_select_class<4>(P, s))) return st;
+        if ((st = launch_select_class<5>(P, s))) return st;
+        if ((st = launch_jk_list_all<double>(P, s))) return st;
+        if (mixed) {
+            P.counts = counts ? counts + DFTK_N_QCLASS : nullptr;
+            if ((st = launch_jk_list_all<float>(P, s))) return st;
+        }
+        k_symmetrize<<<blocks_for((long long)nn, 256), 256, 0, s>>>(N, Y, Za, Zb, J, K_a, K_b, uhf);
+        DFTK_LAUNCHED("k_symmetrize");
+        return DFTK_OK;
+    }
     P.tau_lo = tau;
     P.tau_hi = INFINITY;
     if (mixed) {

@@ -15,27 +15,46 @@ struct EriClass<T, 0, 0> {
   static constexpr int BRA_CLASS = 0, KET_CLASS = 0;
   __device__ static constexpr int cd_c(int m) { constexpr int v[] = {0}; return v[m]; }
   __device__ static constexpr int cd_d(int m) { constexpr int v[] = {0}; return v[m]; }
-  __device__ __forceinline__ static void run(
-      const T* __restrict__ bra, long long bra_stride, int bra_kmax, int bra_row, int bra_n,
-      const T* __restrict__ ket, long long ket_stride, int ket_kmax, int ket_row, int ket_n,
-      T (&I)[NI]) {
+  // Returns the number of primitive quartets evaluated: both sides'
+  // primitive pairs come sorted by descending primitive Schwarz factor q,
+  // and the loops stop once q_bra * q_ket < eps (each skipped primitive
+  // quartet is bounded by that product, Cauchy-Schwarz per primitive pair).
+  __device__ __forceinline__ static int run(
+      const T* __restrict__ bra, const float* __restrict__ bra_q, long long bra_stride, int bra_kmax,
+      int bra_row, int bra_n,
+      const T* __restrict__ ket, const float* __restrict__ ket_q, long long ket_stride, int ket_kmax,
+      int ket_row, int ket_n, float eps, T (&I)[NI]) {
     #pragma unroll
     for (int q = 0; q < NI; ++q) I[q] = T(0);
+    int evaluated = 0;
+    const int bra_st = (int)bra_stride, ket_st = (int)ket_stride;
+    const int bra_fs = bra_kmax * bra_st, ket_fs = ket_kmax * ket_st;
+    const T* __restrict__ bra_p = bra + bra_row;
+    const T* __restrict__ ket_p = ket + ket_row;
+    const float* __restrict__ bra_qp = bra_q + bra_row;
+    const float* __restrict__ ket_qp = ket_q + ket_row;
+    const float bq0 = bra_qp[0];
     #pragma unroll 1
     for (int j = 0; j < ket_n; ++j) {
-      const T kPx = ket[(0 * ket_kmax + j) * ket_stride + ket_row];
-      const T kPy = ket[(1 * ket_kmax + j) * ket_stride + ket_row];
-      const T kPz = ket[(2 * ket_kmax + j) * ket_stride + ket_row];
-      const T kp = ket[(3 * ket_kmax + j) * ket_stride + ket_row];
-      const T kK = ket[(4 * ket_kmax + j) * ket_stride + ket_row];
+      const float qo = __ldg(ket_qp + j * ket_st);
+      if (qo * bq0 < eps) break;
+      const T* __restrict__ krec = ket_p + j * ket_st;
+      const T kPx = __ldg(krec + 0);
+      const T kPy = __ldg(krec + ket_fs);
+      const T kPz = __ldg(krec + 2 * ket_fs);
+      const T kp = __ldg(krec + 3 * ket_fs);
+      const T kK = __ldg(krec + 4 * ket_fs);
       T V0_000 = T(0);
       #pragma unroll 1
       for (int i = 0; i < bra_n; ++i) {
-        const T bPx = bra[(0 * bra_kmax + i) * bra_stride + bra_row];
-        const T bPy = bra[(1 * bra_kmax + i) * bra_stride + bra_row];
-        const T bPz = bra[(2 * bra_kmax + i) * bra_stride + bra_row];
-        const T bp = bra[(3 * bra_kmax + i) * bra_stride + bra_row];
-        const T bK = bra[(4 * bra_kmax + i) * bra_stride + bra_row];
+        if (qo * __ldg(bra_qp + i * bra_st) < eps) break;
+        ++evaluated;
+        const T* __restrict__ brec = bra_p + i * bra_st;
+        const T bPx = __ldg(brec + 0);
+        const T bPy = __ldg(brec + bra_fs);
+        const T bPz = __ldg(brec + 2 * bra_fs);
+        const T bp = __ldg(brec + 3 * bra_fs);
+        const T bK = __ldg(brec + 4 * bra_fs);
         const T s = bp + kp;
         const T rs = Math<T>::rsqrt(s);
         const T rho = bp * kp * (rs * rs);
@@ -49,10 +68,11 @@ struct EriClass<T, 0, 0> {
       }
       I[0] += V0_000;
     }
+    return evaluated;
   }
 };
 
-// class 1: (ps|ss), split 0 of 1, ket primitives outside
+// class 1: (ps|ss), split 0 of 1, bra primitives outside
 template <typename T>
 struct EriClass<T, 1, 0> {
   static constexpr int LA = 1, LB = 0, LC = 0, LD = 0, L = 1;
@@ -61,33 +81,50 @@ struct EriClass<T, 1, 0> {
   static constexpr int BRA_CLASS = 1, KET_CLASS = 0;
   __device__ static constexpr int cd_c(int m) { constexpr int v[] = {0}; return v[m]; }
   __device__ static constexpr int cd_d(int m) { constexpr int v[] = {0}; return v[m]; }
-  __device__ __forceinline__ static void run(
-      const T* __restrict__ bra, long long bra_stride, int bra_kmax, int bra_row, int bra_n,
-      const T* __restrict__ ket, long long ket_stride, int ket_kmax, int ket_row, int ket_n,
-      T (&I)[NI]) {
+  // Returns the number of primitive quartets evaluated: both sides'
+  // primitive pairs come sorted by descending primitive Schwarz factor q,
+  // and the loops stop once q_bra * q_ket < eps (each skipped primitive
+  // quartet is bounded by that product, Cauchy-Schwarz per primitive pair).
+  __device__ __forceinline__ static int run(
+      const T* __restrict__ bra, const float* __restrict__ bra_q, long long bra_stride, int bra_kmax,
+      int bra_row, int bra_n,
+      const T* __restrict__ ket, const float* __restrict__ ket_q, long long ket_stride, int ket_kmax,
+      int ket_row, int ket_n, float eps, T (&I)[NI]) {
     #pragma unroll
     for (int q = 0; q < NI; ++q) I[q] = T(0);
+    int evaluated = 0;
+    const int bra_st = (int)bra_stride, ket_st = (int)ket_stride;
+    const int bra_fs = bra_kmax * bra_st, ket_fs = ket_kmax * ket_st;
+    const T* __restrict__ bra_p = bra + bra_row;
+    const T* __restrict__ ket_p = ket + ket_row;
+    const float* __restrict__ bra_qp = bra_q + bra_row;
+    const float* __restrict__ ket_qp = ket_q + ket_row;
+    const float kq0 = ket_qp[0];
     #pragma unroll 1
-    for (int j = 0; j < ket_n; ++j) {
-      const T kPx = ket[(0 * ket_kmax + j) * ket_stride + ket_row];
-      const T kPy = ket[(1 * ket_kmax + j) * ket_stride + ket_row];
-      const T kPz = ket[(2 * ket_kmax + j) * ket_stride + ket_row];
-      const T kp = ket[(3 * ket_kmax + j) * ket_stride + ket_row];
-      const T kK = ket[(4 * ket_kmax + j) * ket_stride + ket_row];
-      T V0_000 = T(0);
-      T V1_000 = T(0);
-      T V2_000 = T(0);
+    for (int i = 0; i < bra_n; ++i) {
+      const float qo = __ldg(bra_qp + i * bra_st);
+      if (qo * kq0 < eps) break;
+      const T* __restrict__ brec = bra_p + i * bra_st;
+      const T bPx = __ldg(brec + 0);
+      const T bPy = __ldg(brec + bra_fs);
+      const T bPz = __ldg(brec + 2 * bra_fs);
+      const T bp = __ldg(brec + 3 * bra_fs);
+      const T bK = __ldg(brec + 4 * bra_fs);
+      const T bh = __ldg(brec + 5 * bra_fs);
+      const T bAx = __ldg(brec + 6 * bra_fs);
+      const T bAy = __ldg(brec + 7 * bra_fs);
+      const T bAz = __ldg(brec + 8 * bra_fs);
+      T W0_000 = T(0), W0_001 = T(0), W0_010 = T(0), W0_100 = T(0);
       #pragma unroll 1
-      for (int i = 0; i < bra_n; ++i) {
-        const T bPx = bra[(0 * bra_kmax + i) * bra_stride + bra_row];
-        const T bPy = bra[(1 * bra_kmax + i) * bra_stride + bra_row];
-        const T bPz = bra[(2 * bra_kmax + i) * bra_stride + bra_row];
-        const T bp = bra[(3 * bra_kmax + i) * bra_stride + bra_row];
-        const T bK = bra[(4 * bra_kmax + i) * bra_stride + bra_row];
-        const T bh = bra[(5 * bra_kmax + i) * bra_stride + bra_row];
-        const T bAx = bra[(6 * bra_kmax + i) * bra_stride + bra_row];
-        const T bAy = bra[(7 * bra_kmax + i) * bra_stride + bra_row];
-        const T bAz = bra[(8 * bra_kmax + i) * bra_stride + bra_row];
+      for (int j = 0; j < ket_n; ++j) {
+        if (qo * __ldg(ket_qp + j * ket_st) < eps) break;
+        ++evaluated;
+        const T* __restrict__ krec = ket_p + j * ket_st;
+        const T kPx = __ldg(krec + 0);
+        const T kPy = __ldg(krec + ket_fs);
+        const T kPz = __ldg(krec + 2 * ket_fs);
+        const T kp = __ldg(krec + 3 * ket_fs);
+        const T kK = __ldg(krec + 4 * ket_fs);
         const T s = bp + kp;
         const T rs = Math<T>::rsqrt(s);
         const T rho = bp * kp * (rs * rs);
@@ -103,23 +140,19 @@ struct EriClass<T, 1, 0> {
         const T R001_0 = Z * R000_1;
         const T R010_0 = Y * R000_1;
         const T R100_0 = X * R000_1;
-        const T bc0_000 = bAx;
-        V0_000 = fma(bc0_000, R000_0, V0_000);
-        const T bc0_100 = bh;
-        V0_000 = fma(bc0_100, R100_0, V0_000);
-        const T bc1_000 = bAy;
-        V1_000 = fma(bc1_000, R000_0, V1_000);
-        const T bc1_010 = bh;
-        V1_000 = fma(bc1_010, R010_0, V1_000);
-        const T bc2_000 = bAz;
-        V2_000 = fma(bc2_000, R000_0, V2_000);
-        const T bc2_001 = bh;
-        V2_000 = fma(bc2_001, R001_0, V2_000);
+        W0_000 += R000_0;
+        W0_001 += R001_0;
+        W0_010 += R010_0;
+        W0_100 += R100_0;
       }
-      I[0] += V0_000;
-      I[1] += V1_000;
-      I[2] += V2_000;
+      I[0] = fma(bAx, W0_000, I[0]);
+      I[0] = fma(bh, W0_100, I[0]);
+      I[1] = fma(bAy, W0_000, I[1]);
+      I[1] = fma(bh, W0_010, I[1]);
+      I[2] = fma(bAz, W0_000, I[2]);
+      I[2] = fma(bh, W0_001, I[2]);
     }
+    return evaluated;
   }
 };
 
@@ -132,37 +165,56 @@ struct EriClass<T, 2, 0> {
   static constexpr int BRA_CLASS = 1, KET_CLASS = 1;
   __device__ static constexpr int cd_c(int m) { constexpr int v[] = {0, 1, 2}; return v[m]; }
   __device__ static constexpr int cd_d(int m) { constexpr int v[] = {0, 0, 0}; return v[m]; }
-  __device__ __forceinline__ static void run(
-      const T* __restrict__ bra, long long bra_stride, int bra_kmax, int bra_row, int bra_n,
-      const T* __restrict__ ket, long long ket_stride, int ket_kmax, int ket_row, int ket_n,
-      T (&I)[NI]) {
+  // Returns the number of primitive quartets evaluated: both sides'
+  // primitive pairs come sorted by descending primitive Schwarz factor q,
+  // and the loops stop once q_bra * q_ket < eps (each skipped primitive
+  // quartet is bounded by that product, Cauchy-Schwarz per primitive pair).
+  __device__ __forceinline__ static int run(
+      const T* __restrict__ bra, const float* __restrict__ bra_q, long long bra_stride, int bra_kmax,
+      int bra_row, int bra_n,
+      const T* __restrict__ ket, const float* __restrict__ ket_q, long long ket_stride, int ket_kmax,
+      int ket_row, int ket_n, float eps, T (&I)[NI]) {
     #pragma unroll
     for (int q = 0; q < NI; ++q) I[q] = T(0);
+    int evaluated = 0;
+    const int bra_st = (int)bra_stride, ket_st = (int)ket_stride;
+    const int bra_fs = bra_kmax * bra_st, ket_fs = ket_kmax * ket_st;
+    const T* __restrict__ bra_p = bra + bra_row;
+    const T* __restrict__ ket_p = ket + ket_row;
+    const float* __restrict__ bra_qp = bra_q + bra_row;
+    const float* __restrict__ ket_qp = ket_q + ket_row;
+    const float bq0 = bra_qp[0];
     #pragma unroll 1
     for (int j = 0; j < ket_n; ++j) {
-      const T kPx = ket[(0 * ket_kmax + j) * ket_stride + ket_row];
-      const T kPy = ket[(1 * ket_kmax + j) * ket_stride + ket_row];
-      const T kPz = ket[(2 * ket_kmax + j) * ket_stride + ket_row];
-      const T kp = ket[(3 * ket_kmax + j) * ket_stride + ket_row];
-      const T kK = ket[(4 * ket_kmax + j) * ket_stride + ket_row];
-      const T kh = ket[(5 * ket_kmax + j) * ket_stride + ket_row];
-      const T kAx = ket[(6 * ket_kmax + j) * ket_stride + ket_row];
-      const T kAy = ket[(7 * ket_kmax + j) * ket_stride + ket_row];
-      const T kAz = ket[(8 * ket_kmax + j) * ket_stride + ket_row];
+      const float qo = __ldg(ket_qp + j * ket_st);
+      if (qo * bq0 < eps) break;
+      const T* __restrict__ krec = ket_p + j * ket_st;
+      const T kPx = __ldg(krec + 0);
+      const T kPy = __ldg(krec + ket_fs);
+      const T kPz = __ldg(krec + 2 * ket_fs);
+      const T kp = __ldg(krec + 3 * ket_fs);
+      const T kK = __ldg(krec + 4 * ket_fs);
+      const T kh = __ldg(krec + 5 * ket_fs);
+      const T kAx = __ldg(krec + 6 * ket_fs);
+      const T kAy = __ldg(krec + 7 * ket_fs);
+      const T kAz = __ldg(krec + 8 * ket_fs);
       T V0_000 = T(0), V0_001 = T(0), V0_010 = T(0), V0_100 = T(0);
       T V1_000 = T(0), V1_001 = T(0), V1_010 = T(0), V1_100 = T(0);
       T V2_000 = T(0), V2_001 = T(0), V2_010 = T(0), V2_100 = T(0);
       #pragma unroll 1
       for (int i = 0; i < bra_n; ++i) {
-        const T bPx = bra[(0 * bra_kmax + i) * bra_stride + bra_row];
-        const T bPy = bra[(1 * bra_kmax + i) * bra_stride + bra_row];
-        const T bPz = bra[(2 * bra_kmax + i) * bra_stride + bra_row];
-        const T bp = bra[(3 * bra_kmax + i) * bra_stride + bra_row];
-        const T bK = bra[(4 * bra_kmax + i) * bra_stride + bra_row];
-        const T bh = bra[(5 * bra_kmax + i) * bra_stride + bra_row];
-        const T bAx = bra[(6 * bra_kmax + i) * bra_stride + bra_row];
-        const T bAy = bra[(7 * bra_kmax + i) * bra_stride + bra_row];
-        const T bAz = bra[(8 * bra_kmax + i) * bra_stride + bra_row];
+        if (qo * __ldg(bra_qp + i * bra_st) < eps) break;
+        ++evaluated;
+        const T* __restrict__ brec = bra_p + i * bra_st;
+        const T bPx = __ldg(brec + 0);
+        const T bPy = __ldg(brec + bra_fs);
+        const T bPz = __ldg(brec + 2 * bra_fs);
+        const T bp = __ldg(brec + 3 * bra_fs);
+        const T bK = __ldg(brec + 4 * bra_fs);
+        const T bh = __ldg(brec + 5 * bra_fs);
+        const T bAx = __ldg(brec + 6 * bra_fs);
+        const T bAy = __ldg(brec + 7 * bra_fs);
+        const T bAz = __ldg(brec + 8 * bra_fs);
         const T s = bp + kp;
         const T rs = Math<T>::rsqrt(s);
         const T rho = bp * kp * (rs * rs);
@@ -239,6 +291,7 @@ struct EriClass<T, 2, 0> {
       I[8] = fma(kAz, V2_000, I[8]);
       I[8] = fma(-kh, V2_001, I[8]);
     }
+    return evaluated;
   }
 };
 
@@ -251,26 +304,42 @@ struct EriClass<T, 3, 0> {
   static constexpr int BRA_CLASS = 2, KET_CLASS = 0;
   __device__ static constexpr int cd_c(int m) { constexpr int v[] = {0}; return v[m]; }
   __device__ static constexpr int cd_d(int m) { constexpr int v[] = {0}; return v[m]; }
-  __device__ __forceinline__ static void run(
-      const T* __restrict__ bra, long long bra_stride, int bra_kmax, int bra_row, int bra_n,
-      const T* __restrict__ ket, long long ket_stride, int ket_kmax, int ket_row, int ket_n,
-      T (&I)[NI]) {
+  // Returns the number of primitive quartets evaluated: both sides'
+  // primitive pairs come sorted by descending primitive Schwarz factor q,
+  // and the loops stop once q_bra * q_ket < eps (each skipped primitive
+  // quartet is bounded by that product, Cauchy-Schwarz per primitive pair).
+  __device__ __forceinline__ static int run(
+      const T* __restrict__ bra, const float* __restrict__ bra_q, long long bra_stride, int bra_kmax,
+      int bra_row, int bra_n,
+      const T* __restrict__ ket, const float* __restrict__ ket_q, long long ket_stride, int ket_kmax,
+      int ket_row, int ket_n, float eps, T (&I)[NI]) {
     #pragma unroll
     for (int q = 0; q < NI; ++q) I[q] = T(0);
+    int evaluated = 0;
+    const int bra_st = (int)bra_stride, ket_st = (int)ket_stride;
+    const int bra_fs = bra_kmax * bra_st, ket_fs = ket_kmax * ket_st;
+    const T* __restrict__ bra_p = bra + bra_row;
+    const T* __restrict__ ket_p = ket + ket_row;
+    const float* __restrict__ bra_qp = bra_q + bra_row;
+    const float* __restrict__ ket_qp = ket_q + ket_row;
+    const float kq0 = ket_qp[0];
     #pragma unroll 1
     for (int i = 0; i < bra_n; ++i) {
-      const T bPx = bra[(0 * bra_kmax + i) * bra_stride + bra_row];
-      const T bPy = bra[(1 * bra_kmax + i) * bra_stride + bra_row];
-      const T bPz = bra[(2 * bra_kmax + i) * bra_stride + bra_row];
-      const T bp = bra[(3 * bra_kmax + i) * bra_stride + bra_row];
-      const T bK = bra[(4 * bra_kmax + i) * bra_stride + bra_row];
-      const T bh = bra[(5 * bra_kmax + i) * bra_stride + bra_row];
-      const T bAx = bra[(6 * bra_kmax + i) * bra_stride + bra_row];
-      const T bAy = bra[(7 * bra_kmax + i) * bra_stride + bra_row];
-      const T bAz = bra[(8 * bra_kmax + i) * bra_stride + bra_row];
-      const T bBx = bra[(9 * bra_kmax + i) * bra_stride + bra_row];
-      const T bBy = bra[(10 * bra_kmax + i) * bra_stride + bra_row];
-      const T bBz = bra[(11 * bra_kmax + i) * bra_stride + bra_row];
+      const float qo = __ldg(bra_qp + i * bra_st);
+      if (qo * kq0 < eps) break;
+      const T* __restrict__ brec = bra_p + i * bra_st;
+      const T bPx = __ldg(brec + 0);
+      const T bPy = __ldg(brec + bra_fs);
+      const T bPz = __ldg(brec + 2 * bra_fs);
+      const T bp = __ldg(brec + 3 * bra_fs);
+      const T bK = __ldg(brec + 4 * bra_fs);
+      const T bh = __ldg(brec + 5 * bra_fs);
+      const T bAx = __ldg(brec + 6 * bra_fs);
+      const T bAy = __ldg(brec + 7 * bra_fs);
+      const T bAz = __ldg(brec + 8 * bra_fs);
+      const T bBx = __ldg(brec + 9 * bra_fs);
+      const T bBy = __ldg(brec + 10 * bra_fs);
+      const T bBz = __ldg(brec + 11 * bra_fs);
       const T bEx0 = bAx * bBx + bh;
       const T bEx1 = bh * (bAx + bBx);
       const T bEy0 = bAy * bBy + bh;
@@ -281,11 +350,14 @@ struct EriClass<T, 3, 0> {
       T W0_000 = T(0), W0_001 = T(0), W0_002 = T(0), W0_010 = T(0), W0_011 = T(0), W0_020 = T(0), W0_100 = T(0), W0_101 = T(0), W0_110 = T(0), W0_200 = T(0);
       #pragma unroll 1
       for (int j = 0; j < ket_n; ++j) {
-        const T kPx = ket[(0 * ket_kmax + j) * ket_stride + ket_row];
-        const T kPy = ket[(1 * ket_kmax + j) * ket_stride + ket_row];
-        const T kPz = ket[(2 * ket_kmax + j) * ket_stride + ket_row];
-        const T kp = ket[(3 * ket_kmax + j) * ket_stride + ket_row];
-        const T kK = ket[(4 * ket_kmax + j) * ket_stride + ket_row];
+        if (qo * __ldg(ket_qp + j * ket_st) < eps) break;
+        ++evaluated;
+        const T* __restrict__ krec = ket_p + j * ket_st;
+        const T kPx = __ldg(krec + 0);
+        const T kPy = __ldg(krec + ket_fs);
+        const T kPz = __ldg(krec + 2 * ket_fs);
+        const T kp = __ldg(krec + 3 * ket_fs);
+        const T kK = __ldg(krec + 4 * ket_fs);
         const T s = bp + kp;
         const T rs = Math<T>::rsqrt(s);
         const T rho = bp * kp * (rs * rs);
@@ -357,6 +429,7 @@ struct EriClass<T, 3, 0> {
       I[8] = fma(bEz1, W0_001, I[8]);
       I[8] = fma(bh2, W0_002, I[8]);
     }
+    return evaluated;
   }
 };
 
@@ -369,26 +442,42 @@ struct EriClass<T, 4, 0> {
   static constexpr int BRA_CLASS = 2, KET_CLASS = 1;
   __device__ static constexpr int cd_c(int m) { constexpr int v[] = {0, 1, 2}; return v[m]; }
   __device__ static constexpr int cd_d(int m) { constexpr int v[] = {0, 0, 0}; return v[m]; }
-  __device__ __forceinline__ static void run(
-      const T* __restrict__ bra, long long bra_stride, int bra_kmax, int bra_row, int bra_n,
-      const T* __restrict__ ket, long long ket_stride, int ket_kmax, int ket_row, int ket_n,
-      T (&I)[NI]) {
+  // Returns the number of primitive quartets evaluated: both sides'
+  // primitive pairs come sorted by descending primitive Schwarz factor q,
+  // and the loops stop once q_bra * q_ket < eps (each skipped primitive
+  // quartet is bounded by that product, Cauchy-Schwarz per primitive pair).
+  __device__ __forceinline__ static int run(
+      const T* __restrict__ bra, const float* __restrict__ bra_q, long long bra_stride, int bra_kmax,
+      int bra_row, int bra_n,
+      const T* __restrict__ ket, const float* __restrict__ ket_q, long long ket_stride, int ket_kmax,
+      int ket_row, int ket_n, float eps, T (&I)[NI]) {
     #pragma unroll
     for (int q = 0; q < NI; ++q) I[q] = T(0);
+    int evaluated = 0;
+    const int bra_st = (int)bra_stride, ket_st = (int)ket_stride;
+    const int bra_fs = bra_kmax * bra_st, ket_fs = ket_kmax * ket_st;
+    const T* __restrict__ bra_p = bra + bra_row;
+    const T* __restrict__ ket_p = ket + ket_row;
+    const float* __restrict__ bra_qp = bra_q + bra_row;
+    const float* __restrict__ ket_qp = ket_q + ket_row;
+    const float kq0 = ket_qp[0];
     #pragma unroll 1
     for (int i = 0; i < bra_n; ++i) {
-      const T bPx = bra[(0 * bra_kmax + i) * bra_stride + bra_row];
-      const T bPy = bra[(1 * bra_kmax + i) * bra_stride + bra_row];
-      const T bPz = bra[(2 * bra_kmax + i) * bra_stride + bra_row];
-      const T bp = bra[(3 * bra_kmax + i) * bra_stride + bra_row];
-      const T bK = bra[(4 * bra_kmax + i) * bra_stride + bra_row];
-      const T bh = bra[(5 * bra_kmax + i) * bra_stride + bra_row];
-      const T bAx = bra[(6 * bra_kmax + i) * bra_stride + bra_row];
-      const T bAy = bra[(7 * bra_kmax + i) * bra_stride + bra_row];
-      const T bAz = bra[(8 * bra_kmax + i) * bra_stride + bra_row];
-      const T bBx = bra[(9 * bra_kmax + i) * bra_stride + bra_row];
-      const T bBy = bra[(10 * bra_kmax + i) * bra_stride + bra_row];
-      const T bBz = bra[(11 * bra_kmax + i) * bra_stride + bra_row];
+      const float qo = __ldg(bra_qp + i * bra_st);
+      if (qo * kq0 < eps) break;
+      const T* __restrict__ brec = bra_p + i * bra_st;
+      const T bPx = __ldg(brec + 0);
+      const T bPy = __ldg(brec + bra_fs);
+      const T bPz = __ldg(brec + 2 * bra_fs);
+      const T bp = __ldg(brec + 3 * bra_fs);
+      const T bK = __ldg(brec + 4 * bra_fs);
+      const T bh = __ldg(brec + 5 * bra_fs);
+      const T bAx = __ldg(brec + 6 * bra_fs);
+      const T bAy = __ldg(brec + 7 * bra_fs);
+      const T bAz = __ldg(brec + 8 * bra_fs);
+      const T bBx = __ldg(brec + 9 * bra_fs);
+      const T bBy = __ldg(brec + 10 * bra_fs);
+      const T bBz = __ldg(brec + 11 * bra_fs);
       const T bEx0 = bAx * bBx + bh;
       const T bEx1 = bh * (bAx + bBx);
       const T bEy0 = bAy * bBy + bh;
@@ -401,15 +490,18 @@ struct EriClass<T, 4, 0> {
       T W2_000 = T(0), W2_001 = T(0), W2_002 = T(0), W2_010 = T(0), W2_011 = T(0), W2_020 = T(0), W2_100 = T(0), W2_101 = T(0), W2_110 = T(0), W2_200 = T(0);
       #pragma unroll 1
       for (int j = 0; j < ket_n; ++j) {
-        const T kPx = ket[(0 * ket_kmax + j) * ket_stride + ket_row];
-        const T kPy = ket[(1 * ket_kmax + j) * ket_stride + ket_row];
-        const T kPz = ket[(2 * ket_kmax + j) * ket_stride + ket_row];
-        const T kp = ket[(3 * ket_kmax + j) * ket_stride + ket_row];
-        const T kK = ket[(4 * ket_kmax + j) * ket_stride + ket_row];
-        const T kh = ket[(5 * ket_kmax + j) * ket_stride + ket_row];
-        const T kAx = ket[(6 * ket_kmax + j) * ket_stride + ket_row];
-        const T kAy = ket[(7 * ket_kmax + j) * ket_stride + ket_row];
-        const T kAz = ket[(8 * ket_kmax + j) * ket_stride + ket_row];
+        if (qo * __ldg(ket_qp + j * ket_st) < eps) break;
+        ++evaluated;
+        const T* __restrict__ krec = ket_p + j * ket_st;
+        const T kPx = __ldg(krec + 0);
+        const T kPy = __ldg(krec + ket_fs);
+        const T kPz = __ldg(krec + 2 * ket_fs);
+        const T kp = __ldg(krec + 3 * ket_fs);
+        const T kK = __ldg(krec + 4 * ket_fs);
+        const T kh = __ldg(krec + 5 * ket_fs);
+        const T kAx = __ldg(krec + 6 * ket_fs);
+        const T kAy = __ldg(krec + 7 * ket_fs);
+        const T kAz = __ldg(krec + 8 * ket_fs);
         const T s = bp + kp;
         const T rs = Math<T>::rsqrt(s);
         const T rho = bp * kp * (rs * rs);
@@ -624,6 +716,7 @@ struct EriClass<T, 4, 0> {
       I[26] = fma(bEz1, W2_001, I[26]);
       I[26] = fma(bh2, W2_002, I[26]);
     }
+    return evaluated;
   }
 };
 
@@ -636,26 +729,42 @@ struct EriClass<T, 5, 0> {
   static constexpr int BRA_CLASS = 2, KET_CLASS = 2;
   __device__ static constexpr int cd_c(int m) { constexpr int v[] = {0, 0, 0}; return v[m]; }
   __device__ static constexpr int cd_d(int m) { constexpr int v[] = {0, 1, 2}; return v[m]; }
-  __device__ __forceinline__ static void run(
-      const T* __restrict__ bra, long long bra_stride, int bra_kmax, int bra_row, int bra_n,
-      const T* __restrict__ ket, long long ket_stride, int ket_kmax, int ket_row, int ket_n,
-      T (&I)[NI]) {
+  // Returns the number of primitive quartets evaluated: both sides'
+  // primitive pairs come sorted by descending primitive Schwarz factor q,
+  // and the loops stop once q_bra * q_ket < eps (each skipped primitive
+  // quartet is bounded by that product, Cauchy-Schwarz per primitive pair).
+  __device__ __forceinline__ static int run(
+      const T* __restrict__ bra, const float* __restrict__ bra_q, long long bra_stride, int bra_kmax,
+      int bra_row, int bra_n,
+      const T* __restrict__ ket, const float* __restrict__ ket_q, long long ket_stride, int ket_kmax,
+      int ket_row, int ket_n, float eps, T (&I)[NI]) {
     #pragma unroll
     for (int q = 0; q < NI; ++q) I[q] = T(0);
+    int evaluated = 0;
+    const int bra_st = (int)bra_stride, ket_st = (int)ket_stride;
+    const int bra_fs = bra_kmax * bra_st, ket_fs = ket_kmax * ket_st;
+    const T* __restrict__ bra_p = bra + bra_row;
+    const T* __restrict__ ket_p = ket + ket_row;
+    const float* __restrict__ bra_qp = bra_q + bra_row;
+    const float* __restrict__ ket_qp = ket_q + ket_row;
+    const float kq0 = ket_qp[0];
     #pragma unroll 1
     for (int i = 0; i < bra_n; ++i) {
-      const T bPx = bra[(0 * bra_kmax + i) * bra_stride + bra_row];
-      const T bPy = bra[(1 * bra_kmax + i) * bra_stride + bra_row];
-      const T bPz = bra[(2 * bra_kmax + i) * bra_stride + bra_row];
-      const T bp = bra[(3 * bra_kmax + i) * bra_stride + bra_row];
-      const T bK = bra[(4 * bra_kmax + i) * bra_stride + bra_row];
-      const T bh = bra[(5 * bra_kmax + i) * bra_stride + bra_row];
-      const T bAx = bra[(6 * bra_kmax + i) * bra_stride + bra_row];
-      const T bAy = bra[(7 * bra_kmax + i) * bra_stride + bra_row];
-      const T bAz = bra[(8 * bra_kmax + i) * bra_stride + bra_row];
-      const T bBx = bra[(9 * bra_kmax + i) * bra_stride + bra_row];
-      const T bBy = bra[(10 * bra_kmax + i) * bra_stride + bra_row];
-      const T bBz = bra[(11 * bra_kmax + i) * bra_stride + bra_row];
+      const float qo = __ldg(bra_qp + i * bra_st);
+      if (qo * kq0 < eps) break;
+      const T* __restrict__ brec = bra_p + i * bra_st;
+      const T bPx = __ldg(brec + 0);
+      const T bPy = __ldg(brec + bra_fs);
+      const T bPz = __ldg(brec + 2 * bra_fs);
+      const T bp = __ldg(brec + 3 * bra_fs);
+      const T bK = __ldg(brec + 4 * bra_fs);
+      const T bh = __ldg(brec + 5 * bra_fs);
+      const T bAx = __ldg(brec + 6 * bra_fs);
+      const T bAy = __ldg(brec + 7 * bra_fs);
+      const T bAz = __ldg(brec + 8 * bra_fs);
+      const T bBx = __ldg(brec + 9 * bra_fs);
+      const T bBy = __ldg(brec + 10 * bra_fs);
+      const T bBz = __ldg(brec + 11 * bra_fs);
       const T bEx0 = bAx * bBx + bh;
       const T bEx1 = bh * (bAx + bBx);
       const T bEy0 = bAy * bBy + bh;
@@ -668,18 +777,21 @@ struct EriClass<T, 5, 0> {
       T W2_000 = T(0), W2_001 = T(0), W2_002 = T(0), W2_010 = T(0), W2_011 = T(0), W2_020 = T(0), W2_100 = T(0), W2_101 = T(0), W2_110 = T(0), W2_200 = T(0);
       #pragma unroll 1
       for (int j = 0; j < ket_n; ++j) {
-        const T kPx = ket[(0 * ket_kmax + j) * ket_stride + ket_row];
-        const T kPy = ket[(1 * ket_kmax + j) * ket_stride + ket_row];
-        const T kPz = ket[(2 * ket_kmax + j) * ket_stride + ket_row];
-        const T kp = ket[(3 * ket_kmax + j) * ket_stride + ket_row];
-        const T kK = ket[(4 * ket_kmax + j) * ket_stride + ket_row];
-        const T kh = ket[(5 * ket_kmax + j) * ket_stride + ket_row];
-        const T kAx = ket[(6 * ket_kmax + j) * ket_stride + ket_row];
-        const T kAy = ket[(7 * ket_kmax + j) * ket_stride + ket_row];
-        const T kAz = ket[(8 * ket_kmax + j) * ket_stride + ket_row];
-        const T kBx = ket[(9 * ket_kmax + j) * ket_stride + ket_row];
-        const T kBy = ket[(10 * ket_kmax + j) * ket_stride + ket_row];
-        const T kBz = ket[(11 * ket_kmax + j) * ket_stride + ket_row];
+        if (qo * __ldg(ket_qp + j * ket_st) < eps) break;
+        ++evaluated;
+        const T* __restrict__ krec = ket_p + j * ket_st;
+        const T kPx = __ldg(krec + 0);
+        const T kPy = __ldg(krec + ket_fs);
+        const T kPz = __ldg(krec + 2 * ket_fs);
+        const T kp = __ldg(krec + 3 * ket_fs);
+        const T kK = __ldg(krec + 4 * ket_fs);
+        const T kh = __ldg(krec + 5 * ket_fs);
+        const T kAx = __ldg(krec + 6 * ket_fs);
+        const T kAy = __ldg(krec + 7 * ket_fs);
+        const T kAz = __ldg(krec + 8 * ket_fs);
+        const T kBx = __ldg(krec + 9 * ket_fs);
+        const T kBy = __ldg(krec + 10 * ket_fs);
+        const T kBz = __ldg(krec + 11 * ket_fs);
         const T kEx0 = kAx * kBx + kh;
         const T kEx1 = kh * (kAx + kBx);
         const T kEy0 = kAy * kBy + kh;
@@ -987,6 +1099,7 @@ struct EriClass<T, 5, 0> {
       I[26] = fma(bEz1, W2_001, I[26]);
       I[26] = fma(bh2, W2_002, I[26]);
     }
+    return evaluated;
   }
 };
 
@@ -999,26 +1112,42 @@ struct EriClass<T, 5, 1> {
   static constexpr int BRA_CLASS = 2, KET_CLASS = 2;
   __device__ static constexpr int cd_c(int m) { constexpr int v[] = {1, 1, 1}; return v[m]; }
   __device__ static constexpr int cd_d(int m) { constexpr int v[] = {0, 1, 2}; return v[m]; }
-  __device__ __forceinline__ static void run(
-      const T* __restrict__ bra, long long bra_stride, int bra_kmax, int bra_row, int bra_n,
-      const T* __restrict__ ket, long long ket_stride, int ket_kmax, int ket_row, int ket_n,
-      T (&I)[NI]) {
+  // Returns the number of primitive quartets evaluated: both sides'
+  // primitive pairs come sorted by descending primitive Schwarz factor q,
+  // and the loops stop once q_bra * q_ket < eps (each skipped primitive
+  // quartet is bounded by that product, Cauchy-Schwarz per primitive pair).
+  __device__ __forceinline__ static int run(
+      const T* __restrict__ bra, const float* __restrict__ bra_q, long long bra_stride, int bra_kmax,
+      int bra_row, int bra_n,
+      const T* __restrict__ ket, const float* __restrict__ ket_q, long long ket_stride, int ket_kmax,
+      int ket_row, int ket_n, float eps, T (&I)[NI]) {
     #pragma unroll
     for (int q = 0; q < NI; ++q) I[q] = T(0);
+    int evaluated = 0;
+    const int bra_st = (int)bra_stride, ket_st = (int)ket_stride;
+    const int bra_fs = bra_kmax * bra_st, ket_fs = ket_kmax * ket_st;
+    const T* __restrict__ bra_p = bra + bra_row;
+    const T* __restrict__ ket_p = ket + ket_row;
+    const float* __restrict__ bra_qp = bra_q + bra_row;
+    const float* __restrict__ ket_qp = ket_q + ket_row;
+    const float kq0 = ket_qp[0];
     #pragma unroll 1
     for (int i = 0; i < bra_n; ++i) {
-      const T bPx = bra[(0 * bra_kmax + i) * bra_stride + bra_row];
-      const T bPy = bra[(1 * bra_kmax + i) * bra_stride + bra_row];
-      const T bPz = bra[(2 * bra_kmax + i) * bra_stride + bra_row];
-      const T bp = bra[(3 * bra_kmax + i) * bra_stride + bra_row];
-      const T bK = bra[(4 * bra_kmax + i) * bra_stride + bra_row];
-      const T bh = bra[(5 * bra_kmax + i) * bra_stride + bra_row];
-      const T bAx = bra[(6 * bra_kmax + i) * bra_stride + bra_row];
-      const T bAy = bra[(7 * bra_kmax + i) * bra_stride + bra_row];
-      const T bAz = bra[(8 * bra_kmax + i) * bra_stride + bra_row];
-      const T bBx = bra[(9 * bra_kmax + i) * bra_stride + bra_row];
-      const T bBy = bra[(10 * bra_kmax + i) * bra_stride + bra_row];
-      const T bBz = bra[(11 * bra_kmax + i) * bra_stride + bra_row];
+      const float qo = __ldg(bra_qp + i * bra_st);
+      if (qo * kq0 < eps) break;
+      const T* __restrict__ brec = bra_p + i * bra_st;
+      const T bPx = __ldg(brec + 0);
+      const T bPy = __ldg(brec + bra_fs);
+      const T bPz = __ldg(brec + 2 * bra_fs);
+      const T bp = __ldg(brec + 3 * bra_fs);
+      const T bK = __ldg(brec + 4 * bra_fs);
+      const T bh = __ldg(brec + 5 * bra_fs);
+      const T bAx = __ldg(brec + 6 * bra_fs);
+      const T bAy = __ldg(brec + 7 * bra_fs);
+      const T bAz = __ldg(brec + 8 * bra_fs);
+      const T bBx = __ldg(brec + 9 * bra_fs);
+      const T bBy = __ldg(brec + 10 * bra_fs);
+      const T bBz = __ldg(brec + 11 * bra_fs);
       const T bEx0 = bAx * bBx + bh;
       const T bEx1 = bh * (bAx + bBx);
       const T bEy0 = bAy * bBy + bh;
@@ -1031,18 +1160,21 @@ struct EriClass<T, 5, 1> {
       T W2_000 = T(0), W2_001 = T(0), W2_002 = T(0), W2_010 = T(0), W2_011 = T(0), W2_020 = T(0), W2_100 = T(0), W2_101 = T(0), W2_110 = T(0), W2_200 = T(0);
       #pragma unroll 1
       for (int j = 0; j < ket_n; ++j) {
-        const T kPx = ket[(0 * ket_kmax + j) * ket_stride + ket_row];
-        const T kPy = ket[(1 * ket_kmax + j) * ket_stride + ket_row];
-        const T kPz = ket[(2 * ket_kmax + j) * ket_stride + ket_row];
-        const T kp = ket[(3 * ket_kmax + j) * ket_stride + ket_row];
-        const T kK = ket[(4 * ket_kmax + j) * ket_stride + ket_row];
-        const T kh = ket[(5 * ket_kmax + j) * ket_stride + ket_row];
-        const T kAx = ket[(6 * ket_kmax + j) * ket_stride + ket_row];
-        const T kAy = ket[(7 * ket_kmax + j) * ket_stride + ket_row];
-        const T kAz = ket[(8 * ket_kmax + j) * ket_stride + ket_row];
-        const T kBx = ket[(9 * ket_kmax + j) * ket_stride + ket_row];
-        const T kBy = ket[(10 * ket_kmax + j) * ket_stride + ket_row];
-        const T kBz = ket[(11 * ket_kmax + j) * ket_stride + ket_row];
+        if (qo * __ldg(ket_qp + j * ket_st) < eps) break;
+        ++evaluated;
+        const T* __restrict__ krec = ket_p + j * ket_st;
+        const T kPx = __ldg(krec + 0);
+        const T kPy = __ldg(krec + ket_fs);
+        const T kPz = __ldg(krec + 2 * ket_fs);
+        const T kp = __ldg(krec + 3 * ket_fs);
+        const T kK = __ldg(krec + 4 * ket_fs);
+        const T kh = __ldg(krec + 5 * ket_fs);
+        const T kAx = __ldg(krec + 6 * ket_fs);
+        const T kAy = __ldg(krec + 7 * ket_fs);
+        const T kAz = __ldg(krec + 8 * ket_fs);
+        const T kBx = __ldg(krec + 9 * ket_fs);
+        const T kBy = __ldg(krec + 10 * ket_fs);
+        const T kBz = __ldg(krec + 11 * ket_fs);
         const T kEx0 = kAx * kBx + kh;
         const T kEx1 = kh * (kAx + kBx);
         const T kEy0 = kAy * kBy + kh;
@@ -1344,6 +1476,7 @@ struct EriClass<T, 5, 1> {
       I[26] = fma(bEz1, W2_001, I[26]);
       I[26] = fma(bh2, W2_002, I[26]);
     }
+    return evaluated;
   }
 };
 
@@ -1356,26 +1489,42 @@ struct EriClass<T, 5, 2> {
   static constexpr int BRA_CLASS = 2, KET_CLASS = 2;
   __device__ static constexpr int cd_c(int m) { constexpr int v[] = {2, 2, 2}; return v[m]; }
   __device__ static constexpr int cd_d(int m) { constexpr int v[] = {0, 1, 2}; return v[m]; }
-  __device__ __forceinline__ static void run(
-      const T* __restrict__ bra, long long bra_stride, int bra_kmax, int bra_row, int bra_n,
-      const T* __restrict__ ket, long long ket_stride, int ket_kmax, int ket_row, int ket_n,
-      T (&I)[NI]) {
+  // Returns the number of primitive quartets evaluated: both sides'
+  // primitive pairs come sorted by descending primitive Schwarz factor q,
+  // and the loops stop once q_bra * q_ket < eps (each skipped primitive
+  // quartet is bounded by that product, Cauchy-Schwarz per primitive pair).
+  __device__ __forceinline__ static int run(
+      const T* __restrict__ bra, const float* __restrict__ bra_q, long long bra_stride, int bra_kmax,
+      int bra_row, int bra_n,
+      const T* __restrict__ ket, const float* __restrict__ ket_q, long long ket_stride, int ket_kmax,
+      int ket_row, int ket_n, float eps, T (&I)[NI]) {
     #pragma unroll
     for (int q = 0; q < NI; ++q) I[q] = T(0);
+    int evaluated = 0;
+    const int bra_st = (int)bra_stride, ket_st = (int)ket_stride;
+    const int bra_fs = bra_kmax * bra_st, ket_fs = ket_kmax * ket_st;
+    const T* __restrict__ bra_p = bra + bra_row;
+    const T* __restrict__ ket_p = ket + ket_row;
+    const float* __restrict__ bra_qp = bra_q + bra_row;
+    const float* __restrict__ ket_qp = ket_q + ket_row;
+    const float kq0 = ket_qp[0];
     #pragma unroll 1
     for (int i = 0; i < bra_n; ++i) {
-      const T bPx = bra[(0 * bra_kmax + i) * bra_stride + bra_row];
-      const T bPy = bra[(1 * bra_kmax + i) * bra_stride + bra_row];
-      const T bPz = bra[(2 * bra_kmax + i) * bra_stride + bra_row];
-      const T bp = bra[(3 * bra_kmax + i) * bra_stride + bra_row];
-      const T bK = bra[(4 * bra_kmax + i) * bra_stride + bra_row];
-      const T bh = bra[(5 * bra_kmax + i) * bra_stride + bra_row];
-      const T bAx = bra[(6 * bra_kmax + i) * bra_stride + bra_row];
-      const T bAy = bra[(7 * bra_kmax + i) * bra_stride + bra_row];
-      const T bAz = bra[(8 * bra_kmax + i) * bra_stride + bra_row];
-      const T bBx = bra[(9 * bra_kmax + i) * bra_stride + bra_row];
-      const T bBy = bra[(10 * bra_kmax + i) * bra_stride + bra_row];
-      const T bBz = bra[(11 * bra_kmax + i) * bra_stride + bra_row];
+      const float qo = __ldg(bra_qp + i * bra_st);
+      if (qo * kq0 < eps) break;
+      const T* __restrict__ brec = bra_p + i * bra_st;
+      const T bPx = __ldg(brec + 0);
+      const T bPy = __ldg(brec + bra_fs);
+      const T bPz = __ldg(brec + 2 * bra_fs);
+      const T bp = __ldg(brec + 3 * bra_fs);
+      const T bK = __ldg(brec + 4 * bra_fs);
+      const T bh = __ldg(brec + 5 * bra_fs);
+      const T bAx = __ldg(brec + 6 * bra_fs);
+      const T bAy = __ldg(brec + 7 * bra_fs);
+      const T bAz = __ldg(brec + 8 * bra_fs);
+      const T bBx = __ldg(brec + 9 * bra_fs);
+      const T bBy = __ldg(brec + 10 * bra_fs);
+      const T bBz = __ldg(brec + 11 * bra_fs);
       const T bEx0 = bAx * bBx + bh;
       const T bEx1 = bh * (bAx + bBx);
       const T bEy0 = bAy * bBy + bh;
@@ -1388,18 +1537,21 @@ struct EriClass<T, 5, 2> {
       T W2_000 = T(0), W2_001 = T(0), W2_002 = T(0), W2_010 = T(0), W2_011 = T(0), W2_020 = T(0), W2_100 = T(0), W2_101 = T(0), W2_110 = T(0), W2_200 = T(0);
       #pragma unroll 1
       for (int j = 0; j < ket_n; ++j) {
-        const T kPx = ket[(0 * ket_kmax + j) * ket_stride + ket_row];
-        const T kPy = ket[(1 * ket_kmax + j) * ket_stride + ket_row];
-        const T kPz = ket[(2 * ket_kmax + j) * ket_stride + ket_row];
-        const T kp = ket[(3 * ket_kmax + j) * ket_stride + ket_row];
-        const T kK = ket[(4 * ket_kmax + j) * ket_stride + ket_row];
-        const T kh = ket[(5 * ket_kmax + j) * ket_stride + ket_row];
-        const T kAx = ket[(6 * ket_kmax + j) * ket_stride + ket_row];
-        const T kAy = ket[(7 * ket_kmax + j) * ket_stride + ket_row];
-        const T kAz = ket[(8 * ket_kmax + j) * ket_stride + ket_row];
-        const T kBx = ket[(9 * ket_kmax + j) * ket_stride + ket_row];
-        const T kBy = ket[(10 * ket_kmax + j) * ket_stride + ket_row];
-        const T kBz = ket[(11 * ket_kmax + j) * ket_stride + ket_row];
+        if (qo * __ldg(ket_qp + j * ket_st) < eps) break;
+        ++evaluated;
+        const T* __restrict__ krec = ket_p + j * ket_st;
+        const T kPx = __ldg(krec + 0);
+        const T kPy = __ldg(krec + ket_fs);
+        const T kPz = __ldg(krec + 2 * ket_fs);
+        const T kp = __ldg(krec + 3 * ket_fs);
+        const T kK = __ldg(krec + 4 * ket_fs);
+        const T kh = __ldg(krec + 5 * ket_fs);
+        const T kAx = __ldg(krec + 6 * ket_fs);
+        const T kAy = __ldg(krec + 7 * ket_fs);
+        const T kAz = __ldg(krec + 8 * ket_fs);
+        const T kBx = __ldg(krec + 9 * ket_fs);
+        const T kBy = __ldg(krec + 10 * ket_fs);
+        const T kBz = __ldg(krec + 11 * ket_fs);
         const T kEx0 = kAx * kBx + kh;
         const T kEx1 = kh * (kAx + kBx);
         const T kEy0 = kAy * kBy + kh;
@@ -1698,6 +1850,7 @@ struct EriClass<T, 5, 2> {
       I[26] = fma(bEz1, W2_001, I[26]);
       I[26] = fma(bh2, W2_002, I[26]);
     }
+    return evaluated;
   }
 };
 

@@ -16,7 +16,8 @@ of the inner primitive loop (W/V hold the inner-side-transformed,
 inner-primitive-summed Hermite integrals of one outer primitive).  Only
 non-zero Hermite coefficients are emitted.
 
-Primitive-pair record fields (SoA, ``base[(f * kmax + k) * stride + pair]``):
+Primitive-pair record fields (SoA, ``base[(f * kmax + k) * stride + pair]``;
+the primitive Schwarz factors sit beside them in ``q[k * stride + pair]``):
     0 Px, 1 Py, 2 Pz, 3 p, 4 K (sqrt(2 pi^{5/2}) c_a c_b N_a N_b exp(-mu AB^2) / p),
     5 h = 1/(2p), 6-8 PA = P - A, 9-11 PB = P - B.
 ss pairs use fields 0-4, ps pairs 0-8, pp pairs 0-11.
@@ -34,7 +35,7 @@ COMPS = {0: [(0, 0, 0)], 1: [(1, 0, 0), (0, 1, 0), (0, 0, 1)]}
 # it costs no extra FMAs where the bra and ket transforms are equally cheap.
 CLASSES = [
     (0, 0, 0, 0, 1, "ket"),
-    (1, 0, 0, 0, 1, "ket"),
+    (1, 0, 0, 0, 1, "bra"),
     (1, 0, 1, 0, 1, "ket"),
     (1, 1, 0, 0, 1, "bra"),
     (1, 1, 1, 0, 1, "bra"),
@@ -130,12 +131,14 @@ def prod(facs):
 
 
 def side_loads(side, pc, var, idx):
-    """Load the fields of one primitive pair record."""
+    """Load the fields of one primitive pair record through the per-thread
+    base pointer {var}_p (32-bit offsets: field f at f * {var}_fs)."""
     names = ["Px", "Py", "Pz", "p", "K", "h", "Ax", "Ay", "Az", "Bx", "By", "Bz"]
     n = PAIR_FIELDS[pc]
-    out = []
+    out = [f"const T* __restrict__ {side}rec = {var}_p + {idx} * {var}_st;"]
     for f in range(n):
-        out.append(f"const T {side}{names[f]} = {var}[({f} * {var}_kmax + {idx}) * {var}_stride + {var}_row];")
+        off = "0" if f == 0 else (f"{var}_fs" if f == 1 else f"{f} * {var}_fs")
+        out.append(f"const T {side}{names[f]} = __ldg({side}rec + {off});")
     return out
 
 
@@ -184,13 +187,18 @@ def gen_class(cid, la, lb, lc, ld, nsplit, split, order):
     body = []
     if order == "bra":
         w = lambda m, h: f"W{m}_{h[0]}{h[1]}{h[2]}"
+        body.append("const float kq0 = ket_qp[0];")
         body.append("#pragma unroll 1")
         body.append("for (int i = 0; i < bra_n; ++i) {")
+        body.append("  const float qo = __ldg(bra_qp + i * bra_st);")
+        body.append("  if (qo * kq0 < eps) break;")
         body += ["  " + x for x in side_loads("b", pa, "bra", "i") + side_pre("b", pa)]
         for m in range(len(cds)):
             body.append("  T " + ", ".join(f"{w(m, h)} = T(0)" for h in hb) + ";")
         body.append("  #pragma unroll 1")
         body.append("  for (int j = 0; j < ket_n; ++j) {")
+        body.append("    if (qo * __ldg(ket_qp + j * ket_st) < eps) break;")
+        body.append("    ++evaluated;")
         inner = side_loads("k", pk, "ket", "j") + side_pre("k", pk) + list(core)
         for m, terms in ket_terms.items():
             for (tk, uk, vk), sg, facs in terms:
@@ -215,13 +223,18 @@ def gen_class(cid, la, lb, lc, ld, nsplit, split, order):
         body.append("}")
     else:
         w = lambda n, h: f"V{n}_{h[0]}{h[1]}{h[2]}"
+        body.append("const float bq0 = bra_qp[0];")
         body.append("#pragma unroll 1")
         body.append("for (int j = 0; j < ket_n; ++j) {")
+        body.append("  const float qo = __ldg(ket_qp + j * ket_st);")
+        body.append("  if (qo * bq0 < eps) break;")
         body += ["  " + x for x in side_loads("k", pk, "ket", "j") + side_pre("k", pk)]
         for n in range(len(abs_)):
             body.append("  T " + ", ".join(f"{w(n, h)} = T(0)" for h in hk) + ";")
         body.append("  #pragma unroll 1")
         body.append("  for (int i = 0; i < bra_n; ++i) {")
+        body.append("    if (qo * __ldg(bra_qp + i * bra_st) < eps) break;")
+        body.append("    ++evaluated;")
         inner = side_loads("b", pa, "bra", "i") + side_pre("b", pa) + list(core)
         for n, terms in bra_terms.items():
             for (tb, ub, vb), _, facs in terms:
@@ -257,14 +270,26 @@ def gen_class(cid, la, lb, lc, ld, nsplit, split, order):
         f"  static constexpr int BRA_CLASS = {pa}, KET_CLASS = {pk};",
         f"  __device__ static constexpr int cd_c(int m) {{ constexpr int v[] = {{{cd_c}}}; return v[m]; }}",
         f"  __device__ static constexpr int cd_d(int m) {{ constexpr int v[] = {{{cd_d}}}; return v[m]; }}",
-        "  __device__ __forceinline__ static void run(",
-        "      const T* __restrict__ bra, long long bra_stride, int bra_kmax, int bra_row, int bra_n,",
-        "      const T* __restrict__ ket, long long ket_stride, int ket_kmax, int ket_row, int ket_n,",
-        "      T (&I)[NI]) {",
+        "  // Returns the number of primitive quartets evaluated: both sides'",
+        "  // primitive pairs come sorted by descending primitive Schwarz factor q,",
+        "  // and the loops stop once q_bra * q_ket < eps (each skipped primitive",
+        "  // quartet is bounded by that product, Cauchy-Schwarz per primitive pair).",
+        "  __device__ __forceinline__ static int run(",
+        "      const T* __restrict__ bra, const float* __restrict__ bra_q, long long bra_stride, int bra_kmax,",
+        "      int bra_row, int bra_n,",
+        "      const T* __restrict__ ket, const float* __restrict__ ket_q, long long ket_stride, int ket_kmax,",
+        "      int ket_row, int ket_n, float eps, T (&I)[NI]) {",
         "    #pragma unroll",
         "    for (int q = 0; q < NI; ++q) I[q] = T(0);",
+        "    int evaluated = 0;",
+        "    const int bra_st = (int)bra_stride, ket_st = (int)ket_stride;",
+        "    const int bra_fs = bra_kmax * bra_st, ket_fs = ket_kmax * ket_st;",
+        "    const T* __restrict__ bra_p = bra + bra_row;",
+        "    const T* __restrict__ ket_p = ket + ket_row;",
+        "    const float* __restrict__ bra_qp = bra_q + bra_row;",
+        "    const float* __restrict__ ket_qp = ket_q + ket_row;",
     ]
-    tail = ["  }", "};", ""]
+    tail = ["    return evaluated;", "  }", "};", ""]
     return head + ["    " + x for x in body] + tail
 
 

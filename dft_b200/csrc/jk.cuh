@@ -51,43 +51,86 @@ __global__ void k_pair_data(const dftk_shells_t sh, const dftk_pairs_t pr, int n
 
 // ------------------------------------------------------------------ helpers
 template <int C, typename T, int S>
-__device__ __forceinline__ void eri_run(const T *bra, int bra_n_pairs, int bra_kmax, int bra_row,
-                                        int bra_np, const T *ket, int ket_n_pairs, int ket_kmax,
-                                        int ket_row, int ket_np, T (&I)[EriClass<T, C, S>::NI])
+__device__ __forceinline__ int eri_run(const T *bra, const float *bra_q, int bra_n_pairs, int bra_kmax,
+                                       int bra_row, int bra_np, const T *ket, const float *ket_q,
+                                       int ket_n_pairs, int ket_kmax, int ket_row, int ket_np, float eps,
+                                       T (&I)[EriClass<T, C, S>::NI])
 {
-    EriClass<T, C, S>::run(bra, bra_n_pairs, bra_kmax, bra_row, bra_np, ket, ket_n_pairs, ket_kmax,
-                           ket_row, ket_np, I);
+    return EriClass<T, C, S>::run(bra, bra_q, bra_n_pairs, bra_kmax, bra_row, bra_np, ket, ket_q, ket_n_pairs,
+                                  ket_kmax, ket_row, ket_np, eps, I);
 }
 
 // Diagonal class of a pair class: ss -> (ss|ss), ps -> (ps|ps), pp -> (pp|pp).
 template <int PC> struct DiagClass { static constexpr int C = PC == 0 ? 0 : (PC == 1 ? 2 : 5); };
 
+// max |(ab|ab)| over components, primitives k0 .. k0 + np - 1 of the pair
 template <int C, int S>
-__device__ __forceinline__ double diag_max(const dftk_pairs_t &pr, int pair)
+__device__ __forceinline__ double diag_max(const dftk_pairs_t &pr, int pair, int k0, int np)
 {
     double I[EriClass<double, C, S>::NI];
-    const int np = pr.nprim[pair];
-    eri_run<C, double, S>(pr.rec64, pr.n_pairs, pr.kmax, pair, np, pr.rec64, pr.n_pairs, pr.kmax,
-                          pair, np, I);
+    const double *rec = pr.rec64 + (long long)k0 * pr.n_pairs;
+    const float *q = pr.qp + (long long)k0 * pr.n_pairs;
+    eri_run<C, double, S>(rec, q, pr.n_pairs, pr.kmax, pair, np, rec, q, pr.n_pairs, pr.kmax, pair, np, 0.0f, I);
     double m = 0.0;
 #pragma unroll
-    for (int q = 0; q < EriClass<double, C, S>::NI; ++q) m = fmax(m, fabs(I[q]));
+    for (int q2 = 0; q2 < EriClass<double, C, S>::NI; ++q2) m = fmax(m, fabs(I[q2]));
     return m;
 }
 
-// Schwarz factor Q_ab = sqrt(max |(ab|ab)|), one thread per pair.
+template <int C>
+__device__ __forceinline__ double diag_max_all(const dftk_pairs_t &pr, int pair, int k0, int np)
+{
+    double m = diag_max<C, 0>(pr, pair, k0, np);
+    if constexpr (EriClass<double, C, 0>::NSPLIT > 1) {
+        m = fmax(m, diag_max<C, 1>(pr, pair, k0, np));
+        m = fmax(m, diag_max<C, 2>(pr, pair, k0, np));
+    }
+    return m;
+}
+
+#define DFTK_MAX_KPAIR 64
+
+// Schwarz factors, one thread per pair: Q_ab = sqrt(max |(ab|ab)|) of the
+// contracted pair, and per primitive pair q_k = sqrt(max |(ab_k|ab_k)|); the
+// primitive records of the pair are then reordered by descending q_k (both
+// copies) so the ERI loops can stop at the first negligible primitive.
 template <int PC>
-__global__ void k_schwarz(const dftk_pairs_t pr)
+__global__ void k_schwarz(const dftk_pairs_t pr, int nfields)
 {
     const int pair = blockIdx.x * blockDim.x + threadIdx.x;
     if (pair >= pr.n_pairs) return;
     constexpr int C = DiagClass<PC>::C;
-    double m = diag_max<C, 0>(pr, pair);
-    if constexpr (EriClass<double, C, 0>::NSPLIT > 1) {
-        m = fmax(m, diag_max<C, 1>(pr, pair));
-        m = fmax(m, diag_max<C, 2>(pr, pair));
+    const int np = pr.nprim[pair];
+    const long long n = pr.n_pairs;
+    for (int k = 0; k < pr.kmax; ++k) pr.qp[k * n + pair] = 0.0f;  // no screening while measuring
+    pr.q[pair] = sqrt(diag_max_all<C>(pr, pair, 0, np));
+    float qk[DFTK_MAX_KPAIR];
+    int order[DFTK_MAX_KPAIR];
+    const int kk = min(pr.kmax, DFTK_MAX_KPAIR);
+    for (int k = 0; k < kk; ++k) {
+        qk[k] = k < np ? (float)sqrt(diag_max_all<C>(pr, pair, k, 1)) : 0.0f;
+        order[k] = k;
     }
-    pr.q[pair] = sqrt(m);
+    // insertion sort, descending q (kmax <= 64)
+    for (int a = 1; a < kk; ++a) {
+        const int o = order[a];
+        int b = a - 1;
+        while (b >= 0 && qk[order[b]] < qk[o]) { order[b + 1] = order[b]; --b; }
+        order[b + 1] = o;
+    }
+    for (int f = 0; f < nfields; ++f) {
+        double v64[DFTK_MAX_KPAIR];
+        float v32[DFTK_MAX_KPAIR];
+        for (int k = 0; k < kk; ++k) {
+            v64[k] = pr.rec64[((long long)f * pr.kmax + k) * n + pair];
+            v32[k] = pr.rec32[((long long)f * pr.kmax + k) * n + pair];
+        }
+        for (int k = 0; k < kk; ++k) {
+            pr.rec64[((long long)f * pr.kmax + k) * n + pair] = v64[order[k]];
+            pr.rec32[((long long)f * pr.kmax + k) * n + pair] = v32[order[k]];
+        }
+    }
+    for (int k = 0; k < kk; ++k) pr.qp[k * n + pair] = qk[order[k]];
 }
 
 // ------------------------------------------------------------------- J / K
@@ -99,8 +142,10 @@ struct JkParams {
     const double *rec64[3];
     const float *rec32[3];
     const double *q[3];
+    const float *qp[3];
     int n_pairs[3];
     int kmax[3];
+    float tau_prim;
     long long n_rows[DFTK_N_QCLASS];
     long long total[DFTK_N_QCLASS];
     const long long *row_off[DFTK_N_QCLASS];
@@ -108,8 +153,13 @@ struct JkParams {
     double *Y, *Za, *Zb;
     const float *Dsh;
     int uhf;
-    double tau_lo, tau_hi;  // quartet processed if tau_lo <= bound < tau_hi
+    double tau_lo, tau_hi;  // scan path: quartet processed if tau_lo <= bound < tau_hi
+    double tau, tau32;      // select path: FP64 if bound >= tau32, FP32 if tau <= bound < tau32
     long long *counts;
+    // select path: per class one list of (bra row, ket) with capacity total[C];
+    // FP64 entries fill it from the front, FP32 entries from the back
+    int2 *list[DFTK_N_QCLASS];
+    unsigned long long *heads;  // [2 * DFTK_N_QCLASS]: FP64 then FP32 entry counts
 };
 
 // largest r in [0, n_rows) with off[r] <= cand
@@ -273,15 +323,26 @@ __device__ __forceinline__ void jk_one(const JkParams &P, bool valid, int row, i
     const int a = abX[2 * brow], b = abX[2 * brow + 1];
     const int c = valid ? abY[2 * ket] : 0, d = valid ? abY[2 * ket + 1] : 0;
     T I[E::NI];
+    int evaluated = 0;
     if (valid) {
-        eri_run<C, T, S>(RecOf<C, T>::get(P, X), P.n_pairs[X], P.kmax[X], row, P.np[X][row],
-                         RecOf<C, T>::get(P, Yc), P.n_pairs[Yc], P.kmax[Yc], ket, P.np[Yc][ket], I);
+        evaluated = eri_run<C, T, S>(RecOf<C, T>::get(P, X), P.qp[X], P.n_pairs[X], P.kmax[X], row, P.np[X][row],
+                                     RecOf<C, T>::get(P, Yc), P.qp[Yc], P.n_pairs[Yc], P.kmax[Yc], ket,
+                                     P.np[Yc][ket], P.tau_prim, I);
     } else {
 #pragma unroll
         for (int q = 0; q < E::NI; ++q) I[q] = T(0);
     }
     const int ew = (a == b) + (c == d) + ((X == Yc) && (row == ket));
     digest<C, T, S>(P, valid, uniform, a, b, c, d, (double)(1 << ew), I);
+    if (P.counts) {
+        // evaluated primitive quartets: slot 12 + class (the FP32 launch's
+        // counts pointer is offset by 6)
+        int tot = evaluated;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(DFTK_FULL_MASK, tot, o);
+        if ((threadIdx.x & 31) == 0 && tot)
+            atomicAdd((unsigned long long *)(P.counts + 2 * DFTK_N_QCLASS + C), (unsigned long long)tot);
+    }
 }
 
 // One warp per 32 consecutive candidates of class C (and one split of the
@@ -329,6 +390,142 @@ __global__ void __launch_bounds__(128) k_jk(const JkParams P)
     }
 }
 
+// Selection pass: one scan of class C's candidate space computes each
+// quartet's density-weighted Schwarz bound and appends the survivors to the
+// FP64 or FP32 end of the class list.  A block compacts a tile of
+// SELECT_TILE consecutive candidates with a block-wide prefix sum and
+// reserves its output range with one atomic, so the lists keep the candidate
+// order within every tile: the class kernels then see long runs of one bra
+// row with neighbouring kets (shared bra data, warp-uniform J reduction).
+#define SELECT_THREADS 256
+#define SELECT_PER_WARP 8
+#define SELECT_TILE (SELECT_THREADS * SELECT_PER_WARP)
+
+template <int C>
+__device__ __forceinline__ void select_classify(const JkParams &P, long long cand, int &row, int &ket, bool &is64,
+                                                bool &is32, int r0)
+{
+    using E0 = EriClass<double, C, 0>;
+    constexpr int X = E0::BRA_CLASS, Yc = E0::KET_CLASS;
+    const long long *off = P.row_off[C];
+    row = r0;
+    if (cand >= __ldg(off + r0 + 1)) row = find_row(off, P.n_rows[C], cand);
+    ket = (int)(cand - __ldg(off + row));
+    const int a = P.ab[X][2 * row], b = P.ab[X][2 * row + 1];
+    const int c = P.ab[Yc][2 * ket], d = P.ab[Yc][2 * ket + 1];
+    const int ns = P.ns;
+    const float dm = fmaxf(fmaxf(__ldg(P.Dsh + a * ns + b), __ldg(P.Dsh + c * ns + d)),
+                           fmaxf(fmaxf(__ldg(P.Dsh + a * ns + c), __ldg(P.Dsh + a * ns + d)),
+                                 fmaxf(__ldg(P.Dsh + b * ns + c), __ldg(P.Dsh + b * ns + d))));
+    const double bound = __ldg(P.q[X] + row) * __ldg(P.q[Yc] + ket) * (double)dm;
+    is64 = bound >= P.tau32;
+    is32 = !is64 && bound >= P.tau;
+}
+
+template <int C>
+__global__ void __launch_bounds__(SELECT_THREADS) k_select(const JkParams P)
+{
+    __shared__ unsigned s_cnt64[SELECT_THREADS / 32], s_cnt32[SELECT_THREADS / 32];
+    __shared__ unsigned long long s_base64, s_base32;
+    const long long ncand = P.total[C];
+    const long long cap = ncand;
+    const long long ntiles = (ncand + SELECT_TILE - 1) / SELECT_TILE;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned below = (1u << lane) - 1u;
+    const long long *off = P.row_off[C];
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const long long wfirst = tile * SELECT_TILE + (long long)warp * 32 * SELECT_PER_WARP;
+        int r0 = 0;
+        if (lane == 0 && wfirst < ncand) r0 = find_row(off, P.n_rows[C], wfirst);
+        r0 = __shfl_sync(DFTK_FULL_MASK, r0, 0);
+        unsigned m64[SELECT_PER_WARP], m32[SELECT_PER_WARP];
+        int rows[SELECT_PER_WARP], kets[SELECT_PER_WARP];
+        unsigned n64 = 0, n32 = 0;
+#pragma unroll
+        for (int it = 0; it < SELECT_PER_WARP; ++it) {
+            const long long cand = wfirst + it * 32 + lane;
+            bool is64 = false, is32 = false;
+            rows[it] = 0;
+            kets[it] = 0;
+            if (cand < ncand) {
+                select_classify<C>(P, cand, rows[it], kets[it], is64, is32, r0);
+                r0 = rows[it];  // later candidates of this lane lie at or beyond this row
+            }
+            m64[it] = __ballot_sync(DFTK_FULL_MASK, is64);
+            m32[it] = __ballot_sync(DFTK_FULL_MASK, is32);
+            n64 += __popc(m64[it]);
+            n32 += __popc(m32[it]);
+            r0 = __shfl_sync(DFTK_FULL_MASK, r0, 0);
+        }
+        if (lane == 0) {
+            s_cnt64[warp] = n64;
+            s_cnt32[warp] = n32;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned t64 = 0, t32 = 0;
+            for (int w = 0; w < SELECT_THREADS / 32; ++w) {
+                const unsigned a = s_cnt64[w], b = s_cnt32[w];
+                s_cnt64[w] = t64;
+                s_cnt32[w] = t32;
+                t64 += a;
+                t32 += b;
+            }
+            s_base64 = t64 ? atomicAdd(P.heads + C, (unsigned long long)t64) : 0ull;
+            s_base32 = t32 ? atomicAdd(P.heads + DFTK_N_QCLASS + C, (unsigned long long)t32) : 0ull;
+            if (P.counts) {
+                if (t64) atomicAdd((unsigned long long *)(P.counts + C), (unsigned long long)t64);
+                if (t32) atomicAdd((unsigned long long *)(P.counts + DFTK_N_QCLASS + C), (unsigned long long)t32);
+            }
+        }
+        __syncthreads();
+        unsigned long long p64 = s_base64 + s_cnt64[warp];
+        unsigned long long p32 = s_base32 + s_cnt32[warp];
+#pragma unroll
+        for (int it = 0; it < SELECT_PER_WARP; ++it) {
+            if (m64[it] & (1u << lane)) P.list[C][p64 + __popc(m64[it] & below)] = make_int2(rows[it], kets[it]);
+            if (m32[it] & (1u << lane))
+                P.list[C][cap - 1 - (long long)(p32 + __popc(m32[it] & below))] = make_int2(rows[it], kets[it]);
+            p64 += __popc(m64[it]);
+            p32 += __popc(m32[it]);
+        }
+        __syncthreads();  // s_base/s_cnt are rewritten by the next tile
+    }
+}
+
+// J/K over the selected quartets of class C in precision T: warp w takes
+// list entries 32w .. 32w + 31 (one split of the c components at a time).
+template <int C, typename T>
+__global__ void __launch_bounds__(128) k_jk_list(const JkParams P)
+{
+    constexpr int NS = EriClass<T, C, 0>::NSPLIT;
+    constexpr bool fp32 = sizeof(T) == 4;
+    const long long n = (long long)P.heads[(fp32 ? DFTK_N_QCLASS : 0) + C];
+    const long long cap = P.total[C];
+    const int2 *list = P.list[C];
+    const long long nwork = ((n + 31) >> 5) * NS;
+    const int lane = threadIdx.x & 31;
+    const long long wstride = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; gw < nwork; gw += wstride) {
+        const int split = (int)(gw % NS);
+        const long long idx = (gw / NS) * 32 + lane;
+        const bool valid = idx < n;
+        int row = 0, ket = 0;
+        if (valid) {
+            const int2 e = __ldg(list + (fp32 ? cap - 1 - idx : idx));
+            row = e.x;
+            ket = e.y;
+        }
+        if constexpr (NS == 1) {
+            jk_one<C, T, 0>(P, valid, row, ket);
+        } else {
+            if (split == 0) jk_one<C, T, 0>(P, valid, row, ket);
+            else if (split == 1) jk_one<C, T, 1>(P, valid, row, ket);
+            else jk_one<C, T, 2>(P, valid, row, ket);
+        }
+    }
+}
+
 // J = Y + Y^T, K = Z + Z^T
 __global__ void k_symmetrize(int N, const double *Y, const double *Za, const double *Zb, double *J,
                              double *Ka, double *Kb, int uhf)
@@ -350,6 +547,7 @@ struct EmitParams {
     const int *np[3];
     const double *rec64[3];
     const float *rec32[3];
+    const float *qp[3];
     int n_pairs[3];
     int kmax[3];
     long long nq;
@@ -375,8 +573,8 @@ __device__ __forceinline__ void emit_split(const EmitParams &P, int row, int ket
     using E = EriClass<T, C, S>;
     constexpr int X = E::BRA_CLASS, Yc = E::KET_CLASS;
     T I[E::NI];
-    eri_run<C, T, S>(EmitRec<T>::get(P, X), P.n_pairs[X], P.kmax[X], row, P.np[X][row], EmitRec<T>::get(P, Yc),
-                     P.n_pairs[Yc], P.kmax[Yc], ket, P.np[Yc][ket], I);
+    eri_run<C, T, S>(EmitRec<T>::get(P, X), P.qp[X], P.n_pairs[X], P.kmax[X], row, P.np[X][row],
+                     EmitRec<T>::get(P, Yc), P.qp[Yc], P.n_pairs[Yc], P.kmax[Yc], ket, P.np[Yc][ket], 0.0f, I);
 #pragma unroll
     for (int ia = 0; ia < E::NA; ++ia)
 #pragma unroll

@@ -61,7 +61,7 @@ def _dev(device) -> torch.device:
 
 
 class IntegralEngine:
-    def __init__(self, shells: List[Dict], tau_schwarz: float = 1e-12, device=None):
+    def __init__(self, shells: List[Dict], tau_schwarz: float = 1e-12, tau_prim: float = 1e-15, device=None):
         _basis.check_supported(shells)
         _lib.load()
         self.device = _dev(device)
@@ -69,6 +69,7 @@ class IntegralEngine:
         self.ns = len(shells)
         self.n_ao = int(shells[-1]["ao_stop"]) if shells else 0
         self.tau_schwarz = float(tau_schwarz)
+        self.tau_prim = float(tau_prim)
         self.l = np.array([s["angular_momentum"] for s in shells], dtype=np.int32)
         self.nao_sh = np.array([s["n_ao"] for s in shells], dtype=np.int64)
         with torch.cuda.device(self.device):
@@ -76,9 +77,10 @@ class IntegralEngine:
             self._upload_shells()
             self._build_pairs()
             self._build_queue()
-            nbytes = _lib.load().dftk_jk_workspace_bytes(self.ns, self.n_ao)
+            nbytes = _lib.load().dftk_jk_workspace_bytes_queue(self.ns, self.n_ao, ctypes.byref(self.c_queue))
             self.workspace = torch.empty(int(nbytes), dtype=torch.uint8, device=self.device)
             self.workspace_bytes = int(nbytes)
+            self.base_workspace_bytes = int(_lib.load().dftk_jk_workspace_bytes(self.ns, self.n_ao))
 
     # ------------------------------------------------------------------ setup
     def _t(self, arr, dtype):
@@ -115,9 +117,11 @@ class IntegralEngine:
             "rec64": torch.zeros(max(nf * self.kmax * n, 1), dtype=torch.float64, device=self.device),
             "rec32": torch.zeros(max(nf * self.kmax * n, 1), dtype=torch.float32, device=self.device),
             "q": torch.zeros(max(n, 1), dtype=torch.float64, device=self.device),
+            "qp": torch.zeros(max(self.kmax * n, 1), dtype=torch.float32, device=self.device),
         }
         st = _lib.Pairs(n, self.kmax, _lib.ptr(bufs["ab"]).value, _lib.ptr(bufs["nprim"]).value,
-                        _lib.ptr(bufs["rec64"]).value, _lib.ptr(bufs["rec32"]).value, _lib.ptr(bufs["q"]).value)
+                        _lib.ptr(bufs["rec64"]).value, _lib.ptr(bufs["rec32"]).value, _lib.ptr(bufs["q"]).value,
+                        _lib.ptr(bufs["qp"]).value)
         return bufs, st
 
     def _build_pairs(self):
@@ -147,8 +151,8 @@ class IntegralEngine:
                 sel = sel[order]
                 bufs, st = self._alloc_class(pc, ab)
                 _lib.call("dftk_pair_data", ctypes.byref(self.c_shells), pc, ctypes.byref(st), stream)
-                bufs["q"][: ab.shape[0]] = torch.as_tensor(q[order], dtype=torch.float64, device=self.device)
-                self.q_sorted.append(q[order])
+                _lib.call("dftk_schwarz", ctypes.byref(self.c_shells), pc, ctypes.byref(st), stream)
+                self.q_sorted.append(bufs["q"][: ab.shape[0]].cpu().numpy())
             else:
                 self.q_sorted.append(np.zeros(0))
             ref_class[sel] = pc
@@ -176,6 +180,7 @@ class IntegralEngine:
             q.n_rows[c] = nrows if off[-1] > 0 else 0
             q.total[c] = int(off[-1])
             q.row_off[c] = _lib.ptr(d_off).value
+        q.tau_prim = self.tau_prim
         self.c_queue = q
 
     # ---------------------------------------------------------------- queries
@@ -183,10 +188,10 @@ class IntegralEngine:
         """Schwarz-surviving unique quartets per class (ss|ss)..(pp|pp)."""
         return list(self.totals)
 
-    def schwarz_flops(self, counts: Sequence[int]) -> float:
-        """Fixed-accounting flops of evaluating `counts` contracted quartets per class."""
-        nprim_q = self.kmax * self.kmax
-        return float(sum(FLOPS_PER_PRIM_QUARTET[c] * nprim_q * counts[c] for c in range(6)))
+    @staticmethod
+    def fixed_flops(prim_counts: Sequence[int]) -> float:
+        """Fixed-accounting flops of `prim_counts` evaluated primitive quartets per class."""
+        return float(sum(FLOPS_PER_PRIM_QUARTET[c] * prim_counts[c] for c in range(6)))
 
     # ---------------------------------------------------------------- compute
     def one_electron(self, atoms: Sequence[str], centers) -> Tuple[torch.Tensor, torch.Tensor, torch.Tensor]:
@@ -201,12 +206,15 @@ class IntegralEngine:
 
     def jk(self, D: torch.Tensor, D_a: Optional[torch.Tensor] = None, D_b: Optional[torch.Tensor] = None,
            uhf: bool = False, mixed: bool = False, tau: float = 1e-14, tau_fp32: float = 1e-6,
-           out=None, counts: Optional[torch.Tensor] = None):
+           out=None, counts: Optional[torch.Tensor] = None, scan: bool = False):
         """Direct J, K_a (, K_b) for densities on the device.
 
         D is the density J is built from (the reference's P = P_a + P_b);
         K_a uses D_a (defaults to D / 2, the RHF alpha density) and, with
         ``uhf``, K_b uses D_b.  Returns (J, K_a, K_b) with K_b = K_a unless uhf.
+        ``scan`` hands dftk_jk only the base workspace, which selects its
+        direct path (class kernels scan the candidates themselves) instead of
+        the selection pass + quartet lists.
         """
         N = self.n_ao
         dev = self.device
@@ -226,7 +234,8 @@ class IntegralEngine:
         _lib.call("dftk_jk", ctypes.byref(self.c_shells), self.c_pairs, ctypes.byref(self.c_queue),
                   _lib.ptr(D), _lib.ptr(D_a), _lib.ptr(D_b if uhf else None), _lib.ptr(J), _lib.ptr(Ka),
                   _lib.ptr(Kb if uhf else None), flags, float(tau), float(tau_fp32 if mixed else tau),
-                  _lib.ptr(self.workspace), self.workspace_bytes, _lib.ptr(counts), _lib.stream_handle())
+                  _lib.ptr(self.workspace), self.base_workspace_bytes if scan else self.workspace_bytes,
+                  _lib.ptr(counts), _lib.stream_handle())
         return J, Ka, (Kb if uhf else Ka)
 
     def _square(self, M) -> torch.Tensor:

@@ -192,7 +192,7 @@ def scf_rhf(engine: IntegralEngine, H: torch.Tensor, S: torch.Tensor, n_occ: int
     E_prev = None
     builds, tb = 0, 0.0
     energies: List[float] = []
-    counts_t = torch.zeros(12, dtype=torch.int64, device=dev) if count_quartets else None
+    counts_t = torch.zeros(24, dtype=torch.int64, device=dev) if count_quartets else None
     since_full = 0
     E_last = None
     e_last_incremental = None

@@ -75,6 +75,8 @@ typedef struct {
     double *rec64;          /* [nfields * kmax * n_pairs] (written by dftk_pair_data) */
     float *rec32;           /* same, FP32 copy for the mixed path */
     double *q;              /* [n_pairs] Schwarz factor sqrt(max|(ab|ab)|) (written by dftk_schwarz) */
+    float *qp;              /* [kmax * n_pairs] primitive Schwarz factors sqrt(max|(ab_k|ab_k)|), each
+                               pair's primitives reordered by descending qp (written by dftk_schwarz) */
 } dftk_pairs_t;
 
 /* Candidate quartets of each class: bra pair `row` of the bra pair class pairs
@@ -86,6 +88,8 @@ typedef struct {
     long long n_rows[DFTK_N_QCLASS];
     long long total[DFTK_N_QCLASS];           /* host copy of row_off[n_rows] */
     const long long *row_off[DFTK_N_QCLASS];  /* device [n_rows + 1] */
+    double tau_prim;                          /* skip primitive quartets with qp_ab * qp_cd < tau_prim
+                                                 (0 keeps all); each skipped one is bounded by it */
 } dftk_queue_t;
 
 /* library version (integer, 100 * major + minor) */
@@ -109,7 +113,9 @@ int dftk_boys32(int mmax, long long n, const float *T, float *F, dftk_stream_t s
 int dftk_pair_data(const dftk_shells_t *shells, int pair_class, dftk_pairs_t *pairs,
                    dftk_stream_t stream);
 
-/* Schwarz factors pairs->q from the diagonal quartets (ab|ab). */
+/* Schwarz factors pairs->q from the diagonal quartets (ab|ab), primitive
+ * factors pairs->qp, and the primitive records of each pair reordered by
+ * descending qp.  At most 64 primitive pairs per pair. */
 int dftk_schwarz(const dftk_shells_t *shells, int pair_class, dftk_pairs_t *pairs,
                  dftk_stream_t stream);
 
@@ -131,8 +137,17 @@ int dftk_eri_blocks(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N
                     long long n_quartets, const int *desc, const long long *out_off,
                     double *out, dftk_stream_t stream);
 
-/* Workspace bytes dftk_jk needs for n_shells shells and n_ao AOs. */
+/* Workspace bytes dftk_jk needs for n_shells shells and n_ao AOs (direct
+ * path: each class kernel scans its candidate space and skips screened
+ * quartets itself). */
 size_t dftk_jk_workspace_bytes(int n_shells, int n_ao);
+
+/* Workspace bytes for the selection path: a workspace at least this large
+ * makes dftk_jk run one selection pass that writes the surviving quartets of
+ * every class into FP64/FP32 lists, then class kernels over the lists (no
+ * per-kernel scan; one scan for both precisions).  8 bytes per candidate
+ * quartet of the queue on top of dftk_jk_workspace_bytes. */
+size_t dftk_jk_workspace_bytes_queue(int n_shells, int n_ao, const dftk_queue_t *queue);
 
 /* Integral-direct J and K (fill_matrices, shelled.py:770-877, without stored
  * ERIs): J = (mu nu|la si) D_la,si and K_s = (mu la|nu si) Ds_la,si over the
@@ -140,8 +155,9 @@ size_t dftk_jk_workspace_bytes(int n_shells, int n_ao);
  * Q_ab Q_cd max|D block| >= tau.  J, K_a (and K_b with DFTK_JK_UHF) are
  * overwritten, N x N row-major, symmetric.  With DFTK_JK_MIXED the quartets
  * with bound < tau_fp32 run in FP32 (accumulation stays FP64).
- * counts (optional device array of 2 * DFTK_N_QCLASS long long, zeroed by
- * the caller) receives the quartets evaluated per class in FP64 then FP32. */
+ * counts (optional device array of 4 * DFTK_N_QCLASS long long, zeroed by
+ * the caller) receives per class: shell quartets evaluated in FP64, then in
+ * FP32, then primitive quartets evaluated in FP64, then in FP32. */
 int dftk_jk(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N_PCLASS],
             const dftk_queue_t *queue, const double *D, const double *D_a, const double *D_b,
             double *J, double *K_a, double *K_b, int flags, double tau, double tau_fp32,

@@ -220,9 +220,9 @@ def test_jk_screened_lanes_vs_oracle(oracle_mod):
     D = torch.as_tensor(2 * Pa).cuda()
     J, K, _ = eng.jk(D, 0.5 * D, tau=1e-9)
     assert np.abs(J.cpu().numpy() - J0).max() < 1e-6 and np.abs(K.cpu().numpy() - K0).max() < 1e-6
-    counts = torch.zeros(12, dtype=torch.int64, device="cuda")
+    counts = torch.zeros(24, dtype=torch.int64, device="cuda")
     Jm, Km, _ = eng.jk(D, 0.5 * D, mixed=True, tau=0.0, tau_fp32=1e-4, counts=counts)
-    assert counts[6:].sum().item() > 0 and counts[:6].sum().item() > 0
+    assert counts[6:12].sum().item() > 0 and counts[:6].sum().item() > 0
     assert np.abs(Jm.cpu().numpy() - J0).max() < 1e-8 and np.abs(Km.cpu().numpy() - K0).max() < 1e-8
 
 
@@ -245,11 +245,30 @@ def test_jk_properties_h2o64():
     assert (J12 - J1 - J2).abs().max() < 1e-11 and (K12 - K1 - K2).abs().max() < 1e-11
     Jr, Kr, _ = eng.jk(D1, 0.5 * D1, tau=0.0)
     assert (Jr - J1).abs().max() < 1e-12
-    counts = torch.zeros(12, dtype=torch.int64, device="cuda")
+    counts = torch.zeros(24, dtype=torch.int64, device="cuda")
     eng.jk(D1, 0.5 * D1, tau=0.0, counts=counts)
     assert counts[:6].tolist() == eng.quartet_totals()
     counts.zero_()
     Jm, Km, _ = eng.jk(D1, 0.5 * D1, mixed=True, tau=0.0, tau_fp32=1e-5, counts=counts)
     c = counts.tolist()
-    assert sum(c[:6]) + sum(c[6:]) == sum(eng.quartet_totals()) and sum(c[6:]) > 0
+    assert sum(c[:6]) + sum(c[6:12]) == sum(eng.quartet_totals()) and sum(c[6:12]) > 0
     assert (Jm - J1).abs().max() < 1e-7 and (Km - K1).abs().max() < 1e-7
+
+
+def test_select_lists_match_direct_scan():
+    """The selection pass + list kernels and the direct scan path agree, with
+    density screening and the FP32 split active, and count the same quartets."""
+    atoms, centers = geometry.water_cluster((2, 2, 2), seed=7)
+    eng = IntegralEngine(_shells(atoms, centers), tau_schwarz=1e-12)
+    N = eng.n_ao
+    rng = np.random.default_rng(21)
+    A = rng.normal(size=(N, N)) * (rng.random(size=(N, N)) < 0.2)
+    D = torch.as_tensor(0.1 * (A + A.T)).cuda()
+    for kw in (dict(tau=1e-10), dict(mixed=True, tau=1e-12, tau_fp32=1e-5)):
+        c_list = torch.zeros(24, dtype=torch.int64, device="cuda")
+        c_scan = torch.zeros(24, dtype=torch.int64, device="cuda")
+        J1, K1, _ = eng.jk(D, 0.5 * D, counts=c_list, **kw)
+        J2, K2, _ = eng.jk(D, 0.5 * D, counts=c_scan, scan=True, **kw)
+        assert (J1 - J2).abs().max().item() < 1e-12 and (K1 - K2).abs().max().item() < 1e-12
+        assert c_list.tolist() == c_scan.tolist()
+        assert c_list[:6].sum().item() > 0

@@ -52,4 +52,4 @@ def test_mixed_precision_energy_water16():
     assert abs(rmx.energy - r64.energy) < 1e-6
     # the energy of the last mixed incremental build itself, before the final FP64 rebuild
     assert abs(rmx.energy_last_build - r64.energy) < 1e-6
-    assert sum(rmx.counts[6:]) > 0
+    assert sum(rmx.counts[6:12]) > 0
