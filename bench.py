@@ -13,8 +13,10 @@ Reported besides the headline:
              shelled.fill_matrices(shells, P, P_a, P_b, J, K_a, K_b) with host
              NumPy arrays (host->device densities and device->host J/K inside
              the timed region);
-  * mixed    FP64 vs mixed FP32/FP64 incremental builds over the full SCF
-             (builds/s averaged over the build sequence) and |dE| in uEh;
+  * mixed    the incremental (D - D_prev) Fock builds of a full (H2O)_64 SCF,
+             FP64 vs mixed FP32/FP64 (FP32 where Q_ab Q_cd |dD| < 1e-6),
+             as builds/s of the incremental builds, against the plain FP64
+             build, plus whole-SCF rates and |dE| in uEh;
   * roofline the dominant class kernel's achieved FP64 rate from the fixed
              flop accounting, against an FMA-loop peak measured here;
   * cpu_baseline  the reference's integral kernel (oracle/_ref, host-compiled)
@@ -360,6 +362,8 @@ def run_dftk_arm(args, rank, world, local_rank):
         rmx = scf_rhf(eng, H, S, nocc, enn, incremental=True, mixed=True, count_quartets=True)
         b64 = r64.fock_builds / r64.fock_seconds
         bmx = rmx.fock_builds / rmx.fock_seconds
+        i64 = r64.incremental_builds / max(r64.incremental_seconds, 1e-12)
+        imx = rmx.incremental_builds / max(rmx.incremental_seconds, 1e-12)
         traffic = None
         tpath = os.path.join(REPO, "profiles", "jk_traffic.json")
         if os.path.exists(tpath):
@@ -393,8 +397,13 @@ def run_dftk_arm(args, rank, world, local_rank):
                          "whole_build_tflops": total_flops / (ms_per_step / 1e3) / 1e12,
                          "class_ms": {QCLASS_NAMES[c]: float(class_ms[c]) for c in range(6)},
                          "fp32_peak_tflops": fp32_peak, "hbm_peak_gbs": peaks.get("hbm_gbs")},
-            "mixed": {"fp64_incremental_builds_per_s": b64, "mixed_incremental_builds_per_s": bmx,
-                      "speedup": bmx / b64, "scf_iterations_fp64": r64.iterations,
+            "mixed": {"plain_fp64_builds_per_s": value / world,
+                      "fp64_incremental_builds_per_s": i64, "mixed_incremental_builds_per_s": imx,
+                      "speedup_mixed_vs_plain_fp64": imx / (value / world),
+                      "speedup_mixed_vs_fp64_incremental": imx / i64,
+                      "incremental_builds": [r64.incremental_builds, rmx.incremental_builds],
+                      "scf_builds_per_s_fp64": b64, "scf_builds_per_s_mixed": bmx,
+                      "scf_speedup": bmx / b64, "scf_iterations_fp64": r64.iterations,
                       "scf_iterations_mixed": rmx.iterations,
                       "energy_fp64": r64.energy, "energy_mixed_final": rmx.energy,
                       "delta_E_uEh_final": abs(rmx.energy - r64.energy) * 1e6,
@@ -410,6 +419,27 @@ def run_dftk_arm(args, rank, world, local_rank):
     return 0
 
 
+def run_profile(args):
+    """A few builds of the benchmark workload for ncu captures: two full FP64
+    builds, then one mixed build of a scaled-down density (kernel launch order
+    per build: k_dsh, k_select x6, k_jk_list<0..5,double>, [k_jk_list<0..5,float>],
+    k_symmetrize)."""
+    import torch
+
+    atoms, centers, shells, eng, S, H, enn, nocc = setup_workload(torch)
+    X = torch.linalg.inv(torch.linalg.cholesky(S)).T
+    _, C = torch.linalg.eigh(X.T @ H @ X)
+    C = X @ C
+    D = C[:, :nocc] @ C[:, :nocc].T
+    for _ in range(2):
+        eng.jk(2 * D, D, tau=1e-14)
+    dD = D * 1e-3
+    eng.jk(2 * dD, dD, mixed=True, tau=1e-12, tau_fp32=1e-6)
+    torch.cuda.synchronize()
+    print("profile workload done")
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -417,7 +447,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="dftk", choices=["dftk", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true", help="only run a few builds (for ncu captures)")
     args = ap.parse_args()
+    if args.profile:
+        return run_profile(args)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -45,6 +45,8 @@ class SCFResult:
     energy_history: List[float] = field(default_factory=list)
     energy_last_build: Optional[float] = None  # energy of the last incremental (FP64 or mixed) Fock build
     counts: Optional[List[int]] = None
+    incremental_builds: int = 0       # of fock_builds, those built from D - D_prev
+    incremental_seconds: float = 0.0  # and their share of fock_seconds
 
 
 def orthogonalizer(S: torch.Tensor) -> torch.Tensor:
@@ -196,6 +198,7 @@ def scf_rhf(engine: IntegralEngine, H: torch.Tensor, S: torch.Tensor, n_occ: int
     since_full = 0
     E_last = None
     e_last_incremental = None
+    n_inc, t_inc = 0, 0.0
     finishing = False  # density nearly converged: full FP64 builds from here on
     for it in range(max_iter + 1):
         full = (G is None) or (not incremental) or since_full >= rebuild_every or finishing
@@ -213,8 +216,12 @@ def scf_rhf(engine: IntegralEngine, H: torch.Tensor, S: torch.Tensor, n_occ: int
             since_full += 1
             incremental_build = True
         torch.cuda.synchronize(dev)
-        tb += time.perf_counter() - t0
+        dt = time.perf_counter() - t0
+        tb += dt
         builds += 1
+        if incremental_build:
+            n_inc += 1
+            t_inc += dt
         D_ref = D
         F = H + G
         E = float(torch.sum(D * (H + F))) + e_nn
@@ -243,8 +250,8 @@ def scf_rhf(engine: IntegralEngine, H: torch.Tensor, S: torch.Tensor, n_occ: int
             w, Cp = torch.linalg.eigh(X.T @ F @ X)
             C = X @ Cp
             return SCFResult(E, True, it, D, D, C, w, F, builds, tb, energies, e_last_build,
-                             counts_t.tolist() if counts_t is not None else None)
+                             counts_t.tolist() if counts_t is not None else None, n_inc, t_inc)
         E_prev = E
         D = D_new
     return SCFResult(E_last, False, max_iter, D, D, C, w, F, builds, tb, energies, E_last,
-                     counts_t.tolist() if counts_t is not None else None)
+                     counts_t.tolist() if counts_t is not None else None, n_inc, t_inc)
