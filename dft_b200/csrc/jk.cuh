@@ -493,10 +493,56 @@ __global__ void __launch_bounds__(SELECT_THREADS) k_select(const JkParams P)
     }
 }
 
+// Minimum resident 128-thread blocks per SM requested from the compiler for
+// each class kernel (caps its registers; 1 = no cap).  Measured on B200 for
+// (H2O)_64: caps that force 64 registers help the light classes most; the
+// p-rich classes lose to spills beyond these values.
+#ifndef DFTK_MINB_D0
+#define DFTK_MINB_D0 8
+#endif
+#ifndef DFTK_MINB_D1
+#define DFTK_MINB_D1 8
+#endif
+#ifndef DFTK_MINB_D2
+#define DFTK_MINB_D2 5
+#endif
+#ifndef DFTK_MINB_D3
+#define DFTK_MINB_D3 5
+#endif
+#ifndef DFTK_MINB_D4
+#define DFTK_MINB_D4 4
+#endif
+#ifndef DFTK_MINB_D5
+#define DFTK_MINB_D5 2
+#endif
+#ifndef DFTK_MINB_F0
+#define DFTK_MINB_F0 8
+#endif
+#ifndef DFTK_MINB_F1
+#define DFTK_MINB_F1 8
+#endif
+#ifndef DFTK_MINB_F2
+#define DFTK_MINB_F2 8
+#endif
+#ifndef DFTK_MINB_F3
+#define DFTK_MINB_F3 8
+#endif
+#ifndef DFTK_MINB_F4
+#define DFTK_MINB_F4 4
+#endif
+#ifndef DFTK_MINB_F5
+#define DFTK_MINB_F5 3
+#endif
+template <int C, typename T> struct JkMinBlocks {
+    static constexpr int d[6] = {DFTK_MINB_D0, DFTK_MINB_D1, DFTK_MINB_D2, DFTK_MINB_D3, DFTK_MINB_D4, DFTK_MINB_D5};
+    static constexpr int f[6] = {DFTK_MINB_F0, DFTK_MINB_F1, DFTK_MINB_F2, DFTK_MINB_F3, DFTK_MINB_F4, DFTK_MINB_F5};
+    static constexpr int value = sizeof(T) == 8 ? d[C] : f[C];
+};
+
 // J/K over the selected quartets of class C in precision T: warp w takes
 // list entries 32w .. 32w + 31 (one split of the c components at a time).
 template <int C, typename T>
-__global__ void __launch_bounds__(128) k_jk_list(const JkParams P)
+__global__ void __launch_bounds__(128, JkMinBlocks<C, T>::value) k_jk_list(const JkParams P)
 {
     constexpr int NS = EriClass<T, C, 0>::NSPLIT;
     constexpr bool fp32 = sizeof(T) == 4;
