@@ -26,7 +26,7 @@ SYMBOLS = (
     "dftk_version", "dftk_last_error", "dftk_init", "dftk_boys", "dftk_boys32",
     "dftk_pair_data", "dftk_schwarz", "dftk_one_electron", "dftk_eri_blocks",
     "dftk_jk_workspace_bytes", "dftk_jk_workspace_bytes_queue", "dftk_jk", "dftk_nuclear_kernel", "dftk_eri_kernel",
-    "dftk_fma_burn", "dftk_jk_timing", "dftk_jk_timing_read", "dftk_jk_noalloc",
+    "dftk_fma_burn", "dftk_jk_timing", "dftk_jk_timing_read", "dftk_jk_noalloc", "dftk_grad",
 )
 
 
@@ -112,6 +112,8 @@ def load() -> ctypes.CDLL:
         "dftk_fma_burn": ([i, i, i, i, vp, vp], i),
         "dftk_jk_noalloc": ([ctypes.POINTER(Shells), ctypes.POINTER(Pairs), ctypes.POINTER(Queue), vp, vp, vp,
                              vp, vp, vp, i, d, d, vp, vp], i),
+        "dftk_grad": ([ctypes.POINTER(Shells), vp, i, vp, vp, ctypes.POINTER(Pairs), ctypes.POINTER(Queue), vp, vp,
+                       vp, vp, d, vp, vp, sz, vp], i),
         "dftk_jk_timing": ([i], i),
         "dftk_jk_timing_read": ([vp, i], i),
     }

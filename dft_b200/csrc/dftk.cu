@@ -13,6 +13,7 @@
 #include "common.cuh"
 #include "generic.cuh"
 #include "jk.cuh"
+#include "grad.cuh"
 #include "onee.cuh"
 
 namespace {
@@ -488,6 +489,66 @@ int dftk_jk_timing_read(float *ms, int n)
             DFTK_CUDA(cudaEventElapsedTime(&ms[k], g_timing.start[k], g_timing.stop[k]));
         }
     }
+    return DFTK_OK;
+}
+
+int dftk_grad(const dftk_shells_t *shells, const int *shell_atom, int n_atoms, const double *atom_xyz,
+              const double *atom_z, const dftk_pairs_t pairs[DFTK_N_PCLASS], const dftk_queue_t *queue,
+              const double *D, const double *D_a, const double *D_b, const double *W, double tau, double *grad,
+              void *workspace, size_t workspace_bytes, dftk_stream_t stream)
+{
+    if (!shells || !shell_atom || n_atoms <= 0 || !atom_xyz || !atom_z || !pairs || !queue || !D || !D_a || !D_b ||
+        !W || !grad || !workspace)
+        return fail(DFTK_ERR_ARG, "dftk_grad: null argument");
+    const int ns = shells->n_shells, N = shells->n_ao;
+    if (workspace_bytes < (size_t)ns * ns * sizeof(float)) return fail(DFTK_ERR_WORKSPACE, "dftk_grad: workspace too small");
+    DFTK_INIT();
+    cudaStream_t s = (cudaStream_t)stream;
+    float *Dsh = (float *)workspace;
+    DFTK_CUDA(cudaMemsetAsync(grad, 0, 3 * sizeof(double) * n_atoms, s));
+    if (ns == 0) return DFTK_OK;
+    k_dsh<<<blocks_for((long long)ns * ns, 128), 128, 0, s>>>(shells->ao, shells->l, ns, N, D, D_a, D_b, 1, Dsh);
+    DFTK_LAUNCHED("k_dsh");
+    const long long npair = (long long)ns * (ns + 1) / 2;
+    k_grad_onee<<<blocks_for(npair, 64), 64, 0, s>>>(*shells, shell_atom, n_atoms, atom_xyz, atom_z, D, W, grad);
+    DFTK_LAUNCHED("k_grad_onee");
+    GradParams P;
+    memset(&P, 0, sizeof(P));
+    P.sh = *shells;
+    P.shell_atom = shell_atom;
+    for (int k = 0; k < 3; ++k) {
+        P.ab[k] = pairs[k].ab;
+        P.q[k] = pairs[k].q;
+        P.n_pairs[k] = pairs[k].n_pairs;
+    }
+    for (int c = 0; c < DFTK_N_QCLASS; ++c) {
+        P.n_rows[c] = queue->n_rows[c];
+        P.total[c] = queue->n_rows[c] > 0 ? queue->total[c] : 0;
+        P.row_off[c] = queue->row_off[c];
+    }
+    P.D = D;
+    P.Da = D_a;
+    P.Db = D_b;
+    P.Dsh = Dsh;
+    P.N = N;
+    P.ns = ns;
+    P.tau = tau;
+    P.grad = grad;
+    const long long cap = 148LL * 8;
+#define DFTK_GRAD_LAUNCH(CC)                                              \
+    if (P.total[CC] > 0) {                                                \
+        long long blocks = (P.total[CC] + 63) / 64;                       \
+        if (blocks > cap) blocks = cap;                                   \
+        k_grad_eri<CC><<<(unsigned)blocks, 64, 0, s>>>(P);                \
+        DFTK_LAUNCHED("k_grad_eri");                                      \
+    }
+    DFTK_GRAD_LAUNCH(0)
+    DFTK_GRAD_LAUNCH(1)
+    DFTK_GRAD_LAUNCH(2)
+    DFTK_GRAD_LAUNCH(3)
+    DFTK_GRAD_LAUNCH(4)
+    DFTK_GRAD_LAUNCH(5)
+#undef DFTK_GRAD_LAUNCH
     return DFTK_OK;
 }
 

@@ -46,6 +46,7 @@ __device__ __forceinline__ void herm_R(int L, double alpha, double X, double Y, 
     double F[LM + 1];
     boys_runtime(L, alpha * (X * X + Y * Y + Z * Z), F);
     double prev[D * D * D];
+    for (int i = 0; i < D * D * D; ++i) prev[i] = 0.0;  // entries beyond order L read as zero
     double scale[LM + 1];
     scale[0] = 1.0;
     for (int n = 1; n <= L; ++n) scale[n] = scale[n - 1] * (-2.0 * alpha);

@@ -246,6 +246,22 @@ class IntegralEngine:
             raise _lib.DftkError("jk", _lib.ERR_ARG, f"density shape {tuple(M.shape)} != ({self.n_ao}, {self.n_ao})")
         return M
 
+    def gradient(self, atoms: Sequence[str], centers, D: torch.Tensor, D_a: torch.Tensor, D_b: torch.Tensor,
+                 W: torch.Tensor, tau: float = 1e-14) -> np.ndarray:
+        """Electronic nuclear gradient (n_atoms, 3): sum D dH - sum W dS + sum Gamma d(ERI),
+        from the total density D, spin densities D_a/D_b and energy-weighted density W."""
+        n_atoms = len(atoms)
+        if not hasattr(self, "d_shell_atom"):
+            self.d_shell_atom = self._t(np.array([s["atom_idx"] for s in self.shells], dtype=np.int32), torch.int32)
+        xyz = torch.as_tensor(np.asarray(centers, dtype=np.float64).reshape(-1), device=self.device)
+        z = torch.as_tensor(np.array([float(int(a)) for a in atoms]), dtype=torch.float64, device=self.device)
+        g = torch.zeros(3 * n_atoms, dtype=torch.float64, device=self.device)
+        _lib.call("dftk_grad", ctypes.byref(self.c_shells), _lib.ptr(self.d_shell_atom), n_atoms, _lib.ptr(xyz),
+                  _lib.ptr(z), self.c_pairs, ctypes.byref(self.c_queue), _lib.ptr(self._square(D)),
+                  _lib.ptr(self._square(D_a)), _lib.ptr(self._square(D_b)), _lib.ptr(self._square(W)), float(tau),
+                  _lib.ptr(g), _lib.ptr(self.workspace), self.workspace_bytes, _lib.stream_handle())
+        return g.reshape(n_atoms, 3).cpu().numpy()
+
     def quartet_descriptors(self, quads: np.ndarray):
         """Map reference quartets (a, b, c, d) to dftk_eri_blocks descriptors and offsets."""
         quads = np.asarray(quads, dtype=np.int64).reshape(-1, 4)

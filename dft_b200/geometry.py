@@ -124,3 +124,12 @@ def nuclear_repulsion(atoms: Sequence[str], centers: np.ndarray) -> float:
     r = np.sqrt((d * d).sum(-1))
     iu = np.triu_indices(len(z), 1)
     return float((z[:, None] * z[None, :])[iu].dot(1.0 / r[iu]))
+
+
+def nuclear_repulsion_gradient(atoms: Sequence[str], centers: np.ndarray) -> np.ndarray:
+    """dE_NN/dR_A = -sum_{B != A} Z_A Z_B (R_A - R_B) / |R_A - R_B|^3."""
+    z = np.array([int(a) for a in atoms], dtype=np.float64)
+    d = centers[:, None, :] - centers[None, :, :]
+    r = np.sqrt((d * d).sum(-1))
+    np.fill_diagonal(r, np.inf)
+    return -np.einsum("ab,abx->ax", (z[:, None] * z[None, :]) / r ** 3, d)

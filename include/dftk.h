@@ -183,6 +183,18 @@ int dftk_jk_noalloc(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N
 int dftk_jk_timing(int enable);
 int dftk_jk_timing_read(float *ms, int n);
 
+/* Analytic nuclear gradient (no counterpart in the reference): grad[3 * atom
+ * + x] is overwritten with sum D dH/dX - sum W dS/dX + sum Gamma d(ab|cd)/dX
+ * (electronic part; the nuclear repulsion term is the caller's).  D is the
+ * total density, D_a / D_b the spin densities (both D/2 for RHF), W the
+ * energy-weighted density; shell_atom maps shells to atoms, atom_z are the
+ * nuclear charges.  Quartets of `queue` with Q_ab Q_cd max|D|^2 < tau are
+ * skipped.  workspace: at least n_shells^2 floats. */
+int dftk_grad(const dftk_shells_t *shells, const int *shell_atom, int n_atoms, const double *atom_xyz,
+              const double *atom_z, const dftk_pairs_t pairs[DFTK_N_PCLASS], const dftk_queue_t *queue,
+              const double *D, const double *D_a, const double *D_b, const double *W, double tau,
+              double *grad, void *workspace, size_t workspace_bytes, dftk_stream_t stream);
+
 /* Drop-in for the reference's nuclear_kernel (same arguments and output
  * layout, shelled.py:350-371): one thread per primitive-component pair,
  * E arrays with 7 slots per pair, num_atoms nuclei with integer charges. */
