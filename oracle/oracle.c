@@ -683,3 +683,283 @@ int orc_num_threads(void)
     return 1;
 #endif
 }
+
+/* ------------------------------------------------------------ gradients */
+/* Nuclear gradient of the SCF energy (no counterpart in the reference; the
+ * reference has no gradients).  Restated from the definitions, independently
+ * of the GPU kernels' adjoint ordering: every derivative integral is formed
+ * explicitly by the centre-derivative rule of a Cartesian Gaussian,
+ *   d/dA_x [a] = 2 alpha [a + 1_x] - a_x [a - 1_x],
+ * applied on every centre (all four ERI centres, both one-electron centres
+ * and the nuclear-attraction operator centre, whose derivative is
+ * -sum E E E R_{t+1,u,v}), with the MD primitives of this file.  The caller
+ * passes the total density D, the spin densities Da, Db and the
+ * energy-weighted density W; grad[3 * atom + x] receives
+ *   sum D dH - sum W dS + 1/2 sum d(mn|ls) [D_mn D_ls - Da_ml Da_ns - Db_ml Db_ns]. */
+
+/* 1-D E^{i,j}_t for i, j <= 3 of one primitive pair: E[((i * 4) + j) * ORC_E + t] */
+static void orc_E_table(double al, double be, double A, double B, double *E)
+{
+    for (int i = 0; i <= 3; ++i)
+        for (int j = 0; j <= 3; ++j) orc_hermite_E(al, be, A, B, i, j, E + (i * 4 + j) * ORC_E);
+}
+
+/* unnormalised primitive (ab|cd) with powers pa..pd from E tables and an R box
+ * (box side 6, index ((t * 6 + u) * 6 + v) * 6 + n) */
+static double orc_eri_from_tables(const double *Eb[3], const double *Ek[3], const int *pa,
+                                  const int *pb, const int *pc, const int *pd, const double *R,
+                                  double pre)
+{
+    for (int x = 0; x < 3; ++x)
+        if (pa[x] < 0 || pb[x] < 0 || pc[x] < 0 || pd[x] < 0) return 0.0;
+    const double *ex = Eb[0] + (pa[0] * 4 + pb[0]) * ORC_E, *ey = Eb[1] + (pa[1] * 4 + pb[1]) * ORC_E,
+                 *ez = Eb[2] + (pa[2] * 4 + pb[2]) * ORC_E;
+    const double *fx = Ek[0] + (pc[0] * 4 + pd[0]) * ORC_E, *fy = Ek[1] + (pc[1] * 4 + pd[1]) * ORC_E,
+                 *fz = Ek[2] + (pc[2] * 4 + pd[2]) * ORC_E;
+    double s = 0.0;
+    for (int t = 0; t <= pa[0] + pb[0]; ++t)
+        for (int u = 0; u <= pa[1] + pb[1]; ++u)
+            for (int v = 0; v <= pa[2] + pb[2]; ++v) {
+                double e = ex[t] * ey[u] * ez[v];
+                if (e == 0.0) continue;
+                for (int tau = 0; tau <= pc[0] + pd[0]; ++tau)
+                    for (int nu = 0; nu <= pc[1] + pd[1]; ++nu)
+                        for (int phi = 0; phi <= pc[2] + pd[2]; ++phi) {
+                            double f = fx[tau] * fy[nu] * fz[phi];
+                            if ((tau + nu + phi) & 1) f = -f;
+                            s += e * f * R[(((t + tau) * 6 + (u + nu)) * 6 + (v + phi)) * 6];
+                        }
+            }
+    return s * pre;
+}
+
+/* derivative of a primitive integral w.r.t. centre k (0..3) along axis x */
+static double orc_deri(const double *Eb[3], const double *Ek[3], const int *p4[4], const double *ex4,
+                       int k, int x, const double *R, double pre)
+{
+    int q[4][3];
+    for (int m = 0; m < 4; ++m)
+        for (int y = 0; y < 3; ++y) q[m][y] = p4[m][y];
+    q[k][x] += 1;
+    double v = 2.0 * ex4[k] * orc_eri_from_tables(Eb, Ek, q[0], q[1], q[2], q[3], R, pre);
+    if (p4[k][x] > 0) {
+        q[k][x] -= 2;
+        v -= p4[k][x] * orc_eri_from_tables(Eb, Ek, q[0], q[1], q[2], q[3], R, pre);
+    }
+    return v;
+}
+
+/* one primitive of a shell: exponent, powers, and the contraction x norm weight */
+typedef struct {
+    double ex, w;
+    int pw[3];
+    int aoi;
+} OrcPrim;
+
+static int orc_shell_prims(const OrcShells *S, int s, OrcPrim *out)
+{
+    int cmp = orc_ncomp(S->l[s]), ne = S->nexp[s], n = 0;
+    int pw[3 * 28];
+    orc_components(S->l[s], pw);
+    for (int k = 0; k < S->ncontr[s]; ++k)
+        for (int c = 0; c < cmp; ++c)
+            for (int e = 0; e < ne; ++e) {
+                OrcPrim *p = out + n++;
+                p->ex = S->exps[S->exp_off[s] + e];
+                for (int y = 0; y < 3; ++y) p->pw[y] = pw[3 * c + y];
+                p->w = S->coefs[S->coef_off[s] + k * ne + e] * orc_norm(p->ex, p->pw);
+                p->aoi = S->ao[s] + k * cmp + c;
+            }
+    return n;
+}
+
+/* 1-D overlap and kinetic pieces for the one-electron derivatives */
+static double orc_kin_1d(double al, double be, double A, double B, int la, int lb)
+{
+    if (la < 0 || lb < 0) return 0.0;
+    double v = -2.0 * be * (2 * lb + 1) * orc_overlap_1d(al, be, A, B, la, lb) +
+               4.0 * be * be * orc_overlap_1d(al, be, A, B, la, lb + 2);
+    if (lb >= 2) v += lb * (lb - 1) * orc_overlap_1d(al, be, A, B, la, lb - 2);
+    return v;
+}
+
+static double orc_S_prim(double al, double be, const double *A, const double *B, const int *pa, const int *pb)
+{
+    double s = 1.0;
+    for (int d = 0; d < 3; ++d) s *= orc_overlap_1d(al, be, A[d], B[d], pa[d], pb[d]);
+    return s;
+}
+
+static double orc_T_prim(double al, double be, const double *A, const double *B, const int *pa, const int *pb)
+{
+    double ov[3], kin[3];
+    for (int d = 0; d < 3; ++d) {
+        if (pa[d] < 0 || pb[d] < 0) return 0.0;
+        ov[d] = orc_overlap_1d(al, be, A[d], B[d], pa[d], pb[d]);
+        kin[d] = orc_kin_1d(al, be, A[d], B[d], pa[d], pb[d]);
+    }
+    return -0.5 * (kin[0] * ov[1] * ov[2] + kin[1] * ov[0] * ov[2] + kin[2] * ov[0] * ov[1]);
+}
+
+/* -2 pi / p Z sum_tuv E_t E_u E_v R_{t + sx, u + sy, v + sz}(p, P - C): the
+ * nuclear attraction primitive (shift 0) or, with a unit shift, minus its
+ * derivative w.r.t. the nuclear centre C. */
+static double orc_V_prim(double al, double be, const double *A, const double *B, const int *pa, const int *pb,
+                         const double *C, double Z, const int *shift)
+{
+    for (int d = 0; d < 3; ++d)
+        if (pa[d] < 0 || pb[d] < 0) return 0.0;
+    double p = al + be, E[3][ORC_E], P[3];
+    for (int d = 0; d < 3; ++d) {
+        orc_hermite_E(al, be, A[d], B[d], pa[d], pb[d], E[d]);
+        P[d] = (al * A[d] + be * B[d]) / p;
+    }
+    double R[6 * 6 * 6 * 6];
+    orc_hermite_R(6, 6, 6, 6, P[0] - C[0], P[1] - C[1], P[2] - C[2], p, R);
+    double s = 0.0;
+    for (int t = 0; t <= pa[0] + pb[0]; ++t)
+        for (int u = 0; u <= pa[1] + pb[1]; ++u)
+            for (int v = 0; v <= pa[2] + pb[2]; ++v)
+                s += E[0][t] * E[1][u] * E[2][v] * R[(((t + shift[0]) * 6 + u + shift[1]) * 6 + v + shift[2]) * 6];
+    return -2.0 * ORC_PI / p * Z * s;
+}
+
+void orc_gradient(int ns, const double *center, const int *l, const int *nexp, const int *ncontr,
+                  const int *exp_off, const int *coef_off, const int *ao, const double *exps,
+                  const double *coefs, const int *shell_atom, int natoms, const int *Z,
+                  const double *atom_xyz, int N, const double *D, const double *Da, const double *Db,
+                  const double *W, double *grad)
+{
+    OrcShells S = orc_shells(ns, center, l, nexp, ncontr, exp_off, coef_off, ao, exps, coefs);
+    int nthreads = orc_num_threads();
+    double *acc = (double *)calloc((size_t)nthreads * 3 * natoms, sizeof(double));
+    const int npair = ns * (ns + 1) / 2;
+    /* ---- one-electron part over all ordered shell pairs */
+    #pragma omp parallel for schedule(dynamic, 1)
+    for (int a = 0; a < ns; ++a) {
+        int tid = 0;
+#ifdef _OPENMP
+        tid = omp_get_thread_num();
+#endif
+        double *g = acc + (size_t)tid * 3 * natoms;
+        OrcPrim PA[256], PB[256];
+        int na = orc_shell_prims(&S, a, PA);
+        const double *A = center + 3 * a;
+        for (int b = 0; b < ns; ++b) {
+            int nb = orc_shell_prims(&S, b, PB);
+            const double *B = center + 3 * b;
+            for (int i = 0; i < na; ++i)
+                for (int j = 0; j < nb; ++j) {
+                    const OrcPrim *pi = PA + i, *pj = PB + j;
+                    double w = pi->w * pj->w;
+                    double dm = D[(long)pi->aoi * N + pj->aoi] * w, wm = W[(long)pi->aoi * N + pj->aoi] * w;
+                    for (int x = 0; x < 3; ++x) {
+                        int up[3] = {pi->pw[0], pi->pw[1], pi->pw[2]}, dn[3] = {pi->pw[0], pi->pw[1], pi->pw[2]};
+                        up[x] += 1;
+                        dn[x] -= 1;
+                        int bup[3] = {pj->pw[0], pj->pw[1], pj->pw[2]}, bdn[3] = {pj->pw[0], pj->pw[1], pj->pw[2]};
+                        bup[x] += 1;
+                        bdn[x] -= 1;
+                        /* d/dA and d/dB of S and T */
+                        double dSa = 2.0 * pi->ex * orc_S_prim(pi->ex, pj->ex, A, B, up, pj->pw) -
+                                     pi->pw[x] * orc_S_prim(pi->ex, pj->ex, A, B, dn, pj->pw);
+                        double dSb = 2.0 * pj->ex * orc_S_prim(pi->ex, pj->ex, A, B, pi->pw, bup) -
+                                     pj->pw[x] * orc_S_prim(pi->ex, pj->ex, A, B, pi->pw, bdn);
+                        double dTa = 2.0 * pi->ex * orc_T_prim(pi->ex, pj->ex, A, B, up, pj->pw) -
+                                     pi->pw[x] * orc_T_prim(pi->ex, pj->ex, A, B, dn, pj->pw);
+                        double dTb = 2.0 * pj->ex * orc_T_prim(pi->ex, pj->ex, A, B, pi->pw, bup) -
+                                     pj->pw[x] * orc_T_prim(pi->ex, pj->ex, A, B, pi->pw, bdn);
+                        g[3 * shell_atom[a] + x] += dm * dTa - wm * dSa;
+                        g[3 * shell_atom[b] + x] += dm * dTb - wm * dSb;
+                        const int zero[3] = {0, 0, 0};
+                        int unit[3] = {0, 0, 0};
+                        unit[x] = 1;
+                        for (int c = 0; c < natoms; ++c) {
+                            const double *Cc = atom_xyz + 3 * c;
+                            double zc = Z[c];
+                            double dVa = 2.0 * pi->ex * orc_V_prim(pi->ex, pj->ex, A, B, up, pj->pw, Cc, zc, zero) -
+                                         pi->pw[x] * orc_V_prim(pi->ex, pj->ex, A, B, dn, pj->pw, Cc, zc, zero);
+                            double dVb = 2.0 * pj->ex * orc_V_prim(pi->ex, pj->ex, A, B, pi->pw, bup, Cc, zc, zero) -
+                                         pj->pw[x] * orc_V_prim(pi->ex, pj->ex, A, B, pi->pw, bdn, Cc, zc, zero);
+                            /* d/dC_x R_tuv(P - C) = -R_{t+1,u,v} */
+                            double dVc = -orc_V_prim(pi->ex, pj->ex, A, B, pi->pw, pj->pw, Cc, zc, unit);
+                            g[3 * shell_atom[a] + x] += dm * dVa;
+                            g[3 * shell_atom[b] + x] += dm * dVb;
+                            g[3 * c + x] += dm * dVc;
+                        }
+                    }
+                }
+        }
+    }
+    /* ---- two-electron part over unique quartets */
+    #pragma omp parallel for schedule(dynamic, 1)
+    for (int ab = 0; ab < npair; ++ab) {
+        int tid = 0;
+#ifdef _OPENMP
+        tid = omp_get_thread_num();
+#endif
+        double *g = acc + (size_t)tid * 3 * natoms;
+        int a = (int)((sqrt(8.0 * ab + 1.0) - 1.0) / 2.0);
+        while (a * (a + 1) / 2 > ab) --a;
+        while ((a + 1) * (a + 2) / 2 <= ab) ++a;
+        int b = ab - a * (a + 1) / 2;
+        OrcPrim PA[256], PB[256], PC[256], PD[256];
+        int na = orc_shell_prims(&S, a, PA), nb = orc_shell_prims(&S, b, PB);
+        for (int cd = 0; cd <= ab; ++cd) {
+            int c = (int)((sqrt(8.0 * cd + 1.0) - 1.0) / 2.0);
+            while (c * (c + 1) / 2 > cd) --c;
+            while ((c + 1) * (c + 2) / 2 <= cd) ++c;
+            int d = cd - c * (c + 1) / 2;
+            int nc = orc_shell_prims(&S, c, PC), nd = orc_shell_prims(&S, d, PD);
+            int ew = (a == b) + (c == d) + (ab == cd);
+            double f = 8.0 / (double)(1 << ew);
+            const double *Ac = center + 3 * a, *Bc = center + 3 * b, *Cc = center + 3 * c, *Dc = center + 3 * d;
+            int at[4] = {shell_atom[a], shell_atom[b], shell_atom[c], shell_atom[d]};
+            /* loop over exponent quadruples, then over the components that share them */
+            for (int i = 0; i < na; ++i)
+                for (int j = 0; j < nb; ++j) {
+                    double Eb[3][16 * ORC_E];
+                    const OrcPrim *pi = PA + i, *pj = PB + j;
+                    double p = pi->ex + pj->ex, P[3];
+                    for (int x = 0; x < 3; ++x) {
+                        orc_E_table(pi->ex, pj->ex, Ac[x], Bc[x], Eb[x]);
+                        P[x] = (pi->ex * Ac[x] + pj->ex * Bc[x]) / p;
+                    }
+                    const double *Ebp[3] = {Eb[0], Eb[1], Eb[2]};
+                    for (int k = 0; k < nc; ++k)
+                        for (int m = 0; m < nd; ++m) {
+                            const OrcPrim *pk = PC + k, *pm = PD + m;
+                            const int mu = pi->aoi, nu = pj->aoi, la = pk->aoi, si = pm->aoi;
+                            double gam = 0.5 * D[(long)mu * N + nu] * D[(long)la * N + si] -
+                                         0.25 * (Da[(long)mu * N + la] * Da[(long)nu * N + si] +
+                                                 Db[(long)mu * N + la] * Db[(long)nu * N + si] +
+                                                 Da[(long)mu * N + si] * Da[(long)nu * N + la] +
+                                                 Db[(long)mu * N + si] * Db[(long)nu * N + la]);
+                            gam *= f * pi->w * pj->w * pk->w * pm->w;
+                            if (gam == 0.0) continue;
+                            double Ek[3][16 * ORC_E];
+                            double q = pk->ex + pm->ex, Q[3];
+                            for (int x = 0; x < 3; ++x) {
+                                orc_E_table(pk->ex, pm->ex, Cc[x], Dc[x], Ek[x]);
+                                Q[x] = (pk->ex * Cc[x] + pm->ex * Dc[x]) / q;
+                            }
+                            const double *Ekp[3] = {Ek[0], Ek[1], Ek[2]};
+                            double R[6 * 6 * 6 * 6];
+                            orc_hermite_R(6, 6, 6, 6, P[0] - Q[0], P[1] - Q[1], P[2] - Q[2], p * q / (p + q), R);
+                            double pre = 2.0 * ORC_PI * ORC_PI * sqrt(ORC_PI) / (p * q * sqrt(p + q));
+                            const int *p4[4] = {pi->pw, pj->pw, pk->pw, pm->pw};
+                            double ex4[4] = {pi->ex, pj->ex, pk->ex, pm->ex};
+                            for (int cen = 0; cen < 4; ++cen)
+                                for (int x = 0; x < 3; ++x)
+                                    g[3 * at[cen] + x] += gam * orc_deri(Ebp, Ekp, p4, ex4, cen, x, R, pre);
+                        }
+                }
+        }
+    }
+    for (int k = 0; k < 3 * natoms; ++k) {
+        double s = 0.0;
+        for (int t = 0; t < nthreads; ++t) s += acc[(size_t)t * 3 * natoms + k];
+        grad[k] = s;
+    }
+    free(acc);
+}

@@ -351,3 +351,58 @@ def ref_lib():
     for n in ("ref_run_nuclear_kernel", "ref_run_eri_kernel", "ref_run_eri_batch"):
         getattr(lib_, n).restype = None
     return lib_
+
+
+# --------------------------------------------------------------------------- gradients
+def nuclear_repulsion(atoms: Sequence[str], centers: np.ndarray) -> float:
+    z = [int(a) for a in atoms]
+    e = 0.0
+    for i in range(len(z)):
+        for j in range(i):
+            e += z[i] * z[j] / float(np.linalg.norm(centers[i] - centers[j]))
+    return e
+
+
+def nuclear_repulsion_gradient(atoms: Sequence[str], centers: np.ndarray) -> np.ndarray:
+    z = [int(a) for a in atoms]
+    g = np.zeros((len(z), 3))
+    for i in range(len(z)):
+        for j in range(len(z)):
+            if i != j:
+                d = centers[i] - centers[j]
+                g[i] -= z[i] * z[j] * d / float(np.linalg.norm(d)) ** 3
+    return g
+
+
+def gradient(shells: List[Dict], atoms: Sequence[str], centers: np.ndarray, D, Da, Db, W) -> np.ndarray:
+    """Total nuclear gradient (n_atoms, 3): electronic part from orc_gradient
+    (explicit derivative integrals on every centre) plus nuclear repulsion."""
+    sa = ShellArrays(shells)
+    Z = np.array([int(a) for a in atoms], dtype=np.int32)
+    xyz = np.ascontiguousarray(centers, dtype=np.float64).reshape(-1)
+    shell_atom = np.array([s["atom_idx"] for s in shells], dtype=np.int32)
+    D, Da, Db, W = (np.ascontiguousarray(x, dtype=np.float64) for x in (D, Da, Db, W))
+    g = np.zeros(3 * len(Z))
+    lib().orc_gradient(*sa.args(), _p(shell_atom), ctypes.c_int(len(Z)), _p(Z), _p(xyz), ctypes.c_int(sa.N),
+                       _p(D), _p(Da), _p(Db), _p(W), _p(g))
+    return g.reshape(-1, 3) + nuclear_repulsion_gradient(atoms, np.asarray(centers, dtype=np.float64))
+
+
+def scf_energy_gradient(basis_path: str, atoms: Sequence[str], centers: np.ndarray, etol: float = 1e-12,
+                        ptol: float = 1e-10, with_gradient: bool = True):
+    """Oracle SCF (the reference's loop with oracle J/K) and, optionally, its
+    analytic gradient with W = P_a F_a P_a + P_b F_b P_b (valid at convergence)."""
+    centers = np.asarray(centers, dtype=np.float64)
+    sh = build_shells(load_basis(basis_path), list(atoms), centers)
+    S, T, V = one_electron(sh, atoms, centers)
+    H = T + V
+    q = quartet_list(len(sh))
+    na, nb = electron_counts(atoms)
+    r = scf_uhf(H, S, lambda P, Pa, Pb: direct_jk(sh, q, P, Pa, Pb), na, nb, nuclear_repulsion(atoms, centers),
+                etol=etol, ptol=ptol)
+    if not with_gradient:
+        return r["energy"], None
+    Pa, Pb = r["P_a"], r["P_b"]
+    Fa, Fb = H + r["J"] - r["K_a"], H + r["J"] - r["K_b"]
+    W = Pa @ Fa @ Pa + Pb @ Fb @ Pb
+    return r["energy"], gradient(sh, atoms, centers, Pa + Pb, Pa, Pb, W)
