@@ -16,7 +16,10 @@
 // Field indices of a primitive-pair record (see dftk_pairs_t).
 enum { F_PX = 0, F_PY, F_PZ, F_P, F_K, F_H, F_AX, F_AY, F_AZ, F_BX, F_BY, F_BZ };
 
-__host__ __device__ constexpr int pair_fields(int pc) { return pc == 0 ? 5 : (pc == 1 ? 9 : 12); }
+// Stored fields per pair class: the ERI fields (ss 5, ps 9, pp 12) plus the
+// bra-side exponent alpha last (read only by the gradient kernels).
+__host__ __device__ constexpr int pair_fields(int pc) { return pc == 0 ? 6 : (pc == 1 ? 10 : 13); }
+__host__ __device__ constexpr int pair_alpha_field(int pc) { return pair_fields(pc) - 1; }
 
 // Inverse square root for the positive, normal, float-range arguments of the
 // integral kernels (p + q, and T beyond the Boys table): an FP32 estimate

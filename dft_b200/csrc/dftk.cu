@@ -507,18 +507,40 @@ int dftk_grad(const dftk_shells_t *shells, const int *shell_atom, int n_atoms, c
     float *Dsh = (float *)workspace;
     DFTK_CUDA(cudaMemsetAsync(grad, 0, 3 * sizeof(double) * n_atoms, s));
     if (ns == 0) return DFTK_OK;
+    // block-private gradient copies in shared memory when they fit
+    const size_t smem = n_atoms <= GRAD_SMEM_ATOMS ? 3 * sizeof(double) * n_atoms : 0;
+    const long long cap = 148LL * 8;
+    auto grid = [cap](long long work) {
+        long long b = (work + GRAD_THREADS - 1) / GRAD_THREADS;
+        return (unsigned)(b < 1 ? 1 : (b > cap ? cap : b));
+    };
     k_dsh<<<blocks_for((long long)ns * ns, 128), 128, 0, s>>>(shells->ao, shells->l, ns, N, D, D_a, D_b, 1, Dsh);
     DFTK_LAUNCHED("k_dsh");
-    const long long npair = (long long)ns * (ns + 1) / 2;
-    k_grad_onee<<<blocks_for(npair, 64), 64, 0, s>>>(*shells, shell_atom, n_atoms, atom_xyz, atom_z, D, W, grad);
-    DFTK_LAUNCHED("k_grad_onee");
+#define DFTK_GRAD_ONEE(PC)                                                                                   \
+    if (pairs[PC].n_pairs > 0) {                                                                             \
+        k_grad_overlap_kinetic<PC><<<grid(pairs[PC].n_pairs), GRAD_THREADS, smem, s>>>(                       \
+            *shells, pairs[PC].ab, pairs[PC].n_pairs, shell_atom, n_atoms, D, W, grad);                      \
+        DFTK_LAUNCHED("k_grad_overlap_kinetic");                                                             \
+        k_grad_nuclear<PC><<<grid((long long)pairs[PC].n_pairs * n_atoms), GRAD_THREADS, smem, s>>>(         \
+            *shells, pairs[PC].ab, pairs[PC].n_pairs, shell_atom, n_atoms, atom_xyz, atom_z, D, grad);       \
+        DFTK_LAUNCHED("k_grad_nuclear");                                                                     \
+    }
+    DFTK_GRAD_ONEE(0)
+    DFTK_GRAD_ONEE(1)
+    DFTK_GRAD_ONEE(2)
+#undef DFTK_GRAD_ONEE
     GradParams P;
     memset(&P, 0, sizeof(P));
     P.sh = *shells;
     P.shell_atom = shell_atom;
+    P.n_atoms = n_atoms;
+    P.kmax = pairs[0].kmax;
     for (int k = 0; k < 3; ++k) {
+        if (pairs[k].kmax != P.kmax) return fail(DFTK_ERR_ARG, "dftk_grad: pair classes with different kmax");
         P.ab[k] = pairs[k].ab;
         P.q[k] = pairs[k].q;
+        P.rec[k] = pairs[k].rec64;
+        P.nprim[k] = pairs[k].nprim;
         P.n_pairs[k] = pairs[k].n_pairs;
     }
     for (int c = 0; c < DFTK_N_QCLASS; ++c) {
@@ -534,13 +556,10 @@ int dftk_grad(const dftk_shells_t *shells, const int *shell_atom, int n_atoms, c
     P.ns = ns;
     P.tau = tau;
     P.grad = grad;
-    const long long cap = 148LL * 8;
-#define DFTK_GRAD_LAUNCH(CC)                                              \
-    if (P.total[CC] > 0) {                                                \
-        long long blocks = (P.total[CC] + 63) / 64;                       \
-        if (blocks > cap) blocks = cap;                                   \
-        k_grad_eri<CC><<<(unsigned)blocks, 64, 0, s>>>(P);                \
-        DFTK_LAUNCHED("k_grad_eri");                                      \
+#define DFTK_GRAD_LAUNCH(CC)                                                  \
+    if (P.total[CC] > 0) {                                                    \
+        k_grad_eri<CC><<<grid(P.total[CC]), GRAD_THREADS, smem, s>>>(P);      \
+        DFTK_LAUNCHED("k_grad_eri");                                          \
     }
     DFTK_GRAD_LAUNCH(0)
     DFTK_GRAD_LAUNCH(1)

@@ -41,7 +41,7 @@ CLASSES = [
     (1, 1, 1, 0, 1, "bra"),
     (1, 1, 1, 1, 3, "bra"),
 ]
-PAIR_FIELDS = {0: 5, 1: 9, 2: 12}
+PAIR_FIELDS = {0: 5, 1: 9, 2: 12}  # record fields the ERI code loads (the stored records add alpha last)
 
 
 def e1d(side, a, b, axis):

@@ -9,49 +9,38 @@
 // lower the power on that axis, d/dA_x x_A^i e^{-a x_A^2} = 2a x_A^{i+1} - i x_A^{i-1},
 // so every derivative integral is an MD integral at L + 1 whose Hermite
 // coefficients on the differentiated side are 2a E^{i+1,j} - i E^{i-1,j}
-// (exponent-shifted E), recomputed from the shells per primitive pair.  Two
-// electron part: per quartet, Gamma is formed once; the ket-transformed
-// Hermite integrals are contracted with Gamma into bra-Hermite intermediates
-// H[mu nu][tuv] summed over ket primitives, which the derivative E of one bra
-// primitive turns into dE/dA and dE/dB (adjoint order: no derivative integral
-// is stored).  dE/dC comes from the mirrored pass, dE/dD = -(A + B + C) by
-// translational invariance.
+// (exponent-shifted E), recomputed per primitive pair from the pair records
+// (P, p, K_AB, alpha) and the shell centres; nothing is stored per quartet.
+//
+// Two-electron part, one thread per Schwarz candidate shell quartet of a
+// class (compile-time angular momenta, so every Hermite loop unrolls into
+// registers).  Per bra primitive pair the Gamma-weighted bra Hermite density
+// Eg[m][T] = sum_n Gamma[n][m] E^n_T is formed once; per primitive quartet
+//   H[n][T]  += sum_T' (sum_m Gamma[n][m] (-1)^|T'| E^m_T') R_{T+T'}   (|T| <= L_ab + 1)
+//   dE/dC    += sum_m sum_T' dE^m_T'(C) (-1)^|T'| sum_T Eg[m][T] R_{T+T'}
+// and after the ket loop dE/dA, dE/dB = sum_n sum_T dE^n_T(A or B) H[n][T]
+// (adjoint order: no derivative integral is formed).  dE/dD = -(A + B + C)
+// by translational invariance.  Gradient sums go through a block-private
+// shared-memory copy of the gradient (one global atomic per atom coordinate
+// and block) when 3 n_atoms doubles fit, else straight to global atomics.
 #pragma once
 
-#include "generic.cuh"
+#include "boys.cuh"
+#include "common.cuh"
 
-#define GRAD_LMAX 5   // L + 1 for s/p shell quartets
-
-__device__ __forceinline__ int g_ncomp(int l) { return (l + 1) * (l + 2) / 2; }
-
-__device__ __forceinline__ void g_pow(int l, int k, int *pw)
-{
-    if (l == 0) { pw[0] = pw[1] = pw[2] = 0; return; }
-    pw[0] = (k == 0); pw[1] = (k == 1); pw[2] = (k == 2);
-}
-
-// 1-D Hermite E^{i,j}_t for i <= 2, j <= 2 (powers up to l + 1) on one axis:
-// E[(i * 3 + j) * 5 + t], t <= 4, zero beyond t = i + j.
-__device__ __forceinline__ void g_E_table(double al, double be, double A, double B, double *E)
-{
-    for (int i = 0; i <= 2; ++i)
-        for (int j = 0; j <= 2; ++j) {
-            double e[16];
-            herm_E1d(al, be, A, B, i, j, e);
-            for (int t = 0; t < 5; ++t) E[(i * 3 + j) * 5 + t] = t <= i + j ? e[t] : 0.0;
-        }
-}
-
-// Hermite index of (t, u, v) with t + u + v <= 3 in a dense 4^3 box
-#define HIDX(t, u, v) (((t) * 4 + (u)) * 4 + (v))
-#define RIDX5(t, u, v) (((t) * (GRAD_LMAX + 1) + (u)) * (GRAD_LMAX + 1) + (v))
+#define GRAD_THREADS 128
+#define GRAD_SMEM_ATOMS 2048  // 48 KB of shared memory
 
 struct GradParams {
     dftk_shells_t sh;
     const int *shell_atom;
+    int n_atoms;
     const int *ab[3];
     const double *q[3];
+    const double *rec[3];
+    const int *nprim[3];
     int n_pairs[3];
+    int kmax;
     long long n_rows[DFTK_N_QCLASS];
     long long total[DFTK_N_QCLASS];
     const long long *row_off[DFTK_N_QCLASS];
@@ -62,370 +51,605 @@ struct GradParams {
     double *grad;  // [n_atoms * 3], accumulated
 };
 
-// Bra-side pass: g_A and g_B of one shell quartet.
-__device__ void grad_quartet_bra(const GradParams &P, int a, int b, int c, int d, const double *G, double *gA,
-                                 double *gB)
+// Quartet classes (ss|ss)..(pp|pp): angular momenta and pair classes.
+template <int C> struct GradClassOf;
+template <> struct GradClassOf<0> { static constexpr int LA = 0, LB = 0, LC = 0, LD = 0, X = 0, Y = 0; };
+template <> struct GradClassOf<1> { static constexpr int LA = 1, LB = 0, LC = 0, LD = 0, X = 1, Y = 0; };
+template <> struct GradClassOf<2> { static constexpr int LA = 1, LB = 0, LC = 1, LD = 0, X = 1, Y = 1; };
+template <> struct GradClassOf<3> { static constexpr int LA = 1, LB = 1, LC = 0, LD = 0, X = 2, Y = 0; };
+template <> struct GradClassOf<4> { static constexpr int LA = 1, LB = 1, LC = 1, LD = 0, X = 2, Y = 1; };
+template <> struct GradClassOf<5> { static constexpr int LA = 1, LB = 1, LC = 1, LD = 1, X = 2, Y = 2; };
+
+// power of axis x of Cartesian component k of an s or p shell (x, y, z order)
+__device__ __forceinline__ constexpr int g_cp(int l, int k, int x) { return l == 0 ? 0 : (k == x ? 1 : 0); }
+
+// 1-D Hermite coefficients E^{i,j}_t without the Gaussian product factor,
+// i <= IA, j <= JB, t <= i + j:
+//   E^{i+1,j}_t = h E^{ij}_{t-1} + X_PA E^{ij}_t + (t+1) E^{ij}_{t+1}   (h = 1/2p)
+// and the same in j with X_PB.
+template <int IA, int JB>
+__device__ __forceinline__ void g_etab(double PA, double PB, double h, double (&E)[IA + 1][JB + 1][IA + JB + 1])
 {
-    const dftk_shells_t &sh = P.sh;
-    const int la = sh.l[a], lb = sh.l[b], lc = sh.l[c], ld = sh.l[d];
-    const int na = g_ncomp(la), nb = g_ncomp(lb), nc = g_ncomp(lc), nd = g_ncomp(ld);
-    const int Lab = la + lb + 1;  // bra Hermite order after differentiation
-    const int L = la + lb + lc + ld + 1;
-    const double *A = sh.xyz + 3 * a, *B = sh.xyz + 3 * b, *C = sh.xyz + 3 * c, *Dd = sh.xyz + 3 * d;
-    for (int k = 0; k < 3; ++k) gA[k] = gB[k] = 0.0;
-    for (int ia = 0; ia < sh.nprim[a]; ++ia)
-        for (int ib = 0; ib < sh.nprim[b]; ++ib) {
-            const double al = sh.prim_exp[sh.prim_off[a] + ia], be = sh.prim_exp[sh.prim_off[b] + ib];
-            const double cab = sh.prim_cn[sh.prim_off[a] + ia] * sh.prim_cn[sh.prim_off[b] + ib];
-            const double p = al + be;
-            double Pc[3], Eab[3][45];
-            for (int x = 0; x < 3; ++x) {
-                Pc[x] = (al * A[x] + be * B[x]) / p;
-                g_E_table(al, be, A[x], B[x], Eab[x]);
+    E[0][0][0] = 1.0;
+#pragma unroll
+    for (int i = 0; i < IA; ++i)
+#pragma unroll
+        for (int t = 0; t <= i + 1; ++t) {
+            double v;
+            if (t <= i) {
+                v = PA * E[i][0][t];
+                if (t > 0) v = fma(h, E[i][0][t - 1], v);
+            } else {
+                v = h * E[i][0][t - 1];
             }
-            // H[n][tuv] = sum over ket primitives and components m of
-            //             Gamma[n][m] sum_tau (-1)^tau E^m_tau R_{t+tau}
-            double H[9 * 64];
-            for (int i = 0; i < na * nb * 64; ++i) H[i] = 0.0;
-            for (int ic = 0; ic < sh.nprim[c]; ++ic)
-                for (int id = 0; id < sh.nprim[d]; ++id) {
-                    const double ga = sh.prim_exp[sh.prim_off[c] + ic], de = sh.prim_exp[sh.prim_off[d] + id];
-                    const double ccd = sh.prim_cn[sh.prim_off[c] + ic] * sh.prim_cn[sh.prim_off[d] + id];
-                    const double qq = ga + de;
-                    double Qc[3], Ecd[3][45];
-                    for (int x = 0; x < 3; ++x) {
-                        Qc[x] = (ga * C[x] + de * Dd[x]) / qq;
-                        g_E_table(ga, de, C[x], Dd[x], Ecd[x]);
-                    }
-                    const double rho = p * qq / (p + qq);
-                    const double pre = 2.0 * DFTK_PI * DFTK_PI * sqrt(DFTK_PI) / (p * qq * sqrt(p + qq)) * cab * ccd;
-                    double R[(GRAD_LMAX + 1) * (GRAD_LMAX + 1) * (GRAD_LMAX + 1)];
-                    herm_R<GRAD_LMAX>(L, rho, Pc[0] - Qc[0], Pc[1] - Qc[1], Pc[2] - Qc[2], R);
-                    for (int kc = 0; kc < nc; ++kc)
-                        for (int kd = 0; kd < nd; ++kd) {
-                            int pc[3], pd[3];
-                            g_pow(lc, kc, pc);
-                            g_pow(ld, kd, pd);
-                            double Tt[64];
-                            for (int t = 0; t <= Lab; ++t)
-                                for (int u = 0; u + t <= Lab; ++u)
-                                    for (int v = 0; v + u + t <= Lab; ++v) {
-                                        double s = 0.0;
-                                        for (int tx = 0; tx <= pc[0] + pd[0]; ++tx)
-                                            for (int ty = 0; ty <= pc[1] + pd[1]; ++ty)
-                                                for (int tz = 0; tz <= pc[2] + pd[2]; ++tz) {
-                                                    const double e = Ecd[0][(pc[0] * 3 + pd[0]) * 5 + tx] *
-                                                                     Ecd[1][(pc[1] * 3 + pd[1]) * 5 + ty] *
-                                                                     Ecd[2][(pc[2] * 3 + pd[2]) * 5 + tz];
-                                                    const double sg = ((tx + ty + tz) & 1) ? -1.0 : 1.0;
-                                                    s += sg * e * R[RIDX5(t + tx, u + ty, v + tz)];
-                                                }
-                                        Tt[HIDX(t, u, v)] = s * pre;
-                                    }
-                            const int m = kc * nd + kd;
-                            for (int n = 0; n < na * nb; ++n) {
-                                const double g = G[n * 9 + m];
-                                if (g == 0.0) continue;
-                                for (int t = 0; t <= Lab; ++t)
-                                    for (int u = 0; u + t <= Lab; ++u)
-                                        for (int v = 0; v + u + t <= Lab; ++v)
-                                            H[n * 64 + HIDX(t, u, v)] += g * Tt[HIDX(t, u, v)];
-                            }
-                        }
-                }
-            // contract with the exponent-shifted bra E coefficients
-            for (int ka = 0; ka < na; ++ka)
-                for (int kb = 0; kb < nb; ++kb) {
-                    int pa[3], pb[3];
-                    g_pow(la, ka, pa);
-                    g_pow(lb, kb, pb);
-                    const double *Hn = H + (ka * nb + kb) * 64;
-                    for (int dir = 0; dir < 3; ++dir)
-                        for (int side = 0; side < 2; ++side) {
-                            double s = 0.0;
-                            for (int t = 0; t <= Lab; ++t)
-                                for (int u = 0; u + t <= Lab; ++u)
-                                    for (int v = 0; v + u + t <= Lab; ++v) {
-                                        const int tt[3] = {t, u, v};
-                                        double e = 1.0;
-                                        for (int x = 0; x < 3 && e != 0.0; ++x) {
-                                            const int i = pa[x], j = pb[x];
-                                            double f;
-                                            if (x != dir) {
-                                                f = Eab[x][(i * 3 + j) * 5 + tt[x]];
-                                            } else if (side == 0) {
-                                                f = 2.0 * al * Eab[x][((i + 1) * 3 + j) * 5 + tt[x]];
-                                                if (i > 0) f -= i * Eab[x][((i - 1) * 3 + j) * 5 + tt[x]];
-                                            } else {
-                                                f = 2.0 * be * Eab[x][(i * 3 + j + 1) * 5 + tt[x]];
-                                                if (j > 0) f -= j * Eab[x][(i * 3 + j - 1) * 5 + tt[x]];
-                                            }
-                                            e *= f;
-                                        }
-                                        s += e * Hn[HIDX(t, u, v)];
-                                    }
-                            if (side == 0) gA[dir] += s; else gB[dir] += s;
-                        }
-                }
+            if (t + 1 <= i) v = fma((double)(t + 1), E[i][0][t + 1], v);
+            E[i + 1][0][t] = v;
         }
+#pragma unroll
+    for (int j = 0; j < JB; ++j)
+#pragma unroll
+        for (int i = 0; i <= IA; ++i)
+#pragma unroll
+            for (int t = 0; t <= i + j + 1; ++t) {
+                double v;
+                if (t <= i + j) {
+                    v = PB * E[i][j][t];
+                    if (t > 0) v = fma(h, E[i][j][t - 1], v);
+                } else {
+                    v = h * E[i][j][t - 1];
+                }
+                if (t + 1 <= i + j) v = fma((double)(t + 1), E[i][j][t + 1], v);
+                E[i][j + 1][t] = v;
+            }
 }
 
-// Ket-side pass: g_C of one shell quartet (mirror image of the bra pass).
-__device__ void grad_quartet_ket(const GradParams &P, int a, int b, int c, int d, const double *G, double *gC)
+// R_{tuv} = R^{(0)}_{tuv}(rho, X, Y, Z) for t + u + v <= LM, times `pre`:
+// R^{(n)}_{000} = pre (-2 rho)^n F_n and
+// R^{(n)}_{t+1,u,v} = t R^{(n+1)}_{t-1,u,v} + X R^{(n+1)}_{t,u,v} (first non-zero index).
+template <int LM>
+__device__ __forceinline__ void g_rcube(double X, double Y, double Z, double m2rho, double pre, const double *F,
+                                        double (&R)[LM + 1][LM + 1][LM + 1])
 {
-    const dftk_shells_t &sh = P.sh;
-    const int la = sh.l[a], lb = sh.l[b], lc = sh.l[c], ld = sh.l[d];
-    const int na = g_ncomp(la), nb = g_ncomp(lb), nc = g_ncomp(lc), nd = g_ncomp(ld);
-    const int Lcd = lc + ld + 1;
-    const int L = la + lb + lc + ld + 1;
-    const double *A = sh.xyz + 3 * a, *B = sh.xyz + 3 * b, *C = sh.xyz + 3 * c, *Dd = sh.xyz + 3 * d;
-    for (int k = 0; k < 3; ++k) gC[k] = 0.0;
-    for (int ic = 0; ic < sh.nprim[c]; ++ic)
-        for (int id = 0; id < sh.nprim[d]; ++id) {
-            const double ga = sh.prim_exp[sh.prim_off[c] + ic], de = sh.prim_exp[sh.prim_off[d] + id];
-            const double ccd = sh.prim_cn[sh.prim_off[c] + ic] * sh.prim_cn[sh.prim_off[d] + id];
-            const double qq = ga + de;
-            double Qc[3], Ecd[3][45];
-            for (int x = 0; x < 3; ++x) {
-                Qc[x] = (ga * C[x] + de * Dd[x]) / qq;
-                g_E_table(ga, de, C[x], Dd[x], Ecd[x]);
+    double Rn[LM + 1][LM + 1][LM + 1][LM + 1];
+    double c = pre;
+#pragma unroll
+    for (int n = 0; n <= LM; ++n) {
+        Rn[n][0][0][0] = c * F[n];
+        c *= m2rho;
+    }
+#pragma unroll
+    for (int s = 1; s <= LM; ++s)
+#pragma unroll
+        for (int t = 0; t <= s; ++t)
+#pragma unroll
+            for (int u = 0; u <= s - t; ++u) {
+                const int v = s - t - u;
+#pragma unroll
+                for (int n = 0; n <= LM - s; ++n) {
+                    double r;
+                    if (t > 0) {
+                        r = X * Rn[n + 1][t - 1][u][v];
+                        if (t > 1) r = fma((double)(t - 1), Rn[n + 1][t - 2][u][v], r);
+                    } else if (u > 0) {
+                        r = Y * Rn[n + 1][t][u - 1][v];
+                        if (u > 1) r = fma((double)(u - 1), Rn[n + 1][t][u - 2][v], r);
+                    } else {
+                        r = Z * Rn[n + 1][t][u][v - 1];
+                        if (v > 1) r = fma((double)(v - 1), Rn[n + 1][t][u][v - 2], r);
+                    }
+                    Rn[n][t][u][v] = r;
+                }
             }
-            double H[9 * 64];
-            for (int i = 0; i < nc * nd * 64; ++i) H[i] = 0.0;
-            for (int ia = 0; ia < sh.nprim[a]; ++ia)
-                for (int ib = 0; ib < sh.nprim[b]; ++ib) {
-                    const double al = sh.prim_exp[sh.prim_off[a] + ia], be = sh.prim_exp[sh.prim_off[b] + ib];
-                    const double cab = sh.prim_cn[sh.prim_off[a] + ia] * sh.prim_cn[sh.prim_off[b] + ib];
-                    const double p = al + be;
-                    double Pc[3], Eab[3][45];
-                    for (int x = 0; x < 3; ++x) {
-                        Pc[x] = (al * A[x] + be * B[x]) / p;
-                        g_E_table(al, be, A[x], B[x], Eab[x]);
-                    }
-                    const double rho = p * qq / (p + qq);
-                    const double pre = 2.0 * DFTK_PI * DFTK_PI * sqrt(DFTK_PI) / (p * qq * sqrt(p + qq)) * cab * ccd;
-                    double R[(GRAD_LMAX + 1) * (GRAD_LMAX + 1) * (GRAD_LMAX + 1)];
-                    herm_R<GRAD_LMAX>(L, rho, Pc[0] - Qc[0], Pc[1] - Qc[1], Pc[2] - Qc[2], R);
-                    for (int ka = 0; ka < na; ++ka)
-                        for (int kb = 0; kb < nb; ++kb) {
-                            int pa[3], pb[3];
-                            g_pow(la, ka, pa);
-                            g_pow(lb, kb, pb);
-                            double Tt[64];
-                            for (int t = 0; t <= Lcd; ++t)
-                                for (int u = 0; u + t <= Lcd; ++u)
-                                    for (int v = 0; v + u + t <= Lcd; ++v) {
-                                        double s = 0.0;
-                                        for (int tx = 0; tx <= pa[0] + pb[0]; ++tx)
-                                            for (int ty = 0; ty <= pa[1] + pb[1]; ++ty)
-                                                for (int tz = 0; tz <= pa[2] + pb[2]; ++tz) {
-                                                    const double e = Eab[0][(pa[0] * 3 + pb[0]) * 5 + tx] *
-                                                                     Eab[1][(pa[1] * 3 + pb[1]) * 5 + ty] *
-                                                                     Eab[2][(pa[2] * 3 + pb[2]) * 5 + tz];
-                                                    s += e * R[RIDX5(t + tx, u + ty, v + tz)];
-                                                }
-                                        Tt[HIDX(t, u, v)] = s * pre;
-                                    }
-                            const int n = ka * nb + kb;
-                            for (int m = 0; m < nc * nd; ++m) {
-                                const double g = G[n * 9 + m];
-                                if (g == 0.0) continue;
-                                for (int t = 0; t <= Lcd; ++t)
-                                    for (int u = 0; u + t <= Lcd; ++u)
-                                        for (int v = 0; v + u + t <= Lcd; ++v)
-                                            H[m * 64 + HIDX(t, u, v)] += g * Tt[HIDX(t, u, v)];
-                            }
-                        }
-                }
-            for (int kc = 0; kc < nc; ++kc)
-                for (int kd = 0; kd < nd; ++kd) {
-                    int pc[3], pd[3];
-                    g_pow(lc, kc, pc);
-                    g_pow(ld, kd, pd);
-                    const double *Hm = H + (kc * nd + kd) * 64;
-                    for (int dir = 0; dir < 3; ++dir) {
-                        double s = 0.0;
-                        for (int t = 0; t <= Lcd; ++t)
-                            for (int u = 0; u + t <= Lcd; ++u)
-                                for (int v = 0; v + u + t <= Lcd; ++v) {
-                                    const int tt[3] = {t, u, v};
-                                    double e = ((t + u + v) & 1) ? -1.0 : 1.0;
-                                    for (int x = 0; x < 3 && e != 0.0; ++x) {
-                                        const int i = pc[x], j = pd[x];
-                                        double f;
-                                        if (x != dir) {
-                                            f = Ecd[x][(i * 3 + j) * 5 + tt[x]];
-                                        } else {
-                                            f = 2.0 * ga * Ecd[x][((i + 1) * 3 + j) * 5 + tt[x]];
-                                            if (i > 0) f -= i * Ecd[x][((i - 1) * 3 + j) * 5 + tt[x]];
-                                        }
-                                        e *= f;
-                                    }
-                                    s += e * Hm[HIDX(t, u, v)];
-                                }
-                        gC[dir] += s;
-                    }
-                }
-        }
+#pragma unroll
+    for (int t = 0; t <= LM; ++t)
+#pragma unroll
+        for (int u = 0; u <= LM - t; ++u)
+#pragma unroll
+            for (int v = 0; v <= LM - t - u; ++v) R[t][u][v] = Rn[0][t][u][v];
 }
 
-// Two-electron gradient: one thread per Schwarz candidate quartet of class C;
-// quartets with Q_ab Q_cd max|D|^2 < tau are skipped.
+// gradient accumulation into the block's shared copy (or global memory)
+__device__ __forceinline__ void g_add(double *s_grad, double *grad, int idx, double v)
+{
+    if (s_grad) atomicAdd(s_grad + idx, v);
+    else atomicAdd(grad + idx, v);
+}
+
+__device__ __forceinline__ void g_smem_begin(double *s_grad, int n3)
+{
+    if (s_grad)
+        for (int i = threadIdx.x; i < n3; i += blockDim.x) s_grad[i] = 0.0;
+    __syncthreads();
+}
+
+__device__ __forceinline__ void g_smem_end(const double *s_grad, double *grad, int n3)
+{
+    __syncthreads();
+    if (s_grad)
+        for (int i = threadIdx.x; i < n3; i += blockDim.x)
+            if (s_grad[i] != 0.0) atomicAdd(grad + i, s_grad[i]);
+}
+
+// Two-electron gradient, class C; quartets with Q_ab Q_cd max|D|^2 < tau are skipped.
 template <int C>
-__global__ void __launch_bounds__(64) k_grad_eri(const GradParams P)
+__global__ void __launch_bounds__(GRAD_THREADS) k_grad_eri(const GradParams P)
 {
-    constexpr int bra_pc[6] = {0, 1, 1, 2, 2, 2};
-    constexpr int ket_pc[6] = {0, 0, 1, 0, 1, 2};
-    const int X = bra_pc[C], Yc = ket_pc[C];
+    using G = GradClassOf<C>;
+    constexpr int LA = G::LA, LB = G::LB, LC = G::LC, LD = G::LD, X = G::X, Y = G::Y;
+    constexpr int NA = LA ? 3 : 1, NB = LB ? 3 : 1, NC = LC ? 3 : 1, ND = LD ? 3 : 1;
+    constexpr int NN = NA * NB, NM = NC * ND;
+    constexpr int LAB = LA + LB, LCD = LC + LD, LM = LAB + LCD + 1;
+    extern __shared__ double s_grad[];
+    double *sg = P.n_atoms <= GRAD_SMEM_ATOMS ? s_grad : nullptr;
+    g_smem_begin(sg, 3 * P.n_atoms);
     const long long ncand = P.total[C];
     const long long stride = (long long)gridDim.x * blockDim.x;
+    const int nX = P.n_pairs[X], nY = P.n_pairs[Y];
+    const long long fsX = (long long)P.kmax * nX, fsY = (long long)P.kmax * nY;
+    constexpr int faX = pair_alpha_field(X), faY = pair_alpha_field(Y);
     for (long long cand = (long long)blockIdx.x * blockDim.x + threadIdx.x; cand < ncand; cand += stride) {
         const int row = find_row(P.row_off[C], P.n_rows[C], cand);
         const int ket = (int)(cand - P.row_off[C][row]);
         const int a = P.ab[X][2 * row], b = P.ab[X][2 * row + 1];
-        const int c = P.ab[Yc][2 * ket], d = P.ab[Yc][2 * ket + 1];
+        const int c = P.ab[Y][2 * ket], d = P.ab[Y][2 * ket + 1];
         const int ns = P.ns;
         const float dm = fmaxf(fmaxf(P.Dsh[a * ns + b], P.Dsh[c * ns + d]),
                                fmaxf(fmaxf(P.Dsh[a * ns + c], P.Dsh[a * ns + d]),
                                      fmaxf(P.Dsh[b * ns + c], P.Dsh[b * ns + d])));
-        if (P.q[X][row] * P.q[Yc][ket] * (double)dm * (double)dm < P.tau) continue;
-        const int N = P.N;
+        if (P.q[X][row] * P.q[Y][ket] * (double)dm * (double)dm < P.tau) continue;
+        const long long N = P.N;
         const int oa = P.sh.ao[a], ob = P.sh.ao[b], oc = P.sh.ao[c], od = P.sh.ao[d];
-        const int na = g_ncomp(P.sh.l[a]), nb = g_ncomp(P.sh.l[b]), nc = g_ncomp(P.sh.l[c]), nd = g_ncomp(P.sh.l[d]);
-        const int ew = (a == b) + (c == d) + ((X == Yc) && (row == ket));
+        const int ew = (a == b) + (c == d) + ((X == Y) && (row == ket));
         const double f = 8.0 / (double)(1 << ew);  // orientations of the unique quartet
-        double G[81];
-        for (int i = 0; i < na; ++i)
-            for (int j = 0; j < nb; ++j)
-                for (int k = 0; k < nc; ++k)
-                    for (int l = 0; l < nd; ++l) {
-                        const long long I = oa + i, Jn = ob + j, K = oc + k, Ln = od + l;
-                        const double coul = 0.5 * P.D[I * N + Jn] * P.D[K * N + Ln];
-                        const double exch = 0.25 * (P.Da[I * N + K] * P.Da[Jn * N + Ln] + P.Db[I * N + K] * P.Db[Jn * N + Ln] +
-                                                    P.Da[I * N + Ln] * P.Da[Jn * N + K] + P.Db[I * N + Ln] * P.Db[Jn * N + K]);
-                        G[(i * nb + j) * 9 + k * nd + l] = f * (coul - exch);
+        double Gm[NN][NM];
+#pragma unroll
+        for (int i = 0; i < NA; ++i)
+#pragma unroll
+            for (int j = 0; j < NB; ++j)
+#pragma unroll
+                for (int k = 0; k < NC; ++k)
+#pragma unroll
+                    for (int l = 0; l < ND; ++l) {
+                        const long long I = oa + i, J = ob + j, K = oc + k, Lq = od + l;
+                        const double coul = 0.5 * P.D[I * N + J] * P.D[K * N + Lq];
+                        const double exch = 0.25 * (P.Da[I * N + K] * P.Da[J * N + Lq] + P.Db[I * N + K] * P.Db[J * N + Lq] +
+                                                    P.Da[I * N + Lq] * P.Da[J * N + K] + P.Db[I * N + Lq] * P.Db[J * N + K]);
+                        Gm[i * NB + j][k * ND + l] = f * (coul - exch);
                     }
-        double gA[3], gB[3], gC[3];
-        grad_quartet_bra(P, a, b, c, d, G, gA, gB);
-        grad_quartet_ket(P, a, b, c, d, G, gC);
-        const int at[4] = {P.shell_atom[a], P.shell_atom[b], P.shell_atom[c], P.shell_atom[d]};
+        double cA[3], cB[3], cC[3], cD[3];
+#pragma unroll
         for (int x = 0; x < 3; ++x) {
-            atomicAdd(P.grad + 3 * at[0] + x, gA[x]);
-            atomicAdd(P.grad + 3 * at[1] + x, gB[x]);
-            atomicAdd(P.grad + 3 * at[2] + x, gC[x]);
-            atomicAdd(P.grad + 3 * at[3] + x, -(gA[x] + gB[x] + gC[x]));
+            cA[x] = P.sh.xyz[3 * a + x];
+            cB[x] = P.sh.xyz[3 * b + x];
+            cC[x] = P.sh.xyz[3 * c + x];
+            cD[x] = P.sh.xyz[3 * d + x];
         }
-    }
-}
-
-// One-electron gradient: one thread per shell pair (i >= j).  S and T are
-// two-centre (d/dB = -d/dA); V is summed over nuclei with d/dC = -(d/dA + d/dB).
-__global__ void k_grad_onee(const dftk_shells_t sh, const int *shell_atom, int n_atoms, const double *atom_xyz,
-                            const double *atom_z, const double *D, const double *W, double *grad)
-{
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long npair = (long long)sh.n_shells * (sh.n_shells + 1) / 2;
-    if (t >= npair) return;
-    int i = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
-    while ((long long)i * (i + 1) / 2 > t) --i;
-    while ((long long)(i + 1) * (i + 2) / 2 <= t) ++i;
-    const int j = (int)(t - (long long)i * (i + 1) / 2);
-    const int la = sh.l[i], lb = sh.l[j];
-    if (la > 1 || lb > 1 || la < 0 || lb < 0) return;
-    const int na = g_ncomp(la), nb = g_ncomp(lb);
-    const int N = sh.n_ao;
-    const double fpair = (i == j) ? 1.0 : 2.0;
-    const double *A = sh.xyz + 3 * i, *B = sh.xyz + 3 * j;
-    double gA[3] = {0, 0, 0}, gB[3] = {0, 0, 0};
-    for (int ia = 0; ia < sh.nprim[i]; ++ia)
-        for (int ib = 0; ib < sh.nprim[j]; ++ib) {
-            const double al = sh.prim_exp[sh.prim_off[i] + ia], be = sh.prim_exp[sh.prim_off[j] + ib];
-            const double w = sh.prim_cn[sh.prim_off[i] + ia] * sh.prim_cn[sh.prim_off[j] + ib];
-            const double p = al + be;
-            const double sq = sqrt(DFTK_PI / p);
-            double Pc[3];
-            double S1[3][3][4], Eh[3][45];  // 1-D overlaps S(i <= 2, j <= 3); Hermite E (i, j <= 2)
-            for (int x = 0; x < 3; ++x) {
-                Pc[x] = (al * A[x] + be * B[x]) / p;
-                for (int pi = 0; pi <= 2; ++pi)
-                    for (int pj = 0; pj <= 3; ++pj) {
-                        double e[16];
-                        herm_E1d(al, be, A[x], B[x], pi, pj, e);
-                        S1[x][pi][pj] = e[0] * sq;
-                    }
-                g_E_table(al, be, A[x], B[x], Eh[x]);
-            }
-            // 1-D kinetic T(i, j) = b(2j+1) S(i,j) - 2b^2 S(i,j+2) - j(j-1)/2 S(i,j-2), j <= 1
-            auto T1 = [&](int x, int pi, int pj) {
-                double v = be * (2 * pj + 1) * S1[x][pi][pj] - 2.0 * be * be * S1[x][pi][pj + 2];
-                if (pj >= 2) v -= 0.5 * pj * (pj - 1) * S1[x][pi][pj - 2];
-                return v;
-            };
-            for (int ka = 0; ka < na; ++ka)
-                for (int kb = 0; kb < nb; ++kb) {
-                    int pa[3], pb[3];
-                    g_pow(la, ka, pa);
-                    g_pow(lb, kb, pb);
-                    const long long mu = sh.ao[i] + ka, nu = sh.ao[j] + kb;
-                    const double Dm = fpair * w * D[mu * N + nu], Wm = fpair * w * W[mu * N + nu];
-                    double Sx[3], Tx[3];
-                    for (int x = 0; x < 3; ++x) {
-                        Sx[x] = S1[x][pa[x]][pb[x]];
-                        Tx[x] = T1(x, pa[x], pb[x]);
-                    }
-                    for (int dir = 0; dir < 3; ++dir) {
-                        const int ii = pa[dir], jj = pb[dir];
-                        const double dS = 2.0 * al * S1[dir][ii + 1][jj] - (ii > 0 ? ii * S1[dir][ii - 1][jj] : 0.0);
-                        const double dT = 2.0 * al * T1(dir, ii + 1, jj) - (ii > 0 ? ii * T1(dir, ii - 1, jj) : 0.0);
-                        const int o1 = (dir + 1) % 3, o2 = (dir + 2) % 3;
-                        const double dSfull = dS * Sx[o1] * Sx[o2];
-                        const double dTfull = dT * Sx[o1] * Sx[o2] + dS * (Tx[o1] * Sx[o2] + Sx[o1] * Tx[o2]);
-                        gA[dir] += Dm * dTfull - Wm * dSfull;
-                        gB[dir] -= Dm * dTfull - Wm * dSfull;
-                    }
-                    const int L = la + lb + 1;
-                    for (int cnuc = 0; cnuc < n_atoms; ++cnuc) {
-                        double R[(GRAD_LMAX + 1) * (GRAD_LMAX + 1) * (GRAD_LMAX + 1)];
-                        herm_R<GRAD_LMAX>(L, p, Pc[0] - atom_xyz[3 * cnuc], Pc[1] - atom_xyz[3 * cnuc + 1],
-                                          Pc[2] - atom_xyz[3 * cnuc + 2], R);
-                        const double pref = -2.0 * DFTK_PI / p * atom_z[cnuc] * Dm;
-                        double dA[3], dB[3];
-                        for (int dir = 0; dir < 3; ++dir)
-                            for (int side = 0; side < 2; ++side) {
-                                double s = 0.0;
-                                for (int tx = 0; tx <= L; ++tx)
-                                    for (int ty = 0; ty + tx <= L; ++ty)
-                                        for (int tz = 0; tz + ty + tx <= L; ++tz) {
-                                            const int tt[3] = {tx, ty, tz};
-                                            double e = 1.0;
-                                            for (int x = 0; x < 3 && e != 0.0; ++x) {
-                                                const int ii = pa[x], jj = pb[x];
-                                                double f;
-                                                if (x != dir) {
-                                                    f = Eh[x][(ii * 3 + jj) * 5 + tt[x]];
-                                                } else if (side == 0) {
-                                                    f = 2.0 * al * Eh[x][((ii + 1) * 3 + jj) * 5 + tt[x]];
-                                                    if (ii > 0) f -= ii * Eh[x][((ii - 1) * 3 + jj) * 5 + tt[x]];
-                                                } else {
-                                                    f = 2.0 * be * Eh[x][(ii * 3 + jj + 1) * 5 + tt[x]];
-                                                    if (jj > 0) f -= jj * Eh[x][(ii * 3 + jj - 1) * 5 + tt[x]];
-                                                }
-                                                e *= f;
-                                            }
-                                            s += e * R[RIDX5(tx, ty, tz)];
-                                        }
-                                (side == 0 ? dA : dB)[dir] = pref * s;
-                            }
-                        for (int dir = 0; dir < 3; ++dir) {
-                            gA[dir] += dA[dir];
-                            gB[dir] += dB[dir];
-                            atomicAdd(grad + 3 * cnuc + dir, -(dA[dir] + dB[dir]));
+        double gA[3] = {0.0, 0.0, 0.0}, gB[3] = {0.0, 0.0, 0.0}, gC[3] = {0.0, 0.0, 0.0};
+        const double *brec = P.rec[X] + row;
+        const double *krec = P.rec[Y] + ket;
+        const int nbp = P.nprim[X][row], nkp = P.nprim[Y][ket];
+#pragma unroll 1
+        for (int ip = 0; ip < nbp; ++ip) {
+            const double *br = brec + (long long)ip * nX;
+            const double bP[3] = {__ldg(br), __ldg(br + fsX), __ldg(br + 2 * fsX)};
+            const double bp = __ldg(br + F_P * fsX), bK = __ldg(br + F_K * fsX), bal = __ldg(br + faX * fsX);
+            const double bbe = bp - bal, bh = 0.5 / bp;
+            double Eb[3][LA + 2][LB + 2][LAB + 3];
+#pragma unroll
+            for (int x = 0; x < 3; ++x) g_etab<LA + 1, LB + 1>(bP[x] - cA[x], bP[x] - cB[x], bh, Eb[x]);
+            // Gamma-weighted bra Hermite density
+            double Eg[NM][LAB + 1][LAB + 1][LAB + 1];
+#pragma unroll
+            for (int m = 0; m < NM; ++m)
+#pragma unroll
+                for (int t = 0; t <= LAB; ++t)
+#pragma unroll
+                    for (int u = 0; u <= LAB - t; ++u)
+#pragma unroll
+                        for (int v = 0; v <= LAB - t - u; ++v) {
+                            bool first = true;
+                            double s = 0.0;
+#pragma unroll
+                            for (int ka = 0; ka < NA; ++ka)
+#pragma unroll
+                                for (int kb = 0; kb < NB; ++kb) {
+                                    const int ax = g_cp(LA, ka, 0), ay = g_cp(LA, ka, 1), az = g_cp(LA, ka, 2);
+                                    const int bx = g_cp(LB, kb, 0), by = g_cp(LB, kb, 1), bz = g_cp(LB, kb, 2);
+                                    if (t <= ax + bx && u <= ay + by && v <= az + bz) {
+                                        const double e = Eb[0][ax][bx][t] * Eb[1][ay][by][u] * Eb[2][az][bz][v];
+                                        s = first ? Gm[ka * NB + kb][m] * e : fma(Gm[ka * NB + kb][m], e, s);
+                                        first = false;
+                                    }
+                                }
+                            Eg[m][t][u][v] = s;
                         }
+            double H[NN][LAB + 2][LAB + 2][LAB + 2];
+#pragma unroll
+            for (int n = 0; n < NN; ++n)
+#pragma unroll
+                for (int t = 0; t <= LAB + 1; ++t)
+#pragma unroll
+                    for (int u = 0; u <= LAB + 1 - t; ++u)
+#pragma unroll
+                        for (int v = 0; v <= LAB + 1 - t - u; ++v) H[n][t][u][v] = 0.0;
+#pragma unroll 1
+            for (int jp = 0; jp < nkp; ++jp) {
+                const double *kr = krec + (long long)jp * nY;
+                const double kP[3] = {__ldg(kr), __ldg(kr + fsY), __ldg(kr + 2 * fsY)};
+                const double kp = __ldg(kr + F_P * fsY), kK = __ldg(kr + F_K * fsY), kal = __ldg(kr + faY * fsY);
+                const double kh = 0.5 / kp;
+                double Ek[3][LC + 2][LD + 1][LCD + 2];
+#pragma unroll
+                for (int x = 0; x < 3; ++x) g_etab<LC + 1, LD>(kP[x] - cC[x], kP[x] - cD[x], kh, Ek[x]);
+                const double s2 = bp + kp;
+                const double rs = Math<double>::rsqrt(s2);
+                const double rho = bp * kp * (rs * rs);
+                const double PQx = bP[0] - kP[0], PQy = bP[1] - kP[1], PQz = bP[2] - kP[2];
+                double F[LM + 1];
+                Boys<double, LM>::eval(rho * (PQx * PQx + PQy * PQy + PQz * PQz), F);
+                double R[LM + 1][LM + 1][LM + 1];
+                g_rcube<LM>(PQx, PQy, PQz, -2.0 * rho, bK * kK * rs, F, R);
+                // bra side: H[n][T] += sum_T' Gk[T'] R[T + T']
+#pragma unroll
+                for (int ka = 0; ka < NA; ++ka)
+#pragma unroll
+                    for (int kb = 0; kb < NB; ++kb) {
+                        const int n = ka * NB + kb;
+                        double Gk[LCD + 1][LCD + 1][LCD + 1];
+#pragma unroll
+                        for (int t = 0; t <= LCD; ++t)
+#pragma unroll
+                            for (int u = 0; u <= LCD - t; ++u)
+#pragma unroll
+                                for (int v = 0; v <= LCD - t - u; ++v) {
+                                    bool first = true;
+                                    double s = 0.0;
+#pragma unroll
+                                    for (int kc = 0; kc < NC; ++kc)
+#pragma unroll
+                                        for (int kd = 0; kd < ND; ++kd) {
+                                            const int cx = g_cp(LC, kc, 0), cy = g_cp(LC, kc, 1), cz = g_cp(LC, kc, 2);
+                                            const int dx = g_cp(LD, kd, 0), dy = g_cp(LD, kd, 1), dz = g_cp(LD, kd, 2);
+                                            if (t <= cx + dx && u <= cy + dy && v <= cz + dz) {
+                                                double e = Ek[0][cx][dx][t] * Ek[1][cy][dy][u] * Ek[2][cz][dz][v];
+                                                if ((t + u + v) & 1) e = -e;
+                                                s = first ? Gm[n][kc * ND + kd] * e : fma(Gm[n][kc * ND + kd], e, s);
+                                                first = false;
+                                            }
+                                        }
+                                    Gk[t][u][v] = s;
+                                }
+                        const int sx = g_cp(LA, ka, 0) + g_cp(LB, kb, 0), sy = g_cp(LA, ka, 1) + g_cp(LB, kb, 1),
+                                  sz = g_cp(LA, ka, 2) + g_cp(LB, kb, 2);
+#pragma unroll
+                        for (int t = 0; t <= sx + 1; ++t)
+#pragma unroll
+                            for (int u = 0; u <= sy + 1; ++u)
+#pragma unroll
+                                for (int v = 0; v <= sz + 1; ++v) {
+                                    if (t + u + v > sx + sy + sz + 1) continue;
+                                    double acc = H[n][t][u][v];
+#pragma unroll
+                                    for (int t2 = 0; t2 <= LCD; ++t2)
+#pragma unroll
+                                        for (int u2 = 0; u2 <= LCD - t2; ++u2)
+#pragma unroll
+                                            for (int v2 = 0; v2 <= LCD - t2 - u2; ++v2)
+                                                acc = fma(Gk[t2][u2][v2], R[t + t2][u + u2][v + v2], acc);
+                                    H[n][t][u][v] = acc;
+                                }
                     }
+                // ket side: dE/dC
+#pragma unroll
+                for (int kc = 0; kc < NC; ++kc)
+#pragma unroll
+                    for (int kd = 0; kd < ND; ++kd) {
+                        const int m = kc * ND + kd;
+                        const int cx = g_cp(LC, kc, 0), cy = g_cp(LC, kc, 1), cz = g_cp(LC, kc, 2);
+                        const int dx = g_cp(LD, kd, 0), dy = g_cp(LD, kd, 1), dz = g_cp(LD, kd, 2);
+                        const int c3[3] = {cx, cy, cz}, d3[3] = {dx, dy, dz};
+#pragma unroll
+                        for (int t = 0; t <= cx + dx + 1; ++t)
+#pragma unroll
+                            for (int u = 0; u <= cy + dy + 1; ++u)
+#pragma unroll
+                                for (int v = 0; v <= cz + dz + 1; ++v) {
+                                    if (t + u + v > cx + dx + cy + dy + cz + dz + 1) continue;
+                                    double hc = 0.0;
+                                    bool first = true;
+#pragma unroll
+                                    for (int t1 = 0; t1 <= LAB; ++t1)
+#pragma unroll
+                                        for (int u1 = 0; u1 <= LAB - t1; ++u1)
+#pragma unroll
+                                            for (int v1 = 0; v1 <= LAB - t1 - u1; ++v1) {
+                                                hc = first ? Eg[m][t1][u1][v1] * R[t + t1][u + u1][v + v1]
+                                                           : fma(Eg[m][t1][u1][v1], R[t + t1][u + u1][v + v1], hc);
+                                                first = false;
+                                            }
+                                    if ((t + u + v) & 1) hc = -hc;
+                                    const int tt[3] = {t, u, v};
+#pragma unroll
+                                    for (int dir = 0; dir < 3; ++dir) {
+                                        double e = 1.0;
+                                        bool zero = false;
+#pragma unroll
+                                        for (int x = 0; x < 3; ++x) {
+                                            const int i = c3[x], j = d3[x], tx = tt[x];
+                                            if (x != dir) {
+                                                if (tx > i + j) zero = true;
+                                                else e *= Ek[x][i][j][tx];
+                                            } else {
+                                                double fd = tx <= i + j + 1 ? 2.0 * kal * Ek[x][i + 1][j][tx] : 0.0;
+                                                if (i > 0 && tx <= i + j - 1) fd = fma(-(double)i, Ek[x][i - 1][j][tx], fd);
+                                                e *= fd;
+                                            }
+                                        }
+                                        if (!zero) gC[dir] = fma(e, hc, gC[dir]);
+                                    }
+                                }
+                    }
+            }
+            // dE/dA and dE/dB from the bra intermediates
+#pragma unroll
+            for (int ka = 0; ka < NA; ++ka)
+#pragma unroll
+                for (int kb = 0; kb < NB; ++kb) {
+                    const int n = ka * NB + kb;
+                    const int a3[3] = {g_cp(LA, ka, 0), g_cp(LA, ka, 1), g_cp(LA, ka, 2)};
+                    const int b3[3] = {g_cp(LB, kb, 0), g_cp(LB, kb, 1), g_cp(LB, kb, 2)};
+#pragma unroll
+                    for (int t = 0; t <= a3[0] + b3[0] + 1; ++t)
+#pragma unroll
+                        for (int u = 0; u <= a3[1] + b3[1] + 1; ++u)
+#pragma unroll
+                            for (int v = 0; v <= a3[2] + b3[2] + 1; ++v) {
+                                if (t + u + v > a3[0] + b3[0] + a3[1] + b3[1] + a3[2] + b3[2] + 1) continue;
+                                const int tt[3] = {t, u, v};
+                                const double h = H[n][t][u][v];
+#pragma unroll
+                                for (int dir = 0; dir < 3; ++dir) {
+                                    double ea = 1.0, eb = 1.0;
+                                    bool zero = false;
+#pragma unroll
+                                    for (int x = 0; x < 3; ++x) {
+                                        const int i = a3[x], j = b3[x], tx = tt[x];
+                                        if (x != dir) {
+                                            if (tx > i + j) zero = true;
+                                            else {
+                                                ea *= Eb[x][i][j][tx];
+                                                eb *= Eb[x][i][j][tx];
+                                            }
+                                        } else {
+                                            double fa = 2.0 * bal * Eb[x][i + 1][j][tx];
+                                            if (i > 0 && tx <= i + j - 1) fa = fma(-(double)i, Eb[x][i - 1][j][tx], fa);
+                                            double fb = 2.0 * bbe * Eb[x][i][j + 1][tx];
+                                            if (j > 0 && tx <= i + j - 1) fb = fma(-(double)j, Eb[x][i][j - 1][tx], fb);
+                                            ea *= fa;
+                                            eb *= fb;
+                                        }
+                                    }
+                                    if (!zero) {
+                                        gA[dir] = fma(ea, h, gA[dir]);
+                                        gB[dir] = fma(eb, h, gB[dir]);
+                                    }
+                                }
+                            }
                 }
         }
-    for (int dir = 0; dir < 3; ++dir) {
-        atomicAdd(grad + 3 * shell_atom[i] + dir, gA[dir]);
-        atomicAdd(grad + 3 * shell_atom[j] + dir, gB[dir]);
+        const int at[4] = {P.shell_atom[a], P.shell_atom[b], P.shell_atom[c], P.shell_atom[d]};
+#pragma unroll
+        for (int x = 0; x < 3; ++x) {
+            g_add(sg, P.grad, 3 * at[0] + x, gA[x]);
+            g_add(sg, P.grad, 3 * at[1] + x, gB[x]);
+            g_add(sg, P.grad, 3 * at[2] + x, gC[x]);
+            g_add(sg, P.grad, 3 * at[3] + x, -(gA[x] + gB[x] + gC[x]));
+        }
     }
+    g_smem_end(sg, P.grad, 3 * P.n_atoms);
+}
+
+// Nuclear-attraction gradient of pair class PC: one thread per (shell pair,
+// nucleus), nucleus fastest.  Per primitive pair,
+//   V_n = -2 pi / p Z K_ab sum_T E^n_T R_T(p, P - C)
+// with d/dA, d/dB from exponent-shifted E and d/dC_x = -sum_T E^n_T R_{T + 1_x}.
+// Both orientations of an off-diagonal shell pair are counted (factor 2).
+template <int PC>
+__global__ void __launch_bounds__(GRAD_THREADS) k_grad_nuclear(const dftk_shells_t sh, const int *ab, int n_pairs,
+                                                              const int *shell_atom, int n_atoms,
+                                                              const double *atom_xyz, const double *atom_z,
+                                                              const double *D, double *grad)
+{
+    constexpr int LA = PC == 0 ? 0 : 1, LB = PC == 2 ? 1 : 0;
+    constexpr int NA = LA ? 3 : 1, NB = LB ? 3 : 1;
+    constexpr int LM = LA + LB + 1;
+    extern __shared__ double s_grad[];
+    double *sg = n_atoms <= GRAD_SMEM_ATOMS ? s_grad : nullptr;
+    g_smem_begin(sg, 3 * n_atoms);
+    const long long total = (long long)n_pairs * n_atoms;
+    const long long N = sh.n_ao;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int pair = (int)(t / n_atoms), cn = (int)(t % n_atoms);
+        const int a = ab[2 * pair], b = ab[2 * pair + 1];
+        const double cA[3] = {sh.xyz[3 * a], sh.xyz[3 * a + 1], sh.xyz[3 * a + 2]};
+        const double cB[3] = {sh.xyz[3 * b], sh.xyz[3 * b + 1], sh.xyz[3 * b + 2]};
+        const double cC[3] = {atom_xyz[3 * cn], atom_xyz[3 * cn + 1], atom_xyz[3 * cn + 2]};
+        const double fpair = (a == b) ? 1.0 : 2.0;
+        double Dm[NA][NB];
+#pragma unroll
+        for (int i = 0; i < NA; ++i)
+#pragma unroll
+            for (int j = 0; j < NB; ++j) Dm[i][j] = fpair * D[(long long)(sh.ao[a] + i) * N + sh.ao[b] + j];
+        const double ab2 = (cA[0] - cB[0]) * (cA[0] - cB[0]) + (cA[1] - cB[1]) * (cA[1] - cB[1]) +
+                           (cA[2] - cB[2]) * (cA[2] - cB[2]);
+        double gA[3] = {0.0, 0.0, 0.0}, gB[3] = {0.0, 0.0, 0.0}, gC[3] = {0.0, 0.0, 0.0};
+        for (int ia = 0; ia < sh.nprim[a]; ++ia)
+            for (int ib = 0; ib < sh.nprim[b]; ++ib) {
+                const double al = sh.prim_exp[sh.prim_off[a] + ia], be = sh.prim_exp[sh.prim_off[b] + ib];
+                const double p = al + be, ip = 1.0 / p;
+                const double pre = -2.0 * DFTK_PI * ip * atom_z[cn] * sh.prim_cn[sh.prim_off[a] + ia] *
+                                   sh.prim_cn[sh.prim_off[b] + ib] * exp(-al * be * ip * ab2);
+                double Pc[3], E[3][LA + 2][LB + 2][LA + LB + 3];
+#pragma unroll
+                for (int x = 0; x < 3; ++x) {
+                    Pc[x] = (al * cA[x] + be * cB[x]) * ip;
+                    g_etab<LA + 1, LB + 1>(Pc[x] - cA[x], Pc[x] - cB[x], 0.5 * ip, E[x]);
+                }
+                const double X = Pc[0] - cC[0], Y = Pc[1] - cC[1], Z = Pc[2] - cC[2];
+                double F[LM + 1];
+                Boys<double, LM>::eval(p * (X * X + Y * Y + Z * Z), F);
+                double R[LM + 1][LM + 1][LM + 1];
+                g_rcube<LM>(X, Y, Z, -2.0 * p, pre, F, R);
+#pragma unroll
+                for (int ka = 0; ka < NA; ++ka)
+#pragma unroll
+                    for (int kb = 0; kb < NB; ++kb) {
+                        const int a3[3] = {g_cp(LA, ka, 0), g_cp(LA, ka, 1), g_cp(LA, ka, 2)};
+                        const int b3[3] = {g_cp(LB, kb, 0), g_cp(LB, kb, 1), g_cp(LB, kb, 2)};
+                        const double dm = Dm[ka][kb];
+#pragma unroll
+                        for (int t = 0; t <= a3[0] + b3[0] + 1; ++t)
+#pragma unroll
+                            for (int u = 0; u <= a3[1] + b3[1] + 1; ++u)
+#pragma unroll
+                                for (int v = 0; v <= a3[2] + b3[2] + 1; ++v) {
+                                    if (t + u + v > a3[0] + b3[0] + a3[1] + b3[1] + a3[2] + b3[2] + 1) continue;
+                                    const int tt[3] = {t, u, v};
+                                    const double r = dm * R[t][u][v];
+#pragma unroll
+                                    for (int dir = 0; dir < 3; ++dir) {
+                                        double ea = 1.0, eb = 1.0;
+                                        bool zero = false;
+#pragma unroll
+                                        for (int x = 0; x < 3; ++x) {
+                                            const int i = a3[x], j = b3[x], tx = tt[x];
+                                            if (x != dir) {
+                                                if (tx > i + j) zero = true;
+                                                else {
+                                                    ea *= E[x][i][j][tx];
+                                                    eb *= E[x][i][j][tx];
+                                                }
+                                            } else {
+                                                double fa = 2.0 * al * E[x][i + 1][j][tx];
+                                                if (i > 0 && tx <= i + j - 1) fa = fma(-(double)i, E[x][i - 1][j][tx], fa);
+                                                double fb = 2.0 * be * E[x][i][j + 1][tx];
+                                                if (j > 0 && tx <= i + j - 1) fb = fma(-(double)j, E[x][i][j - 1][tx], fb);
+                                                ea *= fa;
+                                                eb *= fb;
+                                            }
+                                        }
+                                        if (!zero) {
+                                            gA[dir] = fma(ea, r, gA[dir]);
+                                            gB[dir] = fma(eb, r, gB[dir]);
+                                        }
+                                    }
+                                    // operator centre: -E^n_T R_{T + 1_dir}
+                                    if (t <= a3[0] + b3[0] && u <= a3[1] + b3[1] && v <= a3[2] + b3[2]) {
+                                        const double e = E[0][a3[0]][b3[0]][t] * E[1][a3[1]][b3[1]][u] *
+                                                         E[2][a3[2]][b3[2]][v] * dm;
+                                        gC[0] = fma(-e, R[t + 1][u][v], gC[0]);
+                                        gC[1] = fma(-e, R[t][u + 1][v], gC[1]);
+                                        gC[2] = fma(-e, R[t][u][v + 1], gC[2]);
+                                    }
+                                }
+                    }
+            }
+        const int atA = shell_atom[a], atB = shell_atom[b];
+#pragma unroll
+        for (int x = 0; x < 3; ++x) {
+            g_add(sg, grad, 3 * atA + x, gA[x]);
+            g_add(sg, grad, 3 * atB + x, gB[x]);
+            g_add(sg, grad, 3 * cn + x, gC[x]);
+        }
+    }
+    g_smem_end(sg, grad, 3 * n_atoms);
+}
+
+// Overlap and kinetic gradient of pair class PC: one thread per shell pair.
+// S and T depend on A - B only, so d/dB = -d/dA.  1-D overlaps
+// S_ij = E^{ij}_0 sqrt(pi / p) and the 1-D kinetic
+// T_ij = b (2j+1) S_ij - 2 b^2 S_{i,j+2} - j (j-1)/2 S_{i,j-2}.
+template <int PC>
+__global__ void __launch_bounds__(GRAD_THREADS) k_grad_overlap_kinetic(const dftk_shells_t sh, const int *ab,
+                                                                      int n_pairs, const int *shell_atom,
+                                                                      int n_atoms, const double *D,
+                                                                      const double *W, double *grad)
+{
+    constexpr int LA = PC == 0 ? 0 : 1, LB = PC == 2 ? 1 : 0;
+    constexpr int NA = LA ? 3 : 1, NB = LB ? 3 : 1;
+    extern __shared__ double s_grad[];
+    double *sg = n_atoms <= GRAD_SMEM_ATOMS ? s_grad : nullptr;
+    g_smem_begin(sg, 3 * n_atoms);
+    const long long N = sh.n_ao;
+    for (int pair = blockIdx.x * blockDim.x + threadIdx.x; pair < n_pairs; pair += gridDim.x * blockDim.x) {
+        const int a = ab[2 * pair], b = ab[2 * pair + 1];
+        const double cA[3] = {sh.xyz[3 * a], sh.xyz[3 * a + 1], sh.xyz[3 * a + 2]};
+        const double cB[3] = {sh.xyz[3 * b], sh.xyz[3 * b + 1], sh.xyz[3 * b + 2]};
+        const double fpair = (a == b) ? 1.0 : 2.0;
+        const double ab2 = (cA[0] - cB[0]) * (cA[0] - cB[0]) + (cA[1] - cB[1]) * (cA[1] - cB[1]) +
+                           (cA[2] - cB[2]) * (cA[2] - cB[2]);
+        double gA[3] = {0.0, 0.0, 0.0};
+        for (int ia = 0; ia < sh.nprim[a]; ++ia)
+            for (int ib = 0; ib < sh.nprim[b]; ++ib) {
+                const double al = sh.prim_exp[sh.prim_off[a] + ia], be = sh.prim_exp[sh.prim_off[b] + ib];
+                const double p = al + be, ip = 1.0 / p;
+                const double w = sh.prim_cn[sh.prim_off[a] + ia] * sh.prim_cn[sh.prim_off[b] + ib] *
+                                 exp(-al * be * ip * ab2) * DFTK_PI * ip * sqrt(DFTK_PI * ip);
+                // S1[x][i][j] = E^{ij}_0 for i <= LA + 1, j <= LB + 3
+                double E[3][LA + 2][LB + 4][LA + LB + 5];
+                double Pc[3];
+#pragma unroll
+                for (int x = 0; x < 3; ++x) {
+                    Pc[x] = (al * cA[x] + be * cB[x]) * ip;
+                    g_etab<LA + 1, LB + 3>(Pc[x] - cA[x], Pc[x] - cB[x], 0.5 * ip, E[x]);
+                }
+#pragma unroll
+                for (int ka = 0; ka < NA; ++ka)
+#pragma unroll
+                    for (int kb = 0; kb < NB; ++kb) {
+                        const int a3[3] = {g_cp(LA, ka, 0), g_cp(LA, ka, 1), g_cp(LA, ka, 2)};
+                        const int b3[3] = {g_cp(LB, kb, 0), g_cp(LB, kb, 1), g_cp(LB, kb, 2)};
+                        const long long mu = sh.ao[a] + ka, nu = sh.ao[b] + kb;
+                        const double dm = fpair * w * D[mu * N + nu], wm = fpair * w * W[mu * N + nu];
+                        double S[3][3], T[3][3];  // [axis][i = a - 1 .. a + 1 -> 0..2] at j = b
+#pragma unroll
+                        for (int x = 0; x < 3; ++x)
+#pragma unroll
+                            for (int di = -1; di <= 1; ++di) {
+                                const int i = a3[x] + di, j = b3[x];
+                                if (i < 0) {
+                                    S[x][di + 1] = 0.0;
+                                    T[x][di + 1] = 0.0;
+                                    continue;
+                                }
+                                const double s = E[x][i][j][0];
+                                double tk = be * (2 * j + 1) * s - 2.0 * be * be * E[x][i][j + 2][0];
+                                if (j >= 2) tk -= 0.5 * j * (j - 1) * E[x][i][j - 2][0];
+                                S[x][di + 1] = s;
+                                T[x][di + 1] = tk;
+                            }
+#pragma unroll
+                        for (int dir = 0; dir < 3; ++dir) {
+                            const int o1 = (dir + 1) % 3, o2 = (dir + 2) % 3;
+                            const int i = a3[dir];
+                            double dS = 2.0 * al * S[dir][2], dT = 2.0 * al * T[dir][2];
+                            if (i > 0) {
+                                dS -= i * S[dir][0];
+                                dT -= i * T[dir][0];
+                            }
+                            const double dSf = dS * S[o1][1] * S[o2][1];
+                            const double dTf = dT * S[o1][1] * S[o2][1] + dS * (T[o1][1] * S[o2][1] + S[o1][1] * T[o2][1]);
+                            gA[dir] += dm * dTf - wm * dSf;
+                        }
+                    }
+            }
+        const int atA = shell_atom[a], atB = shell_atom[b];
+#pragma unroll
+        for (int x = 0; x < 3; ++x) {
+            g_add(sg, grad, 3 * atA + x, gA[x]);
+            g_add(sg, grad, 3 * atB + x, -gA[x]);
+        }
+    }
+    g_smem_end(sg, grad, 3 * n_atoms);
 }

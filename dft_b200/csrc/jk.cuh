@@ -19,9 +19,9 @@ __global__ void k_pair_data(const dftk_shells_t sh, const dftk_pairs_t pr, int n
     const int a = pr.ab[2 * pair], b = pr.ab[2 * pair + 1];
     const int na = sh.nprim[a], nb = sh.nprim[b];
     if (k == 0) pr.nprim[pair] = na * nb;
-    double f[12];
+    double f[13];
 #pragma unroll
-    for (int i = 0; i < 12; ++i) f[i] = 0.0;
+    for (int i = 0; i < 13; ++i) f[i] = 0.0;
     if (k < na * nb) {
         const int ia = k / nb, ib = k % nb;
         const double al = sh.prim_exp[sh.prim_off[a] + ia];
@@ -41,6 +41,7 @@ __global__ void k_pair_data(const dftk_shells_t sh, const dftk_pairs_t pr, int n
         f[F_H] = 0.5 * ip;
         f[F_AX] = Px - Ax; f[F_AY] = Py - Ay; f[F_AZ] = Pz - Az;
         f[F_BX] = Px - Bx; f[F_BY] = Py - By; f[F_BZ] = Pz - Bz;
+        f[nfields - 1] = al;  // overwrites nothing the class reads (alpha field is last)
     }
     for (int i = 0; i < nfields; ++i) {
         const long long o = ((long long)i * pr.kmax + k) * n + pair;

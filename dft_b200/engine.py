@@ -28,7 +28,7 @@ from . import _lib, basis as _basis
 QCLASS_OF = {(0, 0): 0, (1, 0): 1, (1, 1): 2, (2, 0): 3, (2, 1): 4, (2, 2): 5}
 QCLASS_PAIRS = [(0, 0), (1, 0), (1, 1), (2, 0), (2, 1), (2, 2)]
 QCLASS_NAMES = ["(ss|ss)", "(ps|ss)", "(ps|ps)", "(pp|ss)", "(pp|ps)", "(pp|pp)"]
-PAIR_FIELDS = {0: 5, 1: 9, 2: 12}
+PAIR_FIELDS = {0: 6, 1: 10, 2: 13}  # stored record fields per pair class (ERI fields + alpha)
 # Fixed flop accounting per evaluated primitive quartet, by class (ss|ss)..(pp|pp):
 # 2 x (R-recursion FMAs + ket Hermite contraction + bra contraction) + 40 + 3L.
 FLOPS_PER_PRIM_QUARTET = [44, 66, 145, 147, 410, 1402]

@@ -66,7 +66,8 @@ typedef struct {
 
 /* Shell pairs of one pair class (0 ss, 1 ps, 2 pp) with l_a >= l_b, and their
  * primitive-pair records in SoA layout rec[(field * kmax + k) * n_pairs + pair]
- * (fields: P x/y/z, p, K, 1/(2p), PA x/y/z, PB x/y/z; ss uses 5, ps 9, pp 12). */
+ * (fields: P x/y/z, p, K, 1/(2p), PA x/y/z, PB x/y/z, of which ss uses 5, ps 9,
+ * pp 12, followed by the bra exponent alpha: 6 / 10 / 13 fields stored). */
 typedef struct {
     int n_pairs;
     int kmax;               /* primitive-pair slots per pair (max nprim_a * nprim_b) */
