@@ -501,10 +501,13 @@ int dftk_grad(const dftk_shells_t *shells, const int *shell_atom, int n_atoms, c
         !W || !grad || !workspace)
         return fail(DFTK_ERR_ARG, "dftk_grad: null argument");
     const int ns = shells->n_shells, N = shells->n_ao;
-    if (workspace_bytes < (size_t)ns * ns * sizeof(float)) return fail(DFTK_ERR_WORKSPACE, "dftk_grad: workspace too small");
+    if (workspace_bytes < ws_bytes(ns, N)) return fail(DFTK_ERR_WORKSPACE, "dftk_grad: workspace too small");
     DFTK_INIT();
     cudaStream_t s = (cudaStream_t)stream;
-    float *Dsh = (float *)workspace;
+    // same workspace layout as dftk_jk: Dsh after three N x N blocks, then
+    // the selection heads and lists when the workspace holds them
+    float *Dsh = (float *)((double *)workspace + 3 * (size_t)N * N);
+    const bool use_list = workspace_bytes >= ws_list_bytes(ns, N, queue);
     DFTK_CUDA(cudaMemsetAsync(grad, 0, 3 * sizeof(double) * n_atoms, s));
     if (ns == 0) return DFTK_OK;
     // block-private gradient copies in shared memory when they fit
@@ -516,6 +519,12 @@ int dftk_grad(const dftk_shells_t *shells, const int *shell_atom, int n_atoms, c
     };
     k_dsh<<<blocks_for((long long)ns * ns, 128), 128, 0, s>>>(shells->ao, shells->l, ns, N, D, D_a, D_b, 1, Dsh);
     DFTK_LAUNCHED("k_dsh");
+    // with dftk_jk_timing on: slots 0..5 time the class kernels, slot 6 the one-electron part
+    const bool timed = g_timing.enabled;
+    if (timed) {
+        for (int k = 0; k < 2 * DFTK_N_QCLASS; ++k) g_timing.launched[k] = false;
+        DFTK_CUDA(cudaEventRecord(g_timing.start[DFTK_N_QCLASS], s));
+    }
 #define DFTK_GRAD_ONEE(PC)                                                                                   \
     if (pairs[PC].n_pairs > 0) {                                                                             \
         k_grad_overlap_kinetic<PC><<<grid(pairs[PC].n_pairs), GRAD_THREADS, smem, s>>>(                       \
@@ -529,6 +538,10 @@ int dftk_grad(const dftk_shells_t *shells, const int *shell_atom, int n_atoms, c
     DFTK_GRAD_ONEE(1)
     DFTK_GRAD_ONEE(2)
 #undef DFTK_GRAD_ONEE
+    if (timed) {
+        DFTK_CUDA(cudaEventRecord(g_timing.stop[DFTK_N_QCLASS], s));
+        g_timing.launched[DFTK_N_QCLASS] = true;
+    }
     GradParams P;
     memset(&P, 0, sizeof(P));
     P.sh = *shells;
@@ -556,10 +569,56 @@ int dftk_grad(const dftk_shells_t *shells, const int *shell_atom, int n_atoms, c
     P.ns = ns;
     P.tau = tau;
     P.grad = grad;
+    P.tau_prim = (float)queue->tau_prim;
+    for (int k = 0; k < 3; ++k) P.qp[k] = pairs[k].qp;
+    if (use_list) {
+        // selection pass of dftk_jk with the gradient bound Q_ab Q_cd max|D|^2 >= tau
+        JkParams S;
+        memset(&S, 0, sizeof(S));
+        S.ns = ns;
+        for (int k = 0; k < 3; ++k) {
+            S.ab[k] = pairs[k].ab;
+            S.q[k] = pairs[k].q;
+        }
+        for (int c = 0; c < DFTK_N_QCLASS; ++c) {
+            S.n_rows[c] = P.n_rows[c];
+            S.row_off[c] = P.row_off[c];
+            S.total[c] = P.total[c];
+        }
+        S.Dsh = Dsh;
+        S.tau = tau;
+        S.tau32 = tau;
+        S.dm_pow2 = 1;
+        unsigned char *cur = (unsigned char *)workspace + ws_bytes(ns, N);
+        S.heads = (unsigned long long *)cur;
+        cur += 256;
+        for (int c = 0; c < DFTK_N_QCLASS; ++c) {
+            S.list[c] = (int2 *)cur;
+            if (S.total[c] > 0) cur += (((size_t)S.total[c] * sizeof(int2)) + 255) & ~(size_t)255;
+        }
+        DFTK_CUDA(cudaMemsetAsync(S.heads, 0, 2 * DFTK_N_QCLASS * sizeof(unsigned long long), s));
+        int st;
+        if ((st = launch_select_class<0>(S, s))) return st;
+        if ((st = launch_select_class<1>(S, s))) return st;
+        if ((st = launch_select_class<2>(S, s))) return st;
+        if ((st = launch_select_class<3>(S, s))) return st;
+        if ((st = launch_select_class<4>(S, s))) return st;
+        if ((st = launch_select_class<5>(S, s))) return st;
+        for (int c = 0; c < DFTK_N_QCLASS; ++c) P.list[c] = S.list[c];
+        P.heads = S.heads;
+    }
 #define DFTK_GRAD_LAUNCH(CC)                                                  \
     if (P.total[CC] > 0) {                                                    \
-        k_grad_eri<CC><<<grid(P.total[CC]), GRAD_THREADS, smem, s>>>(P);      \
+        if (timed) DFTK_CUDA(cudaEventRecord(g_timing.start[CC], s));         \
+        if (use_list)                                                         \
+            k_grad_eri<CC, true><<<grid(P.total[CC]), GRAD_THREADS, smem, s>>>(P);  \
+        else                                                                  \
+            k_grad_eri<CC, false><<<grid(P.total[CC]), GRAD_THREADS, smem, s>>>(P); \
         DFTK_LAUNCHED("k_grad_eri");                                          \
+        if (timed) {                                                          \
+            DFTK_CUDA(cudaEventRecord(g_timing.stop[CC], s));                 \
+            g_timing.launched[CC] = true;                                     \
+        }                                                                     \
     }
     DFTK_GRAD_LAUNCH(0)
     DFTK_GRAD_LAUNCH(1)

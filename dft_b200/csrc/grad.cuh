@@ -46,9 +46,14 @@ struct GradParams {
     const long long *row_off[DFTK_N_QCLASS];
     const double *D, *Da, *Db;  // total and spin densities (Da == Db for RHF)
     const float *Dsh;
+    const float *qp[3];  // primitive Schwarz factors, descending per pair
+    float tau_prim;      // primitive quartets with qp_bra qp_ket < tau_prim are skipped
     int N, ns;
     double tau;
     double *grad;  // [n_atoms * 3], accumulated
+    // list path: per class the selected (bra row, ket) entries and their count
+    const int2 *list[DFTK_N_QCLASS];
+    const unsigned long long *heads;
 };
 
 // Quartet classes (ss|ss)..(pp|pp): angular momenta and pair classes.
@@ -170,33 +175,75 @@ __device__ __forceinline__ void g_smem_end(const double *s_grad, double *grad, i
             if (s_grad[i] != 0.0) atomicAdd(grad + i, s_grad[i]);
 }
 
-// Two-electron gradient, class C; quartets with Q_ab Q_cd max|D|^2 < tau are skipped.
+// gA, gB += sum_T dE^n_T(A), dE^n_T(B) V[T] over the derivative region of bra
+// component n = (ka, kb): T in the box s_n + 1 per axis with |T| <= |s_n| + 1.
+template <int LA, int LB>
+__device__ __forceinline__ void g_ab_contract(int ka, int kb, const double (&Eb)[3][LA + 2][LB + 2][LA + LB + 3],
+                                              double al, double be, const double (&V)[LA + LB + 2][LA + LB + 2][LA + LB + 2],
+                                              double *gA, double *gB)
+{
+    const int sx = g_cp(LA, ka, 0) + g_cp(LB, kb, 0), sy = g_cp(LA, ka, 1) + g_cp(LB, kb, 1),
+              sz = g_cp(LA, ka, 2) + g_cp(LB, kb, 2);
+#pragma unroll
+    for (int t = 0; t <= sx + 1; ++t)
+#pragma unroll
+        for (int u = 0; u <= sy + 1; ++u)
+#pragma unroll
+            for (int v = 0; v <= sz + 1; ++v) {
+                if (t + u + v > sx + sy + sz + 1) continue;
+                const double h = V[t][u][v];
+#pragma unroll
+                for (int dir = 0; dir < 3; ++dir) {
+                    double ea = 1.0, eb = 1.0;
+                    bool zero = false;
+#pragma unroll
+                    for (int x = 0; x < 3; ++x) {
+                        const int i = g_cp(LA, ka, x), j = g_cp(LB, kb, x), tx = x == 0 ? t : (x == 1 ? u : v);
+                        if (x != dir) {
+                            if (tx > i + j) zero = true;
+                            else {
+                                ea *= Eb[x][i][j][tx];
+                                eb *= Eb[x][i][j][tx];
+                            }
+                        } else {
+                            double fa = 2.0 * al * Eb[x][i + 1][j][tx];
+                            if (i > 0 && tx <= i + j - 1) fa = fma(-(double)i, Eb[x][i - 1][j][tx], fa);
+                            double fb = 2.0 * be * Eb[x][i][j + 1][tx];
+                            if (j > 0 && tx <= i + j - 1) fb = fma(-(double)j, Eb[x][i][j - 1][tx], fb);
+                            ea *= fa;
+                            eb *= fb;
+                        }
+                    }
+                    if (!zero) {
+                        gA[dir] = fma(ea, h, gA[dir]);
+                        gB[dir] = fma(eb, h, gB[dir]);
+                    }
+                }
+            }
+}
+
+// Two-electron gradient contributions gA, gB, gC of one shell quartet (bra
+// row, ket) of class C (gD = -(gA + gB + gC)).  Classes with an s bra (<= 3
+// bra components) hold H[n][T] across the ket primitives; the pp-bra classes
+// contract each primitive quartet's V[T] with the bra derivative
+// coefficients at once (less register state).  Both sides' primitive pairs
+// come sorted by descending primitive Schwarz factor, and the loops stop once
+// qp_bra qp_ket < tau_prim.
 template <int C>
-__global__ void __launch_bounds__(GRAD_THREADS) k_grad_eri(const GradParams P)
+__device__ __forceinline__ void grad_quartet(const GradParams &P, int row, int ket, double *gA, double *gB,
+                                             double *gC)
 {
     using G = GradClassOf<C>;
     constexpr int LA = G::LA, LB = G::LB, LC = G::LC, LD = G::LD, X = G::X, Y = G::Y;
     constexpr int NA = LA ? 3 : 1, NB = LB ? 3 : 1, NC = LC ? 3 : 1, ND = LD ? 3 : 1;
     constexpr int NN = NA * NB, NM = NC * ND;
     constexpr int LAB = LA + LB, LCD = LC + LD, LM = LAB + LCD + 1;
-    extern __shared__ double s_grad[];
-    double *sg = P.n_atoms <= GRAD_SMEM_ATOMS ? s_grad : nullptr;
-    g_smem_begin(sg, 3 * P.n_atoms);
-    const long long ncand = P.total[C];
-    const long long stride = (long long)gridDim.x * blockDim.x;
     const int nX = P.n_pairs[X], nY = P.n_pairs[Y];
     const long long fsX = (long long)P.kmax * nX, fsY = (long long)P.kmax * nY;
     constexpr int faX = pair_alpha_field(X), faY = pair_alpha_field(Y);
-    for (long long cand = (long long)blockIdx.x * blockDim.x + threadIdx.x; cand < ncand; cand += stride) {
-        const int row = find_row(P.row_off[C], P.n_rows[C], cand);
-        const int ket = (int)(cand - P.row_off[C][row]);
+    {
         const int a = P.ab[X][2 * row], b = P.ab[X][2 * row + 1];
         const int c = P.ab[Y][2 * ket], d = P.ab[Y][2 * ket + 1];
-        const int ns = P.ns;
-        const float dm = fmaxf(fmaxf(P.Dsh[a * ns + b], P.Dsh[c * ns + d]),
-                               fmaxf(fmaxf(P.Dsh[a * ns + c], P.Dsh[a * ns + d]),
-                                     fmaxf(P.Dsh[b * ns + c], P.Dsh[b * ns + d])));
-        if (P.q[X][row] * P.q[Y][ket] * (double)dm * (double)dm < P.tau) continue;
         const long long N = P.N;
         const int oa = P.sh.ao[a], ob = P.sh.ao[b], oc = P.sh.ao[c], od = P.sh.ao[d];
         const int ew = (a == b) + (c == d) + ((X == Y) && (row == ket));
@@ -224,12 +271,17 @@ __global__ void __launch_bounds__(GRAD_THREADS) k_grad_eri(const GradParams P)
             cC[x] = P.sh.xyz[3 * c + x];
             cD[x] = P.sh.xyz[3 * d + x];
         }
-        double gA[3] = {0.0, 0.0, 0.0}, gB[3] = {0.0, 0.0, 0.0}, gC[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int x = 0; x < 3; ++x) gA[x] = gB[x] = gC[x] = 0.0;
         const double *brec = P.rec[X] + row;
         const double *krec = P.rec[Y] + ket;
+        const float *bq = P.qp[X] + row, *kq = P.qp[Y] + ket;
         const int nbp = P.nprim[X][row], nkp = P.nprim[Y][ket];
+        const float kq0 = __ldg(kq);
 #pragma unroll 1
         for (int ip = 0; ip < nbp; ++ip) {
+            const float qb = __ldg(bq + (long long)ip * nX);
+            if (qb * kq0 < P.tau_prim) break;
             const double *br = brec + (long long)ip * nX;
             const double bP[3] = {__ldg(br), __ldg(br + fsX), __ldg(br + 2 * fsX)};
             const double bp = __ldg(br + F_P * fsX), bK = __ldg(br + F_K * fsX), bal = __ldg(br + faX * fsX);
@@ -263,17 +315,22 @@ __global__ void __launch_bounds__(GRAD_THREADS) k_grad_eri(const GradParams P)
                                 }
                             Eg[m][t][u][v] = s;
                         }
-            double H[NN][LAB + 2][LAB + 2][LAB + 2];
+            constexpr bool kHoldH = NN <= 3;
+            constexpr int NH = kHoldH ? NN : 1;
+            double H[NH][LAB + 2][LAB + 2][LAB + 2];
+            if constexpr (kHoldH) {
 #pragma unroll
-            for (int n = 0; n < NN; ++n)
+                for (int n = 0; n < NH; ++n)
 #pragma unroll
-                for (int t = 0; t <= LAB + 1; ++t)
+                    for (int t = 0; t <= LAB + 1; ++t)
 #pragma unroll
-                    for (int u = 0; u <= LAB + 1 - t; ++u)
+                        for (int u = 0; u <= LAB + 1 - t; ++u)
 #pragma unroll
-                        for (int v = 0; v <= LAB + 1 - t - u; ++v) H[n][t][u][v] = 0.0;
+                            for (int v = 0; v <= LAB + 1 - t - u; ++v) H[n][t][u][v] = 0.0;
+            }
 #pragma unroll 1
             for (int jp = 0; jp < nkp; ++jp) {
+                if (qb * __ldg(kq + (long long)jp * nY) < P.tau_prim) break;
                 const double *kr = krec + (long long)jp * nY;
                 const double kP[3] = {__ldg(kr), __ldg(kr + fsY), __ldg(kr + 2 * fsY)};
                 const double kp = __ldg(kr + F_P * fsY), kK = __ldg(kr + F_K * fsY), kal = __ldg(kr + faY * fsY);
@@ -328,7 +385,7 @@ __global__ void __launch_bounds__(GRAD_THREADS) k_grad_eri(const GradParams P)
 #pragma unroll
                                 for (int v = 0; v <= sz + 1; ++v) {
                                     if (t + u + v > sx + sy + sz + 1) continue;
-                                    double acc = H[n][t][u][v];
+                                    double acc = kHoldH ? H[kHoldH ? n : 0][t][u][v] : 0.0;
 #pragma unroll
                                     for (int t2 = 0; t2 <= LCD; ++t2)
 #pragma unroll
@@ -336,8 +393,9 @@ __global__ void __launch_bounds__(GRAD_THREADS) k_grad_eri(const GradParams P)
 #pragma unroll
                                             for (int v2 = 0; v2 <= LCD - t2 - u2; ++v2)
                                                 acc = fma(Gk[t2][u2][v2], R[t + t2][u + u2][v + v2], acc);
-                                    H[n][t][u][v] = acc;
+                                    H[kHoldH ? n : 0][t][u][v] = acc;
                                 }
+                        if constexpr (!kHoldH) g_ab_contract<LA, LB>(ka, kb, Eb, bal, bbe, H[0], gA, gB);
                     }
                 // ket side: dE/dC
 #pragma unroll
@@ -347,7 +405,6 @@ __global__ void __launch_bounds__(GRAD_THREADS) k_grad_eri(const GradParams P)
                         const int m = kc * ND + kd;
                         const int cx = g_cp(LC, kc, 0), cy = g_cp(LC, kc, 1), cz = g_cp(LC, kc, 2);
                         const int dx = g_cp(LD, kd, 0), dy = g_cp(LD, kd, 1), dz = g_cp(LD, kd, 2);
-                        const int c3[3] = {cx, cy, cz}, d3[3] = {dx, dy, dz};
 #pragma unroll
                         for (int t = 0; t <= cx + dx + 1; ++t)
 #pragma unroll
@@ -368,14 +425,13 @@ __global__ void __launch_bounds__(GRAD_THREADS) k_grad_eri(const GradParams P)
                                                 first = false;
                                             }
                                     if ((t + u + v) & 1) hc = -hc;
-                                    const int tt[3] = {t, u, v};
 #pragma unroll
                                     for (int dir = 0; dir < 3; ++dir) {
                                         double e = 1.0;
                                         bool zero = false;
 #pragma unroll
                                         for (int x = 0; x < 3; ++x) {
-                                            const int i = c3[x], j = d3[x], tx = tt[x];
+                                            const int i = g_cp(LC, kc, x), j = g_cp(LD, kd, x), tx = x == 0 ? t : (x == 1 ? u : v);
                                             if (x != dir) {
                                                 if (tx > i + j) zero = true;
                                                 else e *= Ek[x][i][j][tx];
@@ -391,59 +447,105 @@ __global__ void __launch_bounds__(GRAD_THREADS) k_grad_eri(const GradParams P)
                     }
             }
             // dE/dA and dE/dB from the bra intermediates
+            if constexpr (kHoldH) {
 #pragma unroll
-            for (int ka = 0; ka < NA; ++ka)
+                for (int ka = 0; ka < NA; ++ka)
 #pragma unroll
-                for (int kb = 0; kb < NB; ++kb) {
-                    const int n = ka * NB + kb;
-                    const int a3[3] = {g_cp(LA, ka, 0), g_cp(LA, ka, 1), g_cp(LA, ka, 2)};
-                    const int b3[3] = {g_cp(LB, kb, 0), g_cp(LB, kb, 1), g_cp(LB, kb, 2)};
-#pragma unroll
-                    for (int t = 0; t <= a3[0] + b3[0] + 1; ++t)
-#pragma unroll
-                        for (int u = 0; u <= a3[1] + b3[1] + 1; ++u)
-#pragma unroll
-                            for (int v = 0; v <= a3[2] + b3[2] + 1; ++v) {
-                                if (t + u + v > a3[0] + b3[0] + a3[1] + b3[1] + a3[2] + b3[2] + 1) continue;
-                                const int tt[3] = {t, u, v};
-                                const double h = H[n][t][u][v];
-#pragma unroll
-                                for (int dir = 0; dir < 3; ++dir) {
-                                    double ea = 1.0, eb = 1.0;
-                                    bool zero = false;
-#pragma unroll
-                                    for (int x = 0; x < 3; ++x) {
-                                        const int i = a3[x], j = b3[x], tx = tt[x];
-                                        if (x != dir) {
-                                            if (tx > i + j) zero = true;
-                                            else {
-                                                ea *= Eb[x][i][j][tx];
-                                                eb *= Eb[x][i][j][tx];
-                                            }
-                                        } else {
-                                            double fa = 2.0 * bal * Eb[x][i + 1][j][tx];
-                                            if (i > 0 && tx <= i + j - 1) fa = fma(-(double)i, Eb[x][i - 1][j][tx], fa);
-                                            double fb = 2.0 * bbe * Eb[x][i][j + 1][tx];
-                                            if (j > 0 && tx <= i + j - 1) fb = fma(-(double)j, Eb[x][i][j - 1][tx], fb);
-                                            ea *= fa;
-                                            eb *= fb;
-                                        }
-                                    }
-                                    if (!zero) {
-                                        gA[dir] = fma(ea, h, gA[dir]);
-                                        gB[dir] = fma(eb, h, gB[dir]);
-                                    }
-                                }
-                            }
-                }
+                    for (int kb = 0; kb < NB; ++kb) g_ab_contract<LA, LB>(ka, kb, Eb, bal, bbe, H[ka * NB + kb], gA, gB);
+            }
         }
-        const int at[4] = {P.shell_atom[a], P.shell_atom[b], P.shell_atom[c], P.shell_atom[d]};
+    }
+}
+
+// Two-electron gradient of class C over the Schwarz candidates (scan path:
+// quartets with Q_ab Q_cd max|D|^2 < tau are skipped) or over the entries
+// the selection pass kept (list path; warp w takes entries 32w .. 32w + 31,
+// and a warp whose entries share the bra pair sums dE/dA, dE/dB in registers).
+template <int C, bool LIST>
+__global__ void __launch_bounds__(GRAD_THREADS) k_grad_eri(const GradParams P)
+{
+    using G = GradClassOf<C>;
+    constexpr int X = G::X, Y = G::Y;
+    extern __shared__ double s_grad[];
+    double *sg = P.n_atoms <= GRAD_SMEM_ATOMS ? s_grad : nullptr;
+    g_smem_begin(sg, 3 * P.n_atoms);
+    if constexpr (LIST) {
+        const long long n = (long long)P.heads[C];
+        const int2 *list = P.list[C];
+        const long long nwork = (n + 31) >> 5;
+        const int lane = threadIdx.x & 31;
+        const long long wstride = ((long long)gridDim.x * blockDim.x) >> 5;
+        for (long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; gw < nwork; gw += wstride) {
+            const long long idx = gw * 32 + lane;
+            const bool valid = idx < n;
+            int row = 0, ket = 0;
+            if (valid) {
+                const int2 e = __ldg(list + idx);
+                row = e.x;
+                ket = e.y;
+            }
+            double gA[3] = {0.0, 0.0, 0.0}, gB[3] = {0.0, 0.0, 0.0}, gC[3] = {0.0, 0.0, 0.0};
+            if (valid) grad_quartet<C>(P, row, ket, gA, gB, gC);
+            const int row0 = __shfl_sync(DFTK_FULL_MASK, row, 0);  // lane 0 is valid whenever any lane is
+            const bool uniform = __all_sync(DFTK_FULL_MASK, !valid || row == row0);
+            if (valid) {
+                const int c = P.ab[Y][2 * ket], d = P.ab[Y][2 * ket + 1];
+                const int atC = P.shell_atom[c], atD = P.shell_atom[d];
 #pragma unroll
-        for (int x = 0; x < 3; ++x) {
-            g_add(sg, P.grad, 3 * at[0] + x, gA[x]);
-            g_add(sg, P.grad, 3 * at[1] + x, gB[x]);
-            g_add(sg, P.grad, 3 * at[2] + x, gC[x]);
-            g_add(sg, P.grad, 3 * at[3] + x, -(gA[x] + gB[x] + gC[x]));
+                for (int x = 0; x < 3; ++x) {
+                    g_add(sg, P.grad, 3 * atC + x, gC[x]);
+                    g_add(sg, P.grad, 3 * atD + x, -(gA[x] + gB[x] + gC[x]));
+                }
+            }
+            const int a = P.ab[X][2 * row0], b = P.ab[X][2 * row0 + 1];
+            const int atA = P.shell_atom[a], atB = P.shell_atom[b];
+            if (uniform) {
+#pragma unroll
+                for (int x = 0; x < 3; ++x)
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) {
+                        gA[x] += __shfl_xor_sync(DFTK_FULL_MASK, gA[x], o);
+                        gB[x] += __shfl_xor_sync(DFTK_FULL_MASK, gB[x], o);
+                    }
+                if (lane == 0) {
+#pragma unroll
+                    for (int x = 0; x < 3; ++x) {
+                        g_add(sg, P.grad, 3 * atA + x, gA[x]);
+                        g_add(sg, P.grad, 3 * atB + x, gB[x]);
+                    }
+                }
+            } else if (valid) {
+                const int ra = P.ab[X][2 * row], rb = P.ab[X][2 * row + 1];
+#pragma unroll
+                for (int x = 0; x < 3; ++x) {
+                    g_add(sg, P.grad, 3 * P.shell_atom[ra] + x, gA[x]);
+                    g_add(sg, P.grad, 3 * P.shell_atom[rb] + x, gB[x]);
+                }
+            }
+        }
+    } else {
+        const long long ncand = P.total[C];
+        const long long stride = (long long)gridDim.x * blockDim.x;
+        for (long long cand = (long long)blockIdx.x * blockDim.x + threadIdx.x; cand < ncand; cand += stride) {
+            const int row = find_row(P.row_off[C], P.n_rows[C], cand);
+            const int ket = (int)(cand - P.row_off[C][row]);
+            const int a = P.ab[X][2 * row], b = P.ab[X][2 * row + 1];
+            const int c = P.ab[Y][2 * ket], d = P.ab[Y][2 * ket + 1];
+            const int ns = P.ns;
+            const float dm = fmaxf(fmaxf(P.Dsh[a * ns + b], P.Dsh[c * ns + d]),
+                                   fmaxf(fmaxf(P.Dsh[a * ns + c], P.Dsh[a * ns + d]),
+                                         fmaxf(P.Dsh[b * ns + c], P.Dsh[b * ns + d])));
+            if (P.q[X][row] * P.q[Y][ket] * (double)dm * (double)dm < P.tau) continue;
+            double gA[3], gB[3], gC[3];
+            grad_quartet<C>(P, row, ket, gA, gB, gC);
+            const int at[4] = {P.shell_atom[a], P.shell_atom[b], P.shell_atom[c], P.shell_atom[d]};
+#pragma unroll
+            for (int x = 0; x < 3; ++x) {
+                g_add(sg, P.grad, 3 * at[0] + x, gA[x]);
+                g_add(sg, P.grad, 3 * at[1] + x, gB[x]);
+                g_add(sg, P.grad, 3 * at[2] + x, gC[x]);
+                g_add(sg, P.grad, 3 * at[3] + x, -(gA[x] + gB[x] + gC[x]));
+            }
         }
     }
     g_smem_end(sg, P.grad, 3 * P.n_atoms);
@@ -505,54 +607,32 @@ __global__ void __launch_bounds__(GRAD_THREADS) k_grad_nuclear(const dftk_shells
                 for (int ka = 0; ka < NA; ++ka)
 #pragma unroll
                     for (int kb = 0; kb < NB; ++kb) {
-                        const int a3[3] = {g_cp(LA, ka, 0), g_cp(LA, ka, 1), g_cp(LA, ka, 2)};
-                        const int b3[3] = {g_cp(LB, kb, 0), g_cp(LB, kb, 1), g_cp(LB, kb, 2)};
                         const double dm = Dm[ka][kb];
+                        double tA[3] = {0.0, 0.0, 0.0}, tB[3] = {0.0, 0.0, 0.0};
+                        g_ab_contract<LA, LB>(ka, kb, E, al, be, R, tA, tB);
+                        // operator centre: -E^n_T R_{T + 1_dir}
+                        const int sx = g_cp(LA, ka, 0) + g_cp(LB, kb, 0), sy = g_cp(LA, ka, 1) + g_cp(LB, kb, 1),
+                                  sz = g_cp(LA, ka, 2) + g_cp(LB, kb, 2);
+                        double tC[3] = {0.0, 0.0, 0.0};
 #pragma unroll
-                        for (int t = 0; t <= a3[0] + b3[0] + 1; ++t)
+                        for (int t = 0; t <= sx; ++t)
 #pragma unroll
-                            for (int u = 0; u <= a3[1] + b3[1] + 1; ++u)
+                            for (int u = 0; u <= sy; ++u)
 #pragma unroll
-                                for (int v = 0; v <= a3[2] + b3[2] + 1; ++v) {
-                                    if (t + u + v > a3[0] + b3[0] + a3[1] + b3[1] + a3[2] + b3[2] + 1) continue;
-                                    const int tt[3] = {t, u, v};
-                                    const double r = dm * R[t][u][v];
-#pragma unroll
-                                    for (int dir = 0; dir < 3; ++dir) {
-                                        double ea = 1.0, eb = 1.0;
-                                        bool zero = false;
-#pragma unroll
-                                        for (int x = 0; x < 3; ++x) {
-                                            const int i = a3[x], j = b3[x], tx = tt[x];
-                                            if (x != dir) {
-                                                if (tx > i + j) zero = true;
-                                                else {
-                                                    ea *= E[x][i][j][tx];
-                                                    eb *= E[x][i][j][tx];
-                                                }
-                                            } else {
-                                                double fa = 2.0 * al * E[x][i + 1][j][tx];
-                                                if (i > 0 && tx <= i + j - 1) fa = fma(-(double)i, E[x][i - 1][j][tx], fa);
-                                                double fb = 2.0 * be * E[x][i][j + 1][tx];
-                                                if (j > 0 && tx <= i + j - 1) fb = fma(-(double)j, E[x][i][j - 1][tx], fb);
-                                                ea *= fa;
-                                                eb *= fb;
-                                            }
-                                        }
-                                        if (!zero) {
-                                            gA[dir] = fma(ea, r, gA[dir]);
-                                            gB[dir] = fma(eb, r, gB[dir]);
-                                        }
-                                    }
-                                    // operator centre: -E^n_T R_{T + 1_dir}
-                                    if (t <= a3[0] + b3[0] && u <= a3[1] + b3[1] && v <= a3[2] + b3[2]) {
-                                        const double e = E[0][a3[0]][b3[0]][t] * E[1][a3[1]][b3[1]][u] *
-                                                         E[2][a3[2]][b3[2]][v] * dm;
-                                        gC[0] = fma(-e, R[t + 1][u][v], gC[0]);
-                                        gC[1] = fma(-e, R[t][u + 1][v], gC[1]);
-                                        gC[2] = fma(-e, R[t][u][v + 1], gC[2]);
-                                    }
+                                for (int v = 0; v <= sz; ++v) {
+                                    const double e = E[0][g_cp(LA, ka, 0)][g_cp(LB, kb, 0)][t] *
+                                                     E[1][g_cp(LA, ka, 1)][g_cp(LB, kb, 1)][u] *
+                                                     E[2][g_cp(LA, ka, 2)][g_cp(LB, kb, 2)][v];
+                                    tC[0] = fma(e, R[t + 1][u][v], tC[0]);
+                                    tC[1] = fma(e, R[t][u + 1][v], tC[1]);
+                                    tC[2] = fma(e, R[t][u][v + 1], tC[2]);
                                 }
+#pragma unroll
+                        for (int x = 0; x < 3; ++x) {
+                            gA[x] = fma(dm, tA[x], gA[x]);
+                            gB[x] = fma(dm, tB[x], gB[x]);
+                            gC[x] = fma(-dm, tC[x], gC[x]);
+                        }
                     }
             }
         const int atA = shell_atom[a], atB = shell_atom[b];
@@ -608,8 +688,6 @@ __global__ void __launch_bounds__(GRAD_THREADS) k_grad_overlap_kinetic(const dft
                 for (int ka = 0; ka < NA; ++ka)
 #pragma unroll
                     for (int kb = 0; kb < NB; ++kb) {
-                        const int a3[3] = {g_cp(LA, ka, 0), g_cp(LA, ka, 1), g_cp(LA, ka, 2)};
-                        const int b3[3] = {g_cp(LB, kb, 0), g_cp(LB, kb, 1), g_cp(LB, kb, 2)};
                         const long long mu = sh.ao[a] + ka, nu = sh.ao[b] + kb;
                         const double dm = fpair * w * D[mu * N + nu], wm = fpair * w * W[mu * N + nu];
                         double S[3][3], T[3][3];  // [axis][i = a - 1 .. a + 1 -> 0..2] at j = b
@@ -617,7 +695,7 @@ __global__ void __launch_bounds__(GRAD_THREADS) k_grad_overlap_kinetic(const dft
                         for (int x = 0; x < 3; ++x)
 #pragma unroll
                             for (int di = -1; di <= 1; ++di) {
-                                const int i = a3[x] + di, j = b3[x];
+                                const int i = g_cp(LA, ka, x) + di, j = g_cp(LB, kb, x);
                                 if (i < 0) {
                                     S[x][di + 1] = 0.0;
                                     T[x][di + 1] = 0.0;
@@ -632,7 +710,7 @@ __global__ void __launch_bounds__(GRAD_THREADS) k_grad_overlap_kinetic(const dft
 #pragma unroll
                         for (int dir = 0; dir < 3; ++dir) {
                             const int o1 = (dir + 1) % 3, o2 = (dir + 2) % 3;
-                            const int i = a3[dir];
+                            const int i = g_cp(LA, ka, dir);
                             double dS = 2.0 * al * S[dir][2], dT = 2.0 * al * T[dir][2];
                             if (i > 0) {
                                 dS -= i * S[dir][0];

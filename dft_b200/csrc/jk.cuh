@@ -156,6 +156,7 @@ struct JkParams {
     int uhf;
     double tau_lo, tau_hi;  // scan path: quartet processed if tau_lo <= bound < tau_hi
     double tau, tau32;      // select path: FP64 if bound >= tau32, FP32 if tau <= bound < tau32
+    int dm_pow2;            // select path: bound Q_ab Q_cd max|D|^2 (gradients) instead of max|D|
     long long *counts;
     // select path: per class one list of (bra row, ket) with capacity total[C];
     // FP64 entries fill it from the front, FP32 entries from the back
@@ -373,7 +374,7 @@ __global__ void __launch_bounds__(128) k_jk(const JkParams P)
             float dm = fmaxf(fmaxf(__ldg(P.Dsh + a * ns + b), __ldg(P.Dsh + c * ns + d)),
                              fmaxf(fmaxf(__ldg(P.Dsh + a * ns + c), __ldg(P.Dsh + a * ns + d)),
                                    fmaxf(__ldg(P.Dsh + b * ns + c), __ldg(P.Dsh + b * ns + d))));
-            const double bound = __ldg(P.q[X] + row) * __ldg(P.q[Yc] + ket) * (double)dm;
+            const double bound = __ldg(P.q[X] + row) * __ldg(P.q[Yc] + ket) * (double)dm * (P.dm_pow2 ? (double)dm : 1.0);
             valid = bound >= P.tau_lo && bound < P.tau_hi;
         }
         if (P.counts && split == 0) {
@@ -418,7 +419,7 @@ __device__ __forceinline__ void select_classify(const JkParams &P, long long can
     const float dm = fmaxf(fmaxf(__ldg(P.Dsh + a * ns + b), __ldg(P.Dsh + c * ns + d)),
                            fmaxf(fmaxf(__ldg(P.Dsh + a * ns + c), __ldg(P.Dsh + a * ns + d)),
                                  fmaxf(__ldg(P.Dsh + b * ns + c), __ldg(P.Dsh + b * ns + d))));
-    const double bound = __ldg(P.q[X] + row) * __ldg(P.q[Yc] + ket) * (double)dm;
+    const double bound = __ldg(P.q[X] + row) * __ldg(P.q[Yc] + ket) * (double)dm * (P.dm_pow2 ? (double)dm : 1.0);
     is64 = bound >= P.tau32;
     is32 = !is64 && bound >= P.tau;
 }

@@ -180,7 +180,8 @@ int dftk_jk_noalloc(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N
 /* Profiling aid: with timing enabled, later dftk_jk calls record CUDA events
  * around each class kernel on their stream.  dftk_jk_timing_read waits for
  * the last recorded call and writes ms[2 * DFTK_N_QCLASS] (FP64 launches,
- * then FP32 launches; 0 where a class did not launch). */
+ * then FP32 launches; 0 where a class did not launch).  A dftk_grad call
+ * records its class kernels in slots 0..5 and its one-electron part in slot 6. */
 int dftk_jk_timing(int enable);
 int dftk_jk_timing_read(float *ms, int n);
 
@@ -190,7 +191,10 @@ int dftk_jk_timing_read(float *ms, int n);
  * total density, D_a / D_b the spin densities (both D/2 for RHF), W the
  * energy-weighted density; shell_atom maps shells to atoms, atom_z are the
  * nuclear charges.  Quartets of `queue` with Q_ab Q_cd max|D|^2 < tau are
- * skipped.  workspace: at least n_shells^2 floats. */
+ * skipped; primitive quartets with qp_bra qp_ket < queue->tau_prim too.
+ * workspace: at least dftk_jk_workspace_bytes(n_shells, n_ao) bytes; with
+ * dftk_jk_workspace_bytes_queue bytes the surviving quartets are compacted
+ * by dftk_jk's selection pass first (the faster path). */
 int dftk_grad(const dftk_shells_t *shells, const int *shell_atom, int n_atoms, const double *atom_xyz,
               const double *atom_z, const dftk_pairs_t pairs[DFTK_N_PCLASS], const dftk_queue_t *queue,
               const double *D, const double *D_a, const double *D_b, const double *W, double tau,
