@@ -26,7 +26,7 @@ SYMBOLS = (
     "dftk_version", "dftk_last_error", "dftk_init", "dftk_boys", "dftk_boys32",
     "dftk_pair_data", "dftk_schwarz", "dftk_one_electron", "dftk_eri_blocks",
     "dftk_jk_workspace_bytes", "dftk_jk_workspace_bytes_queue", "dftk_jk", "dftk_nuclear_kernel", "dftk_eri_kernel",
-    "dftk_fma_burn", "dftk_jk_timing", "dftk_jk_timing_read", "dftk_jk_noalloc", "dftk_grad",
+    "dftk_fma_burn", "dftk_jk_timing", "dftk_jk_timing_read", "dftk_jk_noalloc", "dftk_grad", "dftk_workspace_bytes",
 )
 
 
@@ -49,6 +49,20 @@ class Shells(ctypes.Structure):
         ("ao", ctypes.c_void_p),
         ("prim_exp", ctypes.c_void_p),
         ("prim_cn", ctypes.c_void_p),
+        # batch description (zero / NULL for one molecule)
+        ("n_mol", ctypes.c_int),
+        ("max_ns", ctypes.c_int),
+        ("max_natom", ctypes.c_int),
+        ("mat_elems", ctypes.c_longlong),
+        ("dsh_elems", ctypes.c_longlong),
+        ("mol", ctypes.c_void_p),
+        ("mol_mat", ctypes.c_void_p),
+        ("mol_nao", ctypes.c_void_p),
+        ("mol_shell0", ctypes.c_void_p),
+        ("mol_ns", ctypes.c_void_p),
+        ("mol_dsh", ctypes.c_void_p),
+        ("mol_atom0", ctypes.c_void_p),
+        ("mol_natom", ctypes.c_void_p),
     ]
 
 
@@ -71,6 +85,8 @@ class Queue(ctypes.Structure):
         ("total", ctypes.c_longlong * N_QCLASS),
         ("row_off", ctypes.c_void_p * N_QCLASS),
         ("tau_prim", ctypes.c_double),
+        ("ket_base", ctypes.c_void_p * N_QCLASS),
+        ("mol_active", ctypes.c_void_p),
     ]
 
 
@@ -105,6 +121,7 @@ def load() -> ctypes.CDLL:
         "dftk_eri_blocks": ([ctypes.POINTER(Shells), ctypes.POINTER(Pairs), ll, vp, vp, vp, vp], i),
         "dftk_jk_workspace_bytes": ([i, i], sz),
         "dftk_jk_workspace_bytes_queue": ([i, i, ctypes.POINTER(Queue)], sz),
+        "dftk_workspace_bytes": ([ctypes.POINTER(Shells), ctypes.POINTER(Queue)], sz),
         "dftk_jk": ([ctypes.POINTER(Shells), ctypes.POINTER(Pairs), ctypes.POINTER(Queue), vp, vp, vp,
                      vp, vp, vp, i, d, d, vp, sz, vp, vp], i),
         "dftk_nuclear_kernel": ([vp] * 8 + [i, i, i] + [vp] * 9 + [vp], i),

@@ -212,6 +212,47 @@ int launch_jk_list_all(const JkParams &P, cudaStream_t s)
 
 // Workspace with room for the selection lists: the base layout, then the
 // 2 * DFTK_N_QCLASS list counters, then one int2 per candidate of every class.
+// the same for a shell set that may be a batch (matrix and shell-block sizes summed per molecule)
+size_t ws_bytes_sh(const dftk_shells_t &sh)
+{
+    size_t b = 3 * (size_t)shells_mat_elems(sh) * sizeof(double);
+    b += (size_t)shells_dsh_elems(sh) * sizeof(float);
+    return (b + 255) & ~(size_t)255;
+}
+
+size_t ws_list_bytes_sh(const dftk_shells_t &sh, const dftk_queue_t *q)
+{
+    size_t b = ws_bytes_sh(sh) + 256;
+    for (int c = 0; c < DFTK_N_QCLASS; ++c)
+        if (q->n_rows[c] > 0 && q->total[c] > 0) b += (((size_t)q->total[c] * sizeof(int2)) + 255) & ~(size_t)255;
+    return b;
+}
+
+// shell-block maxima of |D| for every molecule (before the selection or scan)
+int launch_dsh(const dftk_shells_t &sh, const double *D, const double *Da, const double *Db, int uhf, float *Dsh,
+               cudaStream_t s)
+{
+    const int max_ns = sh.mol ? sh.max_ns : sh.n_shells;
+    const long long n = (long long)sh.n_shells * max_ns;
+    if (n == 0) return DFTK_OK;
+    k_dsh<<<blocks_for(n, 128), 128, 0, s>>>(sh, max_ns, D, Da, Db, uhf, Dsh);
+    DFTK_LAUNCHED("k_dsh");
+    return DFTK_OK;
+}
+
+int launch_symmetrize(const dftk_shells_t &sh, const double *Y, const double *Za, const double *Zb, double *J,
+                      double *Ka, double *Kb, int uhf, cudaStream_t s)
+{
+    const long long nn = (long long)sh.n_ao * sh.n_ao;  // the largest molecule's block in a batch
+    long long bx = (nn + 255) / 256;
+    if (bx > 148 * 8) bx = 148 * 8;
+    if (bx < 1) bx = 1;
+    const dim3 grid((unsigned)bx, (unsigned)shells_n_mol(sh));
+    k_symmetrize<<<grid, 256, 0, s>>>(sh, Y, Za, Zb, J, Ka, Kb, uhf);
+    DFTK_LAUNCHED("k_symmetrize");
+    return DFTK_OK;
+}
+
 size_t ws_list_bytes(int ns, int n_ao, const dftk_queue_t *q)
 {
     size_t b = ws_bytes(ns, n_ao) + 256;
@@ -358,6 +399,12 @@ size_t dftk_jk_workspace_bytes_queue(int n_shells, int n_ao, const dftk_queue_t 
     return ws_list_bytes(n_shells, n_ao, queue);
 }
 
+size_t dftk_workspace_bytes(const dftk_shells_t *shells, const dftk_queue_t *queue)
+{
+    if (!shells || shells->n_shells < 0 || shells->n_ao < 0) return 0;
+    return queue ? ws_list_bytes_sh(*shells, queue) : ws_bytes_sh(*shells);
+}
+
 int dftk_jk(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N_PCLASS], const dftk_queue_t *queue,
             const double *D, const double *D_a, const double *D_b, double *J, double *K_a, double *K_b,
             int flags, double tau, double tau_fp32, void *workspace, size_t workspace_bytes,
@@ -370,22 +417,25 @@ int dftk_jk(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N_PCLASS]
     if (uhf && (!D_b || !K_b)) return fail(DFTK_ERR_ARG, "dftk_jk: UHF needs D_b and K_b");
     if (!(tau >= 0.0) || (mixed && !(tau_fp32 >= tau))) return fail(DFTK_ERR_ARG, "dftk_jk: bad thresholds");
     const int ns = shells->n_shells, N = shells->n_ao;
-    if (workspace_bytes < ws_bytes(ns, N)) return fail(DFTK_ERR_WORKSPACE, "dftk_jk: workspace too small");
+    if (shells->mol && (shells->n_mol <= 0 || !shells->mol_mat || !shells->mol_nao || !shells->mol_shell0 ||
+                        !shells->mol_ns || !shells->mol_dsh))
+        return fail(DFTK_ERR_ARG, "dftk_jk: incomplete molecule table");
+    if (workspace_bytes < ws_bytes_sh(*shells)) return fail(DFTK_ERR_WORKSPACE, "dftk_jk: workspace too small");
     DFTK_INIT();
     cudaStream_t s = (cudaStream_t)stream;
-    const size_t nn = (size_t)N * N;
+    const size_t nn = (size_t)shells_mat_elems(*shells);
     double *Y = (double *)workspace;
     double *Za = Y + nn;
     double *Zb = Za + nn;
     float *Dsh = (float *)(Zb + nn);
     DFTK_CUDA(cudaMemsetAsync(Y, 0, 3 * nn * sizeof(double), s));
-    if (ns > 0) {
-        k_dsh<<<blocks_for((long long)ns * ns, 128), 128, 0, s>>>(shells->ao, shells->l, ns, N, D, D_a,
-                                                                  uhf ? D_b : D_a, uhf, Dsh);
-        DFTK_LAUNCHED("k_dsh");
-    }
+    int st;
+    if ((st = launch_dsh(*shells, D, D_a, uhf ? D_b : D_a, uhf, Dsh, s))) return st;
     JkParams P;
     memset(&P, 0, sizeof(P));
+    P.sh = *shells;
+    for (int c = 0; c < DFTK_N_QCLASS; ++c) P.ket_base[c] = queue->ket_base[c];
+    P.mol_active = queue->mol_active;
     P.shell_ao = shells->ao;
     P.N = N;
     P.ns = ns;
@@ -415,10 +465,9 @@ int dftk_jk(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N_PCLASS]
     P.Zb = Zb;
     P.Dsh = Dsh;
     P.uhf = uhf;
-    int st;
-    if (workspace_bytes >= ws_list_bytes(ns, N, queue)) {
+    if (workspace_bytes >= ws_list_bytes_sh(*shells, queue)) {
         // selection pass + list-driven class kernels
-        unsigned char *cur = (unsigned char *)workspace + ws_bytes(ns, N);
+        unsigned char *cur = (unsigned char *)workspace + ws_bytes_sh(*shells);
         P.heads = (unsigned long long *)cur;
         cur += 256;
         for (int c = 0; c < DFTK_N_QCLASS; ++c) {
@@ -440,9 +489,7 @@ int dftk_jk(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N_PCLASS]
             P.counts = counts ? counts + DFTK_N_QCLASS : nullptr;
             if ((st = launch_jk_list_all<float>(P, s))) return st;
         }
-        k_symmetrize<<<blocks_for((long long)nn, 256), 256, 0, s>>>(N, Y, Za, Zb, J, K_a, K_b, uhf);
-        DFTK_LAUNCHED("k_symmetrize");
-        return DFTK_OK;
+        return launch_symmetrize(*shells, Y, Za, Zb, J, K_a, K_b, uhf, s);
     }
     P.tau_lo = tau;
     P.tau_hi = INFINITY;
@@ -458,9 +505,7 @@ int dftk_jk(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N_PCLASS]
         P.counts = counts;
         if ((st = launch_jk_all<double>(P, s))) return st;
     }
-    k_symmetrize<<<blocks_for((long long)nn, 256), 256, 0, s>>>(N, Y, Za, Zb, J, K_a, K_b, uhf);
-    DFTK_LAUNCHED("k_symmetrize");
-    return DFTK_OK;
+    return launch_symmetrize(*shells, Y, Za, Zb, J, K_a, K_b, uhf, s);
 }
 
 int dftk_jk_timing(int enable)
@@ -501,24 +546,27 @@ int dftk_grad(const dftk_shells_t *shells, const int *shell_atom, int n_atoms, c
         !W || !grad || !workspace)
         return fail(DFTK_ERR_ARG, "dftk_grad: null argument");
     const int ns = shells->n_shells, N = shells->n_ao;
-    if (workspace_bytes < ws_bytes(ns, N)) return fail(DFTK_ERR_WORKSPACE, "dftk_grad: workspace too small");
+    if (workspace_bytes < ws_bytes_sh(*shells)) return fail(DFTK_ERR_WORKSPACE, "dftk_grad: workspace too small");
     DFTK_INIT();
     cudaStream_t s = (cudaStream_t)stream;
     // same workspace layout as dftk_jk: Dsh after three N x N blocks, then
     // the selection heads and lists when the workspace holds them
-    float *Dsh = (float *)((double *)workspace + 3 * (size_t)N * N);
-    const bool use_list = workspace_bytes >= ws_list_bytes(ns, N, queue);
+    float *Dsh = (float *)((double *)workspace + 3 * (size_t)shells_mat_elems(*shells));
+    const bool use_list = workspace_bytes >= ws_list_bytes_sh(*shells, queue);
     DFTK_CUDA(cudaMemsetAsync(grad, 0, 3 * sizeof(double) * n_atoms, s));
     if (ns == 0) return DFTK_OK;
     // block-private gradient copies in shared memory when they fit
     const size_t smem = n_atoms <= GRAD_SMEM_ATOMS ? 3 * sizeof(double) * n_atoms : 0;
     const long long cap = 148LL * 8;
+    const int nat_stride = shells->mol ? shells->max_natom : n_atoms;
     auto grid = [cap](long long work) {
         long long b = (work + GRAD_THREADS - 1) / GRAD_THREADS;
         return (unsigned)(b < 1 ? 1 : (b > cap ? cap : b));
     };
-    k_dsh<<<blocks_for((long long)ns * ns, 128), 128, 0, s>>>(shells->ao, shells->l, ns, N, D, D_a, D_b, 1, Dsh);
-    DFTK_LAUNCHED("k_dsh");
+    {
+        const int st = launch_dsh(*shells, D, D_a, D_b, 1, Dsh, s);
+        if (st) return st;
+    }
     // with dftk_jk_timing on: slots 0..5 time the class kernels, slot 6 the one-electron part
     const bool timed = g_timing.enabled;
     if (timed) {
@@ -530,7 +578,7 @@ int dftk_grad(const dftk_shells_t *shells, const int *shell_atom, int n_atoms, c
         k_grad_overlap_kinetic<PC><<<grid(pairs[PC].n_pairs), GRAD_THREADS, smem, s>>>(                       \
             *shells, pairs[PC].ab, pairs[PC].n_pairs, shell_atom, n_atoms, D, W, grad);                      \
         DFTK_LAUNCHED("k_grad_overlap_kinetic");                                                             \
-        k_grad_nuclear<PC><<<grid((long long)pairs[PC].n_pairs * n_atoms), GRAD_THREADS, smem, s>>>(         \
+        k_grad_nuclear<PC><<<grid((long long)pairs[PC].n_pairs * nat_stride), GRAD_THREADS, smem, s>>>(      \
             *shells, pairs[PC].ab, pairs[PC].n_pairs, shell_atom, n_atoms, atom_xyz, atom_z, D, grad);       \
         DFTK_LAUNCHED("k_grad_nuclear");                                                                     \
     }
@@ -571,11 +619,15 @@ int dftk_grad(const dftk_shells_t *shells, const int *shell_atom, int n_atoms, c
     P.grad = grad;
     P.tau_prim = (float)queue->tau_prim;
     for (int k = 0; k < 3; ++k) P.qp[k] = pairs[k].qp;
+    for (int c = 0; c < DFTK_N_QCLASS; ++c) P.ket_base[c] = queue->ket_base[c];
     if (use_list) {
         // selection pass of dftk_jk with the gradient bound Q_ab Q_cd max|D|^2 >= tau
         JkParams S;
         memset(&S, 0, sizeof(S));
+        S.sh = *shells;
         S.ns = ns;
+        for (int c = 0; c < DFTK_N_QCLASS; ++c) S.ket_base[c] = queue->ket_base[c];
+        S.mol_active = queue->mol_active;
         for (int k = 0; k < 3; ++k) {
             S.ab[k] = pairs[k].ab;
             S.q[k] = pairs[k].q;
@@ -589,7 +641,7 @@ int dftk_grad(const dftk_shells_t *shells, const int *shell_atom, int n_atoms, c
         S.tau = tau;
         S.tau32 = tau;
         S.dm_pow2 = 1;
-        unsigned char *cur = (unsigned char *)workspace + ws_bytes(ns, N);
+        unsigned char *cur = (unsigned char *)workspace + ws_bytes_sh(*shells);
         S.heads = (unsigned long long *)cur;
         cur += 256;
         for (int c = 0; c < DFTK_N_QCLASS; ++c) {

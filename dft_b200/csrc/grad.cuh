@@ -54,6 +54,7 @@ struct GradParams {
     // list path: per class the selected (bra row, ket) entries and their count
     const int2 *list[DFTK_N_QCLASS];
     const unsigned long long *heads;
+    const int *ket_base[DFTK_N_QCLASS];  // batches: first ket pair of each row's molecule (NULL = 0)
 };
 
 // Quartet classes (ss|ss)..(pp|pp): angular momenta and pair classes.
@@ -244,7 +245,9 @@ __device__ __forceinline__ void grad_quartet(const GradParams &P, int row, int k
     {
         const int a = P.ab[X][2 * row], b = P.ab[X][2 * row + 1];
         const int c = P.ab[Y][2 * ket], d = P.ab[Y][2 * ket + 1];
-        const long long N = P.N;
+        const MolView mv = mol_view(P.sh, a);
+        const long long N = mv.nao;
+        const double *Dt = P.D + mv.mat, *Dta = P.Da + mv.mat, *Dtb = P.Db + mv.mat;
         const int oa = P.sh.ao[a], ob = P.sh.ao[b], oc = P.sh.ao[c], od = P.sh.ao[d];
         const int ew = (a == b) + (c == d) + ((X == Y) && (row == ket));
         const double f = 8.0 / (double)(1 << ew);  // orientations of the unique quartet
@@ -258,9 +261,9 @@ __device__ __forceinline__ void grad_quartet(const GradParams &P, int row, int k
 #pragma unroll
                     for (int l = 0; l < ND; ++l) {
                         const long long I = oa + i, J = ob + j, K = oc + k, Lq = od + l;
-                        const double coul = 0.5 * P.D[I * N + J] * P.D[K * N + Lq];
-                        const double exch = 0.25 * (P.Da[I * N + K] * P.Da[J * N + Lq] + P.Db[I * N + K] * P.Db[J * N + Lq] +
-                                                    P.Da[I * N + Lq] * P.Da[J * N + K] + P.Db[I * N + Lq] * P.Db[J * N + K]);
+                        const double coul = 0.5 * Dt[I * N + J] * Dt[K * N + Lq];
+                        const double exch = 0.25 * (Dta[I * N + K] * Dta[J * N + Lq] + Dtb[I * N + K] * Dtb[J * N + Lq] +
+                                                    Dta[I * N + Lq] * Dta[J * N + K] + Dtb[I * N + Lq] * Dtb[J * N + K]);
                         Gm[i * NB + j][k * ND + l] = f * (coul - exch);
                     }
         double cA[3], cB[3], cC[3], cD[3];
@@ -528,13 +531,10 @@ __global__ void __launch_bounds__(GRAD_THREADS) k_grad_eri(const GradParams P)
         const long long stride = (long long)gridDim.x * blockDim.x;
         for (long long cand = (long long)blockIdx.x * blockDim.x + threadIdx.x; cand < ncand; cand += stride) {
             const int row = find_row(P.row_off[C], P.n_rows[C], cand);
-            const int ket = (int)(cand - P.row_off[C][row]);
+            const int ket = (int)(cand - P.row_off[C][row]) + (P.ket_base[C] ? P.ket_base[C][row] : 0);
             const int a = P.ab[X][2 * row], b = P.ab[X][2 * row + 1];
             const int c = P.ab[Y][2 * ket], d = P.ab[Y][2 * ket + 1];
-            const int ns = P.ns;
-            const float dm = fmaxf(fmaxf(P.Dsh[a * ns + b], P.Dsh[c * ns + d]),
-                                   fmaxf(fmaxf(P.Dsh[a * ns + c], P.Dsh[a * ns + d]),
-                                         fmaxf(P.Dsh[b * ns + c], P.Dsh[b * ns + d])));
+            const float dm = quartet_dmax(P.sh, P.Dsh, a, b, c, d);
             if (P.q[X][row] * P.q[Y][ket] * (double)dm * (double)dm < P.tau) continue;
             double gA[3], gB[3], gC[3];
             grad_quartet<C>(P, row, ket, gA, gB, gC);
@@ -568,12 +568,21 @@ __global__ void __launch_bounds__(GRAD_THREADS) k_grad_nuclear(const dftk_shells
     extern __shared__ double s_grad[];
     double *sg = n_atoms <= GRAD_SMEM_ATOMS ? s_grad : nullptr;
     g_smem_begin(sg, 3 * n_atoms);
-    const long long total = (long long)n_pairs * n_atoms;
-    const long long N = sh.n_ao;
+    // a batch pairs each shell pair with the nuclei of its own molecule only
+    const int nat_stride = sh.mol ? sh.max_natom : n_atoms;
+    const long long total = (long long)n_pairs * nat_stride;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
-        const int pair = (int)(t / n_atoms), cn = (int)(t % n_atoms);
+        const int pair = (int)(t / nat_stride), cl = (int)(t % nat_stride);
         const int a = ab[2 * pair], b = ab[2 * pair + 1];
+        int cn = cl;
+        if (sh.mol) {
+            const int m = __ldg(sh.mol + a);
+            if (cl >= __ldg(sh.mol_natom + m)) continue;
+            cn = __ldg(sh.mol_atom0 + m) + cl;
+        }
+        const MolView mv = mol_view(sh, a);
+        const long long N = mv.nao;
         const double cA[3] = {sh.xyz[3 * a], sh.xyz[3 * a + 1], sh.xyz[3 * a + 2]};
         const double cB[3] = {sh.xyz[3 * b], sh.xyz[3 * b + 1], sh.xyz[3 * b + 2]};
         const double cC[3] = {atom_xyz[3 * cn], atom_xyz[3 * cn + 1], atom_xyz[3 * cn + 2]};
@@ -582,7 +591,7 @@ __global__ void __launch_bounds__(GRAD_THREADS) k_grad_nuclear(const dftk_shells
 #pragma unroll
         for (int i = 0; i < NA; ++i)
 #pragma unroll
-            for (int j = 0; j < NB; ++j) Dm[i][j] = fpair * D[(long long)(sh.ao[a] + i) * N + sh.ao[b] + j];
+            for (int j = 0; j < NB; ++j) Dm[i][j] = fpair * D[mv.mat + (long long)(sh.ao[a] + i) * N + sh.ao[b] + j];
         const double ab2 = (cA[0] - cB[0]) * (cA[0] - cB[0]) + (cA[1] - cB[1]) * (cA[1] - cB[1]) +
                            (cA[2] - cB[2]) * (cA[2] - cB[2]);
         double gA[3] = {0.0, 0.0, 0.0}, gB[3] = {0.0, 0.0, 0.0}, gC[3] = {0.0, 0.0, 0.0};
@@ -661,9 +670,10 @@ __global__ void __launch_bounds__(GRAD_THREADS) k_grad_overlap_kinetic(const dft
     extern __shared__ double s_grad[];
     double *sg = n_atoms <= GRAD_SMEM_ATOMS ? s_grad : nullptr;
     g_smem_begin(sg, 3 * n_atoms);
-    const long long N = sh.n_ao;
     for (int pair = blockIdx.x * blockDim.x + threadIdx.x; pair < n_pairs; pair += gridDim.x * blockDim.x) {
         const int a = ab[2 * pair], b = ab[2 * pair + 1];
+        const MolView mv = mol_view(sh, a);
+        const long long N = mv.nao;
         const double cA[3] = {sh.xyz[3 * a], sh.xyz[3 * a + 1], sh.xyz[3 * a + 2]};
         const double cB[3] = {sh.xyz[3 * b], sh.xyz[3 * b + 1], sh.xyz[3 * b + 2]};
         const double fpair = (a == b) ? 1.0 : 2.0;
@@ -689,7 +699,7 @@ __global__ void __launch_bounds__(GRAD_THREADS) k_grad_overlap_kinetic(const dft
 #pragma unroll
                     for (int kb = 0; kb < NB; ++kb) {
                         const long long mu = sh.ao[a] + ka, nu = sh.ao[b] + kb;
-                        const double dm = fpair * w * D[mu * N + nu], wm = fpair * w * W[mu * N + nu];
+                        const double dm = fpair * w * D[mv.mat + mu * N + nu], wm = fpair * w * W[mv.mat + mu * N + nu];
                         double S[3][3], T[3][3];  // [axis][i = a - 1 .. a + 1 -> 0..2] at j = b
 #pragma unroll
                         for (int x = 0; x < 3; ++x)

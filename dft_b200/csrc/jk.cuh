@@ -136,6 +136,7 @@ __global__ void k_schwarz(const dftk_pairs_t pr, int nfields)
 
 // ------------------------------------------------------------------- J / K
 struct JkParams {
+    dftk_shells_t sh;  // shells (and molecule table of a batch)
     const int *shell_ao;
     int N, ns;
     const int *ab[3];
@@ -162,7 +163,23 @@ struct JkParams {
     // FP64 entries fill it from the front, FP32 entries from the back
     int2 *list[DFTK_N_QCLASS];
     unsigned long long *heads;  // [2 * DFTK_N_QCLASS]: FP64 then FP32 entry counts
+    const int *ket_base[DFTK_N_QCLASS];  // batches: first ket pair of each row's molecule (NULL = 0)
+    const unsigned char *mol_active;     // batches: molecules still iterating (NULL = all)
 };
+
+// ket pair of candidate `cand` in bra row `row` of class C
+template <int C>
+__device__ __forceinline__ int cand_ket(const JkParams &P, int row, long long cand)
+{
+    const int k = (int)(cand - __ldg(P.row_off[C] + row));
+    return P.ket_base[C] ? k + __ldg(P.ket_base[C] + row) : k;
+}
+
+// whether the molecule of shell a still takes part (per-molecule convergence)
+__device__ __forceinline__ bool mol_is_active(const JkParams &P, int a)
+{
+    return P.mol_active == nullptr || P.sh.mol == nullptr || __ldg(P.mol_active + __ldg(P.sh.mol + a)) != 0;
+}
 
 // largest r in [0, n_rows) with off[r] <= cand
 __device__ __forceinline__ int find_row(const long long *off, long long n_rows, long long cand)
@@ -175,24 +192,30 @@ __device__ __forceinline__ int find_row(const long long *off, long long n_rows, 
     return (int)lo;
 }
 
-// Shell-block maxima of |D| (and |D_a|, |D_b| for UHF): Dsh[x * ns + y].
-__global__ void k_dsh(const int *shell_ao, const int *shell_l, int ns, int N, const double *D,
-                      const double *Da, const double *Db, int uhf, float *Dsh)
+// Shell-block maxima of |D| (and |D_a|, |D_b| for UHF): Dsh[dsh + x * ns + y]
+// per molecule (x, y molecule-local shells).  Thread t = (x global, y local),
+// y < max_ns.
+__global__ void k_dsh(const dftk_shells_t sh, int max_ns, const double *D, const double *Da, const double *Db,
+                      int uhf, float *Dsh)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= ns * ns) return;
-    const int x = t / ns, y = t % ns;
-    const int ox = shell_ao[x], oy = shell_ao[y];
-    const int nx = (shell_l[x] + 1) * (shell_l[x] + 2) / 2, ny = (shell_l[y] + 1) * (shell_l[y] + 2) / 2;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)sh.n_shells * max_ns) return;
+    const int x = (int)(t / max_ns), yl = (int)(t % max_ns);
+    const MolView v = mol_view(sh, x);
+    if (yl >= v.ns) return;
+    const int y = v.s0 + yl;
+    const int ox = sh.ao[x], oy = sh.ao[y];
+    const int nx = (sh.l[x] + 1) * (sh.l[x] + 2) / 2, ny = (sh.l[y] + 1) * (sh.l[y] + 2) / 2;
+    const int N = v.nao;
     double m = 0.0;
     for (int i = 0; i < nx; ++i)
         for (int j = 0; j < ny; ++j) {
-            const long long o = (long long)(ox + i) * N + oy + j;
+            const long long o = v.mat + (long long)(ox + i) * N + oy + j;
             m = fmax(m, fabs(D[o]));
             m = fmax(m, fabs(Da[o]));
             if (uhf) m = fmax(m, fabs(Db[o]));
         }
-    Dsh[t] = (float)m;
+    Dsh[v.dsh + (long long)(x - v.s0) * v.ns + yl] = (float)m;
 }
 
 // Digest one contracted block into the half-accumulators Y (J) and Z (K):
@@ -207,14 +230,16 @@ __device__ __forceinline__ void digest(const JkParams &P, bool valid, bool unifo
 {
     using E = EriClass<T, C, S>;
     constexpr int NA = E::NA, NB = E::NB, NC = E::NC, ND = E::ND, NCD = E::NCD;
-    const int N = P.N;
+    const MolView mv = mol_view(P.sh, a);
+    const int N = mv.nao;
     const int oa = P.shell_ao[a], ob = P.shell_ao[b], oc = P.shell_ao[c], od = P.shell_ao[d];
     const double fJ = valid ? 2.0 / w : 0.0;
     const double fK = valid ? 1.0 / w : 0.0;
     double v[E::NI];
 #pragma unroll
     for (int q = 0; q < E::NI; ++q) v[q] = valid ? (double)I[q] : 0.0;
-    const double *D = P.D;
+    const double *D = P.D + mv.mat;
+    double *Yb = P.Y + mv.mat;
     // Y_cd
 #pragma unroll
     for (int m = 0; m < NCD; ++m) {
@@ -224,7 +249,7 @@ __device__ __forceinline__ void digest(const JkParams &P, bool valid, bool unifo
 #pragma unroll
             for (int ib = 0; ib < NB; ++ib)
                 s = fma(v[(ia * NB + ib) * NCD + m], __ldg(D + (long long)(oa + ia) * N + ob + ib), s);
-        if (valid) atomicAdd(P.Y + (long long)(oc + E::cd_c(m)) * N + od + E::cd_d(m), fJ * s);
+        if (valid) atomicAdd(Yb + (long long)(oc + E::cd_c(m)) * N + od + E::cd_d(m), fJ * s);
     }
     // Y_ab
 #pragma unroll
@@ -239,15 +264,15 @@ __device__ __forceinline__ void digest(const JkParams &P, bool valid, bool unifo
             s *= fJ;
             if (uniform_bra) {
                 s = warp_sum(s);
-                if ((threadIdx.x & 31) == 0) atomicAdd(P.Y + (long long)(oa + ia) * N + ob + ib, s);
+                if ((threadIdx.x & 31) == 0) atomicAdd(Yb + (long long)(oa + ia) * N + ob + ib, s);
             } else if (valid) {
-                atomicAdd(P.Y + (long long)(oa + ia) * N + ob + ib, s);
+                atomicAdd(Yb + (long long)(oa + ia) * N + ob + ib, s);
             }
         }
     // K, one or two spins
     for (int spin = 0; spin < (P.uhf ? 2 : 1); ++spin) {
-        const double *Ds = spin ? P.Db : P.Da;
-        double *Z = spin ? P.Zb : P.Za;
+        const double *Ds = (spin ? P.Db : P.Da) + mv.mat;
+        double *Z = (spin ? P.Zb : P.Za) + mv.mat;
         double zac[NA][NC], zad[NA][ND], zbc[NB][NC], zbd[NB][ND];
 #pragma unroll
         for (int i = 0; i < NA; ++i) {
@@ -367,15 +392,12 @@ __global__ void __launch_bounds__(128) k_jk(const JkParams P)
         int row = 0, ket = 0;
         if (valid) {
             row = find_row(P.row_off[C], P.n_rows[C], cand);
-            ket = (int)(cand - __ldg(P.row_off[C] + row));
+            ket = cand_ket<C>(P, row, cand);
             const int a = P.ab[X][2 * row], b = P.ab[X][2 * row + 1];
             const int c = P.ab[Yc][2 * ket], d = P.ab[Yc][2 * ket + 1];
-            const int ns = P.ns;
-            float dm = fmaxf(fmaxf(__ldg(P.Dsh + a * ns + b), __ldg(P.Dsh + c * ns + d)),
-                             fmaxf(fmaxf(__ldg(P.Dsh + a * ns + c), __ldg(P.Dsh + a * ns + d)),
-                                   fmaxf(__ldg(P.Dsh + b * ns + c), __ldg(P.Dsh + b * ns + d))));
+            const float dm = quartet_dmax(P.sh, P.Dsh, a, b, c, d);
             const double bound = __ldg(P.q[X] + row) * __ldg(P.q[Yc] + ket) * (double)dm * (P.dm_pow2 ? (double)dm : 1.0);
-            valid = bound >= P.tau_lo && bound < P.tau_hi;
+            valid = bound >= P.tau_lo && bound < P.tau_hi && mol_is_active(P, a);
         }
         if (P.counts && split == 0) {
             const unsigned bal = __ballot_sync(DFTK_FULL_MASK, valid);
@@ -412,16 +434,14 @@ __device__ __forceinline__ void select_classify(const JkParams &P, long long can
     const long long *off = P.row_off[C];
     row = r0;
     if (cand >= __ldg(off + r0 + 1)) row = find_row(off, P.n_rows[C], cand);
-    ket = (int)(cand - __ldg(off + row));
+    ket = cand_ket<C>(P, row, cand);
     const int a = P.ab[X][2 * row], b = P.ab[X][2 * row + 1];
     const int c = P.ab[Yc][2 * ket], d = P.ab[Yc][2 * ket + 1];
-    const int ns = P.ns;
-    const float dm = fmaxf(fmaxf(__ldg(P.Dsh + a * ns + b), __ldg(P.Dsh + c * ns + d)),
-                           fmaxf(fmaxf(__ldg(P.Dsh + a * ns + c), __ldg(P.Dsh + a * ns + d)),
-                                 fmaxf(__ldg(P.Dsh + b * ns + c), __ldg(P.Dsh + b * ns + d))));
+    const float dm = quartet_dmax(P.sh, P.Dsh, a, b, c, d);
     const double bound = __ldg(P.q[X] + row) * __ldg(P.q[Yc] + ket) * (double)dm * (P.dm_pow2 ? (double)dm : 1.0);
-    is64 = bound >= P.tau32;
-    is32 = !is64 && bound >= P.tau;
+    const bool active = mol_is_active(P, a);
+    is64 = active && bound >= P.tau32;
+    is32 = active && !is64 && bound >= P.tau;
 }
 
 template <int C>
@@ -574,17 +594,21 @@ __global__ void __launch_bounds__(128, JkMinBlocks<C, T>::value) k_jk_list(const
     }
 }
 
-// J = Y + Y^T, K = Z + Z^T
-__global__ void k_symmetrize(int N, const double *Y, const double *Za, const double *Zb, double *J,
+// J = Y + Y^T, K = Z + Z^T within each molecule's block (blockIdx.y = molecule)
+__global__ void k_symmetrize(const dftk_shells_t sh, const double *Y, const double *Za, const double *Zb, double *J,
                              double *Ka, double *Kb, int uhf)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)N * N) return;
-    const int i = (int)(t / N), j = (int)(t % N);
-    const long long tt = (long long)j * N + i;
-    J[t] = Y[t] + Y[tt];
-    Ka[t] = Za[t] + Za[tt];
-    if (uhf) Kb[t] = Zb[t] + Zb[tt];
+    const int m = blockIdx.y;
+    const long long base = sh.mol ? sh.mol_mat[m] : 0;
+    const int N = sh.mol ? sh.mol_nao[m] : sh.n_ao;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < (long long)N * N;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t / N), j = (int)(t % N);
+        const long long o = base + t, ot = base + (long long)j * N + i;
+        J[o] = Y[o] + Y[ot];
+        Ka[o] = Za[o] + Za[ot];
+        if (uhf) Kb[o] = Zb[o] + Zb[ot];
+    }
 }
 
 // ------------------------------------------------------------- ERI blocks

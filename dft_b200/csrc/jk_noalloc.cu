@@ -55,8 +55,11 @@ extern "C" int dftk_jk_noalloc(const dftk_shells_t *shells, const dftk_pairs_t p
         dftk_internal_set_error("dftk_jk_noalloc: null shells");
         return DFTK_ERR_ARG;
     }
-    if (shells->n_ao < 0 || shells->n_shells < 0 || shells->n_ao > DFTK_NOALLOC_MAX_AO ||
-        shells->n_shells > DFTK_NOALLOC_MAX_SHELLS) {
+    const bool batch_too_big =
+        shells->mol && (shells->mat_elems > (long long)DFTK_NOALLOC_MAX_AO * DFTK_NOALLOC_MAX_AO ||
+                        shells->dsh_elems > (long long)DFTK_NOALLOC_MAX_SHELLS * DFTK_NOALLOC_MAX_SHELLS);
+    if (shells->n_ao < 0 || shells->n_shells < 0 || batch_too_big ||
+        (!shells->mol && (shells->n_ao > DFTK_NOALLOC_MAX_AO || shells->n_shells > DFTK_NOALLOC_MAX_SHELLS))) {
         const std::string msg = "dftk_jk_noalloc: " + std::to_string(shells->n_ao) + " basis functions / " +
                                 std::to_string(shells->n_shells) + " shells exceed the fixed scratch limit of " +
                                 std::to_string(DFTK_NOALLOC_MAX_AO) + " / " +

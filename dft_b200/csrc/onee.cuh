@@ -27,8 +27,17 @@ __global__ void k_one_electron(const dftk_shells_t sh, int n_atoms, const double
     const int j = (int)(t - (long long)i * (i + 1) / 2);
     const int la = sh.l[i], lb = sh.l[j];
     if (la > 1 || lb > 1 || la < 0 || lb < 0) return;  // s and p only; blocks left untouched
+    // a batch: pairs within one molecule, with that molecule's nuclei
+    int atom0 = 0, natom = n_atoms;
+    if (sh.mol) {
+        const int mi = sh.mol[i];
+        if (sh.mol[j] != mi) return;
+        atom0 = sh.mol_atom0[mi];
+        natom = sh.mol_natom[mi];
+    }
+    const MolView mv = mol_view(sh, i);
     const int ca = (la + 1) * (la + 2) / 2, cb = (lb + 1) * (lb + 2) / 2;
-    const int N = sh.n_ao;
+    const int N = mv.nao;
     const double A[3] = {sh.xyz[3 * i], sh.xyz[3 * i + 1], sh.xyz[3 * i + 2]};
     const double B[3] = {sh.xyz[3 * j], sh.xyz[3 * j + 1], sh.xyz[3 * j + 2]};
     double s_acc[3][3], t_acc[3][3], v_acc[3][3];
@@ -61,7 +70,7 @@ __global__ void k_one_electron(const dftk_shells_t sh, int n_atoms, const double
             for (int x = 0; x < 3; ++x)
                 for (int y = 0; y < 3; ++y) vv[x][y] = 0.0;
             const int L = la + lb;
-            for (int c = 0; c < n_atoms; ++c) {
+            for (int c = atom0; c < atom0 + natom; ++c) {
                 double R[27];
                 herm_R<2>(L, p, Pc[0] - atom_xyz[3 * c], Pc[1] - atom_xyz[3 * c + 1],
                           Pc[2] - atom_xyz[3 * c + 2], R);
@@ -100,7 +109,7 @@ __global__ void k_one_electron(const dftk_shells_t sh, int n_atoms, const double
     const int oi = sh.ao[i], oj = sh.ao[j];
     for (int ka = 0; ka < ca; ++ka)
         for (int kb = 0; kb < cb; ++kb) {
-            const long long r = (long long)(oi + ka) * N + oj + kb, c = (long long)(oj + kb) * N + oi + ka;
+            const long long r = mv.mat + (long long)(oi + ka) * N + oj + kb, c = mv.mat + (long long)(oj + kb) * N + oi + ka;
             S[r] = s_acc[ka][kb]; S[c] = s_acc[ka][kb];
             T[r] = t_acc[ka][kb]; T[c] = t_acc[ka][kb];
             V[r] = v_acc[ka][kb]; V[c] = v_acc[ka][kb];

@@ -49,12 +49,20 @@ enum {
 #define DFTK_N_QCLASS 6
 #define DFTK_N_PCLASS 3
 
-/* Shells of one molecule (device arrays).  l <= 1 (s, p) for the ERI and J/K
- * kernels, one contraction per shell (the reference splits sp shells,
- * shelled.py:66-75). */
+/* Shells of one molecule, or of a batch of molecules (device arrays).  l <= 1
+ * (s, p) for the ERI and J/K kernels, one contraction per shell (the
+ * reference splits sp shells, shelled.py:66-75).
+ *
+ * One molecule: mol == NULL; every N x N matrix argument is n_ao x n_ao.
+ * A batch: the shells of each molecule are contiguous, ao[] holds
+ * molecule-local AO indices, and every "N x N" matrix argument (densities,
+ * J, K, S, T, V, W) is the concatenation of the molecules' own n x n blocks,
+ * block m at element offset mol_mat[m].  Shell pairs and quartets never mix
+ * molecules (dftk_queue_t.ket_base).  The workspace functions size the
+ * shell-block arrays per molecule (mol_dsh). */
 typedef struct {
     int n_shells;
-    int n_ao;
+    int n_ao;               /* one molecule: AO count; a batch: largest molecule's */
     const double *xyz;      /* [3 * n_shells] centre of each shell, bohr */
     const int *l;           /* [n_shells] angular momentum */
     const int *nprim;       /* [n_shells] primitives */
@@ -62,6 +70,20 @@ typedef struct {
     const int *ao;          /* [n_shells] first AO (reference ao_start) */
     const double *prim_exp; /* [total primitives] exponents */
     const double *prim_cn;  /* [total primitives] coefficient x primitive norm (normal(), shelled.py:95-101) */
+    /* batch description (n_mol = 0 and NULL pointers for one molecule) */
+    int n_mol;
+    int max_ns;                /* largest shell count of a molecule */
+    int max_natom;             /* largest atom count of a molecule */
+    long long mat_elems;       /* sum of n_ao^2 over the molecules */
+    long long dsh_elems;       /* sum of n_shells^2 over the molecules */
+    const int *mol;            /* [n_shells] molecule of each shell */
+    const long long *mol_mat;  /* [n_mol] offset of the molecule's n_ao x n_ao block */
+    const int *mol_nao;        /* [n_mol] AO count */
+    const int *mol_shell0;     /* [n_mol] first shell */
+    const int *mol_ns;         /* [n_mol] shell count */
+    const long long *mol_dsh;  /* [n_mol] offset of its n_shells x n_shells block in shell-block arrays */
+    const int *mol_atom0;      /* [n_mol] first atom (atom arrays are concatenated too) */
+    const int *mol_natom;      /* [n_mol] atom count */
 } dftk_shells_t;
 
 /* Shell pairs of one pair class (0 ss, 1 ps, 2 pp) with l_a >= l_b, and their
@@ -91,6 +113,13 @@ typedef struct {
     const long long *row_off[DFTK_N_QCLASS];  /* device [n_rows + 1] */
     double tau_prim;                          /* skip primitive quartets with qp_ab * qp_cd < tau_prim
                                                  (0 keeps all); each skipped one is bounded by it */
+    /* batches: ket k of row r is ket pair ket_base[c][r] + k (the first pair of
+     * the row's molecule in the ket class, each molecule's pairs contiguous and
+     * sorted by descending Schwarz factor); NULL = 0 */
+    const int *ket_base[DFTK_N_QCLASS];
+    /* batches: molecules m with mol_active[m] == 0 are skipped by the
+     * selection pass (per-molecule convergence); NULL = all active */
+    const unsigned char *mol_active;
 } dftk_queue_t;
 
 /* library version (integer, 100 * major + minor) */
@@ -149,6 +178,11 @@ size_t dftk_jk_workspace_bytes(int n_shells, int n_ao);
  * per-kernel scan; one scan for both precisions).  8 bytes per candidate
  * quartet of the queue on top of dftk_jk_workspace_bytes. */
 size_t dftk_jk_workspace_bytes_queue(int n_shells, int n_ao, const dftk_queue_t *queue);
+
+/* The same two sizes for any shell set, one molecule or a batch: queue NULL
+ * gives the direct-path size (dftk_jk_workspace_bytes), a queue the
+ * selection-path size (dftk_jk_workspace_bytes_queue). */
+size_t dftk_workspace_bytes(const dftk_shells_t *shells, const dftk_queue_t *queue);
 
 /* Integral-direct J and K (fill_matrices, shelled.py:770-877, without stored
  * ERIs): J = (mu nu|la si) D_la,si and K_s = (mu la|nu si) Ds_la,si over the
