@@ -148,6 +148,119 @@ def setup_workload(torch, shape=(4, 4, 4)):
     return atoms, centers, shells, eng, S, H, enn, nocc
 
 
+# ------------------------------------------------------- batches, gradients
+def gradient_figures(torch, eng, atoms, centers, res):
+    """(H2O)_64 analytic gradient at the converged density: wall time of the
+    dftk_grad call (device-synchronised) and per-class kernel times."""
+    import ctypes
+
+    from dft_b200 import _lib
+
+    n_occ = basis_n_occ(atoms)
+    C = res.C_a[:, :n_occ]
+    D = 2.0 * (C @ C.T)
+    W = 2.0 * ((C * res.eps_a[:n_occ]) @ C.T)
+    Dh = (0.5 * D).contiguous()
+    eng.gradient(atoms, centers, D, Dh, Dh, W)
+    times = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        eng.gradient(atoms, centers, D, Dh, Dh, W)
+        torch.cuda.synchronize()
+        times.append((time.perf_counter() - t0) * 1e3)
+    _lib.call("dftk_jk_timing", 1)
+    eng.gradient(atoms, centers, D, Dh, Dh, W)
+    buf = (ctypes.c_float * 12)()
+    _lib.call("dftk_jk_timing_read", buf, 12)
+    _lib.call("dftk_jk_timing", 0)
+    from dft_b200.engine import QCLASS_NAMES
+
+    return {"h2o64_grad_ms": float(np.median(times)),
+            "class_ms": {QCLASS_NAMES[c]: float(buf[c]) for c in range(6)},
+            "one_electron_ms": float(buf[6]),
+            "note": "FP64 analytic RHF gradient (derivative ERIs + S/T/V derivatives), converged (H2O)_64 density"}
+
+
+def basis_n_occ(atoms):
+    from dft_b200 import basis
+
+    return basis.n_electrons(atoms) // 2
+
+
+def batch_figures(torch, n_mol=512, n_max=24, n_single=64, n_grad=256, n_grad_max=16):
+    """Batched SCF of n_mol seeded water clusters (1..n_max monomers) against
+    a loop of single-molecule solves on the first n_single of them, and
+    batched analytic gradients of n_grad clusters (1..n_grad_max monomers).
+    Wall-clock, device-synchronised; setup (shells, pairs, Schwarz, queue,
+    one-electron matrices) included on both sides."""
+    from dft_b200 import basis, geometry
+    from dft_b200.batch import BatchEngine, rhf_gradient_batch, scf_rhf_batch
+    from dft_b200.engine import IntegralEngine
+    from dft_b200.scf import scf_rhf
+
+    mols = geometry.water_cluster_batch(n_mol, n_max, seed=0)
+    # warm-up (library, cuSOLVER handles, graph machinery) on a small batch
+    scf_rhf_batch(BatchEngine(mols[:4]))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    eng = BatchEngine(mols)
+    torch.cuda.synchronize()
+    t_setup = time.perf_counter() - t0
+    res = scf_rhf_batch(eng)
+    torch.cuda.synchronize()
+    t_total = time.perf_counter() - t0
+    it = res.iterations[res.converged]
+    # loop of single solves on a sample
+    single_t, single_it, dE = [], [], []
+    for m, (atoms, c) in enumerate(mols[:n_single]):
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        e1 = IntegralEngine(basis.build_shells(basis.load_basis(), atoms, c))
+        S, T, V = e1.one_electron(atoms, c)
+        r = scf_rhf(e1, T + V, S, basis.n_electrons(atoms) // 2, geometry.nuclear_repulsion(atoms, c))
+        torch.cuda.synchronize()
+        single_t.append(time.perf_counter() - t1)
+        single_it.append(r.iterations)
+        dE.append(abs(r.energy - res.energy[m]))
+    single_rate = 1.0 / float(np.mean(single_t))
+    out = {
+        "batch_scf": {
+            "workload": f"{n_mol} water clusters, 1..{n_max} monomers (seed 0), RHF/STO-3G FP64, one shell set",
+            "molecules_per_s": n_mol / t_total, "seconds": t_total, "setup_s": t_setup,
+            "solve_s": res.seconds, "fock_graph_replays": res.fock_builds, "fock_s": res.fock_seconds,
+            "converged": int(res.converged.sum()),
+            "iterations_p50": float(np.percentile(it, 50)), "iterations_p99": float(np.percentile(it, 99)),
+            "single_loop": {"sample": n_single, "molecules_per_s": single_rate,
+                            "iterations_p50": float(np.percentile(single_it, 50)),
+                            "iterations_p99": float(np.percentile(single_it, 99)),
+                            "max_abs_dE_vs_batch_Eh": float(np.max(dE))},
+            "speedup_vs_single_loop": (n_mol / t_total) / single_rate,
+        }
+    }
+    gm = geometry.water_cluster_batch(n_grad, n_grad_max, seed=1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    geng = BatchEngine(gm)
+    gres = scf_rhf_batch(geng, etol=1e-11, dtol=1e-9)
+    torch.cuda.synchronize()
+    t_scf = time.perf_counter() - t0
+    rhf_gradient_batch(geng, gres)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    grads = rhf_gradient_batch(geng, gres)
+    torch.cuda.synchronize()
+    t_grad = time.perf_counter() - t1
+    out["batch_grad"] = {
+        "workload": f"{n_grad} water clusters, 1..{n_grad_max} monomers (seed 1), RHF/STO-3G FP64 analytic gradient",
+        "gradient_evals_per_s": n_grad / t_grad, "gradient_s": t_grad,
+        "with_scf_evals_per_s": n_grad / (t_scf + t_grad), "scf_s": t_scf,
+        "converged": int(gres.converged.sum()),
+        "max_abs_translational_sum": float(max(np.abs(g.sum(axis=0)).max() for g in grads)),
+    }
+    return out
+
+
 # ------------------------------------------------------------ reference arm
 def cpu_reference_rate(eng_totals, shells, q_by_class, per_class, seed=0, kernel="reference"):
     """Fock builds/s of the reference's CPU path, from timed per-class samples.
@@ -412,6 +525,9 @@ def run_dftk_arm(args, rank, world, local_rank):
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
         }
+        if not args.no_extras:
+            line["grad"] = gradient_figures(torch, eng, atoms, centers, r64)
+            line.update(batch_figures(torch))
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
@@ -447,6 +563,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="dftk", choices=["dftk", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the gradient and batch figures")
     ap.add_argument("--profile", action="store_true", help="only run a few builds (for ncu captures)")
     args = ap.parse_args()
     if args.profile:

@@ -10,13 +10,17 @@ its own molecule (``ket_base``), so one selection pass and one launch per
 quartet class cover every molecule, and quartets never mix molecules.
 
 :func:`scf_rhf_batch` iterates all molecules together on padded
-(B, Nmax, Nmax) tensors (padding: identity overlap, Hamiltonian diagonal far
-above every orbital energy, so padded functions never mix in or get
-occupied).  Each iteration's Fock build is one replay of a CUDA graph
-captured once (memset, shell-block density maxima, selection, six class
-kernels, symmetrisation).  Molecules converge individually: a converged
-molecule's flag in ``mol_active`` (read by the selection pass inside the
-graph) drops its quartets from later builds.
+(B, Nmax, Nmax) tensors (padding: identity overlap and zero coupling, so
+padded functions never mix in).  Each iteration's Fock build is one replay of
+a CUDA graph captured once (memset, shell-block density maxima, selection,
+six class kernels, symmetrisation).  The new density comes from canonical
+purification of the DIIS-extrapolated Fock matrix in the Cholesky-orthogonal
+basis (Palser and Manolopoulos, Phys. Rev. B 58, 12704 (1998)): batched
+matrix products only, no per-molecule eigensolver, with the padded levels
+put at the top of each molecule's Gershgorin interval so they end up empty.
+Molecules converge individually: a converged molecule's flag in
+``mol_active`` (read by the selection pass inside the graph) drops its
+quartets from later builds.
 """
 from __future__ import annotations
 
@@ -297,9 +301,8 @@ class BatchSCFResult:
     energy: np.ndarray           # per molecule
     converged: np.ndarray        # bool per molecule
     iterations: np.ndarray       # SCF iterations per molecule
-    D: torch.Tensor              # packed alpha densities
-    C: torch.Tensor              # padded MO coefficients (B, Nmax, Nmax)
-    eps: torch.Tensor            # padded orbital energies (B, Nmax)
+    D: torch.Tensor              # packed alpha densities (converged molecules: of their final full build)
+    F: torch.Tensor              # packed Fock matrices of those builds
     n_occ: np.ndarray
     fock_builds: int
     seconds: float
@@ -307,9 +310,48 @@ class BatchSCFResult:
     history: List[int] = field(default_factory=list)  # active molecules per iteration
 
 
-def _batched_orthogonalizer(S: torch.Tensor) -> torch.Tensor:
-    w, U = torch.linalg.eigh(S)
-    return (U * w.rsqrt().unsqueeze(-2)) @ U.transpose(-1, -2)
+def _cholesky_orthogonalizer(S: torch.Tensor) -> torch.Tensor:
+    """X = L^{-T} with S = L L^T, so X^T S X = I (batched)."""
+    L = torch.linalg.cholesky(S)
+    eye = torch.eye(S.shape[-1], dtype=S.dtype, device=S.device).expand_as(S)
+    return torch.linalg.solve_triangular(L, eye, upper=False).transpose(-1, -2)
+
+
+def _purify(Fo: torch.Tensor, n_occ: torch.Tensor, real: torch.Tensor, tol: float = 1e-13,
+            max_iter: int = 200) -> torch.Tensor:
+    """Density D' = sum of the n_occ lowest eigenvectors' projectors of the
+    symmetric Fo (B, N, N), by canonical purification.  Padded levels (real
+    == 0) are placed at the top of the Gershgorin interval.  Converges when
+    every molecule's tr(D - D^2) < tol."""
+    B, N, _ = Fo.shape
+    diag = Fo.diagonal(dim1=1, dim2=2)
+    rad = Fo.abs().sum(dim=2) - diag.abs()
+    e_max = torch.where(real > 0, diag + rad, torch.full_like(diag, -torch.inf)).amax(dim=1)
+    e_min = torch.where(real > 0, diag - rad, torch.full_like(diag, torch.inf)).amin(dim=1)
+    F = Fo + torch.diag_embed((1.0 - real) * e_max[:, None])
+    mu = F.diagonal(dim1=1, dim2=2).sum(dim=1) / N
+    n = n_occ.to(F.dtype)
+    lam = torch.minimum(n / (e_max - mu), (N - n) / (mu - e_min))
+    eye = torch.eye(N, dtype=F.dtype, device=F.device)
+    D = (lam / N)[:, None, None] * (mu[:, None, None] * eye - F) + (n / N)[:, None, None] * eye
+    for it in range(max_iter):
+        D2 = D @ D
+        D3 = D2 @ D
+        t1 = (D - D2).diagonal(dim1=1, dim2=2).sum(dim=1)
+        t2 = (D2 - D3).diagonal(dim1=1, dim2=2).sum(dim=1)
+        ok = t1.abs() > 1e-300
+        c = torch.where(ok, t2 / torch.where(ok, t1, torch.ones_like(t1)), torch.full_like(t1, 0.5))
+        up = ((1.0 + c)[:, None, None] * D2 - D3) / c.clamp_min(1e-300)[:, None, None]
+        lo = ((1.0 - 2.0 * c)[:, None, None] * D + (1.0 + c)[:, None, None] * D2 - D3) / \
+            (1.0 - c).clamp_min(1e-300)[:, None, None]
+        Dn = torch.where((c >= 0.5)[:, None, None], up, lo)
+        D = torch.where(ok[:, None, None], Dn, D)
+        if it % 4 == 3 and float(t1.abs().max()) < tol:
+            break
+    # one McWeeny step, then symmetrise
+    D2 = D @ D
+    D = 3.0 * D2 - 2.0 * (D2 @ D)
+    return 0.5 * (D + D.transpose(1, 2))
 
 
 def _batched_diis(Fh: torch.Tensor, Eh: torch.Tensor, n: int) -> torch.Tensor:
@@ -354,21 +396,21 @@ def scf_rhf_batch(eng: BatchEngine, charges: Optional[Sequence[int]] = None, dii
     e_nn = torch.as_tensor(eng.nuclear_repulsion(), dtype=torch.float64, device=dev)
     eng.mol_active.fill_(1)
     S_p, T_p, V_p = eng.one_electron()
-    big = 1.0e4
     S = eng.to_padded(S_p) + torch.diag_embed(eng.pad_mask)
-    H = eng.to_padded(T_p + V_p) + torch.diag_embed(big * eng.pad_mask)
-    X = _batched_orthogonalizer(S)
-    occ = torch.as_tensor((np.arange(Nm)[None, :] < n_occ[:, None]).astype(np.float64), device=dev)
+    H = eng.to_padded(T_p + V_p)
+    X = _cholesky_orthogonalizer(S)
     nn = torch.as_tensor(eng.mol_nao.astype(np.float64) ** 2, device=dev)
-
-    def density(C):
-        Co = C * occ[:, None, :]
-        return Co @ C.transpose(1, 2)
-
     Xt = X.transpose(1, 2)
-    _, Cp = torch.linalg.eigh(Xt @ H @ X)
-    C = X @ Cp
-    D = density(C)
+    real = 1.0 - eng.pad_mask
+    rmask = real[:, :, None] * real[:, None, :]
+    n_occ_t = torch.as_tensor(n_occ, device=dev)
+
+    def density(Fm):
+        """AO density of the n_occ lowest orbitals of Fm (padded, real block)."""
+        Dp = _purify(Xt @ Fm @ X, n_occ_t, real)
+        return (X @ Dp @ Xt) * rmask
+
+    D = density(H)
     graph = _FockGraph(eng, tau) if use_graph else None
 
     def build(Dp):
@@ -382,6 +424,8 @@ def scf_rhf_batch(eng: BatchEngine, charges: Optional[Sequence[int]] = None, dii
     n_hist = 0
     G = torch.zeros(eng.mat_elems, dtype=torch.float64, device=dev)
     D_ref = torch.zeros_like(D)
+    D_fin = torch.zeros(eng.mat_elems, dtype=torch.float64, device=dev)
+    F_fin = torch.zeros_like(D_fin)
     since_full = np.full(B, rebuild_every, dtype=np.int64)  # first build is full
     finishing = np.zeros(B, dtype=bool)
     active = np.ones(B, dtype=bool)
@@ -391,7 +435,6 @@ def scf_rhf_batch(eng: BatchEngine, charges: Optional[Sequence[int]] = None, dii
     conv = np.zeros(B, dtype=bool)
     builds, t_fock = 0, 0.0
     hist_active: List[int] = []
-    eps = torch.zeros((B, Nm), dtype=torch.float64, device=dev)
     for it in range(max_iter + 1):
         full = (since_full >= rebuild_every) | finishing
         full_t = torch.as_tensor(full, device=dev)
@@ -416,9 +459,7 @@ def scf_rhf_batch(eng: BatchEngine, charges: Optional[Sequence[int]] = None, dii
         Eh[0] = err
         n_hist = min(n_hist + 1, diis)
         Fx = _batched_diis(Fh, Eh, n_hist) if n_hist >= 2 else F
-        w, Cp = torch.linalg.eigh(Xt @ Fx @ X)
-        C_new = X @ Cp
-        D_new = density(C_new)
+        D_new = density(Fx)
         rms = torch.sqrt(((D_new - D) ** 2).sum(dim=(1, 2)) / nn).cpu().numpy()
         dE = np.abs(E - E_prev)
         finishing |= rms < finish_factor * dtol
@@ -429,36 +470,39 @@ def scf_rhf_batch(eng: BatchEngine, charges: Optional[Sequence[int]] = None, dii
             iters[idx] = it
             conv[idx] = True
             active[idx] = False
-            # orbitals of the converged molecules from their final full-build F
-            w2, Cp2 = torch.linalg.eigh(Xt @ F @ X)
             sel = torch.as_tensor(idx, device=dev)
-            C[sel] = (X @ Cp2)[sel]
-            eps[sel] = w2[sel]
+            pm = torch.zeros(B, dtype=torch.bool, device=dev)
+            pm[sel] = True
+            pm = pm[eng.packed_mol]
+            D_fin = torch.where(pm, eng.to_packed(D), D_fin)
+            F_fin = torch.where(pm, eng.to_packed(F), F_fin)
             eng.mol_active[sel] = 0
         if not active.any():
             break
         E_prev = np.where(active, E, E_prev)
         keep = torch.as_tensor(active, device=dev)[:, None, None]
         D = torch.where(keep, D_new, D)
-        C = torch.where(keep, C_new, C)
-    E_fin[active] = E_prev[active]
-    iters[active] = max_iter
-    D_final = eng.to_packed(density(C))
+    if active.any():
+        E_fin[active] = E_prev[active]
+        iters[active] = max_iter
+        pm = torch.as_tensor(active, device=dev)[eng.packed_mol]
+        D_fin = torch.where(pm, eng.to_packed(D), D_fin)
+        F_fin = torch.where(pm, eng.to_packed(F), F_fin)
     eng.mol_active.fill_(1)
     torch.cuda.synchronize(dev)
-    return BatchSCFResult(E_fin, conv, iters, D_final, C, eps, n_occ, builds, time.perf_counter() - t_start,
+    return BatchSCFResult(E_fin, conv, iters, D_fin, F_fin, n_occ, builds, time.perf_counter() - t_start,
                           t_fock, hist_active)
 
 
 def rhf_gradient_batch(eng: BatchEngine, res: BatchSCFResult, tau: float = 1e-14) -> List[np.ndarray]:
     """Analytic RHF gradients of every molecule of a converged batch, one
-    dftk_grad call for the whole batch: per molecule an (n_atoms, 3) array."""
-    occ = torch.as_tensor((np.arange(eng.n_max)[None, :] < res.n_occ[:, None]).astype(np.float64),
-                          device=eng.device)
-    Co = res.C * occ[:, None, :]
-    D = 2.0 * (Co @ res.C.transpose(1, 2))
-    W = 2.0 * ((Co * res.eps[:, None, :]) @ res.C.transpose(1, 2))
-    Dp, Wp = eng.to_packed(D), eng.to_packed(W)
+    dftk_grad call for the whole batch: per molecule an (n_atoms, 3) array.
+    With D_alpha = C_occ C_occ^T of a converged F, the energy-weighted
+    density C_occ diag(eps) C_occ^T equals D_alpha F D_alpha."""
+    Da = eng.to_padded(res.D)
+    Fp = eng.to_padded(res.F)
+    Dp = eng.to_packed(2.0 * Da)
+    Wp = eng.to_packed(2.0 * (Da @ Fp @ Da))
     Dh = (0.5 * Dp).contiguous()
     g = eng.gradient(Dp, Dh, Dh, Wp, tau=tau).cpu().numpy() + eng.nuclear_repulsion_gradient()
     return [g[int(eng.mol_atom0[m]):int(eng.mol_atom0[m] + eng.mol_natom[m])] for m in range(eng.n_mol)]

@@ -306,7 +306,13 @@ def scf_uhf(H: np.ndarray, S: np.ndarray, jk: Callable, n_alpha: int, n_beta: in
             B = (np.einsum("iab,jab->ij", hist["Ra"], hist["Ra"]) +
                  np.einsum("iab,jab->ij", hist["Rb"], hist["Rb"]))
             lim = min(count + 1, history)
-            c = np.linalg.solve(B[:lim, :lim], np.ones(lim))
+            try:
+                c = np.linalg.solve(B[:lim, :lim], np.ones(lim))
+            except np.linalg.LinAlgError:
+                # exactly singular history (tight thresholds, nearly equal error
+                # vectors): the reference would stop here; continue with the
+                # least-squares coefficients
+                c = np.linalg.lstsq(B[:lim, :lim], np.ones(lim), rcond=None)[0]
             c /= c.sum()
             Fa = np.einsum("i,iab->ab", c, hist["Fa"][:lim])
             Fb = np.einsum("i,iab->ab", c, hist["Fb"][:lim])
