@@ -18,6 +18,9 @@
  *   dftk_schwarz          <- (absent in the reference: screening bounds)
  *   dftk_eri_blocks       <- calc_eri quartet blocks          shelled.py:596-700
  *   dftk_jk               <- fill_matrices                    shelled.py:770-877
+ *   dftk_jk_noalloc       <- fill_matrices, for hosts that cannot allocate device memory
+ *   dftk_grad             <- (absent in the reference: analytic nuclear gradients)
+ *   dftk_workspace_bytes  <- (absent: workspace size of one molecule or a batch)
  */
 #ifndef DFTK_H
 #define DFTK_H

@@ -150,3 +150,43 @@ def test_cabi_argument_errors_without_gpu():
     with pytest.raises(_lib.DftkError) as ei:
         _lib.call("dftk_boys", 99, 1, None, None, None)
     assert ei.value.status == _lib.ERR_ARG
+
+
+def test_batched_purification_matches_eigh_projector():
+    """The batched SCF's density step (canonical purification, CPU torch here)
+    against the projector onto the n lowest eigenvectors, padded levels empty."""
+    import torch
+
+    from dft_b200.batch import _purify
+
+    g = torch.Generator().manual_seed(0)
+    B, N, n_real = 16, 40, 33
+    A = torch.randn(B, N, N, dtype=torch.float64, generator=g)
+    real = torch.ones(B, N, dtype=torch.float64)
+    real[:, n_real:] = 0
+    F = (A + A.transpose(1, 2)) * 2 * real[:, :, None] * real[:, None, :]
+    n = torch.randint(3, 20, (B,), generator=g)
+    D = _purify(F, n, real)
+    w, U = torch.linalg.eigh(F[:, :n_real, :n_real])
+    for b in range(B):
+        Uo = U[b][:, : int(n[b])]
+        assert (D[b, :n_real, :n_real] - Uo @ Uo.T).abs().max() < 1e-11
+    assert D[:, n_real:, :].abs().max() < 1e-12
+
+
+def test_batched_diis_matches_single():
+    import torch
+
+    from dft_b200.batch import _batched_diis
+    from dft_b200.scf import _Diis
+
+    g = torch.Generator().manual_seed(1)
+    hist, B, N = 5, 3, 6
+    F = torch.randn(hist, B, N, N, dtype=torch.float64, generator=g)
+    E = torch.randn(hist, B, N, N, dtype=torch.float64, generator=g)
+    out = _batched_diis(F, E, hist)
+    for b in range(B):
+        d = _Diis(8)
+        for k in reversed(range(hist)):  # history index 0 is the newest
+            d.push(F[k, b], E[k, b])
+        assert torch.allclose(out[b], d.extrapolate(), atol=1e-10)
