@@ -27,6 +27,7 @@ SYMBOLS = (
     "dftk_pair_data", "dftk_schwarz", "dftk_one_electron", "dftk_eri_blocks",
     "dftk_jk_workspace_bytes", "dftk_jk_workspace_bytes_queue", "dftk_jk", "dftk_nuclear_kernel", "dftk_eri_kernel",
     "dftk_fma_burn", "dftk_jk_timing", "dftk_jk_timing_read", "dftk_jk_noalloc", "dftk_grad", "dftk_workspace_bytes",
+    "dftk_set_launch", "dftk_get_launch",
 )
 
 
@@ -122,6 +123,8 @@ def load() -> ctypes.CDLL:
         "dftk_jk_workspace_bytes": ([i, i], sz),
         "dftk_jk_workspace_bytes_queue": ([i, i, ctypes.POINTER(Queue)], sz),
         "dftk_workspace_bytes": ([ctypes.POINTER(Shells), ctypes.POINTER(Queue)], sz),
+        "dftk_set_launch": ([i, i, i, i, i], i),
+        "dftk_get_launch": ([i, i, i, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)], i),
         "dftk_jk": ([ctypes.POINTER(Shells), ctypes.POINTER(Pairs), ctypes.POINTER(Queue), vp, vp, vp,
                      vp, vp, vp, i, d, d, vp, sz, vp, vp], i),
         "dftk_nuclear_kernel": ([vp] * 8 + [i, i, i] + [vp] * 9 + [vp], i),

@@ -386,7 +386,7 @@ def _batched_diis(Fh: torch.Tensor, Eh: torch.Tensor, n: int) -> torch.Tensor:
 
 def scf_rhf_batch(eng: BatchEngine, charges: Optional[Sequence[int]] = None, diis: int = 8, etol: float = 1e-10,
                   dtol: float = 1e-8, max_iter: int = 100, tau: float = 1e-12, rebuild_every: int = 12,
-                  finish_factor: float = 100.0, use_graph: bool = True) -> BatchSCFResult:
+                  finish_factor: float = 100.0, use_graph: bool = True, autotune: bool = False) -> BatchSCFResult:
     """Closed-shell SCF of every molecule of the batch at once (same criteria
     as scf.scf_rhf: DIIS(8), |dE| < etol and RMS(dD) < dtol on a full FP64
     Fock build, incremental builds F_k = F_{k-1} + G(D_k - D_{k-1}) in between,
@@ -418,6 +418,13 @@ def scf_rhf_batch(eng: BatchEngine, charges: Optional[Sequence[int]] = None, dii
         return (X @ Dp @ Xt) * rmask
 
     D = density(H)
+    if autotune:
+        # launch shapes per class measured on this batch's first (full) build,
+        # fixed before the graph captures them
+        from . import autotune as _autotune
+
+        Dp0 = eng.to_packed(D)
+        _autotune.tune(eng, lambda: eng.jk(2.0 * Dp0, Dp0, tau=tau), _autotune.FAMILY_JK, repeats=1)
     graph = _FockGraph(eng, tau) if use_graph else None
 
     def build(Dp):

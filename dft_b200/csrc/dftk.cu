@@ -111,6 +111,57 @@ int ensure_init()
     return DFTK_OK;
 }
 
+// Launch shapes of the quartet kernels, per (family, class, precision):
+// threads per block (64 or 128) and resident blocks per SM of the grid cap.
+// Set by dftk_set_launch (the autotuner); read at every launch.
+struct LaunchShape {
+    int threads;
+    int blocks_per_sm;
+};
+LaunchShape g_shape[DFTK_N_FAMILY][DFTK_N_QCLASS][2];
+bool g_shape_init = false;
+std::mutex g_shape_mutex;
+int g_sm_count = 0;
+
+void init_shapes_locked()
+{
+    if (g_shape_init) return;
+    for (int c = 0; c < DFTK_N_QCLASS; ++c)
+        for (int p = 0; p < 2; ++p) {
+            g_shape[DFTK_FAMILY_JK][c][p] = {128, 16};
+            g_shape[DFTK_FAMILY_GRAD][c][p] = {128, 8};
+        }
+    g_shape_init = true;
+}
+
+LaunchShape launch_shape(int family, int c, int fp32)
+{
+    std::lock_guard<std::mutex> lock(g_shape_mutex);
+    init_shapes_locked();
+    return g_shape[family][c][fp32 ? 1 : 0];
+}
+
+int sm_count()
+{
+    if (g_sm_count > 0) return g_sm_count;
+    int dev = 0, n = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+        n > 0)
+        g_sm_count = n;
+    return g_sm_count > 0 ? g_sm_count : 148;
+}
+
+// grid of a quartet kernel: enough blocks for `threads_needed` threads, at
+// most blocks_per_sm x SM count
+unsigned shaped_grid(const LaunchShape &sh, long long threads_needed)
+{
+    long long blocks = (threads_needed + sh.threads - 1) / sh.threads;
+    const long long cap = (long long)sm_count() * sh.blocks_per_sm;
+    if (blocks > cap) blocks = cap;
+    if (blocks < 1) blocks = 1;
+    return (unsigned)blocks;
+}
+
 #define DFTK_INIT()                                                         \
     do {                                                                    \
         int s_ = ensure_init();                                             \
@@ -171,11 +222,10 @@ int launch_jk_list_class(const JkParams &P, cudaStream_t s)
     if (g_timing.enabled) g_timing.launched[slot] = false;
     if (ncand <= 0) return DFTK_OK;
     const long long warps = ((ncand + 31) / 32) * EriClass<T, C, 0>::NSPLIT;
-    long long blocks = (warps * 32 + 127) / 128;
-    const long long cap = 148LL * 16;
-    if (blocks > cap) blocks = cap;
+    const LaunchShape sh = launch_shape(DFTK_FAMILY_JK, C, sizeof(T) == 4);
+    const unsigned blocks = shaped_grid(sh, warps * 32);
     if (g_timing.enabled) DFTK_CUDA(cudaEventRecord(g_timing.start[slot], s));
-    k_jk_list<C, T><<<(unsigned)blocks, 128, 0, s>>>(P);
+    k_jk_list<C, T><<<blocks, sh.threads, 0, s>>>(P);
     DFTK_LAUNCHED("k_jk_list");
     if (g_timing.enabled) {
         DFTK_CUDA(cudaEventRecord(g_timing.stop[slot], s));
@@ -537,6 +587,30 @@ int dftk_jk_timing_read(float *ms, int n)
     return DFTK_OK;
 }
 
+int dftk_set_launch(int family, int qclass, int fp32, int threads, int blocks_per_sm)
+{
+    if (family < 0 || family >= DFTK_N_FAMILY || qclass < 0 || qclass >= DFTK_N_QCLASS || (fp32 != 0 && fp32 != 1))
+        return fail(DFTK_ERR_ARG, "dftk_set_launch: bad family / class / precision");
+    if ((threads != 64 && threads != 128) || blocks_per_sm < 1 || blocks_per_sm > 32)
+        return fail(DFTK_ERR_ARG, "dftk_set_launch: threads must be 64 or 128, blocks_per_sm 1..32");
+    std::lock_guard<std::mutex> lock(g_shape_mutex);
+    init_shapes_locked();
+    g_shape[family][qclass][fp32] = {threads, blocks_per_sm};
+    return DFTK_OK;
+}
+
+int dftk_get_launch(int family, int qclass, int fp32, int *threads, int *blocks_per_sm)
+{
+    if (family < 0 || family >= DFTK_N_FAMILY || qclass < 0 || qclass >= DFTK_N_QCLASS || (fp32 != 0 && fp32 != 1) ||
+        !threads || !blocks_per_sm)
+        return fail(DFTK_ERR_ARG, "dftk_get_launch: bad arguments");
+    std::lock_guard<std::mutex> lock(g_shape_mutex);
+    init_shapes_locked();
+    *threads = g_shape[family][qclass][fp32].threads;
+    *blocks_per_sm = g_shape[family][qclass][fp32].blocks_per_sm;
+    return DFTK_OK;
+}
+
 int dftk_grad(const dftk_shells_t *shells, const int *shell_atom, int n_atoms, const double *atom_xyz,
               const double *atom_z, const dftk_pairs_t pairs[DFTK_N_PCLASS], const dftk_queue_t *queue,
               const double *D, const double *D_a, const double *D_b, const double *W, double tau, double *grad,
@@ -557,7 +631,7 @@ int dftk_grad(const dftk_shells_t *shells, const int *shell_atom, int n_atoms, c
     if (ns == 0) return DFTK_OK;
     // block-private gradient copies in shared memory when they fit
     const size_t smem = n_atoms <= GRAD_SMEM_ATOMS ? 3 * sizeof(double) * n_atoms : 0;
-    const long long cap = 148LL * 8;
+    const long long cap = (long long)sm_count() * 8;
     const int nat_stride = shells->mol ? shells->max_natom : n_atoms;
     auto grid = [cap](long long work) {
         long long b = (work + GRAD_THREADS - 1) / GRAD_THREADS;
@@ -662,10 +736,12 @@ int dftk_grad(const dftk_shells_t *shells, const int *shell_atom, int n_atoms, c
 #define DFTK_GRAD_LAUNCH(CC)                                                  \
     if (P.total[CC] > 0) {                                                    \
         if (timed) DFTK_CUDA(cudaEventRecord(g_timing.start[CC], s));         \
-        if (use_list)                                                         \
-            k_grad_eri<CC, true><<<grid(P.total[CC]), GRAD_THREADS, smem, s>>>(P);  \
-        else                                                                  \
+        if (use_list) {                                                       \
+            const LaunchShape gs = launch_shape(DFTK_FAMILY_GRAD, CC, 0);     \
+            k_grad_eri<CC, true><<<shaped_grid(gs, P.total[CC]), gs.threads, smem, s>>>(P); \
+        } else {                                                              \
             k_grad_eri<CC, false><<<grid(P.total[CC]), GRAD_THREADS, smem, s>>>(P); \
+        }                                                                     \
         DFTK_LAUNCHED("k_grad_eri");                                          \
         if (timed) {                                                          \
             DFTK_CUDA(cudaEventRecord(g_timing.stop[CC], s));                 \

@@ -222,6 +222,19 @@ int dftk_jk_noalloc(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N
 int dftk_jk_timing(int enable);
 int dftk_jk_timing_read(float *ms, int n);
 
+/* Launch shapes of the quartet kernels (no counterpart in the reference):
+ * per kernel family, quartet class and precision (fp32 0/1), the threads per
+ * block (64 or 128) and the grid cap in resident blocks per SM (1..32).  The
+ * autotuner (dft_b200/autotune.py) times candidates and sets the fastest;
+ * the table is process-wide, guarded by a mutex, and read at each launch, so
+ * set it before capturing a CUDA graph.  Defaults: J/K 128 x 16, gradient
+ * 128 x 8. */
+#define DFTK_FAMILY_JK 0      /* dftk_jk class kernels (list path) */
+#define DFTK_FAMILY_GRAD 1    /* dftk_grad class kernels (list path; fp32 = 0 only) */
+#define DFTK_N_FAMILY 2
+int dftk_set_launch(int family, int qclass, int fp32, int threads, int blocks_per_sm);
+int dftk_get_launch(int family, int qclass, int fp32, int *threads, int *blocks_per_sm);
+
 /* Analytic nuclear gradient (no counterpart in the reference): grad[3 * atom
  * + x] is overwritten with sum D dH/dX - sum W dS/dX + sum Gamma d(ab|cd)/dX
  * (electronic part; the nuclear repulsion term is the caller's).  D is the

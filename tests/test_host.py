@@ -190,3 +190,19 @@ def test_batched_diis_matches_single():
         for k in reversed(range(hist)):  # history index 0 is the newest
             d.push(F[k, b], E[k, b])
         assert torch.allclose(out[b], d.extrapolate(), atol=1e-10)
+
+
+def test_launch_shape_table_without_gpu():
+    """dftk_set_launch / dftk_get_launch are host-side: validated and read back."""
+    from dft_b200 import autotune
+
+    before = autotune.get_shapes(autotune.FAMILY_JK)
+    assert all(t in (64, 128) and 1 <= b <= 32 for t, b in before)
+    autotune.set_shapes(autotune.FAMILY_JK, [(64, 8)] * 6)
+    assert autotune.get_shapes(autotune.FAMILY_JK) == [(64, 8)] * 6
+    autotune.set_shapes(autotune.FAMILY_JK, before)
+    lib = _lib.load()
+    assert lib.dftk_set_launch(0, 0, 0, 96, 4) == _lib.ERR_ARG
+    assert lib.dftk_set_launch(0, 6, 0, 128, 4) == _lib.ERR_ARG
+    assert lib.dftk_set_launch(2, 0, 0, 128, 4) == _lib.ERR_ARG
+    assert lib.dftk_set_launch(1, 0, 0, 128, 33) == _lib.ERR_ARG
