@@ -45,16 +45,22 @@ struct EriClass<T, 0, 0> {
       const T kp = __ldg(krec + 3 * ket_fs);
       const T kK = __ldg(krec + 4 * ket_fs);
       T V0_000 = T(0);
+      float bnq = __ldg(bra_qp);
+      T bnPx = __ldg(bra_p + 0), bnPy = __ldg(bra_p + bra_fs), bnPz = __ldg(bra_p + 2 * bra_fs), bnp = __ldg(bra_p + 3 * bra_fs), bnK = __ldg(bra_p + 4 * bra_fs);
       #pragma unroll 1
       for (int i = 0; i < bra_n; ++i) {
-        if (qo * __ldg(bra_qp + i * bra_st) < eps) break;
+        const float bcq = bnq;
+        const T bPx = bnPx, bPy = bnPy, bPz = bnPz, bp = bnp, bK = bnK;
+        if (qo * bcq < eps) break;
+        const int in = i + 1 < bra_n ? i + 1 : i;
+        bnq = __ldg(bra_qp + in * bra_st);
+        const T* __restrict__ bnrec = bra_p + in * bra_st;
+        bnPx = __ldg(bnrec + 0);
+        bnPy = __ldg(bnrec + bra_fs);
+        bnPz = __ldg(bnrec + 2 * bra_fs);
+        bnp = __ldg(bnrec + 3 * bra_fs);
+        bnK = __ldg(bnrec + 4 * bra_fs);
         ++evaluated;
-        const T* __restrict__ brec = bra_p + i * bra_st;
-        const T bPx = __ldg(brec + 0);
-        const T bPy = __ldg(brec + bra_fs);
-        const T bPz = __ldg(brec + 2 * bra_fs);
-        const T bp = __ldg(brec + 3 * bra_fs);
-        const T bK = __ldg(brec + 4 * bra_fs);
         const T s = bp + kp;
         const T rs = Math<T>::rsqrt(s);
         const T rho = bp * kp * (rs * rs);
@@ -348,16 +354,22 @@ struct EriClass<T, 3, 0> {
       const T bEz1 = bh * (bAz + bBz);
       const T bh2 = bh * bh;
       T W0_000 = T(0), W0_001 = T(0), W0_002 = T(0), W0_010 = T(0), W0_011 = T(0), W0_020 = T(0), W0_100 = T(0), W0_101 = T(0), W0_110 = T(0), W0_200 = T(0);
+      float knq = __ldg(ket_qp);
+      T knPx = __ldg(ket_p + 0), knPy = __ldg(ket_p + ket_fs), knPz = __ldg(ket_p + 2 * ket_fs), knp = __ldg(ket_p + 3 * ket_fs), knK = __ldg(ket_p + 4 * ket_fs);
       #pragma unroll 1
       for (int j = 0; j < ket_n; ++j) {
-        if (qo * __ldg(ket_qp + j * ket_st) < eps) break;
+        const float kcq = knq;
+        const T kPx = knPx, kPy = knPy, kPz = knPz, kp = knp, kK = knK;
+        if (qo * kcq < eps) break;
+        const int jn = j + 1 < ket_n ? j + 1 : j;
+        knq = __ldg(ket_qp + jn * ket_st);
+        const T* __restrict__ knrec = ket_p + jn * ket_st;
+        knPx = __ldg(knrec + 0);
+        knPy = __ldg(knrec + ket_fs);
+        knPz = __ldg(knrec + 2 * ket_fs);
+        knp = __ldg(knrec + 3 * ket_fs);
+        knK = __ldg(knrec + 4 * ket_fs);
         ++evaluated;
-        const T* __restrict__ krec = ket_p + j * ket_st;
-        const T kPx = __ldg(krec + 0);
-        const T kPy = __ldg(krec + ket_fs);
-        const T kPz = __ldg(krec + 2 * ket_fs);
-        const T kp = __ldg(krec + 3 * ket_fs);
-        const T kK = __ldg(krec + 4 * ket_fs);
         const T s = bp + kp;
         const T rs = Math<T>::rsqrt(s);
         const T rho = bp * kp * (rs * rs);
@@ -775,23 +787,29 @@ struct EriClass<T, 5, 0> {
       T W0_000 = T(0), W0_001 = T(0), W0_002 = T(0), W0_010 = T(0), W0_011 = T(0), W0_020 = T(0), W0_100 = T(0), W0_101 = T(0), W0_110 = T(0), W0_200 = T(0);
       T W1_000 = T(0), W1_001 = T(0), W1_002 = T(0), W1_010 = T(0), W1_011 = T(0), W1_020 = T(0), W1_100 = T(0), W1_101 = T(0), W1_110 = T(0), W1_200 = T(0);
       T W2_000 = T(0), W2_001 = T(0), W2_002 = T(0), W2_010 = T(0), W2_011 = T(0), W2_020 = T(0), W2_100 = T(0), W2_101 = T(0), W2_110 = T(0), W2_200 = T(0);
+      float knq = __ldg(ket_qp);
+      T knPx = __ldg(ket_p + 0), knPy = __ldg(ket_p + ket_fs), knPz = __ldg(ket_p + 2 * ket_fs), knp = __ldg(ket_p + 3 * ket_fs), knK = __ldg(ket_p + 4 * ket_fs), knh = __ldg(ket_p + 5 * ket_fs), knAx = __ldg(ket_p + 6 * ket_fs), knAy = __ldg(ket_p + 7 * ket_fs), knAz = __ldg(ket_p + 8 * ket_fs), knBx = __ldg(ket_p + 9 * ket_fs), knBy = __ldg(ket_p + 10 * ket_fs), knBz = __ldg(ket_p + 11 * ket_fs);
       #pragma unroll 1
       for (int j = 0; j < ket_n; ++j) {
-        if (qo * __ldg(ket_qp + j * ket_st) < eps) break;
+        const float kcq = knq;
+        const T kPx = knPx, kPy = knPy, kPz = knPz, kp = knp, kK = knK, kh = knh, kAx = knAx, kAy = knAy, kAz = knAz, kBx = knBx, kBy = knBy, kBz = knBz;
+        if (qo * kcq < eps) break;
+        const int jn = j + 1 < ket_n ? j + 1 : j;
+        knq = __ldg(ket_qp + jn * ket_st);
+        const T* __restrict__ knrec = ket_p + jn * ket_st;
+        knPx = __ldg(knrec + 0);
+        knPy = __ldg(knrec + ket_fs);
+        knPz = __ldg(knrec + 2 * ket_fs);
+        knp = __ldg(knrec + 3 * ket_fs);
+        knK = __ldg(knrec + 4 * ket_fs);
+        knh = __ldg(knrec + 5 * ket_fs);
+        knAx = __ldg(knrec + 6 * ket_fs);
+        knAy = __ldg(knrec + 7 * ket_fs);
+        knAz = __ldg(knrec + 8 * ket_fs);
+        knBx = __ldg(knrec + 9 * ket_fs);
+        knBy = __ldg(knrec + 10 * ket_fs);
+        knBz = __ldg(knrec + 11 * ket_fs);
         ++evaluated;
-        const T* __restrict__ krec = ket_p + j * ket_st;
-        const T kPx = __ldg(krec + 0);
-        const T kPy = __ldg(krec + ket_fs);
-        const T kPz = __ldg(krec + 2 * ket_fs);
-        const T kp = __ldg(krec + 3 * ket_fs);
-        const T kK = __ldg(krec + 4 * ket_fs);
-        const T kh = __ldg(krec + 5 * ket_fs);
-        const T kAx = __ldg(krec + 6 * ket_fs);
-        const T kAy = __ldg(krec + 7 * ket_fs);
-        const T kAz = __ldg(krec + 8 * ket_fs);
-        const T kBx = __ldg(krec + 9 * ket_fs);
-        const T kBy = __ldg(krec + 10 * ket_fs);
-        const T kBz = __ldg(krec + 11 * ket_fs);
         const T kEx0 = kAx * kBx + kh;
         const T kEx1 = kh * (kAx + kBx);
         const T kEy0 = kAy * kBy + kh;
@@ -1158,23 +1176,29 @@ struct EriClass<T, 5, 1> {
       T W0_000 = T(0), W0_001 = T(0), W0_002 = T(0), W0_010 = T(0), W0_011 = T(0), W0_020 = T(0), W0_100 = T(0), W0_101 = T(0), W0_110 = T(0), W0_200 = T(0);
       T W1_000 = T(0), W1_001 = T(0), W1_002 = T(0), W1_010 = T(0), W1_011 = T(0), W1_020 = T(0), W1_100 = T(0), W1_101 = T(0), W1_110 = T(0), W1_200 = T(0);
       T W2_000 = T(0), W2_001 = T(0), W2_002 = T(0), W2_010 = T(0), W2_011 = T(0), W2_020 = T(0), W2_100 = T(0), W2_101 = T(0), W2_110 = T(0), W2_200 = T(0);
+      float knq = __ldg(ket_qp);
+      T knPx = __ldg(ket_p + 0), knPy = __ldg(ket_p + ket_fs), knPz = __ldg(ket_p + 2 * ket_fs), knp = __ldg(ket_p + 3 * ket_fs), knK = __ldg(ket_p + 4 * ket_fs), knh = __ldg(ket_p + 5 * ket_fs), knAx = __ldg(ket_p + 6 * ket_fs), knAy = __ldg(ket_p + 7 * ket_fs), knAz = __ldg(ket_p + 8 * ket_fs), knBx = __ldg(ket_p + 9 * ket_fs), knBy = __ldg(ket_p + 10 * ket_fs), knBz = __ldg(ket_p + 11 * ket_fs);
       #pragma unroll 1
       for (int j = 0; j < ket_n; ++j) {
-        if (qo * __ldg(ket_qp + j * ket_st) < eps) break;
+        const float kcq = knq;
+        const T kPx = knPx, kPy = knPy, kPz = knPz, kp = knp, kK = knK, kh = knh, kAx = knAx, kAy = knAy, kAz = knAz, kBx = knBx, kBy = knBy, kBz = knBz;
+        if (qo * kcq < eps) break;
+        const int jn = j + 1 < ket_n ? j + 1 : j;
+        knq = __ldg(ket_qp + jn * ket_st);
+        const T* __restrict__ knrec = ket_p + jn * ket_st;
+        knPx = __ldg(knrec + 0);
+        knPy = __ldg(knrec + ket_fs);
+        knPz = __ldg(knrec + 2 * ket_fs);
+        knp = __ldg(knrec + 3 * ket_fs);
+        knK = __ldg(knrec + 4 * ket_fs);
+        knh = __ldg(knrec + 5 * ket_fs);
+        knAx = __ldg(knrec + 6 * ket_fs);
+        knAy = __ldg(knrec + 7 * ket_fs);
+        knAz = __ldg(knrec + 8 * ket_fs);
+        knBx = __ldg(knrec + 9 * ket_fs);
+        knBy = __ldg(knrec + 10 * ket_fs);
+        knBz = __ldg(knrec + 11 * ket_fs);
         ++evaluated;
-        const T* __restrict__ krec = ket_p + j * ket_st;
-        const T kPx = __ldg(krec + 0);
-        const T kPy = __ldg(krec + ket_fs);
-        const T kPz = __ldg(krec + 2 * ket_fs);
-        const T kp = __ldg(krec + 3 * ket_fs);
-        const T kK = __ldg(krec + 4 * ket_fs);
-        const T kh = __ldg(krec + 5 * ket_fs);
-        const T kAx = __ldg(krec + 6 * ket_fs);
-        const T kAy = __ldg(krec + 7 * ket_fs);
-        const T kAz = __ldg(krec + 8 * ket_fs);
-        const T kBx = __ldg(krec + 9 * ket_fs);
-        const T kBy = __ldg(krec + 10 * ket_fs);
-        const T kBz = __ldg(krec + 11 * ket_fs);
         const T kEx0 = kAx * kBx + kh;
         const T kEx1 = kh * (kAx + kBx);
         const T kEy0 = kAy * kBy + kh;
@@ -1535,23 +1559,29 @@ struct EriClass<T, 5, 2> {
       T W0_000 = T(0), W0_001 = T(0), W0_002 = T(0), W0_010 = T(0), W0_011 = T(0), W0_020 = T(0), W0_100 = T(0), W0_101 = T(0), W0_110 = T(0), W0_200 = T(0);
       T W1_000 = T(0), W1_001 = T(0), W1_002 = T(0), W1_010 = T(0), W1_011 = T(0), W1_020 = T(0), W1_100 = T(0), W1_101 = T(0), W1_110 = T(0), W1_200 = T(0);
       T W2_000 = T(0), W2_001 = T(0), W2_002 = T(0), W2_010 = T(0), W2_011 = T(0), W2_020 = T(0), W2_100 = T(0), W2_101 = T(0), W2_110 = T(0), W2_200 = T(0);
+      float knq = __ldg(ket_qp);
+      T knPx = __ldg(ket_p + 0), knPy = __ldg(ket_p + ket_fs), knPz = __ldg(ket_p + 2 * ket_fs), knp = __ldg(ket_p + 3 * ket_fs), knK = __ldg(ket_p + 4 * ket_fs), knh = __ldg(ket_p + 5 * ket_fs), knAx = __ldg(ket_p + 6 * ket_fs), knAy = __ldg(ket_p + 7 * ket_fs), knAz = __ldg(ket_p + 8 * ket_fs), knBx = __ldg(ket_p + 9 * ket_fs), knBy = __ldg(ket_p + 10 * ket_fs), knBz = __ldg(ket_p + 11 * ket_fs);
       #pragma unroll 1
       for (int j = 0; j < ket_n; ++j) {
-        if (qo * __ldg(ket_qp + j * ket_st) < eps) break;
+        const float kcq = knq;
+        const T kPx = knPx, kPy = knPy, kPz = knPz, kp = knp, kK = knK, kh = knh, kAx = knAx, kAy = knAy, kAz = knAz, kBx = knBx, kBy = knBy, kBz = knBz;
+        if (qo * kcq < eps) break;
+        const int jn = j + 1 < ket_n ? j + 1 : j;
+        knq = __ldg(ket_qp + jn * ket_st);
+        const T* __restrict__ knrec = ket_p + jn * ket_st;
+        knPx = __ldg(knrec + 0);
+        knPy = __ldg(knrec + ket_fs);
+        knPz = __ldg(knrec + 2 * ket_fs);
+        knp = __ldg(knrec + 3 * ket_fs);
+        knK = __ldg(knrec + 4 * ket_fs);
+        knh = __ldg(knrec + 5 * ket_fs);
+        knAx = __ldg(knrec + 6 * ket_fs);
+        knAy = __ldg(knrec + 7 * ket_fs);
+        knAz = __ldg(knrec + 8 * ket_fs);
+        knBx = __ldg(knrec + 9 * ket_fs);
+        knBy = __ldg(knrec + 10 * ket_fs);
+        knBz = __ldg(knrec + 11 * ket_fs);
         ++evaluated;
-        const T* __restrict__ krec = ket_p + j * ket_st;
-        const T kPx = __ldg(krec + 0);
-        const T kPy = __ldg(krec + ket_fs);
-        const T kPz = __ldg(krec + 2 * ket_fs);
-        const T kp = __ldg(krec + 3 * ket_fs);
-        const T kK = __ldg(krec + 4 * ket_fs);
-        const T kh = __ldg(krec + 5 * ket_fs);
-        const T kAx = __ldg(krec + 6 * ket_fs);
-        const T kAy = __ldg(krec + 7 * ket_fs);
-        const T kAz = __ldg(krec + 8 * ket_fs);
-        const T kBx = __ldg(krec + 9 * ket_fs);
-        const T kBy = __ldg(krec + 10 * ket_fs);
-        const T kBz = __ldg(krec + 11 * ket_fs);
         const T kEx0 = kAx * kBx + kh;
         const T kEx1 = kh * (kAx + kBx);
         const T kEy0 = kAy * kBy + kh;

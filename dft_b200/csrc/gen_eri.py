@@ -42,6 +42,9 @@ CLASSES = [
     (1, 1, 1, 1, 3, "bra"),
 ]
 PAIR_FIELDS = {0: 5, 1: 9, 2: 12}  # record fields the ERI code loads (the stored records add alpha last)
+# classes whose inner primitive loop loads the next primitive pair's record
+# one iteration ahead
+PREFETCH_CLASSES = {0, 3, 5}  # measured on B200: the others lose more to register spills
 
 
 def e1d(side, a, b, axis):
@@ -142,6 +145,34 @@ def side_loads(side, pc, var, idx):
     return out
 
 
+def side_fields(pc, var):
+    """(name, offset expression) of the record fields a pair class reads."""
+    names = ["Px", "Py", "Pz", "p", "K", "h", "Ax", "Ay", "Az", "Bx", "By", "Bz"]
+    return [(names[f], "0" if f == 0 else (f"{var}_fs" if f == 1 else f"{f} * {var}_fs"))
+            for f in range(PAIR_FIELDS[pc])]
+
+
+def prefetched_inner_loop(side, pc, var, idx, n, qo, other_q):
+    """Head of an inner primitive loop whose record fields and primitive
+    Schwarz factor are loaded one iteration ahead (software pipelining: the
+    loads of primitive j + 1 are in flight while primitive j is computed)."""
+    f = side_fields(pc, var)
+    q = f"{var}_qp"
+    out = [f"float {side}nq = __ldg({q});"]
+    out.append("T " + ", ".join(f"{side}n{nm} = __ldg({var}_p + {off})" for nm, off in f) + ";")
+    out.append("#pragma unroll 1")
+    out.append(f"for (int {idx} = 0; {idx} < {n}; ++{idx}) {{")
+    out.append(f"  const float {side}cq = {side}nq;")
+    out.append("  const T " + ", ".join(f"{side}{nm} = {side}n{nm}" for nm, _ in f) + ";")
+    out.append(f"  if ({qo} * {side}cq < eps) break;")
+    out.append(f"  const int {idx}n = {idx} + 1 < {n} ? {idx} + 1 : {idx};")
+    out.append(f"  {side}nq = __ldg({q} + {idx}n * {var}_st);")
+    out.append(f"  const T* __restrict__ {side}nrec = {var}_p + {idx}n * {var}_st;")
+    for nm, off in f:
+        out.append(f"  {side}n{nm} = __ldg({side}nrec + {off});")
+    return out
+
+
 def side_pre(side, pc):
     lines = []
     if pc == 2:
@@ -153,6 +184,7 @@ def side_pre(side, pc):
 
 
 def gen_class(cid, la, lb, lc, ld, nsplit, split, order):
+    PREFETCH = cid in PREFETCH_CLASSES
     """order 'bra': bra primitive loop outside, the ket transform per primitive
     quartet and the bra transform hoisted; order 'ket': the mirror image (ket
     records loaded once per quartet, bra records re-read as warp-broadcast)."""
@@ -195,11 +227,16 @@ def gen_class(cid, la, lb, lc, ld, nsplit, split, order):
         body += ["  " + x for x in side_loads("b", pa, "bra", "i") + side_pre("b", pa)]
         for m in range(len(cds)):
             body.append("  T " + ", ".join(f"{w(m, h)} = T(0)" for h in hb) + ";")
-        body.append("  #pragma unroll 1")
-        body.append("  for (int j = 0; j < ket_n; ++j) {")
-        body.append("    if (qo * __ldg(ket_qp + j * ket_st) < eps) break;")
-        body.append("    ++evaluated;")
-        inner = side_loads("k", pk, "ket", "j") + side_pre("k", pk) + list(core)
+        if PREFETCH:
+            body += ["  " + x for x in prefetched_inner_loop("k", pk, "ket", "j", "ket_n", "qo", "ket_qp")]
+            body.append("    ++evaluated;")
+            inner = side_pre("k", pk) + list(core)
+        else:
+            body.append("  #pragma unroll 1")
+            body.append("  for (int j = 0; j < ket_n; ++j) {")
+            body.append("    if (qo * __ldg(ket_qp + j * ket_st) < eps) break;")
+            body.append("    ++evaluated;")
+            inner = side_loads("k", pk, "ket", "j") + side_pre("k", pk) + list(core)
         for m, terms in ket_terms.items():
             for (tk, uk, vk), sg, facs in terms:
                 cname = f"kc{m}_{tk}{uk}{vk}"
@@ -231,11 +268,16 @@ def gen_class(cid, la, lb, lc, ld, nsplit, split, order):
         body += ["  " + x for x in side_loads("k", pk, "ket", "j") + side_pre("k", pk)]
         for n in range(len(abs_)):
             body.append("  T " + ", ".join(f"{w(n, h)} = T(0)" for h in hk) + ";")
-        body.append("  #pragma unroll 1")
-        body.append("  for (int i = 0; i < bra_n; ++i) {")
-        body.append("    if (qo * __ldg(bra_qp + i * bra_st) < eps) break;")
-        body.append("    ++evaluated;")
-        inner = side_loads("b", pa, "bra", "i") + side_pre("b", pa) + list(core)
+        if PREFETCH:
+            body += ["  " + x for x in prefetched_inner_loop("b", pa, "bra", "i", "bra_n", "qo", "bra_qp")]
+            body.append("    ++evaluated;")
+            inner = side_pre("b", pa) + list(core)
+        else:
+            body.append("  #pragma unroll 1")
+            body.append("  for (int i = 0; i < bra_n; ++i) {")
+            body.append("    if (qo * __ldg(bra_qp + i * bra_st) < eps) break;")
+            body.append("    ++evaluated;")
+            inner = side_loads("b", pa, "bra", "i") + side_pre("b", pa) + list(core)
         for n, terms in bra_terms.items():
             for (tb, ub, vb), _, facs in terms:
                 cname = f"bc{n}_{tb}{ub}{vb}"

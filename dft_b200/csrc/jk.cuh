@@ -352,9 +352,16 @@ __device__ __forceinline__ void jk_one(const JkParams &P, bool valid, int row, i
     T I[E::NI];
     int evaluated = 0;
     if (valid) {
+        // FP32 quartets (bound Q_ab Q_cd max|D| < tau_fp32): also skip the
+        // primitive quartets whose qp product is below 2^-20 Q_ab Q_cd, i.e.
+        // whose share of the quartet is below a few FP32 roundings; with the
+        // bound below tau_fp32 that is < 1e-12 absolute per quartet
+        float eps = P.tau_prim;
+        if constexpr (sizeof(T) == 4)
+            eps = fmaxf(eps, 9.5367431640625e-7f * (float)(__ldg(P.q[X] + row) * __ldg(P.q[Yc] + ket)));
         evaluated = eri_run<C, T, S>(RecOf<C, T>::get(P, X), P.qp[X], P.n_pairs[X], P.kmax[X], row, P.np[X][row],
                                      RecOf<C, T>::get(P, Yc), P.qp[Yc], P.n_pairs[Yc], P.kmax[Yc], ket,
-                                     P.np[Yc][ket], P.tau_prim, I);
+                                     P.np[Yc][ket], eps, I);
     } else {
 #pragma unroll
         for (int q = 0; q < E::NI; ++q) I[q] = T(0);
