@@ -430,8 +430,17 @@ def run_dftk_arm(args, rank, world, local_rank):
     J = torch.empty((N, N), dtype=torch.float64, device="cuda")
     Ka = torch.empty((N, N), dtype=torch.float64, device="cuda")
 
+    shard = None
+    if dist is not None and args.shard:
+        from dft_b200.sharding import ShardedFock
+
+        shard = ShardedFock(eng)
+
     def build():
-        eng.jk(Dt, D, tau=1e-14, out=(J, Ka, None))
+        if shard is not None:
+            shard.jk(Dt, D, tau=1e-14)
+        else:
+            eng.jk(Dt, D, tau=1e-14, out=(J, Ka, None))
 
     for _ in range(max(args.warmup, 3)):
         build()
@@ -484,7 +493,10 @@ def run_dftk_arm(args, rank, world, local_rank):
         tot_ms = float(t.item())
         dist.barrier()
     ms_per_step = tot_ms / args.steps
-    value = world * args.steps / (tot_ms / 1e3)
+    plain_rate = args.steps / (tot_ms / 1e3)  # builds/s of one system on this configuration
+    # replicas: every rank builds the whole system (N builds per step);
+    # sharded: the ranks build one system together (one build per step)
+    value = (1 if shard is not None else world) * args.steps / (tot_ms / 1e3)
 
     # e2e through the reference-facing call with host arrays
     Dh = D.cpu().numpy()
@@ -536,13 +548,16 @@ def run_dftk_arm(args, rank, world, local_rank):
             cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "strong" if shard is not None else "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "molecule": "(H2O)_64 4x4x4 lattice seed 0", "basis": "STO-3G",
                        "n_basis": N, "tau_schwarz": 1e-12, "tau_density": 1e-14,
                        "quartets_per_class": eng.quartet_totals(), "evaluated_per_class": evaluated,
                        "primitive_quartets_per_class": prim_evaluated, "tau_prim": eng.tau_prim,
-                       "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}"},
+                       "l2": "flushed between steps (256 MB write)",
+                       "parallelism": (f"candidate space sharded x{world}, NCCL all-reduce of J/K" if shard is not None
+                                       else f"replicas x{world}")},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * N * N * 8,
                     "d2h_bytes_per_step": 3 * N * N * 8, "call": "shelled.fill_matrices (host NumPy arrays)"},
             "gpu_launches": args.steps * (2 + sum(1 for c in range(6) if eng.quartet_totals()[c] > 0)),
@@ -553,9 +568,9 @@ def run_dftk_arm(args, rank, world, local_rank):
                          "whole_build_tflops": total_flops / (ms_per_step / 1e3) / 1e12,
                          "class_ms": {QCLASS_NAMES[c]: float(class_ms[c]) for c in range(6)},
                          "fp32_peak_tflops": fp32_peak, "hbm_peak_gbs": peaks.get("hbm_gbs")},
-            "mixed": {"plain_fp64_builds_per_s": value / world,
+            "mixed": {"plain_fp64_builds_per_s": plain_rate,
                       "fp64_incremental_builds_per_s": i64, "mixed_incremental_builds_per_s": imx,
-                      "speedup_mixed_vs_plain_fp64": imx / (value / world),
+                      "speedup_mixed_vs_plain_fp64": imx / plain_rate,
                       "speedup_mixed_vs_fp64_incremental": imx / i64,
                       "incremental_builds": [r64.incremental_builds, rmx.incremental_builds],
                       "scf_builds_per_s_fp64": b64, "scf_builds_per_s_mixed": bmx,
@@ -587,7 +602,7 @@ def run_profile(args):
     """A few builds of the benchmark workload for ncu captures: two full FP64
     builds, then one mixed build of a scaled-down density (kernel launch order
     per build: k_dsh, k_select x6, k_jk_list<0..5,double>, [k_jk_list<0..5,float>],
-    k_symmetrize)."""
+    k_symmetrize), then one gradient."""
     import torch
 
     atoms, centers, shells, eng, S, H, enn, nocc = setup_workload(torch)
@@ -599,6 +614,10 @@ def run_profile(args):
         eng.jk(2 * D, D, tau=1e-14)
     dD = D * 1e-3
     eng.jk(2 * dD, dD, mixed=True, tau=1e-12, tau_fp32=1e-6)
+    # one analytic gradient at this (core-guess) density: launch order k_dsh,
+    # k_grad_overlap_kinetic/k_grad_nuclear x3, k_select x6, k_grad_eri<0..5>
+    Dt = (2 * D).contiguous()
+    eng.gradient(atoms, centers, Dt, D, D, Dt)
     torch.cuda.synchronize()
     print("profile workload done")
     return 0
@@ -612,6 +631,8 @@ def main():
     ap.add_argument("--impl", default="dftk", choices=["dftk", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the gradient and batch figures")
+    ap.add_argument("--shard", action="store_true",
+                    help="with N > 1: the ranks build one (H2O)_64 Fock matrix together (strong scaling)")
     ap.add_argument("--profile", action="store_true", help="only run a few builds (for ncu captures)")
     args = ap.parse_args()
     if args.profile:

@@ -52,6 +52,27 @@ def candidate_offsets(q_bra: np.ndarray, q_ket: np.ndarray, same_class: bool, ta
     return np.concatenate([[0], np.cumsum(cnt)]).astype(np.int64)
 
 
+def shard_row_offsets(row_off: np.ndarray, rank: int, world: int) -> np.ndarray:
+    """Row offsets of one rank's share of a class's candidate space.
+
+    Rows are split into `world` contiguous ranges holding equal numbers of
+    candidates (the range of rank r starts at the first row whose offset
+    reaches r/world of the total); rows outside the rank's range keep zero
+    candidates, so the kernels take the shard unchanged and every candidate
+    belongs to exactly one rank."""
+    off = np.asarray(row_off, dtype=np.int64)
+    total = int(off[-1])
+    n_rows = off.size - 1
+    bounds = [int(np.searchsorted(off[:-1], total * r // world, side="left")) if r < world else n_rows
+              for r in range(world + 1)]
+    bounds[0] = 0
+    lo, hi = bounds[rank], bounds[rank + 1]
+    cnt = np.diff(off)
+    mine = np.zeros_like(cnt)
+    mine[lo:hi] = cnt[lo:hi]
+    return np.concatenate([[0], np.cumsum(mine)]).astype(np.int64)
+
+
 def _dev(device) -> torch.device:
     if device is None:
         if not torch.cuda.is_available():
@@ -204,9 +225,28 @@ class IntegralEngine:
                   _lib.ptr(S), _lib.ptr(T), _lib.ptr(V), _lib.stream_handle())
         return S, T, V
 
+    def shard_queue(self, rank: int, world: int):
+        """A queue holding this rank's share of every class's candidates
+        (shard_row_offsets); pass it to jk(queue=...) and sum the partial J/K
+        over the ranks."""
+        q = _lib.Queue()
+        keep = []
+        for c in range(len(QCLASS_PAIRS)):
+            off = shard_row_offsets(self.row_off[c].cpu().numpy(), rank, world)
+            d_off = self._t(off, torch.int64)
+            keep.append(d_off)
+            q.n_rows[c] = self.c_queue.n_rows[c] if off[-1] > 0 else 0
+            q.total[c] = int(off[-1])
+            q.row_off[c] = _lib.ptr(d_off).value
+            q.ket_base[c] = self.c_queue.ket_base[c]
+        q.tau_prim = self.c_queue.tau_prim
+        q.mol_active = self.c_queue.mol_active
+        q._keep = keep  # device arrays live as long as the queue
+        return q
+
     def jk(self, D: torch.Tensor, D_a: Optional[torch.Tensor] = None, D_b: Optional[torch.Tensor] = None,
            uhf: bool = False, mixed: bool = False, tau: float = 1e-14, tau_fp32: float = 1e-6,
-           out=None, counts: Optional[torch.Tensor] = None, scan: bool = False):
+           out=None, counts: Optional[torch.Tensor] = None, scan: bool = False, queue=None):
         """Direct J, K_a (, K_b) for densities on the device.
 
         D is the density J is built from (the reference's P = P_a + P_b);
@@ -231,7 +271,8 @@ class IntegralEngine:
         else:
             J, Ka, Kb = out
         flags = (_lib.JK_UHF if uhf else 0) | (_lib.JK_MIXED if mixed else 0)
-        _lib.call("dftk_jk", ctypes.byref(self.c_shells), self.c_pairs, ctypes.byref(self.c_queue),
+        _lib.call("dftk_jk", ctypes.byref(self.c_shells), self.c_pairs,
+                  ctypes.byref(queue if queue is not None else self.c_queue),
                   _lib.ptr(D), _lib.ptr(D_a), _lib.ptr(D_b if uhf else None), _lib.ptr(J), _lib.ptr(Ka),
                   _lib.ptr(Kb if uhf else None), flags, float(tau), float(tau_fp32 if mixed else tau),
                   _lib.ptr(self.workspace), self.base_workspace_bytes if scan else self.workspace_bytes,
