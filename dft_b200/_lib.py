@@ -133,7 +133,7 @@ def load() -> ctypes.CDLL:
         "dftk_jk_noalloc": ([ctypes.POINTER(Shells), ctypes.POINTER(Pairs), ctypes.POINTER(Queue), vp, vp, vp,
                              vp, vp, vp, i, d, d, vp, vp], i),
         "dftk_grad": ([ctypes.POINTER(Shells), vp, i, vp, vp, ctypes.POINTER(Pairs), ctypes.POINTER(Queue), vp, vp,
-                       vp, vp, d, vp, vp, sz, vp], i),
+                       vp, vp, d, d, vp, vp, sz, vp], i),
         "dftk_jk_timing": ([i], i),
         "dftk_jk_timing_read": ([vp, i], i),
     }

@@ -249,14 +249,14 @@ class BatchEngine(IntegralEngine):
                   _lib.ptr(counts), _lib.stream_handle())
         return J, Ka, (Kb if uhf else Ka)
 
-    def gradient(self, D, D_a, D_b, W, tau: float = 1e-14) -> torch.Tensor:
+    def gradient(self, D, D_a, D_b, W, tau: float = 1e-14, tau_fp32: float = 0.0) -> torch.Tensor:
         """Electronic gradient of every atom of the batch, (total atoms, 3), on the device."""
         n = len(self.atoms)
         g = torch.zeros(3 * n, dtype=torch.float64, device=self.device)
         _lib.call("dftk_grad", ctypes.byref(self.c_shells), _lib.ptr(self.d_shell_atom), n,
                   _lib.ptr(self.d_atom_xyz), _lib.ptr(self.d_atom_z), self.c_pairs, ctypes.byref(self.c_queue),
                   _lib.ptr(self._square(D)), _lib.ptr(self._square(D_a)), _lib.ptr(self._square(D_b)),
-                  _lib.ptr(self._square(W)), float(tau), _lib.ptr(g), _lib.ptr(self.workspace),
+                  _lib.ptr(self._square(W)), float(tau), float(tau_fp32), _lib.ptr(g), _lib.ptr(self.workspace),
                   self.workspace_bytes, _lib.stream_handle())
         return g.view(n, 3)
 
@@ -508,7 +508,8 @@ def scf_rhf_batch(eng: BatchEngine, charges: Optional[Sequence[int]] = None, dii
                           t_fock, hist_active)
 
 
-def rhf_gradient_batch(eng: BatchEngine, res: BatchSCFResult, tau: float = 1e-14) -> List[np.ndarray]:
+def rhf_gradient_batch(eng: BatchEngine, res: BatchSCFResult, tau: float = 1e-14,
+                       tau_fp32: float = 0.0) -> List[np.ndarray]:
     """Analytic RHF gradients of every molecule of a converged batch, one
     dftk_grad call for the whole batch: per molecule an (n_atoms, 3) array.
     With D_alpha = C_occ C_occ^T of a converged F, the energy-weighted
@@ -518,5 +519,5 @@ def rhf_gradient_batch(eng: BatchEngine, res: BatchSCFResult, tau: float = 1e-14
     Dp = eng.to_packed(2.0 * Da)
     Wp = eng.to_packed(2.0 * (Da @ Fp @ Da))
     Dh = (0.5 * Dp).contiguous()
-    g = eng.gradient(Dp, Dh, Dh, Wp, tau=tau).cpu().numpy() + eng.nuclear_repulsion_gradient()
+    g = eng.gradient(Dp, Dh, Dh, Wp, tau=tau, tau_fp32=tau_fp32).cpu().numpy() + eng.nuclear_repulsion_gradient()
     return [g[int(eng.mol_atom0[m]):int(eng.mol_atom0[m] + eng.mol_natom[m])] for m in range(eng.n_mol)]

@@ -183,12 +183,14 @@ size_t ws_bytes(int ns, int n_ao)
 }
 
 // Optional per-class event timing of dftk_jk (dftk_jk_timing).
+// slots: FP64 class launches 0..5, FP32 ones 6..11, one-electron part of a gradient 12
+#define DFTK_TIMING_SLOTS (2 * DFTK_N_QCLASS + 1)
 struct JkTiming {
     bool enabled = false;
     bool created = false;
-    bool launched[2 * DFTK_N_QCLASS] = {false};
-    cudaEvent_t start[2 * DFTK_N_QCLASS];
-    cudaEvent_t stop[2 * DFTK_N_QCLASS];
+    bool launched[DFTK_TIMING_SLOTS] = {false};
+    cudaEvent_t start[DFTK_TIMING_SLOTS];
+    cudaEvent_t stop[DFTK_TIMING_SLOTS];
 };
 JkTiming g_timing;
 std::mutex g_timing_mutex;
@@ -562,14 +564,14 @@ int dftk_jk_timing(int enable)
 {
     std::lock_guard<std::mutex> lock(g_timing_mutex);
     if (enable && !g_timing.created) {
-        for (int k = 0; k < 2 * DFTK_N_QCLASS; ++k) {
+        for (int k = 0; k < DFTK_TIMING_SLOTS; ++k) {
             DFTK_CUDA(cudaEventCreate(&g_timing.start[k]));
             DFTK_CUDA(cudaEventCreate(&g_timing.stop[k]));
         }
         g_timing.created = true;
     }
     g_timing.enabled = enable != 0;
-    for (int k = 0; k < 2 * DFTK_N_QCLASS; ++k) g_timing.launched[k] = false;
+    for (int k = 0; k < DFTK_TIMING_SLOTS; ++k) g_timing.launched[k] = false;
     return DFTK_OK;
 }
 
@@ -577,7 +579,8 @@ int dftk_jk_timing_read(float *ms, int n)
 {
     if (!ms || n < 2 * DFTK_N_QCLASS) return fail(DFTK_ERR_ARG, "dftk_jk_timing_read: need 12 floats");
     std::lock_guard<std::mutex> lock(g_timing_mutex);
-    for (int k = 0; k < 2 * DFTK_N_QCLASS; ++k) {
+    const int nslots = n < DFTK_TIMING_SLOTS ? n : DFTK_TIMING_SLOTS;
+    for (int k = 0; k < nslots; ++k) {
         ms[k] = 0.0f;
         if (g_timing.created && g_timing.launched[k]) {
             DFTK_CUDA(cudaEventSynchronize(g_timing.stop[k]));
@@ -613,14 +616,16 @@ int dftk_get_launch(int family, int qclass, int fp32, int *threads, int *blocks_
 
 int dftk_grad(const dftk_shells_t *shells, const int *shell_atom, int n_atoms, const double *atom_xyz,
               const double *atom_z, const dftk_pairs_t pairs[DFTK_N_PCLASS], const dftk_queue_t *queue,
-              const double *D, const double *D_a, const double *D_b, const double *W, double tau, double *grad,
-              void *workspace, size_t workspace_bytes, dftk_stream_t stream)
+              const double *D, const double *D_a, const double *D_b, const double *W, double tau, double tau_fp32,
+              double *grad, void *workspace, size_t workspace_bytes, dftk_stream_t stream)
 {
     if (!shells || !shell_atom || n_atoms <= 0 || !atom_xyz || !atom_z || !pairs || !queue || !D || !D_a || !D_b ||
         !W || !grad || !workspace)
         return fail(DFTK_ERR_ARG, "dftk_grad: null argument");
     const int ns = shells->n_shells, N = shells->n_ao;
     if (workspace_bytes < ws_bytes_sh(*shells)) return fail(DFTK_ERR_WORKSPACE, "dftk_grad: workspace too small");
+    if (!(tau >= 0.0)) return fail(DFTK_ERR_ARG, "dftk_grad: bad threshold");
+    const bool mixed = tau_fp32 > tau;
     DFTK_INIT();
     cudaStream_t s = (cudaStream_t)stream;
     // same workspace layout as dftk_jk: Dsh after three N x N blocks, then
@@ -644,8 +649,8 @@ int dftk_grad(const dftk_shells_t *shells, const int *shell_atom, int n_atoms, c
     // with dftk_jk_timing on: slots 0..5 time the class kernels, slot 6 the one-electron part
     const bool timed = g_timing.enabled;
     if (timed) {
-        for (int k = 0; k < 2 * DFTK_N_QCLASS; ++k) g_timing.launched[k] = false;
-        DFTK_CUDA(cudaEventRecord(g_timing.start[DFTK_N_QCLASS], s));
+        for (int k = 0; k < DFTK_TIMING_SLOTS; ++k) g_timing.launched[k] = false;
+        DFTK_CUDA(cudaEventRecord(g_timing.start[2 * DFTK_N_QCLASS], s));
     }
 #define DFTK_GRAD_ONEE(PC)                                                                                   \
     if (pairs[PC].n_pairs > 0) {                                                                             \
@@ -661,8 +666,8 @@ int dftk_grad(const dftk_shells_t *shells, const int *shell_atom, int n_atoms, c
     DFTK_GRAD_ONEE(2)
 #undef DFTK_GRAD_ONEE
     if (timed) {
-        DFTK_CUDA(cudaEventRecord(g_timing.stop[DFTK_N_QCLASS], s));
-        g_timing.launched[DFTK_N_QCLASS] = true;
+        DFTK_CUDA(cudaEventRecord(g_timing.stop[2 * DFTK_N_QCLASS], s));
+        g_timing.launched[2 * DFTK_N_QCLASS] = true;
     }
     GradParams P;
     memset(&P, 0, sizeof(P));
@@ -675,6 +680,7 @@ int dftk_grad(const dftk_shells_t *shells, const int *shell_atom, int n_atoms, c
         P.ab[k] = pairs[k].ab;
         P.q[k] = pairs[k].q;
         P.rec[k] = pairs[k].rec64;
+        P.rec32[k] = pairs[k].rec32;
         P.nprim[k] = pairs[k].nprim;
         P.n_pairs[k] = pairs[k].n_pairs;
     }
@@ -713,7 +719,7 @@ int dftk_grad(const dftk_shells_t *shells, const int *shell_atom, int n_atoms, c
         }
         S.Dsh = Dsh;
         S.tau = tau;
-        S.tau32 = tau;
+        S.tau32 = mixed ? tau_fp32 : tau;  // FP32 entries: tau <= bound < tau_fp32
         S.dm_pow2 = 1;
         unsigned char *cur = (unsigned char *)workspace + ws_bytes_sh(*shells);
         S.heads = (unsigned long long *)cur;
@@ -746,6 +752,16 @@ int dftk_grad(const dftk_shells_t *shells, const int *shell_atom, int n_atoms, c
         if (timed) {                                                          \
             DFTK_CUDA(cudaEventRecord(g_timing.stop[CC], s));                 \
             g_timing.launched[CC] = true;                                     \
+        }                                                                     \
+        if (use_list && mixed) {                                              \
+            const LaunchShape gs = launch_shape(DFTK_FAMILY_GRAD, CC, 1);     \
+            if (timed) DFTK_CUDA(cudaEventRecord(g_timing.start[DFTK_N_QCLASS + CC], s)); \
+            k_grad_eri<CC, true, float><<<shaped_grid(gs, P.total[CC]), gs.threads, smem, s>>>(P); \
+            DFTK_LAUNCHED("k_grad_eri");                                      \
+            if (timed) {                                                      \
+                DFTK_CUDA(cudaEventRecord(g_timing.stop[DFTK_N_QCLASS + CC], s)); \
+                g_timing.launched[DFTK_N_QCLASS + CC] = true;                 \
+            }                                                                 \
         }                                                                     \
     }
     DFTK_GRAD_LAUNCH(0)

@@ -38,6 +38,7 @@ struct GradParams {
     const int *ab[3];
     const double *q[3];
     const double *rec[3];
+    const float *rec32[3];  // FP32 copies of the records (mixed gradient)
     const int *nprim[3];
     int n_pairs[3];
     int kmax;
@@ -57,6 +58,14 @@ struct GradParams {
     const int *ket_base[DFTK_N_QCLASS];  // batches: first ket pair of each row's molecule (NULL = 0)
 };
 
+template <typename T> struct GradRec;
+template <> struct GradRec<double> {
+    __device__ static const double *get(const GradParams &P, int pc) { return P.rec[pc]; }
+};
+template <> struct GradRec<float> {
+    __device__ static const float *get(const GradParams &P, int pc) { return P.rec32[pc]; }
+};
+
 // Quartet classes (ss|ss)..(pp|pp): angular momenta and pair classes.
 template <int C> struct GradClassOf;
 template <> struct GradClassOf<0> { static constexpr int LA = 0, LB = 0, LC = 0, LD = 0, X = 0, Y = 0; };
@@ -73,22 +82,22 @@ __device__ __forceinline__ constexpr int g_cp(int l, int k, int x) { return l ==
 // i <= IA, j <= JB, t <= i + j:
 //   E^{i+1,j}_t = h E^{ij}_{t-1} + X_PA E^{ij}_t + (t+1) E^{ij}_{t+1}   (h = 1/2p)
 // and the same in j with X_PB.
-template <int IA, int JB>
-__device__ __forceinline__ void g_etab(double PA, double PB, double h, double (&E)[IA + 1][JB + 1][IA + JB + 1])
+template <typename T, int IA, int JB>
+__device__ __forceinline__ void g_etab(T PA, T PB, T h, T (&E)[IA + 1][JB + 1][IA + JB + 1])
 {
-    E[0][0][0] = 1.0;
+    E[0][0][0] = T(1);
 #pragma unroll
     for (int i = 0; i < IA; ++i)
 #pragma unroll
         for (int t = 0; t <= i + 1; ++t) {
-            double v;
+            T v;
             if (t <= i) {
                 v = PA * E[i][0][t];
                 if (t > 0) v = fma(h, E[i][0][t - 1], v);
             } else {
                 v = h * E[i][0][t - 1];
             }
-            if (t + 1 <= i) v = fma((double)(t + 1), E[i][0][t + 1], v);
+            if (t + 1 <= i) v = fma((T)(t + 1), E[i][0][t + 1], v);
             E[i + 1][0][t] = v;
         }
 #pragma unroll
@@ -97,14 +106,14 @@ __device__ __forceinline__ void g_etab(double PA, double PB, double h, double (&
         for (int i = 0; i <= IA; ++i)
 #pragma unroll
             for (int t = 0; t <= i + j + 1; ++t) {
-                double v;
+                T v;
                 if (t <= i + j) {
                     v = PB * E[i][j][t];
                     if (t > 0) v = fma(h, E[i][j][t - 1], v);
                 } else {
                     v = h * E[i][j][t - 1];
                 }
-                if (t + 1 <= i + j) v = fma((double)(t + 1), E[i][j][t + 1], v);
+                if (t + 1 <= i + j) v = fma((T)(t + 1), E[i][j][t + 1], v);
                 E[i][j + 1][t] = v;
             }
 }
@@ -112,12 +121,12 @@ __device__ __forceinline__ void g_etab(double PA, double PB, double h, double (&
 // R_{tuv} = R^{(0)}_{tuv}(rho, X, Y, Z) for t + u + v <= LM, times `pre`:
 // R^{(n)}_{000} = pre (-2 rho)^n F_n and
 // R^{(n)}_{t+1,u,v} = t R^{(n+1)}_{t-1,u,v} + X R^{(n+1)}_{t,u,v} (first non-zero index).
-template <int LM>
-__device__ __forceinline__ void g_rcube(double X, double Y, double Z, double m2rho, double pre, const double *F,
-                                        double (&R)[LM + 1][LM + 1][LM + 1])
+template <typename T, int LM>
+__device__ __forceinline__ void g_rcube(T X, T Y, T Z, T m2rho, T pre, const T *F,
+                                        T (&R)[LM + 1][LM + 1][LM + 1])
 {
-    double Rn[LM + 1][LM + 1][LM + 1][LM + 1];
-    double c = pre;
+    T Rn[LM + 1][LM + 1][LM + 1][LM + 1];
+    T c = pre;
 #pragma unroll
     for (int n = 0; n <= LM; ++n) {
         Rn[n][0][0][0] = c * F[n];
@@ -132,16 +141,16 @@ __device__ __forceinline__ void g_rcube(double X, double Y, double Z, double m2r
                 const int v = s - t - u;
 #pragma unroll
                 for (int n = 0; n <= LM - s; ++n) {
-                    double r;
+                    T r;
                     if (t > 0) {
                         r = X * Rn[n + 1][t - 1][u][v];
-                        if (t > 1) r = fma((double)(t - 1), Rn[n + 1][t - 2][u][v], r);
+                        if (t > 1) r = fma((T)(t - 1), Rn[n + 1][t - 2][u][v], r);
                     } else if (u > 0) {
                         r = Y * Rn[n + 1][t][u - 1][v];
-                        if (u > 1) r = fma((double)(u - 1), Rn[n + 1][t][u - 2][v], r);
+                        if (u > 1) r = fma((T)(u - 1), Rn[n + 1][t][u - 2][v], r);
                     } else {
                         r = Z * Rn[n + 1][t][u][v - 1];
-                        if (v > 1) r = fma((double)(v - 1), Rn[n + 1][t][u][v - 2], r);
+                        if (v > 1) r = fma((T)(v - 1), Rn[n + 1][t][u][v - 2], r);
                     }
                     Rn[n][t][u][v] = r;
                 }
@@ -178,10 +187,10 @@ __device__ __forceinline__ void g_smem_end(const double *s_grad, double *grad, i
 
 // gA, gB += sum_T dE^n_T(A), dE^n_T(B) V[T] over the derivative region of bra
 // component n = (ka, kb): T in the box s_n + 1 per axis with |T| <= |s_n| + 1.
-template <int LA, int LB>
-__device__ __forceinline__ void g_ab_contract(int ka, int kb, const double (&Eb)[3][LA + 2][LB + 2][LA + LB + 3],
-                                              double al, double be, const double (&V)[LA + LB + 2][LA + LB + 2][LA + LB + 2],
-                                              double *gA, double *gB)
+template <typename T, int LA, int LB>
+__device__ __forceinline__ void g_ab_contract(int ka, int kb, const T (&Eb)[3][LA + 2][LB + 2][LA + LB + 3],
+                                              T al, T be, const T (&V)[LA + LB + 2][LA + LB + 2][LA + LB + 2],
+                                              T *gA, T *gB)
 {
     const int sx = g_cp(LA, ka, 0) + g_cp(LB, kb, 0), sy = g_cp(LA, ka, 1) + g_cp(LB, kb, 1),
               sz = g_cp(LA, ka, 2) + g_cp(LB, kb, 2);
@@ -192,10 +201,10 @@ __device__ __forceinline__ void g_ab_contract(int ka, int kb, const double (&Eb)
 #pragma unroll
             for (int v = 0; v <= sz + 1; ++v) {
                 if (t + u + v > sx + sy + sz + 1) continue;
-                const double h = V[t][u][v];
+                const T h = V[t][u][v];
 #pragma unroll
                 for (int dir = 0; dir < 3; ++dir) {
-                    double ea = 1.0, eb = 1.0;
+                    T ea = T(1), eb = T(1);
                     bool zero = false;
 #pragma unroll
                     for (int x = 0; x < 3; ++x) {
@@ -207,10 +216,10 @@ __device__ __forceinline__ void g_ab_contract(int ka, int kb, const double (&Eb)
                                 eb *= Eb[x][i][j][tx];
                             }
                         } else {
-                            double fa = 2.0 * al * Eb[x][i + 1][j][tx];
-                            if (i > 0 && tx <= i + j - 1) fa = fma(-(double)i, Eb[x][i - 1][j][tx], fa);
-                            double fb = 2.0 * be * Eb[x][i][j + 1][tx];
-                            if (j > 0 && tx <= i + j - 1) fb = fma(-(double)j, Eb[x][i][j - 1][tx], fb);
+                            T fa = T(2) * al * Eb[x][i + 1][j][tx];
+                            if (i > 0 && tx <= i + j - 1) fa = fma(-(T)i, Eb[x][i - 1][j][tx], fa);
+                            T fb = T(2) * be * Eb[x][i][j + 1][tx];
+                            if (j > 0 && tx <= i + j - 1) fb = fma(-(T)j, Eb[x][i][j - 1][tx], fb);
                             ea *= fa;
                             eb *= fb;
                         }
@@ -230,9 +239,9 @@ __device__ __forceinline__ void g_ab_contract(int ka, int kb, const double (&Eb)
 // coefficients at once (less register state).  Both sides' primitive pairs
 // come sorted by descending primitive Schwarz factor, and the loops stop once
 // qp_bra qp_ket < tau_prim.
-template <int C>
-__device__ __forceinline__ void grad_quartet(const GradParams &P, int row, int ket, double *gA, double *gB,
-                                             double *gC)
+template <int C, typename T>
+__device__ __forceinline__ void grad_quartet(const GradParams &P, int row, int ket, T *gA, T *gB,
+                                             T *gC)
 {
     using G = GradClassOf<C>;
     constexpr int LA = G::LA, LB = G::LB, LC = G::LC, LD = G::LD, X = G::X, Y = G::Y;
@@ -251,7 +260,7 @@ __device__ __forceinline__ void grad_quartet(const GradParams &P, int row, int k
         const int oa = P.sh.ao[a], ob = P.sh.ao[b], oc = P.sh.ao[c], od = P.sh.ao[d];
         const int ew = (a == b) + (c == d) + ((X == Y) && (row == ket));
         const double f = 8.0 / (double)(1 << ew);  // orientations of the unique quartet
-        double Gm[NN][NM];
+        T Gm[NN][NM];
 #pragma unroll
         for (int i = 0; i < NA; ++i)
 #pragma unroll
@@ -264,9 +273,9 @@ __device__ __forceinline__ void grad_quartet(const GradParams &P, int row, int k
                         const double coul = 0.5 * Dt[I * N + J] * Dt[K * N + Lq];
                         const double exch = 0.25 * (Dta[I * N + K] * Dta[J * N + Lq] + Dtb[I * N + K] * Dtb[J * N + Lq] +
                                                     Dta[I * N + Lq] * Dta[J * N + K] + Dtb[I * N + Lq] * Dtb[J * N + K]);
-                        Gm[i * NB + j][k * ND + l] = f * (coul - exch);
+                        Gm[i * NB + j][k * ND + l] = (T)(f * (coul - exch));
                     }
-        double cA[3], cB[3], cC[3], cD[3];
+        T cA[3], cB[3], cC[3], cD[3];
 #pragma unroll
         for (int x = 0; x < 3; ++x) {
             cA[x] = P.sh.xyz[3 * a + x];
@@ -275,9 +284,9 @@ __device__ __forceinline__ void grad_quartet(const GradParams &P, int row, int k
             cD[x] = P.sh.xyz[3 * d + x];
         }
 #pragma unroll
-        for (int x = 0; x < 3; ++x) gA[x] = gB[x] = gC[x] = 0.0;
-        const double *brec = P.rec[X] + row;
-        const double *krec = P.rec[Y] + ket;
+        for (int x = 0; x < 3; ++x) gA[x] = gB[x] = gC[x] = T(0);
+        const T *brec = GradRec<T>::get(P, X) + row;
+        const T *krec = GradRec<T>::get(P, Y) + ket;
         const float *bq = P.qp[X] + row, *kq = P.qp[Y] + ket;
         const int nbp = P.nprim[X][row], nkp = P.nprim[Y][ket];
         const float kq0 = __ldg(kq);
@@ -285,15 +294,15 @@ __device__ __forceinline__ void grad_quartet(const GradParams &P, int row, int k
         for (int ip = 0; ip < nbp; ++ip) {
             const float qb = __ldg(bq + (long long)ip * nX);
             if (qb * kq0 < P.tau_prim) break;
-            const double *br = brec + (long long)ip * nX;
-            const double bP[3] = {__ldg(br), __ldg(br + fsX), __ldg(br + 2 * fsX)};
-            const double bp = __ldg(br + F_P * fsX), bK = __ldg(br + F_K * fsX), bal = __ldg(br + faX * fsX);
-            const double bbe = bp - bal, bh = 0.5 / bp;
-            double Eb[3][LA + 2][LB + 2][LAB + 3];
+            const T *br = brec + (long long)ip * nX;
+            const T bP[3] = {__ldg(br), __ldg(br + fsX), __ldg(br + 2 * fsX)};
+            const T bp = __ldg(br + F_P * fsX), bK = __ldg(br + F_K * fsX), bal = __ldg(br + faX * fsX);
+            const T bbe = bp - bal, bh = T(0.5) / bp;
+            T Eb[3][LA + 2][LB + 2][LAB + 3];
 #pragma unroll
-            for (int x = 0; x < 3; ++x) g_etab<LA + 1, LB + 1>(bP[x] - cA[x], bP[x] - cB[x], bh, Eb[x]);
+            for (int x = 0; x < 3; ++x) g_etab<T, LA + 1, LB + 1>(bP[x] - cA[x], bP[x] - cB[x], bh, Eb[x]);
             // Gamma-weighted bra Hermite density
-            double Eg[NM][LAB + 1][LAB + 1][LAB + 1];
+            T Eg[NM][LAB + 1][LAB + 1][LAB + 1];
 #pragma unroll
             for (int m = 0; m < NM; ++m)
 #pragma unroll
@@ -303,7 +312,7 @@ __device__ __forceinline__ void grad_quartet(const GradParams &P, int row, int k
 #pragma unroll
                         for (int v = 0; v <= LAB - t - u; ++v) {
                             bool first = true;
-                            double s = 0.0;
+                            T s = T(0);
 #pragma unroll
                             for (int ka = 0; ka < NA; ++ka)
 #pragma unroll
@@ -311,7 +320,7 @@ __device__ __forceinline__ void grad_quartet(const GradParams &P, int row, int k
                                     const int ax = g_cp(LA, ka, 0), ay = g_cp(LA, ka, 1), az = g_cp(LA, ka, 2);
                                     const int bx = g_cp(LB, kb, 0), by = g_cp(LB, kb, 1), bz = g_cp(LB, kb, 2);
                                     if (t <= ax + bx && u <= ay + by && v <= az + bz) {
-                                        const double e = Eb[0][ax][bx][t] * Eb[1][ay][by][u] * Eb[2][az][bz][v];
+                                        const T e = Eb[0][ax][bx][t] * Eb[1][ay][by][u] * Eb[2][az][bz][v];
                                         s = first ? Gm[ka * NB + kb][m] * e : fma(Gm[ka * NB + kb][m], e, s);
                                         first = false;
                                     }
@@ -320,7 +329,7 @@ __device__ __forceinline__ void grad_quartet(const GradParams &P, int row, int k
                         }
             constexpr bool kHoldH = NN <= 3;
             constexpr int NH = kHoldH ? NN : 1;
-            double H[NH][LAB + 2][LAB + 2][LAB + 2];
+            T H[NH][LAB + 2][LAB + 2][LAB + 2];
             if constexpr (kHoldH) {
 #pragma unroll
                 for (int n = 0; n < NH; ++n)
@@ -329,33 +338,33 @@ __device__ __forceinline__ void grad_quartet(const GradParams &P, int row, int k
 #pragma unroll
                         for (int u = 0; u <= LAB + 1 - t; ++u)
 #pragma unroll
-                            for (int v = 0; v <= LAB + 1 - t - u; ++v) H[n][t][u][v] = 0.0;
+                            for (int v = 0; v <= LAB + 1 - t - u; ++v) H[n][t][u][v] = T(0);
             }
 #pragma unroll 1
             for (int jp = 0; jp < nkp; ++jp) {
                 if (qb * __ldg(kq + (long long)jp * nY) < P.tau_prim) break;
-                const double *kr = krec + (long long)jp * nY;
-                const double kP[3] = {__ldg(kr), __ldg(kr + fsY), __ldg(kr + 2 * fsY)};
-                const double kp = __ldg(kr + F_P * fsY), kK = __ldg(kr + F_K * fsY), kal = __ldg(kr + faY * fsY);
-                const double kh = 0.5 / kp;
-                double Ek[3][LC + 2][LD + 1][LCD + 2];
+                const T *kr = krec + (long long)jp * nY;
+                const T kP[3] = {__ldg(kr), __ldg(kr + fsY), __ldg(kr + 2 * fsY)};
+                const T kp = __ldg(kr + F_P * fsY), kK = __ldg(kr + F_K * fsY), kal = __ldg(kr + faY * fsY);
+                const T kh = T(0.5) / kp;
+                T Ek[3][LC + 2][LD + 1][LCD + 2];
 #pragma unroll
-                for (int x = 0; x < 3; ++x) g_etab<LC + 1, LD>(kP[x] - cC[x], kP[x] - cD[x], kh, Ek[x]);
-                const double s2 = bp + kp;
-                const double rs = Math<double>::rsqrt(s2);
-                const double rho = bp * kp * (rs * rs);
-                const double PQx = bP[0] - kP[0], PQy = bP[1] - kP[1], PQz = bP[2] - kP[2];
-                double F[LM + 1];
-                Boys<double, LM>::eval(rho * (PQx * PQx + PQy * PQy + PQz * PQz), F);
-                double R[LM + 1][LM + 1][LM + 1];
-                g_rcube<LM>(PQx, PQy, PQz, -2.0 * rho, bK * kK * rs, F, R);
+                for (int x = 0; x < 3; ++x) g_etab<T, LC + 1, LD>(kP[x] - cC[x], kP[x] - cD[x], kh, Ek[x]);
+                const T s2 = bp + kp;
+                const T rs = Math<T>::rsqrt(s2);
+                const T rho = bp * kp * (rs * rs);
+                const T PQx = bP[0] - kP[0], PQy = bP[1] - kP[1], PQz = bP[2] - kP[2];
+                T F[LM + 1];
+                Boys<T, LM>::eval(rho * (PQx * PQx + PQy * PQy + PQz * PQz), F);
+                T R[LM + 1][LM + 1][LM + 1];
+                g_rcube<T, LM>(PQx, PQy, PQz, T(-2) * rho, bK * kK * rs, F, R);
                 // bra side: H[n][T] += sum_T' Gk[T'] R[T + T']
 #pragma unroll
                 for (int ka = 0; ka < NA; ++ka)
 #pragma unroll
                     for (int kb = 0; kb < NB; ++kb) {
                         const int n = ka * NB + kb;
-                        double Gk[LCD + 1][LCD + 1][LCD + 1];
+                        T Gk[LCD + 1][LCD + 1][LCD + 1];
 #pragma unroll
                         for (int t = 0; t <= LCD; ++t)
 #pragma unroll
@@ -363,7 +372,7 @@ __device__ __forceinline__ void grad_quartet(const GradParams &P, int row, int k
 #pragma unroll
                                 for (int v = 0; v <= LCD - t - u; ++v) {
                                     bool first = true;
-                                    double s = 0.0;
+                                    T s = T(0);
 #pragma unroll
                                     for (int kc = 0; kc < NC; ++kc)
 #pragma unroll
@@ -371,7 +380,7 @@ __device__ __forceinline__ void grad_quartet(const GradParams &P, int row, int k
                                             const int cx = g_cp(LC, kc, 0), cy = g_cp(LC, kc, 1), cz = g_cp(LC, kc, 2);
                                             const int dx = g_cp(LD, kd, 0), dy = g_cp(LD, kd, 1), dz = g_cp(LD, kd, 2);
                                             if (t <= cx + dx && u <= cy + dy && v <= cz + dz) {
-                                                double e = Ek[0][cx][dx][t] * Ek[1][cy][dy][u] * Ek[2][cz][dz][v];
+                                                T e = Ek[0][cx][dx][t] * Ek[1][cy][dy][u] * Ek[2][cz][dz][v];
                                                 if ((t + u + v) & 1) e = -e;
                                                 s = first ? Gm[n][kc * ND + kd] * e : fma(Gm[n][kc * ND + kd], e, s);
                                                 first = false;
@@ -388,7 +397,7 @@ __device__ __forceinline__ void grad_quartet(const GradParams &P, int row, int k
 #pragma unroll
                                 for (int v = 0; v <= sz + 1; ++v) {
                                     if (t + u + v > sx + sy + sz + 1) continue;
-                                    double acc = kHoldH ? H[kHoldH ? n : 0][t][u][v] : 0.0;
+                                    T acc = kHoldH ? H[kHoldH ? n : 0][t][u][v] : T(0);
 #pragma unroll
                                     for (int t2 = 0; t2 <= LCD; ++t2)
 #pragma unroll
@@ -398,7 +407,7 @@ __device__ __forceinline__ void grad_quartet(const GradParams &P, int row, int k
                                                 acc = fma(Gk[t2][u2][v2], R[t + t2][u + u2][v + v2], acc);
                                     H[kHoldH ? n : 0][t][u][v] = acc;
                                 }
-                        if constexpr (!kHoldH) g_ab_contract<LA, LB>(ka, kb, Eb, bal, bbe, H[0], gA, gB);
+                        if constexpr (!kHoldH) g_ab_contract<T, LA, LB>(ka, kb, Eb, bal, bbe, H[0], gA, gB);
                     }
                 // ket side: dE/dC
 #pragma unroll
@@ -415,7 +424,7 @@ __device__ __forceinline__ void grad_quartet(const GradParams &P, int row, int k
 #pragma unroll
                                 for (int v = 0; v <= cz + dz + 1; ++v) {
                                     if (t + u + v > cx + dx + cy + dy + cz + dz + 1) continue;
-                                    double hc = 0.0;
+                                    T hc = T(0);
                                     bool first = true;
 #pragma unroll
                                     for (int t1 = 0; t1 <= LAB; ++t1)
@@ -430,7 +439,7 @@ __device__ __forceinline__ void grad_quartet(const GradParams &P, int row, int k
                                     if ((t + u + v) & 1) hc = -hc;
 #pragma unroll
                                     for (int dir = 0; dir < 3; ++dir) {
-                                        double e = 1.0;
+                                        T e = T(1);
                                         bool zero = false;
 #pragma unroll
                                         for (int x = 0; x < 3; ++x) {
@@ -439,8 +448,8 @@ __device__ __forceinline__ void grad_quartet(const GradParams &P, int row, int k
                                                 if (tx > i + j) zero = true;
                                                 else e *= Ek[x][i][j][tx];
                                             } else {
-                                                double fd = tx <= i + j + 1 ? 2.0 * kal * Ek[x][i + 1][j][tx] : 0.0;
-                                                if (i > 0 && tx <= i + j - 1) fd = fma(-(double)i, Ek[x][i - 1][j][tx], fd);
+                                                T fd = tx <= i + j + 1 ? T(2) * kal * Ek[x][i + 1][j][tx] : T(0);
+                                                if (i > 0 && tx <= i + j - 1) fd = fma(-(T)i, Ek[x][i - 1][j][tx], fd);
                                                 e *= fd;
                                             }
                                         }
@@ -454,7 +463,7 @@ __device__ __forceinline__ void grad_quartet(const GradParams &P, int row, int k
 #pragma unroll
                 for (int ka = 0; ka < NA; ++ka)
 #pragma unroll
-                    for (int kb = 0; kb < NB; ++kb) g_ab_contract<LA, LB>(ka, kb, Eb, bal, bbe, H[ka * NB + kb], gA, gB);
+                    for (int kb = 0; kb < NB; ++kb) g_ab_contract<T, LA, LB>(ka, kb, Eb, bal, bbe, H[ka * NB + kb], gA, gB);
             }
         }
     }
@@ -464,8 +473,36 @@ __device__ __forceinline__ void grad_quartet(const GradParams &P, int row, int k
 // quartets with Q_ab Q_cd max|D|^2 < tau are skipped) or over the entries
 // the selection pass kept (list path; warp w takes entries 32w .. 32w + 31,
 // and a warp whose entries share the bra pair sums dE/dA, dE/dB in registers).
-template <int C, bool LIST>
-__global__ void __launch_bounds__(GRAD_THREADS) k_grad_eri(const GradParams P)
+// Minimum resident blocks per SM requested per class (caps registers).
+// Measured on B200 for (H2O)_64: 4 (128 registers) speeds up the s-bra
+// classes by ~20 %; the p-rich classes lose to spills under any cap.
+#ifndef DFTK_GMINB_0
+#define DFTK_GMINB_0 4
+#endif
+#ifndef DFTK_GMINB_1
+#define DFTK_GMINB_1 4
+#endif
+#ifndef DFTK_GMINB_2
+#define DFTK_GMINB_2 1
+#endif
+#ifndef DFTK_GMINB_3
+#define DFTK_GMINB_3 1
+#endif
+#ifndef DFTK_GMINB_4
+#define DFTK_GMINB_4 1
+#endif
+#ifndef DFTK_GMINB_5
+#define DFTK_GMINB_5 1
+#endif
+template <int C> struct GradMinBlocks {
+    static constexpr int v[6] = {DFTK_GMINB_0, DFTK_GMINB_1, DFTK_GMINB_2, DFTK_GMINB_3, DFTK_GMINB_4, DFTK_GMINB_5};
+    static constexpr int value = v[C];
+};
+
+// T = float (list path only): the FP32 entries the selection pass wrote at
+// the back of the class list (mixed gradient); sums stay FP64.
+template <int C, bool LIST, typename T = double>
+__global__ void __launch_bounds__(GRAD_THREADS, GradMinBlocks<C>::value) k_grad_eri(const GradParams P)
 {
     using G = GradClassOf<C>;
     constexpr int X = G::X, Y = G::Y;
@@ -473,7 +510,9 @@ __global__ void __launch_bounds__(GRAD_THREADS) k_grad_eri(const GradParams P)
     double *sg = P.n_atoms <= GRAD_SMEM_ATOMS ? s_grad : nullptr;
     g_smem_begin(sg, 3 * P.n_atoms);
     if constexpr (LIST) {
-        const long long n = (long long)P.heads[C];
+        constexpr bool fp32 = sizeof(T) == 4;
+        const long long n = (long long)P.heads[(fp32 ? DFTK_N_QCLASS : 0) + C];
+        const long long cap = P.total[C];
         const int2 *list = P.list[C];
         const long long nwork = (n + 31) >> 5;
         const int lane = threadIdx.x & 31;
@@ -483,12 +522,21 @@ __global__ void __launch_bounds__(GRAD_THREADS) k_grad_eri(const GradParams P)
             const bool valid = idx < n;
             int row = 0, ket = 0;
             if (valid) {
-                const int2 e = __ldg(list + idx);
+                const int2 e = __ldg(list + (fp32 ? cap - 1 - idx : idx));
                 row = e.x;
                 ket = e.y;
             }
             double gA[3] = {0.0, 0.0, 0.0}, gB[3] = {0.0, 0.0, 0.0}, gC[3] = {0.0, 0.0, 0.0};
-            if (valid) grad_quartet<C>(P, row, ket, gA, gB, gC);
+            if (valid) {
+                T tA[3], tB[3], tC[3];
+                grad_quartet<C, T>(P, row, ket, tA, tB, tC);
+#pragma unroll
+                for (int x = 0; x < 3; ++x) {
+                    gA[x] = (double)tA[x];
+                    gB[x] = (double)tB[x];
+                    gC[x] = (double)tC[x];
+                }
+            }
             const int row0 = __shfl_sync(DFTK_FULL_MASK, row, 0);  // lane 0 is valid whenever any lane is
             const bool uniform = __all_sync(DFTK_FULL_MASK, !valid || row == row0);
             if (valid) {
@@ -537,7 +585,7 @@ __global__ void __launch_bounds__(GRAD_THREADS) k_grad_eri(const GradParams P)
             const float dm = quartet_dmax(P.sh, P.Dsh, a, b, c, d);
             if (P.q[X][row] * P.q[Y][ket] * (double)dm * (double)dm < P.tau) continue;
             double gA[3], gB[3], gC[3];
-            grad_quartet<C>(P, row, ket, gA, gB, gC);
+            grad_quartet<C, double>(P, row, ket, gA, gB, gC);
             const int at[4] = {P.shell_atom[a], P.shell_atom[b], P.shell_atom[c], P.shell_atom[d]};
 #pragma unroll
             for (int x = 0; x < 3; ++x) {
@@ -605,20 +653,20 @@ __global__ void __launch_bounds__(GRAD_THREADS) k_grad_nuclear(const dftk_shells
 #pragma unroll
                 for (int x = 0; x < 3; ++x) {
                     Pc[x] = (al * cA[x] + be * cB[x]) * ip;
-                    g_etab<LA + 1, LB + 1>(Pc[x] - cA[x], Pc[x] - cB[x], 0.5 * ip, E[x]);
+                    g_etab<double, LA + 1, LB + 1>(Pc[x] - cA[x], Pc[x] - cB[x], 0.5 * ip, E[x]);
                 }
                 const double X = Pc[0] - cC[0], Y = Pc[1] - cC[1], Z = Pc[2] - cC[2];
                 double F[LM + 1];
                 Boys<double, LM>::eval(p * (X * X + Y * Y + Z * Z), F);
                 double R[LM + 1][LM + 1][LM + 1];
-                g_rcube<LM>(X, Y, Z, -2.0 * p, pre, F, R);
+                g_rcube<double, LM>(X, Y, Z, -2.0 * p, pre, F, R);
 #pragma unroll
                 for (int ka = 0; ka < NA; ++ka)
 #pragma unroll
                     for (int kb = 0; kb < NB; ++kb) {
                         const double dm = Dm[ka][kb];
                         double tA[3] = {0.0, 0.0, 0.0}, tB[3] = {0.0, 0.0, 0.0};
-                        g_ab_contract<LA, LB>(ka, kb, E, al, be, R, tA, tB);
+                        g_ab_contract<double, LA, LB>(ka, kb, E, al, be, R, tA, tB);
                         // operator centre: -E^n_T R_{T + 1_dir}
                         const int sx = g_cp(LA, ka, 0) + g_cp(LB, kb, 0), sy = g_cp(LA, ka, 1) + g_cp(LB, kb, 1),
                                   sz = g_cp(LA, ka, 2) + g_cp(LB, kb, 2);
@@ -692,7 +740,7 @@ __global__ void __launch_bounds__(GRAD_THREADS) k_grad_overlap_kinetic(const dft
 #pragma unroll
                 for (int x = 0; x < 3; ++x) {
                     Pc[x] = (al * cA[x] + be * cB[x]) * ip;
-                    g_etab<LA + 1, LB + 3>(Pc[x] - cA[x], Pc[x] - cB[x], 0.5 * ip, E[x]);
+                    g_etab<double, LA + 1, LB + 3>(Pc[x] - cA[x], Pc[x] - cB[x], 0.5 * ip, E[x]);
                 }
 #pragma unroll
                 for (int ka = 0; ka < NA; ++ka)

@@ -218,7 +218,8 @@ int dftk_jk_noalloc(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N
  * around each class kernel on their stream.  dftk_jk_timing_read waits for
  * the last recorded call and writes ms[2 * DFTK_N_QCLASS] (FP64 launches,
  * then FP32 launches; 0 where a class did not launch).  A dftk_grad call
- * records its class kernels in slots 0..5 and its one-electron part in slot 6. */
+ * records its FP64 / FP32 class kernels in slots 0..5 / 6..11 and its
+ * one-electron part in slot 12 (written when n >= 13). */
 int dftk_jk_timing(int enable);
 int dftk_jk_timing_read(float *ms, int n);
 
@@ -240,7 +241,10 @@ int dftk_get_launch(int family, int qclass, int fp32, int *threads, int *blocks_
  * (electronic part; the nuclear repulsion term is the caller's).  D is the
  * total density, D_a / D_b the spin densities (both D/2 for RHF), W the
  * energy-weighted density; shell_atom maps shells to atoms, atom_z are the
- * nuclear charges.  Quartets of `queue` with Q_ab Q_cd max|D|^2 < tau are
+ * nuclear charges.  Mixed form: with tau_fp32 > tau, quartets whose bound
+ * Q_ab Q_cd max|D|^2 lies in [tau, tau_fp32) are differentiated in FP32
+ * (list path only; sums in FP64); tau_fp32 <= tau keeps all of them FP64.
+ * Quartets of `queue` with Q_ab Q_cd max|D|^2 < tau are
  * skipped; primitive quartets with qp_bra qp_ket < queue->tau_prim too.
  * workspace: at least dftk_jk_workspace_bytes(n_shells, n_ao) bytes; with
  * dftk_jk_workspace_bytes_queue bytes the surviving quartets are compacted
@@ -248,7 +252,7 @@ int dftk_get_launch(int family, int qclass, int fp32, int *threads, int *blocks_
 int dftk_grad(const dftk_shells_t *shells, const int *shell_atom, int n_atoms, const double *atom_xyz,
               const double *atom_z, const dftk_pairs_t pairs[DFTK_N_PCLASS], const dftk_queue_t *queue,
               const double *D, const double *D_a, const double *D_b, const double *W, double tau,
-              double *grad, void *workspace, size_t workspace_bytes, dftk_stream_t stream);
+              double tau_fp32, double *grad, void *workspace, size_t workspace_bytes, dftk_stream_t stream);
 
 /* Drop-in for the reference's nuclear_kernel (same arguments and output
  * layout, shelled.py:350-371): one thread per primitive-component pair,
