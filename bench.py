@@ -311,9 +311,19 @@ def batch_figures(torch, n_mol=512, n_max=24, n_single=64, n_grad=256, n_grad_ma
     grads = rhf_gradient_batch(geng, gres)
     torch.cuda.synchronize()
     t_grad = time.perf_counter() - t1
+    from dft_b200.gradient import GRAD_TAU_FP32
+
+    rhf_gradient_batch(geng, gres, tau_fp32=GRAD_TAU_FP32)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    gmx = rhf_gradient_batch(geng, gres, tau_fp32=GRAD_TAU_FP32)
+    torch.cuda.synchronize()
+    t_grad_mx = time.perf_counter() - t1
     out["batch_grad"] = {
         "workload": f"{n_grad} water clusters, 1..{n_grad_max} monomers (seed 1), RHF/STO-3G FP64 analytic gradient",
         "gradient_evals_per_s": n_grad / t_grad, "gradient_s": t_grad,
+        "mixed_gradient_evals_per_s": n_grad / t_grad_mx,
+        "mixed_max_abs_diff_vs_fp64_Eh_per_bohr": float(max(np.abs(a - b).max() for a, b in zip(gmx, grads))),
         "with_scf_evals_per_s": n_grad / (t_scf + t_grad), "scf_s": t_scf,
         "converged": int(gres.converged.sum()),
         "max_abs_translational_sum": float(max(np.abs(g.sum(axis=0)).max() for g in grads)),
