@@ -92,6 +92,8 @@ void build_tables()
         }
         g_exp64[k] = (double)expl(-t64);
         g_exp32[k] = (float)expl(-t32);
+        // FP32 rows use coefficients 0..4; slot 5 carries exp(-T_k) (see boys.cuh)
+        for (int L = 0; L < NL; ++L) g_tab32[((size_t)L * R + k) * W + 5] = g_exp32[k];
     }
 }
 

@@ -252,16 +252,19 @@ __global__ void k_boys_test(int mmax, long long n, const double *T, double *F)
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     double *o = F + t * (mmax + 1);
+    // caller-supplied arguments: T < 0 is evaluated at 0 (the table index
+    // stays in range); NaN takes the asymptotic branch and stays NaN
+    const double x = T[t] < 0.0 ? 0.0 : T[t];
     switch (mmax) {
-    case 0: boys64_store<0>(T[t], o); break;
-    case 1: boys64_store<1>(T[t], o); break;
-    case 2: boys64_store<2>(T[t], o); break;
-    case 3: boys64_store<3>(T[t], o); break;
-    case 4: boys64_store<4>(T[t], o); break;
-    case 5: boys64_store<5>(T[t], o); break;
-    case 6: boys64_store<6>(T[t], o); break;
-    case 7: boys64_store<7>(T[t], o); break;
-    default: boys64_store<8>(T[t], o); break;
+    case 0: boys64_store<0>(x, o); break;
+    case 1: boys64_store<1>(x, o); break;
+    case 2: boys64_store<2>(x, o); break;
+    case 3: boys64_store<3>(x, o); break;
+    case 4: boys64_store<4>(x, o); break;
+    case 5: boys64_store<5>(x, o); break;
+    case 6: boys64_store<6>(x, o); break;
+    case 7: boys64_store<7>(x, o); break;
+    default: boys64_store<8>(x, o); break;
     }
 }
 
@@ -278,15 +281,16 @@ __global__ void k_boys32_test(int mmax, long long n, const float *T, float *F)
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     float *o = F + t * (mmax + 1);
+    const float x = T[t] < 0.0f ? 0.0f : T[t];
     switch (mmax) {
-    case 0: boys32_store<0>(T[t], o); break;
-    case 1: boys32_store<1>(T[t], o); break;
-    case 2: boys32_store<2>(T[t], o); break;
-    case 3: boys32_store<3>(T[t], o); break;
-    case 4: boys32_store<4>(T[t], o); break;
-    case 5: boys32_store<5>(T[t], o); break;
-    case 6: boys32_store<6>(T[t], o); break;
-    case 7: boys32_store<7>(T[t], o); break;
-    default: boys32_store<8>(T[t], o); break;
+    case 0: boys32_store<0>(x, o); break;
+    case 1: boys32_store<1>(x, o); break;
+    case 2: boys32_store<2>(x, o); break;
+    case 3: boys32_store<3>(x, o); break;
+    case 4: boys32_store<4>(x, o); break;
+    case 5: boys32_store<5>(x, o); break;
+    case 6: boys32_store<6>(x, o); break;
+    case 7: boys32_store<7>(x, o); break;
+    default: boys32_store<8>(x, o); break;
     }
 }

@@ -137,7 +137,7 @@ int dftk_init(void);
 
 /* F_0..F_mmax(T) for n arguments: F[i * (mmax + 1) + m] (boys/taylor,
  * shelled.py:174-211), through the evaluators the ERI kernels use:
- * mmax 0..8 in FP64 and (dftk_boys32) FP32. */
+ * mmax 0..8 in FP64 and (dftk_boys32) FP32.  T < 0 is evaluated at 0. */
 int dftk_boys(int mmax, long long n, const double *T, double *F, dftk_stream_t stream);
 int dftk_boys32(int mmax, long long n, const float *T, float *F, dftk_stream_t stream);
 
