@@ -389,6 +389,92 @@ def cpu_reference_rate(eng_totals, shells, q_by_class, per_class, seed=0, kernel
     return 1.0 / total_t, cores, sample, kernel
 
 
+def cpu_reference_class_rates(shells, q_by_class, per_class, seed=0):
+    """Shell quartets/s per class of the reference's CPU path (host-compiled
+    eri_kernel + restated contraction and digestion), on samples of
+    Schwarz-kept quartets (CPU-baseline leg)."""
+    from oracle import oracle as orc
+    from dft_b200.engine import QCLASS_PAIRS
+
+    rng = np.random.default_rng(seed)
+    l = np.array([s_["angular_momentum"] for s_ in shells])
+    ii, jj = np.tril_indices(len(shells))
+    pairs_by_class = [[], [], []]
+    for i, j in zip(ii, jj):
+        a, b = (i, j) if l[i] >= l[j] else (j, i)
+        pairs_by_class[l[a] + l[b]].append((i, j))
+    N = shells[-1]["ao_stop"]
+    A = rng.normal(size=(N, N))
+    P = (A + A.T) * 0.01
+    ref = orc.ref_lib()
+    rates = []
+    for c, (X, Y) in enumerate(QCLASS_PAIRS):
+        qx, qy = q_by_class[X], q_by_class[Y]
+        px, py = pairs_by_class[X], pairs_by_class[Y]
+        picks = []
+        tries = 0
+        while len(picks) < per_class[c] and tries < 200 * per_class[c]:
+            tries += 1
+            r = rng.integers(len(px))
+            k = rng.integers(len(py))
+            if X == Y and k > r:
+                r, k = k, r
+            if qx[r] * qy[k] >= 1e-12:
+                picks.append((*px[r], *py[k]))
+        quads = np.array(picks, dtype=np.int32)
+        t0 = time.perf_counter()
+        if ref is not None:
+            orc.direct_jk_reference_kernel(shells, quads, P, P / 2, P / 2, ref=ref)
+        else:
+            orc.direct_jk(shells, quads, P, P / 2, P / 2)
+        rates.append(len(picks) / (time.perf_counter() - t0))
+    return rates, orc.lib().orc_num_threads(), "reference" if ref is not None else "port"
+
+
+def c10h22_figures(torch, cpu: bool):
+    """C10H22 / STO-3G (72 basis functions): per-class ERI throughput of one
+    full FP64 build at the converged density (CUDA events per class kernel),
+    next to the reference's CPU path per class."""
+    import ctypes
+
+    from dft_b200 import _lib, basis, geometry
+    from dft_b200.engine import QCLASS_NAMES, IntegralEngine
+    from dft_b200.scf import scf_rhf
+
+    atoms, c = geometry.alkane(10)
+    shells = basis.build_shells(basis.load_basis(), atoms, c)
+    eng = IntegralEngine(shells)
+    S, T, V = eng.one_electron(atoms, c)
+    r = scf_rhf(eng, T + V, S, basis.n_electrons(atoms) // 2, geometry.nuclear_repulsion(atoms, c))
+    D = r.D_a
+    Dt = (2 * D).contiguous()
+    for _ in range(3):
+        eng.jk(Dt, D, tau=1e-14)
+    counts = torch.zeros(24, dtype=torch.int64, device="cuda")
+    eng.jk(Dt, D, tau=1e-14, counts=counts)
+    torch.cuda.synchronize()
+    ev = counts[:6].tolist()
+    _lib.call("dftk_jk_timing", 1)
+    ms = []
+    for _ in range(5):
+        eng.jk(Dt, D, tau=1e-14)
+        buf = (ctypes.c_float * 13)()
+        _lib.call("dftk_jk_timing_read", buf, 13)
+        ms.append(buf[:6])
+    _lib.call("dftk_jk_timing", 0)
+    ms = np.median(np.array(ms), axis=0)
+    out = {"energy": r.energy, "quartets_per_class": eng.quartet_totals(), "evaluated_per_class": ev,
+           "class_ms": {QCLASS_NAMES[k]: float(ms[k]) for k in range(6)},
+           "quartets_per_s": {QCLASS_NAMES[k]: (ev[k] / (ms[k] / 1e3) if ms[k] > 0 else None) for k in range(6)}}
+    if cpu:
+        qs = schwarz_by_reference_order(shells)
+        rates, cores, kind = cpu_reference_class_rates(shells, qs, [2000, 2000, 1000, 1000, 500, 200], seed=3)
+        out["cpu_reference_quartets_per_s"] = {QCLASS_NAMES[k]: rates[k] for k in range(6)}
+        out["cpu_reference"] = {"cores": cores, "kind": kind,
+                                "sample": "2000/2000/1000/1000/500/200 Schwarz-kept quartets per class"}
+    return out
+
+
 def schwarz_by_reference_order(shells):
     """Per pair-class Schwarz factors in the reference pair order (CPU oracle)."""
     from oracle import oracle as orc
@@ -622,7 +708,9 @@ def run_dftk_arm(args, rank, world, local_rank):
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
         }
+        line["eri_quartets_per_s"] = sum(evaluated) / (ms_per_step / 1e3)
         if not args.no_extras:
+            line["c10h22"] = c10h22_figures(torch, cpu=world == 1 and not args.no_cpu_baseline)
             line["grad"] = gradient_figures(torch, eng, atoms, centers, r64)
             line["errors"] = error_figures(torch, eng)
             line.update(batch_figures(torch))
