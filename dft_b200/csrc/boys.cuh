@@ -7,8 +7,8 @@
 //           < 2e-15 relative).  The table stores, per order L, the eight
 //           coefficients F_{L+j}(T_k) / j! of one grid point contiguously, so
 //           the polynomial is a plain FMA Horner chain fed by 128-bit loads
-//           (two 256-bit loads per row measured ~2 % slower over the six
-//           FP64 classes on B200).
+//           (order 0: two 256-bit loads, measured 4 % faster on (ss|ss); the
+//           other orders measured slower with them).
 //           exp(-T) = exp(-T_k) exp(T_k - T) with a 7-term Taylor series,
 //           then the downward recursion F_m = (2T F_{m+1} + exp(-T)) / (2m+1),
 //           which is stable.
@@ -35,8 +35,12 @@ __device__ double g_bexp64[DFTK_BOYS_ROWS];
 __device__ __align__(128) float g_boys32[DFTK_BOYS_NL * DFTK_BOYS_ROWS * DFTK_BOYS_W];
 __device__ float g_bexp32[DFTK_BOYS_ROWS];
 
-// 32-byte read-only vector load (sm_100: ld.global.nc.v8.f32); the address
-// must be 32-byte aligned (FP32 table rows are)
+// 32-byte read-only vector loads (sm_100: ld.global.nc.v4.f64 / .v8.f32);
+// the address must be 32-byte aligned (table rows are)
+__device__ __forceinline__ void ldg_v4d(const double *p, double &a, double &b, double &c, double &d)
+{
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(a), "=d"(b), "=d"(c), "=d"(d) : "l"(p));
+}
 __device__ __forceinline__ void ldg_v8f(const float *p, float (&v)[8])
 {
     asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
@@ -54,16 +58,25 @@ template <int L> struct Boys<double, L> {
             const double shifted = fma(x, 10.0, DFTK_ROUND_MAGIC64);  // x >= 0
             const int k = __double2loint(shifted);
             const double d = (shifted - DFTK_ROUND_MAGIC64) * 0.1 - x;
-            const double2 *row = reinterpret_cast<const double2 *>(
-                g_boys64 + ((size_t)L * DFTK_BOYS_ROWS + k) * DFTK_BOYS_W);
-            const double2 c01 = __ldg(row), c23 = __ldg(row + 1), c45 = __ldg(row + 2), c67 = __ldg(row + 3);
-            double f = fma(c67.y, d, c67.x);
-            f = fma(f, d, c45.y);
-            f = fma(f, d, c45.x);
-            f = fma(f, d, c23.y);
-            f = fma(f, d, c23.x);
-            f = fma(f, d, c01.y);
-            F[L] = fma(f, d, c01.x);
+            const double *rowp = g_boys64 + ((size_t)L * DFTK_BOYS_ROWS + k) * DFTK_BOYS_W;
+            double c0, c1, c2, c3, c4, c5, c6, c7;
+            if constexpr (L == 0) {
+                // (ss|ss): two 256-bit loads per row (measured faster for this
+                // order only; the higher orders keep 128-bit loads)
+                ldg_v4d(rowp, c0, c1, c2, c3);
+                ldg_v4d(rowp + 4, c4, c5, c6, c7);
+            } else {
+                const double2 *row = reinterpret_cast<const double2 *>(rowp);
+                const double2 c01 = __ldg(row), c23 = __ldg(row + 1), c45 = __ldg(row + 2), c67 = __ldg(row + 3);
+                c0 = c01.x; c1 = c01.y; c2 = c23.x; c3 = c23.y; c4 = c45.x; c5 = c45.y; c6 = c67.x; c7 = c67.y;
+            }
+            double f = fma(c7, d, c6);
+            f = fma(f, d, c5);
+            f = fma(f, d, c4);
+            f = fma(f, d, c3);
+            f = fma(f, d, c2);
+            f = fma(f, d, c1);
+            F[L] = fma(f, d, c0);
             if (L > 0) {
                 double e = fma(d, 1.0 / 5040.0, 1.0 / 720.0);
                 e = fma(e, d, 1.0 / 120.0);
