@@ -288,9 +288,11 @@ class IntegralEngine:
         return M
 
     def gradient(self, atoms: Sequence[str], centers, D: torch.Tensor, D_a: torch.Tensor, D_b: torch.Tensor,
-                 W: torch.Tensor, tau: float = 1e-14, tau_fp32: float = 0.0) -> np.ndarray:
+                 W: torch.Tensor, tau: float = 1e-14, tau_fp32: float = 0.0, scan: bool = False) -> np.ndarray:
         """Electronic nuclear gradient (n_atoms, 3): sum D dH - sum W dS + sum Gamma d(ERI),
-        from the total density D, spin densities D_a/D_b and energy-weighted density W."""
+        from the total density D, spin densities D_a/D_b and energy-weighted density W.
+        tau_fp32 > tau selects the mixed form; ``scan`` hands dftk_grad only the
+        base workspace (class kernels scan the candidates, FP64 only)."""
         n_atoms = len(atoms)
         if not hasattr(self, "d_shell_atom"):
             self.d_shell_atom = self._t(np.array([s["atom_idx"] for s in self.shells], dtype=np.int32), torch.int32)
@@ -300,7 +302,8 @@ class IntegralEngine:
         _lib.call("dftk_grad", ctypes.byref(self.c_shells), _lib.ptr(self.d_shell_atom), n_atoms, _lib.ptr(xyz),
                   _lib.ptr(z), self.c_pairs, ctypes.byref(self.c_queue), _lib.ptr(self._square(D)),
                   _lib.ptr(self._square(D_a)), _lib.ptr(self._square(D_b)), _lib.ptr(self._square(W)), float(tau),
-                  float(tau_fp32), _lib.ptr(g), _lib.ptr(self.workspace), self.workspace_bytes, _lib.stream_handle())
+                  float(tau_fp32), _lib.ptr(g), _lib.ptr(self.workspace),
+                  self.base_workspace_bytes if scan else self.workspace_bytes, _lib.stream_handle())
         return g.reshape(n_atoms, 3).cpu().numpy()
 
     def quartet_descriptors(self, quads: np.ndarray):

@@ -128,3 +128,32 @@ def test_mixed_scf_gradient_matches_fp64():
     _, g64 = energy_and_gradient(atoms, centers, mixed=False)
     _, gmx = energy_and_gradient(atoms, centers, mixed=True)
     assert np.abs(g64 - gmx).max() < GRAD_TOL
+
+
+def _rand_sym(n, rng, scale):
+    A = rng.normal(size=(n, n)) * scale
+    return A + A.T
+
+
+def test_uhf_scan_and_mixed_paths_vs_oracle(oracle_mod):
+    """dftk_grad with D_a != D_b (the UHF Gamma), the direct-scan path and
+    the mixed path, all at one set of random densities, against the oracle."""
+    from dft_b200 import basis
+    from dft_b200.engine import IntegralEngine
+
+    atoms, centers = geometry.water_cluster((1, 1, 2), seed=8)
+    eng = IntegralEngine(basis.build_shells(basis.load_basis(), atoms, centers), tau_schwarz=0.0)
+    rng = np.random.default_rng(12)
+    N = eng.n_ao
+    Da, Db, W = _rand_sym(N, rng, 0.1), _rand_sym(N, rng, 0.1), _rand_sym(N, rng, 0.05)
+    D = Da + Db
+    t = lambda M: torch.as_tensor(M, device="cuda")
+    gnn = geometry.nuclear_repulsion_gradient(atoms, centers)
+    g_list = eng.gradient(atoms, centers, t(D), t(Da), t(Db), t(W), tau=0.0) + gnn
+    g_scan = eng.gradient(atoms, centers, t(D), t(Da), t(Db), t(W), tau=0.0, scan=True) + gnn
+    g_mix = eng.gradient(atoms, centers, t(D), t(Da), t(Db), t(W), tau=0.0, tau_fp32=1e-6) + gnn
+    osh = oracle_mod.build_shells(oracle_mod.load_basis(basis.STO3G_PATH), atoms, centers)
+    go = oracle_mod.gradient(osh, atoms, centers, D, Da, Db, W)
+    assert np.abs(g_list - go).max() < 1e-10
+    assert np.abs(g_scan - go).max() < 1e-10
+    assert np.abs(g_mix - go).max() < 1e-7
