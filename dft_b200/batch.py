@@ -42,6 +42,38 @@ def _prefix(x: np.ndarray) -> np.ndarray:
     return np.concatenate([[0], np.cumsum(x)[:-1]]).astype(np.int64)
 
 
+def batch_row_offsets(q_bra: np.ndarray, seg_bra: np.ndarray, q_ket: np.ndarray, seg_ket: np.ndarray,
+                      same_class: bool, tau: float) -> Tuple[np.ndarray, np.ndarray]:
+    """Candidate row offsets and per-row ket bases of one quartet class of a
+    batch.  Both pair lists hold each molecule's pairs contiguously
+    (molecule m at seg[m]:seg[m+1]), sorted by descending Schwarz factor
+    within the molecule; bra row r of molecule m pairs with the Schwarz-kept
+    prefix of molecule m's ket segment, ket k of that row being ket pair
+    ket_base[r] + k."""
+    counts, kb = [], []
+    for m in range(seg_bra.size - 1):
+        qx = q_bra[seg_bra[m]:seg_bra[m + 1]]
+        qy = q_ket[seg_ket[m]:seg_ket[m + 1]]
+        if qx.size == 0:
+            continue
+        counts.append(np.diff(candidate_offsets(qx, qy, same_class, tau)))
+        kb.append(np.full(qx.size, seg_ket[m], dtype=np.int32))
+    cnt = np.concatenate(counts) if counts else np.zeros(0, dtype=np.int64)
+    off = np.concatenate([[0], np.cumsum(cnt)]).astype(np.int64)
+    kbase = np.concatenate(kb) if kb else np.zeros(0, dtype=np.int32)
+    return off, kbase
+
+
+def pack_index(mol_nao: np.ndarray, n_max: int) -> np.ndarray:
+    """Position in the padded (B, n_max, n_max) layout of every element of
+    the packed per-molecule blocks (block m: n_m x n_m row-major)."""
+    idx = []
+    for m, n in enumerate(np.asarray(mol_nao, dtype=np.int64)):
+        r, c = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+        idx.append(m * n_max * n_max + r.reshape(-1) * n_max + c.reshape(-1))
+    return np.concatenate(idx) if idx else np.zeros(0, dtype=np.int64)
+
+
 class BatchEngine(IntegralEngine):
     """Integral engine over a batch of molecules given as (atoms, centres) pairs."""
 
@@ -158,25 +190,17 @@ class BatchEngine(IntegralEngine):
         self.row_off, self.totals, self.ket_base = [], [], []
         q = _lib.Queue()
         for c, (X, Y) in enumerate(QCLASS_PAIRS):
-            sx, sy = self.pair_seg[X], self.pair_seg[Y]
-            counts, kb = [], []
-            for m in range(self.n_mol):
-                qx = self.q_sorted[X][sx[m]:sx[m + 1]]
-                qy = self.q_sorted[Y][sy[m]:sy[m + 1]]
-                if qx.size == 0:
-                    continue
-                off = candidate_offsets(qx, qy, X == Y, self.tau_schwarz)
-                counts.append(np.diff(off))
-                kb.append(np.full(qx.size, sy[m], dtype=np.int32))
-            cnt = np.concatenate(counts) if counts else np.zeros(0, dtype=np.int64)
-            off = np.concatenate([[0], np.cumsum(cnt)]).astype(np.int64)
-            kbase = np.concatenate(kb) if kb else np.zeros(1, dtype=np.int32)
+            off, kbase = batch_row_offsets(self.q_sorted[X], self.pair_seg[X], self.q_sorted[Y], self.pair_seg[Y],
+                                           X == Y, self.tau_schwarz)
+            n_rows = off.size - 1
+            if kbase.size == 0:
+                kbase = np.zeros(1, dtype=np.int32)
             d_off = self._t(off, torch.int64)
             d_kb = self._t(kbase.astype(np.int32), torch.int32)
             self.row_off.append(d_off)
             self.ket_base.append(d_kb)
             self.totals.append(int(off[-1]))
-            q.n_rows[c] = cnt.size if off[-1] > 0 else 0
+            q.n_rows[c] = n_rows if off[-1] > 0 else 0
             q.total[c] = int(off[-1])
             q.row_off[c] = _lib.ptr(d_off).value
             q.ket_base[c] = _lib.ptr(d_kb).value
@@ -187,12 +211,7 @@ class BatchEngine(IntegralEngine):
     def _build_packing(self):
         """Index of every packed element in the padded (B, Nmax, Nmax) layout."""
         B, Nm = self.n_mol, self.n_max
-        idx = []
-        for m in range(B):
-            n = int(self.mol_nao[m])
-            r, c = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
-            idx.append(m * Nm * Nm + r.reshape(-1) * Nm + c.reshape(-1))
-        self.pack_index = self._t(np.concatenate(idx), torch.int64)
+        self.pack_index = self._t(pack_index(self.mol_nao, Nm), torch.int64)
         self.packed_mol = self._t(np.repeat(np.arange(B), self.mol_nao ** 2), torch.int64)
         ar = np.arange(Nm)
         self.pad_mask = self._t((ar[None, :] >= self.mol_nao[:, None]).astype(np.float64), torch.float64)

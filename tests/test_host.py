@@ -206,3 +206,48 @@ def test_launch_shape_table_without_gpu():
     assert lib.dftk_set_launch(0, 6, 0, 128, 4) == _lib.ERR_ARG
     assert lib.dftk_set_launch(2, 0, 0, 128, 4) == _lib.ERR_ARG
     assert lib.dftk_set_launch(1, 0, 0, 128, 33) == _lib.ERR_ARG
+
+
+def test_batch_queue_matches_per_molecule_queues():
+    """The batch candidate space (row offsets + ket bases) enumerates exactly
+    the union of the molecules' own candidate quartets, with kets indexing
+    the concatenated ket list."""
+    from dft_b200.batch import batch_row_offsets
+
+    rng = np.random.default_rng(3)
+    sizes_x = [5, 0, 9, 3]
+    sizes_y = [4, 2, 7, 0]
+    qx = [np.sort(rng.uniform(1e-9, 1, n))[::-1] for n in sizes_x]
+    qy = [np.sort(rng.uniform(1e-9, 1, n))[::-1] for n in sizes_y]
+    seg_x = np.concatenate([[0], np.cumsum(sizes_x)])
+    seg_y = np.concatenate([[0], np.cumsum(sizes_y)])
+    off, kb = batch_row_offsets(np.concatenate(qx), seg_x, np.concatenate(qy), seg_y, False, 1e-3)
+    got = set()
+    for r in range(off.size - 1):
+        for k in range(off[r + 1] - off[r]):
+            got.add((r, int(kb[r]) + k))
+    want = set()
+    for m in range(4):
+        o = candidate_offsets(qx[m], qy[m], False, 1e-3)
+        for rl in range(sizes_x[m]):
+            for k in range(o[rl + 1] - o[rl]):
+                want.add((seg_x[m] + rl, seg_y[m] + k))
+    assert got == want and len(got) == off[-1]
+
+
+def test_batch_pack_index_round_trip():
+    import torch
+
+    from dft_b200.batch import pack_index
+
+    nao = np.array([3, 1, 4])
+    idx = pack_index(nao, 4)
+    assert idx.size == (nao ** 2).sum() and len(set(idx.tolist())) == idx.size
+    blocks = [np.arange(n * n, dtype=float).reshape(n, n) + 100 * m for m, n in enumerate(nao)]
+    packed = np.concatenate([b.reshape(-1) for b in blocks])
+    padded = np.zeros(3 * 16)
+    padded[idx] = packed
+    padded = padded.reshape(3, 4, 4)
+    for m, n in enumerate(nao):
+        np.testing.assert_array_equal(padded[m, :n, :n], blocks[m])
+        assert not padded[m, n:, :].any() and not padded[m, :, n:].any()
