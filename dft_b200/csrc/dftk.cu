@@ -470,7 +470,6 @@ int dftk_jk(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N_PCLASS]
     const int mixed = (flags & DFTK_JK_MIXED) != 0;
     if (uhf && (!D_b || !K_b)) return fail(DFTK_ERR_ARG, "dftk_jk: UHF needs D_b and K_b");
     if (!(tau >= 0.0) || (mixed && !(tau_fp32 >= tau))) return fail(DFTK_ERR_ARG, "dftk_jk: bad thresholds");
-    const int ns = shells->n_shells, N = shells->n_ao;
     if (shells->mol && (shells->n_mol <= 0 || !shells->mol_mat || !shells->mol_nao || !shells->mol_shell0 ||
                         !shells->mol_ns || !shells->mol_dsh))
         return fail(DFTK_ERR_ARG, "dftk_jk: incomplete molecule table");
@@ -491,8 +490,6 @@ int dftk_jk(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N_PCLASS]
     for (int c = 0; c < DFTK_N_QCLASS; ++c) P.ket_base[c] = queue->ket_base[c];
     P.mol_active = queue->mol_active;
     P.shell_ao = shells->ao;
-    P.N = N;
-    P.ns = ns;
     for (int k = 0; k < 3; ++k) {
         P.ab[k] = pairs[k].ab;
         P.np[k] = pairs[k].nprim;
@@ -624,7 +621,7 @@ int dftk_grad(const dftk_shells_t *shells, const int *shell_atom, int n_atoms, c
     if (!shells || !shell_atom || n_atoms <= 0 || !atom_xyz || !atom_z || !pairs || !queue || !D || !D_a || !D_b ||
         !W || !grad || !workspace)
         return fail(DFTK_ERR_ARG, "dftk_grad: null argument");
-    const int ns = shells->n_shells, N = shells->n_ao;
+    const int ns = shells->n_shells;
     if (workspace_bytes < ws_bytes_sh(*shells)) return fail(DFTK_ERR_WORKSPACE, "dftk_grad: workspace too small");
     if (!(tau >= 0.0)) return fail(DFTK_ERR_ARG, "dftk_grad: bad threshold");
     const bool mixed = tau_fp32 > tau;
@@ -695,8 +692,6 @@ int dftk_grad(const dftk_shells_t *shells, const int *shell_atom, int n_atoms, c
     P.Da = D_a;
     P.Db = D_b;
     P.Dsh = Dsh;
-    P.N = N;
-    P.ns = ns;
     P.tau = tau;
     P.grad = grad;
     P.tau_prim = (float)queue->tau_prim;
@@ -707,7 +702,6 @@ int dftk_grad(const dftk_shells_t *shells, const int *shell_atom, int n_atoms, c
         JkParams S;
         memset(&S, 0, sizeof(S));
         S.sh = *shells;
-        S.ns = ns;
         for (int c = 0; c < DFTK_N_QCLASS; ++c) S.ket_base[c] = queue->ket_base[c];
         S.mol_active = queue->mol_active;
         for (int k = 0; k < 3; ++k) {

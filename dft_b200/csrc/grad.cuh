@@ -49,7 +49,6 @@ struct GradParams {
     const float *Dsh;
     const float *qp[3];  // primitive Schwarz factors, descending per pair
     float tau_prim;      // primitive quartets with qp_bra qp_ket < tau_prim are skipped
-    int N, ns;
     double tau;
     double *grad;  // [n_atoms * 3], accumulated
     // list path: per class the selected (bra row, ket) entries and their count

@@ -138,7 +138,6 @@ __global__ void k_schwarz(const dftk_pairs_t pr, int nfields)
 struct JkParams {
     dftk_shells_t sh;  // shells (and molecule table of a batch)
     const int *shell_ao;
-    int N, ns;
     const int *ab[3];
     const int *np[3];
     const double *rec64[3];
