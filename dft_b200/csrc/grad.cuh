@@ -326,6 +326,103 @@ __device__ __forceinline__ void grad_quartet(const GradParams &P, int row, int k
                                 }
                             Eg[m][t][u][v] = s;
                         }
+            if constexpr (LC == 0 && LD == 0 && NN > 3) {
+                // (pp|ss): the ket is one s-s component, so the bra side folds
+                // Gamma into the derivative Hermite density once per bra
+                // primitive, DA[dir][T] = sum_n Gamma_n dE^n_T(A, dir); a
+                // primitive quartet then costs sum_T DA R_T per direction.
+                // C and D come from Hc[T'] = sum_T Eg[T] R_{T+T'}, and
+                // dE/dB = -(A + C + D) (translational invariance).
+                T DA[3][LAB + 2][LAB + 2][LAB + 2];
+#pragma unroll
+                for (int dir = 0; dir < 3; ++dir)
+#pragma unroll
+                    for (int t = 0; t <= LAB + 1; ++t)
+#pragma unroll
+                        for (int u = 0; u <= LAB + 1 - t; ++u)
+#pragma unroll
+                            for (int v = 0; v <= LAB + 1 - t - u; ++v) DA[dir][t][u][v] = T(0);
+#pragma unroll
+                for (int ka = 0; ka < NA; ++ka)
+#pragma unroll
+                    for (int kb = 0; kb < NB; ++kb) {
+                        const T gn = Gm[ka * NB + kb][0];
+                        const int sx = g_cp(LA, ka, 0) + g_cp(LB, kb, 0), sy = g_cp(LA, ka, 1) + g_cp(LB, kb, 1),
+                                  sz = g_cp(LA, ka, 2) + g_cp(LB, kb, 2);
+#pragma unroll
+                        for (int dir = 0; dir < 3; ++dir)
+#pragma unroll
+                            for (int t = 0; t <= sx + (dir == 0); ++t)
+#pragma unroll
+                                for (int u = 0; u <= sy + (dir == 1); ++u)
+#pragma unroll
+                                    for (int v = 0; v <= sz + (dir == 2); ++v) {
+                                        T e = gn;
+#pragma unroll
+                                        for (int x = 0; x < 3; ++x) {
+                                            const int i = g_cp(LA, ka, x), j = g_cp(LB, kb, x),
+                                                      tx = x == 0 ? t : (x == 1 ? u : v);
+                                            if (x != dir) {
+                                                e *= Eb[x][i][j][tx];
+                                            } else {
+                                                T fa = T(2) * bal * Eb[x][i + 1][j][tx];
+                                                if (i > 0 && tx <= i + j - 1) fa = fma(-(T)i, Eb[x][i - 1][j][tx], fa);
+                                                e *= fa;
+                                            }
+                                        }
+                                        DA[dir][t][u][v] += e;
+                                    }
+                    }
+#pragma unroll 1
+                for (int jp = 0; jp < nkp; ++jp) {
+                    if (qb * __ldg(kq + (long long)jp * nY) < P.tau_prim) break;
+                    const T *kr = krec + (long long)jp * nY;
+                    const T kP[3] = {__ldg(kr), __ldg(kr + fsY), __ldg(kr + 2 * fsY)};
+                    const T kp = __ldg(kr + F_P * fsY), kK = __ldg(kr + F_K * fsY), kal = __ldg(kr + faY * fsY);
+                    const T kbe = kp - kal, kh = T(0.5) / kp;
+                    const T s2 = bp + kp;
+                    const T rs = Math<T>::rsqrt(s2);
+                    const T rho = bp * kp * (rs * rs);
+                    const T PQx = bP[0] - kP[0], PQy = bP[1] - kP[1], PQz = bP[2] - kP[2];
+                    T F[LM + 1];
+                    Boys<T, LM>::eval(rho * (PQx * PQx + PQy * PQy + PQz * PQz), F);
+                    T R[LM + 1][LM + 1][LM + 1];
+                    g_rcube<T, LM>(PQx, PQy, PQz, T(-2) * rho, bK * kK * rs, F, R);
+#pragma unroll
+                    for (int dir = 0; dir < 3; ++dir) {
+                        T acc = T(0);
+#pragma unroll
+                        for (int t = 0; t <= LAB + 1; ++t)
+#pragma unroll
+                            for (int u = 0; u <= LAB + 1 - t; ++u)
+#pragma unroll
+                                for (int v = 0; v <= LAB + 1 - t - u; ++v) acc = fma(DA[dir][t][u][v], R[t][u][v], acc);
+                        gA[dir] += acc;
+                    }
+                    // Hc at T' = 0 and T' = e_dir
+                    T h0 = T(0), h1[3] = {T(0), T(0), T(0)};
+#pragma unroll
+                    for (int t = 0; t <= LAB; ++t)
+#pragma unroll
+                        for (int u = 0; u <= LAB - t; ++u)
+#pragma unroll
+                            for (int v = 0; v <= LAB - t - u; ++v) {
+                                const T e = Eg[0][t][u][v];
+                                h0 = fma(e, R[t][u][v], h0);
+                                h1[0] = fma(e, R[t + 1][u][v], h1[0]);
+                                h1[1] = fma(e, R[t][u + 1][v], h1[1]);
+                                h1[2] = fma(e, R[t][u][v + 1], h1[2]);
+                            }
+                    // s-s ket: dE/dC_x = 2 gamma (X_QC h0 - h h1_x), dE/dD_x = 2 delta (X_QD h0 - h h1_x)
+#pragma unroll
+                    for (int dir = 0; dir < 3; ++dir) {
+                        const T qc = kP[dir] - cC[dir], qd = kP[dir] - cD[dir];
+                        gC[dir] = fma(T(2) * kal, fma(qc, h0, -kh * h1[dir]), gC[dir]);
+                        gB[dir] = fma(T(2) * kbe, fma(qd, h0, -kh * h1[dir]), gB[dir]);  // gD for now
+                    }
+                }
+                continue;
+            }
             constexpr bool kHoldH = NN <= 3;
             constexpr int NH = kHoldH ? NN : 1;
             T H[NH][LAB + 2][LAB + 2][LAB + 2];
@@ -464,6 +561,11 @@ __device__ __forceinline__ void grad_quartet(const GradParams &P, int row, int k
 #pragma unroll
                     for (int kb = 0; kb < NB; ++kb) g_ab_contract<T, LA, LB>(ka, kb, Eb, bal, bbe, H[ka * NB + kb], gA, gB);
             }
+        }
+        if constexpr (LC == 0 && LD == 0 && NN > 3) {
+            // gB holds dE/dD here; dE/dB = -(A + C + D)
+#pragma unroll
+            for (int x = 0; x < 3; ++x) gB[x] = -(gA[x] + gC[x] + gB[x]);
         }
     }
 }
