@@ -186,7 +186,7 @@ __device__ __forceinline__ void g_smem_end(const double *s_grad, double *grad, i
 
 // gA, gB += sum_T dE^n_T(A), dE^n_T(B) V[T] over the derivative region of bra
 // component n = (ka, kb): T in the box s_n + 1 per axis with |T| <= |s_n| + 1.
-template <typename T, int LA, int LB>
+template <typename T, int LA, int LB, bool WITH_B = true>
 __device__ __forceinline__ void g_ab_contract(int ka, int kb, const T (&Eb)[3][LA + 2][LB + 2][LA + LB + 3],
                                               T al, T be, const T (&V)[LA + LB + 2][LA + LB + 2][LA + LB + 2],
                                               T *gA, T *gB)
@@ -217,15 +217,17 @@ __device__ __forceinline__ void g_ab_contract(int ka, int kb, const T (&Eb)[3][L
                         } else {
                             T fa = T(2) * al * Eb[x][i + 1][j][tx];
                             if (i > 0 && tx <= i + j - 1) fa = fma(-(T)i, Eb[x][i - 1][j][tx], fa);
-                            T fb = T(2) * be * Eb[x][i][j + 1][tx];
-                            if (j > 0 && tx <= i + j - 1) fb = fma(-(T)j, Eb[x][i][j - 1][tx], fb);
                             ea *= fa;
-                            eb *= fb;
+                            if constexpr (WITH_B) {
+                                T fb = T(2) * be * Eb[x][i][j + 1][tx];
+                                if (j > 0 && tx <= i + j - 1) fb = fma(-(T)j, Eb[x][i][j - 1][tx], fb);
+                                eb *= fb;
+                            }
                         }
                     }
                     if (!zero) {
                         gA[dir] = fma(ea, h, gA[dir]);
-                        gB[dir] = fma(eb, h, gB[dir]);
+                        if constexpr (WITH_B) gB[dir] = fma(eb, h, gB[dir]);
                     }
                 }
             }
@@ -443,9 +445,12 @@ __device__ __forceinline__ void grad_quartet(const GradParams &P, int row, int k
                 const T kP[3] = {__ldg(kr), __ldg(kr + fsY), __ldg(kr + 2 * fsY)};
                 const T kp = __ldg(kr + F_P * fsY), kK = __ldg(kr + F_K * fsY), kal = __ldg(kr + faY * fsY);
                 const T kh = T(0.5) / kp;
-                T Ek[3][LC + 2][LD + 1][LCD + 2];
+                // streaming (pp-bra) classes also need d raised: dE/dD from the ket side
+                constexpr int JD = kHoldH ? LD : LD + 1;
+                T Ek[3][LC + 2][JD + 1][LC + JD + 2];
 #pragma unroll
-                for (int x = 0; x < 3; ++x) g_etab<T, LC + 1, LD>(kP[x] - cC[x], kP[x] - cD[x], kh, Ek[x]);
+                for (int x = 0; x < 3; ++x) g_etab<T, LC + 1, JD>(kP[x] - cC[x], kP[x] - cD[x], kh, Ek[x]);
+                const T kbe = kp - kal;
                 const T s2 = bp + kp;
                 const T rs = Math<T>::rsqrt(s2);
                 const T rho = bp * kp * (rs * rs);
@@ -503,7 +508,8 @@ __device__ __forceinline__ void grad_quartet(const GradParams &P, int row, int k
                                                 acc = fma(Gk[t2][u2][v2], R[t + t2][u + u2][v + v2], acc);
                                     H[kHoldH ? n : 0][t][u][v] = acc;
                                 }
-                        if constexpr (!kHoldH) g_ab_contract<T, LA, LB>(ka, kb, Eb, bal, bbe, H[0], gA, gB);
+                        // streaming classes: dE/dA only, dE/dB by translational invariance
+                        if constexpr (!kHoldH) g_ab_contract<T, LA, LB, false>(ka, kb, Eb, bal, bbe, H[0], gA, gB);
                     }
                 // ket side: dE/dC
 #pragma unroll
@@ -535,21 +541,32 @@ __device__ __forceinline__ void grad_quartet(const GradParams &P, int row, int k
                                     if ((t + u + v) & 1) hc = -hc;
 #pragma unroll
                                     for (int dir = 0; dir < 3; ++dir) {
-                                        T e = T(1);
+                                        T e = T(1), ed = T(1);
                                         bool zero = false;
 #pragma unroll
                                         for (int x = 0; x < 3; ++x) {
                                             const int i = g_cp(LC, kc, x), j = g_cp(LD, kd, x), tx = x == 0 ? t : (x == 1 ? u : v);
                                             if (x != dir) {
                                                 if (tx > i + j) zero = true;
-                                                else e *= Ek[x][i][j][tx];
+                                                else {
+                                                    e *= Ek[x][i][j][tx];
+                                                    if constexpr (!kHoldH) ed *= Ek[x][i][j][tx];
+                                                }
                                             } else {
                                                 T fd = tx <= i + j + 1 ? T(2) * kal * Ek[x][i + 1][j][tx] : T(0);
                                                 if (i > 0 && tx <= i + j - 1) fd = fma(-(T)i, Ek[x][i - 1][j][tx], fd);
                                                 e *= fd;
+                                                if constexpr (!kHoldH) {
+                                                    T fdd = tx <= i + j + 1 ? T(2) * kbe * Ek[x][i][j + 1][tx] : T(0);
+                                                    if (j > 0 && tx <= i + j - 1) fdd = fma(-(T)j, Ek[x][i][j - 1][tx], fdd);
+                                                    ed *= fdd;
+                                                }
                                             }
                                         }
-                                        if (!zero) gC[dir] = fma(e, hc, gC[dir]);
+                                        if (!zero) {
+                                            gC[dir] = fma(e, hc, gC[dir]);
+                                            if constexpr (!kHoldH) gB[dir] = fma(ed, hc, gB[dir]);  // dE/dD for now
+                                        }
                                     }
                                 }
                     }
@@ -562,8 +579,8 @@ __device__ __forceinline__ void grad_quartet(const GradParams &P, int row, int k
                     for (int kb = 0; kb < NB; ++kb) g_ab_contract<T, LA, LB>(ka, kb, Eb, bal, bbe, H[ka * NB + kb], gA, gB);
             }
         }
-        if constexpr (LC == 0 && LD == 0 && NN > 3) {
-            // gB holds dE/dD here; dE/dB = -(A + C + D)
+        if constexpr (NN > 3) {
+            // pp-bra classes: gB holds dE/dD here; dE/dB = -(A + C + D)
 #pragma unroll
             for (int x = 0; x < 3; ++x) gB[x] = -(gA[x] + gC[x] + gB[x]);
         }
