@@ -307,7 +307,7 @@ int jk_stream_count()
     return g_timing.enabled ? 1 : n;
 }
 
-int fork_class_streams(cudaStream_t s, cudaStream_t *cls, int &n_aux)
+int fork_class_streams(cudaStream_t s, cudaStream_t *cls, int &n_aux, bool gradient = false)
 {
     int dev = 0;
     DFTK_CUDA(cudaGetDevice(&dev));
@@ -322,8 +322,11 @@ int fork_class_streams(cudaStream_t s, cudaStream_t *cls, int &n_aux)
     // classes by cost on (H2O)_64: (ps|ss) 9.1 ms, (ss|ss) 6.0, (ps|ps) 3.3, (pp|ss) 1.8, (pp|ps) 1.8, (pp|pp) 0.5
     static const int two[DFTK_N_QCLASS] = {1, 0, 1, 0, 1, 0};
     static const int three[DFTK_N_QCLASS] = {1, 0, 2, 2, 1, 2};
+    // gradient classes: (ss|ss) 12.5 ms, (ps|ss) 17.4, (ps|ps) 8.1, (pp|ss) 4.9, (pp|ps) 14.0, (pp|pp) 11.6
+    static const int two_g[DFTK_N_QCLASS] = {1, 0, 1, 0, 1, 0};
+    static const int three_g[DFTK_N_QCLASS] = {1, 0, 2, 2, 1, 2};
     for (int c = 0; c < DFTK_N_QCLASS; ++c) {
-        const int k = n == 2 ? two[c] : three[c];
+        const int k = gradient ? (n == 2 ? two_g[c] : three_g[c]) : (n == 2 ? two[c] : three[c]);
         cls[c] = k == 0 ? s : sp.aux[k - 1];
     }
     return DFTK_OK;
@@ -822,37 +825,47 @@ int dftk_grad(const dftk_shells_t *shells, const int *shell_atom, int n_atoms, c
     }
 #define DFTK_GRAD_LAUNCH(CC)                                                  \
     if (P.total[CC] > 0) {                                                    \
-        if (timed) DFTK_CUDA(cudaEventRecord(g_timing.start[CC], s));         \
+        if (timed) DFTK_CUDA(cudaEventRecord(g_timing.start[CC], cls[CC]));         \
         if (use_list) {                                                       \
             const LaunchShape gs = launch_shape(DFTK_FAMILY_GRAD, CC, 0);     \
-            k_grad_eri<CC, true><<<shaped_grid(gs, P.total[CC]), gs.threads, smem, s>>>(P); \
+            k_grad_eri<CC, true><<<shaped_grid(gs, P.total[CC]), gs.threads, smem, cls[CC]>>>(P); \
         } else {                                                              \
-            k_grad_eri<CC, false><<<grid(P.total[CC]), GRAD_THREADS, smem, s>>>(P); \
+            k_grad_eri<CC, false><<<grid(P.total[CC]), GRAD_THREADS, smem, cls[CC]>>>(P); \
         }                                                                     \
         DFTK_LAUNCHED("k_grad_eri");                                          \
         if (timed) {                                                          \
-            DFTK_CUDA(cudaEventRecord(g_timing.stop[CC], s));                 \
+            DFTK_CUDA(cudaEventRecord(g_timing.stop[CC], cls[CC]));                 \
             g_timing.launched[CC] = true;                                     \
         }                                                                     \
         if (use_list && mixed) {                                              \
             const LaunchShape gs = launch_shape(DFTK_FAMILY_GRAD, CC, 1);     \
-            if (timed) DFTK_CUDA(cudaEventRecord(g_timing.start[DFTK_N_QCLASS + CC], s)); \
-            k_grad_eri<CC, true, float><<<shaped_grid(gs, P.total[CC]), gs.threads, smem, s>>>(P); \
+            if (timed) DFTK_CUDA(cudaEventRecord(g_timing.start[DFTK_N_QCLASS + CC], cls[CC])); \
+            k_grad_eri<CC, true, float><<<shaped_grid(gs, P.total[CC]), gs.threads, smem, cls[CC]>>>(P); \
             DFTK_LAUNCHED("k_grad_eri");                                      \
             if (timed) {                                                      \
-                DFTK_CUDA(cudaEventRecord(g_timing.stop[DFTK_N_QCLASS + CC], s)); \
+                DFTK_CUDA(cudaEventRecord(g_timing.stop[DFTK_N_QCLASS + CC], cls[CC])); \
                 g_timing.launched[DFTK_N_QCLASS + CC] = true;                 \
             }                                                                 \
         }                                                                     \
     }
-    DFTK_GRAD_LAUNCH(0)
+    // class kernels on the forked streams (their gradient sums are atomics, which commute)
+    cudaStream_t cls[DFTK_N_QCLASS];
+    int n_aux = 0;
+    int dev = 0;
+    DFTK_CUDA(cudaGetDevice(&dev));
+    std::unique_lock<std::mutex> fork_lock(g_pool[dev].mutex);
+    {
+        const int st = fork_class_streams(s, cls, n_aux, true);
+        if (st) return st;
+    }
     DFTK_GRAD_LAUNCH(1)
-    DFTK_GRAD_LAUNCH(2)
-    DFTK_GRAD_LAUNCH(3)
+    DFTK_GRAD_LAUNCH(0)
     DFTK_GRAD_LAUNCH(4)
     DFTK_GRAD_LAUNCH(5)
+    DFTK_GRAD_LAUNCH(2)
+    DFTK_GRAD_LAUNCH(3)
 #undef DFTK_GRAD_LAUNCH
-    return DFTK_OK;
+    return join_class_streams(s, n_aux);
 }
 
 int dftk_nuclear_kernel(const double *exp_a, const double *exp_b, const double *cen_a, const double *cen_b,
