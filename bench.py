@@ -681,7 +681,8 @@ def run_dftk_arm(args, rank, world, local_rank):
                                        else f"replicas x{world}")},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * N * N * 8,
                     "d2h_bytes_per_step": 3 * N * N * 8, "call": "shelled.fill_matrices (host NumPy arrays)"},
-            "gpu_launches": args.steps * (2 + sum(1 for c in range(6) if eng.quartet_totals()[c] > 0)),
+            # per build: k_dsh, one k_select and one k_jk_list per class with candidates, k_symmetrize
+            "gpu_launches": args.steps * (2 + 2 * sum(1 for c in range(6) if eng.quartet_totals()[c] > 0)),
             "roofline": {"bound": "fp64_fma", "kernel": f"k_jk<{dom},double> {QCLASS_NAMES[dom]}",
                          "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
                          "peak_source": "measured FP64 FMA loop (dftk_fma_burn) on this GPU",
