@@ -195,7 +195,12 @@ size_t dftk_workspace_bytes(const dftk_shells_t *shells, const dftk_queue_t *que
  * with bound < tau_fp32 run in FP32 (accumulation stays FP64).
  * counts (optional device array of 4 * DFTK_N_QCLASS long long, zeroed by
  * the caller) receives per class: shell quartets evaluated in FP64, then in
- * FP32, then primitive quartets evaluated in FP64, then in FP32. */
+ * FP32, then primitive quartets evaluated in FP64, then in FP32.
+ * With the selection workspace the class kernels may run on a second,
+ * library-owned stream of the same device, forked from and joined back into
+ * `stream` with events (dftk_grad does the same): the call's work still
+ * completes in `stream` order, and concurrent calls on one device take turns
+ * at the fork. */
 int dftk_jk(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N_PCLASS],
             const dftk_queue_t *queue, const double *D, const double *D_a, const double *D_b,
             double *J, double *K_a, double *K_b, int flags, double tau, double tau_fp32,
