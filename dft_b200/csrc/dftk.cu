@@ -277,16 +277,20 @@ int launch_select_class(const JkParams &P, cudaStream_t s)
     return DFTK_OK;
 }
 
-template <typename T>
-int launch_jk_list_all(const JkParams &P, cudaStream_t s, const cudaStream_t *cls_stream)
+
+// One class of the list path on stream cs: its selection pass, then its FP64
+// class kernel and, for a mixed build, its FP32 one (counts slots as in dftk_jk).
+template <int C>
+int launch_class_pipeline(JkParams P, bool mixed, long long *counts, cudaStream_t cs)
 {
     int st;
-    if ((st = launch_jk_list_class<1, T>(P, cls_stream[1]))) return st;
-    if ((st = launch_jk_list_class<0, T>(P, cls_stream[0]))) return st;
-    if ((st = launch_jk_list_class<2, T>(P, cls_stream[2]))) return st;
-    if ((st = launch_jk_list_class<3, T>(P, cls_stream[3]))) return st;
-    if ((st = launch_jk_list_class<4, T>(P, cls_stream[4]))) return st;
-    if ((st = launch_jk_list_class<5, T>(P, cls_stream[5]))) return st;
+    P.counts = counts;
+    if ((st = launch_select_class<C>(P, cs))) return st;
+    if ((st = launch_jk_list_class<C, double>(P, cs))) return st;
+    if (mixed) {
+        P.counts = counts ? counts + DFTK_N_QCLASS : nullptr;
+        if ((st = launch_jk_list_class<C, float>(P, cs))) return st;
+    }
     return DFTK_OK;
 }
 
@@ -610,23 +614,19 @@ int dftk_jk(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N_PCLASS]
         P.tau = tau;
         P.tau32 = mixed ? tau_fp32 : tau;
         P.counts = counts;
-        if ((st = launch_select_class<0>(P, s))) return st;
-        if ((st = launch_select_class<1>(P, s))) return st;
-        if ((st = launch_select_class<2>(P, s))) return st;
-        if ((st = launch_select_class<3>(P, s))) return st;
-        if ((st = launch_select_class<4>(P, s))) return st;
-        if ((st = launch_select_class<5>(P, s))) return st;
+        // per class on its stream: selection, then the FP64 (and FP32) list kernel
         cudaStream_t cls[DFTK_N_QCLASS];
         int n_aux = 0;
         int dev = 0;
         DFTK_CUDA(cudaGetDevice(&dev));
         std::unique_lock<std::mutex> fork_lock(g_pool[dev].mutex);
         if ((st = fork_class_streams(s, cls, n_aux))) return st;
-        if ((st = launch_jk_list_all<double>(P, s, cls))) return st;
-        if (mixed) {
-            P.counts = counts ? counts + DFTK_N_QCLASS : nullptr;
-            if ((st = launch_jk_list_all<float>(P, s, cls))) return st;
-        }
+        if ((st = launch_class_pipeline<1>(P, mixed, counts, cls[1]))) return st;
+        if ((st = launch_class_pipeline<0>(P, mixed, counts, cls[0]))) return st;
+        if ((st = launch_class_pipeline<2>(P, mixed, counts, cls[2]))) return st;
+        if ((st = launch_class_pipeline<3>(P, mixed, counts, cls[3]))) return st;
+        if ((st = launch_class_pipeline<4>(P, mixed, counts, cls[4]))) return st;
+        if ((st = launch_class_pipeline<5>(P, mixed, counts, cls[5]))) return st;
         if ((st = join_class_streams(s, n_aux))) return st;
         return launch_symmetrize(*shells, Y, Za, Zb, J, K_a, K_b, uhf, s);
     }
