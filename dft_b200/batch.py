@@ -340,7 +340,9 @@ def _purify(Fo: torch.Tensor, n_occ: torch.Tensor, real: torch.Tensor, tol: floa
             max_iter: int = 200) -> torch.Tensor:
     """Density D' = sum of the n_occ lowest eigenvectors' projectors of the
     symmetric Fo (B, N, N), by canonical purification.  Padded levels (real
-    == 0) are placed at the top of the Gershgorin interval.  Stops when every
+    == 0) are placed above the Gershgorin interval of the real block, by its
+    width (at least 1), so they stay apart from the real levels even when
+    every real level is occupied (a single-function atom).  Stops when every
     molecule's tr(D - D^2) (the summed deviation of its eigenvalues from 0 or
     1) is below tol, or, once below 1e-6, stops halving; the closing McWeeny step
     D <- 3D^2 - 2D^3 then squares the remaining deviations."""
@@ -349,6 +351,7 @@ def _purify(Fo: torch.Tensor, n_occ: torch.Tensor, real: torch.Tensor, tol: floa
     rad = Fo.abs().sum(dim=2) - diag.abs()
     e_max = torch.where(real > 0, diag + rad, torch.full_like(diag, -torch.inf)).amax(dim=1)
     e_min = torch.where(real > 0, diag - rad, torch.full_like(diag, torch.inf)).amin(dim=1)
+    e_max = e_max + (e_max - e_min).clamp_min(1.0)
     F = Fo + torch.diag_embed((1.0 - real) * e_max[:, None])
     mu = F.diagonal(dim1=1, dim2=2).sum(dim=1) / N
     n = n_occ.to(F.dtype)

@@ -174,6 +174,25 @@ def test_batched_purification_matches_eigh_projector():
     assert D[:, n_real:, :].abs().max() < 1e-12
 
 
+def test_purify_fully_occupied_blocks():
+    """A molecule whose every real level is occupied (one function, or a
+    closed shell filling its basis) next to padded levels: D is the identity
+    on the real block and zero on the padding, never NaN."""
+    import torch
+
+    from dft_b200.batch import _purify
+
+    F = torch.zeros(3, 4, 4, dtype=torch.float64)
+    F[0, 0, 0] = -0.9
+    F[1, :2, :2] = torch.tensor([[-1.0, 0.2], [0.2, 0.5]])
+    F[2] = torch.diag(torch.tensor([-2.0, -1.0, 0.5, 0.7], dtype=torch.float64))
+    real = torch.tensor([[1, 0, 0, 0], [1, 1, 0, 0], [1, 1, 1, 1]], dtype=torch.float64)
+    D = _purify(F, torch.tensor([1, 2, 4]), real)
+    expect = torch.diag_embed(real)
+    assert torch.isfinite(D).all()
+    assert (D - expect).abs().max() < 1e-12
+
+
 def test_batched_diis_matches_single():
     import torch
 
