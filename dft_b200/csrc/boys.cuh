@@ -18,6 +18,11 @@
 // Tables: orders L = 0..8, grid points T_k = 0, 0.1, ..., 50, computed on the
 // host in long double from the all-positive series
 // F_m(T) = exp(-T) sum_i (2T)^i / ((2m+1)(2m+3)...(2m+2i+1)).
+// Orders >= 1 in FP64 read a half-step table instead (T_k = k / 20, so
+// |T_k - T| <= 0.025): seven coefficients F_{L+j}(T_k) / j! and exp(-T_k) in
+// one 64-byte row, two 256-bit loads and no separate exp table load; the
+// seven-term series truncate below 1e-16 relative (measured 1-4 % faster on
+// the p classes than the full-step rows).
 // FP32 uses the same scheme with the first five coefficients of a float table
 // built at the float grid points, and a 5-term exp series; slot 5 of each
 // 32-byte FP32 row holds exp(-T_k), so one 256-bit load serves both.
@@ -32,6 +37,12 @@
 
 __device__ __align__(128) double g_boys64[DFTK_BOYS_NL * DFTK_BOYS_ROWS * DFTK_BOYS_W];
 __device__ double g_bexp64[DFTK_BOYS_ROWS];
+#ifndef DFTK_BOYS_HALFSTEP
+#define DFTK_BOYS_HALFSTEP 1
+#endif
+#define DFTK_BOYS_HROWS 1001   // half-step grid T_k = k / 20, k = 0..1000
+// half-step rows (orders >= 1): F_{L+j}(T_k) / j!, j = 0..6, then exp(-T_k)
+__device__ __align__(128) double g_boys64h[DFTK_BOYS_NL * DFTK_BOYS_HROWS * DFTK_BOYS_W];
 __device__ __align__(128) float g_boys32[DFTK_BOYS_NL * DFTK_BOYS_ROWS * DFTK_BOYS_W];
 __device__ float g_bexp32[DFTK_BOYS_ROWS];
 
@@ -54,7 +65,33 @@ template <int L> struct Boys<double, L> {
     static_assert(L < DFTK_BOYS_NL, "Boys order beyond the table");
     __device__ __forceinline__ static void eval(double x, double *F)
     {
-        if (x < DFTK_BOYS_TMAX) {
+        if (DFTK_BOYS_HALFSTEP && L > 0 && x < DFTK_BOYS_TMAX) {
+            // one 64-byte row: seven Taylor coefficients of F_L and exp(-T_k)
+            const double shifted = fma(x, 20.0, DFTK_ROUND_MAGIC64);  // x >= 0
+            const int k = __double2loint(shifted);
+            const double d = (shifted - DFTK_ROUND_MAGIC64) * 0.05 - x;
+            const double *rowp = g_boys64h + ((size_t)L * DFTK_BOYS_HROWS + k) * DFTK_BOYS_W;
+            double c0, c1, c2, c3, c4, c5, c6, ek;
+            ldg_v4d(rowp, c0, c1, c2, c3);
+            ldg_v4d(rowp + 4, c4, c5, c6, ek);
+            double f = fma(c6, d, c5);
+            f = fma(f, d, c4);
+            f = fma(f, d, c3);
+            f = fma(f, d, c2);
+            f = fma(f, d, c1);
+            F[L] = fma(f, d, c0);
+            double e = fma(d, 1.0 / 5040.0, 1.0 / 720.0);
+            e = fma(e, d, 1.0 / 120.0);
+            e = fma(e, d, 1.0 / 24.0);
+            e = fma(e, d, 1.0 / 6.0);
+            e = fma(e, d, 0.5);
+            e = fma(e, d, 1.0);
+            e = fma(e, d, 1.0);
+            e *= ek;
+            const double x2 = x + x;
+#pragma unroll
+            for (int m = L - 1; m >= 0; --m) F[m] = fma(x2, F[m + 1], e) * (1.0 / (2 * m + 1));
+        } else if (x < DFTK_BOYS_TMAX) {
             const double shifted = fma(x, 10.0, DFTK_ROUND_MAGIC64);  // x >= 0
             const int k = __double2loint(shifted);
             const double d = (shifted - DFTK_ROUND_MAGIC64) * 0.1 - x;

@@ -79,6 +79,7 @@ long double boys_series_ld(int m, long double T)
 
 std::vector<double> g_exp64;
 std::vector<float> g_exp32;
+std::vector<double> g_tab64h;
 
 // Per-order Taylor coefficients F_{L+j}(T_k) / j! (see boys.cuh).
 void build_tables()
@@ -110,6 +111,22 @@ void build_tables()
         // FP32 rows use coefficients 0..4; slot 5 carries exp(-T_k) (see boys.cuh)
         for (int L = 0; L < NL; ++L) g_tab32[((size_t)L * R + k) * W + 5] = g_exp32[k];
     }
+    // half-step FP64 rows: F_{L+j}(T_k) / j! for j = 0..6 and exp(-T_k) in slot 7
+    const int RH = DFTK_BOYS_HROWS;
+    g_tab64h.assign((size_t)NL * RH * W, 0.0);
+    for (int k = 0; k < RH; ++k) {
+        const long double t = (long double)((double)k * 0.05);  // grid the evaluator rounds to
+        for (int m = 0; m < NL + W; ++m) F64[m] = boys_series_ld(m, t);
+        const double ek = (double)expl(-t);
+        for (int L = 0; L < NL; ++L) {
+            long double fact = 1.0L;
+            for (int j = 0; j < W - 1; ++j) {
+                if (j > 0) fact *= j;
+                g_tab64h[((size_t)L * RH + k) * W + j] = (double)(F64[L + j] / fact);
+            }
+            g_tab64h[((size_t)L * RH + k) * W + W - 1] = ek;
+        }
+    }
 }
 
 int ensure_init()
@@ -124,6 +141,7 @@ int ensure_init()
     DFTK_CUDA(cudaMemcpyToSymbol(g_boys32, g_tab32.data(), sizeof(float) * g_tab32.size()));
     DFTK_CUDA(cudaMemcpyToSymbol(g_bexp64, g_exp64.data(), sizeof(double) * g_exp64.size()));
     DFTK_CUDA(cudaMemcpyToSymbol(g_bexp32, g_exp32.data(), sizeof(float) * g_exp32.size()));
+    DFTK_CUDA(cudaMemcpyToSymbol(g_boys64h, g_tab64h.data(), sizeof(double) * g_tab64h.size()));
     StreamPool &sp = g_pool[dev];
     for (int i = 0; i < 2; ++i) {
         DFTK_CUDA(cudaStreamCreateWithFlags(&sp.aux[i], cudaStreamNonBlocking));

@@ -121,35 +121,74 @@ struct EriClass<T, 1, 0> {
       const T bAy = __ldg(brec + 7 * bra_fs);
       const T bAz = __ldg(brec + 8 * bra_fs);
       T W0_000 = T(0), W0_001 = T(0), W0_010 = T(0), W0_100 = T(0);
-      #pragma unroll 1
-      for (int j = 0; j < ket_n; ++j) {
-        if (qo * __ldg(ket_qp + j * ket_st) < eps) break;
-        ++evaluated;
-        const T* __restrict__ krec = ket_p + j * ket_st;
-        const T kPx = __ldg(krec + 0);
-        const T kPy = __ldg(krec + ket_fs);
-        const T kPz = __ldg(krec + 2 * ket_fs);
-        const T kp = __ldg(krec + 3 * ket_fs);
-        const T kK = __ldg(krec + 4 * ket_fs);
-        const T s = bp + kp;
-        const T rs = Math<T>::rsqrt(s);
-        const T rho = bp * kp * (rs * rs);
-        const T X = bPx - kPx, Y = bPy - kPy, Z = bPz - kPz;
-        const T pre = bK * kK * rs;
-        const T m2rho = T(-2) * rho;
-        T F[2];
-        Boys<T, 1>::eval(rho * (X * X + Y * Y + Z * Z), F);
-        T cpow = pre;
-        const T R000_0 = cpow * F[0];
-        cpow *= m2rho;
-        const T R000_1 = cpow * F[1];
-        const T R001_0 = Z * R000_1;
-        const T R010_0 = Y * R000_1;
-        const T R100_0 = X * R000_1;
-        W0_000 += R000_0;
-        W0_001 += R001_0;
-        W0_010 += R010_0;
-        W0_100 += R100_0;
+      if constexpr (sizeof(T) == 4) {
+        float knq = __ldg(ket_qp);
+        T knPx = __ldg(ket_p + 0), knPy = __ldg(ket_p + ket_fs), knPz = __ldg(ket_p + 2 * ket_fs), knp = __ldg(ket_p + 3 * ket_fs), knK = __ldg(ket_p + 4 * ket_fs);
+        #pragma unroll 1
+        for (int j = 0; j < ket_n; ++j) {
+          const float kcq = knq;
+          const T kPx = knPx, kPy = knPy, kPz = knPz, kp = knp, kK = knK;
+          if (qo * kcq < eps) break;
+          const int jn = j + 1 < ket_n ? j + 1 : j;
+          knq = __ldg(ket_qp + jn * ket_st);
+          const T* __restrict__ knrec = ket_p + jn * ket_st;
+          knPx = __ldg(knrec + 0);
+          knPy = __ldg(knrec + ket_fs);
+          knPz = __ldg(knrec + 2 * ket_fs);
+          knp = __ldg(knrec + 3 * ket_fs);
+          knK = __ldg(knrec + 4 * ket_fs);
+          ++evaluated;
+          const T s = bp + kp;
+          const T rs = Math<T>::rsqrt(s);
+          const T rho = bp * kp * (rs * rs);
+          const T X = bPx - kPx, Y = bPy - kPy, Z = bPz - kPz;
+          const T pre = bK * kK * rs;
+          const T m2rho = T(-2) * rho;
+          T F[2];
+          Boys<T, 1>::eval(rho * (X * X + Y * Y + Z * Z), F);
+          T cpow = pre;
+          const T R000_0 = cpow * F[0];
+          cpow *= m2rho;
+          const T R000_1 = cpow * F[1];
+          const T R001_0 = Z * R000_1;
+          const T R010_0 = Y * R000_1;
+          const T R100_0 = X * R000_1;
+          W0_000 += R000_0;
+          W0_001 += R001_0;
+          W0_010 += R010_0;
+          W0_100 += R100_0;
+        }
+      } else {
+        #pragma unroll 1
+        for (int j = 0; j < ket_n; ++j) {
+          if (qo * __ldg(ket_qp + j * ket_st) < eps) break;
+          const T* __restrict__ krec = ket_p + j * ket_st;
+          const T kPx = __ldg(krec + 0);
+          const T kPy = __ldg(krec + ket_fs);
+          const T kPz = __ldg(krec + 2 * ket_fs);
+          const T kp = __ldg(krec + 3 * ket_fs);
+          const T kK = __ldg(krec + 4 * ket_fs);
+          ++evaluated;
+          const T s = bp + kp;
+          const T rs = Math<T>::rsqrt(s);
+          const T rho = bp * kp * (rs * rs);
+          const T X = bPx - kPx, Y = bPy - kPy, Z = bPz - kPz;
+          const T pre = bK * kK * rs;
+          const T m2rho = T(-2) * rho;
+          T F[2];
+          Boys<T, 1>::eval(rho * (X * X + Y * Y + Z * Z), F);
+          T cpow = pre;
+          const T R000_0 = cpow * F[0];
+          cpow *= m2rho;
+          const T R000_1 = cpow * F[1];
+          const T R001_0 = Z * R000_1;
+          const T R010_0 = Y * R000_1;
+          const T R100_0 = X * R000_1;
+          W0_000 += R000_0;
+          W0_001 += R001_0;
+          W0_010 += R010_0;
+          W0_100 += R100_0;
+        }
       }
       I[0] = fma(bAx, W0_000, I[0]);
       I[0] = fma(bh, W0_100, I[0]);
@@ -200,17 +239,12 @@ struct EriClass<T, 2, 0> {
       const T kPz = __ldg(krec + 2 * ket_fs);
       const T kp = __ldg(krec + 3 * ket_fs);
       const T kK = __ldg(krec + 4 * ket_fs);
-      const T kh = __ldg(krec + 5 * ket_fs);
-      const T kAx = __ldg(krec + 6 * ket_fs);
-      const T kAy = __ldg(krec + 7 * ket_fs);
-      const T kAz = __ldg(krec + 8 * ket_fs);
       T V0_000 = T(0), V0_001 = T(0), V0_010 = T(0), V0_100 = T(0);
       T V1_000 = T(0), V1_001 = T(0), V1_010 = T(0), V1_100 = T(0);
       T V2_000 = T(0), V2_001 = T(0), V2_010 = T(0), V2_100 = T(0);
       #pragma unroll 1
       for (int i = 0; i < bra_n; ++i) {
         if (qo * __ldg(bra_qp + i * bra_st) < eps) break;
-        ++evaluated;
         const T* __restrict__ brec = bra_p + i * bra_st;
         const T bPx = __ldg(brec + 0);
         const T bPy = __ldg(brec + bra_fs);
@@ -221,6 +255,7 @@ struct EriClass<T, 2, 0> {
         const T bAx = __ldg(brec + 6 * bra_fs);
         const T bAy = __ldg(brec + 7 * bra_fs);
         const T bAz = __ldg(brec + 8 * bra_fs);
+        ++evaluated;
         const T s = bp + kp;
         const T rs = Math<T>::rsqrt(s);
         const T rho = bp * kp * (rs * rs);
@@ -278,6 +313,10 @@ struct EriClass<T, 2, 0> {
         V2_010 = fma(bc2_001, R011_0, V2_010);
         V2_100 = fma(bc2_001, R101_0, V2_100);
       }
+      const T kh = __ldg(krec + 5 * ket_fs);
+      const T kAx = __ldg(krec + 6 * ket_fs);
+      const T kAy = __ldg(krec + 7 * ket_fs);
+      const T kAz = __ldg(krec + 8 * ket_fs);
       I[0] = fma(kAx, V0_000, I[0]);
       I[0] = fma(-kh, V0_100, I[0]);
       I[3] = fma(kAx, V1_000, I[3]);
@@ -339,20 +378,6 @@ struct EriClass<T, 3, 0> {
       const T bPz = __ldg(brec + 2 * bra_fs);
       const T bp = __ldg(brec + 3 * bra_fs);
       const T bK = __ldg(brec + 4 * bra_fs);
-      const T bh = __ldg(brec + 5 * bra_fs);
-      const T bAx = __ldg(brec + 6 * bra_fs);
-      const T bAy = __ldg(brec + 7 * bra_fs);
-      const T bAz = __ldg(brec + 8 * bra_fs);
-      const T bBx = __ldg(brec + 9 * bra_fs);
-      const T bBy = __ldg(brec + 10 * bra_fs);
-      const T bBz = __ldg(brec + 11 * bra_fs);
-      const T bEx0 = bAx * bBx + bh;
-      const T bEx1 = bh * (bAx + bBx);
-      const T bEy0 = bAy * bBy + bh;
-      const T bEy1 = bh * (bAy + bBy);
-      const T bEz0 = bAz * bBz + bh;
-      const T bEz1 = bh * (bAz + bBz);
-      const T bh2 = bh * bh;
       T W0_000 = T(0), W0_001 = T(0), W0_002 = T(0), W0_010 = T(0), W0_011 = T(0), W0_020 = T(0), W0_100 = T(0), W0_101 = T(0), W0_110 = T(0), W0_200 = T(0);
       float knq = __ldg(ket_qp);
       T knPx = __ldg(ket_p + 0), knPy = __ldg(ket_p + ket_fs), knPz = __ldg(ket_p + 2 * ket_fs), knp = __ldg(ket_p + 3 * ket_fs), knK = __ldg(ket_p + 4 * ket_fs);
@@ -407,6 +432,20 @@ struct EriClass<T, 3, 0> {
         W0_110 += R110_0;
         W0_200 += R200_0;
       }
+      const T bh = __ldg(brec + 5 * bra_fs);
+      const T bAx = __ldg(brec + 6 * bra_fs);
+      const T bAy = __ldg(brec + 7 * bra_fs);
+      const T bAz = __ldg(brec + 8 * bra_fs);
+      const T bBx = __ldg(brec + 9 * bra_fs);
+      const T bBy = __ldg(brec + 10 * bra_fs);
+      const T bBz = __ldg(brec + 11 * bra_fs);
+      const T bEx0 = bAx * bBx + bh;
+      const T bEx1 = bh * (bAx + bBx);
+      const T bEy0 = bAy * bBy + bh;
+      const T bEy1 = bh * (bAy + bBy);
+      const T bEz0 = bAz * bBz + bh;
+      const T bEz1 = bh * (bAz + bBz);
+      const T bh2 = bh * bh;
       I[0] = fma(bEx0, W0_000, I[0]);
       I[0] = fma(bEx1, W0_100, I[0]);
       I[0] = fma(bh2, W0_200, I[0]);
@@ -483,27 +522,12 @@ struct EriClass<T, 4, 0> {
       const T bPz = __ldg(brec + 2 * bra_fs);
       const T bp = __ldg(brec + 3 * bra_fs);
       const T bK = __ldg(brec + 4 * bra_fs);
-      const T bh = __ldg(brec + 5 * bra_fs);
-      const T bAx = __ldg(brec + 6 * bra_fs);
-      const T bAy = __ldg(brec + 7 * bra_fs);
-      const T bAz = __ldg(brec + 8 * bra_fs);
-      const T bBx = __ldg(brec + 9 * bra_fs);
-      const T bBy = __ldg(brec + 10 * bra_fs);
-      const T bBz = __ldg(brec + 11 * bra_fs);
-      const T bEx0 = bAx * bBx + bh;
-      const T bEx1 = bh * (bAx + bBx);
-      const T bEy0 = bAy * bBy + bh;
-      const T bEy1 = bh * (bAy + bBy);
-      const T bEz0 = bAz * bBz + bh;
-      const T bEz1 = bh * (bAz + bBz);
-      const T bh2 = bh * bh;
       T W0_000 = T(0), W0_001 = T(0), W0_002 = T(0), W0_010 = T(0), W0_011 = T(0), W0_020 = T(0), W0_100 = T(0), W0_101 = T(0), W0_110 = T(0), W0_200 = T(0);
       T W1_000 = T(0), W1_001 = T(0), W1_002 = T(0), W1_010 = T(0), W1_011 = T(0), W1_020 = T(0), W1_100 = T(0), W1_101 = T(0), W1_110 = T(0), W1_200 = T(0);
       T W2_000 = T(0), W2_001 = T(0), W2_002 = T(0), W2_010 = T(0), W2_011 = T(0), W2_020 = T(0), W2_100 = T(0), W2_101 = T(0), W2_110 = T(0), W2_200 = T(0);
       #pragma unroll 1
       for (int j = 0; j < ket_n; ++j) {
         if (qo * __ldg(ket_qp + j * ket_st) < eps) break;
-        ++evaluated;
         const T* __restrict__ krec = ket_p + j * ket_st;
         const T kPx = __ldg(krec + 0);
         const T kPy = __ldg(krec + ket_fs);
@@ -514,6 +538,7 @@ struct EriClass<T, 4, 0> {
         const T kAx = __ldg(krec + 6 * ket_fs);
         const T kAy = __ldg(krec + 7 * ket_fs);
         const T kAz = __ldg(krec + 8 * ket_fs);
+        ++evaluated;
         const T s = bp + kp;
         const T rs = Math<T>::rsqrt(s);
         const T rho = bp * kp * (rs * rs);
@@ -628,6 +653,20 @@ struct EriClass<T, 4, 0> {
         W2_110 = fma(kc2_001, R111_0, W2_110);
         W2_200 = fma(kc2_001, R201_0, W2_200);
       }
+      const T bh = __ldg(brec + 5 * bra_fs);
+      const T bAx = __ldg(brec + 6 * bra_fs);
+      const T bAy = __ldg(brec + 7 * bra_fs);
+      const T bAz = __ldg(brec + 8 * bra_fs);
+      const T bBx = __ldg(brec + 9 * bra_fs);
+      const T bBy = __ldg(brec + 10 * bra_fs);
+      const T bBz = __ldg(brec + 11 * bra_fs);
+      const T bEx0 = bAx * bBx + bh;
+      const T bEx1 = bh * (bAx + bBx);
+      const T bEy0 = bAy * bBy + bh;
+      const T bEy1 = bh * (bAy + bBy);
+      const T bEz0 = bAz * bBz + bh;
+      const T bEz1 = bh * (bAz + bBz);
+      const T bh2 = bh * bh;
       I[0] = fma(bEx0, W0_000, I[0]);
       I[0] = fma(bEx1, W0_100, I[0]);
       I[0] = fma(bh2, W0_200, I[0]);
@@ -770,20 +809,6 @@ struct EriClass<T, 5, 0> {
       const T bPz = __ldg(brec + 2 * bra_fs);
       const T bp = __ldg(brec + 3 * bra_fs);
       const T bK = __ldg(brec + 4 * bra_fs);
-      const T bh = __ldg(brec + 5 * bra_fs);
-      const T bAx = __ldg(brec + 6 * bra_fs);
-      const T bAy = __ldg(brec + 7 * bra_fs);
-      const T bAz = __ldg(brec + 8 * bra_fs);
-      const T bBx = __ldg(brec + 9 * bra_fs);
-      const T bBy = __ldg(brec + 10 * bra_fs);
-      const T bBz = __ldg(brec + 11 * bra_fs);
-      const T bEx0 = bAx * bBx + bh;
-      const T bEx1 = bh * (bAx + bBx);
-      const T bEy0 = bAy * bBy + bh;
-      const T bEy1 = bh * (bAy + bBy);
-      const T bEz0 = bAz * bBz + bh;
-      const T bEz1 = bh * (bAz + bBz);
-      const T bh2 = bh * bh;
       T W0_000 = T(0), W0_001 = T(0), W0_002 = T(0), W0_010 = T(0), W0_011 = T(0), W0_020 = T(0), W0_100 = T(0), W0_101 = T(0), W0_110 = T(0), W0_200 = T(0);
       T W1_000 = T(0), W1_001 = T(0), W1_002 = T(0), W1_010 = T(0), W1_011 = T(0), W1_020 = T(0), W1_100 = T(0), W1_101 = T(0), W1_110 = T(0), W1_200 = T(0);
       T W2_000 = T(0), W2_001 = T(0), W2_002 = T(0), W2_010 = T(0), W2_011 = T(0), W2_020 = T(0), W2_100 = T(0), W2_101 = T(0), W2_110 = T(0), W2_200 = T(0);
@@ -1017,6 +1042,20 @@ struct EriClass<T, 5, 0> {
         W2_110 = fma(kc2_101, R211_0, W2_110);
         W2_200 = fma(kc2_101, R301_0, W2_200);
       }
+      const T bh = __ldg(brec + 5 * bra_fs);
+      const T bAx = __ldg(brec + 6 * bra_fs);
+      const T bAy = __ldg(brec + 7 * bra_fs);
+      const T bAz = __ldg(brec + 8 * bra_fs);
+      const T bBx = __ldg(brec + 9 * bra_fs);
+      const T bBy = __ldg(brec + 10 * bra_fs);
+      const T bBz = __ldg(brec + 11 * bra_fs);
+      const T bEx0 = bAx * bBx + bh;
+      const T bEx1 = bh * (bAx + bBx);
+      const T bEy0 = bAy * bBy + bh;
+      const T bEy1 = bh * (bAy + bBy);
+      const T bEz0 = bAz * bBz + bh;
+      const T bEz1 = bh * (bAz + bBz);
+      const T bh2 = bh * bh;
       I[0] = fma(bEx0, W0_000, I[0]);
       I[0] = fma(bEx1, W0_100, I[0]);
       I[0] = fma(bh2, W0_200, I[0]);
@@ -1159,20 +1198,6 @@ struct EriClass<T, 5, 1> {
       const T bPz = __ldg(brec + 2 * bra_fs);
       const T bp = __ldg(brec + 3 * bra_fs);
       const T bK = __ldg(brec + 4 * bra_fs);
-      const T bh = __ldg(brec + 5 * bra_fs);
-      const T bAx = __ldg(brec + 6 * bra_fs);
-      const T bAy = __ldg(brec + 7 * bra_fs);
-      const T bAz = __ldg(brec + 8 * bra_fs);
-      const T bBx = __ldg(brec + 9 * bra_fs);
-      const T bBy = __ldg(brec + 10 * bra_fs);
-      const T bBz = __ldg(brec + 11 * bra_fs);
-      const T bEx0 = bAx * bBx + bh;
-      const T bEx1 = bh * (bAx + bBx);
-      const T bEy0 = bAy * bBy + bh;
-      const T bEy1 = bh * (bAy + bBy);
-      const T bEz0 = bAz * bBz + bh;
-      const T bEz1 = bh * (bAz + bBz);
-      const T bh2 = bh * bh;
       T W0_000 = T(0), W0_001 = T(0), W0_002 = T(0), W0_010 = T(0), W0_011 = T(0), W0_020 = T(0), W0_100 = T(0), W0_101 = T(0), W0_110 = T(0), W0_200 = T(0);
       T W1_000 = T(0), W1_001 = T(0), W1_002 = T(0), W1_010 = T(0), W1_011 = T(0), W1_020 = T(0), W1_100 = T(0), W1_101 = T(0), W1_110 = T(0), W1_200 = T(0);
       T W2_000 = T(0), W2_001 = T(0), W2_002 = T(0), W2_010 = T(0), W2_011 = T(0), W2_020 = T(0), W2_100 = T(0), W2_101 = T(0), W2_110 = T(0), W2_200 = T(0);
@@ -1400,6 +1425,20 @@ struct EriClass<T, 5, 1> {
         W2_110 = fma(kc2_011, R121_0, W2_110);
         W2_200 = fma(kc2_011, R211_0, W2_200);
       }
+      const T bh = __ldg(brec + 5 * bra_fs);
+      const T bAx = __ldg(brec + 6 * bra_fs);
+      const T bAy = __ldg(brec + 7 * bra_fs);
+      const T bAz = __ldg(brec + 8 * bra_fs);
+      const T bBx = __ldg(brec + 9 * bra_fs);
+      const T bBy = __ldg(brec + 10 * bra_fs);
+      const T bBz = __ldg(brec + 11 * bra_fs);
+      const T bEx0 = bAx * bBx + bh;
+      const T bEx1 = bh * (bAx + bBx);
+      const T bEy0 = bAy * bBy + bh;
+      const T bEy1 = bh * (bAy + bBy);
+      const T bEz0 = bAz * bBz + bh;
+      const T bEz1 = bh * (bAz + bBz);
+      const T bh2 = bh * bh;
       I[0] = fma(bEx0, W0_000, I[0]);
       I[0] = fma(bEx1, W0_100, I[0]);
       I[0] = fma(bh2, W0_200, I[0]);
@@ -1542,20 +1581,6 @@ struct EriClass<T, 5, 2> {
       const T bPz = __ldg(brec + 2 * bra_fs);
       const T bp = __ldg(brec + 3 * bra_fs);
       const T bK = __ldg(brec + 4 * bra_fs);
-      const T bh = __ldg(brec + 5 * bra_fs);
-      const T bAx = __ldg(brec + 6 * bra_fs);
-      const T bAy = __ldg(brec + 7 * bra_fs);
-      const T bAz = __ldg(brec + 8 * bra_fs);
-      const T bBx = __ldg(brec + 9 * bra_fs);
-      const T bBy = __ldg(brec + 10 * bra_fs);
-      const T bBz = __ldg(brec + 11 * bra_fs);
-      const T bEx0 = bAx * bBx + bh;
-      const T bEx1 = bh * (bAx + bBx);
-      const T bEy0 = bAy * bBy + bh;
-      const T bEy1 = bh * (bAy + bBy);
-      const T bEz0 = bAz * bBz + bh;
-      const T bEz1 = bh * (bAz + bBz);
-      const T bh2 = bh * bh;
       T W0_000 = T(0), W0_001 = T(0), W0_002 = T(0), W0_010 = T(0), W0_011 = T(0), W0_020 = T(0), W0_100 = T(0), W0_101 = T(0), W0_110 = T(0), W0_200 = T(0);
       T W1_000 = T(0), W1_001 = T(0), W1_002 = T(0), W1_010 = T(0), W1_011 = T(0), W1_020 = T(0), W1_100 = T(0), W1_101 = T(0), W1_110 = T(0), W1_200 = T(0);
       T W2_000 = T(0), W2_001 = T(0), W2_002 = T(0), W2_010 = T(0), W2_011 = T(0), W2_020 = T(0), W2_100 = T(0), W2_101 = T(0), W2_110 = T(0), W2_200 = T(0);
@@ -1780,6 +1805,20 @@ struct EriClass<T, 5, 2> {
         W2_110 = fma(kc2_002, R112_0, W2_110);
         W2_200 = fma(kc2_002, R202_0, W2_200);
       }
+      const T bh = __ldg(brec + 5 * bra_fs);
+      const T bAx = __ldg(brec + 6 * bra_fs);
+      const T bAy = __ldg(brec + 7 * bra_fs);
+      const T bAz = __ldg(brec + 8 * bra_fs);
+      const T bBx = __ldg(brec + 9 * bra_fs);
+      const T bBy = __ldg(brec + 10 * bra_fs);
+      const T bBz = __ldg(brec + 11 * bra_fs);
+      const T bEx0 = bAx * bBx + bh;
+      const T bEx1 = bh * (bAx + bBx);
+      const T bEy0 = bAy * bBy + bh;
+      const T bEy1 = bh * (bAy + bBy);
+      const T bEz0 = bAz * bBz + bh;
+      const T bEz1 = bh * (bAz + bBz);
+      const T bh2 = bh * bh;
       I[0] = fma(bEx0, W0_000, I[0]);
       I[0] = fma(bEx1, W0_100, I[0]);
       I[0] = fma(bh2, W0_200, I[0]);

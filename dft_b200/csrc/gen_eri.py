@@ -45,6 +45,16 @@ PAIR_FIELDS = {0: 5, 1: 9, 2: 12}  # record fields the ERI code loads (the store
 # classes whose inner primitive loop loads the next primitive pair's record
 # one iteration ahead
 PREFETCH_CLASSES = {0, 3, 5}  # measured on B200: the others lose more to register spills
+# classes whose FP32 instantiation prefetches although the FP64 one does not
+# (FP32 records take half the registers)
+PREFETCH_FP32_CLASSES = {1}
+# classes whose outer side's transform fields (h, PA, PB and the Hermite
+# coefficients built from them) are loaded after the inner primitive loop,
+# where the outer-side Hermite-to-Cartesian transform uses them, so they hold
+# no registers across the loop (measured on B200: (ps|ps) 3.29 -> 3.17 ms,
+# (pp|ss) 1.79 -> 1.62, (pp|ps) 1.74 -> 1.63 per (H2O)_64 build; (ps|ss)
+# 9.0 -> 9.3, so it loads them up front)
+DEFER_CLASSES = {2, 3, 4, 5}
 
 
 def e1d(side, a, b, axis):
@@ -133,13 +143,17 @@ def prod(facs):
     return " * ".join(facs) if facs else "T(1)"
 
 
-def side_loads(side, pc, var, idx):
-    """Load the fields of one primitive pair record through the per-thread
-    base pointer {var}_p (32-bit offsets: field f at f * {var}_fs)."""
+N_CORE_FIELDS = 5  # Px, Py, Pz, p, K: what the primitive-quartet core reads
+
+
+def side_loads(side, pc, var, idx, first=0, last=None):
+    """Load fields [first, last) of one primitive pair record through the
+    per-thread base pointer {var}_p (32-bit offsets: field f at f * {var}_fs);
+    the record pointer is declared with the first field range."""
     names = ["Px", "Py", "Pz", "p", "K", "h", "Ax", "Ay", "Az", "Bx", "By", "Bz"]
-    n = PAIR_FIELDS[pc]
-    out = [f"const T* __restrict__ {side}rec = {var}_p + {idx} * {var}_st;"]
-    for f in range(n):
+    n = PAIR_FIELDS[pc] if last is None else min(last, PAIR_FIELDS[pc])
+    out = [f"const T* __restrict__ {side}rec = {var}_p + {idx} * {var}_st;"] if first == 0 else []
+    for f in range(first, n):
         off = "0" if f == 0 else (f"{var}_fs" if f == 1 else f"{f} * {var}_fs")
         out.append(f"const T {side}{names[f]} = __ldg({side}rec + {off});")
     return out
@@ -183,8 +197,25 @@ def side_pre(side, pc):
     return lines
 
 
+def inner_loop_variants(cid, pf_loop, plain_loop, plain_loads, inner_pre, inner):
+    """The inner primitive loop (indented into the outer loop's body): the
+    prefetching form, the plain form, or both behind an FP32/FP64 switch."""
+    def form(pf):
+        head = pf_loop if pf else plain_loop
+        pre = [] if pf else ["  " + x for x in plain_loads]
+        return head + pre + ["  ++evaluated;"] + ["  " + x for x in inner_pre + inner] + ["}"]
+
+    if cid in PREFETCH_CLASSES:
+        lines = form(True)
+    elif cid in PREFETCH_FP32_CLASSES:
+        lines = ["if constexpr (sizeof(T) == 4) {"] + ["  " + x for x in form(True)] + ["} else {"]
+        lines += ["  " + x for x in form(False)] + ["}"]
+    else:
+        lines = form(False)
+    return ["  " + x for x in lines]
+
+
 def gen_class(cid, la, lb, lc, ld, nsplit, split, order):
-    PREFETCH = cid in PREFETCH_CLASSES
     """order 'bra': bra primitive loop outside, the ket transform per primitive
     quartet and the bra transform hoisted; order 'ket': the mirror image (ket
     records loaded once per quartet, bra records re-read as warp-broadcast)."""
@@ -224,19 +255,15 @@ def gen_class(cid, la, lb, lc, ld, nsplit, split, order):
         body.append("for (int i = 0; i < bra_n; ++i) {")
         body.append("  const float qo = __ldg(bra_qp + i * bra_st);")
         body.append("  if (qo * kq0 < eps) break;")
-        body += ["  " + x for x in side_loads("b", pa, "bra", "i") + side_pre("b", pa)]
+        ncore = N_CORE_FIELDS if cid in DEFER_CLASSES else None
+        body += ["  " + x for x in side_loads("b", pa, "bra", "i", 0, ncore)]
         for m in range(len(cds)):
             body.append("  T " + ", ".join(f"{w(m, h)} = T(0)" for h in hb) + ";")
-        if PREFETCH:
-            body += ["  " + x for x in prefetched_inner_loop("k", pk, "ket", "j", "ket_n", "qo", "ket_qp")]
-            body.append("    ++evaluated;")
-            inner = side_pre("k", pk) + list(core)
-        else:
-            body.append("  #pragma unroll 1")
-            body.append("  for (int j = 0; j < ket_n; ++j) {")
-            body.append("    if (qo * __ldg(ket_qp + j * ket_st) < eps) break;")
-            body.append("    ++evaluated;")
-            inner = side_loads("k", pk, "ket", "j") + side_pre("k", pk) + list(core)
+        pf_loop = prefetched_inner_loop("k", pk, "ket", "j", "ket_n", "qo", "ket_qp")
+        plain_loop = ["#pragma unroll 1", "for (int j = 0; j < ket_n; ++j) {",
+                      "  if (qo * __ldg(ket_qp + j * ket_st) < eps) break;"]
+        inner_pre = side_pre("k", pk)
+        inner = list(core)
         for m, terms in ket_terms.items():
             for (tk, uk, vk), sg, facs in terms:
                 cname = f"kc{m}_{tk}{uk}{vk}"
@@ -249,8 +276,10 @@ def gen_class(cid, la, lb, lc, ld, nsplit, split, order):
                         inner.append(f"{tgt} = fma({cname}, {r}, {tgt});")
                     else:
                         inner.append(f"{tgt} {'-=' if sg < 0 else '+='} {r};")
-        body += ["    " + x for x in inner]
-        body.append("  }")
+        body += inner_loop_variants(cid, pf_loop, plain_loop, side_loads("k", pk, "ket", "j"), inner_pre, inner)
+        if ncore is not None:
+            body += ["  " + x for x in side_loads("b", pa, "bra", "i", ncore)]
+        body += ["  " + x for x in side_pre("b", pa)]
         for n, terms in bra_terms.items():
             for m in range(len(cds)):
                 acc = f"I[{n * len(cds) + m}]"
@@ -265,19 +294,15 @@ def gen_class(cid, la, lb, lc, ld, nsplit, split, order):
         body.append("for (int j = 0; j < ket_n; ++j) {")
         body.append("  const float qo = __ldg(ket_qp + j * ket_st);")
         body.append("  if (qo * bq0 < eps) break;")
-        body += ["  " + x for x in side_loads("k", pk, "ket", "j") + side_pre("k", pk)]
+        ncore = N_CORE_FIELDS if cid in DEFER_CLASSES else None
+        body += ["  " + x for x in side_loads("k", pk, "ket", "j", 0, ncore)]
         for n in range(len(abs_)):
             body.append("  T " + ", ".join(f"{w(n, h)} = T(0)" for h in hk) + ";")
-        if PREFETCH:
-            body += ["  " + x for x in prefetched_inner_loop("b", pa, "bra", "i", "bra_n", "qo", "bra_qp")]
-            body.append("    ++evaluated;")
-            inner = side_pre("b", pa) + list(core)
-        else:
-            body.append("  #pragma unroll 1")
-            body.append("  for (int i = 0; i < bra_n; ++i) {")
-            body.append("    if (qo * __ldg(bra_qp + i * bra_st) < eps) break;")
-            body.append("    ++evaluated;")
-            inner = side_loads("b", pa, "bra", "i") + side_pre("b", pa) + list(core)
+        pf_loop = prefetched_inner_loop("b", pa, "bra", "i", "bra_n", "qo", "bra_qp")
+        plain_loop = ["#pragma unroll 1", "for (int i = 0; i < bra_n; ++i) {",
+                      "  if (qo * __ldg(bra_qp + i * bra_st) < eps) break;"]
+        inner_pre = side_pre("b", pa)
+        inner = list(core)
         for n, terms in bra_terms.items():
             for (tb, ub, vb), _, facs in terms:
                 cname = f"bc{n}_{tb}{ub}{vb}"
@@ -287,8 +312,10 @@ def gen_class(cid, la, lb, lc, ld, nsplit, split, order):
                     r = rname(tb + tk, ub + uk, vb + vk, 0)
                     tgt = w(n, (tk, uk, vk))
                     inner.append(f"{tgt} = fma({cname}, {r}, {tgt});" if facs else f"{tgt} += {r};")
-        body += ["    " + x for x in inner]
-        body.append("  }")
+        body += inner_loop_variants(cid, pf_loop, plain_loop, side_loads("b", pa, "bra", "i"), inner_pre, inner)
+        if ncore is not None:
+            body += ["  " + x for x in side_loads("k", pk, "ket", "j", ncore)]
+        body += ["  " + x for x in side_pre("k", pk)]
         # ket transform with the (-1)^{tau+nu+phi} sign
         for m, terms in ket_terms.items():
             for n in range(len(abs_)):
