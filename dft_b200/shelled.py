@@ -41,9 +41,14 @@ _ENGINES: Dict[Tuple, IntegralEngine] = {}
 
 
 def _fingerprint(shells: List[Dict]) -> Tuple:
-    return tuple((s["angular_momentum"], s["ao_start"], tuple(np.round(np.asarray(s["atom_pos"]), 12)),
-                  tuple(np.asarray(s["exponents"]).tolist()), tuple(np.asarray(s["coefficients"]).ravel().tolist()))
-                 for s in shells)
+    """Value key of a shell list (momenta, AO offsets, centres to 1e-12,
+    exponents, coefficients): a call with equal shells finds the cached engine,
+    a changed geometry or basis builds a new one."""
+    meta = tuple((s["angular_momentum"], s["ao_start"]) for s in shells)
+    pos = np.round(np.array([np.ravel(s["atom_pos"]) for s in shells], dtype=np.float64), 12).tobytes()
+    ex = tuple(tuple(np.asarray(s["exponents"], dtype=np.float64).tolist()) for s in shells)
+    co = tuple(tuple(np.asarray(s["coefficients"], dtype=np.float64).ravel().tolist()) for s in shells)
+    return (meta, pos, ex, co)
 
 
 def get_engine(shells: List[Dict], tau_schwarz: float = 1e-12) -> IntegralEngine:
@@ -222,11 +227,18 @@ def fill_matrices(shells, P, P_a, P_b, J_matrix, K_a, K_b, tau: float = 0.0):
     same = (P_a is P_b) or (np.shares_memory(P_a, P_b) if isinstance(P_a, np.ndarray) and isinstance(P_b, np.ndarray)
                             else False)
     J, Ka, Kb = eng.jk(P, P_a, None if same else P_b, uhf=not same, tau=tau)
-    for dst, src in ((J_matrix, J), (K_a, Ka), (K_b, Kb)):
+    pairs = ((J_matrix, J), (K_a, Ka), (K_b, Kb))
+    # host destinations: one device-to-host copy of the distinct results
+    srcs = []
+    for dst, src in pairs:
+        if not isinstance(dst, torch.Tensor) and not any(src is x for x in srcs):
+            srcs.append(src)
+    host = torch.stack(srcs).cpu().numpy() if srcs else None
+    for dst, src in pairs:
         if isinstance(dst, torch.Tensor):
             dst += src.to(dst.device, dst.dtype)
         else:
-            dst += src.cpu().numpy()
+            dst += host[next(i for i, x in enumerate(srcs) if x is src)]
 
 
 def independent(shells, sphere_total_ao, C):
