@@ -431,6 +431,82 @@ def cpu_reference_class_rates(shells, q_by_class, per_class, seed=0):
     return rates, orc.lib().orc_num_threads(), "reference" if ref is not None else "port"
 
 
+def grid_figures(torch, eng, centers, res, nocc, cpu: bool, n_points=1_000_000):
+    """Orbital densities of the converged (H2O)_64 RHF on a grid (the
+    evaluation-script workload): 320 occupied orbitals x 448 AOs at 1e6 random
+    points in the cluster's box.  Device time per chunk (AO kernel, FP64 MO
+    GEMM, density kernel) with CUDA events, the host-to-host rate through
+    OrbitalGrid.evaluate, and the oracle on a 2,000-point sample."""
+    import ctypes
+
+    import numpy as np
+
+    from dft_b200 import _lib, grid
+
+    C = res.C_a.detach().cpu().numpy()
+    n = eng.n_ao
+    ck = {"centers": np.asarray(centers), "N_a": np.float64(nocc), "N_b": np.float64(nocc), "C_a": C, "C_b": C,
+          "total_ao": np.int64(n), "shells": eng.shells, "A": np.eye(n)}
+    og = grid.OrbitalGrid(ck)
+    c = np.asarray(centers)
+    rng = np.random.default_rng(0)
+    host_pts = rng.uniform(c.min(0) - 2.0, c.max(0) + 2.0, size=(n_points, 3)).astype(np.float32)
+    pts = torch.as_tensor(host_pts, device=eng.device)
+    tot = torch.empty((og.n_mo, n_points), dtype=torch.float32, device=eng.device)
+    ph = torch.empty((og.n_a, n_points), dtype=torch.float32, device=eng.device)
+    for _ in range(3):
+        og.chunk(pts, tot, ph)
+    ms = []
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        og.chunk(pts, tot, ph)
+        e1.record()
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    ao = torch.empty((n, n_points), dtype=torch.float64, device=eng.device)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    ev[0].record()
+    _lib.call("dftk_grid_ao", ctypes.byref(eng.c_shells), n_points, _lib.ptr(pts), _lib.ptr(ao), n_points,
+              _lib.stream_handle())
+    ev[1].record()
+    psi = og.Ca @ ao
+    ev[2].record()
+    _lib.call("dftk_grid_density", og.n_mo, og.n_a, og.n_b, n_points, _lib.ptr(psi), _lib.ptr(psi), n_points,
+              _lib.ptr(tot), _lib.ptr(ph), n_points, _lib.stream_handle())
+    ev[3].record()
+    ev[3].synchronize()
+    part = [ev[i].elapsed_time(ev[i + 1]) for i in range(3)]
+    del ao, psi
+    # host to host, steady state: outputs and pinned staging allocated by a
+    # first call, the second call timed
+    h_tot = np.zeros((og.n_mo, n_points), dtype=np.float32)
+    h_ph = np.zeros((og.n_mo, n_points), dtype=np.float32)
+    og.evaluate(host_pts, chunk_size=n_points, total=h_tot, phase=h_ph)
+    t0 = time.perf_counter()
+    og.evaluate(host_pts, chunk_size=n_points, total=h_tot, phase=h_ph)
+    e2e_s = time.perf_counter() - t0
+    chunk_ms = float(np.median(ms))
+    out = {"workload": "(H2O)_64 RHF/STO-3G, 320 occupied orbitals x 448 AOs, 1e6 random points in the box",
+           "points_per_s": n_points / (chunk_ms / 1e3), "chunk_ms": chunk_ms,
+           "ao_kernel_ms": part[0], "mo_gemm_ms": part[1], "density_kernel_ms": part[2],
+           "mo_gemm_tflops": 2.0 * og.n_mo * n * n_points / (part[1] / 1e3) / 1e12,
+           "density_kernel_gbs": (og.n_mo * n_points * 8 + 2 * og.n_mo * n_points * 4) / (part[2] / 1e3) / 1e9,
+           "e2e_points_per_s": n_points / e2e_s,
+           "e2e_note": "host FP32 points in, host FP32 total and phase arrays out (2.56 GB per 1e6 points), "
+                       "outputs and pinned staging reused (steady state of a multi-chunk run)"}
+    if cpu:
+        from oracle import oracle
+
+        sample = host_pts[:2000]
+        t0 = time.perf_counter()
+        oracle.grid_densities(ck, sample)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": len(sample) / dt, "unit": "points/s", "cores": 1, "kind": "port",
+                               "sample": "oracle.grid_densities (NumPy) on 2,000 of the points"}
+    return out
+
+
 def c10h22_figures(torch, cpu: bool):
     """C10H22 / STO-3G (72 basis functions): per-class ERI throughput of one
     full FP64 build at the converged density (CUDA events per class kernel),
@@ -718,6 +794,7 @@ def run_dftk_arm(args, rank, world, local_rank):
         if not args.no_extras:
             line["c10h22"] = c10h22_figures(torch, cpu=world == 1 and not args.no_cpu_baseline)
             line["grad"] = gradient_figures(torch, eng, atoms, centers, r64)
+            line["grid"] = grid_figures(torch, eng, centers, r64, nocc, cpu=world == 1 and not args.no_cpu_baseline)
             line["errors"] = error_figures(torch, eng)
             line.update(batch_figures(torch))
         print(json.dumps(line), flush=True)

@@ -27,7 +27,7 @@ SYMBOLS = (
     "dftk_pair_data", "dftk_schwarz", "dftk_one_electron", "dftk_eri_blocks",
     "dftk_jk_workspace_bytes", "dftk_jk_workspace_bytes_queue", "dftk_jk", "dftk_nuclear_kernel", "dftk_eri_kernel",
     "dftk_fma_burn", "dftk_jk_timing", "dftk_jk_timing_read", "dftk_jk_noalloc", "dftk_grad", "dftk_workspace_bytes",
-    "dftk_set_launch", "dftk_get_launch",
+    "dftk_set_launch", "dftk_get_launch", "dftk_grid_ao", "dftk_grid_density",
 )
 
 
@@ -136,7 +136,12 @@ def load() -> ctypes.CDLL:
                        vp, vp, d, d, vp, vp, sz, vp], i),
         "dftk_jk_timing": ([i], i),
         "dftk_jk_timing_read": ([vp, i], i),
+        "dftk_grid_ao": ([ctypes.POINTER(Shells), ll, vp, vp, ll, vp], i),
+        "dftk_grid_density": ([i, i, i, ll, vp, vp, ll, vp, vp, ll, vp], i),
     }
+    missing = set(SYMBOLS) - set(sig)
+    if missing:  # every entry point gets explicit argument types (64-bit sizes)
+        raise DftkError("load", -1, f"no argument types for {sorted(missing)}")
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
         fn.argtypes = args
@@ -158,6 +163,14 @@ def stream_handle(stream=None) -> ctypes.c_void_p:
 
     s = stream if stream is not None else torch.cuda.current_stream()
     return ctypes.c_void_p(s.cuda_stream)
+
+
+def row_ptr(t) -> ctypes.c_void_p:
+    """Device pointer of a CUDA matrix whose rows are contiguous (a column
+    slice of a wider matrix; the leading dimension is t.stride(0))."""
+    if not t.is_cuda or t.dim() != 2 or t.stride(1) != 1:
+        raise DftkError("ptr", ERR_ARG, "expected a CUDA matrix with contiguous rows")
+    return ctypes.c_void_p(t.data_ptr())
 
 
 def ptr(t) -> ctypes.c_void_p:

@@ -16,6 +16,7 @@
 #include "jk.cuh"
 #include "grad.cuh"
 #include "onee.cuh"
+#include "grid.cuh"
 
 namespace {
 
@@ -513,6 +514,47 @@ int dftk_one_electron(const dftk_shells_t *shells, int n_atoms, const double *at
     if (npair == 0) return DFTK_OK;
     k_one_electron<<<blocks_for(npair, 64), 64, 0, (cudaStream_t)stream>>>(*shells, n_atoms, atom_xyz, atom_z, S, T, V);
     DFTK_LAUNCHED("k_one_electron");
+    return DFTK_OK;
+}
+
+int dftk_grid_ao(const dftk_shells_t *shells, long long n_points, const float *points, double *ao, long long ld,
+                 dftk_stream_t stream)
+{
+    if (!shells || n_points < 0 || ld < n_points || (n_points > 0 && (!points || !ao)) || shells->n_shells < 0 ||
+        (shells->n_shells > 0 && (!shells->xyz || !shells->l || !shells->nprim || !shells->prim_off || !shells->ao ||
+                                  !shells->prim_exp || !shells->prim_cn)))
+        return fail(DFTK_ERR_ARG, "dftk_grid_ao: bad arguments");
+    if (shells->n_mol > 0) return fail(DFTK_ERR_UNSUPPORTED, "dftk_grid_ao: one molecule at a time");
+    DFTK_INIT();
+    if (n_points == 0 || shells->n_shells == 0) return DFTK_OK;
+    if ((n_points + 127) / 128 > 0x7fffffffLL) return fail(DFTK_ERR_SIZE, "dftk_grid_ao: too many points in one call");
+    // momenta beyond p have no AO code here: refuse them before launch
+    std::vector<int> l(shells->n_shells);
+    DFTK_CUDA(cudaMemcpyAsync(l.data(), shells->l, sizeof(int) * l.size(), cudaMemcpyDeviceToHost,
+                              (cudaStream_t)stream));
+    DFTK_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    for (int v : l)
+        if (v < 0 || v > 1) return fail(DFTK_ERR_UNSUPPORTED, "dftk_grid_ao: shells beyond p");
+    k_grid_ao<<<blocks_for(n_points, 128), 128, 0, (cudaStream_t)stream>>>(*shells, n_points, points, ao, ld);
+    DFTK_LAUNCHED("k_grid_ao");
+    return DFTK_OK;
+}
+
+int dftk_grid_density(int n_mo, int n_a, int n_b, long long n_points, const double *psi_a, const double *psi_b,
+                      long long ld_psi, float *total, float *phase, long long ld_out, dftk_stream_t stream)
+{
+    if (n_mo < 0 || n_mo > 65535 || n_a < 0 || n_b < 0 || n_a > n_mo || n_b > n_mo || n_points < 0 ||
+        ld_psi < n_points || ld_out < n_points ||
+        (n_points > 0 && n_mo > 0 && (!psi_a || !psi_b || !total || (n_a > 0 && !phase))))
+        return fail(DFTK_ERR_ARG, "dftk_grid_density: bad arguments");
+    DFTK_INIT();
+    if (n_points == 0 || n_mo == 0) return DFTK_OK;
+    const long long bx = (n_points + 255) / 256;
+    if (bx > 0x7fffffffLL) return fail(DFTK_ERR_SIZE, "dftk_grid_density: too many points in one call");
+    k_grid_density<<<dim3((unsigned)bx, (unsigned)n_mo), 256, 0, (cudaStream_t)stream>>>(n_a, n_b, n_points, psi_a,
+                                                                                         psi_b, ld_psi, total, phase,
+                                                                                         ld_out);
+    DFTK_LAUNCHED("k_grid_density");
     return DFTK_OK;
 }
 

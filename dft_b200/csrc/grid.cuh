@@ -1,0 +1,61 @@
+// Orbitals on a grid of points (the reference's evaluation script,
+// shelled_eval.py:88-131): AO values, then (after the MO GEMM the host does
+// with the library GEMM) per-orbital densities.
+//
+// k_grid_ao: one thread per point, all shells of the molecule in order (the
+// shell table is read as warp-uniform broadcasts).  Like the reference, the
+// point comes in FP32 and everything after the centre difference is FP64:
+//   ao[a][g] = x^i y^j z^k * sum_p cn_p exp(-alpha_p r^2)
+// with cn_p = contraction coefficient x primitive normalisation (the same for
+// every component of an s or p shell).  Rows are AOs, columns points, so the
+// stores of a warp are contiguous.
+//
+// k_grid_density: psi_a, psi_b are the MO values (rows = orbitals); for
+// orbital k < n_mo and point g
+//   total[k][g] = [k < n_a] psi_a^2 + [k < n_b] psi_b^2   (FP64, stored FP32)
+//   phase[k][g] = psi_a                                     (k < n_a only)
+#pragma once
+
+#include "common.cuh"
+
+__global__ void __launch_bounds__(128) k_grid_ao(const dftk_shells_t sh, long long n, const float *pts, double *ao,
+                                                 long long ld)
+{
+    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const double x = (double)pts[3 * g], y = (double)pts[3 * g + 1], z = (double)pts[3 * g + 2];
+    for (int s = 0; s < sh.n_shells; ++s) {
+        const double dx = x - __ldg(sh.xyz + 3 * s), dy = y - __ldg(sh.xyz + 3 * s + 1),
+                     dz = z - __ldg(sh.xyz + 3 * s + 2);
+        // the reference's sum of squares, without contraction into FMAs
+        const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+        const int p0 = __ldg(sh.prim_off + s), np = __ldg(sh.nprim + s);
+        double rad = 0.0;
+        for (int p = 0; p < np; ++p) rad += __ldg(sh.prim_cn + p0 + p) * exp(-__ldg(sh.prim_exp + p0 + p) * r2);
+        const int l = __ldg(sh.l + s);
+        double *row = ao + (long long)__ldg(sh.ao + s) * ld + g;
+        if (l == 0) {
+            row[0] = rad;
+        } else if (l == 1) {
+            row[0] = dx * rad;
+            row[ld] = dy * rad;
+            row[2 * ld] = dz * rad;
+        }
+        // other momenta are rejected by the host before launch
+    }
+}
+
+__global__ void __launch_bounds__(256) k_grid_density(int n_a, int n_b, long long n, const double *psi_a,
+                                                      const double *psi_b, long long ld_psi, float *total,
+                                                      float *phase, long long ld_out)
+{
+    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.y;
+    if (g >= n) return;
+    // closed shells pass the same matrix twice: read it once
+    const double pa = psi_a[(long long)k * ld_psi + g];
+    const double pb = psi_b == psi_a ? pa : psi_b[(long long)k * ld_psi + g];
+    const double da = k < n_a ? pa * pa : 0.0, db = k < n_b ? pb * pb : 0.0;
+    total[(long long)k * ld_out + g] = (float)(da + db);
+    if (k < n_a) phase[(long long)k * ld_out + g] = (float)pa;
+}

@@ -158,6 +158,26 @@ int dftk_one_electron(const dftk_shells_t *shells, int n_atoms, const double *at
                       const double *atom_z, double *S, double *T, double *V,
                       dftk_stream_t stream);
 
+/* AO values at points (the AO loop of the reference's orbital evaluation,
+ * shelled_eval.py:88-107): ao[a * ld + g] = x^i y^j z^k sum_p cn_p
+ * exp(-alpha_p r^2) for every AO a of the molecule and point g < n_points,
+ * with (x, y, z) = point g - the shell centre.  Points are FP32 xyz triples
+ * (the reference's grid dtype), the arithmetic and ao are FP64.  One molecule
+ * (shells->n_mol == 0) with s and p shells (else DFTK_ERR_UNSUPPORTED); ao
+ * holds shells->n_ao rows of ld >= n_points doubles.  Reads shells->l back to
+ * the host to check the momenta (synchronises the stream). */
+int dftk_grid_ao(const dftk_shells_t *shells, long long n_points, const float *points, double *ao,
+                 long long ld, dftk_stream_t stream);
+
+/* Per-orbital densities on points (shelled_eval.py:110-131), from MO values
+ * psi_a, psi_b (n_mo rows of ld_psi >= n_points doubles; the MO step
+ * psi = C^T ao is a plain GEMM left to the caller's BLAS): for k < n_mo
+ *   total[k * ld_out + g] = [k < n_a] psi_a^2 + [k < n_b] psi_b^2  (FP64, stored FP32)
+ *   phase[k * ld_out + g] = psi_a (FP32), rows k < n_a only (others untouched). */
+int dftk_grid_density(int n_mo, int n_a, int n_b, long long n_points, const double *psi_a,
+                      const double *psi_b, long long ld_psi, float *total, float *phase,
+                      long long ld_out, dftk_stream_t stream);
+
 /* Contracted ERI blocks of explicit quartets (debug / parity path of calc_eri,
  * shelled.py:640-691).  desc[4 * t] = {quartet class, bra row, ket row, flags}
  * with flags bit0 = bra pair stored as (b, a), bit1 = ket pair stored as

@@ -15,8 +15,12 @@ It restates the reference (yegor-gondhal/DFT, ``shelled.py``) on the CPU:
 * the arithmetic in plain C (``oracle.c``): Boys, Hermite E/R, primitive and
   contracted ERIs, one-electron S/T/V, and J/K digestion.
 
-Pinned by ``tests/test_oracle_golden.py`` against fixtures generated by running
-the reference itself (``tests/golden/make_golden.py``).
+* orbital densities on a grid of points (the reference's evaluation script,
+  shelled_eval.py:88-131) in NumPy: ``grid_ao``, ``grid_densities``.
+
+Pinned by ``tests/test_oracle_golden.py`` and ``tests/test_oracle_grid.py``
+against fixtures generated by running the reference itself
+(``tests/golden/make_golden.py``).
 """
 from __future__ import annotations
 
@@ -412,3 +416,47 @@ def scf_energy_gradient(basis_path: str, atoms: Sequence[str], centers: np.ndarr
     Fa, Fb = H + r["J"] - r["K_a"], H + r["J"] - r["K_b"]
     W = Pa @ Fa @ Pa + Pb @ Fb @ Pb
     return r["energy"], gradient(sh, atoms, centers, Pa + Pb, Pa, Pb, W)
+
+
+# ------------------------------------------------------------------ grid
+def grid_ao(shells: List[Dict], points: np.ndarray) -> np.ndarray:
+    """AO values (total_ao, n_points) at FP32 points (shelled_eval.py:91-107):
+    per shell, Cartesian component (i, j, k), primitive p and contraction c,
+    coefficient[c, p] * normalization[comp, p] * x^i y^j z^k exp(-alpha_p r^2)
+    summed over p, with (x, y, z) the FP64 difference of the FP32 point and
+    the shell centre."""
+    pts = np.asarray(points, dtype=np.float32)
+    n_ao = int(shells[-1]["ao_stop"]) if shells else 0
+    out = np.empty((n_ao, pts.shape[0]))
+    for sh in shells:
+        d = pts.astype(np.float64) - np.asarray(sh["atom_pos"], dtype=np.float64)
+        r2 = d[:, 0] ** 2 + d[:, 1] ** 2 + d[:, 2] ** 2
+        nexp = int(sh["n_exponents"])
+        comps = np.asarray(sh["components"])
+        norm = np.asarray(sh["normalization"]).reshape(len(comps), nexp)
+        coef = np.asarray(sh["coefficients"]).reshape(-1, nexp)
+        gauss = np.exp(-np.asarray(sh["exponents"], dtype=np.float64)[:, None] * r2[None, :])  # (nexp, n)
+        row = int(sh["ao_start"])
+        for c in range(coef.shape[0]):
+            for a, (i, j, k) in enumerate(comps):
+                poly = d[:, 0] ** i * d[:, 1] ** j * d[:, 2] ** k
+                out[row] = ((coef[c] * norm[a])[:, None] * gauss).sum(axis=0) * poly
+                row += 1
+    return out
+
+
+def grid_densities(ckpt: Dict, points: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
+    """(total, phase), each (max(N_a, N_b), n_points) FP32, from an evaluation
+    checkpoint (shelled_eval.py:108-131): psi_s = C_s[:, :n]^T (rounded to
+    FP32, applied in FP64) A ao; total = [k < N_a] psi_a^2 + [k < N_b] psi_b^2;
+    phase = psi_a in rows k < N_a, zero elsewhere."""
+    n_a, n_b = int(ckpt["N_a"]), int(ckpt["N_b"])
+    n = max(n_a, n_b)
+    ao = np.asarray(ckpt["A"], dtype=np.float64) @ grid_ao(ckpt["shells"], points)
+    psi = [np.asarray(ckpt[k]).astype(np.float32)[:, :n].T.astype(np.float64) @ ao for k in ("C_a", "C_b")]
+    occ_a = (np.arange(n) < n_a)[:, None]
+    occ_b = (np.arange(n) < n_b)[:, None]
+    total = (np.where(occ_a, psi[0] ** 2, 0.0) + np.where(occ_b, psi[1] ** 2, 0.0)).astype(np.float32)
+    phase = np.zeros((n, ao.shape[1]), dtype=np.float32)
+    phase[:n_a] = psi[0][:n_a]
+    return total, phase

@@ -23,6 +23,7 @@ Usage::
     python tests/golden/make_golden.py h2o            # seconds
     python tests/golden/make_golden.py c10h22         # ~10-15 min
     python tests/golden/make_golden.py h2o64          # ~2 min (pair setup + sampled quartets)
+    python tests/golden/make_golden.py grid           # seconds (H2O SCF + evaluation script)
 """
 from __future__ import annotations
 
@@ -257,13 +258,58 @@ def case_h2o64(out_dir, n_subsets=12, subset_pairs=24, seed=1234):
     print("h2o64 sampled quartets", len(all_quads), "values", res["sample_values"].shape)
 
 
+def patched_eval(spacing=0.15, chunk=500):
+    """The reference's evaluation script with the H2O checkpoint the reference
+    SCF just wrote, a coarser grid whose x range is widened by 1 bohr each way
+    (the script's own x bounds assume a molecule that is not flat in x) and a
+    small chunk size, so several chunks, the last one partial, run."""
+    with open(os.path.join(REFERENCE, "shelled_eval.py")) as fh:
+        text = fh.read()
+    text = _replace_once(text, '"eval_checkpoints/cerium_3_fluoride_eval_checkpoint.npz"',
+                         '"eval_checkpoints/gadolinium_3_fluoride_eval_checkpoint.npz"')
+    text = _replace_once(text, "grid_spacing = 0.008", f"grid_spacing = {spacing!r}")
+    text = _replace_once(text, "minx = float(xp.min(centers[:, 0]))", "minx = float(xp.min(centers[:, 0]) - 1.0)")
+    text = _replace_once(text, "maxx = float(xp.max(centers[:, 0]) - 1.0)", "maxx = float(xp.max(centers[:, 0]) + 1.0)")
+    text = _replace_once(text, "chunk_size = int(1e6)", f"chunk_size = int({chunk})")
+    return text
+
+
+def case_grid(out_dir):
+    """Orbital densities on a grid for H2O: the reference SCF (its own
+    thresholds) writes its evaluation checkpoint, then the reference's
+    evaluation script runs on it.  Writes the checkpoint file as it is and the
+    grid, total and phase densities."""
+    import shutil
+
+    atoms, centers = geometry.water()
+    ns, work = run_reference(atoms, centers)
+    ckpt = os.path.join(work, "eval_checkpoints", "gadolinium_3_fluoride_eval_checkpoint.npz")
+    os.makedirs(os.path.join(work, "preprocess"))
+    cwd = os.getcwd()
+    os.chdir(work)
+    try:
+        with contextlib.redirect_stdout(io.StringIO()):
+            exec(compile(patched_eval(), os.path.join(REFERENCE, "shelled_eval.py") + ":patched", "exec"),
+                 {"__name__": "shelled_eval_reference_run"})
+    finally:
+        os.chdir(cwd)
+    pre = os.path.join(work, "preprocess")
+    res = {"grid": np.load(os.path.join(pre, "grid.npy")),
+           "total_density": np.load(os.path.join(pre, "total_density.npy")),
+           "phase_density": np.load(os.path.join(pre, "phase_density.npy")),
+           "energy": float(ns["E_total_new"])}
+    np.savez_compressed(os.path.join(out_dir, "grid_h2o.npz"), **res)
+    shutil.copyfile(ckpt, os.path.join(out_dir, "h2o_eval_checkpoint.npz"))
+    print("grid", res["grid"].shape, "total", res["total_density"].shape, "energy", res["energy"])
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["h2o", "c10h22", "h2o64"])
+    ap.add_argument("case", choices=["h2o", "c10h22", "h2o64", "grid"])
     ap.add_argument("--out", default=HERE)
     args = ap.parse_args()
     install_fake_cupy()
-    {"h2o": case_h2o, "c10h22": case_c10h22, "h2o64": case_h2o64}[args.case](args.out)
+    {"h2o": case_h2o, "c10h22": case_c10h22, "h2o64": case_h2o64, "grid": case_grid}[args.case](args.out)
 
 
 if __name__ == "__main__":

@@ -135,6 +135,14 @@ def test_header_symbols_exported():
     assert lib.dftk_version() == 100
 
 
+def test_every_symbol_has_argument_types():
+    """ctypes passes undeclared integer arguments as 32-bit ints; every entry
+    point (64-bit sizes among them) is declared."""
+    lib = _lib.load()
+    for name in _lib.SYMBOLS:
+        assert getattr(lib, name).argtypes is not None, name
+
+
 def test_cabi_argument_errors_without_gpu():
     """Argument validation happens before any CUDA call and reports through
     the status code and dftk_last_error()."""
