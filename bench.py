@@ -808,7 +808,7 @@ def run_profile(args):
     """A few builds of the benchmark workload for ncu captures: two full FP64
     builds, then one mixed build of a scaled-down density (kernel launch order
     per build: k_dsh, k_select x6, k_jk_list<0..5,double>, [k_jk_list<0..5,float>],
-    k_symmetrize), then one gradient."""
+    k_symmetrize), then one gradient (and with --profile-grid two grid chunks)."""
     import torch
 
     atoms, centers, shells, eng, S, H, enn, nocc = setup_workload(torch)
@@ -825,6 +825,25 @@ def run_profile(args):
     Dt = (2 * D).contiguous()
     eng.gradient(atoms, centers, Dt, D, D, Dt)
     torch.cuda.synchronize()
+    if args.profile_grid:
+        # two 200,000-point grid chunks with the core-guess orbitals: launch
+        # order k_grid_ao, (DGEMM), k_grid_density, twice
+        from dft_b200 import grid
+
+        n = eng.n_ao
+        Ch = C.detach().cpu().numpy()
+        ck = {"centers": np.asarray(centers), "N_a": np.float64(nocc), "N_b": np.float64(nocc), "C_a": Ch,
+              "C_b": Ch, "total_ao": np.int64(n), "shells": eng.shells, "A": np.eye(n)}
+        og = grid.OrbitalGrid(ck)
+        c = np.asarray(centers)
+        m = 200_000
+        pts = torch.as_tensor(np.random.default_rng(0).uniform(c.min(0) - 2, c.max(0) + 2, size=(m, 3))
+                              .astype(np.float32), device=eng.device)
+        tot = torch.empty((og.n_mo, m), dtype=torch.float32, device=eng.device)
+        ph = torch.empty((og.n_a, m), dtype=torch.float32, device=eng.device)
+        for _ in range(2):
+            og.chunk(pts, tot, ph)
+        torch.cuda.synchronize()
     print("profile workload done")
     return 0
 
@@ -840,6 +859,7 @@ def main():
     ap.add_argument("--shard", action="store_true",
                     help="with N > 1: the ranks build one (H2O)_64 Fock matrix together (strong scaling)")
     ap.add_argument("--profile", action="store_true", help="only run a few builds (for ncu captures)")
+    ap.add_argument("--profile-grid", action="store_true", help="with --profile: also two grid-evaluation chunks")
     args = ap.parse_args()
     if args.profile:
         return run_profile(args)
