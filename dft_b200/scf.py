@@ -13,7 +13,7 @@
   FP32, accumulation in FP64).  Full FP64 rebuilds every ``rebuild_every``
   iterations, and for every iteration once RMS(dD) < ``finish_factor`` x
   dtol, bound the drift of the incremental sum, so convergence is always
-  judged on a full FP64 Fock matrix.
+  tested on a full FP64 Fock matrix.
 
 Dense linear algebra (eigh via cuSOLVER, DIIS solves) runs in torch float64
 on the same device; it is O(N^3) with N <= a few hundred, far below the J/K
