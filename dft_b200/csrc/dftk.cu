@@ -549,7 +549,8 @@ int dftk_grid_density(int n_mo, int n_a, int n_b, long long n_points, const doub
         return fail(DFTK_ERR_ARG, "dftk_grid_density: bad arguments");
     DFTK_INIT();
     if (n_points == 0 || n_mo == 0) return DFTK_OK;
-    const long long bx = (n_points + 255) / 256;
+    const long long per_block = 256LL * GRID_DENSITY_UNROLL;
+    const long long bx = (n_points + per_block - 1) / per_block;
     if (bx > 0x7fffffffLL) return fail(DFTK_ERR_SIZE, "dftk_grid_density: too many points in one call");
     k_grid_density<<<dim3((unsigned)bx, (unsigned)n_mo), 256, 0, (cudaStream_t)stream>>>(n_a, n_b, n_points, psi_a,
                                                                                          psi_b, ld_psi, total, phase,

@@ -45,17 +45,32 @@ __global__ void __launch_bounds__(128) k_grid_ao(const dftk_shells_t sh, long lo
     }
 }
 
+// GRID_DENSITY_UNROLL points per thread, blockDim apart (coalesced), so each
+// thread has that many independent loads in flight
+#define GRID_DENSITY_UNROLL 4
+
 __global__ void __launch_bounds__(256) k_grid_density(int n_a, int n_b, long long n, const double *psi_a,
                                                       const double *psi_b, long long ld_psi, float *total,
                                                       float *phase, long long ld_out)
 {
-    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int k = blockIdx.y;
-    if (g >= n) return;
-    // closed shells pass the same matrix twice: read it once
-    const double pa = psi_a[(long long)k * ld_psi + g];
-    const double pb = psi_b == psi_a ? pa : psi_b[(long long)k * ld_psi + g];
-    const double da = k < n_a ? pa * pa : 0.0, db = k < n_b ? pb * pb : 0.0;
-    total[(long long)k * ld_out + g] = (float)(da + db);
-    if (k < n_a) phase[(long long)k * ld_out + g] = (float)pa;
+    const long long g0 = (long long)blockIdx.x * blockDim.x * GRID_DENSITY_UNROLL + threadIdx.x;
+    const double *ra = psi_a + (long long)k * ld_psi;
+    const double *rb = psi_b + (long long)k * ld_psi;
+    const bool same = psi_b == psi_a;  // closed shells pass one matrix twice: read it once
+    double pa[GRID_DENSITY_UNROLL], pb[GRID_DENSITY_UNROLL];
+#pragma unroll
+    for (int j = 0; j < GRID_DENSITY_UNROLL; ++j) {
+        const long long g = g0 + (long long)j * blockDim.x;
+        pa[j] = g < n ? ra[g] : 0.0;
+        pb[j] = g < n ? (same ? pa[j] : rb[g]) : 0.0;
+    }
+#pragma unroll
+    for (int j = 0; j < GRID_DENSITY_UNROLL; ++j) {
+        const long long g = g0 + (long long)j * blockDim.x;
+        if (g >= n) break;
+        const double da = k < n_a ? pa[j] * pa[j] : 0.0, db = k < n_b ? pb[j] * pb[j] : 0.0;
+        total[(long long)k * ld_out + g] = (float)(da + db);
+        if (k < n_a) phase[(long long)k * ld_out + g] = (float)pa[j];
+    }
 }
