@@ -66,3 +66,20 @@ def test_grid_device_chunk_and_empty():
     ph = torch.zeros((5, 1), dtype=torch.float32, device="cuda")
     og.chunk(pts, tot, ph)
     assert (tot >= 0).all() and torch.isfinite(ph).all()
+
+
+def test_grid_doublet_without_beta_electrons(oracle_mod):
+    """One alpha and no beta electron (an H atom's doublet): total = psi_a^2
+    in row 0, phase row 0 only."""
+    from dft_b200 import basis, grid
+
+    atoms, centers = ["1"], np.zeros((1, 3))
+    shells = basis.build_shells(basis.load_basis(), atoms, centers)
+    ck = {"centers": centers, "N_a": np.float64(1), "N_b": np.float64(0), "C_a": np.ones((1, 1)),
+          "C_b": np.ones((1, 1)), "total_ao": np.int64(1), "shells": shells, "A": np.eye(1)}
+    pts = np.random.default_rng(5).uniform(-3, 3, size=(999, 3)).astype(np.float32)
+    total, phase = grid.OrbitalGrid(ck).evaluate(pts, chunk_size=256)
+    t_ref, p_ref = oracle_mod.grid_densities(ck, pts)
+    _close(total, t_ref)
+    _close(phase, p_ref)
+    np.testing.assert_allclose(total[0], phase[0].astype(np.float64) ** 2, rtol=1e-6)
