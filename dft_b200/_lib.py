@@ -27,7 +27,7 @@ SYMBOLS = (
     "dftk_pair_data", "dftk_schwarz", "dftk_one_electron", "dftk_eri_blocks",
     "dftk_jk_workspace_bytes", "dftk_jk_workspace_bytes_queue", "dftk_jk", "dftk_nuclear_kernel", "dftk_eri_kernel",
     "dftk_fma_burn", "dftk_jk_timing", "dftk_jk_timing_read", "dftk_jk_noalloc", "dftk_grad", "dftk_workspace_bytes",
-    "dftk_set_launch", "dftk_get_launch", "dftk_grid_ao", "dftk_grid_density",
+    "dftk_set_launch", "dftk_get_launch", "dftk_grid_ao", "dftk_grid_density", "dftk_prepare_bytes", "dftk_prepare",
 )
 
 
@@ -138,6 +138,8 @@ def load() -> ctypes.CDLL:
         "dftk_jk_timing_read": ([vp, i], i),
         "dftk_grid_ao": ([ctypes.POINTER(Shells), ll, vp, vp, ll, vp], i),
         "dftk_grid_density": ([i, i, i, ll, vp, vp, ll, vp, vp, ll, vp], i),
+        "dftk_prepare_bytes": ([ctypes.POINTER(Shells), ctypes.POINTER(ctypes.c_size_t)], i),
+        "dftk_prepare": ([ctypes.POINTER(Shells), d, d, vp, sz, ctypes.POINTER(Pairs), ctypes.POINTER(Queue), vp], i),
     }
     missing = set(SYMBOLS) - set(sig)
     if missing:  # every entry point gets explicit argument types (64-bit sizes)

@@ -2,6 +2,7 @@
 //
 // One translation unit: the device tables (g_boys64/g_boys32) and all kernels
 // live here, so the library needs no relocatable device code.
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstdio>
@@ -501,6 +502,173 @@ int dftk_schwarz(const dftk_shells_t *shells, int pair_class, dftk_pairs_t *pair
     else if (pair_class == 1) k_schwarz<1><<<blocks_for(n, 64), 64, 0, s>>>(*pairs, nf);
     else k_schwarz<2><<<blocks_for(n, 64), 64, 0, s>>>(*pairs, nf);
     DFTK_LAUNCHED("k_schwarz");
+    return DFTK_OK;
+}
+
+}  // extern "C" (the setup helpers below are C++)
+
+namespace {
+
+// One molecule's setup plan: the pair lists of each pair class in the
+// reference's pair order (i, j <= i; stored with l_a >= l_b) and the byte
+// offsets of every array in the caller's storage.
+struct PreparePlan {
+    int kmax = 1;
+    std::vector<int> ab[DFTK_N_PCLASS];
+    size_t off_ab[DFTK_N_PCLASS], off_np[DFTK_N_PCLASS], off_r64[DFTK_N_PCLASS], off_r32[DFTK_N_PCLASS],
+        off_q[DFTK_N_PCLASS], off_qp[DFTK_N_PCLASS], off_row[DFTK_N_QCLASS];
+    size_t bytes = 0;
+};
+
+constexpr int kQX[DFTK_N_QCLASS] = {0, 1, 1, 2, 2, 2}, kQY[DFTK_N_QCLASS] = {0, 0, 1, 0, 1, 2};
+
+size_t carve(size_t &at, size_t n)
+{
+    const size_t o = at;
+    at += (n + 255) / 256 * 256;
+    return o;
+}
+
+int prepare_plan(const dftk_shells_t *shells, PreparePlan &pl)
+{
+    const int ns = shells->n_shells;
+    std::vector<int> l(ns), np(ns);
+    if (ns > 0) {
+        DFTK_CUDA(cudaMemcpy(l.data(), shells->l, sizeof(int) * ns, cudaMemcpyDeviceToHost));
+        DFTK_CUDA(cudaMemcpy(np.data(), shells->nprim, sizeof(int) * ns, cudaMemcpyDeviceToHost));
+    }
+    int pmax = 1;
+    for (int i = 0; i < ns; ++i) {
+        if (l[i] < 0 || l[i] > 1) return fail(DFTK_ERR_UNSUPPORTED, "dftk_prepare: shells beyond p");
+        if (np[i] < 1) return fail(DFTK_ERR_ARG, "dftk_prepare: a shell without primitives");
+        pmax = std::max(pmax, np[i]);
+    }
+    pl.kmax = pmax * pmax;
+    if (pl.kmax > DFTK_MAX_KPAIR) return fail(DFTK_ERR_SIZE, "dftk_prepare: more than 64 primitive pairs per pair");
+    for (int i = 0; i < ns; ++i)
+        for (int j = 0; j <= i; ++j) {
+            const bool swap = l[i] < l[j];
+            const int a = swap ? j : i, b = swap ? i : j;
+            auto &v = pl.ab[l[a] + l[b]];
+            v.push_back(a);
+            v.push_back(b);
+        }
+    size_t at = 0;
+    for (int pc = 0; pc < DFTK_N_PCLASS; ++pc) {
+        const size_t n = pl.ab[pc].size() / 2, rec = (size_t)pair_fields(pc) * pl.kmax * n;
+        pl.off_ab[pc] = carve(at, sizeof(int) * 2 * std::max<size_t>(n, 1));
+        pl.off_np[pc] = carve(at, sizeof(int) * std::max<size_t>(n, 1));
+        pl.off_r64[pc] = carve(at, sizeof(double) * std::max<size_t>(rec, 1));
+        pl.off_r32[pc] = carve(at, sizeof(float) * std::max<size_t>(rec, 1));
+        pl.off_q[pc] = carve(at, sizeof(double) * std::max<size_t>(n, 1));
+        pl.off_qp[pc] = carve(at, sizeof(float) * std::max<size_t>((size_t)pl.kmax * n, 1));
+    }
+    for (int c = 0; c < DFTK_N_QCLASS; ++c) pl.off_row[c] = carve(at, sizeof(long long) * (pl.ab[kQX[c]].size() / 2 + 1));
+    pl.bytes = at;
+    return DFTK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dftk_prepare_bytes(const dftk_shells_t *shells, size_t *bytes)
+{
+    if (!shells || !bytes || shells->n_shells < 0 || (shells->n_shells > 0 && (!shells->l || !shells->nprim)))
+        return fail(DFTK_ERR_ARG, "dftk_prepare_bytes: bad arguments");
+    if (shells->n_mol > 0) return fail(DFTK_ERR_UNSUPPORTED, "dftk_prepare_bytes: one molecule at a time");
+    DFTK_INIT();
+    PreparePlan pl;
+    const int st = prepare_plan(shells, pl);
+    if (st != DFTK_OK) return st;
+    *bytes = pl.bytes;
+    return DFTK_OK;
+}
+
+int dftk_prepare(const dftk_shells_t *shells, double tau_schwarz, double tau_prim, void *storage,
+                 size_t storage_bytes, dftk_pairs_t pairs[DFTK_N_PCLASS], dftk_queue_t *queue, dftk_stream_t stream)
+{
+    if (!shells || !pairs || !queue || !(tau_schwarz >= 0.0) || !(tau_prim >= 0.0) || shells->n_shells < 0 ||
+        (shells->n_shells > 0 && (!shells->l || !shells->nprim)))
+        return fail(DFTK_ERR_ARG, "dftk_prepare: bad arguments");
+    if (shells->n_mol > 0) return fail(DFTK_ERR_UNSUPPORTED, "dftk_prepare: one molecule at a time");
+    DFTK_INIT();
+    cudaStream_t s = (cudaStream_t)stream;
+    DFTK_CUDA(cudaStreamSynchronize(s));  // the shell arrays may still be in flight on the caller's stream
+    PreparePlan pl;
+    int st = prepare_plan(shells, pl);
+    if (st != DFTK_OK) return st;
+    if (!storage || storage_bytes < pl.bytes) return fail(DFTK_ERR_WORKSPACE, "dftk_prepare: storage too small");
+    char *base = (char *)storage;
+    std::vector<double> qs[DFTK_N_PCLASS];
+    for (int pc = 0; pc < DFTK_N_PCLASS; ++pc) {
+        dftk_pairs_t &P = pairs[pc];
+        std::vector<int> &ab = pl.ab[pc];
+        const int n = (int)(ab.size() / 2);
+        P.n_pairs = n;
+        P.kmax = pl.kmax;
+        P.ab = (const int *)(base + pl.off_ab[pc]);
+        P.nprim = (int *)(base + pl.off_np[pc]);
+        P.rec64 = (double *)(base + pl.off_r64[pc]);
+        P.rec32 = (float *)(base + pl.off_r32[pc]);
+        P.q = (double *)(base + pl.off_q[pc]);
+        P.qp = (float *)(base + pl.off_qp[pc]);
+        if (n == 0) continue;
+        // Schwarz factors in enumeration order, then the pairs sorted by
+        // descending factor (stable) and their records rebuilt in that order
+        for (int pass = 0; pass < 2; ++pass) {
+            DFTK_CUDA(cudaMemcpyAsync(base + pl.off_ab[pc], ab.data(), sizeof(int) * ab.size(), cudaMemcpyHostToDevice, s));
+            if ((st = dftk_pair_data(shells, pc, &P, stream)) != DFTK_OK) return st;
+            if ((st = dftk_schwarz(shells, pc, &P, stream)) != DFTK_OK) return st;
+            qs[pc].assign(n, 0.0);
+            DFTK_CUDA(cudaMemcpyAsync(qs[pc].data(), P.q, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+            DFTK_CUDA(cudaStreamSynchronize(s));
+            if (pass == 1) break;
+            std::vector<int> order(n);
+            for (int i = 0; i < n; ++i) order[i] = i;
+            const std::vector<double> &q = qs[pc];
+            std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return q[x] > q[y]; });
+            std::vector<int> sorted(ab.size());
+            for (int i = 0; i < n; ++i) {
+                sorted[2 * i] = ab[2 * order[i]];
+                sorted[2 * i + 1] = ab[2 * order[i] + 1];
+            }
+            ab.swap(sorted);
+        }
+    }
+    // candidate offsets: bra row r keeps the ket prefix with q_ket >= tau / q_bra[r]
+    // (the ket factors are sorted descending), cut at k <= r when bra and ket
+    // share a pair class so each unique quartet appears once
+    for (int c = 0; c < DFTK_N_QCLASS; ++c) {
+        const std::vector<double> &qx = qs[kQX[c]], &qy = qs[kQY[c]];
+        const size_t nr = pl.ab[kQX[c]].size() / 2, nk = pl.ab[kQY[c]].size() / 2;
+        std::vector<long long> off(nr + 1, 0);
+        for (size_t r = 0; r < nr; ++r) {
+            long long cnt = 0;
+            if (nk > 0 && qx[r] > 0.0) {
+                const double thr = tau_schwarz / qx[r];
+                // first index with qy < thr (qy descending)
+                size_t lo = 0, hi = nk;
+                while (lo < hi) {
+                    const size_t mid = (lo + hi) / 2;
+                    if (qy[mid] >= thr) lo = mid + 1;
+                    else hi = mid;
+                }
+                cnt = (long long)lo;
+            }
+            if (kQX[c] == kQY[c]) cnt = std::min<long long>(cnt, (long long)r + 1);
+            off[r + 1] = off[r] + cnt;
+        }
+        long long *d_off = (long long *)(base + pl.off_row[c]);
+        DFTK_CUDA(cudaMemcpyAsync(d_off, off.data(), sizeof(long long) * off.size(), cudaMemcpyHostToDevice, s));
+        queue->total[c] = off[nr];
+        queue->n_rows[c] = off[nr] > 0 ? (long long)nr : 0;
+        queue->row_off[c] = d_off;
+        queue->ket_base[c] = nullptr;
+    }
+    queue->tau_prim = tau_prim;
+    queue->mol_active = nullptr;
+    DFTK_CUDA(cudaStreamSynchronize(s));  // the host vectors above are sources of the copies
     return DFTK_OK;
 }
 

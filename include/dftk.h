@@ -152,6 +152,23 @@ int dftk_pair_data(const dftk_shells_t *shells, int pair_class, dftk_pairs_t *pa
 int dftk_schwarz(const dftk_shells_t *shells, int pair_class, dftk_pairs_t *pairs,
                  dftk_stream_t stream);
 
+/* One-call setup of a molecule's pairs and queue for dftk_jk / dftk_grad,
+ * everything a host would otherwise do itself: the shell pairs of each pair
+ * class in the reference's pair order (i, j <= i; pair_list, shelled.py:962-964,
+ * stored with l_a >= l_b), their records and Schwarz factors
+ * (dftk_pair_data, dftk_schwarz), the pairs sorted by descending Schwarz
+ * factor (stable) with the records rebuilt in that order, and the candidate
+ * offsets of every quartet class at tau_schwarz (the unique-quartet
+ * enumeration cd <= ab of shelled.py:599-603, Schwarz-screened).  All arrays
+ * live in the caller's device `storage` (dftk_prepare_bytes bytes); pairs[3]
+ * and *queue are filled with pointers into it.  One molecule, s and p shells.
+ * Reads shells->l and shells->nprim back to the host and synchronises
+ * `stream`.  No counterpart in the reference as one call. */
+int dftk_prepare_bytes(const dftk_shells_t *shells, size_t *bytes);
+int dftk_prepare(const dftk_shells_t *shells, double tau_schwarz, double tau_prim, void *storage,
+                 size_t storage_bytes, dftk_pairs_t pairs[DFTK_N_PCLASS], dftk_queue_t *queue,
+                 dftk_stream_t stream);
+
 /* Contracted Cartesian S, T, V (N x N, row-major) over all shell pairs
  * (shelled.py:961-1069); atom_z are the nuclear charges as doubles. */
 int dftk_one_electron(const dftk_shells_t *shells, int n_atoms, const double *atom_xyz,

@@ -154,6 +154,8 @@ def test_cabi_argument_errors_without_gpu():
     assert st == _lib.ERR_ARG
     st = lib.dftk_fma_burn(16, 1, 32, 1, None, None)
     assert st == _lib.ERR_ARG
+    assert lib.dftk_prepare_bytes(None, None) == _lib.ERR_ARG
+    assert lib.dftk_prepare(None, 1e-12, 1e-15, None, 0, None, None, None) == _lib.ERR_ARG
     assert lib.dftk_jk_workspace_bytes(10, 20) >= 3 * 20 * 20 * 8
     with pytest.raises(_lib.DftkError) as ei:
         _lib.call("dftk_boys", 99, 1, None, None, None)
