@@ -21,6 +21,10 @@
  *   dftk_jk_noalloc       <- fill_matrices, for hosts that cannot allocate device memory
  *   dftk_grad             <- (absent in the reference: analytic nuclear gradients)
  *   dftk_workspace_bytes  <- (absent: workspace size of one molecule or a batch)
+ *   dftk_prepare          <- pair_list + pair_cache setup and the quartet enumeration
+ *                            shelled.py:599-603, 962-964, 1000-1059 (one call, Schwarz-sorted)
+ *   dftk_grid_ao          <- AO loop of the evaluation script     shelled_eval.py:88-107
+ *   dftk_grid_density     <- its density lines                    shelled_eval.py:108-131
  */
 #ifndef DFTK_H
 #define DFTK_H

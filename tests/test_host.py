@@ -135,6 +135,18 @@ def test_header_symbols_exported():
     assert lib.dftk_version() == 100
 
 
+def test_header_is_plain_c():
+    """include/dftk.h and the C host example compile as C99 (no C++ in the ABI)."""
+    import shutil
+    import subprocess
+
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc not found")
+    cuda_inc = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "include")
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-fsyntax-only", "-I", os.path.join(REPO, "include"),
+                    "-I", cuda_inc, os.path.join(REPO, "tests", "cabi", "jk_host.c")], check=True)
+
+
 def test_every_symbol_has_argument_types():
     """ctypes passes undeclared integer arguments as 32-bit ints; every entry
     point (64-bit sizes among them) is declared."""
