@@ -66,6 +66,12 @@ class ClockSampler:
                  "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # nvidia-smi takes a moment to print its first sample: start the
+            # timed region once it has (bounded wait), counting only what follows
+            t_end = time.time() + 3.0
+            while not self.lines and time.time() < t_end and self.proc.poll() is None:
+                time.sleep(0.01)
+            self.lines.clear()
         except (FileNotFoundError, OSError):
             self.proc = None
         return self
@@ -851,7 +857,7 @@ def run_profile(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="dftk", choices=["dftk", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
