@@ -120,46 +120,44 @@ __device__ __forceinline__ void g_etab(T PA, T PB, T h, T (&E)[IA + 1][JB + 1][I
 // R_{tuv} = R^{(0)}_{tuv}(rho, X, Y, Z) for t + u + v <= LM, times `pre`:
 // R^{(n)}_{000} = pre (-2 rho)^n F_n and
 // R^{(n)}_{t+1,u,v} = t R^{(n+1)}_{t-1,u,v} + X R^{(n+1)}_{t,u,v} (first non-zero index).
+// Computed in place, one order n at a time from n = LM down to 0: order n's
+// entries of index sum s need order n + 1's entries of sums s - 1 and s - 2,
+// so writing the sums in decreasing order never overwrites an entry still to
+// be read.  One cube of storage (no per-order copies), every index fixed at
+// compile time.
 template <typename T, int LM>
 __device__ __forceinline__ void g_rcube(T X, T Y, T Z, T m2rho, T pre, const T *F,
                                         T (&R)[LM + 1][LM + 1][LM + 1])
 {
-    T Rn[LM + 1][LM + 1][LM + 1][LM + 1];
-    T c = pre;
+    T cp[LM + 1];
+    cp[0] = pre;
 #pragma unroll
-    for (int n = 0; n <= LM; ++n) {
-        Rn[n][0][0][0] = c * F[n];
-        c *= m2rho;
-    }
+    for (int n = 1; n <= LM; ++n) cp[n] = cp[n - 1] * m2rho;
+    R[0][0][0] = cp[LM] * F[LM];
 #pragma unroll
-    for (int s = 1; s <= LM; ++s)
+    for (int n = LM - 1; n >= 0; --n) {
 #pragma unroll
-        for (int t = 0; t <= s; ++t)
+        for (int s = LM - n; s >= 1; --s)
 #pragma unroll
-            for (int u = 0; u <= s - t; ++u) {
-                const int v = s - t - u;
+            for (int t = 0; t <= s; ++t)
 #pragma unroll
-                for (int n = 0; n <= LM - s; ++n) {
+                for (int u = 0; u <= s - t; ++u) {
+                    const int v = s - t - u;
                     T r;
                     if (t > 0) {
-                        r = X * Rn[n + 1][t - 1][u][v];
-                        if (t > 1) r = fma((T)(t - 1), Rn[n + 1][t - 2][u][v], r);
+                        r = X * R[t - 1][u][v];
+                        if (t > 1) r = fma((T)(t - 1), R[t - 2][u][v], r);
                     } else if (u > 0) {
-                        r = Y * Rn[n + 1][t][u - 1][v];
-                        if (u > 1) r = fma((T)(u - 1), Rn[n + 1][t][u - 2][v], r);
+                        r = Y * R[t][u - 1][v];
+                        if (u > 1) r = fma((T)(u - 1), R[t][u - 2][v], r);
                     } else {
-                        r = Z * Rn[n + 1][t][u][v - 1];
-                        if (v > 1) r = fma((T)(v - 1), Rn[n + 1][t][u][v - 2], r);
+                        r = Z * R[t][u][v - 1];
+                        if (v > 1) r = fma((T)(v - 1), R[t][u][v - 2], r);
                     }
-                    Rn[n][t][u][v] = r;
+                    R[t][u][v] = r;
                 }
-            }
-#pragma unroll
-    for (int t = 0; t <= LM; ++t)
-#pragma unroll
-        for (int u = 0; u <= LM - t; ++u)
-#pragma unroll
-            for (int v = 0; v <= LM - t - u; ++v) R[t][u][v] = Rn[0][t][u][v];
+        R[0][0][0] = cp[n] * F[n];
+    }
 }
 
 // gradient accumulation into the block's shared copy (or global memory)
