@@ -338,102 +338,130 @@ def batch_figures(torch, n_mol=512, n_max=24, n_single=64, n_grad=256, n_grad_ma
 
 
 # ------------------------------------------------------------ reference arm
-def cpu_reference_rate(eng_totals, shells, q_by_class, per_class, seed=0, kernel="reference"):
-    """Fock builds/s of the reference's CPU path, from timed per-class samples.
-
-    Samples `per_class[c]` Schwarz-surviving quartets of each class, digests
-    them with the reference's host-compiled eri_kernel (kernel="reference")
-    or the restated one ("port"), and extrapolates each class's time by its
-    quartet count.  Returns (builds_per_s, cores, sample description)."""
-    from oracle import oracle as orc
-
-    rng = np.random.default_rng(seed)
+def _pairs_by_class(shells):
+    """Shell pairs (i, j), j <= i, in the reference's pair order, per pair class
+    (l_a + l_b)."""
     l = np.array([s["angular_momentum"] for s in shells])
     ii, jj = np.tril_indices(len(shells))
-    pairs_by_class = [[], [], []]
-    for i, j in zip(ii, jj):
-        a, b = (i, j) if l[i] >= l[j] else (j, i)
-        pairs_by_class[l[a] + l[b]].append((i, j))
-    from dft_b200.engine import QCLASS_PAIRS
+    lo, hi = np.minimum(l[ii], l[jj]), np.maximum(l[ii], l[jj])
+    pc = lo + hi
+    return [np.stack([ii[pc == c], jj[pc == c]], axis=1) for c in range(3)]
 
-    N = shells[-1]["ao_stop"]
+
+def _sample_quartets(rng, pairs, q_by_class, X, Y, n, tau=1e-12):
+    """n random Schwarz-kept unique quartets (Q_ab Q_cd >= tau) of the quartet
+    class with pair classes (X, Y), as an (n, 4) int32 array of shells."""
+    px, py = pairs[X], pairs[Y]
+    qx, qy = q_by_class[X], q_by_class[Y]
+    out = []
+    have = 0
+    while have < n:
+        r = rng.integers(len(px), size=8 * n)
+        k = rng.integers(len(py), size=8 * n)
+        if X == Y:
+            r, k = np.maximum(r, k), np.minimum(r, k)
+        keep = qx[r] * qy[k] >= tau
+        r, k = r[keep], k[keep]
+        out.append(np.hstack([px[r], py[k]]))
+        have += len(r)
+    return np.ascontiguousarray(np.vstack(out)[:n], dtype=np.int32)
+
+
+# Sample sizes (quartets) of the two timed calls per class: the marginal cost
+# per quartet is the slope between them, so the fixed cost of one call (shell
+# arrays, per-thread accumulators of 3 N^2 doubles, their reduction, thread
+# start-up) is not multiplied by the class counts.  About 3 s of work on 16
+# host threads for (H2O)_64.
+CPU_SAMPLE_SMALL = (4000, 4000, 2000, 2000, 1000, 250)
+CPU_SAMPLE_LARGE = (60000, 60000, 24000, 24000, 9000, 2250)
+
+
+def cpu_reference_rate(eng_totals, shells, q_by_class, seed=0, small=CPU_SAMPLE_SMALL, large=CPU_SAMPLE_LARGE):
+    """Fock builds/s of the reference's CPU path from per-class marginal costs.
+
+    For each quartet class, two samples of Schwarz-kept quartets (sizes
+    small[c] and large[c]) go through the reference's host-compiled
+    eri_kernel (oracle/_ref; the restated one when it is not built) with the
+    restated contraction and fill_matrices digestion; the slope between the
+    two timings is the class's cost per quartet, the intercept the fixed cost
+    of one call.  One build = sum_c slope_c * count_c + one fixed cost.
+    Returns a dict: builds_per_s, cores, kind, us_per_quartet (per class),
+    fixed_ms, sample_s (wall time of the timed calls), sample (description)."""
+    from oracle import oracle as orc
+    from dft_b200.engine import QCLASS_NAMES, QCLASS_PAIRS
+
+    rng = np.random.default_rng(seed)
+    pairs = _pairs_by_class(shells)
+    sa = orc.ShellArrays(shells)
+    N = sa.N
     A = rng.normal(size=(N, N))
     P = (A + A.T) * 0.01
-    ref = orc.ref_lib() if kernel == "reference" else None
-    if kernel == "reference" and ref is None:
-        kernel = "port"
-    total_t = 0.0
-    desc = []
-    for c, (X, Y) in enumerate(QCLASS_PAIRS):
-        n = per_class[c]
-        if eng_totals[c] == 0 or n == 0:
-            continue
-        qx, qy = q_by_class[X], q_by_class[Y]
-        px, py = pairs_by_class[X], pairs_by_class[Y]
-        picks = []
-        tries = 0
-        while len(picks) < n and tries < 200 * n:
-            tries += 1
-            r = rng.integers(len(px))
-            k = rng.integers(len(py))
-            if X == Y and k > r:
-                r, k = k, r
-            if qx[r] * qy[k] >= 1e-12:
-                picks.append((*px[r], *py[k]))
-        quads = np.array(picks, dtype=np.int32)
+    Ph = P / 2
+    ref = orc.ref_lib()
+    kind = "reference" if ref is not None else "port"
+
+    def run(quads):
         t0 = time.perf_counter()
-        if kernel == "reference":
-            orc.direct_jk_reference_kernel(shells, quads, P, P / 2, P / 2, ref=ref)
+        if ref is not None:
+            orc.direct_jk_reference_kernel(shells, quads, P, Ph, Ph, ref=ref, sa=sa)
         else:
-            orc.direct_jk(shells, quads, P, P / 2, P / 2)
-        dt = time.perf_counter() - t0
-        total_t += dt / len(picks) * eng_totals[c]
-        desc.append(f"{len(picks)}")
+            orc.direct_jk(shells, quads, P, Ph, Ph, sa=sa)
+        return time.perf_counter() - t0
+
+    run(_sample_quartets(rng, pairs, q_by_class, 0, 0, 64))  # thread pool and caches warm
+    us, fixed, wall = {}, [], 0.0
+    build_s = 0.0
+    for c, (X, Y) in enumerate(QCLASS_PAIRS):
+        if eng_totals[c] == 0:
+            continue
+        q1 = _sample_quartets(rng, pairs, q_by_class, X, Y, small[c])
+        q2 = _sample_quartets(rng, pairs, q_by_class, X, Y, large[c])
+        t1, t2 = run(q1), run(q2)
+        wall += t1 + t2
+        slope = max(t2 - t1, 1e-9) / (large[c] - small[c])
+        us[QCLASS_NAMES[c]] = slope * 1e6
+        fixed.append(max(t1 - slope * small[c], 0.0))
+        build_s += slope * eng_totals[c]
+    fixed_s = float(np.median(fixed)) if fixed else 0.0
+    build_s += fixed_s
     cores = orc.lib().orc_num_threads()
-    sample = (f"{'/'.join(desc)} Schwarz-kept quartets per class (ss|ss)..(pp|pp) of (H2O)_64, "
-              f"timed with {cores} OpenMP threads, extrapolated by class counts {list(eng_totals)}")
-    return 1.0 / total_t, cores, sample, kernel
+    sample = (f"per class two timed calls of {'/'.join(map(str, small))} and {'/'.join(map(str, large))} "
+              f"Schwarz-kept quartets (ss|ss)..(pp|pp) of (H2O)_64; the slope is the cost per quartet, "
+              f"extrapolated by the class counts {list(map(int, eng_totals))} plus one fixed call cost; "
+              f"{cores} OpenMP threads")
+    return {"builds_per_s": 1.0 / build_s, "cores": cores, "kind": kind, "us_per_quartet": us,
+            "fixed_ms": fixed_s * 1e3, "sample_s": wall, "sample": sample}
 
 
-def cpu_reference_class_rates(shells, q_by_class, per_class, seed=0):
+def cpu_reference_class_rates(shells, q_by_class, small, large, seed=0):
     """Shell quartets/s per class of the reference's CPU path (host-compiled
-    eri_kernel + restated contraction and digestion), on samples of
-    Schwarz-kept quartets (CPU-baseline leg)."""
+    eri_kernel + restated contraction and digestion) from the slope between
+    two sample sizes of Schwarz-kept quartets (CPU-baseline leg)."""
     from oracle import oracle as orc
     from dft_b200.engine import QCLASS_PAIRS
 
     rng = np.random.default_rng(seed)
-    l = np.array([s_["angular_momentum"] for s_ in shells])
-    ii, jj = np.tril_indices(len(shells))
-    pairs_by_class = [[], [], []]
-    for i, j in zip(ii, jj):
-        a, b = (i, j) if l[i] >= l[j] else (j, i)
-        pairs_by_class[l[a] + l[b]].append((i, j))
-    N = shells[-1]["ao_stop"]
+    pairs = _pairs_by_class(shells)
+    sa = orc.ShellArrays(shells)
+    N = sa.N
     A = rng.normal(size=(N, N))
     P = (A + A.T) * 0.01
     ref = orc.ref_lib()
-    rates = []
-    for c, (X, Y) in enumerate(QCLASS_PAIRS):
-        qx, qy = q_by_class[X], q_by_class[Y]
-        px, py = pairs_by_class[X], pairs_by_class[Y]
-        picks = []
-        tries = 0
-        while len(picks) < per_class[c] and tries < 200 * per_class[c]:
-            tries += 1
-            r = rng.integers(len(px))
-            k = rng.integers(len(py))
-            if X == Y and k > r:
-                r, k = k, r
-            if qx[r] * qy[k] >= 1e-12:
-                picks.append((*px[r], *py[k]))
-        quads = np.array(picks, dtype=np.int32)
+
+    def run(quads):
         t0 = time.perf_counter()
         if ref is not None:
-            orc.direct_jk_reference_kernel(shells, quads, P, P / 2, P / 2, ref=ref)
+            orc.direct_jk_reference_kernel(shells, quads, P, P / 2, P / 2, ref=ref, sa=sa)
         else:
-            orc.direct_jk(shells, quads, P, P / 2, P / 2)
-        rates.append(len(picks) / (time.perf_counter() - t0))
+            orc.direct_jk(shells, quads, P, P / 2, P / 2, sa=sa)
+        return time.perf_counter() - t0
+
+    run(_sample_quartets(rng, pairs, q_by_class, 0, 0, 64))
+    rates = []
+    for c, (X, Y) in enumerate(QCLASS_PAIRS):
+        t1 = run(_sample_quartets(rng, pairs, q_by_class, X, Y, small[c]))
+        t2 = run(_sample_quartets(rng, pairs, q_by_class, X, Y, large[c]))
+        rates.append((large[c] - small[c]) / max(t2 - t1, 1e-9))
     return rates, orc.lib().orc_num_threads(), "reference" if ref is not None else "port"
 
 
@@ -550,10 +578,12 @@ def c10h22_figures(torch, cpu: bool):
            "quartets_per_s": {QCLASS_NAMES[k]: (ev[k] / (ms[k] / 1e3) if ms[k] > 0 else None) for k in range(6)}}
     if cpu:
         qs = schwarz_by_reference_order(shells)
-        rates, cores, kind = cpu_reference_class_rates(shells, qs, [2000, 2000, 1000, 1000, 500, 200], seed=3)
+        small, large = (2000, 2000, 1000, 1000, 500, 200), (10000, 10000, 5000, 5000, 2500, 1000)
+        rates, cores, kind = cpu_reference_class_rates(shells, qs, small, large, seed=3)
         out["cpu_reference_quartets_per_s"] = {QCLASS_NAMES[k]: rates[k] for k in range(6)}
         out["cpu_reference"] = {"cores": cores, "kind": kind,
-                                "sample": "2000/2000/1000/1000/500/200 Schwarz-kept quartets per class"}
+                                "sample": (f"slope between {'/'.join(map(str, small))} and {'/'.join(map(str, large))} "
+                                           "Schwarz-kept quartets per class")}
     return out
 
 
@@ -571,6 +601,9 @@ def schwarz_by_reference_order(shells):
 
 
 def run_reference_arm(args, rank, world):
+    """The reference's CPU path on the host cores: each step times the
+    per-class samples of cpu_reference_rate (a bounded sample of one (H2O)_64
+    build) and extrapolates one build from their slopes.  Rank 0 only."""
     if rank != 0:
         return 0
     from dft_b200 import basis, geometry
@@ -581,28 +614,44 @@ def run_reference_arm(args, rank, world):
     qs = schwarz_by_reference_order(shells)
     qsorted = [np.sort(q)[::-1] for q in qs]
     totals = [int(candidate_offsets(qsorted[X], qsorted[Y], X == Y, 1e-12)[-1]) for X, Y in QCLASS_PAIRS]
-    per_class = [4000, 4000, 2000, 2000, 800, 160]
-    for _ in range(max(0, args.warmup)):
-        cpu_reference_rate(totals, shells, qs, [max(1, n // 10) for n in per_class], seed=1)
-    rates = []
+    small = tuple(max(1, n // 10) for n in CPU_SAMPLE_SMALL)
+    large = tuple(max(2, n // 10) for n in CPU_SAMPLE_LARGE)
+    for w in range(max(0, args.warmup)):
+        cpu_reference_rate(totals, shells, qs, seed=1 + w, small=small, large=large)
+    rates, step_s, res = [], [], None
     t0 = time.perf_counter()
     for s in range(args.steps):
-        r, cores, sample, kind = cpu_reference_rate(totals, shells, qs, per_class, seed=100 + s)
-        rates.append(r)
+        ts = time.perf_counter()
+        res = cpu_reference_rate(totals, shells, qs, seed=100 + s)
+        step_s.append(time.perf_counter() - ts)
+        rates.append(res["builds_per_s"])
     wall = time.perf_counter() - t0
     value = float(np.mean(rates))
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
+        "steps": args.steps, "warmup": args.warmup,
+        # one step is a timed sample of a build, not a whole build (about 1e4 s)
+        "ms_per_step": 1e3 * float(np.mean(step_s)), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "molecule": "(H2O)_64", "basis": "STO-3G", "n_basis": 448,
-                   "quartets_per_class": totals},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+        "config": workload_config(len(shells) and shells[-1]["ao_stop"]),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": res["cores"], "kind": res["kind"],
+                         "sample": res["sample"], "us_per_quartet": res["us_per_quartet"],
+                         "fixed_ms_per_call": res["fixed_ms"]},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "extrapolated_s_per_build": 1.0 / value,
+        "builds_per_s_per_step": rates,
         "wall_s": wall,
+        "quartets_per_class": totals,
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def workload_config(n_basis):
+    """The config object both arms print for the (H2O)_64 J/K workload."""
+    return {"workload": WORKLOAD, "molecule": "(H2O)_64 4x4x4 lattice seed 0", "basis": "STO-3G",
+            "n_basis": int(n_basis), "tau_schwarz": 1e-12, "tau_density": 1e-14,
+            "l2": "flushed between steps (256 MB write)", "parallelism": "replicas x1"}
 
 
 # ---------------------------------------------------------------- main arm
@@ -750,21 +799,20 @@ def run_dftk_arm(args, rank, world, local_rank):
             from dft_b200.engine import QCLASS_PAIRS
 
             qs = schwarz_by_reference_order(shells)
-            rate, cores, sample, kind = cpu_reference_rate(eng.quartet_totals(), shells, qs,
-                                                           [6000, 6000, 3000, 3000, 1200, 240], seed=7)
-            cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+            res = cpu_reference_rate(eng.quartet_totals(), shells, qs, seed=7)
+            cpu = {"value": res["builds_per_s"], "unit": UNIT, "cores": res["cores"], "kind": res["kind"],
+                   "sample": res["sample"], "us_per_quartet": res["us_per_quartet"],
+                   "fixed_ms_per_call": res["fixed_ms"], "sample_s": res["sample_s"]}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "strong" if shard is not None else "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "molecule": "(H2O)_64 4x4x4 lattice seed 0", "basis": "STO-3G",
-                       "n_basis": N, "tau_schwarz": 1e-12, "tau_density": 1e-14,
-                       "quartets_per_class": eng.quartet_totals(), "evaluated_per_class": evaluated,
-                       "primitive_quartets_per_class": prim_evaluated, "tau_prim": eng.tau_prim,
-                       "l2": "flushed between steps (256 MB write)",
-                       "parallelism": (f"candidate space sharded x{world}, NCCL all-reduce of J/K" if shard is not None
-                                       else f"replicas x{world}")},
+            "config": dict(workload_config(N), parallelism=(
+                f"candidate space sharded x{world}, NCCL all-reduce of J/K" if shard is not None
+                else f"replicas x{world}")),
+            "quartets_per_class": eng.quartet_totals(), "evaluated_per_class": evaluated,
+            "primitive_quartets_per_class": prim_evaluated, "tau_prim": eng.tau_prim,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * N * N * 8,
                     "d2h_bytes_per_step": 3 * N * N * 8, "call": "shelled.fill_matrices (host NumPy arrays)"},
             # per build: k_dsh, one k_select and one k_jk_list per class with candidates, k_symmetrize
@@ -773,6 +821,9 @@ def run_dftk_arm(args, rank, world, local_rank):
                          "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
                          "peak_source": "measured FP64 FMA loop (dftk_fma_burn) on this GPU",
                          "traffic": traffic,
+                         "traffic_source": ("profiles/jk_traffic.json: dram__bytes_read.sum + dram__bytes_write.sum "
+                                            "of one launch of this kernel from an earlier ncu capture of this "
+                                            "workload, read by the bench (not measured in this run)"),
                          "whole_build_tflops": total_flops / (ms_per_step / 1e3) / 1e12,
                          "whole_build_tflops_81_prims_per_quartet": full_prim_flops / (ms_per_step / 1e3) / 1e12,
                          "class_ms": {QCLASS_NAMES[c]: float(class_ms[c]) for c in range(6)},

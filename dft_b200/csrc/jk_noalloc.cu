@@ -20,7 +20,9 @@
 //     start at zero, so the contents a previous call left behind do no harm;
 //   * the first call on a device looks up the array's device address
 //     (cudaGetSymbolAddress) with that device current; make that first call
-//     before any stream capture.
+//     before any stream capture.  The address is cached for the life of the
+//     process, which assumes the device's primary context is not reset
+//     (cudaDeviceReset) in between.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -60,10 +62,19 @@ extern "C" int dftk_jk_noalloc(const dftk_shells_t *shells, const dftk_pairs_t p
                         shells->dsh_elems > (long long)DFTK_NOALLOC_MAX_SHELLS * DFTK_NOALLOC_MAX_SHELLS);
     if (shells->n_ao < 0 || shells->n_shells < 0 || batch_too_big ||
         (!shells->mol && (shells->n_ao > DFTK_NOALLOC_MAX_AO || shells->n_shells > DFTK_NOALLOC_MAX_SHELLS))) {
-        const std::string msg = "dftk_jk_noalloc: " + std::to_string(shells->n_ao) + " basis functions / " +
-                                std::to_string(shells->n_shells) + " shells exceed the fixed scratch limit of " +
-                                std::to_string(DFTK_NOALLOC_MAX_AO) + " / " +
-                                std::to_string(DFTK_NOALLOC_MAX_SHELLS) + "; use dftk_jk with a workspace";
+        // a batch is limited by its packed matrix and density-maxima sizes,
+        // a single molecule by its basis functions and shells
+        const std::string lim = std::to_string(DFTK_NOALLOC_MAX_AO);
+        const std::string lims = std::to_string(DFTK_NOALLOC_MAX_SHELLS);
+        const std::string msg =
+            shells->mol
+                ? "dftk_jk_noalloc: the batch's packed matrices (" + std::to_string(shells->mat_elems) +
+                      " elements) or density maxima (" + std::to_string(shells->dsh_elems) +
+                      " elements) exceed the fixed scratch limit of " + lim + "^2 / " + lims +
+                      "^2; use dftk_jk with a workspace"
+                : "dftk_jk_noalloc: " + std::to_string(shells->n_ao) + " basis functions / " +
+                      std::to_string(shells->n_shells) + " shells exceed the fixed scratch limit of " + lim +
+                      " / " + lims + "; use dftk_jk with a workspace";
         dftk_internal_set_error(msg.c_str());
         return DFTK_ERR_SIZE;
     }

@@ -18,7 +18,7 @@
  *   dftk_schwarz          <- (absent in the reference: screening bounds)
  *   dftk_eri_blocks       <- calc_eri quartet blocks          shelled.py:596-700
  *   dftk_jk               <- fill_matrices                    shelled.py:770-877
- *   dftk_jk_noalloc       <- fill_matrices, for hosts that cannot allocate device memory
+ *   dftk_jk_noalloc       <- (absent in the reference: dftk_jk with fixed in-library scratch)
  *   dftk_grad             <- (absent in the reference: analytic nuclear gradients)
  *   dftk_workspace_bytes  <- (absent: workspace size of one molecule or a batch)
  *   dftk_prepare          <- pair_list + pair_cache setup and the quartet enumeration
@@ -254,7 +254,9 @@ int dftk_jk(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N_PCLASS]
  * most 512 basis functions and 512 shells (DFTK_ERR_SIZE otherwise).  All
  * calls share that array: calls that overlap on the GPU race, so keep them on
  * one stream.  The first call on a device looks up the array's address with
- * that device current; make it before any stream capture. */
+ * that device current; make it before any stream capture.  The address is
+ * kept for the life of the process, so it assumes the device's primary
+ * context is not reset (cudaDeviceReset) between calls. */
 int dftk_jk_noalloc(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N_PCLASS],
                     const dftk_queue_t *queue, const double *D, const double *D_a,
                     const double *D_b, double *J, double *K_a, double *K_b, int flags,

@@ -115,7 +115,22 @@ def extract_kernel_source(reference_dir: str) -> str:
     raise RuntimeError(f"no `source = ...` assignment found in {path}")
 
 
-def build(reference_dir: str = "/root/reference", quiet: bool = False) -> str:
+# Where this recipe looks for the reference checkout when DFT_REFERENCE is not
+# set (the build container's read-only copy; absent on machines that only run
+# the prebuilt files).
+_CONTAINER_REFERENCE = "/root/reference"
+
+
+def reference_dir():
+    """The reference checkout to compile from: $DFT_REFERENCE, else the build
+    container's copy; None when neither exists (nothing to build)."""
+    for d in (os.environ.get("DFT_REFERENCE"), _CONTAINER_REFERENCE):
+        if d and os.path.isfile(os.path.join(d, "shelled.py")):
+            return d
+    return None
+
+
+def build(reference_dir: str, quiet: bool = False) -> str:
     src = extract_kernel_source(reference_dir)
     lines = [ln for ln in src.splitlines() if "#include <math_constants.h>" not in ln]
     os.makedirs(OUT_DIR, exist_ok=True)
@@ -132,9 +147,12 @@ def build(reference_dir: str = "/root/reference", quiet: bool = False) -> str:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("DFT_REFERENCE", "/root/reference"))
+    ap.add_argument("--reference", default=None, help="reference checkout (default: $DFT_REFERENCE)")
     args = ap.parse_args()
-    print(build(args.reference))
+    ref = args.reference or reference_dir()
+    if ref is None:
+        ap.error("no reference checkout: pass --reference or set DFT_REFERENCE")
+    print(build(ref))
 
 
 if __name__ == "__main__":

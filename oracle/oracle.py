@@ -226,9 +226,10 @@ def fill_matrices(shells, quads, values, offsets, P, P_a, P_b):
     return J, Ka, Kb
 
 
-def direct_jk(shells, quads, P, P_a, P_b):
-    """Integral-direct J, K_a, K_b over the given unique quartets."""
-    sa = ShellArrays(shells)
+def direct_jk(shells, quads, P, P_a, P_b, sa=None):
+    """Integral-direct J, K_a, K_b over the given unique quartets (``sa``: the
+    molecule's ShellArrays, built here when not given)."""
+    sa = sa if sa is not None else ShellArrays(shells)
     N = sa.N
     J, Ka, Kb = (np.zeros((N, N)) for _ in range(3))
     P, P_a, P_b = (np.ascontiguousarray(x, dtype=np.float64) for x in (P, P_a, P_b))
@@ -238,13 +239,13 @@ def direct_jk(shells, quads, P, P_a, P_b):
     return J, Ka, Kb
 
 
-def direct_jk_reference_kernel(shells, quads, P, P_a, P_b, ref=None):
+def direct_jk_reference_kernel(shells, quads, P, P_a, P_b, ref=None, sa=None):
     """direct_jk with the primitive ERIs from the reference's own eri_kernel
     (oracle/_ref), contraction and digestion from the restatement."""
     ref = ref if ref is not None else ref_lib()
     if ref is None:
         raise RuntimeError("oracle/_ref/libref.so not built")
-    sa = ShellArrays(shells)
+    sa = sa if sa is not None else ShellArrays(shells)
     N = sa.N
     J, Ka, Kb = (np.zeros((N, N)) for _ in range(3))
     P, P_a, P_b = (np.ascontiguousarray(x, dtype=np.float64) for x in (P, P_a, P_b))

@@ -62,6 +62,62 @@ def test_noalloc_matches_workspace_jk(shape):
         assert (J - J1).abs().max().item() < TOL and (Ka - K1).abs().max().item() < TOL
 
 
+@pytest.mark.gpu
+def test_noalloc_mixed_and_scan_path_near_limit():
+    """(H2O)_64 (448 basis functions, 320 shells) is near the 512 limit: its
+    selection lists (about 0.9 GB) do not fit the fixed scratch, so the call
+    takes the direct path, where the class kernels scan the candidates
+    themselves.  Checked against dftk_jk with a full workspace, FP64 and mixed
+    FP32/FP64 (same thresholds, so the same quartets run in FP32), twice each."""
+    import torch
+
+    from dft_b200.engine import IntegralEngine
+
+    atoms, centers = geometry.water_cluster((4, 4, 4))
+    eng = IntegralEngine(basis.build_shells(basis.load_basis(), atoms, centers), tau_schwarz=1e-12)
+    N = eng.n_ao
+    assert N == 448
+    rng = np.random.default_rng(6)
+    A = rng.normal(size=(N, N))
+    D = torch.as_tensor(0.01 * (A + A.T)).cuda()
+    Dh = (0.5 * D).contiguous()
+    for mixed in (False, True):
+        J0, K0, _ = eng.jk(D, Dh, mixed=mixed, tau=1e-12, tau_fp32=1e-6)
+        # the two paths add the same terms in different orders: FP64 atomics
+        # over ~1e8 terms per build, so compare relative to the largest element
+        tol = 1e-12 * max(1.0, J0.abs().max().item())
+        for _ in range(2):
+            J, Ka, _ = _noalloc(eng, D, Dh, None, uhf=False, tau=1e-12, mixed=mixed, tau_fp32=1e-6)
+            torch.cuda.synchronize()
+            assert (J - J0).abs().max().item() < tol, mixed
+            assert (Ka - K0).abs().max().item() < tol, mixed
+
+
+@pytest.mark.gpu
+def test_noalloc_mixed_small():
+    """Mixed FP32/FP64 call on a small cluster, against dftk_jk, twice."""
+    import torch
+
+    from dft_b200.engine import IntegralEngine
+
+    atoms, centers = geometry.water_cluster((2, 2, 2), seed=5)
+    eng = IntegralEngine(basis.build_shells(basis.load_basis(), atoms, centers), tau_schwarz=1e-12)
+    N = eng.n_ao
+    rng = np.random.default_rng(8)
+    A = rng.normal(size=(N, N))
+    D = torch.as_tensor(1e-4 * (A + A.T)).cuda()  # small, so many quartets fall below tau_fp32
+    Dh = (0.5 * D).contiguous()
+    counts = torch.zeros(24, dtype=torch.int64, device="cuda")
+    J0, K0, _ = eng.jk(D, Dh, mixed=True, tau=1e-14, tau_fp32=1e-6, counts=counts)
+    torch.cuda.synchronize()
+    assert counts[6:12].sum().item() > 0  # some quartets did run in FP32
+    for _ in range(2):
+        J, Ka, _ = _noalloc(eng, D, Dh, None, uhf=False, tau=1e-14, mixed=True, tau_fp32=1e-6)
+        torch.cuda.synchronize()
+        assert (J - J0).abs().max().item() < TOL and (Ka - K0).abs().max().item() < TOL
+
+
+@pytest.mark.gpu
 def test_noalloc_rejects_oversize_molecule():
     """Sizes beyond the fixed scratch are refused before any device work."""
     lib = _lib.load()
