@@ -18,6 +18,7 @@ N_QCLASS = 6
 N_PCLASS = 3
 JK_UHF = 1
 JK_MIXED = 2
+PCLASS_GENERIC = 3  # dftk_pair_data: the 13-field record layout of the d-shell path
 
 OK, ERR_ARG, ERR_CUDA, ERR_UNSUPPORTED, ERR_WORKSPACE, ERR_SIZE = range(6)
 
@@ -28,6 +29,7 @@ SYMBOLS = (
     "dftk_jk_workspace_bytes", "dftk_jk_workspace_bytes_queue", "dftk_jk", "dftk_nuclear_kernel", "dftk_eri_kernel",
     "dftk_fma_burn", "dftk_jk_timing", "dftk_jk_timing_read", "dftk_jk_noalloc", "dftk_grad", "dftk_workspace_bytes",
     "dftk_set_launch", "dftk_get_launch", "dftk_grid_ao", "dftk_grid_density", "dftk_prepare_bytes", "dftk_prepare",
+    "dftk_hl_schwarz", "dftk_jk_hl", "dftk_hl_eri_blocks",
 )
 
 
@@ -91,6 +93,18 @@ class Queue(ctypes.Structure):
     ]
 
 
+class HlSet(ctypes.Structure):
+    """dftk_hl_t: the pair sets and candidate spaces of the quartets with a d shell."""
+    _fields_ = [
+        ("hi", Pairs),
+        ("lo", Pairs),
+        ("n_rows", ctypes.c_longlong),
+        ("total", ctypes.c_longlong * 2),
+        ("row_off", ctypes.c_void_p * 2),
+        ("tau_prim", ctypes.c_double),
+    ]
+
+
 PairsArray = Pairs * N_PCLASS
 
 _lib: Optional[ctypes.CDLL] = None
@@ -140,6 +154,9 @@ def load() -> ctypes.CDLL:
         "dftk_grid_density": ([i, i, i, ll, vp, vp, ll, vp, vp, ll, vp], i),
         "dftk_prepare_bytes": ([ctypes.POINTER(Shells), ctypes.POINTER(ctypes.c_size_t)], i),
         "dftk_prepare": ([ctypes.POINTER(Shells), d, d, vp, sz, ctypes.POINTER(Pairs), ctypes.POINTER(Queue), vp], i),
+        "dftk_hl_schwarz": ([ctypes.POINTER(Shells), ctypes.POINTER(Pairs), vp], i),
+        "dftk_jk_hl": ([ctypes.POINTER(Shells), ctypes.POINTER(HlSet), vp, vp, vp, vp, vp, vp, i, d, vp, sz, vp, vp], i),
+        "dftk_hl_eri_blocks": ([ctypes.POINTER(Shells), ctypes.POINTER(HlSet), ll, vp, vp, vp, vp], i),
     }
     missing = set(SYMBOLS) - set(sig)
     if missing:  # every entry point gets explicit argument types (64-bit sizes)

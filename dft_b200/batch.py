@@ -88,7 +88,7 @@ class BatchEngine(IntegralEngine):
             raise _lib.DftkError("batch", _lib.ERR_ARG, "empty batch")
         per = [_basis.build_shells(basis_data, a, c) for a, c in self.molecules]
         for sh in per:
-            _basis.check_supported(sh)
+            _basis.check_sp(sh, "batch")
         self.n_mol = len(per)
         self.mol_ns = np.array([len(s) for s in per], dtype=np.int64)
         self.mol_nao = np.array([int(s[-1]["ao_stop"]) for s in per], dtype=np.int64)

@@ -18,6 +18,7 @@
 #include "grad.cuh"
 #include "onee.cuh"
 #include "grid.cuh"
+#include "hl.cuh"
 
 namespace {
 
@@ -476,14 +477,16 @@ int dftk_boys32(int mmax, long long n, const float *T, float *F, dftk_stream_t s
 
 int dftk_pair_data(const dftk_shells_t *shells, int pair_class, dftk_pairs_t *pairs, dftk_stream_t stream)
 {
-    if (!shells || !pairs || pair_class < 0 || pair_class > 2) return fail(DFTK_ERR_ARG, "dftk_pair_data: bad arguments");
+    if (!shells || !pairs || pair_class < 0 || pair_class > DFTK_PCLASS_GENERIC)
+        return fail(DFTK_ERR_ARG, "dftk_pair_data: bad arguments");
     if (pairs->n_pairs < 0 || pairs->kmax <= 0) return fail(DFTK_ERR_ARG, "dftk_pair_data: bad pair counts");
-    if ((long long)pairs->n_pairs * pairs->kmax * pair_fields(pair_class) >= (1LL << 31))
+    const int nf = pair_class == DFTK_PCLASS_GENERIC ? HL_FIELDS : pair_fields(pair_class);
+    if ((long long)pairs->n_pairs * pairs->kmax * nf >= (1LL << 31))
         return fail(DFTK_ERR_SIZE, "dftk_pair_data: records exceed 2^31 elements (32-bit offsets)");
     DFTK_INIT();
     const long long n = (long long)pairs->n_pairs * pairs->kmax;
     if (n == 0) return DFTK_OK;
-    k_pair_data<<<blocks_for(n, 128), 128, 0, (cudaStream_t)stream>>>(*shells, *pairs, pair_fields(pair_class));
+    k_pair_data<<<blocks_for(n, 128), 128, 0, (cudaStream_t)stream>>>(*shells, *pairs, nf);
     DFTK_LAUNCHED("k_pair_data");
     return DFTK_OK;
 }
@@ -495,7 +498,7 @@ int dftk_schwarz(const dftk_shells_t *shells, int pair_class, dftk_pairs_t *pair
     const int n = pairs->n_pairs;
     if (n == 0) return DFTK_OK;
     cudaStream_t s = (cudaStream_t)stream;
-    if (pairs->kmax > DFTK_MAX_KPAIR) return fail(DFTK_ERR_SIZE, "dftk_schwarz: more than 64 primitive pairs per pair");
+    if (pairs->kmax > DFTK_MAX_KPAIR) return fail(DFTK_ERR_SIZE, "dftk_schwarz: more than 128 primitive pairs per pair");
     if (!pairs->qp) return fail(DFTK_ERR_ARG, "dftk_schwarz: null qp");
     const int nf = pair_fields(pair_class);
     if (pair_class == 0) k_schwarz<0><<<blocks_for(n, 64), 64, 0, s>>>(*pairs, nf);
@@ -544,7 +547,7 @@ int prepare_plan(const dftk_shells_t *shells, PreparePlan &pl)
         pmax = std::max(pmax, np[i]);
     }
     pl.kmax = pmax * pmax;
-    if (pl.kmax > DFTK_MAX_KPAIR) return fail(DFTK_ERR_SIZE, "dftk_prepare: more than 64 primitive pairs per pair");
+    if (pl.kmax > DFTK_MAX_KPAIR) return fail(DFTK_ERR_SIZE, "dftk_prepare: more than 128 primitive pairs per pair");
     for (int i = 0; i < ns; ++i)
         for (int j = 0; j <= i; ++j) {
             const bool swap = l[i] < l[j];
@@ -682,6 +685,12 @@ int dftk_one_electron(const dftk_shells_t *shells, int n_atoms, const double *at
     if (npair == 0) return DFTK_OK;
     k_one_electron<<<blocks_for(npair, 64), 64, 0, (cudaStream_t)stream>>>(*shells, n_atoms, atom_xyz, atom_z, S, T, V);
     DFTK_LAUNCHED("k_one_electron");
+    if (!shells->mol) {
+        // pairs with a d shell (the kernel returns at once for the others)
+        k_one_electron_hl<<<blocks_for(npair, 64), 64, 0, (cudaStream_t)stream>>>(*shells, n_atoms, atom_xyz, atom_z,
+                                                                                 S, T, V);
+        DFTK_LAUNCHED("k_one_electron_hl");
+    }
     return DFTK_OK;
 }
 
@@ -874,6 +883,95 @@ int dftk_jk(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N_PCLASS]
         if ((st = launch_jk_all<double>(P, s))) return st;
     }
     return launch_symmetrize(*shells, Y, Za, Zb, J, K_a, K_b, uhf, s);
+}
+
+int dftk_hl_schwarz(const dftk_shells_t *shells, dftk_pairs_t *pairs, dftk_stream_t stream)
+{
+    if (!shells || !pairs || !pairs->qp || !pairs->q || !pairs->rec64 || !pairs->rec32 || pairs->n_pairs < 0)
+        return fail(DFTK_ERR_ARG, "dftk_hl_schwarz: bad arguments");
+    if (pairs->kmax > HL_MAX_KPAIR) return fail(DFTK_ERR_SIZE, "dftk_hl_schwarz: more than 128 primitive pairs per pair");
+    if (shells->mol) return fail(DFTK_ERR_UNSUPPORTED, "dftk_hl_schwarz: one molecule at a time");
+    DFTK_INIT();
+    if (pairs->n_pairs == 0) return DFTK_OK;
+    k_hl_schwarz<<<(unsigned)pairs->n_pairs, 32, 0, (cudaStream_t)stream>>>(*shells, *pairs);
+    DFTK_LAUNCHED("k_hl_schwarz");
+    return DFTK_OK;
+}
+
+int dftk_jk_hl(const dftk_shells_t *shells, const dftk_hl_t *hl, const double *D, const double *D_a,
+               const double *D_b, double *J, double *K_a, double *K_b, int flags, double tau, void *workspace,
+               size_t workspace_bytes, long long *counts, dftk_stream_t stream)
+{
+    if (!shells || !hl || !D || !D_a || !J || !K_a || !workspace) return fail(DFTK_ERR_ARG, "dftk_jk_hl: null argument");
+    const int uhf = (flags & DFTK_JK_UHF) != 0;
+    if (uhf && (!D_b || !K_b)) return fail(DFTK_ERR_ARG, "dftk_jk_hl: UHF needs D_b and K_b");
+    if (!(tau >= 0.0)) return fail(DFTK_ERR_ARG, "dftk_jk_hl: bad threshold");
+    if (shells->mol) return fail(DFTK_ERR_UNSUPPORTED, "dftk_jk_hl: one molecule at a time");
+    if (hl->n_rows < 0 || hl->n_rows != hl->hi.n_pairs || hl->total[0] < 0 || hl->total[1] < 0 ||
+        ((hl->total[0] > 0 || hl->total[1] > 0) && (!hl->row_off[0] || !hl->row_off[1])))
+        return fail(DFTK_ERR_ARG, "dftk_jk_hl: inconsistent candidate spaces");
+    if (workspace_bytes < ws_bytes(shells->n_shells, shells->n_ao))
+        return fail(DFTK_ERR_WORKSPACE, "dftk_jk_hl: workspace too small");
+    DFTK_INIT();
+    const long long total = hl->total[0] + hl->total[1];
+    if (total == 0 || hl->n_rows == 0) return DFTK_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int N = shells->n_ao;
+    const size_t nn = (size_t)N * N;
+    double *Y = (double *)workspace;
+    double *Za = Y + nn;
+    double *Zb = Za + nn;
+    float *Dsh = (float *)(Zb + nn);
+    DFTK_CUDA(cudaMemsetAsync(Y, 0, 3 * nn * sizeof(double), s));
+    int st;
+    if ((st = launch_dsh(*shells, D, D_a, uhf ? D_b : D_a, uhf, Dsh, s))) return st;
+    HlJkParams P;
+    memset(&P, 0, sizeof(P));
+    P.sh = *shells;
+    P.hi = hl->hi;
+    P.lo = hl->lo;
+    P.n_rows = hl->n_rows;
+    for (int k = 0; k < 2; ++k) {
+        P.total[k] = hl->total[k];
+        P.row_off[k] = hl->row_off[k];
+    }
+    P.tau_prim = (float)hl->tau_prim;
+    P.D = D;
+    P.Da = D_a;
+    P.Db = uhf ? D_b : D_a;
+    P.Y = Y;
+    P.Za = Za;
+    P.Zb = Zb;
+    P.Dsh = Dsh;
+    P.uhf = uhf;
+    P.tau = tau;
+    P.counts = counts;
+    long long blocks = total;
+    const long long cap = (long long)sm_count() * 8;  // 8 one-warp blocks per SM (26.6 KB shared each)
+    if (blocks > cap) blocks = cap;
+    k_hl_jk<<<(unsigned)blocks, 32, 0, s>>>(P);
+    DFTK_LAUNCHED("k_hl_jk");
+    long long bx = ((long long)nn + 255) / 256;
+    if (bx > 148 * 8) bx = 148 * 8;
+    k_symmetrize_add<<<(unsigned)bx, 256, 0, s>>>(N, Y, Za, Zb, J, K_a, K_b, uhf);
+    DFTK_LAUNCHED("k_symmetrize_add");
+    return DFTK_OK;
+}
+
+int dftk_hl_eri_blocks(const dftk_shells_t *shells, const dftk_hl_t *hl, long long n_quartets, const int *desc,
+                       const long long *out_off, double *out, dftk_stream_t stream)
+{
+    if (!shells || !hl || n_quartets < 0 || (n_quartets > 0 && (!desc || !out_off || !out)))
+        return fail(DFTK_ERR_ARG, "dftk_hl_eri_blocks: bad arguments");
+    DFTK_INIT();
+    if (n_quartets == 0) return DFTK_OK;
+    long long blocks = n_quartets;
+    const long long cap = (long long)sm_count() * 8;
+    if (blocks > cap) blocks = cap;
+    k_hl_emit<<<(unsigned)blocks, 32, 0, (cudaStream_t)stream>>>(*shells, hl->hi, hl->lo, n_quartets, desc, out_off,
+                                                                  out);
+    DFTK_LAUNCHED("k_hl_emit");
+    return DFTK_OK;
 }
 
 int dftk_jk_timing(int enable)

@@ -89,7 +89,7 @@ __device__ __forceinline__ double diag_max_all(const dftk_pairs_t &pr, int pair,
     return m;
 }
 
-#define DFTK_MAX_KPAIR 64
+#define DFTK_MAX_KPAIR 128
 
 // Schwarz factors, one thread per pair: Q_ab = sqrt(max |(ab|ab)|) of the
 // contracted pair, and per primitive pair q_k = sqrt(max |(ab_k|ab_k)|); the
@@ -112,7 +112,7 @@ __global__ void k_schwarz(const dftk_pairs_t pr, int nfields)
         qk[k] = k < np ? (float)sqrt(diag_max_all<C>(pr, pair, k, 1)) : 0.0f;
         order[k] = k;
     }
-    // insertion sort, descending q (kmax <= 64)
+    // insertion sort, descending q (kmax <= DFTK_MAX_KPAIR)
     for (int a = 1; a < kk; ++a) {
         const int o = order[a];
         int b = a - 1;

@@ -29,6 +29,7 @@ QCLASS_OF = {(0, 0): 0, (1, 0): 1, (1, 1): 2, (2, 0): 3, (2, 1): 4, (2, 2): 5}
 QCLASS_PAIRS = [(0, 0), (1, 0), (1, 1), (2, 0), (2, 1), (2, 2)]
 QCLASS_NAMES = ["(ss|ss)", "(ps|ss)", "(ps|ps)", "(pp|ss)", "(pp|ps)", "(pp|pp)"]
 PAIR_FIELDS = {0: 6, 1: 10, 2: 13}  # stored record fields per pair class (ERI fields + alpha)
+GENERIC_FIELDS = 13  # the d-shell path's pair sets: every ERI field + alpha
 # Fixed flop accounting per evaluated primitive quartet, by class (ss|ss)..(pp|pp):
 # 2 x (R-recursion FMAs + ket Hermite contraction + bra contraction) + 40 + 3L.
 FLOPS_PER_PRIM_QUARTET = [44, 66, 145, 147, 410, 1402]
@@ -87,17 +88,24 @@ class IntegralEngine:
         _lib.load()
         self.device = _dev(device)
         self.shells = shells
-        self.ns = len(shells)
+        # integral shells: one per contraction row (basis.segments); equal to
+        # the shells unless a shell is generally contracted
+        self.segs = _basis.segments(shells)
+        self.general = len(self.segs) != len(shells)
+        self.ns = len(self.segs)
         self.n_ao = int(shells[-1]["ao_stop"]) if shells else 0
         self.tau_schwarz = float(tau_schwarz)
         self.tau_prim = float(tau_prim)
-        self.l = np.array([s["angular_momentum"] for s in shells], dtype=np.int32)
-        self.nao_sh = np.array([s["n_ao"] for s in shells], dtype=np.int64)
+        self.l = np.array([s["l"] for s in self.segs], dtype=np.int32)
+        self.nao_sh = np.array([s["n_ao"] for s in shells], dtype=np.int64)  # per reference shell
+        self.has_hl = bool((self.l >= 2).any())
         with torch.cuda.device(self.device):
             _lib.call("dftk_init")
             self._upload_shells()
             self._build_pairs()
             self._build_queue()
+            if self.has_hl:
+                self._build_hl()
             nbytes = _lib.load().dftk_jk_workspace_bytes_queue(self.ns, self.n_ao, ctypes.byref(self.c_queue))
             self.workspace = torch.empty(int(nbytes), dtype=torch.uint8, device=self.device)
             self.workspace_bytes = int(nbytes)
@@ -108,20 +116,21 @@ class IntegralEngine:
         return torch.as_tensor(np.ascontiguousarray(arr), dtype=dtype).to(self.device)
 
     def _upload_shells(self):
-        sh = self.shells
-        nprim = np.array([s["n_exponents"] for s in sh], dtype=np.int32)
+        sh = self.segs
+        nprim = np.array([s["exponents"].size for s in sh], dtype=np.int32)
         prim_off = np.concatenate([[0], np.cumsum(nprim)[:-1]]).astype(np.int32)
         exps = np.concatenate([s["exponents"] for s in sh]) if sh else np.zeros(0)
-        # coefficient x primitive normalisation; for s and p shells the norm of
-        # every component is the same, so the first component's values serve.
-        cn = np.concatenate([s["coefficients"][0] * s["normalization"][: s["n_exponents"]] for s in sh]) \
-            if sh else np.zeros(0)
+        # coefficient x radial norm per primitive (for s and p shells this is
+        # normal() itself; d components get their remaining factor in-kernel)
+        cn = np.concatenate([s["cn"] for s in sh]) if sh else np.zeros(0)
         self.kmax = int(max(1, (nprim.max() if sh else 1) ** 2))
         self.d_xyz = self._t(np.array([s["atom_pos"] for s in sh], dtype=np.float64).reshape(-1), torch.float64)
         self.d_l = self._t(self.l, torch.int32)
         self.d_nprim = self._t(nprim, torch.int32)
         self.d_prim_off = self._t(prim_off, torch.int32)
         self.d_ao = self._t(np.array([s["ao_start"] for s in sh], dtype=np.int32), torch.int32)
+        if self.kmax > 128:
+            raise _basis.UnsupportedBasis(f"{int(nprim.max())} primitives in one contraction (at most 11)")
         self.d_exp = self._t(exps.astype(np.float64), torch.float64)
         self.d_cn = self._t(cn.astype(np.float64), torch.float64)
         self.c_shells = _lib.Shells(
@@ -131,7 +140,7 @@ class IntegralEngine:
 
     def _alloc_class(self, pc: int, ab: np.ndarray):
         n = ab.shape[0]
-        nf = PAIR_FIELDS[pc]
+        nf = PAIR_FIELDS.get(pc, GENERIC_FIELDS)
         bufs = {
             "ab": self._t(ab.reshape(-1).astype(np.int32), torch.int32) if n else torch.zeros(2, dtype=torch.int32, device=self.device),
             "nprim": torch.zeros(max(n, 1), dtype=torch.int32, device=self.device),
@@ -153,7 +162,9 @@ class IntegralEngine:
         swap = self.l[ii] < self.l[jj]
         a = np.where(swap, jj, ii)
         b = np.where(swap, ii, jj)
-        pclass = self.l[a] + self.l[b]
+        # s/p pairs by l_a + l_b; pairs with a d shell (class 3) go to _build_hl
+        pclass = np.where(self.l[a] >= 2, 3, self.l[a] + self.l[b])
+        self._pair_a, self._pair_b, self._pair_class = a, b, pclass
         stream = _lib.stream_handle()
         self.pair_bufs, self.c_pairs_list = [], []
         ref_class = np.zeros(ii.size, dtype=np.int32)
@@ -181,6 +192,7 @@ class IntegralEngine:
             self.pair_bufs.append(bufs)
             self.c_pairs_list.append(st)
         self.c_pairs = _lib.PairsArray(*self.c_pairs_list)
+        ref_class[pclass == 3] = 3  # rows of these pairs are set by _build_hl
         # reference pair index i(i+1)/2 + j -> (class, sorted row, stored as (j, i))
         self.ref_pair_class = ref_class
         self.ref_pair_row = ref_row
@@ -203,6 +215,52 @@ class IntegralEngine:
             q.row_off[c] = _lib.ptr(d_off).value
         q.tau_prim = self.tau_prim
         self.c_queue = q
+
+    def _generic_set(self, sel: np.ndarray):
+        """Pairs `sel` (indices into the pair list) in the generic 13-field
+        layout, sorted by descending Schwarz factor: (buffers, struct, q, sel)."""
+        a, b = self._pair_a, self._pair_b
+        stream = _lib.stream_handle()
+        ab = np.stack([a[sel], b[sel]], axis=1)
+        bufs, st = self._alloc_class(_lib.PCLASS_GENERIC, ab)
+        if ab.shape[0] == 0:
+            return bufs, st, np.zeros(0), sel
+        for _ in range(2):  # measure, sort, then build the sorted set
+            _lib.call("dftk_pair_data", ctypes.byref(self.c_shells), _lib.PCLASS_GENERIC, ctypes.byref(st), stream)
+            _lib.call("dftk_hl_schwarz", ctypes.byref(self.c_shells), ctypes.byref(st), stream)
+            q = bufs["q"][: ab.shape[0]].cpu().numpy()
+            if _ == 1:
+                break
+            order = np.argsort(-q, kind="stable")
+            ab, sel = ab[order], sel[order]
+            bufs, st = self._alloc_class(_lib.PCLASS_GENERIC, ab)
+        return bufs, st, q, sel
+
+    def _build_hl(self):
+        """Pair sets and candidate spaces of the quartets with a d shell:
+        rows are the d pairs; kets the s/p pairs ((hi|lo)) or the d pairs up
+        to the row ((hi|hi)), each a Schwarz prefix as in the s/p queue."""
+        pclass = self._pair_class
+        hi_bufs, hi_st, q_hi, sel_hi = self._generic_set(np.nonzero(pclass == 3)[0])
+        lo_bufs, lo_st, q_lo, sel_lo = self._generic_set(np.nonzero(pclass < 3)[0])
+        self.ref_pair_row[sel_hi] = np.arange(sel_hi.size)
+        self.ref_pair_lo_row = np.full(pclass.size, -1, dtype=np.int64)
+        self.ref_pair_lo_row[sel_lo] = np.arange(sel_lo.size)
+        off_lo = candidate_offsets(q_hi, q_lo, False, self.tau_schwarz)
+        off_hi = candidate_offsets(q_hi, q_hi, True, self.tau_schwarz)
+        self.hl_bufs = (hi_bufs, lo_bufs)
+        self.hl_row_off = (self._t(off_lo, torch.int64), self._t(off_hi, torch.int64))
+        self.hl_q = (q_hi, q_lo)
+        self.hl_totals = [int(off_lo[-1]), int(off_hi[-1])]
+        hl = _lib.HlSet()
+        hl.hi = hi_st
+        hl.lo = lo_st
+        hl.n_rows = int(q_hi.size)
+        for k in range(2):
+            hl.total[k] = self.hl_totals[k]
+            hl.row_off[k] = _lib.ptr(self.hl_row_off[k]).value
+        hl.tau_prim = self.tau_prim
+        self.c_hl = hl
 
     # ---------------------------------------------------------------- queries
     def quartet_totals(self) -> List[int]:
@@ -271,12 +329,20 @@ class IntegralEngine:
         else:
             J, Ka, Kb = out
         flags = (_lib.JK_UHF if uhf else 0) | (_lib.JK_MIXED if mixed else 0)
+        if self.has_hl and queue is not None:
+            raise _basis.UnsupportedBasis("jk(queue=...): sharded builds cover s/p bases")
         _lib.call("dftk_jk", ctypes.byref(self.c_shells), self.c_pairs,
                   ctypes.byref(queue if queue is not None else self.c_queue),
                   _lib.ptr(D), _lib.ptr(D_a), _lib.ptr(D_b if uhf else None), _lib.ptr(J), _lib.ptr(Ka),
                   _lib.ptr(Kb if uhf else None), flags, float(tau), float(tau_fp32 if mixed else tau),
                   _lib.ptr(self.workspace), self.base_workspace_bytes if scan else self.workspace_bytes,
                   _lib.ptr(counts), _lib.stream_handle())
+        if self.has_hl:
+            # quartets with a d shell (FP64), added to the s/p part
+            _lib.call("dftk_jk_hl", ctypes.byref(self.c_shells), ctypes.byref(self.c_hl), _lib.ptr(D), _lib.ptr(D_a),
+                      _lib.ptr(D_b if uhf else None), _lib.ptr(J), _lib.ptr(Ka), _lib.ptr(Kb if uhf else None),
+                      _lib.JK_UHF if uhf else 0, float(tau), _lib.ptr(self.workspace), self.workspace_bytes, None,
+                      _lib.stream_handle())
         return J, Ka, (Kb if uhf else Ka)
 
     def _square(self, M) -> torch.Tensor:
@@ -293,9 +359,11 @@ class IntegralEngine:
         from the total density D, spin densities D_a/D_b and energy-weighted density W.
         tau_fp32 > tau selects the mixed form; ``scan`` hands dftk_grad only the
         base workspace (class kernels scan the candidates, FP64 only)."""
+        if self.has_hl:
+            raise _basis.UnsupportedBasis("gradient: the derivative kernels cover s and p shells")
         n_atoms = len(atoms)
         if not hasattr(self, "d_shell_atom"):
-            self.d_shell_atom = self._t(np.array([s["atom_idx"] for s in self.shells], dtype=np.int32), torch.int32)
+            self.d_shell_atom = self._t(np.array([s["atom_idx"] for s in self.segs], dtype=np.int32), torch.int32)
         xyz = torch.as_tensor(np.asarray(centers, dtype=np.float64).reshape(-1), device=self.device)
         z = torch.as_tensor(np.array([float(int(a)) for a in atoms]), dtype=torch.float64, device=self.device)
         g = torch.zeros(3 * n_atoms, dtype=torch.float64, device=self.device)
@@ -341,14 +409,58 @@ class IntegralEngine:
 
     def eri_blocks(self, quads: np.ndarray, fp32: bool = False) -> Tuple[torch.Tensor, np.ndarray]:
         """Contracted ERI blocks of reference quartets, flat in calc_eri layout
-        (fp32=True evaluates with the mixed path's FP32 kernels)."""
-        desc, off = self.quartet_descriptors(quads)
-        if fp32:
-            desc[:, 3] |= 8
-        d_desc = self._t(desc.reshape(-1), torch.int32)
-        d_off = self._t(off[:-1], torch.int64)
+        (fp32=True evaluates the s/p quartets with the mixed path's FP32
+        kernels; quartets with a d shell are always FP64)."""
+        quads = np.asarray(quads, dtype=np.int64).reshape(-1, 4)
+        if self.general:
+            raise _basis.UnsupportedBasis("eri_blocks: generally contracted shells (use jk)")
+        a, b, c, d = quads.T
+        sizes = self.nao_sh[a] * self.nao_sh[b] * self.nao_sh[c] * self.nao_sh[d]
+        off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
         out = torch.zeros(int(off[-1]), dtype=torch.float64, device=self.device)
-        if desc.shape[0]:
+        hi = np.zeros(quads.shape[0], dtype=bool)
+        if self.has_hl and quads.shape[0]:
+            hi = (np.maximum(self.l[a], self.l[b]) >= 2) | (np.maximum(self.l[c], self.l[d]) >= 2)
+        sp = np.nonzero(~hi)[0]
+        if sp.size:
+            desc, _ = self.quartet_descriptors(quads[sp])
+            if fp32:
+                desc[:, 3] |= 8
+            d_desc = self._t(desc.reshape(-1), torch.int32)
+            d_off = self._t(off[:-1][sp], torch.int64)
             _lib.call("dftk_eri_blocks", ctypes.byref(self.c_shells), self.c_pairs, desc.shape[0],
                       _lib.ptr(d_desc), _lib.ptr(d_off), _lib.ptr(out), _lib.stream_handle())
+        hq = np.nonzero(hi)[0]
+        if hq.size:
+            desc = self._hl_descriptors(quads[hq])
+            d_desc = self._t(desc.reshape(-1), torch.int32)
+            d_off = self._t(off[:-1][hq], torch.int64)
+            _lib.call("dftk_hl_eri_blocks", ctypes.byref(self.c_shells), ctypes.byref(self.c_hl), desc.shape[0],
+                      _lib.ptr(d_desc), _lib.ptr(d_off), _lib.ptr(out), _lib.stream_handle())
         return out, off
+
+    def _hl_descriptors(self, quads: np.ndarray) -> np.ndarray:
+        """dftk_hl_eri_blocks descriptors of reference quartets with a d shell:
+        the pair holding a d shell (the first one if both do) is the bra."""
+        a, b, c, d = quads.T
+
+        def pair_info(x, y):
+            i = np.maximum(x, y)
+            j = np.minimum(x, y)
+            idx = i * (i + 1) // 2 + j
+            is_hi = self.ref_pair_class[idx] == 3
+            row = np.where(is_hi, self.ref_pair_row[idx], self.ref_pair_lo_row[idx])
+            first = np.where(self.ref_pair_swap[idx], j, i)
+            return is_hi, row, (first != x).astype(np.int32)
+
+        h1, r1, f1 = pair_info(a, b)
+        h2, r2, f2 = pair_info(c, d)
+        exch = ~h1
+        kind = (h1 & h2).astype(np.int32)
+        rb = np.where(exch, r2, r1)
+        rk = np.where(exch, r1, r2)
+        fb = np.where(exch, f2, f1)
+        fk = np.where(exch, f1, f2)
+        flags = fb | (fk << 1) | (exch.astype(np.int32) << 2)
+        n = self.nao_sh
+        return np.stack([kind, rb, rk, flags, n[a], n[b], n[c], n[d]], axis=1).astype(np.int32)

@@ -4,8 +4,9 @@
   core-Hamiltonian guess, damping from rate 0.4 (divided by 1.1 after four
   strikes), DIIS on FPS - SPF with a 10-deep history once |dE| < 1e-3,
   convergence at |dE| < etol and max|dP| < ptol, then one rebuild with the
-  last density.  The Cartesian-to-spherical transform is the identity for s
-  and p shells (shelled.py:878-920), which are all the kernels take.
+  last density.  With d shells it iterates in the spherical basis of the
+  reference's transform A (shelled.py:878-920, :1071-1074, :1166-1176):
+  S, H and J/K as A M A^T, densities back to Cartesian as A^T P A.
 * :func:`scf_rhf` is the closed-shell driver the benchmarks use: Pulay DIIS
   with 8 vectors, convergence at |dE| < 1e-10 and RMS(dD) < 1e-8, and an
   incremental Fock build F_k = F_{k-1} + G(D_k - D_{k-1}) with optional mixed
@@ -49,6 +50,30 @@ class SCFResult:
     incremental_seconds: float = 0.0  # and their share of fock_seconds
 
 
+def spherical(engine: IntegralEngine, dev) -> Optional[torch.Tensor]:
+    """The reference's Cartesian-to-spherical matrix A (shelled.py:1071) as a
+    device tensor, or None when every shell is s or p (A is the identity)."""
+    if not engine.has_hl:
+        return None
+    from .basis import spherical_transform
+
+    return torch.as_tensor(spherical_transform(engine.shells), dtype=torch.float64, device=dev)
+
+
+def _jk_in(engine: IntegralEngine, A: Optional[torch.Tensor]):
+    """engine.jk on densities of the SCF's basis: with A (spherical basis)
+    P_cart = A^T P A in and A J A^T out (shelled.py:1166-1176)."""
+    if A is None:
+        return engine.jk
+
+    def jk(D, D_a=None, D_b=None, **kw):
+        c = lambda M: None if M is None else (A.T @ M @ A).contiguous()
+        out = engine.jk(c(D), c(D_a), c(D_b), **kw)
+        return tuple(None if M is None else A @ M @ A.T for M in out)
+
+    return jk
+
+
 def orthogonalizer(S: torch.Tensor) -> torch.Tensor:
     """X = U s^{-1/2} U^T (shelled.py:1083-1088)."""
     w, U = torch.linalg.eigh(S)
@@ -66,6 +91,10 @@ def scf_reference(engine: IntegralEngine, H: torch.Tensor, S: torch.Tensor, n_al
     dev = engine.device
     H = H.to(dev, torch.float64)
     S = S.to(dev, torch.float64)
+    A = spherical(engine, dev)
+    if A is not None:  # d shells: the reference iterates in the spherical basis (shelled.py:1071-1074)
+        H, S = A @ H @ A.T, A @ S @ A.T
+    jk = _jk_in(engine, A)
     N = H.shape[0]
     X = orthogonalizer(S)
     _, Cp = torch.linalg.eigh(X.T @ H @ X)
@@ -83,7 +112,7 @@ def scf_reference(engine: IntegralEngine, H: torch.Tensor, S: torch.Tensor, n_al
         nonlocal builds, tb
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
-        J, Ka, Kb = engine.jk(P, Pa, Pb, uhf=True, tau=tau)
+        J, Ka, Kb = jk(P, Pa, Pb, uhf=True, tau=tau)
         torch.cuda.synchronize(dev)
         tb += time.perf_counter() - t0
         builds += 1
@@ -182,6 +211,10 @@ def scf_rhf(engine: IntegralEngine, H: torch.Tensor, S: torch.Tensor, n_occ: int
     dev = engine.device
     H = H.to(dev, torch.float64)
     S = S.to(dev, torch.float64)
+    A = spherical(engine, dev)
+    if A is not None:
+        H, S = A @ H @ A.T, A @ S @ A.T
+    jk = _jk_in(engine, A)
     X = orthogonalizer(S)
     if D_guess is None:
         _, Cp = torch.linalg.eigh(X.T @ H @ X)
@@ -206,12 +239,12 @@ def scf_rhf(engine: IntegralEngine, H: torch.Tensor, S: torch.Tensor, n_occ: int
         t0 = time.perf_counter()
         incremental_build = False
         if full:
-            J, K, _ = engine.jk(2.0 * D, D, tau=min(tau, 1e-14), counts=counts_t)
+            J, K, _ = jk(2.0 * D, D, tau=min(tau, 1e-14), counts=counts_t)
             G = J - K
             since_full = 0
         else:
             dD = D - D_ref
-            J, K, _ = engine.jk(2.0 * dD, dD, mixed=mixed, tau=tau, tau_fp32=tau_fp32, counts=counts_t)
+            J, K, _ = jk(2.0 * dD, dD, mixed=mixed, tau=tau, tau_fp32=tau_fp32, counts=counts_t)
             G = G + (J - K)
             since_full += 1
             incremental_build = True

@@ -15,7 +15,7 @@ this module                             reference (shelled.py)
 ``calc_eri(pair_list, pair_cache, shells)``  :596-700 (returns the arrays; writes the .npy files if asked)
 ``process_eri(...)``                    :702-768
 ``fill_matrices(shells, P, P_a, P_b, J, K_a, K_b)``  :770-877 (integral-direct, in place)
-``independent(shells, sphere_total_ao, C)``  :878-920 (s/p only: identity)
+``independent(shells, sphere_total_ao, C)``  :878-920
 ``UHF_density``, ``init_UHF_density``   :549-574
 ``scf(...)``                            the SCF loop :1079-1293
 =====================================  ====================================================
@@ -242,14 +242,13 @@ def fill_matrices(shells, P, P_a, P_b, J_matrix, K_a, K_b, tau: float = 0.0):
 
 
 def independent(shells, sphere_total_ao, C):
-    """Cartesian-to-spherical row transform (shelled.py:878-920); s and p rows
-    are copied, which is all the kernels produce."""
-    C_new = np.empty((sphere_total_ao, C.shape[1]))
-    for sh in shells:
-        if sh["angular_momentum"] > 1:
-            raise _basis.UnsupportedBasis("spherical transform beyond p is not provided")
-        C_new[sh["sphere_ao_start"]:sh["sphere_ao_stop"], :] = C[sh["ao_start"]:sh["ao_stop"], :]
-    return C_new
+    """Cartesian-to-spherical row transform (shelled.py:878-920): A @ C with
+    the reference's A (s/p rows copied; d and f contractions mapped to their
+    five and seven combinations, basis.spherical_transform)."""
+    A = _basis.spherical_transform(shells)
+    if A.shape[0] != int(sphere_total_ao):
+        raise ValueError(f"sphere_total_ao {sphere_total_ao} != {A.shape[0]}")
+    return A @ np.asarray(C, dtype=np.float64)
 
 
 def init_UHF_density(C_a, C_b, N_a, N_b):

@@ -278,15 +278,56 @@ def full_eri_tensor(shells: List[Dict]) -> np.ndarray:
 
 
 # --------------------------------------------------------------------------- SCF
-def scf_uhf(H: np.ndarray, S: np.ndarray, jk: Callable, n_alpha: int, n_beta: int, e_nn: float,
-            etol: float = 1e-8, ptol: float = 1e-6, max_iter: int = 500, history: int = 10):
-    """The reference's UHF loop (shelled.py:1079-1293), A = identity (s/p shells).
+def spherical_transform(shells: List[Dict]) -> np.ndarray:
+    """The reference's A = independent(shells, sphere_total_ao, I)
+    (shelled.py:878-920, :1071), restated row by row for s, p and d."""
+    n_cart = sum(int(s["n_ao"]) for s in shells)
+    n_sph = sum(int(s["n_contractions"]) * (2 * int(s["angular_momentum"]) + 1) for s in shells)
+    A = np.zeros((n_sph, n_cart))
+    r = 0
+    for sh in shells:
+        l, c0 = int(sh["angular_momentum"]), int(sh["ao_start"])
+        for k in range(int(sh["n_contractions"])):
+            c = c0 + k * int(sh["n_components"])
+            if l <= 1:
+                for m in range(2 * l + 1):
+                    A[r + m, c + m] = 1.0
+            elif l == 2:
+                A[r, c + 1] = 1.0
+                A[r + 1, c + 3] = 1.0
+                A[r + 2, c + 4] = 1.0
+                A[r + 3, c] = np.sqrt(3) / 2
+                A[r + 3, c + 2] = -np.sqrt(3) / 2
+                A[r + 4, c + 5] = 1.0
+                A[r + 4, c] = -0.5
+                A[r + 4, c + 2] = -0.5
+            else:
+                raise ValueError("oracle spherical transform: s, p and d")
+            r += 2 * l + 1
+    return A
 
+
+def scf_uhf(H: np.ndarray, S: np.ndarray, jk: Callable, n_alpha: int, n_beta: int, e_nn: float,
+            etol: float = 1e-8, ptol: float = 1e-6, max_iter: int = 500, history: int = 10,
+            A: np.ndarray = None):
+    """The reference's UHF loop (shelled.py:1079-1293).
+
+    With A (d shells) the loop runs in the spherical basis as the reference's
+    does: S, H, J and K as A M A^T and the densities handed to jk as A^T P A
+    (shelled.py:1071-1074, :1166-1176); without it A is the identity.
     Core-H guess, damping from rate 0.4 (divided by 1.1 after 4 strikes),
     DIIS on the commutator FPS - SPF once |dE| < 1e-3, convergence at
     |dE| < etol and max|dP| < ptol, then one rebuild with the last density.
     Returns a dict with the energy, densities and iteration count.
     """
+    if A is not None:
+        H, S = A @ H @ A.T, A @ S @ A.T
+        jk_cart = jk
+
+        def jk(P, Pa, Pb):
+            out = jk_cart(A.T @ P @ A, A.T @ Pa @ A, A.T @ Pb @ A)
+            return tuple(A @ M @ A.T for M in out)
+
     w, U = np.linalg.eigh(S)
     X = U @ np.diag(w ** -0.5) @ U.T
     _, Cp = np.linalg.eigh(X.T @ H @ X)

@@ -24,6 +24,8 @@ Usage::
     python tests/golden/make_golden.py c10h22         # ~10-15 min
     python tests/golden/make_golden.py h2o64          # ~2 min (pair setup + sampled quartets)
     python tests/golden/make_golden.py grid           # seconds (H2O SCF + evaluation script)
+    python tests/golden/make_golden.py br2            # d shells (STO-3G Br2)
+    python tests/golden/make_golden.py gc             # general contractions + d (H2O, test basis)
 """
 from __future__ import annotations
 
@@ -139,7 +141,7 @@ def patched_shelled(etol=None, ptol=None, stop_before_eri=False):
     return text
 
 
-def run_reference(atoms, centers, mult=1, etol=None, ptol=None, stop_before_eri=False):
+def run_reference(atoms, centers, mult=1, etol=None, ptol=None, stop_before_eri=False, basis_path=None):
     """Execute the patched reference script; return (namespace, workdir)."""
     text = patched_shelled(etol, ptol, stop_before_eri)
     work = tempfile.mkdtemp(prefix="dft_ref_")
@@ -147,7 +149,7 @@ def run_reference(atoms, centers, mult=1, etol=None, ptol=None, stop_before_eri=
     os.makedirs(os.path.join(work, "eval_checkpoints"))
     ns = {
         "__name__": "shelled_reference_run",
-        "__BASIS_PATH__": os.path.join(REFERENCE, "STO-3G.json"),
+        "__BASIS_PATH__": basis_path or os.path.join(REFERENCE, "STO-3G.json"),
         "__ATOMS__": list(atoms),
         "__CENTERS__": [[float(x) for x in c] for c in centers],
         "__MULT__": mult,
@@ -258,6 +260,39 @@ def case_h2o64(out_dir, n_subsets=12, subset_pairs=24, seed=1234):
     print("h2o64 sampled quartets", len(all_quads), "values", res["sample_values"].shape)
 
 
+BR2 = (["35", "35"], np.array([[0.0, 0.0, 0.0], [0.2, -0.3, 4.29]]))
+
+
+def case_dshell(out_dir):
+    """Br2 with the reference's STO-3G (3d shells on both atoms): every
+    processed ERI, the spherical-basis S/T/V, the converged densities, J/K
+    and the energy at tightened thresholds."""
+    atoms, centers = BR2
+    ns, work = run_reference(atoms, centers, etol=1e-11, ptol=1e-8)
+    res = {"atoms": np.array(atoms), "centers": centers, "energy": float(ns["E_total_new"]),
+           "iterations": int(ns["count"]), "E_NN": float(ns["E_NN"])}
+    for k in ("overlaps", "T_matrix", "V_matrix", "P_a", "P_b", "J_matrix", "K_a", "K_b", "A"):
+        res[k] = np.asarray(ns[k], dtype=np.float64)
+    res.update(_load_processed(work))
+    np.savez_compressed(os.path.join(out_dir, "br2.npz"), **res)
+    print("br2 energy", res["energy"], "iters", res["iterations"], "eri values", res["processed_eri_values"].shape)
+
+
+def case_gc(out_dir):
+    """H2O with the generally contracted, d-polarised test basis
+    (tests/golden/dz_gc_test.json): spherical-basis S/T/V, densities, J/K and
+    the energy at tightened thresholds."""
+    atoms, centers = geometry.water()
+    ns, work = run_reference(atoms, centers, etol=1e-11, ptol=1e-8,
+                             basis_path=os.path.join(HERE, "dz_gc_test.json"))
+    res = {"atoms": np.array(atoms), "centers": centers, "energy": float(ns["E_total_new"]),
+           "iterations": int(ns["count"]), "E_NN": float(ns["E_NN"])}
+    for k in ("overlaps", "T_matrix", "V_matrix", "P_a", "P_b", "J_matrix", "K_a", "K_b", "A"):
+        res[k] = np.asarray(ns[k], dtype=np.float64)
+    np.savez_compressed(os.path.join(out_dir, "h2o_gc.npz"), **res)
+    print("h2o gc energy", res["energy"], "iters", res["iterations"], "n_sph", res["overlaps"].shape)
+
+
 def patched_eval(spacing=0.15, chunk=500):
     """The reference's evaluation script with the H2O checkpoint the reference
     SCF just wrote, a coarser grid whose x range is widened by 1 bohr each way
@@ -305,11 +340,12 @@ def case_grid(out_dir):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["h2o", "c10h22", "h2o64", "grid"])
+    ap.add_argument("case", choices=["h2o", "c10h22", "h2o64", "grid", "br2", "gc"])
     ap.add_argument("--out", default=HERE)
     args = ap.parse_args()
     install_fake_cupy()
-    {"h2o": case_h2o, "c10h22": case_c10h22, "h2o64": case_h2o64, "grid": case_grid}[args.case](args.out)
+    {"h2o": case_h2o, "c10h22": case_c10h22, "h2o64": case_h2o64, "grid": case_grid, "br2": case_dshell,
+     "gc": case_gc}[args.case](args.out)
 
 
 if __name__ == "__main__":

@@ -1,0 +1,144 @@
+"""d shells and general contractions on the GPU against the reference's own
+outputs (tests/golden/make_golden.py br2 / gc) and the oracle.
+
+* Br2 / STO-3G (3d shells on both atoms): every processed ERI at 1e-12
+  absolute, S/T/V in the reference's spherical basis, J/K at the reference's
+  converged densities, and the SCF energy of the reference loop at 1e-8 Eh.
+* H2O with a generally contracted, d-polarised test basis: S/T/V, J/K and
+  the energy (reference loop and the RHF/DIIS driver) at 1e-8 Eh.
+* J/K with random densities against the oracle's direct J/K (1e-11).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import GOLDEN, load_golden
+from dft_b200 import basis, geometry, shelled
+from dft_b200.engine import IntegralEngine
+from dft_b200.scf import scf_reference, scf_rhf
+
+pytestmark = pytest.mark.gpu
+
+ERI_TOL = 1e-12
+GC_BASIS = os.path.join(GOLDEN, "dz_gc_test.json")
+
+
+def _mol(g):
+    return [str(a) for a in g["atoms"]], np.asarray(g["centers"])
+
+
+def _gc_basis():
+    with open(GC_BASIS) as fh:
+        return json.load(fh)
+
+
+def _sph(A, M):
+    return A @ M @ A.T
+
+
+def test_br2_all_eris_match_reference(tmp_path):
+    g = load_golden("br2.npz")
+    atoms, centers = _mol(g)
+    sh = basis.build_shells(basis.load_basis(), atoms, centers)
+    pair_list, pair_cache = shelled.pair_data(sh, atoms, centers)
+    eri = shelled.calc_eri(pair_list, pair_cache, sh, out_dir=str(tmp_path))
+    np.testing.assert_array_equal(eri["eri_quads"], g["eri_quads"])
+    np.testing.assert_array_equal(eri["eri_indices"], g["eri_indices"])
+    proc = shelled.process_eri(out_dir=str(tmp_path))
+    np.testing.assert_array_equal(proc["processed_eri_quads"], g["processed_eri_quads"])
+    err = np.abs(proc["processed_eri_values"] - g["processed_eri_values"])
+    assert err.max() < ERI_TOL, err.max()
+
+
+@pytest.mark.parametrize("case", ["br2", "gc"])
+def test_one_electron_spherical_match_reference(case):
+    g = load_golden("br2.npz" if case == "br2" else "h2o_gc.npz")
+    atoms, centers = _mol(g)
+    data = basis.load_basis() if case == "br2" else _gc_basis()
+    sh = basis.build_shells(data, atoms, centers)
+    A = basis.spherical_transform(sh)
+    np.testing.assert_allclose(A, g["A"], atol=1e-15, rtol=0)
+    S, T, V = shelled.one_electron(sh, atoms, centers)
+    for M, key in ((S, "overlaps"), (T, "T_matrix"), (V, "V_matrix")):
+        ref = g[key]
+        err = np.abs(_sph(A, M.cpu().numpy()) - ref).max()
+        assert err < 1e-12 * max(1.0, np.abs(ref).max()), (key, err)
+
+
+@pytest.mark.parametrize("case", ["br2", "gc"])
+def test_jk_at_reference_density(case):
+    """fill_matrices at the reference's converged densities (UHF call shape),
+    compared in the reference's spherical basis."""
+    g = load_golden("br2.npz" if case == "br2" else "h2o_gc.npz")
+    atoms, centers = _mol(g)
+    data = basis.load_basis() if case == "br2" else _gc_basis()
+    sh = basis.build_shells(data, atoms, centers)
+    A = g["A"]
+    Pa_c, Pb_c = A.T @ g["P_a"] @ A, A.T @ g["P_b"] @ A
+    N = A.shape[1]
+    J, Ka, Kb = np.zeros((N, N)), np.zeros((N, N)), np.zeros((N, N))
+    shelled.fill_matrices(sh, Pa_c + Pb_c, Pa_c, Pb_c.copy(), J, Ka, Kb)
+    for M, key in ((J, "J_matrix"), (Ka, "K_a"), (Kb, "K_b")):
+        ref = g[key]
+        err = np.abs(_sph(A, M) - ref).max()
+        assert err < 1e-11 * max(1.0, np.abs(ref).max()), (key, err)
+
+
+@pytest.mark.parametrize("case", ["br2", "gc"])
+def test_scf_energy_matches_reference(case):
+    g = load_golden("br2.npz" if case == "br2" else "h2o_gc.npz")
+    atoms, centers = _mol(g)
+    data = basis.load_basis() if case == "br2" else _gc_basis()
+    sh = basis.build_shells(data, atoms, centers)
+    eng = IntegralEngine(sh, tau_schwarz=0.0)
+    S, T, V = eng.one_electron(atoms, centers)
+    n = basis.n_electrons(atoms)
+    e_nn = geometry.nuclear_repulsion(atoms, centers)
+    r = scf_reference(eng, T + V, S, n // 2, n // 2, e_nn, etol=1e-11, ptol=1e-8)
+    assert abs(r.energy - g["energy"]) < 1e-8, (r.energy, g["energy"])
+    r2 = scf_rhf(eng, T + V, S, n // 2, e_nn, tau=1e-13)
+    assert abs(r2.energy - g["energy"]) < 1e-8, (r2.energy, g["energy"])
+
+
+@pytest.mark.parametrize("case", ["br2", "gc"])
+def test_jk_random_density_vs_oracle(oracle_mod, case):
+    """Every quartet, UHF densities with no structure: the d path and the
+    segmented general contractions against the oracle's direct J/K."""
+    if case == "br2":
+        atoms, centers = ["35", "1"], np.array([[0.0, 0.0, 0.0], [0.3, 0.1, 2.7]])
+        data = basis.load_basis()
+    else:
+        atoms, centers = geometry.water()
+        data = _gc_basis()
+    sh = basis.build_shells(data, atoms, centers)
+    eng = IntegralEngine(sh, tau_schwarz=0.0)
+    N = eng.n_ao
+    rng = np.random.default_rng(7)
+    M1, M2 = rng.normal(size=(N, N)), rng.normal(size=(N, N))
+    Pa, Pb = 0.1 * (M1 + M1.T), 0.1 * (M2 + M2.T)
+    dev = eng.device
+    J, Ka, Kb = eng.jk(torch.as_tensor(Pa + Pb, device=dev), torch.as_tensor(Pa, device=dev),
+                       torch.as_tensor(Pb, device=dev), uhf=True, tau=0.0)
+    osh = oracle_mod.build_shells(data, atoms, centers)
+    q = oracle_mod.quartet_list(len(osh))
+    J0, Ka0, Kb0 = oracle_mod.direct_jk(osh, q, Pa + Pb, Pa, Pb)
+    for M, M0 in ((J, J0), (Ka, Ka0), (Kb, Kb0)):
+        err = np.abs(M.cpu().numpy() - M0).max()
+        assert err < 1e-11 * max(1.0, np.abs(M0).max()), err
+
+
+def test_br2_eri_blocks_vs_oracle(oracle_mod):
+    """HBr quartets through dftk_hl_eri_blocks / dftk_eri_blocks against the
+    oracle's contracted blocks, every quartet."""
+    atoms, centers = ["35", "1"], np.array([[0.0, 0.0, 0.0], [0.3, 0.1, 2.7]])
+    sh = basis.build_shells(basis.load_basis(), atoms, centers)
+    eng = IntegralEngine(sh, tau_schwarz=0.0)
+    q = shelled.quartet_list([(i, j) for i in range(len(sh)) for j in range(i + 1)])
+    vals, off = eng.eri_blocks(q)
+    osh = oracle_mod.build_shells(basis.load_basis(), atoms, centers)
+    v0, off0 = oracle_mod.eri_quartets(osh, q)
+    np.testing.assert_array_equal(off, off0)
+    assert np.abs(vals.cpu().numpy() - v0).max() < ERI_TOL

@@ -40,8 +40,12 @@ def test_combinations_order():
 
 def test_unsupported_basis_is_rejected():
     shells = basis.build_shells(basis.load_basis(), ["21"], np.zeros((1, 3)))  # Sc has d shells
+    basis.check_supported(shells)  # d shells are covered
     with pytest.raises(basis.UnsupportedBasis):
-        basis.check_supported(shells)
+        basis.check_sp(shells, "batch")  # the s/p-only paths refuse them
+    f_basis = {"1": [[[3], [1.0], [[1.0]]]]}
+    with pytest.raises(basis.UnsupportedBasis):
+        basis.check_supported(basis.build_shells(f_basis, ["1"], np.zeros((1, 3))))
 
 
 def test_geometry_alkane():

@@ -190,3 +190,83 @@ def test_pair_and_eri_prims_match_reference_kernels(oracle_mod):
         ref.ref_run_eri_kernel(ctypes.c_longlong(K * K), ctypes.c_int(K), *pair, ctypes.c_int(K), *pair, _p(o_ref))
         lib.orc_eri_prims(ctypes.c_int(K), *pair, ctypes.c_int(K), *pair, _p(o_orc))
         np.testing.assert_allclose(o_orc, o_ref, atol=1e-13, rtol=1e-12)
+
+
+# ------------------------------------------------------- d shells, contractions
+def _gc_path():
+    import os
+
+    from conftest import GOLDEN
+
+    return os.path.join(GOLDEN, "dz_gc_test.json")
+
+
+def test_br2_eris_and_energy(oracle_mod):
+    """Br2 / STO-3G (3d shells on both atoms): every processed ERI, the
+    spherical transform and the reference loop's energy in its spherical basis."""
+    from conftest import load_golden
+
+    g = load_golden("br2.npz")
+    atoms, centers = [str(a) for a in g["atoms"]], g["centers"]
+    sh = _shells(oracle_mod, atoms, centers)
+    q = oracle_mod.quartet_list(len(sh))
+    assert (q == g["eri_quads"]).all()
+    vals, off = oracle_mod.eri_quartets(sh, q)
+    order = oracle_mod.process_order(sh, q)
+    assert (q[order] == g["processed_eri_quads"]).all()
+    pv = np.concatenate([vals[off[i]:off[i + 1]] for i in order])
+    np.testing.assert_allclose(pv, g["processed_eri_values"], atol=1e-13, rtol=0)
+    A = oracle_mod.spherical_transform(sh)
+    np.testing.assert_allclose(A, g["A"], atol=1e-15, rtol=0)
+    S, T, V = oracle_mod.one_electron(sh, atoms, centers)
+    for M, key in ((S, "overlaps"), (T, "T_matrix"), (V, "V_matrix")):
+        assert np.abs(A @ M @ A.T - g[key]).max() < 1e-12 * max(1.0, np.abs(g[key]).max()), key
+    na, nb = oracle_mod.electron_counts(atoms)
+    jk = lambda P, Pa, Pb: oracle_mod.fill_matrices(sh, q, vals, off, P, Pa, Pb)
+    r = oracle_mod.scf_uhf(T + V, S, jk, na, nb, geometry.nuclear_repulsion(atoms, centers), etol=1e-11,
+                           ptol=1e-8, A=A)
+    assert abs(r["energy"] - g["energy"]) < 1e-8
+
+
+def test_general_contraction_energy(oracle_mod):
+    """H2O with the generally contracted, d-polarised test basis: the oracle's
+    contraction-matrix integrals reproduce the reference's spherical S/T/V and
+    its SCF energy."""
+    from conftest import load_golden
+
+    g = load_golden("h2o_gc.npz")
+    atoms, centers = [str(a) for a in g["atoms"]], g["centers"]
+    sh = oracle_mod.build_shells(oracle_mod.load_basis(_gc_path()), atoms, centers)
+    A = oracle_mod.spherical_transform(sh)
+    np.testing.assert_allclose(A, g["A"], atol=1e-15, rtol=0)
+    S, T, V = oracle_mod.one_electron(sh, atoms, centers)
+    for M, key in ((S, "overlaps"), (T, "T_matrix"), (V, "V_matrix")):
+        assert np.abs(A @ M @ A.T - g[key]).max() < 1e-12 * max(1.0, np.abs(g[key]).max()), key
+    q = oracle_mod.quartet_list(len(sh))
+    na, nb = oracle_mod.electron_counts(atoms)
+    jk = lambda P, Pa, Pb: oracle_mod.direct_jk(sh, q, P, Pa, Pb)
+    r = oracle_mod.scf_uhf(T + V, S, jk, na, nb, geometry.nuclear_repulsion(atoms, centers), etol=1e-11,
+                           ptol=1e-8, A=A)
+    assert abs(r["energy"] - g["energy"]) < 1e-8
+
+
+def test_segments_and_spherical_transform_host():
+    """Host side of the d path: segments cover every AO row of a generally
+    contracted shell once, and basis.spherical_transform is the reference's A."""
+    import json
+
+    from conftest import load_golden
+    from dft_b200 import basis
+
+    g = load_golden("h2o_gc.npz")
+    with open(_gc_path()) as fh:
+        data = json.load(fh)
+    sh = basis.build_shells(data, [str(a) for a in g["atoms"]], g["centers"])
+    segs = basis.segments(sh)
+    rows = np.concatenate([np.arange(s["ao_start"], s["ao_start"] + s["n_ao"]) for s in segs])
+    assert np.array_equal(np.sort(rows), np.arange(sh[-1]["ao_stop"]))
+    assert len(segs) > len(sh)
+    np.testing.assert_allclose(basis.spherical_transform(sh), g["A"], atol=1e-15, rtol=0)
+    b = load_golden("br2.npz")
+    shb = basis.build_shells(basis.load_basis(), [str(a) for a in b["atoms"]], b["centers"])
+    np.testing.assert_allclose(basis.spherical_transform(shb), b["A"], atol=1e-15, rtol=0)
