@@ -669,7 +669,7 @@ def run_dftk_arm(args, rank, world, local_rank):
                                 device_id=torch.device("cuda", local_rank))
     from dft_b200 import _lib, shelled
     from dft_b200.engine import FLOPS_PER_PRIM_QUARTET, QCLASS_NAMES
-    from dft_b200.scf import scf_rhf
+    from dft_b200.scf import fp32_threshold, scf_rhf
 
     atoms, centers, shells, eng, S, H, enn, nocc = setup_workload(torch)
     # converged FP64 SCF (setup, untimed) gives the density of the timed builds
@@ -828,10 +828,14 @@ def run_dftk_arm(args, rank, world, local_rank):
                          "whole_build_tflops_81_prims_per_quartet": full_prim_flops / (ms_per_step / 1e3) / 1e12,
                          "class_ms": {QCLASS_NAMES[c]: float(class_ms[c]) for c in range(6)},
                          "fp32_peak_tflops": fp32_peak, "hbm_peak_gbs": peaks.get("hbm_gbs")},
-            "mixed": {"plain_fp64_builds_per_s": plain_rate,
+            "mixed": {"speedup_mixed_vs_fp64_incremental": imx / i64,
+                      "comparison": "like for like: the incremental (D - D_prev) builds of the same SCF, "
+                                    "FP64 against mixed; same screening, only the precision differs",
+                      "tau_fp32": fp32_threshold(sum(eng.quartet_totals())),
+                      "tau_fp32_rule": "1 uEh budget / (2^-20 sqrt(Schwarz candidates)), clamped to [1e-6, 1e-4]",
+                      "plain_fp64_builds_per_s": plain_rate,
                       "fp64_incremental_builds_per_s": i64, "mixed_incremental_builds_per_s": imx,
                       "speedup_mixed_vs_plain_fp64": imx / plain_rate,
-                      "speedup_mixed_vs_fp64_incremental": imx / i64,
                       "incremental_builds": [r64.incremental_builds, rmx.incremental_builds],
                       "scf_builds_per_s_fp64": b64, "scf_builds_per_s_mixed": bmx,
                       "scf_speedup": bmx / b64, "scf_iterations_fp64": r64.iterations,

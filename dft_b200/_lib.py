@@ -79,6 +79,8 @@ class Pairs(ctypes.Structure):
         ("rec32", ctypes.c_void_p),
         ("q", ctypes.c_void_p),
         ("qp", ctypes.c_void_p),
+        ("core64", ctypes.c_void_p),
+        ("core32", ctypes.c_void_p),
     ]
 
 

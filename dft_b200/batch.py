@@ -99,6 +99,9 @@ class BatchEngine(IntegralEngine):
         self.mol_dsh = _prefix(self.mol_ns ** 2)
         self.mat_elems = int((self.mol_nao ** 2).sum())
         self.shells = [s for sh in per for s in sh]
+        self.segs = _basis.segments(self.shells)  # s/p shells, one contraction each: one segment per shell
+        self.general = False
+        self.has_hl = False
         self.shell_mol = np.repeat(np.arange(self.n_mol), self.mol_ns)
         self.shell_atom = np.array([s["atom_idx"] for s in self.shells], dtype=np.int64) + \
             self.mol_atom0[self.shell_mol]

@@ -59,6 +59,22 @@ __device__ __forceinline__ void ldg_v8f(const float *p, float (&v)[8])
         : "l"(p));
 }
 
+// One packed core record of a primitive pair (P x/y/z, p, K, q, 1/(2p), 0):
+// 64 bytes in FP64 (two 256-bit loads), 32 bytes in FP32 (one).
+__device__ __forceinline__ void core_ld(const double *p, double &a, double &b, double &c, double &d, double &e,
+                                        double &f, double &g, double &h)
+{
+    ldg_v4d(p, a, b, c, d);
+    ldg_v4d(p + 4, e, f, g, h);
+}
+__device__ __forceinline__ void core_ld(const float *p, float &a, float &b, float &c, float &d, float &e, float &f,
+                                        float &g, float &h)
+{
+    float v[8];
+    ldg_v8f(p, v);
+    a = v[0]; b = v[1]; c = v[2]; d = v[3]; e = v[4]; f = v[5]; g = v[6]; h = v[7];
+}
+
 template <typename T, int L> struct Boys;
 
 template <int L> struct Boys<double, L> {

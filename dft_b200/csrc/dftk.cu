@@ -500,6 +500,7 @@ int dftk_schwarz(const dftk_shells_t *shells, int pair_class, dftk_pairs_t *pair
     cudaStream_t s = (cudaStream_t)stream;
     if (pairs->kmax > DFTK_MAX_KPAIR) return fail(DFTK_ERR_SIZE, "dftk_schwarz: more than 128 primitive pairs per pair");
     if (!pairs->qp) return fail(DFTK_ERR_ARG, "dftk_schwarz: null qp");
+    if (!pairs->core64 || !pairs->core32) return fail(DFTK_ERR_ARG, "dftk_schwarz: null core records");
     const int nf = pair_fields(pair_class);
     if (pair_class == 0) k_schwarz<0><<<blocks_for(n, 64), 64, 0, s>>>(*pairs, nf);
     else if (pair_class == 1) k_schwarz<1><<<blocks_for(n, 64), 64, 0, s>>>(*pairs, nf);
@@ -519,7 +520,8 @@ struct PreparePlan {
     int kmax = 1;
     std::vector<int> ab[DFTK_N_PCLASS];
     size_t off_ab[DFTK_N_PCLASS], off_np[DFTK_N_PCLASS], off_r64[DFTK_N_PCLASS], off_r32[DFTK_N_PCLASS],
-        off_q[DFTK_N_PCLASS], off_qp[DFTK_N_PCLASS], off_row[DFTK_N_QCLASS];
+        off_q[DFTK_N_PCLASS], off_qp[DFTK_N_PCLASS], off_c64[DFTK_N_PCLASS], off_c32[DFTK_N_PCLASS],
+        off_row[DFTK_N_QCLASS];
     size_t bytes = 0;
 };
 
@@ -565,6 +567,8 @@ int prepare_plan(const dftk_shells_t *shells, PreparePlan &pl)
         pl.off_r32[pc] = carve(at, sizeof(float) * std::max<size_t>(rec, 1));
         pl.off_q[pc] = carve(at, sizeof(double) * std::max<size_t>(n, 1));
         pl.off_qp[pc] = carve(at, sizeof(float) * std::max<size_t>((size_t)pl.kmax * n, 1));
+        pl.off_c64[pc] = carve(at, sizeof(double) * 8 * std::max<size_t>((size_t)pl.kmax * n, 1));
+        pl.off_c32[pc] = carve(at, sizeof(float) * 8 * std::max<size_t>((size_t)pl.kmax * n, 1));
     }
     for (int c = 0; c < DFTK_N_QCLASS; ++c) pl.off_row[c] = carve(at, sizeof(long long) * (pl.ab[kQX[c]].size() / 2 + 1));
     pl.bytes = at;
@@ -616,6 +620,8 @@ int dftk_prepare(const dftk_shells_t *shells, double tau_schwarz, double tau_pri
         P.rec32 = (float *)(base + pl.off_r32[pc]);
         P.q = (double *)(base + pl.off_q[pc]);
         P.qp = (float *)(base + pl.off_qp[pc]);
+        P.core64 = (double *)(base + pl.off_c64[pc]);
+        P.core32 = (float *)(base + pl.off_c32[pc]);
         if (n == 0) continue;
         // Schwarz factors in enumeration order, then the pairs sorted by
         // descending factor (stable) and their records rebuilt in that order
@@ -747,10 +753,14 @@ int dftk_eri_blocks(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N
     P.shell_ao = shells->ao;
     P.shell_l = shells->l;
     for (int k = 0; k < 3; ++k) {
+        if (pairs[k].n_pairs > 0 && (!pairs[k].core64 || !pairs[k].core32))
+            return fail(DFTK_ERR_ARG, "dftk_eri_blocks: pair class without core records");
         P.ab[k] = pairs[k].ab;
         P.np[k] = pairs[k].nprim;
         P.rec64[k] = pairs[k].rec64;
         P.rec32[k] = pairs[k].rec32;
+        P.core64[k] = pairs[k].core64;
+        P.core32[k] = pairs[k].core32;
         P.qp[k] = pairs[k].qp;
         P.n_pairs[k] = pairs[k].n_pairs;
         P.kmax[k] = pairs[k].kmax;
@@ -814,10 +824,14 @@ int dftk_jk(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N_PCLASS]
     P.mol_active = queue->mol_active;
     P.shell_ao = shells->ao;
     for (int k = 0; k < 3; ++k) {
+        if (pairs[k].n_pairs > 0 && (!pairs[k].core64 || !pairs[k].core32))
+            return fail(DFTK_ERR_ARG, "dftk_jk: pair class without core records");
         P.ab[k] = pairs[k].ab;
         P.np[k] = pairs[k].nprim;
         P.rec64[k] = pairs[k].rec64;
         P.rec32[k] = pairs[k].rec32;
+        P.core64[k] = pairs[k].core64;
+        P.core32[k] = pairs[k].core32;
         P.q[k] = pairs[k].q;
         P.qp[k] = pairs[k].qp;
         P.n_pairs[k] = pairs[k].n_pairs;

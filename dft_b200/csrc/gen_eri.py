@@ -187,6 +187,42 @@ def prefetched_inner_loop(side, pc, var, idx, n, qo, other_q):
     return out
 
 
+CORE_NAMES = ["Px", "Py", "Pz", "p", "K", "qd", "h", "zz"]  # packed core record slots
+
+
+def core_inner_loop(side, pc, var, idx, n, qo, prefetch):
+    """Head of an inner primitive loop that reads each primitive pair's packed
+    core record (P, p, K, q, 1/(2p): one 64-byte FP64 or 32-byte FP32 record,
+    core_ld) and the remaining transform fields (PA, PB) from the SoA
+    records; with `prefetch` the next core record is loaded one iteration
+    ahead."""
+    names = [f"{side}{nm}" for nm in CORE_NAMES]
+    nxt = [f"{side}n{k}" for k in range(8)]
+    out = []
+    if prefetch:
+        out.append("T " + ", ".join(nxt) + ";")
+        out.append(f"core_ld({var}_c, {', '.join(nxt)});")
+        out.append("#pragma unroll 1")
+        out.append(f"for (int {idx} = 0; {idx} < {n}; ++{idx}) {{")
+        out.append("  const T " + ", ".join(f"{a} = {b}" for a, b in zip(names, nxt)) + ";")
+        out.append(f"  if ({qo} * (float){side}qd < eps) break;")
+        out.append(f"  const int {idx}n = {idx} + 1 < {n} ? {idx} + 1 : {idx};")
+        out.append(f"  core_ld({var}_c + {idx}n * {var}_cst, {', '.join(nxt)});")
+    else:
+        out.append("#pragma unroll 1")
+        out.append(f"for (int {idx} = 0; {idx} < {n}; ++{idx}) {{")
+        out.append("  T " + ", ".join(names) + ";")
+        out.append(f"  core_ld({var}_c + {idx} * {var}_cst, {', '.join(names)});")
+        out.append(f"  if ({qo} * (float){side}qd < eps) break;")
+    extra = {0: [], 1: [6, 7, 8], 2: [6, 7, 8, 9, 10, 11]}[pc]
+    if extra:
+        fn = ["Px", "Py", "Pz", "p", "K", "h", "Ax", "Ay", "Az", "Bx", "By", "Bz"]
+        out.append(f"  const T* __restrict__ {side}rec = {var}_p + {idx} * {var}_st;")
+        for f in extra:
+            out.append(f"  const T {side}{fn[f]} = __ldg({side}rec + {f} * {var}_fs);")
+    return out
+
+
 def side_pre(side, pc):
     lines = []
     if pc == 2:
@@ -197,21 +233,34 @@ def side_pre(side, pc):
     return lines
 
 
-def inner_loop_variants(cid, pf_loop, plain_loop, plain_loads, inner_pre, inner):
-    """The inner primitive loop (indented into the outer loop's body): the
-    prefetching form, the plain form, or both behind an FP32/FP64 switch."""
-    def form(pf):
-        head = pf_loop if pf else plain_loop
-        pre = [] if pf else ["  " + x for x in plain_loads]
-        return head + pre + ["  ++evaluated;"] + ["  " + x for x in inner_pre + inner] + ["}"]
+def inner_loop_variants(cid, side, pc, var, idx, n, qo, inner_pre, inner, uniform):
+    """The inner primitive loop (indented into the outer loop's body), FP32
+    and FP64 forms behind a switch.  FP32 reads the packed core records; FP64
+    reads them where the inner side is the warp-uniform one (`uniform`: two
+    broadcast vector loads instead of six) and keeps the SoA fields where
+    every lane reads its own pair (64-byte records per lane cost more L1
+    wavefronts than five coalesced 8-byte fields: measured on B200, (ps|ss)
+    9.1 -> 10.8 ms and (pp|ss) 1.7 -> 2.1 ms per (H2O)_64 build)."""
+    q = f"{var}_qp"
 
-    if cid in PREFETCH_CLASSES:
-        lines = form(True)
-    elif cid in PREFETCH_FP32_CLASSES:
-        lines = ["if constexpr (sizeof(T) == 4) {"] + ["  " + x for x in form(True)] + ["} else {"]
-        lines += ["  " + x for x in form(False)] + ["}"]
-    else:
-        lines = form(False)
+    def core_form(pf):
+        head = core_inner_loop(side, pc, var, idx, n, qo, pf)
+        return head + ["  ++evaluated;"] + ["  " + x for x in inner_pre + inner] + ["}"]
+
+    def soa_form(pf):
+        if pf:
+            head = prefetched_inner_loop(side, pc, var, idx, n, qo, q)
+        else:
+            head = ["#pragma unroll 1", f"for (int {idx} = 0; {idx} < {n}; ++{idx}) {{",
+                    f"  if ({qo} * __ldg({q} + {idx} * {var}_st) < eps) break;"]
+            head += ["  " + x for x in side_loads(side, pc, var, idx)]
+        return head + ["  ++evaluated;"] + ["  " + x for x in inner_pre + inner] + ["}"]
+
+    pf32 = cid in PREFETCH_CLASSES or cid in PREFETCH_FP32_CLASSES
+    pf64 = cid in PREFETCH_CLASSES
+    f64 = core_form(pf64) if uniform else soa_form(pf64)
+    lines = ["if constexpr (sizeof(T) == 4) {"] + ["  " + x for x in core_form(pf32)] + ["} else {"]
+    lines += ["  " + x for x in f64] + ["}"]
     return ["  " + x for x in lines]
 
 
@@ -259,9 +308,6 @@ def gen_class(cid, la, lb, lc, ld, nsplit, split, order):
         body += ["  " + x for x in side_loads("b", pa, "bra", "i", 0, ncore)]
         for m in range(len(cds)):
             body.append("  T " + ", ".join(f"{w(m, h)} = T(0)" for h in hb) + ";")
-        pf_loop = prefetched_inner_loop("k", pk, "ket", "j", "ket_n", "qo", "ket_qp")
-        plain_loop = ["#pragma unroll 1", "for (int j = 0; j < ket_n; ++j) {",
-                      "  if (qo * __ldg(ket_qp + j * ket_st) < eps) break;"]
         inner_pre = side_pre("k", pk)
         inner = list(core)
         for m, terms in ket_terms.items():
@@ -276,7 +322,7 @@ def gen_class(cid, la, lb, lc, ld, nsplit, split, order):
                         inner.append(f"{tgt} = fma({cname}, {r}, {tgt});")
                     else:
                         inner.append(f"{tgt} {'-=' if sg < 0 else '+='} {r};")
-        body += inner_loop_variants(cid, pf_loop, plain_loop, side_loads("k", pk, "ket", "j"), inner_pre, inner)
+        body += inner_loop_variants(cid, "k", pk, "ket", "j", "ket_n", "qo", inner_pre, inner, False)
         if ncore is not None:
             body += ["  " + x for x in side_loads("b", pa, "bra", "i", ncore)]
         body += ["  " + x for x in side_pre("b", pa)]
@@ -298,9 +344,6 @@ def gen_class(cid, la, lb, lc, ld, nsplit, split, order):
         body += ["  " + x for x in side_loads("k", pk, "ket", "j", 0, ncore)]
         for n in range(len(abs_)):
             body.append("  T " + ", ".join(f"{w(n, h)} = T(0)" for h in hk) + ";")
-        pf_loop = prefetched_inner_loop("b", pa, "bra", "i", "bra_n", "qo", "bra_qp")
-        plain_loop = ["#pragma unroll 1", "for (int i = 0; i < bra_n; ++i) {",
-                      "  if (qo * __ldg(bra_qp + i * bra_st) < eps) break;"]
         inner_pre = side_pre("b", pa)
         inner = list(core)
         for n, terms in bra_terms.items():
@@ -312,7 +355,7 @@ def gen_class(cid, la, lb, lc, ld, nsplit, split, order):
                     r = rname(tb + tk, ub + uk, vb + vk, 0)
                     tgt = w(n, (tk, uk, vk))
                     inner.append(f"{tgt} = fma({cname}, {r}, {tgt});" if facs else f"{tgt} += {r};")
-        body += inner_loop_variants(cid, pf_loop, plain_loop, side_loads("b", pa, "bra", "i"), inner_pre, inner)
+        body += inner_loop_variants(cid, "b", pa, "bra", "i", "bra_n", "qo", inner_pre, inner, True)
         if ncore is not None:
             body += ["  " + x for x in side_loads("k", pk, "ket", "j", ncore)]
         body += ["  " + x for x in side_pre("k", pk)]
@@ -343,20 +386,24 @@ def gen_class(cid, la, lb, lc, ld, nsplit, split, order):
         "  // primitive pairs come sorted by descending primitive Schwarz factor q,",
         "  // and the loops stop once q_bra * q_ket < eps (each skipped primitive",
         "  // quartet is bounded by that product, Cauchy-Schwarz per primitive pair).",
+        "  // bra_core / ket_core: packed core records, core[(k * n_pairs + pair) * 8 + slot].",
         "  __device__ __forceinline__ static int run(",
-        "      const T* __restrict__ bra, const float* __restrict__ bra_q, long long bra_stride, int bra_kmax,",
-        "      int bra_row, int bra_n,",
-        "      const T* __restrict__ ket, const float* __restrict__ ket_q, long long ket_stride, int ket_kmax,",
-        "      int ket_row, int ket_n, float eps, T (&I)[NI]) {",
+        "      const T* __restrict__ bra, const T* __restrict__ bra_core, const float* __restrict__ bra_q,",
+        "      long long bra_stride, int bra_kmax, int bra_row, int bra_n,",
+        "      const T* __restrict__ ket, const T* __restrict__ ket_core, const float* __restrict__ ket_q,",
+        "      long long ket_stride, int ket_kmax, int ket_row, int ket_n, float eps, T (&I)[NI]) {",
         "    #pragma unroll",
         "    for (int q = 0; q < NI; ++q) I[q] = T(0);",
         "    int evaluated = 0;",
         "    const int bra_st = (int)bra_stride, ket_st = (int)ket_stride;",
-        "    const int bra_fs = bra_kmax * bra_st, ket_fs = ket_kmax * ket_st;",
+        "    [[maybe_unused]] const int bra_fs = bra_kmax * bra_st, ket_fs = ket_kmax * ket_st;",
         "    const T* __restrict__ bra_p = bra + bra_row;",
         "    const T* __restrict__ ket_p = ket + ket_row;",
         "    const float* __restrict__ bra_qp = bra_q + bra_row;",
         "    const float* __restrict__ ket_qp = ket_q + ket_row;",
+        "    const T* __restrict__ bra_c = bra_core + 8 * bra_row;",
+        "    const T* __restrict__ ket_c = ket_core + 8 * ket_row;",
+        "    [[maybe_unused]] const int bra_cst = 8 * bra_st, ket_cst = 8 * ket_st;",
     ]
     tail = ["    return evaluated;", "  }", "};", ""]
     return head + ["    " + x for x in body] + tail

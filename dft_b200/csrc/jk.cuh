@@ -5,6 +5,19 @@
 #include "common.cuh"
 #include "eri_classes.cuh"
 
+// Packed core record of primitive slot (k * n_pairs + pair): P, p, K, the
+// primitive Schwarz factor and 1/(2p) in both precisions.
+__device__ __forceinline__ void write_core(const dftk_pairs_t &pr, long long slot, double Px, double Py, double Pz,
+                                           double p, double K, float qp)
+{
+    const double v[8] = {Px, Py, Pz, p, K, (double)qp, p > 0.0 ? 0.5 / p : 0.0, 0.0};
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        pr.core64[slot * 8 + i] = v[i];
+        pr.core32[slot * 8 + i] = (float)v[i];
+    }
+}
+
 // ----------------------------------------------------------------- pair data
 // One thread per (primitive slot k, pair); pair index fastest so the SoA
 // record writes are coalesced.  Replaces the per-pair nuclear_kernel launch
@@ -48,17 +61,18 @@ __global__ void k_pair_data(const dftk_shells_t sh, const dftk_pairs_t pr, int n
         pr.rec64[o] = f[i];
         pr.rec32[o] = (float)f[i];
     }
+    if (pr.core64) write_core(pr, (long long)k * n + pair, f[F_PX], f[F_PY], f[F_PZ], f[F_P], f[F_K], 0.0f);
 }
 
 // ------------------------------------------------------------------ helpers
 template <int C, typename T, int S>
-__device__ __forceinline__ int eri_run(const T *bra, const float *bra_q, int bra_n_pairs, int bra_kmax,
-                                       int bra_row, int bra_np, const T *ket, const float *ket_q,
-                                       int ket_n_pairs, int ket_kmax, int ket_row, int ket_np, float eps,
-                                       T (&I)[EriClass<T, C, S>::NI])
+__device__ __forceinline__ int eri_run(const T *bra, const T *bra_core, const float *bra_q, int bra_n_pairs,
+                                       int bra_kmax, int bra_row, int bra_np, const T *ket, const T *ket_core,
+                                       const float *ket_q, int ket_n_pairs, int ket_kmax, int ket_row, int ket_np,
+                                       float eps, T (&I)[EriClass<T, C, S>::NI])
 {
-    return EriClass<T, C, S>::run(bra, bra_q, bra_n_pairs, bra_kmax, bra_row, bra_np, ket, ket_q, ket_n_pairs,
-                                  ket_kmax, ket_row, ket_np, eps, I);
+    return EriClass<T, C, S>::run(bra, bra_core, bra_q, bra_n_pairs, bra_kmax, bra_row, bra_np, ket, ket_core, ket_q,
+                                  ket_n_pairs, ket_kmax, ket_row, ket_np, eps, I);
 }
 
 // Diagonal class of a pair class: ss -> (ss|ss), ps -> (ps|ps), pp -> (pp|pp).
@@ -70,8 +84,10 @@ __device__ __forceinline__ double diag_max(const dftk_pairs_t &pr, int pair, int
 {
     double I[EriClass<double, C, S>::NI];
     const double *rec = pr.rec64 + (long long)k0 * pr.n_pairs;
+    const double *core = pr.core64 + 8LL * k0 * pr.n_pairs;
     const float *q = pr.qp + (long long)k0 * pr.n_pairs;
-    eri_run<C, double, S>(rec, q, pr.n_pairs, pr.kmax, pair, np, rec, q, pr.n_pairs, pr.kmax, pair, np, 0.0f, I);
+    eri_run<C, double, S>(rec, core, q, pr.n_pairs, pr.kmax, pair, np, rec, core, q, pr.n_pairs, pr.kmax, pair, np,
+                          0.0f, I);
     double m = 0.0;
 #pragma unroll
     for (int q2 = 0; q2 < EriClass<double, C, S>::NI; ++q2) m = fmax(m, fabs(I[q2]));
@@ -132,6 +148,12 @@ __global__ void k_schwarz(const dftk_pairs_t pr, int nfields)
         }
     }
     for (int k = 0; k < kk; ++k) pr.qp[k * n + pair] = qk[order[k]];
+    if (pr.core64)
+        for (int k = 0; k < kk; ++k) {
+            const long long o = (long long)k * n + pair;
+            write_core(pr, o, pr.rec64[o], pr.rec64[(long long)pr.kmax * n + o], pr.rec64[2LL * pr.kmax * n + o],
+                       pr.rec64[3LL * pr.kmax * n + o], pr.rec64[4LL * pr.kmax * n + o], qk[order[k]]);
+        }
 }
 
 // ------------------------------------------------------------------- J / K
@@ -142,6 +164,8 @@ struct JkParams {
     const int *np[3];
     const double *rec64[3];
     const float *rec32[3];
+    const double *core64[3];
+    const float *core32[3];
     const double *q[3];
     const float *qp[3];
     int n_pairs[3];
@@ -326,9 +350,11 @@ __device__ __forceinline__ void digest(const JkParams &P, bool valid, bool unifo
 template <int C, typename T> struct RecOf;
 template <int C> struct RecOf<C, double> {
     __device__ static const double *get(const JkParams &P, int pc) { return P.rec64[pc]; }
+    __device__ static const double *core(const JkParams &P, int pc) { return P.core64[pc]; }
 };
 template <int C> struct RecOf<C, float> {
     __device__ static const float *get(const JkParams &P, int pc) { return P.rec32[pc]; }
+    __device__ static const float *core(const JkParams &P, int pc) { return P.core32[pc]; }
 };
 
 template <int C, typename T, int S>
@@ -358,8 +384,9 @@ __device__ __forceinline__ void jk_one(const JkParams &P, bool valid, int row, i
         float eps = P.tau_prim;
         if constexpr (sizeof(T) == 4)
             eps = fmaxf(eps, 9.5367431640625e-7f * (float)(__ldg(P.q[X] + row) * __ldg(P.q[Yc] + ket)));
-        evaluated = eri_run<C, T, S>(RecOf<C, T>::get(P, X), P.qp[X], P.n_pairs[X], P.kmax[X], row, P.np[X][row],
-                                     RecOf<C, T>::get(P, Yc), P.qp[Yc], P.n_pairs[Yc], P.kmax[Yc], ket,
+        evaluated = eri_run<C, T, S>(RecOf<C, T>::get(P, X), RecOf<C, T>::core(P, X), P.qp[X], P.n_pairs[X],
+                                     P.kmax[X], row, P.np[X][row], RecOf<C, T>::get(P, Yc),
+                                     RecOf<C, T>::core(P, Yc), P.qp[Yc], P.n_pairs[Yc], P.kmax[Yc], ket,
                                      P.np[Yc][ket], eps, I);
     } else {
 #pragma unroll
@@ -625,6 +652,8 @@ struct EmitParams {
     const int *np[3];
     const double *rec64[3];
     const float *rec32[3];
+    const double *core64[3];
+    const float *core32[3];
     const float *qp[3];
     int n_pairs[3];
     int kmax[3];
@@ -639,9 +668,11 @@ __device__ __forceinline__ int ncomp(int l) { return (l + 1) * (l + 2) / 2; }
 template <typename T> struct EmitRec;
 template <> struct EmitRec<double> {
     __device__ static const double *get(const EmitParams &P, int pc) { return P.rec64[pc]; }
+    __device__ static const double *core(const EmitParams &P, int pc) { return P.core64[pc]; }
 };
 template <> struct EmitRec<float> {
     __device__ static const float *get(const EmitParams &P, int pc) { return P.rec32[pc]; }
+    __device__ static const float *core(const EmitParams &P, int pc) { return P.core32[pc]; }
 };
 
 template <int C, typename T, int S>
@@ -651,8 +682,9 @@ __device__ __forceinline__ void emit_split(const EmitParams &P, int row, int ket
     using E = EriClass<T, C, S>;
     constexpr int X = E::BRA_CLASS, Yc = E::KET_CLASS;
     T I[E::NI];
-    eri_run<C, T, S>(EmitRec<T>::get(P, X), P.qp[X], P.n_pairs[X], P.kmax[X], row, P.np[X][row],
-                     EmitRec<T>::get(P, Yc), P.qp[Yc], P.n_pairs[Yc], P.kmax[Yc], ket, P.np[Yc][ket], 0.0f, I);
+    eri_run<C, T, S>(EmitRec<T>::get(P, X), EmitRec<T>::core(P, X), P.qp[X], P.n_pairs[X], P.kmax[X], row,
+                     P.np[X][row], EmitRec<T>::get(P, Yc), EmitRec<T>::core(P, Yc), P.qp[Yc], P.n_pairs[Yc],
+                     P.kmax[Yc], ket, P.np[Yc][ket], 0.0f, I);
 #pragma unroll
     for (int ia = 0; ia < E::NA; ++ia)
 #pragma unroll

@@ -6,10 +6,17 @@ An :class:`IntegralEngine` owns, on one CUDA device:
   coefficient x normalisation products),
 * every shell pair (i >= j, the reference's ``pair_list``, shelled.py:962-964)
   in canonical orientation l_a >= l_b, split into the pair classes ss/ps/pp and
-  sorted by descending Schwarz factor, with SoA primitive-pair records,
+  sorted by descending Schwarz factor, with SoA primitive-pair records and
+  packed core records,
 * the candidate-quartet queue: per quartet class, bra row r pairs with the
   ket prefix whose Schwarz product clears ``tau_schwarz``,
+* with d shells: the pairs holding a d shell and every s/p pair again in the
+  generic record layout, and the two candidate spaces (d pair | s/p pair),
+  (d pair | d pair) that dftk_jk_hl adds to the s/p build,
 * the J/K workspace.
+
+Generally contracted shells enter the kernels as one shell per contraction
+row (basis.segments); matrices keep the reference's AO order.
 
 PyTorch only provides the device buffers and the stream; all arithmetic is in
 ``libdftk.so``.
@@ -149,9 +156,14 @@ class IntegralEngine:
             "q": torch.zeros(max(n, 1), dtype=torch.float64, device=self.device),
             "qp": torch.zeros(max(self.kmax * n, 1), dtype=torch.float32, device=self.device),
         }
+        core = pc in PAIR_FIELDS  # packed core records: the s/p class kernels' inner loops read them
+        if core:
+            bufs["core64"] = torch.zeros(max(8 * self.kmax * n, 8), dtype=torch.float64, device=self.device)
+            bufs["core32"] = torch.zeros(max(8 * self.kmax * n, 8), dtype=torch.float32, device=self.device)
         st = _lib.Pairs(n, self.kmax, _lib.ptr(bufs["ab"]).value, _lib.ptr(bufs["nprim"]).value,
                         _lib.ptr(bufs["rec64"]).value, _lib.ptr(bufs["rec32"]).value, _lib.ptr(bufs["q"]).value,
-                        _lib.ptr(bufs["qp"]).value)
+                        _lib.ptr(bufs["qp"]).value, _lib.ptr(bufs["core64"]).value if core else None,
+                        _lib.ptr(bufs["core32"]).value if core else None)
         return bufs, st
 
     def _build_pairs(self):

@@ -11,7 +11,8 @@
   with 8 vectors, convergence at |dE| < 1e-10 and RMS(dD) < 1e-8, and an
   incremental Fock build F_k = F_{k-1} + G(D_k - D_{k-1}) with optional mixed
   precision (quartets whose Schwarz bound times |dD| is below tau_fp32 run in
-  FP32, accumulation in FP64).  Full FP64 rebuilds every ``rebuild_every``
+  FP32, accumulation in FP64; tau_fp32 "auto" derives it from a 1 uEh budget,
+  fp32_threshold).  Full FP64 rebuilds every ``rebuild_every``
   iterations, and for every iteration once RMS(dD) < ``finish_factor`` x
   dtol, bound the drift of the incremental sum, so convergence is always
   tested on a full FP64 Fock matrix.
@@ -202,9 +203,24 @@ class _Diis:
         return torch.einsum("i,iab->ab", c, torch.stack(self.F))
 
 
+# Relative error of one quartet evaluated in FP32 (records, Boys and MD in
+# FP32 with FP64 accumulation): a few FP32 roundings, bounded here by 2^-20.
+FP32_REL_ERR = 2.0 ** -20
+
+
+def fp32_threshold(n_quartets: int, budget: float = 1e-6, lo: float = 1e-6, hi: float = 1e-4) -> float:
+    """tau_fp32 from an energy budget (Eh).  A quartet below the bound
+    Q_ab Q_cd max|dD| < tau_fp32 runs in FP32 with an error below
+    FP32_REL_ERR x tau_fp32; the errors of n independent quartets add like a
+    random walk, so the Fock build's energy error stays near
+    FP32_REL_ERR tau_fp32 sqrt(n) <= budget.  Clamped to [lo, hi]."""
+    t = budget / (FP32_REL_ERR * max(float(n_quartets), 1.0) ** 0.5)
+    return float(min(max(t, lo), hi))
+
+
 def scf_rhf(engine: IntegralEngine, H: torch.Tensor, S: torch.Tensor, n_occ: int, e_nn: float,
             diis: int = 8, etol: float = 1e-10, dtol: float = 1e-8, max_iter: int = 200,
-            incremental: bool = True, mixed: bool = False, tau: float = 1e-12, tau_fp32: float = 1e-6,
+            incremental: bool = True, mixed: bool = False, tau: float = 1e-12, tau_fp32="auto",
             rebuild_every: int = 12, count_quartets: bool = False,
             finish_factor: float = 100.0,
             D_guess: Optional[torch.Tensor] = None, callback=None) -> SCFResult:
@@ -215,6 +231,8 @@ def scf_rhf(engine: IntegralEngine, H: torch.Tensor, S: torch.Tensor, n_occ: int
     if A is not None:
         H, S = A @ H @ A.T, A @ S @ A.T
     jk = _jk_in(engine, A)
+    if tau_fp32 == "auto":
+        tau_fp32 = fp32_threshold(sum(engine.quartet_totals()))
     X = orthogonalizer(S)
     if D_guess is None:
         _, Cp = torch.linalg.eigh(X.T @ H @ X)

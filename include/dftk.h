@@ -83,7 +83,8 @@ typedef struct {
     const int *prim_off;    /* [n_shells] first primitive in prim_exp/prim_cn */
     const int *ao;          /* [n_shells] first AO (reference ao_start) */
     const double *prim_exp; /* [total primitives] exponents */
-    const double *prim_cn;  /* [total primitives] coefficient x primitive norm (normal(), shelled.py:95-101) */
+    const double *prim_cn;  /* [total primitives] coefficient x radial norm sqrt((4a)^l) (2a/pi)^{3/4}, which is
+                               normal() of every component for s and p (shelled.py:95-101) */
     /* batch description (n_mol = 0 and NULL pointers for one molecule) */
     int n_mol;
     int max_ns;                /* largest shell count of a molecule */
@@ -114,6 +115,11 @@ typedef struct {
     double *q;              /* [n_pairs] Schwarz factor sqrt(max|(ab|ab)|) (written by dftk_schwarz) */
     float *qp;              /* [kmax * n_pairs] primitive Schwarz factors sqrt(max|(ab_k|ab_k)|), each
                                pair's primitives reordered by descending qp (written by dftk_schwarz) */
+    /* packed core records core[(k * n_pairs + pair) * 8 + slot], slots P x/y/z, p, K, qp, 1/(2p), 0:
+       what the class kernels' inner primitive loops read in one or two vector loads (written by
+       dftk_pair_data and, sorted, by dftk_schwarz; 64-byte aligned; NULL for the generic layout) */
+    double *core64;         /* [8 * kmax * n_pairs] */
+    float *core32;          /* [8 * kmax * n_pairs] */
 } dftk_pairs_t;
 
 /* Candidate quartets of each class: bra pair `row` of the bra pair class pairs

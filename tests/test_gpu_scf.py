@@ -53,3 +53,22 @@ def test_mixed_precision_energy_water16():
     # the energy of the last mixed incremental build itself, before the final FP64 rebuild
     assert abs(rmx.energy_last_build - r64.energy) < 1e-6
     assert sum(rmx.counts[6:12]) > 0
+
+
+def test_mixed_precision_energy_water64():
+    """Config-size check of the mixed form: (H2O)_64, budget-derived tau_fp32,
+    against the FP64 incremental SCF: the final energy and the energy of the
+    last mixed incremental build within 1 uEh, with most quartets in FP32."""
+    from dft_b200.scf import fp32_threshold
+
+    atoms, centers = geometry.water_cluster((4, 4, 4))
+    eng, S, H, enn = _setup(atoms, centers)
+    tau32 = fp32_threshold(sum(eng.quartet_totals()))
+    assert 1e-6 <= tau32 <= 1e-4
+    r64 = scf_rhf(eng, H, S, 5 * 64, enn, mixed=False)
+    rmx = scf_rhf(eng, H, S, 5 * 64, enn, mixed=True, count_quartets=True)
+    assert r64.converged and rmx.converged
+    assert abs(rmx.energy - r64.energy) < 1e-6
+    assert abs(rmx.energy_last_build - r64.energy) < 1e-6
+    # the incremental builds put over 1e8 quartets (about one full build's worth) through FP32
+    assert sum(rmx.counts[6:12]) > 1e8
