@@ -213,6 +213,59 @@ def gradient_figures(torch, eng, atoms, centers, res):
             "note": "analytic RHF gradient (derivative ERIs + S/T/V derivatives), converged (H2O)_64 density"}
 
 
+def config4_gradients(torch):
+    """The gradient workloads named for nuclear gradients: (H2O)_16 (2x2x4
+    lattice) and C10H22, each the analytic RHF/STO-3G gradient at its
+    converged density in FP64 and in the mixed form (median of 3 timed calls
+    after a warm-up, device-synchronised), the mixed-vs-FP64 difference, and
+    a central-difference check (h = 1e-4 bohr) of three coordinates."""
+    from dft_b200 import basis, geometry
+    from dft_b200.engine import IntegralEngine
+    from dft_b200.gradient import GRAD_TAU_FP32, rhf_gradient
+    from dft_b200.scf import scf_rhf
+
+    def energy(atoms, c):
+        sh = basis.build_shells(basis.load_basis(), atoms, c)
+        eng = IntegralEngine(sh, tau_schwarz=1e-12)
+        S, T, V = eng.one_electron(atoms, c)
+        return scf_rhf(eng, T + V, S, basis.n_electrons(atoms) // 2, geometry.nuclear_repulsion(atoms, c),
+                       etol=1e-12, dtol=1e-10).energy
+
+    out = {}
+    for name, (atoms, c) in (("h2o16", geometry.water_cluster((2, 2, 4))), ("c10h22", geometry.alkane(10))):
+        c = np.asarray(c, dtype=np.float64)
+        sh = basis.build_shells(basis.load_basis(), atoms, c)
+        eng = IntegralEngine(sh, tau_schwarz=1e-12)
+        S, T, V = eng.one_electron(atoms, c)
+        nocc = basis.n_electrons(atoms) // 2
+        res = scf_rhf(eng, T + V, S, nocc, geometry.nuclear_repulsion(atoms, c), etol=1e-12, dtol=1e-10)
+        fig = {}
+        for form, t32 in (("fp64", 0.0), ("mixed", GRAD_TAU_FP32)):
+            rhf_gradient(eng, atoms, c, res, nocc, tau_fp32=t32)
+            ts = []
+            for _ in range(3):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                g = rhf_gradient(eng, atoms, c, res, nocc, tau_fp32=t32)
+                torch.cuda.synchronize()
+                ts.append((time.perf_counter() - t0) * 1e3)
+            fig[f"{form}_ms"] = float(np.median(ts))
+            fig[f"grad_{form}"] = g
+        fd = []
+        for k in (0, 4, 3 * len(atoms) - 1):
+            a, x = divmod(k, 3)
+            cp, cm = c.copy(), c.copy()
+            cp[a, x] += 1e-4
+            cm[a, x] -= 1e-4
+            fd.append(abs((energy(atoms, cp) - energy(atoms, cm)) / 2e-4 - fig["grad_fp64"][a, x]))
+        out[name] = {"n_atoms": len(atoms), "n_basis": eng.n_ao, "fp64_ms": fig["fp64_ms"],
+                     "mixed_ms": fig["mixed_ms"], "mixed_tau_fp32": GRAD_TAU_FP32,
+                     "mixed_max_abs_diff_vs_fp64_Eh_per_bohr": float(np.abs(fig["grad_mixed"] - fig["grad_fp64"]).max()),
+                     "fd_max_abs_err_Eh_per_bohr": float(max(fd)), "fd_coordinates": 3,
+                     "grad_evals_per_s_fp64": 1e3 / fig["fp64_ms"]}
+    return out
+
+
 def error_figures(torch, eng):
     """Errors stated next to the results: ERIs of the (H2O)_64 quartets sampled
     from the reference's own run (tests/golden/h2o64_sample.npz, 3,600
@@ -855,6 +908,7 @@ def run_dftk_arm(args, rank, world, local_rank):
         if not args.no_extras:
             line["c10h22"] = c10h22_figures(torch, cpu=world == 1 and not args.no_cpu_baseline)
             line["grad"] = gradient_figures(torch, eng, atoms, centers, r64)
+            line["grad"]["config4"] = config4_gradients(torch)
             line["grid"] = grid_figures(torch, eng, centers, r64, nocc, cpu=world == 1 and not args.no_cpu_baseline)
             line["errors"] = error_figures(torch, eng)
             line.update(batch_figures(torch))

@@ -104,6 +104,7 @@ class HlSet(ctypes.Structure):
         ("total", ctypes.c_longlong * 2),
         ("row_off", ctypes.c_void_p * 2),
         ("tau_prim", ctypes.c_double),
+        ("lmax", ctypes.c_int),
     ]
 
 
@@ -156,7 +157,7 @@ def load() -> ctypes.CDLL:
         "dftk_grid_density": ([i, i, i, ll, vp, vp, ll, vp, vp, ll, vp], i),
         "dftk_prepare_bytes": ([ctypes.POINTER(Shells), ctypes.POINTER(ctypes.c_size_t)], i),
         "dftk_prepare": ([ctypes.POINTER(Shells), d, d, vp, sz, ctypes.POINTER(Pairs), ctypes.POINTER(Queue), vp], i),
-        "dftk_hl_schwarz": ([ctypes.POINTER(Shells), ctypes.POINTER(Pairs), vp], i),
+        "dftk_hl_schwarz": ([ctypes.POINTER(Shells), ctypes.POINTER(Pairs), i, vp], i),
         "dftk_jk_hl": ([ctypes.POINTER(Shells), ctypes.POINTER(HlSet), vp, vp, vp, vp, vp, vp, i, d, vp, sz, vp, vp], i),
         "dftk_hl_eri_blocks": ([ctypes.POINTER(Shells), ctypes.POINTER(HlSet), ll, vp, vp, vp, vp], i),
     }

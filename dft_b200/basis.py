@@ -26,7 +26,7 @@ STO3G_PATH = os.path.join(DATA_DIR, "sto-3g.json")
 
 
 class UnsupportedBasis(ValueError):
-    """The basis needs something the kernels do not provide (momenta beyond d)."""
+    """The basis needs something the kernels do not provide (momenta beyond f)."""
 
 
 def load_basis(path: str = STO3G_PATH) -> Dict:
@@ -117,14 +117,14 @@ def n_electrons(atoms: Sequence[str], charge: int = 0) -> int:
     return sum(int(a) for a in atoms) - charge
 
 
-LMAX = 2  # d shells: the largest momentum the integral kernels take
+LMAX = 3  # f shells: the largest momentum the integral kernels take
 
 
 def check_supported(shells: List[Dict]) -> None:
-    """The integral kernels take s, p and d shells, generally contracted or not."""
+    """The integral kernels take s, p, d and f shells, generally contracted or not."""
     for k, sh in enumerate(shells):
         if sh["angular_momentum"] > LMAX:
-            raise UnsupportedBasis(f"shell {k}: l = {sh['angular_momentum']} (kernels cover s, p and d)")
+            raise UnsupportedBasis(f"shell {k}: l = {sh['angular_momentum']} (kernels cover s, p, d and f)")
 
 
 def check_sp(shells: List[Dict], what: str) -> None:

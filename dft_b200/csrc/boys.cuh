@@ -15,7 +15,7 @@
 //   T >= 50: F_0 = sqrt(pi / T) / 2 (erfc(7) < 5e-23) and the upward
 //           recursion F_{m+1} = (2m + 1) F_m / (2T); the exp(-T) < 2e-22 term
 //           it drops changes F_m by < 2e-14 relative for m <= 7.
-// Tables: orders L = 0..8, grid points T_k = 0, 0.1, ..., 50, computed on the
+// Tables: orders L = 0..12, grid points T_k = 0, 0.1, ..., 50, computed on the
 // host in long double from the all-positive series
 // F_m(T) = exp(-T) sum_i (2T)^i / ((2m+1)(2m+3)...(2m+2i+1)).
 // Orders >= 1 in FP64 read a half-step table instead (T_k = k / 20, so
@@ -31,7 +31,7 @@
 #include "common.cuh"
 
 #define DFTK_BOYS_ROWS 501
-#define DFTK_BOYS_NL 9         // orders 0..8
+#define DFTK_BOYS_NL 13        // orders 0..12 ((ff|ff) quartets)
 #define DFTK_BOYS_W 8          // coefficients per grid point
 #define DFTK_BOYS_TMAX 50.0
 

@@ -899,15 +899,38 @@ int dftk_jk(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N_PCLASS]
     return launch_symmetrize(*shells, Y, Za, Zb, J, K_a, K_b, uhf, s);
 }
 
-int dftk_hl_schwarz(const dftk_shells_t *shells, dftk_pairs_t *pairs, dftk_stream_t stream)
+}  // extern "C"
+
+namespace {
+// Shared scratch of the d/f kernels: the LM = 2 layout fits the default
+// 48 KB, the LM = 3 one needs the opt-in (set before each launch).
+template <int LM, typename K> int hl_smem_optin(K kernel, size_t extra_static = 0)
 {
-    if (!shells || !pairs || !pairs->qp || !pairs->q || !pairs->rec64 || !pairs->rec32 || pairs->n_pairs < 0)
-        return fail(DFTK_ERR_ARG, "dftk_hl_schwarz: bad arguments");
+    const size_t bytes = sizeof(HlScratch<LM>);
+    if (bytes + extra_static > 48 * 1024)
+        DFTK_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    return DFTK_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int dftk_hl_schwarz(const dftk_shells_t *shells, dftk_pairs_t *pairs, int lmax, dftk_stream_t stream)
+{
+    if (!shells || !pairs || !pairs->qp || !pairs->q || !pairs->rec64 || !pairs->rec32 || pairs->n_pairs < 0 ||
+        lmax < 0 || lmax > HL_LMAX)
+        return fail(DFTK_ERR_ARG, "dftk_hl_schwarz: bad arguments (lmax 0..3)");
     if (pairs->kmax > HL_MAX_KPAIR) return fail(DFTK_ERR_SIZE, "dftk_hl_schwarz: more than 128 primitive pairs per pair");
     if (shells->mol) return fail(DFTK_ERR_UNSUPPORTED, "dftk_hl_schwarz: one molecule at a time");
     DFTK_INIT();
     if (pairs->n_pairs == 0) return DFTK_OK;
-    k_hl_schwarz<<<(unsigned)pairs->n_pairs, 32, 0, (cudaStream_t)stream>>>(*shells, *pairs);
+    int st;
+    if (lmax <= 2) {
+        k_hl_schwarz<2><<<(unsigned)pairs->n_pairs, 32, sizeof(HlScratch<2>), (cudaStream_t)stream>>>(*shells, *pairs);
+    } else {
+        if ((st = hl_smem_optin<3>(k_hl_schwarz<3>, 4096))) return st;
+        k_hl_schwarz<3><<<(unsigned)pairs->n_pairs, 32, sizeof(HlScratch<3>), (cudaStream_t)stream>>>(*shells, *pairs);
+    }
     DFTK_LAUNCHED("k_hl_schwarz");
     return DFTK_OK;
 }
@@ -921,7 +944,8 @@ int dftk_jk_hl(const dftk_shells_t *shells, const dftk_hl_t *hl, const double *D
     if (uhf && (!D_b || !K_b)) return fail(DFTK_ERR_ARG, "dftk_jk_hl: UHF needs D_b and K_b");
     if (!(tau >= 0.0)) return fail(DFTK_ERR_ARG, "dftk_jk_hl: bad threshold");
     if (shells->mol) return fail(DFTK_ERR_UNSUPPORTED, "dftk_jk_hl: one molecule at a time");
-    if (hl->n_rows < 0 || hl->n_rows != hl->hi.n_pairs || hl->total[0] < 0 || hl->total[1] < 0 ||
+    if (hl->lmax < 2 || hl->lmax > HL_LMAX || hl->n_rows < 0 || hl->n_rows != hl->hi.n_pairs || hl->total[0] < 0 ||
+        hl->total[1] < 0 ||
         ((hl->total[0] > 0 || hl->total[1] > 0) && (!hl->row_off[0] || !hl->row_off[1])))
         return fail(DFTK_ERR_ARG, "dftk_jk_hl: inconsistent candidate spaces");
     if (workspace_bytes < ws_bytes(shells->n_shells, shells->n_ao))
@@ -961,9 +985,15 @@ int dftk_jk_hl(const dftk_shells_t *shells, const dftk_hl_t *hl, const double *D
     P.tau = tau;
     P.counts = counts;
     long long blocks = total;
-    const long long cap = (long long)sm_count() * 8;  // 8 one-warp blocks per SM (26.6 KB shared each)
+    // one-warp blocks: 8 per SM with the d layout (26.6 KB shared each), 1 with the f one (167 KB)
+    const long long cap = (long long)sm_count() * (hl->lmax <= 2 ? 8 : 1);
     if (blocks > cap) blocks = cap;
-    k_hl_jk<<<(unsigned)blocks, 32, 0, s>>>(P);
+    if (hl->lmax <= 2) {
+        k_hl_jk<2><<<(unsigned)blocks, 32, sizeof(HlScratch<2>), s>>>(P);
+    } else {
+        if ((st = hl_smem_optin<3>(k_hl_jk<3>))) return st;
+        k_hl_jk<3><<<(unsigned)blocks, 32, sizeof(HlScratch<3>), s>>>(P);
+    }
     DFTK_LAUNCHED("k_hl_jk");
     long long bx = ((long long)nn + 255) / 256;
     if (bx > 148 * 8) bx = 148 * 8;
@@ -975,15 +1005,24 @@ int dftk_jk_hl(const dftk_shells_t *shells, const dftk_hl_t *hl, const double *D
 int dftk_hl_eri_blocks(const dftk_shells_t *shells, const dftk_hl_t *hl, long long n_quartets, const int *desc,
                        const long long *out_off, double *out, dftk_stream_t stream)
 {
-    if (!shells || !hl || n_quartets < 0 || (n_quartets > 0 && (!desc || !out_off || !out)))
+    if (!shells || !hl || n_quartets < 0 || (n_quartets > 0 && (!desc || !out_off || !out)) || hl->lmax < 2 ||
+        hl->lmax > HL_LMAX)
         return fail(DFTK_ERR_ARG, "dftk_hl_eri_blocks: bad arguments");
     DFTK_INIT();
     if (n_quartets == 0) return DFTK_OK;
     long long blocks = n_quartets;
-    const long long cap = (long long)sm_count() * 8;
+    const long long cap = (long long)sm_count() * (hl->lmax <= 2 ? 8 : 1);
     if (blocks > cap) blocks = cap;
-    k_hl_emit<<<(unsigned)blocks, 32, 0, (cudaStream_t)stream>>>(*shells, hl->hi, hl->lo, n_quartets, desc, out_off,
-                                                                  out);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (hl->lmax <= 2) {
+        k_hl_emit<2><<<(unsigned)blocks, 32, sizeof(HlScratch<2>), s>>>(*shells, hl->hi, hl->lo, n_quartets, desc,
+                                                                        out_off, out);
+    } else {
+        int st;
+        if ((st = hl_smem_optin<3>(k_hl_emit<3>))) return st;
+        k_hl_emit<3><<<(unsigned)blocks, 32, sizeof(HlScratch<3>), s>>>(*shells, hl->hi, hl->lo, n_quartets, desc,
+                                                                        out_off, out);
+    }
     DFTK_LAUNCHED("k_hl_emit");
     return DFTK_OK;
 }

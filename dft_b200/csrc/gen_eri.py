@@ -47,7 +47,7 @@ PAIR_FIELDS = {0: 5, 1: 9, 2: 12}  # record fields the ERI code loads (the store
 PREFETCH_CLASSES = {0, 3, 5}  # measured on B200: the others lose more to register spills
 # classes whose FP32 instantiation prefetches although the FP64 one does not
 # (FP32 records take half the registers)
-PREFETCH_FP32_CLASSES = {1}
+PREFETCH_FP32_CLASSES = {1, 4}
 # classes whose outer side's transform fields (h, PA, PB and the Hermite
 # coefficients built from them) are loaded after the inner primitive loop,
 # where the outer-side Hermite-to-Cartesian transform uses them, so they hold

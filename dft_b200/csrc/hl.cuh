@@ -1,4 +1,4 @@
-// Shell quartets with a d shell (l <= 2): one warp per quartet,
+// Shell quartets with a d or f shell (l <= 3): one warp per quartet,
 // McMurchie-Davidson with run-time momenta, the Cartesian block and the
 // Hermite intermediates in shared memory.
 //
@@ -22,38 +22,49 @@
 #include "generic.cuh"
 #include "jk.cuh"
 
-#define HL_LMAX 2                                   // largest shell momentum
-#define HL_NC 6                                     // components of an l = HL_LMAX shell
-#define HL_LP (2 * HL_LMAX)                         // largest pair momentum
-#define HL_L (4 * HL_LMAX)                          // largest quartet momentum (Boys order)
-#define HL_NH 35                                    // Hermite (t,u,v) with t+u+v <= HL_LP
-#define HL_NR 495                                   // R^{(n)}_{tuv} with t+u+v+n <= HL_L
-#define HL_NE (3 * (HL_LMAX + 1) * (HL_LMAX + 1) * (HL_LP + 1))
-#define HL_MAX_KPAIR 128                            // primitive pairs per pair (Schwarz sort)
-#define HL_FIELDS 13                                // record fields (generic layout, alpha last)
+#define HL_LMAX 3          // largest shell momentum the kernels take (f)
+#define HL_NC 10           // components of an f shell
+#define HL_MAX_KPAIR 128   // primitive pairs per pair (Schwarz sort)
+#define HL_FIELDS 13       // record fields (generic layout, alpha last)
 
-static_assert(HL_L < DFTK_BOYS_NL, "Boys table too short for the d quartets");
+// Sizes of the per-warp scratch for quartets of shells up to momentum LM:
+// LM = 2 (d) takes 26.6 KB of shared memory per warp, LM = 3 (f) 167 KB, so
+// a molecule runs the smallest instantiation that covers its shells.
+template <int LM> struct HlDims {
+    static constexpr int NC = (LM + 1) * (LM + 2) / 2;                    // components of one shell
+    static constexpr int LP = 2 * LM;                                     // pair momentum
+    static constexpr int L = 4 * LM;                                      // quartet momentum (Boys order)
+    static constexpr int NH = (LP + 1) * (LP + 2) * (LP + 3) / 6;         // (t,u,v), t+u+v <= LP
+    static constexpr int NR = (L + 1) * (L + 2) * (L + 3) * (L + 4) / 24;  // R^{(n)}_{tuv}, t+u+v+n <= L
+    static constexpr int NE = 3 * (LM + 1) * (LM + 1) * (LP + 1);         // E^{ij}_t of one pair, 3 axes
+};
+static_assert(HlDims<HL_LMAX>::L < DFTK_BOYS_NL, "Boys table too short for the f quartets");
 
-struct HlScratch {
-    double Eb[HL_NE];
-    double Ek[HL_NE];
-    double R[HL_NR];
-    double W[HL_NH * HL_NC * HL_NC];
-    double I[HL_NC * HL_NC * HL_NC * HL_NC];
+template <int LM> struct HlScratch {
+    using D = HlDims<LM>;
+    double Eb[D::NE];
+    double Ek[D::NE];
+    double R[D::NR];
+    double W[D::NH * D::NC * D::NC];
+    double I[D::NC * D::NC * D::NC * D::NC];
 };
 
 // Cartesian powers of component k of momentum l, in combinations() order
 // (z power outer, then y, x innermost); packed x | y << 4 | z << 8.
 __constant__ int c_hl_comp[HL_LMAX + 1][HL_NC] = {
-    {0x000, 0, 0, 0, 0, 0},
-    {0x001, 0x010, 0x100, 0, 0, 0},
+    {0x000},
+    {0x001, 0x010, 0x100},
     {0x002, 0x011, 0x020, 0x101, 0x110, 0x200},
+    {0x003, 0x012, 0x021, 0x030, 0x102, 0x111, 0x120, 0x201, 0x210, 0x300},
 };
-// 1 / sqrt(prod (2 l_i - 1)!!) per component
+// 1 / sqrt(prod (2 l_i - 1)!!) per component (1/sqrt(3), 1/sqrt(15))
+#define HL_R3 0.57735026918962576451
+#define HL_R15 0.25819888974716112568
 __constant__ double c_hl_cnorm[HL_LMAX + 1][HL_NC] = {
-    {1.0, 0, 0, 0, 0, 0},
-    {1.0, 1.0, 1.0, 0, 0, 0},
-    {0.57735026918962576451, 1.0, 0.57735026918962576451, 1.0, 1.0, 0.57735026918962576451},
+    {1.0},
+    {1.0, 1.0, 1.0},
+    {HL_R3, 1.0, HL_R3, 1.0, 1.0, HL_R3},
+    {HL_R15, HL_R3, HL_R3, HL_R15, HL_R3, 1.0, HL_R3, HL_R3, HL_R3, HL_R15},
 };
 
 __device__ __forceinline__ int hl_ncomp(int l) { return (l + 1) * (l + 2) / 2; }
@@ -81,29 +92,32 @@ __device__ __forceinline__ void hl_untet(int h, int &t, int &u, int &v)
 __device__ __forceinline__ int hl_c4(int x) { return x * (x - 1) * (x - 2) * (x - 3) / 24; }
 // first entry of level n in the R array of a quartet of momentum L
 __device__ __forceinline__ int hl_rbase(int L, int n) { return hl_c4(L + 4) - hl_c4(L - n + 4); }
+template <int LM>
 __device__ __forceinline__ int hl_eidx(int axis, int i, int j, int t)
 {
-    return ((axis * (HL_LMAX + 1) + i) * (HL_LMAX + 1) + j) * (HL_LP + 1) + t;
+    return ((axis * (LM + 1) + i) * (LM + 1) + j) * (2 * LM + 1) + t;
 }
 
 // E^{ij}_t for every axis, i <= la, j <= lb of one primitive pair: lane
 // (axis, i, j) raises a i times from E^{00}_0 = 1, then b j times.
+template <int LM>
 __device__ __forceinline__ void hl_hermite_E(double *E, int la, int lb, double h, const double (&PA)[3],
                                              const double (&PB)[3], int lane)
 {
+    constexpr int LP = 2 * LM;
     const int nij = (la + 1) * (lb + 1);
-    if (lane < 3 * nij) {
-        const int axis = lane / nij, r = lane % nij, i = r / (lb + 1), j = r % (lb + 1);
-        double cur[HL_LP + 1];
+    for (int e = lane; e < 3 * nij; e += 32) {
+        const int axis = e / nij, r = e % nij, i = r / (lb + 1), j = r % (lb + 1);
+        double cur[LP + 1];
 #pragma unroll
-        for (int t = 0; t <= HL_LP; ++t) cur[t] = 0.0;
+        for (int t = 0; t <= LP; ++t) cur[t] = 0.0;
         cur[0] = 1.0;
         int order = 0;
         for (int step = 0; step < i + j; ++step) {
             const double sh = step < i ? PA[axis] : PB[axis];
-            double nxt[HL_LP + 1];
+            double nxt[LP + 1];
 #pragma unroll
-            for (int t = 0; t <= HL_LP; ++t) {
+            for (int t = 0; t <= LP; ++t) {
                 double v = 0.0;
                 if (t <= order) v = sh * cur[t];
                 if (t > 0 && t <= order + 1) v = fma(h, cur[t - 1], v);
@@ -112,9 +126,9 @@ __device__ __forceinline__ void hl_hermite_E(double *E, int la, int lb, double h
             }
             ++order;
 #pragma unroll
-            for (int t = 0; t <= HL_LP; ++t) cur[t] = nxt[t];
+            for (int t = 0; t <= LP; ++t) cur[t] = nxt[t];
         }
-        for (int t = 0; t <= i + j; ++t) E[hl_eidx(axis, i, j, t)] = cur[t];
+        for (int t = 0; t <= i + j; ++t) E[hl_eidx<LM>(axis, i, j, t)] = cur[t];
     }
 }
 
@@ -145,7 +159,8 @@ __device__ __forceinline__ HlRec hl_load_rec(const double *rec, long long fs)
 // their pair (rec64 + pair, qp + pair); st = n_pairs, fs = kmax * n_pairs.
 // Primitive pairs come sorted by descending qp; both loops stop once
 // qp_bra * qp_ket < eps.  Every lane of the warp must call this.
-__device__ void hl_quartet(HlScratch &s, int la, int lb, int lc, int ld, const double *bra, const float *bra_qp,
+template <int LM>
+__device__ void hl_quartet(HlScratch<LM> &s, int la, int lb, int lc, int ld, const double *bra, const float *bra_qp,
                            long long bst, long long bfs, int bra_n, const double *ket, const float *ket_qp,
                            long long kst, long long kfs, int ket_n, float eps)
 {
@@ -161,19 +176,19 @@ __device__ void hl_quartet(HlScratch &s, int la, int lb, int lc, int ld, const d
         if (qb * kq0 < eps) break;
         const HlRec br = hl_load_rec(bra + i * bst, bfs);
         __syncwarp();
-        hl_hermite_E(s.Eb, la, lb, br.h, br.A, br.B, lane);
+        hl_hermite_E<LM>(s.Eb, la, lb, br.h, br.A, br.B, lane);
         for (int e = lane; e < nhb * ncd; e += 32) s.W[e] = 0.0;
         for (int j = 0; j < ket_n; ++j) {
             const float qk = __ldg(ket_qp + j * kst);
             if (qb * qk < eps) break;
             const HlRec kr = hl_load_rec(ket + j * kst, kfs);
             __syncwarp();  // the previous primitive quartet is done with Ek and R
-            hl_hermite_E(s.Ek, lc, ld, kr.h, kr.A, kr.B, lane);
+            hl_hermite_E<LM>(s.Ek, lc, ld, kr.h, kr.A, kr.B, lane);
             const double sum = br.p + kr.p;
             const double rho = br.p * kr.p / sum;
             const double X = br.P[0] - kr.P[0], Y = br.P[1] - kr.P[1], Z = br.P[2] - kr.P[2];
             const double pre = br.K * kr.K / sqrt(sum);
-            double F[HL_L + 1];
+            double F[4 * LM + 1];
             boys_runtime(L, rho * (X * X + Y * Y + Z * Z), F);
             if (lane <= L) {
                 double sc = pre;
@@ -214,11 +229,11 @@ __device__ void hl_quartet(HlScratch &s, int la, int lb, int lc, int ld, const d
                 const int dx = hl_pow(ld, id, 0), dy = hl_pow(ld, id, 1), dz = hl_pow(ld, id, 2);
                 double acc = 0.0;
                 for (int tt = 0; tt <= cx + dx; ++tt) {
-                    const double ex = s.Ek[hl_eidx(0, cx, dx, tt)];
+                    const double ex = s.Ek[hl_eidx<LM>(0, cx, dx, tt)];
                     for (int uu = 0; uu <= cy + dy; ++uu) {
-                        const double exy = ex * s.Ek[hl_eidx(1, cy, dy, uu)];
+                        const double exy = ex * s.Ek[hl_eidx<LM>(1, cy, dy, uu)];
                         for (int vv = 0; vv <= cz + dz; ++vv) {
-                            const double c = exy * s.Ek[hl_eidx(2, cz, dz, vv)];
+                            const double c = exy * s.Ek[hl_eidx<LM>(2, cz, dz, vv)];
                             const double r = s.R[hl_tet(t + tt, u + uu, v + vv)];
                             acc = ((tt + uu + vv) & 1) ? fma(-c, r, acc) : fma(c, r, acc);
                         }
@@ -235,11 +250,11 @@ __device__ void hl_quartet(HlScratch &s, int la, int lb, int lc, int ld, const d
             const int bx = hl_pow(lb, ib, 0), by = hl_pow(lb, ib, 1), bz = hl_pow(lb, ib, 2);
             double acc = 0.0;
             for (int t = 0; t <= ax + bx; ++t) {
-                const double ex = s.Eb[hl_eidx(0, ax, bx, t)];
+                const double ex = s.Eb[hl_eidx<LM>(0, ax, bx, t)];
                 for (int u = 0; u <= ay + by; ++u) {
-                    const double exy = ex * s.Eb[hl_eidx(1, ay, by, u)];
+                    const double exy = ex * s.Eb[hl_eidx<LM>(1, ay, by, u)];
                     for (int v = 0; v <= az + bz; ++v)
-                        acc = fma(exy * s.Eb[hl_eidx(2, az, bz, v)], s.W[hl_tet(t, u, v) * ncd + cd], acc);
+                        acc = fma(exy * s.Eb[hl_eidx<LM>(2, az, bz, v)], s.W[hl_tet(t, u, v) * ncd + cd], acc);
                 }
             }
             s.I[e] += acc;
@@ -259,9 +274,12 @@ __device__ void hl_quartet(HlScratch &s, int la, int lb, int lc, int ld, const d
 // One warp per pair of a 13-field pair set (any momenta <= HL_LMAX): Q_ab =
 // sqrt(max |(ab|ab)|) over the block, per primitive pair q_k likewise, then
 // the pair's primitive records reordered by descending q_k (both copies).
+extern __shared__ __align__(16) unsigned char hl_smem[];
+
+template <int LM>
 __global__ void __launch_bounds__(32) k_hl_schwarz(const dftk_shells_t sh, const dftk_pairs_t pr)
 {
-    __shared__ HlScratch s;
+    HlScratch<LM> &s = *reinterpret_cast<HlScratch<LM> *>(hl_smem);
     __shared__ float qk[HL_MAX_KPAIR];
     __shared__ int order[HL_MAX_KPAIR];
     __shared__ double tmp[HL_MAX_KPAIR];
@@ -284,12 +302,13 @@ __global__ void __launch_bounds__(32) k_hl_schwarz(const dftk_shells_t sh, const
         __syncwarp();
         return m;
     };
-    hl_quartet(s, la, lb, la, lb, rec, qp, n, fs, np, rec, qp, n, fs, np, 0.0f);
+    hl_quartet<LM>(s, la, lb, la, lb, rec, qp, n, fs, np, rec, qp, n, fs, np, 0.0f);
     const double qfull = sqrt(block_max());
     for (int k = 0; k < kk; ++k) {
         float v = 0.0f;
         if (k < np) {
-            hl_quartet(s, la, lb, la, lb, rec + k * n, qp + k * n, n, fs, 1, rec + k * n, qp + k * n, n, fs, 1, 0.0f);
+            hl_quartet<LM>(s, la, lb, la, lb, rec + k * n, qp + k * n, n, fs, 1, rec + k * n, qp + k * n, n, fs, 1,
+                           0.0f);
             v = (float)sqrt(block_max());
         }
         if (lane == 0) {
@@ -342,7 +361,8 @@ struct HlJkParams {
 // Digest the block s.I of quartet (ab|cd) into Y (J) and Z (K) with the
 // weights of the unique-quartet enumeration (same identities as the s/p
 // digestion: J = Y + Y^T, K = Z + Z^T afterwards).
-__device__ void hl_digest(const HlJkParams &P, const HlScratch &s, int a, int b, int c, int d, bool same_pair)
+template <int LM>
+__device__ void hl_digest(const HlJkParams &P, const HlScratch<LM> &s, int a, int b, int c, int d, bool same_pair)
 {
     const int lane = threadIdx.x & 31;
     const int la = P.sh.l[a], lb = P.sh.l[b], lc = P.sh.l[c], ld = P.sh.l[d];
@@ -416,9 +436,10 @@ __device__ void hl_digest(const HlJkParams &P, const HlScratch &s, int a, int b,
 // One block (one warp) per candidate at a time over the two candidate
 // spaces: (hi | lo) then (hi | hi); quartets whose density-weighted Schwarz
 // bound Q_ab Q_cd max|D| falls below tau are skipped.
+template <int LM>
 __global__ void __launch_bounds__(32) k_hl_jk(const HlJkParams P)
 {
-    __shared__ HlScratch s;
+    HlScratch<LM> &s = *reinterpret_cast<HlScratch<LM> *>(hl_smem);
     const long long total = P.total[0] + P.total[1];
     const long long hfs = (long long)P.hi.kmax * P.hi.n_pairs;
     const long long lfs = (long long)P.lo.kmax * P.lo.n_pairs;
@@ -433,10 +454,10 @@ __global__ void __launch_bounds__(32) k_hl_jk(const HlJkParams P)
         const int c = K.ab[2 * ket], d = K.ab[2 * ket + 1];
         const float dm = quartet_dmax(P.sh, P.Dsh, a, b, c, d);
         if (P.hi.q[row] * K.q[ket] * (double)dm < P.tau) continue;
-        hl_quartet(s, P.sh.l[a], P.sh.l[b], P.sh.l[c], P.sh.l[d], P.hi.rec64 + row, P.hi.qp + row, P.hi.n_pairs,
+        hl_quartet<LM>(s, P.sh.l[a], P.sh.l[b], P.sh.l[c], P.sh.l[d], P.hi.rec64 + row, P.hi.qp + row, P.hi.n_pairs,
                    hfs, P.hi.nprim[row], K.rec64 + ket, K.qp + ket, K.n_pairs, kind ? hfs : lfs, K.nprim[ket],
                    P.tau_prim);
-        hl_digest(P, s, a, b, c, d, kind == 1 && row == ket);
+        hl_digest<LM>(P, s, a, b, c, d, kind == 1 && row == ket);
         __syncwarp();
         ++evaluated;
     }
@@ -450,10 +471,11 @@ __global__ void __launch_bounds__(32) k_hl_jk(const HlJkParams P)
 // the pair's second, bit 1 likewise for the ket, bit 2: the reference's bra
 // is this quartet's ket.  n0..n3 are the reference slot AO counts (strides of
 // the flat block), out_off[q] the block's first element.
+template <int LM>
 __global__ void __launch_bounds__(32) k_hl_emit(const dftk_shells_t sh, const dftk_pairs_t hi, const dftk_pairs_t lo,
                                                 long long nq, const int *desc, const long long *out_off, double *out)
 {
-    __shared__ HlScratch s;
+    HlScratch<LM> &s = *reinterpret_cast<HlScratch<LM> *>(hl_smem);
     const long long hfs = (long long)hi.kmax * hi.n_pairs, lfs = (long long)lo.kmax * lo.n_pairs;
     for (long long q = blockIdx.x; q < nq; q += gridDim.x) {
         const int *dq = desc + 8 * q;
@@ -463,7 +485,7 @@ __global__ void __launch_bounds__(32) k_hl_emit(const dftk_shells_t sh, const df
         if (ket < 0 || ket >= K.n_pairs) continue;
         const int sha[4] = {hi.ab[2 * row], hi.ab[2 * row + 1], K.ab[2 * ket], K.ab[2 * ket + 1]};
         const int l4[4] = {sh.l[sha[0]], sh.l[sha[1]], sh.l[sha[2]], sh.l[sha[3]]};
-        hl_quartet(s, l4[0], l4[1], l4[2], l4[3], hi.rec64 + row, hi.qp + row, hi.n_pairs, hfs, hi.nprim[row],
+        hl_quartet<LM>(s, l4[0], l4[1], l4[2], l4[3], hi.rec64 + row, hi.qp + row, hi.n_pairs, hfs, hi.nprim[row],
                    K.rec64 + ket, K.qp + ket, K.n_pairs, kind ? hfs : lfs, K.nprim[ket], 0.0f);
         int slot[4];
         const int bra0 = (flags & 4) ? 2 : 0, ket0 = (flags & 4) ? 0 : 2;
@@ -491,12 +513,12 @@ __global__ void __launch_bounds__(32) k_hl_emit(const dftk_shells_t sh, const df
 }
 
 // ------------------------------------------------------- one-electron blocks
-// R^{(0)}_{tuv}(alpha, X, Y, Z), t+u+v <= L <= HL_LP, for one thread,
+// R^{(0)}_{tuv}(alpha, X, Y, Z), t+u+v <= L <= 2 HL_LMAX, for one thread,
 // tet-indexed (hl_tet): the same level-by-level recursion as hl_quartet.
-#define HL_NR1 70  // R^{(n)}_{tuv} with t+u+v+n <= HL_LP
+#define HL_NR1 210  // R^{(n)}_{tuv} with t+u+v+n <= 2 HL_LMAX
 __device__ void hl_R_thread(int L, double alpha, double X, double Y, double Z, double *R0)
 {
-    double F[HL_LP + 1];
+    double F[2 * HL_LMAX + 1];
     boys_runtime(L, alpha * (X * X + Y * Y + Z * Z), F);
     double R[HL_NR1];
     double sc = 1.0;
@@ -572,7 +594,7 @@ __global__ void k_one_electron_hl(const dftk_shells_t sh, int n_atoms, const dou
             for (int x = 0; x < 3; ++x) Pc[x] = (al * A[x] + be * B[x]) / p;
             // ov[axis][a power][b power 0..lb+2]; eh = E^{ab}_t for V
             double ov[3 * (HL_LMAX + 1) * (HL_LMAX + 3)];
-            double eh[HL_NE];
+            double eh[HlDims<HL_LMAX>::NE];
 #pragma unroll 1
             for (int x = 0; x < 3; ++x)
 #pragma unroll 1
@@ -583,14 +605,14 @@ __global__ void k_one_electron_hl(const dftk_shells_t sh, int n_atoms, const dou
                         herm_E1d(al, be, A[x], B[x], pa, pb, E);
                         ov[(x * (HL_LMAX + 1) + pa) * (HL_LMAX + 3) + pb] = E[0] * sq;
                         if (pb <= lb)
-                            for (int tt = 0; tt <= pa + pb; ++tt) eh[hl_eidx(x, pa, pb, tt)] = E[tt];
+                            for (int tt = 0; tt <= pa + pb; ++tt) eh[hl_eidx<HL_LMAX>(x, pa, pb, tt)] = E[tt];
                     }
             double vv[HL_NC * HL_NC];
 #pragma unroll 1
             for (int x = 0; x < ca * cb; ++x) vv[x] = 0.0;
 #pragma unroll 1
             for (int c = 0; c < n_atoms; ++c) {
-                double R[HL_NH];
+                double R[HlDims<HL_LMAX>::NH];
                 hl_R_thread(L, p, Pc[0] - atom_xyz[3 * c], Pc[1] - atom_xyz[3 * c + 1], Pc[2] - atom_xyz[3 * c + 2],
                             R);
 #pragma unroll 1
@@ -605,8 +627,8 @@ __global__ void k_one_electron_hl(const dftk_shells_t sh, int n_atoms, const dou
                         for (int ty = 0; ty <= ay + by; ++ty)
 #pragma unroll 1
                             for (int tz = 0; tz <= az + bz; ++tz)
-                                s += eh[hl_eidx(0, ax, bx, tx)] * eh[hl_eidx(1, ay, by, ty)] *
-                                     eh[hl_eidx(2, az, bz, tz)] * R[hl_tet(tx, ty, tz)];
+                                s += eh[hl_eidx<HL_LMAX>(0, ax, bx, tx)] * eh[hl_eidx<HL_LMAX>(1, ay, by, ty)] *
+                                     eh[hl_eidx<HL_LMAX>(2, az, bz, tz)] * R[hl_tet(tx, ty, tz)];
                     vv[k] += atom_z[c] * s;
                 }
             }

@@ -239,7 +239,7 @@ class IntegralEngine:
             return bufs, st, np.zeros(0), sel
         for _ in range(2):  # measure, sort, then build the sorted set
             _lib.call("dftk_pair_data", ctypes.byref(self.c_shells), _lib.PCLASS_GENERIC, ctypes.byref(st), stream)
-            _lib.call("dftk_hl_schwarz", ctypes.byref(self.c_shells), ctypes.byref(st), stream)
+            _lib.call("dftk_hl_schwarz", ctypes.byref(self.c_shells), ctypes.byref(st), self.hl_lmax, stream)
             q = bufs["q"][: ab.shape[0]].cpu().numpy()
             if _ == 1:
                 break
@@ -253,6 +253,7 @@ class IntegralEngine:
         rows are the d pairs; kets the s/p pairs ((hi|lo)) or the d pairs up
         to the row ((hi|hi)), each a Schwarz prefix as in the s/p queue."""
         pclass = self._pair_class
+        self.hl_lmax = int(self.l.max())
         hi_bufs, hi_st, q_hi, sel_hi = self._generic_set(np.nonzero(pclass == 3)[0])
         lo_bufs, lo_st, q_lo, sel_lo = self._generic_set(np.nonzero(pclass < 3)[0])
         self.ref_pair_row[sel_hi] = np.arange(sel_hi.size)
@@ -272,6 +273,7 @@ class IntegralEngine:
             hl.total[k] = self.hl_totals[k]
             hl.row_off[k] = _lib.ptr(self.hl_row_off[k]).value
         hl.tau_prim = self.tau_prim
+        hl.lmax = self.hl_lmax
         self.c_hl = hl
 
     # ---------------------------------------------------------------- queries

@@ -17,8 +17,8 @@
  *   dftk_one_electron     <- overlap/T_raw/V block loop       shelled.py:961-1069
  *   dftk_schwarz          <- (absent in the reference: screening bounds)
  *   dftk_eri_blocks       <- calc_eri quartet blocks          shelled.py:596-700
- *   dftk_hl_eri_blocks    <- the same for quartets with a d shell
- *   dftk_jk_hl            <- fill_matrices, quartets with a d shell (adds to dftk_jk's J/K)
+ *   dftk_hl_eri_blocks    <- the same for quartets with a d or f shell
+ *   dftk_jk_hl            <- fill_matrices, quartets with a d or f shell (adds to dftk_jk's J/K)
  *   dftk_hl_schwarz       <- (absent in the reference: screening bounds, generic pair layout)
  *   dftk_jk               <- fill_matrices                    shelled.py:770-877
  *   dftk_jk_noalloc       <- (absent in the reference: dftk_jk with fixed in-library scratch)
@@ -60,7 +60,7 @@ enum {
 #define DFTK_N_PCLASS 3
 
 /* Shells of one molecule, or of a batch of molecules (device arrays).  l <= 1
- * (s, p) for dftk_jk's class kernels and the gradient, l <= 2 for
+ * (s, p) for dftk_jk's class kernels and the gradient, l <= 3 for
  * dftk_jk_hl, dftk_hl_eri_blocks and dftk_one_electron (one molecule).  One
  * contraction per shell: the reference splits sp shells (shelled.py:66-75),
  * and a generally contracted shell (a coefficient matrix, shelled.py:49-64)
@@ -142,25 +142,27 @@ typedef struct {
     const unsigned char *mol_active;
 } dftk_queue_t;
 
-/* Shell quartets with a d shell (l <= 2).  The reference's eri_kernel takes
+/* Shell quartets with a d or f shell (l <= 3).  The reference's eri_kernel takes
  * any momenta (shelled.py:452-532, max_e = 7); here the s/p classes run the
- * generated kernels behind dftk_jk and every quartet with a d shell runs a
- * warp-per-quartet kernel with run-time momenta behind dftk_jk_hl.  Both
+ * generated kernels behind dftk_jk and every quartet with a d or f shell runs a
+ * warp-per-quartet kernel with run-time momenta behind dftk_jk_hl (shared
+ * scratch per warp: 26.6 KB when lmax = 2, 167 KB when lmax = 3).  Both
  * pair sets use the generic record layout (pair_class DFTK_PCLASS_GENERIC in
  * dftk_pair_data: the 12 ERI fields and alpha, 13 fields) and are sorted by
- * descending Schwarz factor (dftk_hl_schwarz).  Shells may carry l <= 2;
+ * descending Schwarz factor (dftk_hl_schwarz).  Shells may carry l <= 3;
  * prim_cn holds coefficient x radial norm sqrt((4a)^l) (2a/pi)^{3/4}, and the
  * kernels apply each Cartesian component's 1/sqrt(prod (2 l_i - 1)!!) (for
  * s and p shells both conventions agree). */
 #define DFTK_PCLASS_GENERIC 3
-#define DFTK_HL_LMAX 2
+#define DFTK_HL_LMAX 3
 typedef struct {
-    dftk_pairs_t hi;              /* pairs with a d shell, l_a >= l_b */
+    dftk_pairs_t hi;              /* pairs with a d or f shell, l_a >= l_b */
     dftk_pairs_t lo;              /* every s/p pair of the molecule, same layout */
     long long n_rows;             /* hi.n_pairs */
     long long total[2];           /* candidates of (hi|lo) and of (hi|hi) (ket <= row) */
     const long long *row_off[2];  /* device [n_rows + 1] each: Schwarz prefixes as in dftk_queue_t */
     double tau_prim;              /* primitive-quartet cut, as in dftk_queue_t */
+    int lmax;                     /* largest shell momentum, 2 (d) or 3 (f): selects the kernels' scratch layout */
 } dftk_hl_t;
 
 /* library version (integer, 100 * major + minor) */
@@ -296,12 +298,12 @@ int dftk_jk_noalloc(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N
                     const double *D_b, double *J, double *K_a, double *K_b, int flags,
                     double tau, double tau_fp32, long long *counts, dftk_stream_t stream);
 
-/* Schwarz factors of a generic-layout pair set (any momenta <= 2), with each
+/* Schwarz factors of a generic-layout pair set (momenta <= lmax <= 3), with each
  * pair's primitive records reordered by descending primitive factor (no
  * counterpart in the reference: screening bounds).  kmax <= 128. */
-int dftk_hl_schwarz(const dftk_shells_t *shells, dftk_pairs_t *pairs, dftk_stream_t stream);
+int dftk_hl_schwarz(const dftk_shells_t *shells, dftk_pairs_t *pairs, int lmax, dftk_stream_t stream);
 
-/* Adds the Coulomb and exchange contributions of every quartet with a d shell
+/* Adds the Coulomb and exchange contributions of every quartet with a d or f shell
  * to J, K_a (, K_b): the rest of fill_matrices (shelled.py:770-877) after
  * dftk_jk has written the s/p part.  FP64; quartets whose bound
  * Q_ab Q_cd max|D| is below tau are skipped.  Workspace: at least
@@ -310,7 +312,7 @@ int dftk_jk_hl(const dftk_shells_t *shells, const dftk_hl_t *hl, const double *D
                const double *D_b, double *J, double *K_a, double *K_b, int flags, double tau, void *workspace,
                size_t workspace_bytes, long long *counts, dftk_stream_t stream);
 
-/* Contracted ERI blocks of quartets with a d shell <- calc_eri quartet blocks
+/* Contracted ERI blocks of quartets with a d or f shell <- calc_eri quartet blocks
  * shelled.py:596-700.  desc[8 q ..]: {0 = (hi|lo) / 1 = (hi|hi), hi row, ket
  * row, flags (bit 0: the reference's first bra shell is the pair's second,
  * bit 1 the same for the ket, bit 2: the reference's bra is the ket pair),

@@ -538,6 +538,15 @@ void orc_direct_jk_fn(int ns, const double *center, const int *l, const int *nex
 {
     OrcShells S = orc_shells(ns, center, l, nexp, ncontr, exp_off, coef_off, ao, exps, coefs);
     long NN = (long)N * N;
+    /* largest contracted block and primitive block of any quartet */
+    size_t nao_max = 1, np_max = 1;
+    for (int s = 0; s < ns; ++s) {
+        size_t a = (size_t)orc_shell_nao(&S, s), p = (size_t)orc_ncomp(l[s]) * nexp[s];
+        if (a > nao_max) nao_max = a;
+        if (p > np_max) np_max = p;
+    }
+    const size_t blk_max = nao_max * nao_max * nao_max * nao_max;
+    const size_t prim_max = np_max * np_max * np_max * np_max;
     int nthreads = 1;
 #ifdef _OPENMP
     nthreads = omp_get_max_threads();
@@ -550,8 +559,8 @@ void orc_direct_jk_fn(int ns, const double *center, const int *l, const int *nex
         tid = omp_get_thread_num();
 #endif
         double *aj = acc + (long)tid * 3 * NN;
-        double *prim = (double *)malloc(sizeof(double) * ((size_t)1 << 20));
-        double blk[4096];
+        double *prim = (double *)malloc(sizeof(double) * prim_max);
+        double *blk = (double *)malloc(sizeof(double) * blk_max);
         #pragma omp for schedule(dynamic, 16)
         for (long t = 0; t < nq; ++t) {
             const int *q = quads + 4 * t;
@@ -564,6 +573,7 @@ void orc_direct_jk_fn(int ns, const double *center, const int *l, const int *nex
             orc_pair_free(&cd);
         }
         free(prim);
+        free(blk);
     }
     orc_reduce(nthreads, NN, acc, J, Ka, Kb);
     free(acc);

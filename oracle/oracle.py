@@ -280,7 +280,7 @@ def full_eri_tensor(shells: List[Dict]) -> np.ndarray:
 # --------------------------------------------------------------------------- SCF
 def spherical_transform(shells: List[Dict]) -> np.ndarray:
     """The reference's A = independent(shells, sphere_total_ao, I)
-    (shelled.py:878-920, :1071), restated row by row for s, p and d."""
+    (shelled.py:878-920, :1071), restated row by row for s, p, d and f."""
     n_cart = sum(int(s["n_ao"]) for s in shells)
     n_sph = sum(int(s["n_contractions"]) * (2 * int(s["angular_momentum"]) + 1) for s in shells)
     A = np.zeros((n_sph, n_cart))
@@ -301,8 +301,26 @@ def spherical_transform(shells: List[Dict]) -> np.ndarray:
                 A[r + 4, c + 5] = 1.0
                 A[r + 4, c] = -0.5
                 A[r + 4, c + 2] = -0.5
+            elif l == 3:
+                s2, s3, s5, s6, s10, s30 = (np.sqrt(x) for x in (2.0, 3.0, 5.0, 6.0, 10.0, 30.0))
+                A[r, c + 4] = -3 * s5 / 10
+                A[r, c + 6] = -3 * s5 / 10
+                A[r, c + 9] = 1.0
+                A[r + 1, c] = -s6 / 4
+                A[r + 1, c + 2] = -s30 / 20
+                A[r + 1, c + 7] = s30 / 5
+                A[r + 2, c + 1] = -s30 / 20
+                A[r + 2, c + 3] = -s6 / 4
+                A[r + 2, c + 8] = s30 / 5
+                A[r + 3, c + 4] = s3 / 2
+                A[r + 3, c + 6] = -s3 / 2
+                A[r + 4, c + 5] = 1.0
+                A[r + 5, c] = s10 / 4
+                A[r + 5, c + 2] = -3 * s2 / 4
+                A[r + 6, c + 1] = 3 * s2 / 4
+                A[r + 6, c + 3] = -s10 / 4
             else:
-                raise ValueError("oracle spherical transform: s, p and d")
+                raise ValueError("oracle spherical transform: s, p, d and f")
             r += 2 * l + 1
     return A
 

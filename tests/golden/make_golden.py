@@ -26,6 +26,7 @@ Usage::
     python tests/golden/make_golden.py grid           # seconds (H2O SCF + evaluation script)
     python tests/golden/make_golden.py br2            # d shells (STO-3G Br2)
     python tests/golden/make_golden.py gc             # general contractions + d (H2O, test basis)
+    python tests/golden/make_golden.py gcf            # the same with f (O) and d (H) shells
 """
 from __future__ import annotations
 
@@ -278,19 +279,20 @@ def case_dshell(out_dir):
     print("br2 energy", res["energy"], "iters", res["iterations"], "eri values", res["processed_eri_values"].shape)
 
 
-def case_gc(out_dir):
+def case_gc(out_dir, basis_file="dz_gc_test.json", out_name="h2o_gc.npz"):
     """H2O with the generally contracted, d-polarised test basis
-    (tests/golden/dz_gc_test.json): spherical-basis S/T/V, densities, J/K and
+    (tests/golden/dz_gc_test.json; with basis_file dzf_gc_test.json also an f
+    shell on O and a d shell on H): spherical-basis S/T/V, densities, J/K and
     the energy at tightened thresholds."""
     atoms, centers = geometry.water()
     ns, work = run_reference(atoms, centers, etol=1e-11, ptol=1e-8,
-                             basis_path=os.path.join(HERE, "dz_gc_test.json"))
+                             basis_path=os.path.join(HERE, basis_file))
     res = {"atoms": np.array(atoms), "centers": centers, "energy": float(ns["E_total_new"]),
            "iterations": int(ns["count"]), "E_NN": float(ns["E_NN"])}
     for k in ("overlaps", "T_matrix", "V_matrix", "P_a", "P_b", "J_matrix", "K_a", "K_b", "A"):
         res[k] = np.asarray(ns[k], dtype=np.float64)
-    np.savez_compressed(os.path.join(out_dir, "h2o_gc.npz"), **res)
-    print("h2o gc energy", res["energy"], "iters", res["iterations"], "n_sph", res["overlaps"].shape)
+    np.savez_compressed(os.path.join(out_dir, out_name), **res)
+    print(out_name, "energy", res["energy"], "iters", res["iterations"], "n_sph", res["overlaps"].shape)
 
 
 def patched_eval(spacing=0.15, chunk=500):
@@ -340,12 +342,12 @@ def case_grid(out_dir):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["h2o", "c10h22", "h2o64", "grid", "br2", "gc"])
+    ap.add_argument("case", choices=["h2o", "c10h22", "h2o64", "grid", "br2", "gc", "gcf"])
     ap.add_argument("--out", default=HERE)
     args = ap.parse_args()
     install_fake_cupy()
     {"h2o": case_h2o, "c10h22": case_c10h22, "h2o64": case_h2o64, "grid": case_grid, "br2": case_dshell,
-     "gc": case_gc}[args.case](args.out)
+     "gc": case_gc, "gcf": lambda out: case_gc(out, "dzf_gc_test.json", "h2o_gcf.npz")}[args.case](args.out)
 
 
 if __name__ == "__main__":

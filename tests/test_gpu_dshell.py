@@ -1,11 +1,12 @@
-"""d shells and general contractions on the GPU against the reference's own
-outputs (tests/golden/make_golden.py br2 / gc) and the oracle.
+"""d and f shells and general contractions on the GPU against the reference's
+own outputs (tests/golden/make_golden.py br2 / gc / gcf) and the oracle.
 
 * Br2 / STO-3G (3d shells on both atoms): every processed ERI at 1e-12
   absolute, S/T/V in the reference's spherical basis, J/K at the reference's
   converged densities, and the SCF energy of the reference loop at 1e-8 Eh.
-* H2O with a generally contracted, d-polarised test basis: S/T/V, J/K and
-  the energy (reference loop and the RHF/DIIS driver) at 1e-8 Eh.
+* H2O with a generally contracted, d-polarised test basis, and the same with
+  an f shell on O and a d shell on H: S/T/V, J/K and the energy (reference
+  loop and the RHF/DIIS driver) at 1e-8 Eh.
 * J/K with random densities against the oracle's direct J/K (1e-11).
 """
 import json
@@ -24,15 +25,23 @@ pytestmark = pytest.mark.gpu
 
 ERI_TOL = 1e-12
 GC_BASIS = os.path.join(GOLDEN, "dz_gc_test.json")
+GCF_BASIS = os.path.join(GOLDEN, "dzf_gc_test.json")
+CASES = {"br2": ("br2.npz", None), "gc": ("h2o_gc.npz", GC_BASIS), "gcf": ("h2o_gcf.npz", GCF_BASIS)}
 
 
 def _mol(g):
     return [str(a) for a in g["atoms"]], np.asarray(g["centers"])
 
 
-def _gc_basis():
-    with open(GC_BASIS) as fh:
+def _gc_basis(path=GC_BASIS):
+    with open(path) as fh:
         return json.load(fh)
+
+
+def _case(case):
+    name, path = CASES[case]
+    g = load_golden(name)
+    return g, (basis.load_basis() if path is None else _gc_basis(path))
 
 
 def _sph(A, M):
@@ -53,11 +62,10 @@ def test_br2_all_eris_match_reference(tmp_path):
     assert err.max() < ERI_TOL, err.max()
 
 
-@pytest.mark.parametrize("case", ["br2", "gc"])
+@pytest.mark.parametrize("case", ["br2", "gc", "gcf"])
 def test_one_electron_spherical_match_reference(case):
-    g = load_golden("br2.npz" if case == "br2" else "h2o_gc.npz")
+    g, data = _case(case)
     atoms, centers = _mol(g)
-    data = basis.load_basis() if case == "br2" else _gc_basis()
     sh = basis.build_shells(data, atoms, centers)
     A = basis.spherical_transform(sh)
     np.testing.assert_allclose(A, g["A"], atol=1e-15, rtol=0)
@@ -68,13 +76,12 @@ def test_one_electron_spherical_match_reference(case):
         assert err < 1e-12 * max(1.0, np.abs(ref).max()), (key, err)
 
 
-@pytest.mark.parametrize("case", ["br2", "gc"])
+@pytest.mark.parametrize("case", ["br2", "gc", "gcf"])
 def test_jk_at_reference_density(case):
     """fill_matrices at the reference's converged densities (UHF call shape),
     compared in the reference's spherical basis."""
-    g = load_golden("br2.npz" if case == "br2" else "h2o_gc.npz")
+    g, data = _case(case)
     atoms, centers = _mol(g)
-    data = basis.load_basis() if case == "br2" else _gc_basis()
     sh = basis.build_shells(data, atoms, centers)
     A = g["A"]
     Pa_c, Pb_c = A.T @ g["P_a"] @ A, A.T @ g["P_b"] @ A
@@ -87,11 +94,10 @@ def test_jk_at_reference_density(case):
         assert err < 1e-11 * max(1.0, np.abs(ref).max()), (key, err)
 
 
-@pytest.mark.parametrize("case", ["br2", "gc"])
+@pytest.mark.parametrize("case", ["br2", "gc", "gcf"])
 def test_scf_energy_matches_reference(case):
-    g = load_golden("br2.npz" if case == "br2" else "h2o_gc.npz")
+    g, data = _case(case)
     atoms, centers = _mol(g)
-    data = basis.load_basis() if case == "br2" else _gc_basis()
     sh = basis.build_shells(data, atoms, centers)
     eng = IntegralEngine(sh, tau_schwarz=0.0)
     S, T, V = eng.one_electron(atoms, centers)
@@ -142,3 +148,30 @@ def test_br2_eri_blocks_vs_oracle(oracle_mod):
     v0, off0 = oracle_mod.eri_quartets(osh, q)
     np.testing.assert_array_equal(off, off0)
     assert np.abs(vals.cpu().numpy() - v0).max() < ERI_TOL
+
+
+def test_f_shell_eris_and_jk_vs_oracle(oracle_mod):
+    """HF with STO-3G plus an f shell on each atom (single contractions): every
+    ERI block through dftk_hl_eri_blocks against the oracle at 1e-12, and J/K
+    with random densities at 1e-11 relative."""
+    data = basis.load_basis()
+    data = {"1": data["1"] + [[[3], [0.8], [[1.0]]]], "9": data["9"] + [[[3], [1.1], [[1.0]]]]}
+    atoms, centers = ["9", "1"], np.array([[0.0, 0.0, 0.0], [0.2, -0.1, 1.75]])
+    sh = basis.build_shells(data, atoms, centers)
+    eng = IntegralEngine(sh, tau_schwarz=0.0)
+    assert eng.hl_lmax == 3
+    q = shelled.quartet_list([(i, j) for i in range(len(sh)) for j in range(i + 1)])
+    vals, off = eng.eri_blocks(q)
+    osh = oracle_mod.build_shells(data, atoms, centers)
+    v0, off0 = oracle_mod.eri_quartets(osh, q)
+    np.testing.assert_array_equal(off, off0)
+    assert np.abs(vals.cpu().numpy() - v0).max() < ERI_TOL
+    N = eng.n_ao
+    rng = np.random.default_rng(3)
+    M = rng.normal(size=(N, N))
+    P = 0.1 * (M + M.T)
+    dev = eng.device
+    J, K, _ = eng.jk(torch.as_tensor(2 * P, device=dev), torch.as_tensor(P, device=dev), tau=0.0)
+    J0, K0, _ = oracle_mod.direct_jk(osh, q, 2 * P, P, P)
+    for A_, B_ in ((J, J0), (K, K0)):
+        assert np.abs(A_.cpu().numpy() - B_).max() < 1e-11 * max(1.0, np.abs(B_).max())

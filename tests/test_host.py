@@ -43,9 +43,9 @@ def test_unsupported_basis_is_rejected():
     basis.check_supported(shells)  # d shells are covered
     with pytest.raises(basis.UnsupportedBasis):
         basis.check_sp(shells, "batch")  # the s/p-only paths refuse them
-    f_basis = {"1": [[[3], [1.0], [[1.0]]]]}
+    g_basis = {"1": [[[4], [1.0], [[1.0]]]]}  # g shells are beyond the kernels
     with pytest.raises(basis.UnsupportedBasis):
-        basis.check_supported(basis.build_shells(f_basis, ["1"], np.zeros((1, 3))))
+        basis.check_supported(basis.build_shells(g_basis, ["1"], np.zeros((1, 3))))
 
 
 def test_geometry_alkane():

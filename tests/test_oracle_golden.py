@@ -228,15 +228,19 @@ def test_br2_eris_and_energy(oracle_mod):
     assert abs(r["energy"] - g["energy"]) < 1e-8
 
 
-def test_general_contraction_energy(oracle_mod):
-    """H2O with the generally contracted, d-polarised test basis: the oracle's
-    contraction-matrix integrals reproduce the reference's spherical S/T/V and
-    its SCF energy."""
-    from conftest import load_golden
+@pytest.mark.parametrize("case", ["gc", "gcf"])
+def test_general_contraction_energy(oracle_mod, case):
+    """H2O with the generally contracted, d-polarised test basis (gcf: with an
+    f shell on O and a d shell on H as well): the oracle's contraction-matrix
+    integrals reproduce the reference's spherical S/T/V and its SCF energy."""
+    import os
 
-    g = load_golden("h2o_gc.npz")
+    from conftest import GOLDEN, load_golden
+
+    g = load_golden("h2o_gc.npz" if case == "gc" else "h2o_gcf.npz")
+    path = _gc_path() if case == "gc" else os.path.join(GOLDEN, "dzf_gc_test.json")
     atoms, centers = [str(a) for a in g["atoms"]], g["centers"]
-    sh = oracle_mod.build_shells(oracle_mod.load_basis(_gc_path()), atoms, centers)
+    sh = oracle_mod.build_shells(oracle_mod.load_basis(path), atoms, centers)
     A = oracle_mod.spherical_transform(sh)
     np.testing.assert_allclose(A, g["A"], atol=1e-15, rtol=0)
     S, T, V = oracle_mod.one_electron(sh, atoms, centers)
@@ -270,3 +274,12 @@ def test_segments_and_spherical_transform_host():
     b = load_golden("br2.npz")
     shb = basis.build_shells(basis.load_basis(), [str(a) for a in b["atoms"]], b["centers"])
     np.testing.assert_allclose(basis.spherical_transform(shb), b["A"], atol=1e-15, rtol=0)
+    import os
+
+    from conftest import GOLDEN
+
+    f = load_golden("h2o_gcf.npz")
+    with open(os.path.join(GOLDEN, "dzf_gc_test.json")) as fh:
+        shf = basis.build_shells(json.load(fh), [str(a) for a in f["atoms"]], f["centers"])
+    assert max(s["angular_momentum"] for s in shf) == 3
+    np.testing.assert_allclose(basis.spherical_transform(shf), f["A"], atol=1e-15, rtol=0)
