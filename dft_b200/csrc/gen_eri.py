@@ -46,7 +46,8 @@ PAIR_FIELDS = {0: 5, 1: 9, 2: 12}  # record fields the ERI code loads (the store
 # one iteration ahead
 PREFETCH_CLASSES = {0, 3, 5}  # measured on B200: the others lose more to register spills
 # classes whose FP32 instantiation prefetches although the FP64 one does not
-# (FP32 records take half the registers)
+# (FP32 records take half the registers; measured on B200, mixed (H2O)_64
+# build: (pp|ps) 0.60 -> 0.56 ms, while (ps|ps) loses, 1.28 -> 1.38)
 PREFETCH_FP32_CLASSES = {1, 4}
 # classes whose outer side's transform fields (h, PA, PB and the Hermite
 # coefficients built from them) are loaded after the inner primitive loop,
