@@ -18,6 +18,7 @@ N_QCLASS = 6
 N_PCLASS = 3
 JK_UHF = 1
 JK_MIXED = 2
+JK_PERSIST = 4
 PCLASS_GENERIC = 3  # dftk_pair_data: the 13-field record layout of the d-shell path
 
 OK, ERR_ARG, ERR_CUDA, ERR_UNSUPPORTED, ERR_WORKSPACE, ERR_SIZE = range(6)

@@ -251,7 +251,7 @@ class BatchEngine(IntegralEngine):
         return M
 
     def jk(self, D, D_a=None, D_b=None, uhf=False, mixed=False, tau=1e-14, tau_fp32=1e-6, out=None, counts=None,
-           scan=False):
+           scan=False, persist=False):
         """Packed J, K_a (, K_b) of every active molecule (see IntegralEngine.jk)."""
         D = self._square(D)
         D_a = self._square(D_a) if D_a is not None else (0.5 * D).contiguous()
@@ -263,7 +263,7 @@ class BatchEngine(IntegralEngine):
             Kb = torch.empty_like(J) if uhf else None
         else:
             J, Ka, Kb = out
-        flags = (_lib.JK_UHF if uhf else 0) | (_lib.JK_MIXED if mixed else 0)
+        flags = (_lib.JK_UHF if uhf else 0) | (_lib.JK_MIXED if mixed else 0) | (_lib.JK_PERSIST if persist else 0)
         _lib.call("dftk_jk", ctypes.byref(self.c_shells), self.c_pairs, ctypes.byref(self.c_queue),
                   _lib.ptr(D), _lib.ptr(D_a), _lib.ptr(D_b if uhf else None), _lib.ptr(J), _lib.ptr(Ka),
                   _lib.ptr(Kb if uhf else None), flags, float(tau), float(tau_fp32 if mixed else tau),
@@ -293,7 +293,7 @@ class _FockGraph:
     """The packed J/K build of a batch captured once as a CUDA graph: static
     density input, static J and K outputs."""
 
-    def __init__(self, eng: BatchEngine, tau: float):
+    def __init__(self, eng: BatchEngine, tau: float, persist: bool = False):
         self.eng = eng
         self.D = torch.zeros(eng.mat_elems, dtype=torch.float64, device=eng.device)
         self.Dh = torch.zeros_like(self.D)
@@ -304,11 +304,11 @@ class _FockGraph:
         s = torch.cuda.Stream(device=eng.device)
         s.wait_stream(torch.cuda.current_stream(eng.device))
         with torch.cuda.stream(s):
-            eng.jk(self.D, self.Dh, tau=tau, out=(self.J, self.K, None))
+            eng.jk(self.D, self.Dh, tau=tau, out=(self.J, self.K, None), persist=persist)
         torch.cuda.current_stream(eng.device).wait_stream(s)
         self.graph = torch.cuda.CUDAGraph()
         with torch.cuda.graph(self.graph):
-            eng.jk(self.D, self.Dh, tau=tau, out=(self.J, self.K, None))
+            eng.jk(self.D, self.Dh, tau=tau, out=(self.J, self.K, None), persist=persist)
 
     def run(self, D_alpha_packed: torch.Tensor):
         """G = J - K for the RHF alpha density (J from 2 D_alpha, K from D_alpha)."""
@@ -411,12 +411,16 @@ def _batched_diis(Fh: torch.Tensor, Eh: torch.Tensor, n: int) -> torch.Tensor:
 
 def scf_rhf_batch(eng: BatchEngine, charges: Optional[Sequence[int]] = None, diis: int = 8, etol: float = 1e-10,
                   dtol: float = 1e-8, max_iter: int = 100, tau: float = 1e-12, rebuild_every: int = 12,
-                  finish_factor: float = 100.0, use_graph: bool = True, autotune: bool = False) -> BatchSCFResult:
+                  finish_factor: float = 100.0, use_graph: bool = True, autotune: bool = False,
+                  persist: bool = False) -> BatchSCFResult:
     """Closed-shell SCF of every molecule of the batch at once (same criteria
     as scf.scf_rhf: DIIS(8), |dE| < etol and RMS(dD) < dtol on a full FP64
     Fock build, incremental builds F_k = F_{k-1} + G(D_k - D_{k-1}) in between,
     full builds every ``rebuild_every`` iterations and once RMS(dD) <
-    finish_factor x dtol)."""
+    finish_factor x dtol).  ``persist``: each Fock build is one selection
+    launch plus one persistent launch over every molecule's quartet tiles of
+    every class (DFTK_JK_PERSIST) instead of a selection and a class kernel per
+    class."""
     dev = eng.device
     t_start = time.perf_counter()
     B, Nm = eng.n_mol, eng.n_max
@@ -450,12 +454,12 @@ def scf_rhf_batch(eng: BatchEngine, charges: Optional[Sequence[int]] = None, dii
 
         Dp0 = eng.to_packed(D)
         _autotune.tune(eng, lambda: eng.jk(2.0 * Dp0, Dp0, tau=tau), _autotune.FAMILY_JK, repeats=1)
-    graph = _FockGraph(eng, tau) if use_graph else None
+    graph = _FockGraph(eng, tau, persist) if use_graph else None
 
     def build(Dp):
         if graph is not None:
             return graph.run(Dp)
-        J, K, _ = eng.jk(2.0 * Dp, Dp, tau=tau)
+        J, K, _ = eng.jk(2.0 * Dp, Dp, tau=tau, persist=persist)
         return J - K
 
     Fh = torch.zeros((diis, B, Nm, Nm), dtype=torch.float64, device=dev)

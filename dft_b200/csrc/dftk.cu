@@ -421,6 +421,38 @@ size_t ws_list_bytes(int ns, int n_ao, const dftk_queue_t *q)
     return b;
 }
 
+// The persistent class kernel: every block resident (SM count x MINB blocks
+// of 128 threads).  MINB (the register cap shared by all classes) comes from
+// DFTK_PERSIST_MINB64 / DFTK_PERSIST_MINB32 (instantiated: FP64 4 or 6,
+// FP32 6 or 8; defaults 4 and 6).
+template <typename T>
+int launch_jk_persist(const JkParams &P, cudaStream_t s)
+{
+    static int minb64 = -1, minb32 = -1;
+    if (minb64 < 0) {
+        const char *e = getenv("DFTK_PERSIST_MINB64");
+        minb64 = (e && atoi(e) == 6) ? 6 : 4;
+        e = getenv("DFTK_PERSIST_MINB32");
+        minb32 = (e && atoi(e) == 8) ? 8 : 6;
+    }
+    const int slot = sizeof(T) == 4 ? DFTK_N_QCLASS : 0;
+    if (g_timing.enabled) DFTK_CUDA(cudaEventRecord(g_timing.start[slot], s));
+    if constexpr (sizeof(T) == 8) {
+        if (minb64 == 6) k_jk_persist<double, 6><<<(unsigned)(sm_count() * 6), 128, 0, s>>>(P);
+        else k_jk_persist<double, 4><<<(unsigned)(sm_count() * 4), 128, 0, s>>>(P);
+    } else {
+        if (minb32 == 8) k_jk_persist<float, 8><<<(unsigned)(sm_count() * 8), 128, 0, s>>>(P);
+        else k_jk_persist<float, 6><<<(unsigned)(sm_count() * 6), 128, 0, s>>>(P);
+    }
+    DFTK_LAUNCHED("k_jk_persist");
+    if (g_timing.enabled) {
+        DFTK_CUDA(cudaEventRecord(g_timing.stop[slot], s));
+        g_timing.launched[slot] = true;
+        for (int c = 1; c < DFTK_N_QCLASS; ++c) g_timing.launched[slot + c] = false;
+    }
+    return DFTK_OK;
+}
+
 template <typename T>
 int launch_jk_all(const JkParams &P, cudaStream_t s)
 {
@@ -862,10 +894,27 @@ int dftk_jk(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N_PCLASS]
             P.list[c] = (int2 *)cur;
             if (P.total[c] > 0) cur += (((size_t)P.total[c] * sizeof(int2)) + 255) & ~(size_t)255;
         }
-        DFTK_CUDA(cudaMemsetAsync(P.heads, 0, 2 * DFTK_N_QCLASS * sizeof(unsigned long long), s));
+        // list counters, then the persistent kernel's two work counters
+        DFTK_CUDA(cudaMemsetAsync(P.heads, 0, (2 * DFTK_N_QCLASS + 2) * sizeof(unsigned long long), s));
         P.tau = tau;
         P.tau32 = mixed ? tau_fp32 : tau;
         P.counts = counts;
+        if (flags & DFTK_JK_PERSIST) {
+            // one selection launch over every class, then one persistent launch per precision
+            long long tiles = 0;
+            for (int c = 0; c < DFTK_N_QCLASS; ++c) tiles += (P.total[c] + SELECT_TILE - 1) / SELECT_TILE;
+            if (tiles > 0) {
+                long long sb = tiles < 148LL * 8 ? tiles : 148LL * 8;
+                k_select_all<<<(unsigned)sb, SELECT_THREADS, 0, s>>>(P);
+                DFTK_LAUNCHED("k_select_all");
+                if ((st = launch_jk_persist<double>(P, s))) return st;
+                if (mixed) {
+                    P.counts = counts ? counts + DFTK_N_QCLASS : nullptr;
+                    if ((st = launch_jk_persist<float>(P, s))) return st;
+                }
+            }
+            return launch_symmetrize(*shells, Y, Za, Zb, J, K_a, K_b, uhf, s);
+        }
         // per class on its stream: selection, then the FP64 (and FP32) list kernel
         cudaStream_t cls[DFTK_N_QCLASS];
         int n_aux = 0;

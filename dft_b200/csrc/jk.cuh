@@ -477,18 +477,18 @@ __device__ __forceinline__ void select_classify(const JkParams &P, long long can
     is32 = active && !is64 && bound >= P.tau;
 }
 
+// One tile of class C's candidates (the block's SELECT_TILE consecutive
+// candidates starting at tile * SELECT_TILE).
 template <int C>
-__global__ void __launch_bounds__(SELECT_THREADS) k_select(const JkParams P)
+__device__ __forceinline__ void select_tile(const JkParams &P, long long tile, unsigned *s_cnt64, unsigned *s_cnt32,
+                                            unsigned long long &s_base64, unsigned long long &s_base32)
 {
-    __shared__ unsigned s_cnt64[SELECT_THREADS / 32], s_cnt32[SELECT_THREADS / 32];
-    __shared__ unsigned long long s_base64, s_base32;
     const long long ncand = P.total[C];
     const long long cap = ncand;
-    const long long ntiles = (ncand + SELECT_TILE - 1) / SELECT_TILE;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned below = (1u << lane) - 1u;
     const long long *off = P.row_off[C];
-    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    {
         const long long wfirst = tile * SELECT_TILE + (long long)warp * 32 * SELECT_PER_WARP;
         int r0 = 0;
         if (lane == 0 && wfirst < ncand) r0 = find_row(off, P.n_rows[C], wfirst);
@@ -545,6 +545,42 @@ __global__ void __launch_bounds__(SELECT_THREADS) k_select(const JkParams P)
             p32 += __popc(m32[it]);
         }
         __syncthreads();  // s_base/s_cnt are rewritten by the next tile
+    }
+}
+
+template <int C>
+__global__ void __launch_bounds__(SELECT_THREADS) k_select(const JkParams P)
+{
+    __shared__ unsigned s_cnt64[SELECT_THREADS / 32], s_cnt32[SELECT_THREADS / 32];
+    __shared__ unsigned long long s_base64, s_base32;
+    const long long ntiles = (P.total[C] + SELECT_TILE - 1) / SELECT_TILE;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+        select_tile<C>(P, tile, s_cnt64, s_cnt32, s_base64, s_base32);
+}
+
+// All classes' selection passes in one launch: block b takes tile b of the
+// concatenated tile ranges (tile_base[c] .. tile_base[c + 1] for class c),
+// grid-striding over the total.
+__global__ void __launch_bounds__(SELECT_THREADS) k_select_all(const JkParams P)
+{
+    __shared__ unsigned s_cnt64[SELECT_THREADS / 32], s_cnt32[SELECT_THREADS / 32];
+    __shared__ unsigned long long s_base64, s_base32;
+    long long base[DFTK_N_QCLASS + 1];
+    base[0] = 0;
+#pragma unroll
+    for (int c = 0; c < DFTK_N_QCLASS; ++c) base[c + 1] = base[c] + (P.total[c] + SELECT_TILE - 1) / SELECT_TILE;
+    for (long long t = blockIdx.x; t < base[DFTK_N_QCLASS]; t += gridDim.x) {
+        int c = 0;
+        while (t >= base[c + 1]) ++c;
+        const long long tile = t - base[c];
+        switch (c) {
+        case 0: select_tile<0>(P, tile, s_cnt64, s_cnt32, s_base64, s_base32); break;
+        case 1: select_tile<1>(P, tile, s_cnt64, s_cnt32, s_base64, s_base32); break;
+        case 2: select_tile<2>(P, tile, s_cnt64, s_cnt32, s_base64, s_base32); break;
+        case 3: select_tile<3>(P, tile, s_cnt64, s_cnt32, s_base64, s_base32); break;
+        case 4: select_tile<4>(P, tile, s_cnt64, s_cnt32, s_base64, s_base32); break;
+        default: select_tile<5>(P, tile, s_cnt64, s_cnt32, s_base64, s_base32); break;
+        }
     }
 }
 
@@ -623,6 +659,77 @@ __global__ void __launch_bounds__(128, JkMinBlocks<C, T>::value) k_jk_list(const
             if (split == 0) jk_one<C, T, 0>(P, valid, row, ket);
             else if (split == 1) jk_one<C, T, 1>(P, valid, row, ket);
             else jk_one<C, T, 2>(P, valid, row, ket);
+        }
+    }
+}
+
+// One 32-entry tile of class C's list in precision T (split S of the c
+// components for the split class): the body of k_jk_list for one warp.
+template <int C, typename T>
+__device__ __forceinline__ void list_tile(const JkParams &P, long long t)
+{
+    constexpr int NS = EriClass<T, C, 0>::NSPLIT;
+    constexpr bool fp32 = sizeof(T) == 4;
+    const long long n = (long long)P.heads[(fp32 ? DFTK_N_QCLASS : 0) + C];
+    const long long cap = P.total[C];
+    const int lane = threadIdx.x & 31;
+    const int split = (int)(t % NS);
+    const long long idx = (t / NS) * 32 + lane;
+    const bool valid = idx < n;
+    int row = 0, ket = 0;
+    if (valid) {
+        const int2 e = __ldg(P.list[C] + (fp32 ? cap - 1 - idx : idx));
+        row = e.x;
+        ket = e.y;
+    }
+    if constexpr (NS == 1) {
+        jk_one<C, T, 0>(P, valid, row, ket);
+    } else {
+        if (split == 0) jk_one<C, T, 0>(P, valid, row, ket);
+        else if (split == 1) jk_one<C, T, 1>(P, valid, row, ket);
+        else jk_one<C, T, 2>(P, valid, row, ket);
+    }
+}
+
+// Persistent J/K over the selected quartets of every class in precision T:
+// a grid of resident blocks whose warps pull 32-entry tiles from one device
+// work counter (P.heads[2 * DFTK_N_QCLASS + fp32]) over the concatenated
+// tile ranges of all classes, heaviest class first, so the classes share the
+// SMs without a launch per class and the tail of each class overlaps the next.
+// MINB caps the registers of the whole kernel (every class runs under it).
+template <typename T, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_jk_persist(const JkParams P)
+{
+    constexpr bool fp32 = sizeof(T) == 4;
+    constexpr int order[DFTK_N_QCLASS] = {5, 4, 3, 2, 1, 0};
+    constexpr int nsplit[DFTK_N_QCLASS] = {EriClass<T, 0, 0>::NSPLIT, EriClass<T, 1, 0>::NSPLIT,
+                                           EriClass<T, 2, 0>::NSPLIT, EriClass<T, 3, 0>::NSPLIT,
+                                           EriClass<T, 4, 0>::NSPLIT, EriClass<T, 5, 0>::NSPLIT};
+    long long base[DFTK_N_QCLASS + 1];
+    base[0] = 0;
+#pragma unroll
+    for (int k = 0; k < DFTK_N_QCLASS; ++k) {
+        const int c = order[k];
+        const long long n = (long long)P.heads[(fp32 ? DFTK_N_QCLASS : 0) + c];
+        base[k + 1] = base[k] + ((n + 31) >> 5) * nsplit[c];
+    }
+    unsigned long long *ctr = P.heads + 2 * DFTK_N_QCLASS + (fp32 ? 1 : 0);
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        unsigned long long t = 0;
+        if (lane == 0) t = atomicAdd(ctr, 1ull);
+        t = __shfl_sync(DFTK_FULL_MASK, t, 0);
+        if ((long long)t >= base[DFTK_N_QCLASS]) break;
+        int k = 0;
+        while ((long long)t >= base[k + 1]) ++k;
+        const long long local = (long long)t - base[k];
+        switch (order[k]) {
+        case 0: list_tile<0, T>(P, local); break;
+        case 1: list_tile<1, T>(P, local); break;
+        case 2: list_tile<2, T>(P, local); break;
+        case 3: list_tile<3, T>(P, local); break;
+        case 4: list_tile<4, T>(P, local); break;
+        default: list_tile<5, T>(P, local); break;
         }
     }
 }

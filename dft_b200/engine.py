@@ -318,7 +318,8 @@ class IntegralEngine:
 
     def jk(self, D: torch.Tensor, D_a: Optional[torch.Tensor] = None, D_b: Optional[torch.Tensor] = None,
            uhf: bool = False, mixed: bool = False, tau: float = 1e-14, tau_fp32: float = 1e-6,
-           out=None, counts: Optional[torch.Tensor] = None, scan: bool = False, queue=None):
+           out=None, counts: Optional[torch.Tensor] = None, scan: bool = False, queue=None,
+           persist: bool = False):
         """Direct J, K_a (, K_b) for densities on the device.
 
         D is the density J is built from (the reference's P = P_a + P_b);
@@ -326,7 +327,9 @@ class IntegralEngine:
         ``uhf``, K_b uses D_b.  Returns (J, K_a, K_b) with K_b = K_a unless uhf.
         ``scan`` hands dftk_jk only the base workspace, which selects its
         direct path (class kernels scan the candidates themselves) instead of
-        the selection pass + quartet lists.
+        the selection pass + quartet lists; ``persist`` runs the list path as
+        one selection launch and one persistent launch per precision
+        (DFTK_JK_PERSIST).
         """
         N = self.n_ao
         dev = self.device
@@ -342,7 +345,7 @@ class IntegralEngine:
             Kb = torch.empty((N, N), dtype=torch.float64, device=dev) if uhf else None
         else:
             J, Ka, Kb = out
-        flags = (_lib.JK_UHF if uhf else 0) | (_lib.JK_MIXED if mixed else 0)
+        flags = (_lib.JK_UHF if uhf else 0) | (_lib.JK_MIXED if mixed else 0) | (_lib.JK_PERSIST if persist else 0)
         if self.has_hl and queue is not None:
             raise _basis.UnsupportedBasis("jk(queue=...): sharded builds cover s/p bases")
         _lib.call("dftk_jk", ctypes.byref(self.c_shells), self.c_pairs,

@@ -53,6 +53,11 @@ enum {
 /* dftk_jk flags */
 #define DFTK_JK_UHF 1          /* K_a from D_a and K_b from D_b; else K_b untouched and D_b unused */
 #define DFTK_JK_MIXED 2        /* FP32 for quartets with Q_ab Q_cd Dmax < tau_fp32 */
+#define DFTK_JK_PERSIST 4      /* list path: one selection launch over every class, then one persistent
+                                  launch per precision whose warps pull 32-quartet tiles of all classes
+                                  (heaviest first) from a device work counter, instead of a selection
+                                  and a class kernel per class (timing hook: slot 0 / 6 holds the
+                                  persistent FP64 / FP32 launch) */
 
 /* Quartet classes, in the order dftk_jk and dftk_queue_t use them:
  * 0 (ss|ss), 1 (ps|ss), 2 (ps|ps), 3 (pp|ss), 4 (pp|ps), 5 (pp|pp). */

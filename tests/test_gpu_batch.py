@@ -87,3 +87,29 @@ def test_batch_gradient_matches_single():
         E, g = energy_and_gradient(atoms, c, etol=1e-11, dtol=1e-9)
         assert abs(E - res.energy[m]) < 1e-8
         assert np.abs(grads[m] - g).max() < 1e-7, np.abs(grads[m] - g).max()
+
+
+def test_persistent_launch_matches_class_launches():
+    """DFTK_JK_PERSIST (one selection launch, one persistent launch per
+    precision pulling tiles of every class) gives the class-by-class build's
+    J/K: a packed batch (FP64) and one molecule (FP64 and mixed)."""
+    mols = _molecules()
+    eng = BatchEngine(mols, tau_schwarz=1e-12)
+    rng = np.random.default_rng(5)
+    Dp = torch.as_tensor(0.05 * rng.normal(size=eng.mat_elems), device=eng.device)
+    blocks = [eng.block(Dp, m) for m in range(eng.n_mol)]
+    for m, b in enumerate(blocks):  # symmetric per-molecule blocks
+        b.copy_(0.5 * (b + b.T))
+    J0, K0, _ = eng.jk(2 * Dp, Dp, tau=1e-14)
+    J1, K1, _ = eng.jk(2 * Dp, Dp, tau=1e-14, persist=True)
+    assert torch.abs(J1 - J0).max().item() < 1e-12 and torch.abs(K1 - K0).max().item() < 1e-12
+    atoms, centers = geometry.water_cluster((2, 2, 2))
+    e1 = IntegralEngine(basis.build_shells(basis.load_basis(), atoms, centers))
+    N = e1.n_ao
+    M = rng.normal(size=(N, N))
+    D = torch.as_tensor(0.05 * (M + M.T), device=e1.device)
+    for mixed in (False, True):
+        a = e1.jk(2 * D, D, mixed=mixed, tau=1e-12, tau_fp32=1e-4)
+        b = e1.jk(2 * D, D, mixed=mixed, tau=1e-12, tau_fp32=1e-4, persist=True)
+        for x, y in zip(a[:2], b[:2]):
+            assert torch.abs(x - y).max().item() < 1e-11
