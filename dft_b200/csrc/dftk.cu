@@ -743,13 +743,13 @@ int dftk_grid_ao(const dftk_shells_t *shells, long long n_points, const float *p
     DFTK_INIT();
     if (n_points == 0 || shells->n_shells == 0) return DFTK_OK;
     if ((n_points + 127) / 128 > 0x7fffffffLL) return fail(DFTK_ERR_SIZE, "dftk_grid_ao: too many points in one call");
-    // momenta beyond p have no AO code here: refuse them before launch
+    // momenta beyond f have no AO code here: refuse them before launch
     std::vector<int> l(shells->n_shells);
     DFTK_CUDA(cudaMemcpyAsync(l.data(), shells->l, sizeof(int) * l.size(), cudaMemcpyDeviceToHost,
                               (cudaStream_t)stream));
     DFTK_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
     for (int v : l)
-        if (v < 0 || v > 1) return fail(DFTK_ERR_UNSUPPORTED, "dftk_grid_ao: shells beyond p");
+        if (v < 0 || v > HL_LMAX) return fail(DFTK_ERR_UNSUPPORTED, "dftk_grid_ao: shells beyond f");
     k_grid_ao<<<blocks_for(n_points, 128), 128, 0, (cudaStream_t)stream>>>(*shells, n_points, points, ao, ld);
     DFTK_LAUNCHED("k_grid_ao");
     return DFTK_OK;

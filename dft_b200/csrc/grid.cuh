@@ -5,10 +5,11 @@
 // k_grid_ao: one thread per point, all shells of the molecule in order (the
 // shell table is read as warp-uniform broadcasts).  Like the reference, the
 // point comes in FP32 and everything after the centre difference is FP64:
-//   ao[a][g] = x^i y^j z^k * sum_p cn_p exp(-alpha_p r^2)
-// with cn_p = contraction coefficient x primitive normalisation (the same for
-// every component of an s or p shell).  Rows are AOs, columns points, so the
-// stores of a warp are contiguous.
+//   ao[a][g] = x^i y^j z^k * sum_p cn_p exp(-alpha_p r^2) * g(i, j, k)
+// with cn_p = contraction coefficient x radial norm and g the component's
+// 1/sqrt(prod (2 l_i - 1)!!) (1 for s and p); shells up to f, a generally
+// contracted shell arriving as one shell per contraction row.  Rows are AOs,
+// columns points, so the stores of a warp are contiguous.
 //
 // k_grid_density: psi_a, psi_b are the MO values (rows = orbitals); for
 // orbital k < n_mo and point g
@@ -17,6 +18,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "hl.cuh"
 
 __global__ void __launch_bounds__(128) k_grid_ao(const dftk_shells_t sh, long long n, const float *pts, double *ao,
                                                  long long ld)
@@ -40,8 +42,17 @@ __global__ void __launch_bounds__(128) k_grid_ao(const dftk_shells_t sh, long lo
             row[0] = dx * rad;
             row[ld] = dy * rad;
             row[2 * ld] = dz * rad;
+        } else if (l <= HL_LMAX) {
+            const int nc = hl_ncomp(l);
+            for (int k = 0; k < nc; ++k) {
+                double v = 1.0;
+                for (int i = 0; i < hl_pow(l, k, 0); ++i) v *= dx;
+                for (int i = 0; i < hl_pow(l, k, 1); ++i) v *= dy;
+                for (int i = 0; i < hl_pow(l, k, 2); ++i) v *= dz;
+                row[(long long)k * ld] = v * rad * c_hl_cnorm[l][k];
+            }
         }
-        // other momenta are rejected by the host before launch
+        // momenta beyond f are rejected by the host before launch
     }
 }
 

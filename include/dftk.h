@@ -222,10 +222,11 @@ int dftk_one_electron(const dftk_shells_t *shells, int n_atoms, const double *at
 
 /* AO values at points (the AO loop of the reference's orbital evaluation,
  * shelled_eval.py:88-107): ao[a * ld + g] = x^i y^j z^k sum_p cn_p
- * exp(-alpha_p r^2) for every AO a of the molecule and point g < n_points,
- * with (x, y, z) = point g - the shell centre.  Points are FP32 xyz triples
- * (the reference's grid dtype), the arithmetic and ao are FP64.  One molecule
- * (shells->n_mol == 0) with s and p shells (else DFTK_ERR_UNSUPPORTED); ao
+ * exp(-alpha_p r^2) / sqrt(prod (2 l_i - 1)!!) for every AO a of the molecule
+ * and point g < n_points, with (x, y, z) = point g - the shell centre.  Points
+ * are FP32 xyz triples (the reference's grid dtype), the arithmetic and ao
+ * are FP64.  One molecule (shells->n_mol == 0) with shells up to f (else
+ * DFTK_ERR_UNSUPPORTED); ao
  * holds shells->n_ao rows of ld >= n_points doubles.  Reads shells->l back to
  * the host to check the momenta (synchronises the stream). */
 int dftk_grid_ao(const dftk_shells_t *shells, long long n_points, const float *points, double *ao,

@@ -27,6 +27,7 @@ Usage::
     python tests/golden/make_golden.py br2            # d shells (STO-3G Br2)
     python tests/golden/make_golden.py gc             # general contractions + d (H2O, test basis)
     python tests/golden/make_golden.py gcf            # the same with f (O) and d (H) shells
+    python tests/golden/make_golden.py grid_gc        # grid evaluation on the generally contracted H2O
 """
 from __future__ import annotations
 
@@ -311,15 +312,18 @@ def patched_eval(spacing=0.15, chunk=500):
     return text
 
 
-def case_grid(out_dir):
+def case_grid(out_dir, basis_file=None, prefix="h2o"):
     """Orbital densities on a grid for H2O: the reference SCF (its own
     thresholds) writes its evaluation checkpoint, then the reference's
     evaluation script runs on it.  Writes the checkpoint file as it is and the
-    grid, total and phase densities."""
+    grid, total and phase densities.  With basis_file (a test basis in
+    tests/golden/) the checkpoint carries d shells, general contractions and a
+    non-identity spherical transform A."""
     import shutil
 
     atoms, centers = geometry.water()
-    ns, work = run_reference(atoms, centers)
+    ns, work = run_reference(atoms, centers,
+                             basis_path=os.path.join(HERE, basis_file) if basis_file else None)
     ckpt = os.path.join(work, "eval_checkpoints", "gadolinium_3_fluoride_eval_checkpoint.npz")
     os.makedirs(os.path.join(work, "preprocess"))
     cwd = os.getcwd()
@@ -335,19 +339,20 @@ def case_grid(out_dir):
            "total_density": np.load(os.path.join(pre, "total_density.npy")),
            "phase_density": np.load(os.path.join(pre, "phase_density.npy")),
            "energy": float(ns["E_total_new"])}
-    np.savez_compressed(os.path.join(out_dir, "grid_h2o.npz"), **res)
-    shutil.copyfile(ckpt, os.path.join(out_dir, "h2o_eval_checkpoint.npz"))
+    np.savez_compressed(os.path.join(out_dir, f"grid_{prefix}.npz"), **res)
+    shutil.copyfile(ckpt, os.path.join(out_dir, f"{prefix}_eval_checkpoint.npz"))
     print("grid", res["grid"].shape, "total", res["total_density"].shape, "energy", res["energy"])
 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["h2o", "c10h22", "h2o64", "grid", "br2", "gc", "gcf"])
+    ap.add_argument("case", choices=["h2o", "c10h22", "h2o64", "grid", "br2", "gc", "gcf", "grid_gc"])
     ap.add_argument("--out", default=HERE)
     args = ap.parse_args()
     install_fake_cupy()
     {"h2o": case_h2o, "c10h22": case_c10h22, "h2o64": case_h2o64, "grid": case_grid, "br2": case_dshell,
-     "gc": case_gc, "gcf": lambda out: case_gc(out, "dzf_gc_test.json", "h2o_gcf.npz")}[args.case](args.out)
+     "gc": case_gc, "gcf": lambda out: case_gc(out, "dzf_gc_test.json", "h2o_gcf.npz"),
+     "grid_gc": lambda out: case_grid(out, "dz_gc_test.json", "h2o_gc")}[args.case](args.out)
 
 
 if __name__ == "__main__":

@@ -35,6 +35,21 @@ def test_grid_h2o_matches_reference_script():
     _close(p2, phase)
 
 
+def test_grid_d_shells_general_contractions_match_reference_script():
+    """The reference's evaluation script on the checkpoint its SCF wrote for
+    H2O with the generally contracted, d-polarised test basis: d shells,
+    contraction matrices and the spherical transform A in the checkpoint."""
+    from dft_b200 import grid
+
+    g = load_golden("grid_h2o_gc.npz")
+    ck = grid.load_eval_checkpoint(os.path.join(GOLDEN, "h2o_gc_eval_checkpoint.npz"))
+    assert max(s["angular_momentum"] for s in ck["shells"]) == 2
+    assert ck["A"].shape[0] < ck["A"].shape[1]
+    total, phase = grid.OrbitalGrid(ck).evaluate(g["grid"], chunk_size=500)
+    _close(total, g["total_density"])
+    _close(phase, g["phase_density"])
+
+
 def test_grid_open_shell_c10h22_against_oracle(oracle_mod):
     """A 72-AO molecule with distinct alpha/beta coefficients and N_a != N_b."""
     from dft_b200 import basis, geometry, grid

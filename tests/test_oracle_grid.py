@@ -34,6 +34,18 @@ def test_oracle_grid_matches_reference_script(oracle_mod):
                                atol=1e-12 * float(total.max()))
 
 
+def test_oracle_grid_d_shells_matches_reference_script(oracle_mod):
+    """The evaluation script's densities for the checkpoint with d shells,
+    general contractions and a spherical transform A."""
+    from dft_b200 import grid
+
+    g = load_golden("grid_h2o_gc.npz")
+    ck = grid.load_eval_checkpoint(os.path.join(GOLDEN, "h2o_gc_eval_checkpoint.npz"))
+    total, phase = oracle_mod.grid_densities(ck, g["grid"])
+    _close(total, g["total_density"])
+    _close(phase, g["phase_density"])
+
+
 def test_reference_grid_reproduces_script_grid():
     from dft_b200 import grid
 
