@@ -897,9 +897,10 @@ def run_dftk_arm(args, rank, world, local_rank):
                       "delta_E_uEh_final": abs(rmx.energy - r64.energy) * 1e6,
                       "delta_E_uEh_last_mixed_build": abs(rmx.energy_last_build - r64.energy) * 1e6,
                       "quartets_fp64_fp32_mixed": rmx.counts},
-            "autotune": {"shapes_threads_x_blocks_per_sm": tuned["shapes"],
+            "autotune": {"shapes_threads_x_blocks_per_sm": tuned["shapes"], "tiles": tuned.get("tiles"),
                          "default_class_ms": tuned["default_ms"], "tuned_class_ms": tuned["tuned_ms"],
-                         "fp32_shapes": tuned32["shapes"], "fp32_default_class_ms": tuned32["default_ms"],
+                         "fp32_shapes": tuned32["shapes"], "fp32_tiles": tuned32.get("tiles"),
+                         "fp32_default_class_ms": tuned32["default_ms"],
                          "fp32_tuned_class_ms": tuned32["tuned_ms"]},
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,

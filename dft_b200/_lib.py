@@ -30,7 +30,8 @@ SYMBOLS = (
     "dftk_jk_workspace_bytes", "dftk_jk_workspace_bytes_queue", "dftk_jk", "dftk_nuclear_kernel", "dftk_eri_kernel",
     "dftk_fma_burn", "dftk_jk_timing", "dftk_jk_timing_read", "dftk_jk_noalloc", "dftk_grad", "dftk_workspace_bytes",
     "dftk_set_launch", "dftk_get_launch", "dftk_grid_ao", "dftk_grid_density", "dftk_prepare_bytes", "dftk_prepare",
-    "dftk_hl_schwarz", "dftk_jk_hl", "dftk_hl_eri_blocks",
+    "dftk_hl_schwarz", "dftk_jk_hl", "dftk_hl_eri_blocks", "dftk_set_tile", "dftk_get_tile",
+    "dftk_prepare_hl_bytes", "dftk_prepare_hl",
 )
 
 
@@ -143,6 +144,10 @@ def load() -> ctypes.CDLL:
         "dftk_workspace_bytes": ([ctypes.POINTER(Shells), ctypes.POINTER(Queue)], sz),
         "dftk_set_launch": ([i, i, i, i, i], i),
         "dftk_get_launch": ([i, i, i, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)], i),
+        "dftk_set_tile": ([i, i, i], i),
+        "dftk_prepare_hl_bytes": ([ctypes.POINTER(Shells), ctypes.POINTER(ctypes.c_size_t)], i),
+        "dftk_prepare_hl": ([ctypes.POINTER(Shells), d, d, vp, sz, ctypes.POINTER(HlSet), vp], i),
+        "dftk_get_tile": ([i, i, ctypes.POINTER(ctypes.c_int)], i),
         "dftk_jk": ([ctypes.POINTER(Shells), ctypes.POINTER(Pairs), ctypes.POINTER(Queue), vp, vp, vp,
                      vp, vp, vp, i, d, d, vp, sz, vp, vp], i),
         "dftk_nuclear_kernel": ([vp] * 8 + [i, i, i] + [vp] * 9 + [vp], i),

@@ -11,6 +11,12 @@ every candidate shape is applied to all classes at once, one build is timed
 per class with CUDA events (``dftk_jk_timing``), and each class keeps its
 fastest shape.  Results are cached in memory per (device, workload
 signature) and can be saved to / loaded from a JSON file.
+
+The J/K family has a third dimension, the tile: how many consecutive
+32-quartet work items a warp takes per step of its loop (1, 2, 4, 8), i.e.
+how long a warp stays on neighbouring list entries (shared bra pairs); with
+the shapes chosen, every tile is timed the same way and each class keeps its
+fastest.
 """
 from __future__ import annotations
 
@@ -27,6 +33,7 @@ from . import _lib
 FAMILY_JK, FAMILY_GRAD = 0, 1
 N_QCLASS = 6
 CANDIDATES: Tuple[Tuple[int, int], ...] = ((128, 4), (128, 8), (128, 16), (128, 32), (64, 8), (64, 16), (64, 32))
+TILES: Tuple[int, ...] = (1, 2, 4, 8)
 
 _cache: Dict[str, Dict] = {}
 
@@ -43,6 +50,20 @@ def get_shapes(family: int, fp32: bool = False) -> List[Tuple[int, int]]:
 def set_shapes(family: int, shapes: Sequence[Tuple[int, int]], fp32: bool = False) -> None:
     for c, (t, b) in enumerate(shapes):
         _lib.call("dftk_set_launch", family, c, int(fp32), int(t), int(b))
+
+
+def get_tiles(fp32: bool = False) -> List[int]:
+    out = []
+    for c in range(N_QCLASS):
+        t = ctypes.c_int()
+        _lib.call("dftk_get_tile", c, int(fp32), ctypes.byref(t))
+        out.append(t.value)
+    return out
+
+
+def set_tiles(tiles: Sequence[int], fp32: bool = False) -> None:
+    for c, t in enumerate(tiles):
+        _lib.call("dftk_set_tile", c, int(fp32), int(t))
 
 
 def _signature(engine, family: int, fp32: bool) -> str:
@@ -78,6 +99,8 @@ def tune(engine, run, family: int = FAMILY_JK, fp32: bool = False,
         res = _cache[key]
         if apply:
             set_shapes(family, res["shapes"], fp32)
+            if "tiles" in res:
+                set_tiles(res["tiles"], fp32)
         return res
     default = get_shapes(family, fp32)
     run()  # warm-up
@@ -100,9 +123,27 @@ def tune(engine, run, family: int = FAMILY_JK, fp32: bool = False,
            "ms": {f"{t}x{b}": [float(x) for x in v] for (t, b), v in table.items()},
            "default_ms": [float(x) for x in base],
            "tuned_ms": tuned}
+    if family == FAMILY_JK:
+        # the tile, with the chosen shapes in place
+        set_shapes(family, res["shapes"], fp32)
+        default_tiles = get_tiles(fp32)
+        ttab = {}
+        try:
+            for t in TILES:
+                set_tiles([t] * N_QCLASS, fp32)
+                ttab[t] = _time_classes(run, repeats, fp32)
+        finally:
+            set_tiles(default_tiles, fp32)
+            set_shapes(family, default, fp32)
+        tiles = [min(TILES, key=lambda t: ttab[t][c]) for c in range(N_QCLASS)]
+        res["tiles"] = tiles
+        res["tile_ms"] = {str(t): [float(x) for x in v] for t, v in ttab.items()}
+        res["tuned_ms"] = [min(tuned[c], float(ttab[tiles[c]][c])) for c in range(N_QCLASS)]
     _cache[key] = res
     if apply:
         set_shapes(family, res["shapes"], fp32)
+        if "tiles" in res:
+            set_tiles(res["tiles"], fp32)
     return res
 
 

@@ -162,6 +162,7 @@ int ensure_init()
 struct LaunchShape {
     int threads;
     int blocks_per_sm;
+    int tile = 1;  // J/K list kernels: consecutive 32-entry work items per warp step
 };
 LaunchShape g_shape[DFTK_N_FAMILY][DFTK_N_QCLASS][2];
 bool g_shape_init = false;
@@ -173,8 +174,8 @@ void init_shapes_locked()
     if (g_shape_init) return;
     for (int c = 0; c < DFTK_N_QCLASS; ++c)
         for (int p = 0; p < 2; ++p) {
-            g_shape[DFTK_FAMILY_JK][c][p] = {128, 16};
-            g_shape[DFTK_FAMILY_GRAD][c][p] = {128, 8};
+            g_shape[DFTK_FAMILY_JK][c][p] = {128, 16, 1};
+            g_shape[DFTK_FAMILY_GRAD][c][p] = {128, 8, 1};
         }
     g_shape_init = true;
 }
@@ -576,7 +577,7 @@ int prepare_plan(const dftk_shells_t *shells, PreparePlan &pl)
     }
     int pmax = 1;
     for (int i = 0; i < ns; ++i) {
-        if (l[i] < 0 || l[i] > 1) return fail(DFTK_ERR_UNSUPPORTED, "dftk_prepare: shells beyond p");
+        if (l[i] < 0 || l[i] > HL_LMAX) return fail(DFTK_ERR_UNSUPPORTED, "dftk_prepare: shells beyond f");
         if (np[i] < 1) return fail(DFTK_ERR_ARG, "dftk_prepare: a shell without primitives");
         pmax = std::max(pmax, np[i]);
     }
@@ -586,6 +587,7 @@ int prepare_plan(const dftk_shells_t *shells, PreparePlan &pl)
         for (int j = 0; j <= i; ++j) {
             const bool swap = l[i] < l[j];
             const int a = swap ? j : i, b = swap ? i : j;
+            if (l[a] >= 2) continue;  // pairs with a d or f shell: dftk_prepare_hl
             auto &v = pl.ab[l[a] + l[b]];
             v.push_back(a);
             v.push_back(b);
@@ -607,9 +609,164 @@ int prepare_plan(const dftk_shells_t *shells, PreparePlan &pl)
     return DFTK_OK;
 }
 
+// The d/f part of a molecule's setup: the pairs with a d or f shell ("hi")
+// and every s/p pair ("lo") in the generic 13-field layout.
+struct PrepareHlPlan {
+    int kmax = 1, lmax = 2;
+    std::vector<int> ab[2];  // 0 hi, 1 lo
+    size_t off_ab[2], off_np[2], off_r64[2], off_r32[2], off_q[2], off_qp[2], off_row[2];
+    size_t bytes = 0;
+};
+
+int prepare_hl_plan(const dftk_shells_t *shells, PrepareHlPlan &pl)
+{
+    const int ns = shells->n_shells;
+    std::vector<int> l(ns), np(ns);
+    if (ns > 0) {
+        DFTK_CUDA(cudaMemcpy(l.data(), shells->l, sizeof(int) * ns, cudaMemcpyDeviceToHost));
+        DFTK_CUDA(cudaMemcpy(np.data(), shells->nprim, sizeof(int) * ns, cudaMemcpyDeviceToHost));
+    }
+    int pmax = 1;
+    for (int i = 0; i < ns; ++i) {
+        if (l[i] < 0 || l[i] > HL_LMAX) return fail(DFTK_ERR_UNSUPPORTED, "dftk_prepare_hl: shells beyond f");
+        if (np[i] < 1) return fail(DFTK_ERR_ARG, "dftk_prepare_hl: a shell without primitives");
+        pmax = std::max(pmax, np[i]);
+        pl.lmax = std::max(pl.lmax, l[i]);
+    }
+    pl.kmax = pmax * pmax;
+    if (pl.kmax > HL_MAX_KPAIR) return fail(DFTK_ERR_SIZE, "dftk_prepare_hl: more than 128 primitive pairs per pair");
+    for (int i = 0; i < ns; ++i)
+        for (int j = 0; j <= i; ++j) {
+            const bool swap = l[i] < l[j];
+            const int a = swap ? j : i, b = swap ? i : j;
+            auto &v = pl.ab[l[a] >= 2 ? 0 : 1];
+            v.push_back(a);
+            v.push_back(b);
+        }
+    size_t at = 0;
+    for (int k = 0; k < 2; ++k) {
+        const size_t n = pl.ab[k].size() / 2, rec = (size_t)HL_FIELDS * pl.kmax * n;
+        pl.off_ab[k] = carve(at, sizeof(int) * 2 * std::max<size_t>(n, 1));
+        pl.off_np[k] = carve(at, sizeof(int) * std::max<size_t>(n, 1));
+        pl.off_r64[k] = carve(at, sizeof(double) * std::max<size_t>(rec, 1));
+        pl.off_r32[k] = carve(at, sizeof(float) * std::max<size_t>(rec, 1));
+        pl.off_q[k] = carve(at, sizeof(double) * std::max<size_t>(n, 1));
+        pl.off_qp[k] = carve(at, sizeof(float) * std::max<size_t>((size_t)pl.kmax * n, 1));
+    }
+    for (int k = 0; k < 2; ++k) pl.off_row[k] = carve(at, sizeof(long long) * (pl.ab[0].size() / 2 + 1));
+    pl.bytes = at;
+    return DFTK_OK;
+}
+
+// Row offsets of one candidate space: bra row r keeps the ket prefix with
+// q_ket >= tau / q_bra[r] (both sorted descending), cut at k <= r when
+// `same` (bra and ket are one pair set) so each unique quartet appears once.
+std::vector<long long> prefix_offsets(const std::vector<double> &qx, const std::vector<double> &qy, bool same,
+                                      double tau)
+{
+    const size_t nr = qx.size(), nk = qy.size();
+    std::vector<long long> off(nr + 1, 0);
+    for (size_t r = 0; r < nr; ++r) {
+        long long cnt = 0;
+        if (nk > 0 && qx[r] > 0.0) {
+            const double thr = tau / qx[r];
+            size_t lo = 0, hi = nk;
+            while (lo < hi) {
+                const size_t mid = (lo + hi) / 2;
+                if (qy[mid] >= thr) lo = mid + 1;
+                else hi = mid;
+            }
+            cnt = (long long)lo;
+        }
+        if (same) cnt = std::min<long long>(cnt, (long long)r + 1);
+        off[r + 1] = off[r] + cnt;
+    }
+    return off;
+}
+
 }  // namespace
 
 extern "C" {
+
+int dftk_prepare_hl_bytes(const dftk_shells_t *shells, size_t *bytes)
+{
+    if (!shells || !bytes || shells->n_shells < 0 || (shells->n_shells > 0 && (!shells->l || !shells->nprim)))
+        return fail(DFTK_ERR_ARG, "dftk_prepare_hl_bytes: bad arguments");
+    if (shells->n_mol > 0) return fail(DFTK_ERR_UNSUPPORTED, "dftk_prepare_hl_bytes: one molecule at a time");
+    DFTK_INIT();
+    PrepareHlPlan pl;
+    const int st = prepare_hl_plan(shells, pl);
+    if (st != DFTK_OK) return st;
+    *bytes = pl.bytes;
+    return DFTK_OK;
+}
+
+int dftk_prepare_hl(const dftk_shells_t *shells, double tau_schwarz, double tau_prim, void *storage,
+                    size_t storage_bytes, dftk_hl_t *hl, dftk_stream_t stream)
+{
+    if (!shells || !hl || !(tau_schwarz >= 0.0) || !(tau_prim >= 0.0) || shells->n_shells < 0 ||
+        (shells->n_shells > 0 && (!shells->l || !shells->nprim)))
+        return fail(DFTK_ERR_ARG, "dftk_prepare_hl: bad arguments");
+    if (shells->n_mol > 0) return fail(DFTK_ERR_UNSUPPORTED, "dftk_prepare_hl: one molecule at a time");
+    DFTK_INIT();
+    cudaStream_t s = (cudaStream_t)stream;
+    DFTK_CUDA(cudaStreamSynchronize(s));
+    PrepareHlPlan pl;
+    int st = prepare_hl_plan(shells, pl);
+    if (st != DFTK_OK) return st;
+    if (!storage || storage_bytes < pl.bytes) return fail(DFTK_ERR_WORKSPACE, "dftk_prepare_hl: storage too small");
+    char *base = (char *)storage;
+    std::vector<double> qs[2];
+    dftk_pairs_t *sets[2] = {&hl->hi, &hl->lo};
+    for (int k = 0; k < 2; ++k) {
+        dftk_pairs_t &P = *sets[k];
+        std::vector<int> &ab = pl.ab[k];
+        const int n = (int)(ab.size() / 2);
+        memset(&P, 0, sizeof(P));
+        P.n_pairs = n;
+        P.kmax = pl.kmax;
+        P.ab = (const int *)(base + pl.off_ab[k]);
+        P.nprim = (int *)(base + pl.off_np[k]);
+        P.rec64 = (double *)(base + pl.off_r64[k]);
+        P.rec32 = (float *)(base + pl.off_r32[k]);
+        P.q = (double *)(base + pl.off_q[k]);
+        P.qp = (float *)(base + pl.off_qp[k]);
+        if (n == 0) continue;
+        for (int pass = 0; pass < 2; ++pass) {
+            DFTK_CUDA(cudaMemcpyAsync(base + pl.off_ab[k], ab.data(), sizeof(int) * ab.size(), cudaMemcpyHostToDevice, s));
+            if ((st = dftk_pair_data(shells, DFTK_PCLASS_GENERIC, &P, stream)) != DFTK_OK) return st;
+            if ((st = dftk_hl_schwarz(shells, &P, pl.lmax, stream)) != DFTK_OK) return st;
+            qs[k].assign(n, 0.0);
+            DFTK_CUDA(cudaMemcpyAsync(qs[k].data(), P.q, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+            DFTK_CUDA(cudaStreamSynchronize(s));
+            if (pass == 1) break;
+            std::vector<int> order(n);
+            for (int i = 0; i < n; ++i) order[i] = i;
+            const std::vector<double> &q = qs[k];
+            std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return q[x] > q[y]; });
+            std::vector<int> sorted(ab.size());
+            for (int i = 0; i < n; ++i) {
+                sorted[2 * i] = ab[2 * order[i]];
+                sorted[2 * i + 1] = ab[2 * order[i] + 1];
+            }
+            ab.swap(sorted);
+        }
+    }
+    const std::vector<long long> off_lo = prefix_offsets(qs[0], qs[1], false, tau_schwarz);
+    const std::vector<long long> off_hi = prefix_offsets(qs[0], qs[0], true, tau_schwarz);
+    long long *d_lo = (long long *)(base + pl.off_row[0]), *d_hi = (long long *)(base + pl.off_row[1]);
+    DFTK_CUDA(cudaMemcpyAsync(d_lo, off_lo.data(), sizeof(long long) * off_lo.size(), cudaMemcpyHostToDevice, s));
+    DFTK_CUDA(cudaMemcpyAsync(d_hi, off_hi.data(), sizeof(long long) * off_hi.size(), cudaMemcpyHostToDevice, s));
+    hl->n_rows = (long long)qs[0].size();
+    hl->total[0] = off_lo.back();
+    hl->total[1] = off_hi.back();
+    hl->row_off[0] = d_lo;
+    hl->row_off[1] = d_hi;
+    hl->tau_prim = tau_prim;
+    hl->lmax = pl.lmax;
+    DFTK_CUDA(cudaStreamSynchronize(s));  // the host vectors above are sources of the copies
+    return DFTK_OK;
+}
 
 int dftk_prepare_bytes(const dftk_shells_t *shells, size_t *bytes)
 {
@@ -877,6 +1034,8 @@ int dftk_jk(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N_PCLASS]
         if (P.total[c] > 0 && !queue->row_off[c]) return fail(DFTK_ERR_ARG, "dftk_jk: missing row offsets");
     }
     P.tau_prim = (float)queue->tau_prim;
+    for (int c = 0; c < DFTK_N_QCLASS; ++c)
+        for (int p = 0; p < 2; ++p) P.tile[p * DFTK_N_QCLASS + c] = launch_shape(DFTK_FAMILY_JK, c, p).tile;
     P.D = D;
     P.Da = D_a;
     P.Db = uhf ? D_b : D_a;
@@ -1114,7 +1273,29 @@ int dftk_set_launch(int family, int qclass, int fp32, int threads, int blocks_pe
         return fail(DFTK_ERR_ARG, "dftk_set_launch: threads must be 64 or 128, blocks_per_sm 1..32");
     std::lock_guard<std::mutex> lock(g_shape_mutex);
     init_shapes_locked();
-    g_shape[family][qclass][fp32] = {threads, blocks_per_sm};
+    g_shape[family][qclass][fp32].threads = threads;
+    g_shape[family][qclass][fp32].blocks_per_sm = blocks_per_sm;
+    return DFTK_OK;
+}
+
+int dftk_set_tile(int qclass, int fp32, int tile)
+{
+    if (qclass < 0 || qclass >= DFTK_N_QCLASS || (fp32 != 0 && fp32 != 1) || (tile != 1 && tile != 2 && tile != 4 &&
+                                                                               tile != 8))
+        return fail(DFTK_ERR_ARG, "dftk_set_tile: bad class / precision, or tile not 1, 2, 4, 8");
+    std::lock_guard<std::mutex> lock(g_shape_mutex);
+    init_shapes_locked();
+    g_shape[DFTK_FAMILY_JK][qclass][fp32].tile = tile;
+    return DFTK_OK;
+}
+
+int dftk_get_tile(int qclass, int fp32, int *tile)
+{
+    if (qclass < 0 || qclass >= DFTK_N_QCLASS || (fp32 != 0 && fp32 != 1) || !tile)
+        return fail(DFTK_ERR_ARG, "dftk_get_tile: bad arguments");
+    std::lock_guard<std::mutex> lock(g_shape_mutex);
+    init_shapes_locked();
+    *tile = g_shape[DFTK_FAMILY_JK][qclass][fp32].tile;
     return DFTK_OK;
 }
 

@@ -188,6 +188,7 @@ struct JkParams {
     unsigned long long *heads;  // [2 * DFTK_N_QCLASS]: FP64 then FP32 entry counts
     const int *ket_base[DFTK_N_QCLASS];  // batches: first ket pair of each row's molecule (NULL = 0)
     const unsigned char *mol_active;     // batches: molecules still iterating (NULL = all)
+    int tile[2 * DFTK_N_QCLASS];         // list kernels: consecutive work items per warp step (FP64, FP32)
 };
 
 // ket pair of candidate `cand` in bra row `row` of class C
@@ -642,23 +643,30 @@ __global__ void __launch_bounds__(128, JkMinBlocks<C, T>::value) k_jk_list(const
     const int2 *list = P.list[C];
     const long long nwork = ((n + 31) >> 5) * NS;
     const int lane = threadIdx.x & 31;
-    const long long wstride = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; gw < nwork; gw += wstride) {
-        const int split = (int)(gw % NS);
-        const long long idx = (gw / NS) * 32 + lane;
-        const bool valid = idx < n;
-        int row = 0, ket = 0;
-        if (valid) {
-            const int2 e = __ldg(list + (fp32 ? cap - 1 - idx : idx));
-            row = e.x;
-            ket = e.y;
-        }
-        if constexpr (NS == 1) {
-            jk_one<C, T, 0>(P, valid, row, ket);
-        } else {
-            if (split == 0) jk_one<C, T, 0>(P, valid, row, ket);
-            else if (split == 1) jk_one<C, T, 1>(P, valid, row, ket);
-            else jk_one<C, T, 2>(P, valid, row, ket);
+    // each warp step takes `tile` consecutive work items (32-entry groups, or
+    // their c-component splits), so a warp stays on neighbouring list entries
+    const int tile = P.tile[(fp32 ? DFTK_N_QCLASS : 0) + C] > 0 ? P.tile[(fp32 ? DFTK_N_QCLASS : 0) + C] : 1;
+    const long long wstride = (((long long)gridDim.x * blockDim.x) >> 5) * tile;
+    for (long long g0 = (((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * tile; g0 < nwork; g0 += wstride) {
+        for (int k = 0; k < tile; ++k) {
+            const long long gw = g0 + k;
+            if (gw >= nwork) break;
+            const int split = (int)(gw % NS);
+            const long long idx = (gw / NS) * 32 + lane;
+            const bool valid = idx < n;
+            int row = 0, ket = 0;
+            if (valid) {
+                const int2 e = __ldg(list + (fp32 ? cap - 1 - idx : idx));
+                row = e.x;
+                ket = e.y;
+            }
+            if constexpr (NS == 1) {
+                jk_one<C, T, 0>(P, valid, row, ket);
+            } else {
+                if (split == 0) jk_one<C, T, 0>(P, valid, row, ket);
+                else if (split == 1) jk_one<C, T, 1>(P, valid, row, ket);
+                else jk_one<C, T, 2>(P, valid, row, ket);
+            }
         }
     }
 }

@@ -193,7 +193,7 @@ int dftk_pair_data(const dftk_shells_t *shells, int pair_class, dftk_pairs_t *pa
 
 /* Schwarz factors pairs->q from the diagonal quartets (ab|ab), primitive
  * factors pairs->qp, and the primitive records of each pair reordered by
- * descending qp.  At most 64 primitive pairs per pair. */
+ * descending qp.  At most 128 primitive pairs per pair. */
 int dftk_schwarz(const dftk_shells_t *shells, int pair_class, dftk_pairs_t *pairs,
                  dftk_stream_t stream);
 
@@ -206,7 +206,8 @@ int dftk_schwarz(const dftk_shells_t *shells, int pair_class, dftk_pairs_t *pair
  * offsets of every quartet class at tau_schwarz (the unique-quartet
  * enumeration cd <= ab of shelled.py:599-603, Schwarz-screened).  All arrays
  * live in the caller's device `storage` (dftk_prepare_bytes bytes); pairs[3]
- * and *queue are filled with pointers into it.  One molecule, s and p shells.
+ * and *queue are filled with pointers into it.  One molecule; the pairs with
+ * a d or f shell are left to dftk_prepare_hl.
  * Reads shells->l and shells->nprim back to the host and synchronises
  * `stream`.  No counterpart in the reference as one call. */
 int dftk_prepare_bytes(const dftk_shells_t *shells, size_t *bytes);
@@ -304,6 +305,17 @@ int dftk_jk_noalloc(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N
                     const double *D_b, double *J, double *K_a, double *K_b, int flags,
                     double tau, double tau_fp32, long long *counts, dftk_stream_t stream);
 
+/* The d/f part of one molecule's setup for C hosts (dftk_prepare does the
+ * s/p part and skips the pairs with a d or f shell): both generic-layout pair
+ * sets built, Schwarz-sorted and described, with the two candidate spaces'
+ * row offsets, inside caller storage of dftk_prepare_hl_bytes bytes (device
+ * memory, 256-byte aligned).  Shells must already be one per contraction row.
+ * Synchronises the stream; storage must outlive the calls that use *hl.
+ * No counterpart in the reference beyond pair_list / pair_cache setup. */
+int dftk_prepare_hl_bytes(const dftk_shells_t *shells, size_t *bytes);
+int dftk_prepare_hl(const dftk_shells_t *shells, double tau_schwarz, double tau_prim, void *storage,
+                    size_t storage_bytes, dftk_hl_t *hl, dftk_stream_t stream);
+
 /* Schwarz factors of a generic-layout pair set (momenta <= lmax <= 3), with each
  * pair's primitive records reordered by descending primitive factor (no
  * counterpart in the reference: screening bounds).  kmax <= 128. */
@@ -348,6 +360,13 @@ int dftk_jk_timing_read(float *ms, int n);
 #define DFTK_N_FAMILY 2
 int dftk_set_launch(int family, int qclass, int fp32, int threads, int blocks_per_sm);
 int dftk_get_launch(int family, int qclass, int fp32, int *threads, int *blocks_per_sm);
+/* Tile of the J/K list kernels (no counterpart in the reference): per class
+ * and precision, how many consecutive 32-quartet work items a warp takes per
+ * step of its grid-stride loop (1, 2, 4 or 8; default 1) -- larger tiles keep
+ * a warp on neighbouring list entries (same bra pairs).  Set by the
+ * autotuner beside the launch shape. */
+int dftk_set_tile(int qclass, int fp32, int tile);
+int dftk_get_tile(int qclass, int fp32, int *tile);
 
 /* Analytic nuclear gradient (no counterpart in the reference): grad[3 * atom
  * + x] is overwritten with sum D dH/dX - sum W dS/dX + sum Gamma d(ab|cd)/dX

@@ -49,3 +49,52 @@ def test_prepare_matches_engine(shape, tau):
         _lib.call("dftk_prepare", ctypes.byref(eng.c_shells), tau, eng.tau_prim, _lib.ptr(storage),
                   nbytes.value - 1, pairs, ctypes.byref(queue), _lib.stream_handle())
     assert ei.value.status == _lib.ERR_WORKSPACE
+
+
+def test_prepare_hl_d_shells_through_the_c_abi():
+    """A C host's whole d-shell path with no Python setup: dftk_prepare (s/p
+    part) and dftk_prepare_hl (d part) fill the pair sets and candidate
+    spaces; dftk_jk then dftk_jk_hl give the engine's J/K (HBr / STO-3G, and
+    the generally contracted d-polarised test basis on H2O)."""
+    import json
+    import os
+
+    from conftest import GOLDEN
+
+    with open(os.path.join(GOLDEN, "dz_gc_test.json")) as fh:
+        gc = json.load(fh)
+    cases = [(basis.load_basis(), ["35", "1"], np.array([[0.0, 0.0, 0.0], [0.3, 0.1, 2.7]])),
+             (gc,) + tuple(geometry.water())]
+    for data, atoms, centers in cases:
+        sh = basis.build_shells(data, atoms, centers)
+        eng = IntegralEngine(sh, tau_schwarz=1e-12)
+        N = eng.n_ao
+        rng = np.random.default_rng(2)
+        M = rng.normal(size=(N, N))
+        D = torch.as_tensor(0.05 * (M + M.T), device=eng.device)
+        Da = (0.5 * D).contiguous()
+        J0, K0, _ = eng.jk(D, Da, tau=1e-14)
+        stream = _lib.stream_handle()
+        nbytes = ctypes.c_size_t()
+        _lib.call("dftk_prepare_bytes", ctypes.byref(eng.c_shells), ctypes.byref(nbytes))
+        storage = torch.empty(nbytes.value, dtype=torch.uint8, device=eng.device)
+        pairs = _lib.PairsArray()
+        queue = _lib.Queue()
+        _lib.call("dftk_prepare", ctypes.byref(eng.c_shells), 1e-12, eng.tau_prim, _lib.ptr(storage), nbytes.value,
+                  pairs, ctypes.byref(queue), stream)
+        hbytes = ctypes.c_size_t()
+        _lib.call("dftk_prepare_hl_bytes", ctypes.byref(eng.c_shells), ctypes.byref(hbytes))
+        hstore = torch.empty(hbytes.value, dtype=torch.uint8, device=eng.device)
+        hl = _lib.HlSet()
+        _lib.call("dftk_prepare_hl", ctypes.byref(eng.c_shells), 1e-12, eng.tau_prim, _lib.ptr(hstore), hbytes.value,
+                  ctypes.byref(hl), stream)
+        assert hl.n_rows == eng.c_hl.n_rows and list(hl.total) == list(eng.c_hl.total) and hl.lmax == 2
+        ws_bytes = _lib.load().dftk_jk_workspace_bytes_queue(eng.ns, N, ctypes.byref(queue))
+        ws = torch.empty(ws_bytes, dtype=torch.uint8, device=eng.device)
+        J = torch.empty((N, N), dtype=torch.float64, device=eng.device)
+        K = torch.empty_like(J)
+        _lib.call("dftk_jk", ctypes.byref(eng.c_shells), pairs, ctypes.byref(queue), _lib.ptr(D), _lib.ptr(Da),
+                  None, _lib.ptr(J), _lib.ptr(K), None, 0, 1e-14, 1e-14, _lib.ptr(ws), ws_bytes, None, stream)
+        _lib.call("dftk_jk_hl", ctypes.byref(eng.c_shells), ctypes.byref(hl), _lib.ptr(D), _lib.ptr(Da), None,
+                  _lib.ptr(J), _lib.ptr(K), None, 0, 1e-14, _lib.ptr(ws), ws_bytes, None, stream)
+        assert torch.abs(J - J0).max().item() < 1e-12 and torch.abs(K - K0).max().item() < 1e-12

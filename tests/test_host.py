@@ -251,6 +251,12 @@ def test_launch_shape_table_without_gpu():
     assert lib.dftk_set_launch(0, 6, 0, 128, 4) == _lib.ERR_ARG
     assert lib.dftk_set_launch(2, 0, 0, 128, 4) == _lib.ERR_ARG
     assert lib.dftk_set_launch(1, 0, 0, 128, 33) == _lib.ERR_ARG
+    t = ctypes.c_int()
+    assert lib.dftk_set_tile(2, 1, 4) == _lib.OK
+    assert lib.dftk_get_tile(2, 1, ctypes.byref(t)) == _lib.OK and t.value == 4
+    assert lib.dftk_set_tile(2, 1, 3) == _lib.ERR_ARG
+    assert lib.dftk_set_tile(6, 0, 1) == _lib.ERR_ARG
+    assert lib.dftk_set_tile(2, 1, 1) == _lib.OK
 
 
 def test_batch_queue_matches_per_molecule_queues():
