@@ -594,6 +594,58 @@ def grid_figures(torch, eng, centers, res, nocc, cpu: bool, n_points=1_000_000):
     return out
 
 
+def dshell_figures(torch):
+    """The d/f path on a polarised basis: (H2O)_16 (2x2x4 lattice) with the
+    generally contracted, d-polarised test basis (tests/golden/dz_gc_test.json;
+    384 basis functions): one full FP64 J/K build at a converged-looking
+    density, the s/p part (dftk_jk) and the d part (dftk_jk_hl) timed with
+    CUDA events, and the quartets with a d shell."""
+    import ctypes
+
+    from dft_b200 import _lib, basis, geometry
+    from dft_b200.engine import IntegralEngine
+
+    with open(os.path.join(REPO, "tests", "golden", "dz_gc_test.json")) as fh:
+        data = json.load(fh)
+    atoms, centers = geometry.water_cluster((2, 2, 4))
+    sh = basis.build_shells(data, atoms, centers)
+    eng = IntegralEngine(sh, tau_schwarz=1e-12)
+    N = eng.n_ao
+    rng = np.random.default_rng(4)
+    M = rng.normal(size=(N, N)) * np.exp(-0.2 * np.abs(np.subtract.outer(np.arange(N), np.arange(N))))
+    D = torch.as_tensor(0.05 * (M + M.T), device=eng.device)
+    Dh = (0.5 * D).contiguous()
+    J = torch.empty((N, N), dtype=torch.float64, device=eng.device)
+    K = torch.empty_like(J)
+    stream = _lib.stream_handle()
+
+    def sp():
+        _lib.call("dftk_jk", ctypes.byref(eng.c_shells), eng.c_pairs, ctypes.byref(eng.c_queue), _lib.ptr(D),
+                  _lib.ptr(Dh), None, _lib.ptr(J), _lib.ptr(K), None, 0, 1e-14, 1e-14, _lib.ptr(eng.workspace),
+                  eng.workspace_bytes, None, stream)
+
+    def hl():
+        _lib.call("dftk_jk_hl", ctypes.byref(eng.c_shells), ctypes.byref(eng.c_hl), _lib.ptr(D), _lib.ptr(Dh), None,
+                  _lib.ptr(J), _lib.ptr(K), None, 0, 1e-14, _lib.ptr(eng.workspace), eng.workspace_bytes, None,
+                  stream)
+
+    def timed(fn, reps=5):
+        fn()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        s.record()
+        for _ in range(reps):
+            fn()
+        e.record()
+        torch.cuda.synchronize()
+        return s.elapsed_time(e) / reps
+
+    return {"workload": "(H2O)_16 2x2x4 lattice, generally contracted d-polarised test basis, FP64 J/K",
+            "n_basis": N, "n_shells_segmented": eng.ns,
+            "sp_part_ms": timed(sp), "d_part_ms": timed(hl), "full_build_ms": timed(lambda: eng.jk(D, Dh, tau=1e-14)),
+            "d_candidate_quartets": [int(x) for x in eng.hl_totals], "sp_candidate_quartets": int(sum(eng.totals))}
+
+
 def c10h22_figures(torch, cpu: bool):
     """C10H22 / STO-3G (72 basis functions): per-class ERI throughput of one
     full FP64 build at the converged density (CUDA events per class kernel),
@@ -908,6 +960,7 @@ def run_dftk_arm(args, rank, world, local_rank):
         line["eri_quartets_per_s"] = sum(evaluated) / (ms_per_step / 1e3)
         if not args.no_extras:
             line["c10h22"] = c10h22_figures(torch, cpu=world == 1 and not args.no_cpu_baseline)
+            line["d_basis"] = dshell_figures(torch)
             line["grad"] = gradient_figures(torch, eng, atoms, centers, r64)
             line["grad"]["config4"] = config4_gradients(torch)
             line["grid"] = grid_figures(torch, eng, centers, r64, nocc, cpu=world == 1 and not args.no_cpu_baseline)
