@@ -107,6 +107,12 @@ class HlSet(ctypes.Structure):
         ("row_off", ctypes.c_void_p * 2),
         ("tau_prim", ctypes.c_double),
         ("lmax", ctypes.c_int),
+        ("cls_rows", ctypes.c_void_p * 2),
+        ("n_cls_rows", ctypes.c_longlong * 2),
+        ("cls_kets", ctypes.c_void_p * 3),
+        ("n_cls_kets", ctypes.c_longlong * 3),
+        ("cls_off", ctypes.c_void_p * 6),
+        ("cls_total", ctypes.c_longlong * 6),
     ]
 
 

@@ -13,7 +13,7 @@ PKG = os.path.dirname(HERE)
 REPO = os.path.dirname(PKG)
 LIB = os.path.join(PKG, "libdftk.so")
 SOURCES = ["dftk.cu", "jk_noalloc.cu"]
-HEADERS = ["common.cuh", "boys.cuh", "eri_classes.cuh", "jk.cuh", "generic.cuh", "onee.cuh", "grad.cuh", "grid.cuh", "hl.cuh"]
+HEADERS = ["common.cuh", "boys.cuh", "eri_classes.cuh", "jk.cuh", "generic.cuh", "onee.cuh", "grad.cuh", "grid.cuh", "hl.cuh", "hl_classes.cuh", "hlc.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -19,6 +19,7 @@
 #include "onee.cuh"
 #include "grid.cuh"
 #include "hl.cuh"
+#include "hlc.cuh"
 
 namespace {
 
@@ -613,8 +614,10 @@ int prepare_plan(const dftk_shells_t *shells, PreparePlan &pl)
 // and every s/p pair ("lo") in the generic 13-field layout.
 struct PrepareHlPlan {
     int kmax = 1, lmax = 2;
+    std::vector<int> l;      // shell momenta
     std::vector<int> ab[2];  // 0 hi, 1 lo
     size_t off_ab[2], off_np[2], off_r64[2], off_r32[2], off_q[2], off_qp[2], off_row[2];
+    size_t off_cls_rows[2], off_cls_kets[3], off_cls_off[HLC_N_CLASSES];
     size_t bytes = 0;
 };
 
@@ -654,6 +657,11 @@ int prepare_hl_plan(const dftk_shells_t *shells, PrepareHlPlan &pl)
         pl.off_qp[k] = carve(at, sizeof(float) * std::max<size_t>((size_t)pl.kmax * n, 1));
     }
     for (int k = 0; k < 2; ++k) pl.off_row[k] = carve(at, sizeof(long long) * (pl.ab[0].size() / 2 + 1));
+    const size_t nhi = pl.ab[0].size() / 2, nlo = pl.ab[1].size() / 2;
+    for (int x = 0; x < 2; ++x) pl.off_cls_rows[x] = carve(at, sizeof(int) * std::max<size_t>(nhi, 1));
+    for (int y = 0; y < 3; ++y) pl.off_cls_kets[y] = carve(at, sizeof(int) * std::max<size_t>(nlo, 1));
+    for (int c = 0; c < HLC_N_CLASSES; ++c) pl.off_cls_off[c] = carve(at, sizeof(long long) * (nhi + 1));
+    pl.l = l;
     pl.bytes = at;
     return DFTK_OK;
 }
@@ -752,8 +760,49 @@ int dftk_prepare_hl(const dftk_shells_t *shells, double tau_schwarz, double tau_
             ab.swap(sorted);
         }
     }
-    const std::vector<long long> off_lo = prefix_offsets(qs[0], qs[1], false, tau_schwarz);
+    std::vector<long long> off_lo = prefix_offsets(qs[0], qs[1], false, tau_schwarz);
     const std::vector<long long> off_hi = prefix_offsets(qs[0], qs[0], true, tau_schwarz);
+    // thread-per-quartet classes: hi rows of pairs (d,s) / (d,p), lo rows by
+    // l_a + l_b, each ascending; those hi rows leave the (hi|lo) space
+    std::vector<int> cls_rows[2], cls_kets[3];
+    std::vector<long long> cls_off[HLC_N_CLASSES];
+    for (size_t r = 0; r < qs[0].size(); ++r) {
+        const int la = pl.l[pl.ab[0][2 * r]], lb = pl.l[pl.ab[0][2 * r + 1]];
+        if (la == 2 && lb <= 1) cls_rows[lb].push_back((int)r);
+    }
+    for (size_t k = 0; k < qs[1].size(); ++k) cls_kets[pl.l[pl.ab[1][2 * k]] + pl.l[pl.ab[1][2 * k + 1]]].push_back((int)k);
+    for (int c = 0; c < HLC_N_CLASSES; ++c) {
+        const int x = c / 3, y = c % 3;
+        std::vector<double> qx, qy;
+        for (int r : cls_rows[x]) qx.push_back(qs[0][r]);
+        for (int k : cls_kets[y]) qy.push_back(qs[1][k]);
+        cls_off[c] = prefix_offsets(qx, qy, false, tau_schwarz);
+        hl->cls_off[c] = (const long long *)(base + pl.off_cls_off[c]);
+        hl->cls_total[c] = cls_off[c].back();
+        DFTK_CUDA(cudaMemcpyAsync(base + pl.off_cls_off[c], cls_off[c].data(), sizeof(long long) * cls_off[c].size(),
+                                  cudaMemcpyHostToDevice, s));
+    }
+    for (int x = 0; x < 2; ++x) {
+        hl->cls_rows[x] = (const int *)(base + pl.off_cls_rows[x]);
+        hl->n_cls_rows[x] = (long long)cls_rows[x].size();
+        if (!cls_rows[x].empty())
+            DFTK_CUDA(cudaMemcpyAsync(base + pl.off_cls_rows[x], cls_rows[x].data(), sizeof(int) * cls_rows[x].size(),
+                                      cudaMemcpyHostToDevice, s));
+    }
+    for (int y = 0; y < 3; ++y) {
+        hl->cls_kets[y] = (const int *)(base + pl.off_cls_kets[y]);
+        hl->n_cls_kets[y] = (long long)cls_kets[y].size();
+        if (!cls_kets[y].empty())
+            DFTK_CUDA(cudaMemcpyAsync(base + pl.off_cls_kets[y], cls_kets[y].data(), sizeof(int) * cls_kets[y].size(),
+                                      cudaMemcpyHostToDevice, s));
+    }
+    {
+        std::vector<long long> cnt(qs[0].size());
+        for (size_t r = 0; r < cnt.size(); ++r) cnt[r] = off_lo[r + 1] - off_lo[r];
+        for (int x = 0; x < 2; ++x)
+            for (int r : cls_rows[x]) cnt[r] = 0;
+        for (size_t r = 0; r < cnt.size(); ++r) off_lo[r + 1] = off_lo[r] + cnt[r];
+    }
     long long *d_lo = (long long *)(base + pl.off_row[0]), *d_hi = (long long *)(base + pl.off_row[1]);
     DFTK_CUDA(cudaMemcpyAsync(d_lo, off_lo.data(), sizeof(long long) * off_lo.size(), cudaMemcpyHostToDevice, s));
     DFTK_CUDA(cudaMemcpyAsync(d_hi, off_hi.data(), sizeof(long long) * off_hi.size(), cudaMemcpyHostToDevice, s));
@@ -1119,6 +1168,21 @@ template <int LM, typename K> int hl_smem_optin(K kernel, size_t extra_static = 
         DFTK_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
     return DFTK_OK;
 }
+
+// One class kernel of the thread-per-quartet d classes: 128-thread blocks,
+// a grid of at most 16 resident blocks per SM striding over the class's
+// warp work items (32 candidates x ket-component split).
+template <int C> int launch_hlc(const HlcParams &P, cudaStream_t s)
+{
+    if (P.total[C] == 0) return DFTK_OK;
+    const long long items = ((P.total[C] + 31) / 32) * HlClass<double, C, 0>::NSPLIT;
+    long long blocks = (items + 3) / 4;
+    const long long cap = (long long)sm_count() * 16;
+    if (blocks > cap) blocks = cap;
+    k_hlc<C><<<(unsigned)blocks, 128, 0, s>>>(P);
+    DFTK_LAUNCHED("k_hlc");
+    return DFTK_OK;
+}
 }  // namespace
 
 extern "C" {
@@ -1158,9 +1222,19 @@ int dftk_jk_hl(const dftk_shells_t *shells, const dftk_hl_t *hl, const double *D
         return fail(DFTK_ERR_ARG, "dftk_jk_hl: inconsistent candidate spaces");
     if (workspace_bytes < ws_bytes(shells->n_shells, shells->n_ao))
         return fail(DFTK_ERR_WORKSPACE, "dftk_jk_hl: workspace too small");
+    long long cls_sum = 0;
+    for (int c = 0; c < HLC_N_CLASSES; ++c) {
+        const int x = c / 3, y = c % 3;
+        if (hl->cls_total[c] < 0 ||
+            (hl->cls_total[c] > 0 && (!hl->cls_off[c] || !hl->cls_rows[x] || !hl->cls_kets[y] ||
+                                      hl->n_cls_rows[x] <= 0 || hl->n_cls_rows[x] > hl->n_rows ||
+                                      hl->n_cls_kets[y] <= 0 || hl->n_cls_kets[y] > hl->lo.n_pairs)))
+            return fail(DFTK_ERR_ARG, "dftk_jk_hl: inconsistent class spaces");
+        cls_sum += hl->cls_total[c];
+    }
     DFTK_INIT();
     const long long total = hl->total[0] + hl->total[1];
-    if (total == 0 || hl->n_rows == 0) return DFTK_OK;
+    if ((total == 0 && cls_sum == 0) || hl->n_rows == 0) return DFTK_OK;
     cudaStream_t s = (cudaStream_t)stream;
     const int N = shells->n_ao;
     const size_t nn = (size_t)N * N;
@@ -1192,17 +1266,50 @@ int dftk_jk_hl(const dftk_shells_t *shells, const dftk_hl_t *hl, const double *D
     P.uhf = uhf;
     P.tau = tau;
     P.counts = counts;
-    long long blocks = total;
-    // one-warp blocks: 8 per SM with the d layout (26.6 KB shared each), 1 with the f one (167 KB)
-    const long long cap = (long long)sm_count() * (hl->lmax <= 2 ? 8 : 1);
-    if (blocks > cap) blocks = cap;
-    if (hl->lmax <= 2) {
-        k_hl_jk<2><<<(unsigned)blocks, 32, sizeof(HlScratch<2>), s>>>(P);
-    } else {
-        if ((st = hl_smem_optin<3>(k_hl_jk<3>))) return st;
-        k_hl_jk<3><<<(unsigned)blocks, 32, sizeof(HlScratch<3>), s>>>(P);
+    if (cls_sum > 0) {
+        HlcParams C;
+        memset(&C, 0, sizeof(C));
+        C.sh = *shells;
+        C.shell_ao = shells->ao;
+        C.hi = hl->hi;
+        C.lo = hl->lo;
+        for (int x = 0; x < 2; ++x) {
+            C.rows[x] = hl->cls_rows[x];
+            C.n_rows[x] = hl->n_cls_rows[x];
+        }
+        for (int y = 0; y < 3; ++y) C.kets[y] = hl->cls_kets[y];
+        for (int c = 0; c < HLC_N_CLASSES; ++c) {
+            C.off[c] = hl->cls_off[c];
+            C.total[c] = hl->cls_total[c];
+        }
+        C.tau_prim = (float)hl->tau_prim;
+        C.D = D;
+        C.Da = D_a;
+        C.Db = uhf ? D_b : D_a;
+        C.Y = Y;
+        C.Za = Za;
+        C.Zb = Zb;
+        C.Dsh = Dsh;
+        C.uhf = uhf;
+        C.tau = tau;
+        C.counts = counts;
+        if ((st = launch_hlc<0>(C, s)) || (st = launch_hlc<1>(C, s)) || (st = launch_hlc<2>(C, s)) ||
+            (st = launch_hlc<3>(C, s)) || (st = launch_hlc<4>(C, s)) || (st = launch_hlc<5>(C, s)))
+            return st;
     }
-    DFTK_LAUNCHED("k_hl_jk");
+    if (total > 0) {
+        long long blocks = total;
+        // one-warp blocks: 8 per SM with the d layout (26.6 KB shared each), 1 with the f one (167 KB)
+        const long long cap = (long long)sm_count() * (hl->lmax <= 2 ? 8 : 1);
+        if (blocks > cap) blocks = cap;
+        if (hl->lmax <= 2) {
+            k_hl_jk<2><<<(unsigned)blocks, 32, sizeof(HlScratch<2>), s>>>(P);
+        } else {
+            if ((st = hl_smem_optin<3>(k_hl_jk<3>))) return st;
+            k_hl_jk<3><<<(unsigned)blocks, 32, sizeof(HlScratch<3>), s>>>(P);
+        }
+        DFTK_LAUNCHED("k_hl_jk");
+    }
     long long bx = ((long long)nn + 255) / 256;
     if (bx > 148 * 8) bx = 148 * 8;
     k_symmetrize_add<<<(unsigned)bx, 256, 0, s>>>(N, Y, Za, Zb, J, K_a, K_b, uhf);

@@ -248,11 +248,29 @@ __global__ void k_dsh(const dftk_shells_t sh, int max_ns, const double *D, const
 //   Z_bc += 1/w sum_ad I D_ad,  Z_bd += 1/w sum_ac I D_ac,
 // w = 2^{[a=b]+[c=d]+[ab=cd]}; J = Y + Y^T and K = Z + Z^T afterwards give the
 // eight orientations of fill_matrices (shelled.py:791-859) with its weights.
-template <int C, typename T, int S>
-__device__ __forceinline__ void digest(const JkParams &P, bool valid, bool uniform_bra, int a, int b,
-                                       int c, int d, double w, const T (&I)[EriClass<T, C, S>::NI])
+// Whether a thread's share of the ket components (one split of class E)
+// holds ket component cc (c) or dd (d).
+template <typename E>
+__device__ __forceinline__ constexpr bool split_has_c(int cc)
 {
-    using E = EriClass<T, C, S>;
+    for (int m = 0; m < E::NCD; ++m)
+        if (E::cd_c(m) == cc) return true;
+    return false;
+}
+template <typename E>
+__device__ __forceinline__ constexpr bool split_has_d(int dd)
+{
+    for (int m = 0; m < E::NCD; ++m)
+        if (E::cd_d(m) == dd) return true;
+    return false;
+}
+
+// The digestion of one block of class E (EriClass or HlClass: NA..ND, NCD,
+// cd_c, cd_d); PT holds sh, shell_ao, D, Da, Db, Y, Za, Zb and uhf.
+template <typename E, typename PT, typename T>
+__device__ __forceinline__ void digest_block(const PT &P, bool valid, bool uniform_bra, int a, int b, int c, int d,
+                                             double w, const T (&I)[E::NI])
+{
     constexpr int NA = E::NA, NB = E::NB, NC = E::NC, ND = E::ND, NCD = E::NCD;
     const MolView mv = mol_view(P.sh, a);
     const int N = mv.nao;
@@ -330,22 +348,29 @@ __device__ __forceinline__ void digest(const JkParams &P, bool valid, bool unifo
             for (int ia = 0; ia < NA; ++ia) {
 #pragma unroll
                 for (int cc = 0; cc < NC; ++cc)
-                    if (E::NSPLIT == 1 || cc == S)
-                        atomicAdd(Z + (long long)(oa + ia) * N + oc + cc, zac[ia][cc]);
+                    if (split_has_c<E>(cc)) atomicAdd(Z + (long long)(oa + ia) * N + oc + cc, zac[ia][cc]);
 #pragma unroll
-                for (int dd = 0; dd < ND; ++dd) atomicAdd(Z + (long long)(oa + ia) * N + od + dd, zad[ia][dd]);
+                for (int dd = 0; dd < ND; ++dd)
+                    if (split_has_d<E>(dd)) atomicAdd(Z + (long long)(oa + ia) * N + od + dd, zad[ia][dd]);
             }
 #pragma unroll
             for (int ib = 0; ib < NB; ++ib) {
 #pragma unroll
                 for (int cc = 0; cc < NC; ++cc)
-                    if (E::NSPLIT == 1 || cc == S)
-                        atomicAdd(Z + (long long)(ob + ib) * N + oc + cc, zbc[ib][cc]);
+                    if (split_has_c<E>(cc)) atomicAdd(Z + (long long)(ob + ib) * N + oc + cc, zbc[ib][cc]);
 #pragma unroll
-                for (int dd = 0; dd < ND; ++dd) atomicAdd(Z + (long long)(ob + ib) * N + od + dd, zbd[ib][dd]);
+                for (int dd = 0; dd < ND; ++dd)
+                    if (split_has_d<E>(dd)) atomicAdd(Z + (long long)(ob + ib) * N + od + dd, zbd[ib][dd]);
             }
         }
     }
+}
+
+template <int C, typename T, int S>
+__device__ __forceinline__ void digest(const JkParams &P, bool valid, bool uniform_bra, int a, int b,
+                                       int c, int d, double w, const T (&I)[EriClass<T, C, S>::NI])
+{
+    digest_block<EriClass<T, C, S>>(P, valid, uniform_bra, a, b, c, d, w, I);
 }
 
 template <int C, typename T> struct RecOf;

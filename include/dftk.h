@@ -168,6 +168,21 @@ typedef struct {
     const long long *row_off[2];  /* device [n_rows + 1] each: Schwarz prefixes as in dftk_queue_t */
     double tau_prim;              /* primitive-quartet cut, as in dftk_queue_t */
     int lmax;                     /* largest shell momentum, 2 (d) or 3 (f): selects the kernels' scratch layout */
+    /* Thread-per-quartet classes (ds|ss), (ds|ps), (ds|pp), (dp|ss), (dp|ps),
+     * (dp|pp) (class 3 x + y: x = 0 for hi pairs (d,s), 1 for (d,p); y = the
+     * lo pair's l_a + l_b).  cls_rows[x] lists the hi rows of pairs of kind x
+     * and cls_kets[y] the lo rows of kind y, each ascending (so by descending
+     * Schwarz factor); cls_off[3 x + y] are the candidate offsets over those
+     * lists (the ket prefix of row r: cls_kets[y][0 .. count_r)), cls_total
+     * their totals.  These spaces and (hi|lo) must not overlap: give the rows
+     * in cls_rows zero (hi|lo) candidates in row_off[0].  All zero: (hi|lo)
+     * runs entirely in the warp-per-quartet kernel. */
+    const int *cls_rows[2];
+    long long n_cls_rows[2];
+    const int *cls_kets[3];
+    long long n_cls_kets[3];
+    const long long *cls_off[6];
+    long long cls_total[6];
 } dftk_hl_t;
 
 /* library version (integer, 100 * major + minor) */

@@ -9,6 +9,7 @@ own outputs (tests/golden/make_golden.py br2 / gc / gcf) and the oracle.
   loop and the RHF/DIIS driver) at 1e-8 Eh.
 * J/K with random densities against the oracle's direct J/K (1e-11).
 """
+import ctypes
 import json
 import os
 
@@ -17,7 +18,7 @@ import pytest
 import torch
 
 from conftest import GOLDEN, load_golden
-from dft_b200 import basis, geometry, shelled
+from dft_b200 import _lib, basis, geometry, shelled
 from dft_b200.engine import IntegralEngine
 from dft_b200.scf import scf_reference, scf_rhf
 
@@ -175,3 +176,62 @@ def test_f_shell_eris_and_jk_vs_oracle(oracle_mod):
     J0, K0, _ = oracle_mod.direct_jk(osh, q, 2 * P, P, P)
     for A_, B_ in ((J, J0), (K, K0)):
         assert np.abs(A_.cpu().numpy() - B_).max() < 1e-11 * max(1.0, np.abs(B_).max())
+
+
+def test_thread_classes_match_warp_path_and_oracle(oracle_mod):
+    """(H2O)_2 with the generally contracted d-polarised basis: the generated
+    thread-per-quartet kernels of (ds|ss)..(dp|pp) plus the warp kernel for
+    the rest give the warp kernel's J/K alone (1e-12) and the oracle's direct
+    J/K (1e-11 relative), UHF densities with no structure; the class spaces
+    and the remaining (hi|lo) space partition the unmasked (hi|lo) space."""
+    atoms, centers = geometry.water_cluster((1, 1, 2))
+    data = _gc_basis()
+    sh = basis.build_shells(data, atoms, centers)
+    eng = IntegralEngine(sh, tau_schwarz=0.0)
+    warp = IntegralEngine(sh, tau_schwarz=0.0, hl_classes=False)
+    assert all(t > 0 for t in eng.hlc_totals)
+    assert sum(eng.hlc_totals) + eng.hl_totals[0] == warp.hl_totals[0]
+    assert eng.hl_totals[1] == warp.hl_totals[1] and sum(warp.hlc_totals) == 0
+    N = eng.n_ao
+    rng = np.random.default_rng(17)
+    M1, M2 = rng.normal(size=(N, N)), rng.normal(size=(N, N))
+    Pa, Pb = 0.1 * (M1 + M1.T), 0.1 * (M2 + M2.T)
+    dev = eng.device
+    args = [torch.as_tensor(x, device=dev) for x in (Pa + Pb, Pa, Pb)]
+    J, Ka, Kb = eng.jk(*args, uhf=True, tau=0.0)
+    J1, Ka1, Kb1 = warp.jk(*args, uhf=True, tau=0.0)
+    for A_, B_ in ((J, J1), (Ka, Ka1), (Kb, Kb1)):
+        assert torch.abs(A_ - B_).max().item() < 1e-12 * max(1.0, torch.abs(B_).max().item())
+    osh = oracle_mod.build_shells(data, atoms, centers)
+    q = oracle_mod.quartet_list(len(osh))
+    J0, Ka0, Kb0 = oracle_mod.direct_jk(osh, q, Pa + Pb, Pa, Pb)
+    for M, M0 in ((J, J0), (Ka, Ka0), (Kb, Kb0)):
+        err = np.abs(M.cpu().numpy() - M0).max()
+        assert err < 1e-11 * max(1.0, np.abs(M0).max()), err
+
+
+def test_thread_classes_screened_density_counts():
+    """Screening through the class kernels: at a tau that cuts part of the
+    (ds|ss)..(dp|pp) quartets the J/K still equal the warp kernel's at the
+    same tau, and the evaluated-quartet counters of both paths agree."""
+    atoms, centers = geometry.water_cluster((1, 2, 2))
+    sh = basis.build_shells(_gc_basis(), atoms, centers)
+    eng = IntegralEngine(sh, tau_schwarz=1e-12)
+    warp = IntegralEngine(sh, tau_schwarz=1e-12, hl_classes=False)
+    N = eng.n_ao
+    rng = np.random.default_rng(5)
+    M = rng.normal(size=(N, N)) * np.exp(-0.3 * np.abs(np.subtract.outer(np.arange(N), np.arange(N))))
+    D = torch.as_tensor(0.05 * (M + M.T), device=eng.device)
+    Dh = (0.5 * D).contiguous()
+    out = []
+    for e in (eng, warp):
+        counts = torch.zeros(2, dtype=torch.int64, device=e.device)
+        J = torch.zeros((N, N), dtype=torch.float64, device=e.device)
+        K = torch.zeros_like(J)
+        _lib.call("dftk_jk_hl", ctypes.byref(e.c_shells), ctypes.byref(e.c_hl), _lib.ptr(D), _lib.ptr(Dh), None,
+                  _lib.ptr(J), _lib.ptr(K), None, 0, 1e-9, _lib.ptr(e.workspace), e.workspace_bytes,
+                  _lib.ptr(counts), _lib.stream_handle())
+        out.append((J, K, int(counts[0].item())))
+    (J, K, n), (J1, K1, n1) = out
+    assert n == n1 and n > 0
+    assert torch.abs(J - J1).max().item() < 1e-12 and torch.abs(K - K1).max().item() < 1e-12

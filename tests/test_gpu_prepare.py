@@ -89,6 +89,8 @@ def test_prepare_hl_d_shells_through_the_c_abi():
         _lib.call("dftk_prepare_hl", ctypes.byref(eng.c_shells), 1e-12, eng.tau_prim, _lib.ptr(hstore), hbytes.value,
                   ctypes.byref(hl), stream)
         assert hl.n_rows == eng.c_hl.n_rows and list(hl.total) == list(eng.c_hl.total) and hl.lmax == 2
+        assert list(hl.cls_total) == list(eng.c_hl.cls_total)
+        assert list(hl.n_cls_rows) == list(eng.c_hl.n_cls_rows) and list(hl.n_cls_kets) == list(eng.c_hl.n_cls_kets)
         ws_bytes = _lib.load().dftk_jk_workspace_bytes_queue(eng.ns, N, ctypes.byref(queue))
         ws = torch.empty(ws_bytes, dtype=torch.uint8, device=eng.device)
         J = torch.empty((N, N), dtype=torch.float64, device=eng.device)
