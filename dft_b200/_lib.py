@@ -97,6 +97,12 @@ class Queue(ctypes.Structure):
     ]
 
 
+# thread-per-quartet d classes: (bra pair kind, ket pair kind), kinds 0 ss,
+# 1 ps, 2 pp, 3 ds, 4 dp, 5 dd (the table of hl_classes.cuh)
+HLC_CLASS_KINDS = [(3, 0), (3, 1), (3, 2), (4, 0), (4, 1), (4, 2), (5, 0), (5, 1), (3, 3), (4, 3)]
+HLC_N_CLASSES = len(HLC_CLASS_KINDS)
+
+
 class HlSet(ctypes.Structure):
     """dftk_hl_t: the pair sets and candidate spaces of the quartets with a d shell."""
     _fields_ = [
@@ -107,12 +113,12 @@ class HlSet(ctypes.Structure):
         ("row_off", ctypes.c_void_p * 2),
         ("tau_prim", ctypes.c_double),
         ("lmax", ctypes.c_int),
-        ("cls_rows", ctypes.c_void_p * 2),
-        ("n_cls_rows", ctypes.c_longlong * 2),
+        ("cls_rows", ctypes.c_void_p * 3),
+        ("n_cls_rows", ctypes.c_longlong * 3),
         ("cls_kets", ctypes.c_void_p * 3),
         ("n_cls_kets", ctypes.c_longlong * 3),
-        ("cls_off", ctypes.c_void_p * 6),
-        ("cls_total", ctypes.c_longlong * 6),
+        ("cls_off", ctypes.c_void_p * HLC_N_CLASSES),
+        ("cls_total", ctypes.c_longlong * HLC_N_CLASSES),
     ]
 
 

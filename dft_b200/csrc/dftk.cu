@@ -617,7 +617,7 @@ struct PrepareHlPlan {
     std::vector<int> l;      // shell momenta
     std::vector<int> ab[2];  // 0 hi, 1 lo
     size_t off_ab[2], off_np[2], off_r64[2], off_r32[2], off_q[2], off_qp[2], off_row[2];
-    size_t off_cls_rows[2], off_cls_kets[3], off_cls_off[HLC_N_CLASSES];
+    size_t off_cls_rows[3], off_cls_kets[3], off_cls_off[HLC_N_CLASSES];
     size_t bytes = 0;
 };
 
@@ -658,7 +658,7 @@ int prepare_hl_plan(const dftk_shells_t *shells, PrepareHlPlan &pl)
     }
     for (int k = 0; k < 2; ++k) pl.off_row[k] = carve(at, sizeof(long long) * (pl.ab[0].size() / 2 + 1));
     const size_t nhi = pl.ab[0].size() / 2, nlo = pl.ab[1].size() / 2;
-    for (int x = 0; x < 2; ++x) pl.off_cls_rows[x] = carve(at, sizeof(int) * std::max<size_t>(nhi, 1));
+    for (int x = 0; x < 3; ++x) pl.off_cls_rows[x] = carve(at, sizeof(int) * std::max<size_t>(nhi, 1));
     for (int y = 0; y < 3; ++y) pl.off_cls_kets[y] = carve(at, sizeof(int) * std::max<size_t>(nlo, 1));
     for (int c = 0; c < HLC_N_CLASSES; ++c) pl.off_cls_off[c] = carve(at, sizeof(long long) * (nhi + 1));
     pl.l = l;
@@ -762,27 +762,31 @@ int dftk_prepare_hl(const dftk_shells_t *shells, double tau_schwarz, double tau_
     }
     std::vector<long long> off_lo = prefix_offsets(qs[0], qs[1], false, tau_schwarz);
     const std::vector<long long> off_hi = prefix_offsets(qs[0], qs[0], true, tau_schwarz);
-    // thread-per-quartet classes: hi rows of pairs (d,s) / (d,p), lo rows by
-    // l_a + l_b, each ascending; those hi rows leave the (hi|lo) space
-    std::vector<int> cls_rows[2], cls_kets[3];
+    // thread-per-quartet classes: hi rows of kinds (d,s), (d,p), (d,d) and lo
+    // rows by l_a + l_b, each ascending; hi rows whose every (hi|lo) quartet
+    // belongs to a class leave the (hi|lo) space
+    std::vector<int> cls_rows[3], cls_kets[3];
     std::vector<long long> cls_off[HLC_N_CLASSES];
     for (size_t r = 0; r < qs[0].size(); ++r) {
         const int la = pl.l[pl.ab[0][2 * r]], lb = pl.l[pl.ab[0][2 * r + 1]];
-        if (la == 2 && lb <= 1) cls_rows[lb].push_back((int)r);
+        if (la == 2) cls_rows[lb].push_back((int)r);
     }
     for (size_t k = 0; k < qs[1].size(); ++k) cls_kets[pl.l[pl.ab[1][2 * k]] + pl.l[pl.ab[1][2 * k + 1]]].push_back((int)k);
     for (int c = 0; c < HLC_N_CLASSES; ++c) {
-        const int x = c / 3, y = c % 3;
+        const int bk = hlc_class_kinds[c][0], kk = hlc_class_kinds[c][1];
+        const std::vector<int> &bra = cls_rows[bk - 3];
+        const std::vector<int> &ket = kk < 3 ? cls_kets[kk] : cls_rows[kk - 3];
+        const std::vector<double> &qk = kk < 3 ? qs[1] : qs[0];
         std::vector<double> qx, qy;
-        for (int r : cls_rows[x]) qx.push_back(qs[0][r]);
-        for (int k : cls_kets[y]) qy.push_back(qs[1][k]);
-        cls_off[c] = prefix_offsets(qx, qy, false, tau_schwarz);
+        for (int r : bra) qx.push_back(qs[0][r]);
+        for (int k : ket) qy.push_back(qk[k]);
+        cls_off[c] = prefix_offsets(qx, qy, bk == kk, tau_schwarz);
         hl->cls_off[c] = (const long long *)(base + pl.off_cls_off[c]);
         hl->cls_total[c] = cls_off[c].back();
         DFTK_CUDA(cudaMemcpyAsync(base + pl.off_cls_off[c], cls_off[c].data(), sizeof(long long) * cls_off[c].size(),
                                   cudaMemcpyHostToDevice, s));
     }
-    for (int x = 0; x < 2; ++x) {
+    for (int x = 0; x < 3; ++x) {
         hl->cls_rows[x] = (const int *)(base + pl.off_cls_rows[x]);
         hl->n_cls_rows[x] = (long long)cls_rows[x].size();
         if (!cls_rows[x].empty())
@@ -799,8 +803,13 @@ int dftk_prepare_hl(const dftk_shells_t *shells, double tau_schwarz, double tau_
     {
         std::vector<long long> cnt(qs[0].size());
         for (size_t r = 0; r < cnt.size(); ++r) cnt[r] = off_lo[r + 1] - off_lo[r];
-        for (int x = 0; x < 2; ++x)
-            for (int r : cls_rows[x]) cnt[r] = 0;
+        for (int x = 0; x < 3; ++x) {
+            // rows of kind x leave (hi|lo) when classes (x|ss), (x|ps), (x|pp) all exist
+            int n = 0;
+            for (int c = 0; c < HLC_N_CLASSES; ++c) n += hlc_class_kinds[c][0] == x + 3 && hlc_class_kinds[c][1] < 3;
+            if (n == 3)
+                for (int r : cls_rows[x]) cnt[r] = 0;
+        }
         for (size_t r = 0; r < cnt.size(); ++r) off_lo[r + 1] = off_lo[r] + cnt[r];
     }
     long long *d_lo = (long long *)(base + pl.off_row[0]), *d_hi = (long long *)(base + pl.off_row[1]);
@@ -1172,6 +1181,8 @@ template <int LM, typename K> int hl_smem_optin(K kernel, size_t extra_static = 
 // One class kernel of the thread-per-quartet d classes: 128-thread blocks,
 // a grid of at most 16 resident blocks per SM striding over the class's
 // warp work items (32 candidates x ket-component split).
+static_assert(HLC_N_CLASSES == sizeof(((dftk_hl_t *)nullptr)->cls_off) / sizeof(void *),
+              "dftk_hl_t holds one candidate space per generated d class");
 template <int C> int launch_hlc(const HlcParams &P, cudaStream_t s)
 {
     if (P.total[C] == 0) return DFTK_OK;
@@ -1223,14 +1234,17 @@ int dftk_jk_hl(const dftk_shells_t *shells, const dftk_hl_t *hl, const double *D
     if (workspace_bytes < ws_bytes(shells->n_shells, shells->n_ao))
         return fail(DFTK_ERR_WORKSPACE, "dftk_jk_hl: workspace too small");
     long long cls_sum = 0;
+    unsigned long long cover = 0;
     for (int c = 0; c < HLC_N_CLASSES; ++c) {
-        const int x = c / 3, y = c % 3;
+        const int bk = hlc_class_kinds[c][0], kk = hlc_class_kinds[c][1];
+        const long long nb = hl->n_cls_rows[bk - 3], nk = kk < 3 ? hl->n_cls_kets[kk] : hl->n_cls_rows[kk - 3];
+        const void *kl = kk < 3 ? (const void *)hl->cls_kets[kk] : (const void *)hl->cls_rows[kk - 3];
         if (hl->cls_total[c] < 0 ||
-            (hl->cls_total[c] > 0 && (!hl->cls_off[c] || !hl->cls_rows[x] || !hl->cls_kets[y] ||
-                                      hl->n_cls_rows[x] <= 0 || hl->n_cls_rows[x] > hl->n_rows ||
-                                      hl->n_cls_kets[y] <= 0 || hl->n_cls_kets[y] > hl->lo.n_pairs)))
+            (hl->cls_total[c] > 0 && (!hl->cls_off[c] || !hl->cls_rows[bk - 3] || !kl || nb <= 0 ||
+                                      nb > hl->n_rows || nk <= 0 || nk > (kk < 3 ? hl->lo.n_pairs : hl->n_rows))))
             return fail(DFTK_ERR_ARG, "dftk_jk_hl: inconsistent class spaces");
         cls_sum += hl->cls_total[c];
+        if (hl->cls_off[c]) cover |= (1ull << (6 * bk + kk)) | (1ull << (6 * kk + bk));
     }
     DFTK_INIT();
     const long long total = hl->total[0] + hl->total[1];
@@ -1266,6 +1280,7 @@ int dftk_jk_hl(const dftk_shells_t *shells, const dftk_hl_t *hl, const double *D
     P.uhf = uhf;
     P.tau = tau;
     P.counts = counts;
+    P.cover = cover;
     if (cls_sum > 0) {
         HlcParams C;
         memset(&C, 0, sizeof(C));
@@ -1273,7 +1288,7 @@ int dftk_jk_hl(const dftk_shells_t *shells, const dftk_hl_t *hl, const double *D
         C.shell_ao = shells->ao;
         C.hi = hl->hi;
         C.lo = hl->lo;
-        for (int x = 0; x < 2; ++x) {
+        for (int x = 0; x < 3; ++x) {
             C.rows[x] = hl->cls_rows[x];
             C.n_rows[x] = hl->n_cls_rows[x];
         }
@@ -1294,7 +1309,9 @@ int dftk_jk_hl(const dftk_shells_t *shells, const dftk_hl_t *hl, const double *D
         C.tau = tau;
         C.counts = counts;
         if ((st = launch_hlc<0>(C, s)) || (st = launch_hlc<1>(C, s)) || (st = launch_hlc<2>(C, s)) ||
-            (st = launch_hlc<3>(C, s)) || (st = launch_hlc<4>(C, s)) || (st = launch_hlc<5>(C, s)))
+            (st = launch_hlc<3>(C, s)) || (st = launch_hlc<4>(C, s)) || (st = launch_hlc<5>(C, s)) ||
+            (st = launch_hlc<6>(C, s)) || (st = launch_hlc<7>(C, s)) || (st = launch_hlc<8>(C, s)) ||
+            (st = launch_hlc<9>(C, s)))
             return st;
     }
     if (total > 0) {

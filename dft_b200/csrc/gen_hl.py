@@ -1,6 +1,8 @@
-"""Generate straight-line McMurchie-Davidson code for the most frequent ERI
-classes with one d shell: (ds|ss), (ds|ps), (ds|pp), (dp|ss), (dp|ps),
-(dp|pp).
+"""Generate straight-line McMurchie-Davidson code for the ERI classes with a
+d shell and total momentum L <= 5: (ds|ss), (ds|ps), (ds|pp), (dp|ss),
+(dp|ps), (dp|pp), (dd|ss), (dd|ps), (ds|ds), (dp|ds).  Classes of higher L
+stay with the warp-per-quartet kernel (hl.cuh), whose shared scratch holds
+their larger Hermite sets.
 
 Writes ``hl_classes.cuh`` next to this file (committed, so a build needs no
 Python).  The scheme is the s/p generator's (gen_eri.py) with the bra
@@ -22,7 +24,7 @@ zz) and the block is scaled by 1/sqrt(prod (2 l_i - 1)!!) per component
 
 Records are the generic 13-field pair sets of the d path (SoA,
 ``base[(f * kmax + k) * stride + pair]``; 0 Px, 1 Py, 2 Pz, 3 p, 4 K, 5 h,
-6-8 PA, 9-11 PB); the bra pair's first shell is the d shell.
+6-8 PA, 9-11 PB); each pair's first shell has the larger momentum.
 """
 from __future__ import annotations
 
@@ -38,19 +40,23 @@ COMPS = {
     1: [(1, 0, 0), (0, 1, 0), (0, 0, 1)],
     2: [(2, 0, 0), (1, 1, 0), (0, 2, 0), (1, 0, 1), (0, 1, 1), (0, 0, 2)],
 }
-# (La, Lb, Lc, Ld, nsplit): nsplit > 1 splits the ket components (c, d) into
-# that many consecutive chunks, one per thread, so the W intermediates and the
-# block fit in registers.
+# Pair kinds (l_a >= l_b): 0 ss, 1 ps, 2 pp (the lo set), 3 ds, 4 dp, 5 dd
+# (the hi set).  A class is (bra kind | ket kind); its code is split into
+# chunks of bra components x chunks of ket components, one chunk per thread,
+# so the W intermediates and the block fit in registers.
+# (La, Lb, Lc, Ld, bra chunks, ket chunks)
 CLASSES = [
-    (2, 0, 0, 0, 1),
-    (2, 0, 1, 0, 1),
-    (2, 0, 1, 1, 3),
-    (2, 1, 0, 0, 1),
-    (2, 1, 1, 0, 3),
-    (2, 1, 1, 1, 9),
+    (2, 0, 0, 0, 1, 1),   # 0 (ds|ss)
+    (2, 0, 1, 0, 1, 1),   # 1 (ds|ps)
+    (2, 0, 1, 1, 1, 3),   # 2 (ds|pp)
+    (2, 1, 0, 0, 1, 1),   # 3 (dp|ss)
+    (2, 1, 1, 0, 1, 3),   # 4 (dp|ps)
+    (2, 1, 1, 1, 1, 9),   # 5 (dp|pp)
+    (2, 2, 0, 0, 3, 1),   # 6 (dd|ss)
+    (2, 2, 1, 0, 3, 3),   # 7 (dd|ps)
+    (2, 0, 2, 0, 1, 3),   # 8 (ds|ds)
+    (2, 1, 2, 0, 1, 6),   # 9 (dp|ds)
 ]
-# record fields the code reads per pair momentum sum on the ket side (s/p kets)
-KET_FIELDS = {0: 5, 1: 9, 2: 12}
 FIELD_NAMES = ["Px", "Py", "Pz", "p", "K", "h", "Ax", "Ay", "Az", "Bx", "By", "Bz"]
 
 
@@ -128,18 +134,33 @@ def loads(side, var, idx, fields):
     return out
 
 
-def gen_class(cid, la, lb, lc, ld, nsplit, split):
+def chunks(items, n):
+    size = len(items) // n
+    assert size * n == len(items)
+    return [items[k * size:(k + 1) * size] for k in range(n)]
+
+
+def kind(l1, l2):
+    return {(0, 0): 0, (1, 0): 1, (1, 1): 2, (2, 0): 3, (2, 1): 4, (2, 2): 5}[(l1, l2)]
+
+
+def gen_class(cid, la, lb, lc, ld, nab_split, ncd_split, split):
     pa, pk = la + lb, lc + ld
     L = pa + pk
+    nsplit = nab_split * ncd_split
     A, B, C, D = COMPS[la], COMPS[lb], COMPS[lc], COMPS[ld]
     all_cds = [(ic, id_) for ic in range(len(C)) for id_ in range(len(D))]
-    chunk = len(all_cds) // nsplit
-    assert chunk * nsplit == len(all_cds)
-    cds = all_cds[split * chunk:(split + 1) * chunk]
-    abs_ = [(ia, ib) for ia in range(len(A)) for ib in range(len(B))]
+    all_abs = [(ia, ib) for ia in range(len(A)) for ib in range(len(B))]
+    abs_ = chunks(all_abs, nab_split)[split // ncd_split]
+    cds = chunks(all_cds, ncd_split)[split % ncd_split]
     ket_terms = {m: e3d("k", C[ic], D[id_], sign=True) for m, (ic, id_) in enumerate(cds)}
     bra_terms = {n: e3d("b", A[ia], B[ib]) for n, (ia, ib) in enumerate(abs_)}
-    hb = herm(pa)
+    # Hermite bra indices this chunk's bra components use
+    hb_used = set()
+    for terms in bra_terms.values():
+        for h, _, _ in terms:
+            hb_used.add(h)
+    hb = [h for h in herm(pa) if h in hb_used]
     needed = set()
     for terms in ket_terms.values():
         for (tk, uk, vk), _, _ in terms:
@@ -165,9 +186,10 @@ def gen_class(cid, la, lb, lc, ld, nsplit, split):
         body.append("  T " + ", ".join(f"{w(m, h)} = T(0)" for h in hb) + ";")
     inner = ["#pragma unroll 1", "for (int j = 0; j < ket_n; ++j) {",
              "  if (qo * __ldg(ket_qp + j * ket_st) < eps) break;"]
-    inner += ["  " + x for x in loads("k", "ket", "j", range(KET_FIELDS[pk]))]
+    nket_fields = 5 if pk == 0 else (9 if ld == 0 else 12)
+    inner += ["  " + x for x in loads("k", "ket", "j", range(nket_fields))]
     inner.append("  ++evaluated;")
-    if pk == 2:
+    if (lc, ld) not in ((0, 0), (1, 0)):
         inner += ["  " + x for x in e_defs("k", lc, ld)]
     inner += ["  " + x for x in core]
     for m, terms in ket_terms.items():
@@ -204,19 +226,23 @@ def gen_class(cid, la, lb, lc, ld, nsplit, split):
                 body.append(f"I[{n * len(cds) + m}] *= T({f!r});")
     cd_c = ", ".join(str(ic) for ic, _ in cds)
     cd_d = ", ".join(str(id_) for _, id_ in cds)
+    ab_a = ", ".join(str(ia) for ia, _ in abs_)
+    ab_b = ", ".join(str(ib) for _, ib in abs_)
     nm = "spd"
     head = [
-        f"// class {cid}: ({nm[la]}{nm[lb]}|{nm[lc]}{nm[ld]}), ket components {split * chunk}..{(split + 1) * chunk - 1}"
-        f" of {len(all_cds)} (split {split} of {nsplit})",
+        f"// class {cid}: ({nm[la]}{nm[lb]}|{nm[lc]}{nm[ld]}), split {split} of {nsplit}: bra components"
+        f" {', '.join(f'{ia}{ib}' for ia, ib in abs_)}, ket components {', '.join(f'{ic}{id_}' for ic, id_ in cds)}",
         "template <typename T>",
         f"struct HlClass<T, {cid}, {split}> {{",
         f"  static constexpr int LA = {la}, LB = {lb}, LC = {lc}, LD = {ld}, L = {L};",
         f"  static constexpr int NA = {len(A)}, NB = {len(B)}, NC = {len(C)}, ND = {len(D)};",
-        f"  static constexpr int NSPLIT = {nsplit}, NCD = {len(cds)}, NI = {nloc};",
-        f"  static constexpr int KET_CLASS = {pk}, BRA_L = {lb};",
+        f"  static constexpr int NSPLIT = {nsplit}, NAB = {len(abs_)}, NCD = {len(cds)}, NI = {nloc};",
+        f"  static constexpr int BRA_KIND = {kind(la, lb)}, KET_KIND = {kind(lc, ld)};",
+        f"  __device__ static constexpr int ab_a(int n) {{ constexpr int v[] = {{{ab_a}}}; return v[n]; }}",
+        f"  __device__ static constexpr int ab_b(int n) {{ constexpr int v[] = {{{ab_b}}}; return v[n]; }}",
         f"  __device__ static constexpr int cd_c(int m) {{ constexpr int v[] = {{{cd_c}}}; return v[m]; }}",
         f"  __device__ static constexpr int cd_d(int m) {{ constexpr int v[] = {{{cd_d}}}; return v[m]; }}",
-        "  // Contracted, normalised block I[(ia NB + ib) NCD + m] of one quartet;",
+        "  // Contracted, normalised block I[n NCD + m] (bra component n, ket m) of one quartet;",
         "  // returns the primitive quartets evaluated (both sides sorted by",
         "  // descending primitive Schwarz factor, loops stop once q_bra q_ket < eps).",
         "  __device__ __forceinline__ static int run(",
@@ -237,24 +263,31 @@ def gen_class(cid, la, lb, lc, ld, nsplit, split):
     return head + ["    " + x for x in body] + tail
 
 
-def main():
+def render() -> str:
     out = [
         "// GENERATED by gen_hl.py -- do not edit by hand.",
-        "// Straight-line McMurchie-Davidson bodies for the (d s|s/p s/p) and",
-        "// (d p|s/p s/p) ERI classes.",
+        "// Straight-line McMurchie-Davidson bodies of the ERI classes with a d",
+        "// shell and total momentum <= 5.",
         "#pragma once",
         "",
         "template <typename T, int C, int S> struct HlClass;",
         "",
         f"#define HLC_N_CLASSES {len(CLASSES)}",
+        "// (bra kind, ket kind) per class: 0 ss, 1 ps, 2 pp, 3 ds, 4 dp, 5 dd",
+        "static const int hlc_class_kinds[HLC_N_CLASSES][2] = {"
+        + ", ".join(f"{{{kind(la, lb)}, {kind(lc, ld)}}}" for la, lb, lc, ld, _, _ in CLASSES) + "};",
         "",
     ]
-    for cid, (la, lb, lc, ld, ns) in enumerate(CLASSES):
-        for s in range(ns):
-            out += gen_class(cid, la, lb, lc, ld, ns, s)
+    for cid, (la, lb, lc, ld, nab, ncd) in enumerate(CLASSES):
+        for s in range(nab * ncd):
+            out += gen_class(cid, la, lb, lc, ld, nab, ncd, s)
+    return "\n".join(out) + "\n"
+
+
+def main():
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "hl_classes.cuh")
     with open(path, "w") as fh:
-        fh.write("\n".join(out) + "\n")
+        fh.write(render())
     print(path)
 
 

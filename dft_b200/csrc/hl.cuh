@@ -356,7 +356,18 @@ struct HlJkParams {
     int uhf;
     double tau;
     long long *counts;  // [2]: quartets evaluated, primitive quartets (NULL = not counted)
+    // bit 6 x + y: quartets of bra pair kind x and ket pair kind y belong to
+    // a thread-per-quartet class kernel (pair kinds: hlc_kind)
+    unsigned long long cover;
 };
+
+// Kind of the pair (a, b), l_a >= l_b: 0 ss, 1 ps, 2 pp, 3 ds, 4 dp, 5 dd;
+// -1 with an f shell.
+__device__ __forceinline__ int hlc_kind(int la, int lb)
+{
+    if (la > 2) return -1;
+    return la == 0 ? 0 : (la == 1 ? 1 + lb : 3 + lb);
+}
 
 // Digest the block s.I of quartet (ab|cd) into Y (J) and Z (K) with the
 // weights of the unique-quartet enumeration (same identities as the s/p
@@ -452,6 +463,10 @@ __global__ void __launch_bounds__(32) k_hl_jk(const HlJkParams P)
         const dftk_pairs_t &K = kind ? P.hi : P.lo;
         const int a = P.hi.ab[2 * row], b = P.hi.ab[2 * row + 1];
         const int c = K.ab[2 * ket], d = K.ab[2 * ket + 1];
+        if (P.cover) {
+            const int x = hlc_kind(P.sh.l[a], P.sh.l[b]), y = hlc_kind(P.sh.l[c], P.sh.l[d]);
+            if (x >= 0 && y >= 0 && ((P.cover >> (6 * x + y)) & 1)) continue;
+        }
         const float dm = quartet_dmax(P.sh, P.Dsh, a, b, c, d);
         if (P.hi.q[row] * K.q[ket] * (double)dm < P.tau) continue;
         hl_quartet<LM>(s, P.sh.l[a], P.sh.l[b], P.sh.l[c], P.sh.l[d], P.hi.rec64 + row, P.hi.qp + row, P.hi.n_pairs,

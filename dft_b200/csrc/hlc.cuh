@@ -1,23 +1,28 @@
-// Thread-per-quartet J/K kernels of the classes (ds|ss), (ds|ps), (ds|pp),
-// (dp|ss), (dp|ps), (dp|pp): the generated straight-line bodies of
-// hl_classes.cuh (gen_hl.py) over candidate spaces indexed through the d
-// path's pair sets (class rows of the hi set, class kets of the lo set), and
-// the s/p digestion (digest_block).  One warp takes 32 consecutive
-// candidates of one class (and one split of the ket components), as the s/p
-// scan kernel does; the quartets of a row are consecutive, so the bra pair is
-// usually warp-uniform.
+// Thread-per-quartet J/K kernels of the d classes with total momentum <= 5
+// ((ds|ss) .. (dp|ds), hl_classes.cuh, generated by gen_hl.py): candidate
+// spaces indexed through the d path's pair sets (the hi rows of one pair kind
+// as bras; the lo rows of one kind, or the hi rows of one kind, as kets), and
+// the s/p digestion generalised to threads that hold a chunk of bra and of
+// ket components.  One warp takes 32 consecutive candidates of one class (and
+// one component chunk), as the s/p scan kernel does; the quartets of a row
+// are consecutive, so the bra pair is usually warp-uniform.
+//
+// Pair kinds: 0 ss, 1 ps, 2 pp (lo set), 3 ds, 4 dp, 5 dd (hi set); pairs
+// with an f shell have no kind and stay with the warp-per-quartet kernel.
 #pragma once
 
 #include "hl.cuh"
 #include "hl_classes.cuh"
 
+#define HLC_N_KINDS 6
+
 struct HlcParams {
     dftk_shells_t sh;
     const int *shell_ao;
     dftk_pairs_t hi, lo;
-    const int *rows[2];
-    long long n_rows[2];
-    const int *kets[3];
+    const int *rows[3];  // hi rows of kinds ds, dp, dd
+    long long n_rows[3];
+    const int *kets[3];  // lo rows of kinds ss, ps, pp
     const long long *off[HLC_N_CLASSES];
     long long total[HLC_N_CLASSES];
     float tau_prim;
@@ -29,30 +34,143 @@ struct HlcParams {
     long long *counts;  // [2]: quartets evaluated, primitive quartets (NULL = not counted)
 };
 
+// whether a thread's chunk of class E holds bra component ia (a) / ib (b)
+template <typename E>
+__device__ __forceinline__ constexpr bool chunk_has_a(int ia)
+{
+    for (int n = 0; n < E::NAB; ++n)
+        if (E::ab_a(n) == ia) return true;
+    return false;
+}
+template <typename E>
+__device__ __forceinline__ constexpr bool chunk_has_b(int ib)
+{
+    for (int n = 0; n < E::NAB; ++n)
+        if (E::ab_b(n) == ib) return true;
+    return false;
+}
+
+// Digest a chunk I[n NCD + m] (bra components ab_a/ab_b(n), ket components
+// cd_c/cd_d(m)) into Y and Z with the identities of digest_block; each
+// thread adds its chunk's partial sums.
+template <typename E>
+__device__ __forceinline__ void hlc_digest(const HlcParams &P, bool valid, bool uniform_bra, int a, int b, int c,
+                                           int d, double w, const double (&I)[E::NI])
+{
+    constexpr int NA = E::NA, NB = E::NB, NC = E::NC, ND = E::ND, NAB = E::NAB, NCD = E::NCD;
+    const MolView mv = mol_view(P.sh, a);
+    const int N = mv.nao;
+    const int oa = P.shell_ao[a], ob = P.shell_ao[b], oc = P.shell_ao[c], od = P.shell_ao[d];
+    const double fJ = valid ? 2.0 / w : 0.0;
+    const double fK = valid ? 1.0 / w : 0.0;
+    double v[E::NI];
+#pragma unroll
+    for (int q = 0; q < E::NI; ++q) v[q] = valid ? I[q] : 0.0;
+    const double *D = P.D + mv.mat;
+    double *Yb = P.Y + mv.mat;
+    // Y_cd
+#pragma unroll
+    for (int m = 0; m < NCD; ++m) {
+        double s = 0.0;
+#pragma unroll
+        for (int n = 0; n < NAB; ++n)
+            s = fma(v[n * NCD + m], __ldg(D + (long long)(oa + E::ab_a(n)) * N + ob + E::ab_b(n)), s);
+        if (valid) atomicAdd(Yb + (long long)(oc + E::cd_c(m)) * N + od + E::cd_d(m), fJ * s);
+    }
+    // Y_ab
+#pragma unroll
+    for (int n = 0; n < NAB; ++n) {
+        double s = 0.0;
+#pragma unroll
+        for (int m = 0; m < NCD; ++m)
+            s = fma(v[n * NCD + m], __ldg(D + (long long)(oc + E::cd_c(m)) * N + od + E::cd_d(m)), s);
+        s *= fJ;
+        if (uniform_bra) {
+            s = warp_sum(s);
+            if ((threadIdx.x & 31) == 0) atomicAdd(Yb + (long long)(oa + E::ab_a(n)) * N + ob + E::ab_b(n), s);
+        } else if (valid) {
+            atomicAdd(Yb + (long long)(oa + E::ab_a(n)) * N + ob + E::ab_b(n), s);
+        }
+    }
+    for (int spin = 0; spin < (P.uhf ? 2 : 1); ++spin) {
+        const double *Ds = (spin ? P.Db : P.Da) + mv.mat;
+        double *Z = (spin ? P.Zb : P.Za) + mv.mat;
+        double zac[NA][NC], zad[NA][ND], zbc[NB][NC], zbd[NB][ND];
+#pragma unroll
+        for (int i = 0; i < NA; ++i) {
+#pragma unroll
+            for (int j = 0; j < NC; ++j) zac[i][j] = 0.0;
+#pragma unroll
+            for (int j = 0; j < ND; ++j) zad[i][j] = 0.0;
+        }
+#pragma unroll
+        for (int i = 0; i < NB; ++i) {
+#pragma unroll
+            for (int j = 0; j < NC; ++j) zbc[i][j] = 0.0;
+#pragma unroll
+            for (int j = 0; j < ND; ++j) zbd[i][j] = 0.0;
+        }
+#pragma unroll
+        for (int n = 0; n < NAB; ++n)
+#pragma unroll
+            for (int m = 0; m < NCD; ++m) {
+                const int ia = E::ab_a(n), ib = E::ab_b(n), cc = E::cd_c(m), dd = E::cd_d(m);
+                const double val = v[n * NCD + m] * fK;
+                zac[ia][cc] = fma(val, __ldg(Ds + (long long)(ob + ib) * N + od + dd), zac[ia][cc]);
+                zad[ia][dd] = fma(val, __ldg(Ds + (long long)(ob + ib) * N + oc + cc), zad[ia][dd]);
+                zbc[ib][cc] = fma(val, __ldg(Ds + (long long)(oa + ia) * N + od + dd), zbc[ib][cc]);
+                zbd[ib][dd] = fma(val, __ldg(Ds + (long long)(oa + ia) * N + oc + cc), zbd[ib][dd]);
+            }
+        if (valid) {
+#pragma unroll
+            for (int ia = 0; ia < NA; ++ia) {
+                if (!chunk_has_a<E>(ia)) continue;
+#pragma unroll
+                for (int cc = 0; cc < NC; ++cc)
+                    if (split_has_c<E>(cc)) atomicAdd(Z + (long long)(oa + ia) * N + oc + cc, zac[ia][cc]);
+#pragma unroll
+                for (int dd = 0; dd < ND; ++dd)
+                    if (split_has_d<E>(dd)) atomicAdd(Z + (long long)(oa + ia) * N + od + dd, zad[ia][dd]);
+            }
+#pragma unroll
+            for (int ib = 0; ib < NB; ++ib) {
+                if (!chunk_has_b<E>(ib)) continue;
+#pragma unroll
+                for (int cc = 0; cc < NC; ++cc)
+                    if (split_has_c<E>(cc)) atomicAdd(Z + (long long)(ob + ib) * N + oc + cc, zbc[ib][cc]);
+#pragma unroll
+                for (int dd = 0; dd < ND; ++dd)
+                    if (split_has_d<E>(dd)) atomicAdd(Z + (long long)(ob + ib) * N + od + dd, zbd[ib][dd]);
+            }
+        }
+    }
+}
+
 template <int C, int S>
 __device__ __forceinline__ void hlc_one(const HlcParams &P, bool valid, int row, int ket)
 {
     using E = HlClass<double, C, S>;
+    constexpr bool KET_HI = E::KET_KIND >= 3;
+    const dftk_pairs_t &K = KET_HI ? P.hi : P.lo;
     const int lead = __ffs(__ballot_sync(DFTK_FULL_MASK, valid)) - 1;
     const int row0 = __shfl_sync(DFTK_FULL_MASK, row, lead < 0 ? 0 : lead);
     const bool uniform = __all_sync(DFTK_FULL_MASK, !valid || row == row0);
     const int brow = valid ? row : row0;
     const int a = P.hi.ab[2 * brow], b = P.hi.ab[2 * brow + 1];
-    const int c = valid ? P.lo.ab[2 * ket] : 0, d = valid ? P.lo.ab[2 * ket + 1] : 0;
+    const int c = valid ? K.ab[2 * ket] : 0, d = valid ? K.ab[2 * ket + 1] : 0;
     double I[E::NI];
     int evaluated = 0;
     if (valid) {
-        evaluated = E::run(P.hi.rec64, P.hi.qp, P.hi.n_pairs, P.hi.kmax, row, P.hi.nprim[row], P.lo.rec64, P.lo.qp,
-                           P.lo.n_pairs, P.lo.kmax, ket, P.lo.nprim[ket], P.tau_prim, I);
+        evaluated = E::run(P.hi.rec64, P.hi.qp, P.hi.n_pairs, P.hi.kmax, row, P.hi.nprim[row], K.rec64, K.qp,
+                           K.n_pairs, K.kmax, ket, K.nprim[ket], P.tau_prim, I);
     } else {
 #pragma unroll
         for (int q = 0; q < E::NI; ++q) I[q] = 0.0;
     }
-    // a hi pair never equals a lo pair, and a != b (different momenta)
-    const int ew = c == d;
-    digest_block<E>(P, valid, uniform, a, b, c, d, (double)(1 << ew), I);
+    const int ew = (a == b) + (c == d) + ((E::BRA_KIND == E::KET_KIND) && row == ket);
+    hlc_digest<E>(P, valid, uniform, a, b, c, d, (double)(1 << ew), I);
     if (P.counts) {
-        // each split evaluates the same primitive quartets: count split 0
+        // every chunk evaluates the same primitive quartets: count chunk 0
         int tot = S == 0 ? evaluated : 0;
         int nq = (S == 0 && valid) ? 1 : 0;
 #pragma unroll
@@ -82,7 +200,10 @@ __global__ void __launch_bounds__(128) k_hlc(const HlcParams P)
 {
     using E0 = HlClass<double, C, 0>;
     constexpr int NS = E0::NSPLIT;
-    constexpr int X = E0::BRA_L, Yc = E0::KET_CLASS;
+    constexpr int X = E0::BRA_KIND - 3, Yk = E0::KET_KIND;
+    constexpr bool KET_HI = Yk >= 3;
+    const dftk_pairs_t &K = KET_HI ? P.hi : P.lo;
+    const int *kets = KET_HI ? P.rows[Yk - 3] : P.kets[Yk];
     const long long ncand = P.total[C];
     const long long nwork = ((ncand + 31) >> 5) * NS;
     const int lane = threadIdx.x & 31;
@@ -95,11 +216,11 @@ __global__ void __launch_bounds__(128) k_hlc(const HlcParams P)
         if (valid) {
             const int r = find_row(P.off[C], P.n_rows[X], cand);
             row = __ldg(P.rows[X] + r);
-            ket = __ldg(P.kets[Yc] + (cand - __ldg(P.off[C] + r)));
+            ket = __ldg(kets + (cand - __ldg(P.off[C] + r)));
             const int a = P.hi.ab[2 * row], b = P.hi.ab[2 * row + 1];
-            const int c = P.lo.ab[2 * ket], d = P.lo.ab[2 * ket + 1];
+            const int c = K.ab[2 * ket], d = K.ab[2 * ket + 1];
             const float dm = quartet_dmax(P.sh, P.Dsh, a, b, c, d);
-            valid = __ldg(P.hi.q + row) * __ldg(P.lo.q + ket) * (double)dm >= P.tau;
+            valid = __ldg(P.hi.q + row) * __ldg(K.q + ket) * (double)dm >= P.tau;
         }
         if (!__any_sync(DFTK_FULL_MASK, valid)) continue;
         hlc_split<C, 0>(P, split, valid, row, ket);

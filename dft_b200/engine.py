@@ -267,21 +267,27 @@ class IntegralEngine:
         off_lo = candidate_offsets(q_hi, q_lo, False, self.tau_schwarz)
         off_hi = candidate_offsets(q_hi, q_hi, True, self.tau_schwarz)
         a, b = self._pair_a, self._pair_b
-        # thread-per-quartet classes: hi rows of pairs (d,s) / (d,p), lo rows by l_a + l_b
+        # thread-per-quartet classes: hi rows of kinds (d,s), (d,p), (d,d)
+        # and lo rows by l_a + l_b, as index lists into the two pair sets
         hi_kind = np.where(self.l[a[sel_hi]] == 2, self.l[b[sel_hi]], 9)
         lo_kind = self.l[a[sel_lo]] + self.l[b[sel_lo]]
-        self.hlc_rows = [np.nonzero(hi_kind == x)[0].astype(np.int32) if self.hl_classes else np.zeros(0, np.int32)
-                         for x in range(2)]
+        self.hlc_rows = [np.nonzero(hi_kind == x)[0].astype(np.int32) for x in range(3)]
         self.hlc_kets = [np.nonzero(lo_kind == y)[0].astype(np.int32) for y in range(3)]
         hlc_off = []
-        for c in range(6):
-            x, y = divmod(c, 3)
-            hlc_off.append(candidate_offsets(q_hi[self.hlc_rows[x]], q_lo[self.hlc_kets[y]], False, self.tau_schwarz))
+        for bk, kk in _lib.HLC_CLASS_KINDS:
+            bra = self.hlc_rows[bk - 3]
+            ket, qk = (self.hlc_kets[kk], q_lo) if kk < 3 else (self.hlc_rows[kk - 3], q_hi)
+            hlc_off.append(candidate_offsets(q_hi[bra], qk[ket], bk == kk, self.tau_schwarz))
         if self.hl_classes:
-            # those rows' (hi|lo) quartets leave the warp kernel's space
+            # rows whose every (hi|lo) quartet belongs to a class leave the
+            # warp kernel's (hi|lo) space
             cnt = np.diff(off_lo)
-            cnt[np.concatenate(self.hlc_rows)] = 0
+            for x in range(3):
+                if sum(1 for bk, kk in _lib.HLC_CLASS_KINDS if bk == x + 3 and kk < 3) == 3:
+                    cnt[self.hlc_rows[x]] = 0
             off_lo = np.concatenate([[0], np.cumsum(cnt)]).astype(np.int64)
+        else:
+            hlc_off = [np.zeros(1, dtype=np.int64) for _ in hlc_off]
         self.hlc_totals = [int(o[-1]) for o in hlc_off]
         self.hl_bufs = (hi_bufs, lo_bufs)
         self.hl_row_off = (self._t(off_lo, torch.int64), self._t(off_hi, torch.int64))
@@ -296,20 +302,21 @@ class IntegralEngine:
             hl.row_off[k] = _lib.ptr(self.hl_row_off[k]).value
         hl.tau_prim = self.tau_prim
         hl.lmax = self.hl_lmax
-        self.hlc_dev = ([self._t(r, torch.int32) if r.size else None for r in self.hlc_rows],
-                        [self._t(k, torch.int32) if k.size else None for k in self.hlc_kets],
-                        [self._t(o, torch.int64) for o in hlc_off])
-        for x in range(2):
-            if self.hlc_rows[x].size:
-                hl.cls_rows[x] = _lib.ptr(self.hlc_dev[0][x]).value
-                hl.n_cls_rows[x] = int(self.hlc_rows[x].size)
-        for y in range(3):
-            if self.hlc_kets[y].size:
-                hl.cls_kets[y] = _lib.ptr(self.hlc_dev[1][y]).value
-                hl.n_cls_kets[y] = int(self.hlc_kets[y].size)
-        for c in range(6):
-            hl.cls_off[c] = _lib.ptr(self.hlc_dev[2][c]).value
-            hl.cls_total[c] = self.hlc_totals[c]
+        if self.hl_classes:
+            self.hlc_dev = ([self._t(r, torch.int32) if r.size else None for r in self.hlc_rows],
+                            [self._t(k, torch.int32) if k.size else None for k in self.hlc_kets],
+                            [self._t(o, torch.int64) for o in hlc_off])
+            for x in range(3):
+                if self.hlc_rows[x].size:
+                    hl.cls_rows[x] = _lib.ptr(self.hlc_dev[0][x]).value
+                    hl.n_cls_rows[x] = int(self.hlc_rows[x].size)
+            for y in range(3):
+                if self.hlc_kets[y].size:
+                    hl.cls_kets[y] = _lib.ptr(self.hlc_dev[1][y]).value
+                    hl.n_cls_kets[y] = int(self.hlc_kets[y].size)
+            for c in range(_lib.HLC_N_CLASSES):
+                hl.cls_off[c] = _lib.ptr(self.hlc_dev[2][c]).value
+                hl.cls_total[c] = self.hlc_totals[c]
         self.c_hl = hl
 
     # ---------------------------------------------------------------- queries

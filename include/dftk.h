@@ -168,21 +168,25 @@ typedef struct {
     const long long *row_off[2];  /* device [n_rows + 1] each: Schwarz prefixes as in dftk_queue_t */
     double tau_prim;              /* primitive-quartet cut, as in dftk_queue_t */
     int lmax;                     /* largest shell momentum, 2 (d) or 3 (f): selects the kernels' scratch layout */
-    /* Thread-per-quartet classes (ds|ss), (ds|ps), (ds|pp), (dp|ss), (dp|ps),
-     * (dp|pp) (class 3 x + y: x = 0 for hi pairs (d,s), 1 for (d,p); y = the
-     * lo pair's l_a + l_b).  cls_rows[x] lists the hi rows of pairs of kind x
-     * and cls_kets[y] the lo rows of kind y, each ascending (so by descending
-     * Schwarz factor); cls_off[3 x + y] are the candidate offsets over those
-     * lists (the ket prefix of row r: cls_kets[y][0 .. count_r)), cls_total
-     * their totals.  These spaces and (hi|lo) must not overlap: give the rows
-     * in cls_rows zero (hi|lo) candidates in row_off[0].  All zero: (hi|lo)
-     * runs entirely in the warp-per-quartet kernel. */
-    const int *cls_rows[2];
-    long long n_cls_rows[2];
+    /* Thread-per-quartet classes (generated code, total momentum <= 5): class
+     * c = 0 (ds|ss), 1 (ds|ps), 2 (ds|pp), 3 (dp|ss), 4 (dp|ps), 5 (dp|pp),
+     * 6 (dd|ss), 7 (dd|ps), 8 (ds|ds), 9 (dp|ds).  cls_rows[x] lists the hi
+     * rows of pair kind x = 0 (d,s), 1 (d,p), 2 (d,d) and cls_kets[y] the lo
+     * rows of kind y = 0 (s,s), 1 (p,s), 2 (p,p), each ascending (so by
+     * descending Schwarz factor).  cls_off[c] are the candidate offsets over
+     * the class's bra list (row r keeps the ket prefix of its ket list:
+     * cls_kets[y] for kets from the lo set, cls_rows[y] for (ds|ds) and
+     * (dp|ds); (ds|ds) cut at k <= r), cls_total[c] their totals.  A class
+     * whose cls_off is non-NULL takes every quartet of its two pair kinds:
+     * the warp-per-quartet kernel skips them, and a host may give the hi rows
+     * whose every (hi|lo) quartet belongs to a class zero candidates in
+     * row_off[0].  All NULL: every d quartet runs in the warp kernel. */
+    const int *cls_rows[3];
+    long long n_cls_rows[3];
     const int *cls_kets[3];
     long long n_cls_kets[3];
-    const long long *cls_off[6];
-    long long cls_total[6];
+    const long long *cls_off[10];
+    long long cls_total[10];
 } dftk_hl_t;
 
 /* library version (integer, 100 * major + minor) */

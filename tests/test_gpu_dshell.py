@@ -180,17 +180,18 @@ def test_f_shell_eris_and_jk_vs_oracle(oracle_mod):
 
 def test_thread_classes_match_warp_path_and_oracle(oracle_mod):
     """(H2O)_2 with the generally contracted d-polarised basis: the generated
-    thread-per-quartet kernels of (ds|ss)..(dp|pp) plus the warp kernel for
-    the rest give the warp kernel's J/K alone (1e-12) and the oracle's direct
-    J/K (1e-11 relative), UHF densities with no structure; the class spaces
-    and the remaining (hi|lo) space partition the unmasked (hi|lo) space."""
+    thread-per-quartet kernels of the ten d classes with L <= 5 plus the warp
+    kernel for the rest give the warp kernel's J/K alone (1e-12) and the
+    oracle's direct J/K (1e-11 relative), UHF densities with no structure."""
     atoms, centers = geometry.water_cluster((1, 1, 2))
     data = _gc_basis()
     sh = basis.build_shells(data, atoms, centers)
     eng = IntegralEngine(sh, tau_schwarz=0.0)
     warp = IntegralEngine(sh, tau_schwarz=0.0, hl_classes=False)
     assert all(t > 0 for t in eng.hlc_totals)
-    assert sum(eng.hlc_totals) + eng.hl_totals[0] == warp.hl_totals[0]
+    # (ds|..) and (dp|..) rows leave the warp kernel's (hi|lo) space; (dd|..)
+    # rows and (hi|hi) stay there, their class quartets skipped in-kernel
+    assert sum(eng.hlc_totals[:6]) + eng.hl_totals[0] == warp.hl_totals[0]
     assert eng.hl_totals[1] == warp.hl_totals[1] and sum(warp.hlc_totals) == 0
     N = eng.n_ao
     rng = np.random.default_rng(17)
@@ -212,8 +213,9 @@ def test_thread_classes_match_warp_path_and_oracle(oracle_mod):
 
 def test_thread_classes_screened_density_counts():
     """Screening through the class kernels: at a tau that cuts part of the
-    (ds|ss)..(dp|pp) quartets the J/K still equal the warp kernel's at the
-    same tau, and the evaluated-quartet counters of both paths agree."""
+    d quartets the J/K still equal the warp kernel's at the same tau, and the
+    evaluated-quartet counters of both paths agree (every quartet is
+    evaluated by exactly one kernel)."""
     atoms, centers = geometry.water_cluster((1, 2, 2))
     sh = basis.build_shells(_gc_basis(), atoms, centers)
     eng = IntegralEngine(sh, tau_schwarz=1e-12)

@@ -302,3 +302,23 @@ def test_batch_pack_index_round_trip():
     for m, n in enumerate(nao):
         np.testing.assert_array_equal(padded[m, :n, :n], blocks[m])
         assert not padded[m, n:, :].any() and not padded[m, :, n:].any()
+
+
+def test_generated_d_classes_are_current():
+    """hl_classes.cuh is exactly what gen_hl.py renders, and the class kind
+    table the host uses equals the one the kernels were generated with."""
+    import os
+    import sys
+
+    from dft_b200 import _lib
+
+    csrc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "dft_b200", "csrc")
+    sys.path.insert(0, csrc)
+    try:
+        import gen_hl
+    finally:
+        sys.path.remove(csrc)
+    with open(os.path.join(csrc, "hl_classes.cuh")) as fh:
+        assert fh.read() == gen_hl.render()
+    kinds = [(gen_hl.kind(la, lb), gen_hl.kind(lc, ld)) for la, lb, lc, ld, _, _ in gen_hl.CLASSES]
+    assert kinds == _lib.HLC_CLASS_KINDS
