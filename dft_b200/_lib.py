@@ -99,8 +99,12 @@ class Queue(ctypes.Structure):
 
 # thread-per-quartet d classes: (bra pair kind, ket pair kind), kinds 0 ss,
 # 1 ps, 2 pp, 3 ds, 4 dp, 5 dd (the table of hl_classes.cuh)
-HLC_CLASS_KINDS = [(3, 0), (3, 1), (3, 2), (4, 0), (4, 1), (4, 2), (5, 0), (5, 1), (3, 3), (4, 3)]
+HLC_CLASS_KINDS = [(3, 0), (3, 1), (3, 2), (4, 0), (4, 1), (4, 2), (5, 0), (5, 1), (3, 3), (4, 3), (4, 4), (5, 2),
+                   (5, 3)]
 HLC_N_CLASSES = len(HLC_CLASS_KINDS)
+# primitive-pair-count buckets of the class ket lists (DFTK_HLC_BUCKET_BOUNDS)
+HLC_BUCKET_BOUNDS = [1, 4, 9, 16, 36, 1 << 30]
+HLC_NB = len(HLC_BUCKET_BOUNDS)
 
 
 class HlSet(ctypes.Structure):
@@ -115,8 +119,8 @@ class HlSet(ctypes.Structure):
         ("lmax", ctypes.c_int),
         ("cls_rows", ctypes.c_void_p * 3),
         ("n_cls_rows", ctypes.c_longlong * 3),
-        ("cls_kets", ctypes.c_void_p * 3),
-        ("n_cls_kets", ctypes.c_longlong * 3),
+        ("cls_kets", ctypes.c_void_p * 6),
+        ("cls_ket_seg", (ctypes.c_longlong * (HLC_NB + 1)) * 6),
         ("cls_off", ctypes.c_void_p * HLC_N_CLASSES),
         ("cls_total", ctypes.c_longlong * HLC_N_CLASSES),
     ]

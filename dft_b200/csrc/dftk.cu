@@ -617,7 +617,8 @@ struct PrepareHlPlan {
     std::vector<int> l;      // shell momenta
     std::vector<int> ab[2];  // 0 hi, 1 lo
     size_t off_ab[2], off_np[2], off_r64[2], off_r32[2], off_q[2], off_qp[2], off_row[2];
-    size_t off_cls_rows[3], off_cls_kets[3], off_cls_off[HLC_N_CLASSES];
+    size_t off_cls_rows[3], off_cls_kets[HLC_N_KINDS], off_cls_off[HLC_N_CLASSES];
+    std::vector<int> np;  // primitives per shell
     size_t bytes = 0;
 };
 
@@ -659,9 +660,10 @@ int prepare_hl_plan(const dftk_shells_t *shells, PrepareHlPlan &pl)
     for (int k = 0; k < 2; ++k) pl.off_row[k] = carve(at, sizeof(long long) * (pl.ab[0].size() / 2 + 1));
     const size_t nhi = pl.ab[0].size() / 2, nlo = pl.ab[1].size() / 2;
     for (int x = 0; x < 3; ++x) pl.off_cls_rows[x] = carve(at, sizeof(int) * std::max<size_t>(nhi, 1));
-    for (int y = 0; y < 3; ++y) pl.off_cls_kets[y] = carve(at, sizeof(int) * std::max<size_t>(nlo, 1));
-    for (int c = 0; c < HLC_N_CLASSES; ++c) pl.off_cls_off[c] = carve(at, sizeof(long long) * (nhi + 1));
+    for (int y = 0; y < HLC_N_KINDS; ++y) pl.off_cls_kets[y] = carve(at, sizeof(int) * std::max<size_t>(y < 3 ? nlo : nhi, 1));
+    for (int c = 0; c < HLC_N_CLASSES; ++c) pl.off_cls_off[c] = carve(at, sizeof(long long) * (nhi * DFTK_HLC_NB + 1));
     pl.l = l;
+    pl.np = np;
     pl.bytes = at;
     return DFTK_OK;
 }
@@ -690,6 +692,86 @@ std::vector<long long> prefix_offsets(const std::vector<double> &qx, const std::
         off[r + 1] = off[r] + cnt;
     }
     return off;
+}
+
+// Candidate spaces of the thread-per-quartet d classes over one pair
+// layout (hi / lo lists of (a, b) in Schwarz order with their q): bra lists
+// per hi kind, ket lists per kind grouped by primitive-count bucket, and the
+// offsets over (bra position, bucket), as dftk_hl_t documents them.
+struct ClassSpaces {
+    std::vector<int> rows[3], kets[HLC_N_KINDS];
+    long long seg[HLC_N_KINDS][DFTK_HLC_NB + 1];
+    std::vector<long long> off[HLC_N_CLASSES];
+};
+
+int hlc_bucket(long long nprim)
+{
+    static const long long bounds[DFTK_HLC_NB] = DFTK_HLC_BUCKET_BOUNDS;
+    for (int b = 0; b < DFTK_HLC_NB; ++b)
+        if (nprim <= bounds[b]) return b;
+    return DFTK_HLC_NB - 1;
+}
+
+void class_spaces(const std::vector<int> &l, const std::vector<int> &np, const std::vector<int> (&ab)[2],
+                  const std::vector<double> (&qs)[2], double tau, ClassSpaces &cs)
+{
+    std::vector<int> kind_lists[HLC_N_KINDS];
+    for (int set = 0; set < 2; ++set)
+        for (size_t r = 0; r < qs[set].size(); ++r) {
+            const int la = l[ab[set][2 * r]], lb = l[ab[set][2 * r + 1]];
+            if (la > 2) continue;
+            const int kind = la == 0 ? 0 : (la == 1 ? 1 + lb : 3 + lb);
+            if (kind >= 3) cs.rows[kind - 3].push_back((int)r);
+            kind_lists[kind].push_back((int)r);
+        }
+    for (int y = 0; y < HLC_N_KINDS; ++y) {
+        const int set = y < 3 ? 1 : 0;
+        std::vector<int> &kl = cs.kets[y];
+        kl.clear();
+        for (int b = 0; b < DFTK_HLC_NB; ++b) {
+            cs.seg[y][b] = (long long)kl.size();
+            for (int r : kind_lists[y]) {
+                const long long n = (long long)np[ab[set][2 * r]] * np[ab[set][2 * r + 1]];
+                if (hlc_bucket(n) == b) kl.push_back(r);
+            }
+        }
+        cs.seg[y][DFTK_HLC_NB] = (long long)kl.size();
+    }
+    for (int c = 0; c < HLC_N_CLASSES; ++c) {
+        const int bk = hlc_class_kinds[c][0], kk = hlc_class_kinds[c][1];
+        const std::vector<int> &bra = cs.rows[bk - 3];
+        const std::vector<double> &qk = kk < 3 ? qs[1] : qs[0];
+        const std::vector<int> &kl = cs.kets[kk];
+        std::vector<long long> &off = cs.off[c];
+        off.assign(bra.size() * DFTK_HLC_NB + 1, 0);
+        for (size_t i = 0; i < bra.size(); ++i) {
+            const int r = bra[i];
+            for (int b = 0; b < DFTK_HLC_NB; ++b) {
+                long long lo = cs.seg[kk][b], hi = cs.seg[kk][b + 1], cnt = 0;
+                if (qs[0][r] > 0.0) {
+                    const double thr = tau / qs[0][r];
+                    long long x = lo, y = hi;  // first ket of the segment with q < thr
+                    while (x < y) {
+                        const long long mid = (x + y) / 2;
+                        if (qk[kl[mid]] >= thr) x = mid + 1;
+                        else y = mid;
+                    }
+                    long long end = x;
+                    if (bk == kk) {  // same pair set: kets whose row is <= the bra's
+                        long long u = lo, v = hi;
+                        while (u < v) {
+                            const long long mid = (u + v) / 2;
+                            if (kl[mid] <= r) u = mid + 1;
+                            else v = mid;
+                        }
+                        end = std::min(end, u);
+                    }
+                    cnt = end - lo;
+                }
+                off[i * DFTK_HLC_NB + b + 1] = off[i * DFTK_HLC_NB + b] + cnt;
+            }
+        }
+    }
 }
 
 }  // namespace
@@ -761,43 +843,28 @@ int dftk_prepare_hl(const dftk_shells_t *shells, double tau_schwarz, double tau_
         }
     }
     std::vector<long long> off_lo = prefix_offsets(qs[0], qs[1], false, tau_schwarz);
-    const std::vector<long long> off_hi = prefix_offsets(qs[0], qs[0], true, tau_schwarz);
-    // thread-per-quartet classes: hi rows of kinds (d,s), (d,p), (d,d) and lo
-    // rows by l_a + l_b, each ascending; hi rows whose every (hi|lo) quartet
-    // belongs to a class leave the (hi|lo) space
-    std::vector<int> cls_rows[3], cls_kets[3];
-    std::vector<long long> cls_off[HLC_N_CLASSES];
-    for (size_t r = 0; r < qs[0].size(); ++r) {
-        const int la = pl.l[pl.ab[0][2 * r]], lb = pl.l[pl.ab[0][2 * r + 1]];
-        if (la == 2) cls_rows[lb].push_back((int)r);
-    }
-    for (size_t k = 0; k < qs[1].size(); ++k) cls_kets[pl.l[pl.ab[1][2 * k]] + pl.l[pl.ab[1][2 * k + 1]]].push_back((int)k);
+    std::vector<long long> off_hi = prefix_offsets(qs[0], qs[0], true, tau_schwarz);
+    // thread-per-quartet classes
+    ClassSpaces cs;
+    class_spaces(pl.l, pl.np, pl.ab, qs, tau_schwarz, cs);
     for (int c = 0; c < HLC_N_CLASSES; ++c) {
-        const int bk = hlc_class_kinds[c][0], kk = hlc_class_kinds[c][1];
-        const std::vector<int> &bra = cls_rows[bk - 3];
-        const std::vector<int> &ket = kk < 3 ? cls_kets[kk] : cls_rows[kk - 3];
-        const std::vector<double> &qk = kk < 3 ? qs[1] : qs[0];
-        std::vector<double> qx, qy;
-        for (int r : bra) qx.push_back(qs[0][r]);
-        for (int k : ket) qy.push_back(qk[k]);
-        cls_off[c] = prefix_offsets(qx, qy, bk == kk, tau_schwarz);
         hl->cls_off[c] = (const long long *)(base + pl.off_cls_off[c]);
-        hl->cls_total[c] = cls_off[c].back();
-        DFTK_CUDA(cudaMemcpyAsync(base + pl.off_cls_off[c], cls_off[c].data(), sizeof(long long) * cls_off[c].size(),
+        hl->cls_total[c] = cs.off[c].back();
+        DFTK_CUDA(cudaMemcpyAsync(base + pl.off_cls_off[c], cs.off[c].data(), sizeof(long long) * cs.off[c].size(),
                                   cudaMemcpyHostToDevice, s));
     }
     for (int x = 0; x < 3; ++x) {
         hl->cls_rows[x] = (const int *)(base + pl.off_cls_rows[x]);
-        hl->n_cls_rows[x] = (long long)cls_rows[x].size();
-        if (!cls_rows[x].empty())
-            DFTK_CUDA(cudaMemcpyAsync(base + pl.off_cls_rows[x], cls_rows[x].data(), sizeof(int) * cls_rows[x].size(),
+        hl->n_cls_rows[x] = (long long)cs.rows[x].size();
+        if (!cs.rows[x].empty())
+            DFTK_CUDA(cudaMemcpyAsync(base + pl.off_cls_rows[x], cs.rows[x].data(), sizeof(int) * cs.rows[x].size(),
                                       cudaMemcpyHostToDevice, s));
     }
-    for (int y = 0; y < 3; ++y) {
+    for (int y = 0; y < HLC_N_KINDS; ++y) {
         hl->cls_kets[y] = (const int *)(base + pl.off_cls_kets[y]);
-        hl->n_cls_kets[y] = (long long)cls_kets[y].size();
-        if (!cls_kets[y].empty())
-            DFTK_CUDA(cudaMemcpyAsync(base + pl.off_cls_kets[y], cls_kets[y].data(), sizeof(int) * cls_kets[y].size(),
+        for (int b = 0; b <= DFTK_HLC_NB; ++b) hl->cls_ket_seg[y][b] = cs.seg[y][b];
+        if (!cs.kets[y].empty())
+            DFTK_CUDA(cudaMemcpyAsync(base + pl.off_cls_kets[y], cs.kets[y].data(), sizeof(int) * cs.kets[y].size(),
                                       cudaMemcpyHostToDevice, s));
     }
     {
@@ -808,9 +875,24 @@ int dftk_prepare_hl(const dftk_shells_t *shells, double tau_schwarz, double tau_
             int n = 0;
             for (int c = 0; c < HLC_N_CLASSES; ++c) n += hlc_class_kinds[c][0] == x + 3 && hlc_class_kinds[c][1] < 3;
             if (n == 3)
-                for (int r : cls_rows[x]) cnt[r] = 0;
+                for (int r : cs.rows[x]) cnt[r] = 0;
         }
         for (size_t r = 0; r < cnt.size(); ++r) off_lo[r + 1] = off_lo[r] + cnt[r];
+        // (hi|hi) likewise, for rows of a kind that has a class with every
+        // hi kind, when no hi pair has an f shell
+        bool has_f = false;
+        for (size_t r = 0; r < qs[0].size(); ++r) has_f = has_f || pl.l[pl.ab[0][2 * r]] > 2;
+        for (size_t r = 0; r < cnt.size(); ++r) cnt[r] = off_hi[r + 1] - off_hi[r];
+        for (int x = 0; x < 3 && !has_f; ++x) {
+            int n = 0;
+            for (int c = 0; c < HLC_N_CLASSES; ++c) {
+                const int bk = hlc_class_kinds[c][0], kk = hlc_class_kinds[c][1];
+                n += (bk == x + 3 && kk >= 3) || (kk == x + 3 && bk >= 3 && bk != kk);
+            }
+            if (n == 3)
+                for (int r : cs.rows[x]) cnt[r] = 0;
+        }
+        for (size_t r = 0; r < cnt.size(); ++r) off_hi[r + 1] = off_hi[r] + cnt[r];
     }
     long long *d_lo = (long long *)(base + pl.off_row[0]), *d_hi = (long long *)(base + pl.off_row[1]);
     DFTK_CUDA(cudaMemcpyAsync(d_lo, off_lo.data(), sizeof(long long) * off_lo.size(), cudaMemcpyHostToDevice, s));
@@ -1237,11 +1319,13 @@ int dftk_jk_hl(const dftk_shells_t *shells, const dftk_hl_t *hl, const double *D
     unsigned long long cover = 0;
     for (int c = 0; c < HLC_N_CLASSES; ++c) {
         const int bk = hlc_class_kinds[c][0], kk = hlc_class_kinds[c][1];
-        const long long nb = hl->n_cls_rows[bk - 3], nk = kk < 3 ? hl->n_cls_kets[kk] : hl->n_cls_rows[kk - 3];
-        const void *kl = kk < 3 ? (const void *)hl->cls_kets[kk] : (const void *)hl->cls_rows[kk - 3];
+        const long long nb = hl->n_cls_rows[bk - 3], nk = hl->cls_ket_seg[kk][DFTK_HLC_NB];
+        bool seg_ok = hl->cls_ket_seg[kk][0] == 0;
+        for (int b = 0; b < DFTK_HLC_NB; ++b) seg_ok = seg_ok && hl->cls_ket_seg[kk][b] <= hl->cls_ket_seg[kk][b + 1];
         if (hl->cls_total[c] < 0 ||
-            (hl->cls_total[c] > 0 && (!hl->cls_off[c] || !hl->cls_rows[bk - 3] || !kl || nb <= 0 ||
-                                      nb > hl->n_rows || nk <= 0 || nk > (kk < 3 ? hl->lo.n_pairs : hl->n_rows))))
+            (hl->cls_total[c] > 0 && (!hl->cls_off[c] || !hl->cls_rows[bk - 3] || !hl->cls_kets[kk] || !seg_ok ||
+                                      nb <= 0 || nb > hl->n_rows || nk <= 0 ||
+                                      nk > (kk < 3 ? hl->lo.n_pairs : hl->n_rows))))
             return fail(DFTK_ERR_ARG, "dftk_jk_hl: inconsistent class spaces");
         cls_sum += hl->cls_total[c];
         if (hl->cls_off[c]) cover |= (1ull << (6 * bk + kk)) | (1ull << (6 * kk + bk));
@@ -1292,7 +1376,10 @@ int dftk_jk_hl(const dftk_shells_t *shells, const dftk_hl_t *hl, const double *D
             C.rows[x] = hl->cls_rows[x];
             C.n_rows[x] = hl->n_cls_rows[x];
         }
-        for (int y = 0; y < 3; ++y) C.kets[y] = hl->cls_kets[y];
+        for (int y = 0; y < HLC_N_KINDS; ++y) {
+            C.kets[y] = hl->cls_kets[y];
+            for (int b = 0; b <= DFTK_HLC_NB; ++b) C.seg[y][b] = hl->cls_ket_seg[y][b];
+        }
         for (int c = 0; c < HLC_N_CLASSES; ++c) {
             C.off[c] = hl->cls_off[c];
             C.total[c] = hl->cls_total[c];
@@ -1311,7 +1398,8 @@ int dftk_jk_hl(const dftk_shells_t *shells, const dftk_hl_t *hl, const double *D
         if ((st = launch_hlc<0>(C, s)) || (st = launch_hlc<1>(C, s)) || (st = launch_hlc<2>(C, s)) ||
             (st = launch_hlc<3>(C, s)) || (st = launch_hlc<4>(C, s)) || (st = launch_hlc<5>(C, s)) ||
             (st = launch_hlc<6>(C, s)) || (st = launch_hlc<7>(C, s)) || (st = launch_hlc<8>(C, s)) ||
-            (st = launch_hlc<9>(C, s)))
+            (st = launch_hlc<9>(C, s)) || (st = launch_hlc<10>(C, s)) || (st = launch_hlc<11>(C, s)) ||
+            (st = launch_hlc<12>(C, s)))
             return st;
     }
     if (total > 0) {

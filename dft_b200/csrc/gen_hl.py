@@ -1,8 +1,9 @@
 """Generate straight-line McMurchie-Davidson code for the ERI classes with a
-d shell and total momentum L <= 5: (ds|ss), (ds|ps), (ds|pp), (dp|ss),
-(dp|ps), (dp|pp), (dd|ss), (dd|ps), (ds|ds), (dp|ds).  Classes of higher L
-stay with the warp-per-quartet kernel (hl.cuh), whose shared scratch holds
-their larger Hermite sets.
+d shell up to total momentum L = 6: (ds|ss), (ds|ps), (ds|pp), (dp|ss),
+(dp|ps), (dp|pp), (dd|ss), (dd|ps), (ds|ds), (dp|ds), (dp|dp), (dd|pp),
+(dd|ds).  (dd|dp), (dd|dd) and every class with an f shell stay with the
+warp-per-quartet kernel (hl.cuh), whose shared scratch holds their larger
+Hermite sets.
 
 Writes ``hl_classes.cuh`` next to this file (committed, so a build needs no
 Python).  The scheme is the s/p generator's (gen_eri.py) with the bra
@@ -56,6 +57,9 @@ CLASSES = [
     (2, 2, 1, 0, 3, 3),   # 7 (dd|ps)
     (2, 0, 2, 0, 1, 3),   # 8 (ds|ds)
     (2, 1, 2, 0, 1, 6),   # 9 (dp|ds)
+    (2, 1, 2, 1, 1, 18),  # 10 (dp|dp)
+    (2, 2, 1, 1, 3, 9),   # 11 (dd|pp)
+    (2, 2, 2, 0, 3, 6),   # 12 (dd|ds)
 ]
 FIELD_NAMES = ["Px", "Py", "Pz", "p", "K", "h", "Ax", "Ay", "Az", "Bx", "By", "Bz"]
 
@@ -267,7 +271,7 @@ def render() -> str:
     out = [
         "// GENERATED by gen_hl.py -- do not edit by hand.",
         "// Straight-line McMurchie-Davidson bodies of the ERI classes with a d",
-        "// shell and total momentum <= 5.",
+        "// shell and total momentum <= 6 (but (dd|dp)).",
         "#pragma once",
         "",
         "template <typename T, int C, int S> struct HlClass;",

@@ -20,10 +20,11 @@ struct HlcParams {
     dftk_shells_t sh;
     const int *shell_ao;
     dftk_pairs_t hi, lo;
-    const int *rows[3];  // hi rows of kinds ds, dp, dd
+    const int *rows[3];  // hi rows of kinds ds, dp, dd (bras, Schwarz order)
     long long n_rows[3];
-    const int *kets[3];  // lo rows of kinds ss, ps, pp
-    const long long *off[HLC_N_CLASSES];
+    const int *kets[HLC_N_KINDS];  // rows of each kind grouped by primitive-count bucket
+    long long seg[HLC_N_KINDS][DFTK_HLC_NB + 1];
+    const long long *off[HLC_N_CLASSES];  // over (bra position, bucket)
     long long total[HLC_N_CLASSES];
     float tau_prim;
     const double *D, *Da, *Db;
@@ -203,7 +204,7 @@ __global__ void __launch_bounds__(128) k_hlc(const HlcParams P)
     constexpr int X = E0::BRA_KIND - 3, Yk = E0::KET_KIND;
     constexpr bool KET_HI = Yk >= 3;
     const dftk_pairs_t &K = KET_HI ? P.hi : P.lo;
-    const int *kets = KET_HI ? P.rows[Yk - 3] : P.kets[Yk];
+    const int *kets = P.kets[Yk];
     const long long ncand = P.total[C];
     const long long nwork = ((ncand + 31) >> 5) * NS;
     const int lane = threadIdx.x & 31;
@@ -214,9 +215,9 @@ __global__ void __launch_bounds__(128) k_hlc(const HlcParams P)
         bool valid = cand < ncand;
         int row = 0, ket = 0;
         if (valid) {
-            const int r = find_row(P.off[C], P.n_rows[X], cand);
-            row = __ldg(P.rows[X] + r);
-            ket = __ldg(kets + (cand - __ldg(P.off[C] + r)));
+            const int rb = find_row(P.off[C], P.n_rows[X] * DFTK_HLC_NB, cand);
+            row = __ldg(P.rows[X] + rb / DFTK_HLC_NB);
+            ket = __ldg(kets + P.seg[Yk][rb % DFTK_HLC_NB] + (cand - __ldg(P.off[C] + rb)));
             const int a = P.hi.ab[2 * row], b = P.hi.ab[2 * row + 1];
             const int c = K.ab[2 * ket], d = K.ab[2 * ket + 1];
             const float dm = quartet_dmax(P.sh, P.Dsh, a, b, c, d);

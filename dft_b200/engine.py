@@ -60,6 +60,50 @@ def candidate_offsets(q_bra: np.ndarray, q_ket: np.ndarray, same_class: bool, ta
     return np.concatenate([[0], np.cumsum(cnt)]).astype(np.int64)
 
 
+def hlc_bucket(nprim: np.ndarray) -> np.ndarray:
+    """Primitive-pair-count bucket of each pair (DFTK_HLC_BUCKET_BOUNDS)."""
+    return np.searchsorted(np.asarray(_lib.HLC_BUCKET_BOUNDS), nprim, side="left").clip(0, _lib.HLC_NB - 1)
+
+
+def hlc_spaces(l, nprim, hi_ab, lo_ab, q_hi, q_lo, tau):
+    """Candidate spaces of the thread-per-quartet d classes (the layout
+    dftk_hl_t documents): bra lists per hi kind (Schwarz order), ket lists
+    per pair kind grouped by primitive-count bucket with their segment
+    starts, and per class the offsets over (bra position, bucket): each
+    segment's Schwarz prefix, cut at kets whose hi row is <= the bra's for a
+    class whose two kinds are equal."""
+    nb = _lib.HLC_NB
+    sets = []
+    for (a, b), q in ((lo_ab, q_lo), (hi_ab, q_hi)):
+        la, lb = l[a], l[b]
+        kind = np.where(la > 2, -1, np.where(la == 0, 0, np.where(la == 1, 1 + lb, 3 + lb)))
+        sets.append((kind, hlc_bucket(nprim[a].astype(np.int64) * nprim[b]), q))
+    rows = [np.nonzero(sets[1][0] == 3 + x)[0].astype(np.int32) for x in range(3)]
+    kets, seg = [], []
+    for y in range(6):
+        kind, bucket, _ = sets[0 if y < 3 else 1]
+        idx = np.nonzero(kind == y)[0]
+        order = np.argsort(bucket[idx], kind="stable")
+        kets.append(idx[order].astype(np.int32))
+        seg.append(np.searchsorted(bucket[idx][order], np.arange(nb + 1), side="left").astype(np.int64))
+    offs = []
+    for bk, kk in _lib.HLC_CLASS_KINDS:
+        bra = rows[bk - 3]
+        qk = sets[0 if kk < 3 else 1][2]
+        with np.errstate(divide="ignore"):
+            qb = q_hi[bra]
+            thr = np.where(qb > 0, tau / np.where(qb > 0, qb, 1.0), np.inf)
+        cnt = np.zeros((bra.size, nb), dtype=np.int64)
+        for b in range(nb):
+            segk = kets[kk][seg[kk][b]:seg[kk][b + 1]]
+            c = np.searchsorted(-qk[segk], -thr, side="right")
+            if bk == kk:
+                c = np.minimum(c, np.searchsorted(segk, bra, side="right"))
+            cnt[:, b] = np.where(qb > 0, c, 0)
+        offs.append(np.concatenate([[0], np.cumsum(cnt.reshape(-1))]).astype(np.int64))
+    return rows, kets, seg, offs
+
+
 def shard_row_offsets(row_off: np.ndarray, rank: int, world: int) -> np.ndarray:
     """Row offsets of one rank's share of a class's candidate space.
 
@@ -130,6 +174,7 @@ class IntegralEngine:
     def _upload_shells(self):
         sh = self.segs
         nprim = np.array([s["exponents"].size for s in sh], dtype=np.int32)
+        self._seg_nprim = nprim
         prim_off = np.concatenate([[0], np.cumsum(nprim)[:-1]]).astype(np.int32)
         exps = np.concatenate([s["exponents"] for s in sh]) if sh else np.zeros(0)
         # coefficient x radial norm per primitive (for s and p shells this is
@@ -266,18 +311,9 @@ class IntegralEngine:
         self.ref_pair_lo_row[sel_lo] = np.arange(sel_lo.size)
         off_lo = candidate_offsets(q_hi, q_lo, False, self.tau_schwarz)
         off_hi = candidate_offsets(q_hi, q_hi, True, self.tau_schwarz)
-        a, b = self._pair_a, self._pair_b
-        # thread-per-quartet classes: hi rows of kinds (d,s), (d,p), (d,d)
-        # and lo rows by l_a + l_b, as index lists into the two pair sets
-        hi_kind = np.where(self.l[a[sel_hi]] == 2, self.l[b[sel_hi]], 9)
-        lo_kind = self.l[a[sel_lo]] + self.l[b[sel_lo]]
-        self.hlc_rows = [np.nonzero(hi_kind == x)[0].astype(np.int32) for x in range(3)]
-        self.hlc_kets = [np.nonzero(lo_kind == y)[0].astype(np.int32) for y in range(3)]
-        hlc_off = []
-        for bk, kk in _lib.HLC_CLASS_KINDS:
-            bra = self.hlc_rows[bk - 3]
-            ket, qk = (self.hlc_kets[kk], q_lo) if kk < 3 else (self.hlc_rows[kk - 3], q_hi)
-            hlc_off.append(candidate_offsets(q_hi[bra], qk[ket], bk == kk, self.tau_schwarz))
+        spaces = hlc_spaces(self.l, self._seg_nprim, (self._pair_a[sel_hi], self._pair_b[sel_hi]),
+                            (self._pair_a[sel_lo], self._pair_b[sel_lo]), q_hi, q_lo, self.tau_schwarz)
+        self.hlc_rows, self.hlc_kets, self.hlc_seg, hlc_off = spaces
         if self.hl_classes:
             # rows whose every (hi|lo) quartet belongs to a class leave the
             # warp kernel's (hi|lo) space
@@ -286,6 +322,16 @@ class IntegralEngine:
                 if sum(1 for bk, kk in _lib.HLC_CLASS_KINDS if bk == x + 3 and kk < 3) == 3:
                     cnt[self.hlc_rows[x]] = 0
             off_lo = np.concatenate([[0], np.cumsum(cnt)]).astype(np.int64)
+            # (hi|hi) likewise, for rows of a kind that has a class with every
+            # hi kind, when no hi pair has an f shell
+            if self.hl_lmax <= 2:
+                cnt = np.diff(off_hi)
+                for x in range(3):
+                    n = sum(1 for bk, kk in _lib.HLC_CLASS_KINDS
+                            if (bk == x + 3 and kk >= 3) or (kk == x + 3 and bk >= 3 and bk != kk))
+                    if n == 3:
+                        cnt[self.hlc_rows[x]] = 0
+                off_hi = np.concatenate([[0], np.cumsum(cnt)]).astype(np.int64)
         else:
             hlc_off = [np.zeros(1, dtype=np.int64) for _ in hlc_off]
         self.hlc_totals = [int(o[-1]) for o in hlc_off]
@@ -310,10 +356,11 @@ class IntegralEngine:
                 if self.hlc_rows[x].size:
                     hl.cls_rows[x] = _lib.ptr(self.hlc_dev[0][x]).value
                     hl.n_cls_rows[x] = int(self.hlc_rows[x].size)
-            for y in range(3):
+            for y in range(6):
                 if self.hlc_kets[y].size:
                     hl.cls_kets[y] = _lib.ptr(self.hlc_dev[1][y]).value
-                    hl.n_cls_kets[y] = int(self.hlc_kets[y].size)
+                for b in range(_lib.HLC_NB + 1):
+                    hl.cls_ket_seg[y][b] = int(self.hlc_seg[y][b])
             for c in range(_lib.HLC_N_CLASSES):
                 hl.cls_off[c] = _lib.ptr(self.hlc_dev[2][c]).value
                 hl.cls_total[c] = self.hlc_totals[c]

@@ -160,6 +160,9 @@ typedef struct {
  * s and p shells both conventions agree). */
 #define DFTK_PCLASS_GENERIC 3
 #define DFTK_HL_LMAX 3
+/* primitive-pair-count buckets of the class ket lists (upper bounds) */
+#define DFTK_HLC_NB 6
+#define DFTK_HLC_BUCKET_BOUNDS {1, 4, 9, 16, 36, 1 << 30}
 typedef struct {
     dftk_pairs_t hi;              /* pairs with a d or f shell, l_a >= l_b */
     dftk_pairs_t lo;              /* every s/p pair of the molecule, same layout */
@@ -168,25 +171,32 @@ typedef struct {
     const long long *row_off[2];  /* device [n_rows + 1] each: Schwarz prefixes as in dftk_queue_t */
     double tau_prim;              /* primitive-quartet cut, as in dftk_queue_t */
     int lmax;                     /* largest shell momentum, 2 (d) or 3 (f): selects the kernels' scratch layout */
-    /* Thread-per-quartet classes (generated code, total momentum <= 5): class
-     * c = 0 (ds|ss), 1 (ds|ps), 2 (ds|pp), 3 (dp|ss), 4 (dp|ps), 5 (dp|pp),
-     * 6 (dd|ss), 7 (dd|ps), 8 (ds|ds), 9 (dp|ds).  cls_rows[x] lists the hi
-     * rows of pair kind x = 0 (d,s), 1 (d,p), 2 (d,d) and cls_kets[y] the lo
-     * rows of kind y = 0 (s,s), 1 (p,s), 2 (p,p), each ascending (so by
-     * descending Schwarz factor).  cls_off[c] are the candidate offsets over
-     * the class's bra list (row r keeps the ket prefix of its ket list:
-     * cls_kets[y] for kets from the lo set, cls_rows[y] for (ds|ds) and
-     * (dp|ds); (ds|ds) cut at k <= r), cls_total[c] their totals.  A class
-     * whose cls_off is non-NULL takes every quartet of its two pair kinds:
-     * the warp-per-quartet kernel skips them, and a host may give the hi rows
-     * whose every (hi|lo) quartet belongs to a class zero candidates in
-     * row_off[0].  All NULL: every d quartet runs in the warp kernel. */
+    /* Thread-per-quartet classes (generated code): class c = 0 (ds|ss),
+     * 1 (ds|ps), 2 (ds|pp), 3 (dp|ss), 4 (dp|ps), 5 (dp|pp), 6 (dd|ss),
+     * 7 (dd|ps), 8 (ds|ds), 9 (dp|ds), 10 (dp|dp), 11 (dd|pp), 12 (dd|ds);
+     * (dd|dp), (dd|dd) and f quartets run in the warp kernel.  Pair kinds: 0 (s,s),
+     * 1 (p,s), 2 (p,p) in the lo set, 3 (d,s), 4 (d,p), 5 (d,d) in the hi set.
+     * cls_rows[x] lists the hi rows of kind 3 + x ascending (the bras, by
+     * descending Schwarz factor).  cls_kets[y] lists the rows of kind y (lo
+     * rows for y < 3, hi rows for y >= 3) grouped by primitive-pair count
+     * (bucket b holds nprim in (bound[b - 1], bound[b]] of DFTK_HLC_BUCKET_BOUNDS),
+     * ascending within a bucket; bucket b starts at cls_ket_seg[y][b].
+     * cls_off[c] are the candidate offsets over (bra position r, bucket b),
+     * entry r * DFTK_HLC_NB + b: the quartets of bra r with the Schwarz
+     * prefix of bucket b's kets (for (ds|ds) and (dp|dp) only kets whose hi
+     * row is <= the bra's, so each unique quartet appears once); cls_total[c] = the last
+     * offset.  Bucketing keeps the 32 lanes of a warp on kets with similar
+     * primitive counts.  A class whose cls_off is non-NULL takes every
+     * quartet of its two pair kinds: the warp-per-quartet kernel skips them,
+     * and a host may give the hi rows whose every (hi|lo) quartet belongs to a
+     * class zero candidates in row_off[0].  All NULL: every d quartet runs in
+     * the warp kernel. */
     const int *cls_rows[3];
     long long n_cls_rows[3];
-    const int *cls_kets[3];
-    long long n_cls_kets[3];
-    const long long *cls_off[10];
-    long long cls_total[10];
+    const int *cls_kets[6];
+    long long cls_ket_seg[6][7];
+    const long long *cls_off[13];
+    long long cls_total[13];
 } dftk_hl_t;
 
 /* library version (integer, 100 * major + minor) */

@@ -90,7 +90,8 @@ def test_prepare_hl_d_shells_through_the_c_abi():
                   ctypes.byref(hl), stream)
         assert hl.n_rows == eng.c_hl.n_rows and list(hl.total) == list(eng.c_hl.total) and hl.lmax == 2
         assert list(hl.cls_total) == list(eng.c_hl.cls_total)
-        assert list(hl.n_cls_rows) == list(eng.c_hl.n_cls_rows) and list(hl.n_cls_kets) == list(eng.c_hl.n_cls_kets)
+        assert list(hl.n_cls_rows) == list(eng.c_hl.n_cls_rows)
+        assert [list(x) for x in hl.cls_ket_seg] == [list(x) for x in eng.c_hl.cls_ket_seg]
         ws_bytes = _lib.load().dftk_jk_workspace_bytes_queue(eng.ns, N, ctypes.byref(queue))
         ws = torch.empty(ws_bytes, dtype=torch.uint8, device=eng.device)
         J = torch.empty((N, N), dtype=torch.float64, device=eng.device)

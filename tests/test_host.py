@@ -322,3 +322,56 @@ def test_generated_d_classes_are_current():
         assert fh.read() == gen_hl.render()
     kinds = [(gen_hl.kind(la, lb), gen_hl.kind(lc, ld)) for la, lb, lc, ld, _, _ in gen_hl.CLASSES]
     assert kinds == _lib.HLC_CLASS_KINDS
+
+
+def test_hlc_spaces_enumerate_each_quartet_once():
+    """The bucketed candidate spaces of the d classes hold exactly the
+    quartets of their two pair kinds whose Schwarz product reaches tau, each
+    once ((ds|ds): ket row <= bra row), and every (row, bucket) segment has
+    kets of one primitive-count bucket only."""
+    from dft_b200 import _lib
+    from dft_b200.engine import hlc_bucket, hlc_spaces
+
+    rng = np.random.default_rng(3)
+    ns = 40
+    l = rng.integers(0, 3, size=ns).astype(np.int32)
+    nprim = rng.choice([1, 3, 4, 9], size=ns).astype(np.int32)
+    ii, jj = np.tril_indices(ns)
+    swap = l[ii] < l[jj]
+    a, b = np.where(swap, jj, ii), np.where(swap, ii, jj)
+    hi = l[a] >= 2
+    sets = {}
+    for name, m in (("hi", hi), ("lo", ~hi)):
+        q = rng.uniform(1e-9, 1.0, size=int(m.sum()))
+        order = np.argsort(-q, kind="stable")
+        sets[name] = (a[m][order], b[m][order], q[order])
+    tau = 1e-3
+    rows, kets, seg, offs = hlc_spaces(l, nprim, sets["hi"][:2], sets["lo"][:2], sets["hi"][2], sets["lo"][2], tau)
+
+    def kind(set_name, r):
+        la, lb = l[sets[set_name][0][r]], l[sets[set_name][1][r]]
+        return 0 if la == 0 else (1 + lb if la == 1 else 3 + lb)
+
+    nb = _lib.HLC_NB
+    for c, (bk, kk) in enumerate(_lib.HLC_CLASS_KINDS):
+        kset = "lo" if kk < 3 else "hi"
+        got = []
+        for i, r in enumerate(rows[bk - 3]):
+            for bb in range(nb):
+                lo_, hi_ = offs[c][i * nb + bb], offs[c][i * nb + bb + 1]
+                for t in range(hi_ - lo_):
+                    k = kets[kk][seg[kk][bb] + t]
+                    pa, pb = sets[kset][0][k], sets[kset][1][k]
+                    assert hlc_bucket(np.array([int(nprim[pa]) * int(nprim[pb])]))[0] == bb
+                    got.append((int(r), int(k)))
+        want = []
+        for r in range(sets["hi"][2].size):
+            if kind("hi", r) != bk:
+                continue
+            for k in range(sets[kset][2].size):
+                if kind(kset, k) != kk or sets["hi"][2][r] * sets[kset][2][k] < tau:
+                    continue
+                if bk == kk and k > r:
+                    continue
+                want.append((r, k))
+        assert sorted(got) == sorted(want) and len(got) == len(set(got)), c
