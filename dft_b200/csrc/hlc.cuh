@@ -196,8 +196,14 @@ __device__ __forceinline__ void hlc_split(const HlcParams &P, int split, bool va
     }
 }
 
+// resident 128-thread blocks per SM the class kernels are compiled for
+// (register cap 65536 / (128 x value))
+#ifndef DFTK_HLC_MINB
+#define DFTK_HLC_MINB 1
+#endif
+
 template <int C>
-__global__ void __launch_bounds__(128) k_hlc(const HlcParams P)
+__global__ void __launch_bounds__(128, DFTK_HLC_MINB) k_hlc(const HlcParams P)
 {
     using E0 = HlClass<double, C, 0>;
     constexpr int NS = E0::NSPLIT;
