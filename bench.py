@@ -594,6 +594,23 @@ def grid_figures(torch, eng, centers, res, nocc, cpu: bool, n_points=1_000_000):
     return out
 
 
+def dshell_workload(torch):
+    """(H2O)_16 (2x2x4 lattice) with the generally contracted, d-polarised test
+    basis and a banded symmetric density: (engine, D, D/2)."""
+    from dft_b200 import basis, geometry
+    from dft_b200.engine import IntegralEngine
+
+    with open(os.path.join(REPO, "tests", "golden", "dz_gc_test.json")) as fh:
+        data = json.load(fh)
+    atoms, centers = geometry.water_cluster((2, 2, 4))
+    eng = IntegralEngine(basis.build_shells(data, atoms, centers), tau_schwarz=1e-12)
+    N = eng.n_ao
+    rng = np.random.default_rng(4)
+    M = rng.normal(size=(N, N)) * np.exp(-0.2 * np.abs(np.subtract.outer(np.arange(N), np.arange(N))))
+    D = torch.as_tensor(0.05 * (M + M.T), device=eng.device)
+    return eng, D, (0.5 * D).contiguous()
+
+
 def dshell_figures(torch):
     """The d/f path on a polarised basis: (H2O)_16 (2x2x4 lattice) with the
     generally contracted, d-polarised test basis (tests/golden/dz_gc_test.json;
@@ -602,19 +619,10 @@ def dshell_figures(torch):
     CUDA events, and the quartets with a d shell."""
     import ctypes
 
-    from dft_b200 import _lib, basis, geometry
-    from dft_b200.engine import IntegralEngine
+    from dft_b200 import _lib
 
-    with open(os.path.join(REPO, "tests", "golden", "dz_gc_test.json")) as fh:
-        data = json.load(fh)
-    atoms, centers = geometry.water_cluster((2, 2, 4))
-    sh = basis.build_shells(data, atoms, centers)
-    eng = IntegralEngine(sh, tau_schwarz=1e-12)
+    eng, D, Dh = dshell_workload(torch)
     N = eng.n_ao
-    rng = np.random.default_rng(4)
-    M = rng.normal(size=(N, N)) * np.exp(-0.2 * np.abs(np.subtract.outer(np.arange(N), np.arange(N))))
-    D = torch.as_tensor(0.05 * (M + M.T), device=eng.device)
-    Dh = (0.5 * D).contiguous()
     J = torch.empty((N, N), dtype=torch.float64, device=eng.device)
     K = torch.empty_like(J)
     stream = _lib.stream_handle()
@@ -980,6 +988,16 @@ def run_profile(args):
     k_symmetrize), then one gradient (and with --profile-grid two grid chunks)."""
     import torch
 
+    if args.profile_dshell:
+        # two full FP64 J/K builds of the d-basis workload: k_dsh, the s/p
+        # class kernels, k_symmetrize, then k_dsh, k_hlc<0..12>, k_hl_jk<2>,
+        # k_symmetrize_add per build
+        deng, D, Dh = dshell_workload(torch)
+        for _ in range(2):
+            deng.jk(D, Dh, tau=1e-14)
+        torch.cuda.synchronize()
+        print("profile workload done")
+        return 0
     atoms, centers, shells, eng, S, H, enn, nocc = setup_workload(torch)
     X = torch.linalg.inv(torch.linalg.cholesky(S)).T
     _, C = torch.linalg.eigh(X.T @ H @ X)
@@ -1029,6 +1047,8 @@ def main():
                     help="with N > 1: the ranks build one (H2O)_64 Fock matrix together (strong scaling)")
     ap.add_argument("--profile", action="store_true", help="only run a few builds (for ncu captures)")
     ap.add_argument("--profile-grid", action="store_true", help="with --profile: also two grid-evaluation chunks")
+    ap.add_argument("--profile-dshell", action="store_true",
+                    help="with --profile: only two J/K builds of the d-basis (H2O)_16 workload")
     args = ap.parse_args()
     if args.profile:
         return run_profile(args)

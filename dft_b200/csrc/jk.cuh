@@ -666,18 +666,21 @@ __global__ void __launch_bounds__(128, JkMinBlocks<C, T>::value) k_jk_list(const
     const long long n = (long long)P.heads[(fp32 ? DFTK_N_QCLASS : 0) + C];
     const long long cap = P.total[C];
     const int2 *list = P.list[C];
-    const long long nwork = ((n + 31) >> 5) * NS;
+    const long long nq = (n + 31) >> 5;
+    const long long nwork = nq * NS;
     const int lane = threadIdx.x & 31;
     // each warp step takes `tile` consecutive work items (32-entry groups, or
-    // their c-component splits), so a warp stays on neighbouring list entries
+    // their c-component splits), so a warp stays on neighbouring list entries;
+    // split-major order: the grid sweeps the list with split 0's code, then
+    // split 1's, so resident warps share one straight-line body
     const int tile = P.tile[(fp32 ? DFTK_N_QCLASS : 0) + C] > 0 ? P.tile[(fp32 ? DFTK_N_QCLASS : 0) + C] : 1;
     const long long wstride = (((long long)gridDim.x * blockDim.x) >> 5) * tile;
     for (long long g0 = (((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * tile; g0 < nwork; g0 += wstride) {
         for (int k = 0; k < tile; ++k) {
             const long long gw = g0 + k;
             if (gw >= nwork) break;
-            const int split = (int)(gw % NS);
-            const long long idx = (gw / NS) * 32 + lane;
+            const int split = (int)(gw / nq);
+            const long long idx = (gw % nq) * 32 + lane;
             const bool valid = idx < n;
             int row = 0, ket = 0;
             if (valid) {
