@@ -990,7 +990,8 @@ def run_profile(args):
 
     if args.profile_dshell:
         # two full FP64 J/K builds of the d-basis workload: k_dsh, the s/p
-        # class kernels, k_symmetrize, then k_dsh, k_hlc<0..12>, k_hl_jk<2>,
+        # class kernels, k_symmetrize, then k_dsh, k_hlc<C, S> per class and
+        # component chunk, k_hl_jk<2>,
         # k_symmetrize_add per build
         deng, D, Dh = dshell_workload(torch)
         for _ in range(2):

@@ -1265,15 +1265,16 @@ template <int LM, typename K> int hl_smem_optin(K kernel, size_t extra_static = 
 // warp work items (32 candidates x ket-component split).
 static_assert(HLC_N_CLASSES == sizeof(((dftk_hl_t *)nullptr)->cls_off) / sizeof(void *),
               "dftk_hl_t holds one candidate space per generated d class");
-template <int C> int launch_hlc(const HlcParams &P, cudaStream_t s)
+template <int C, int S = 0> int launch_hlc(const HlcParams &P, cudaStream_t s)
 {
     if (P.total[C] == 0) return DFTK_OK;
-    const long long items = ((P.total[C] + 31) / 32) * HlClass<double, C, 0>::NSPLIT;
+    const long long items = (P.total[C] + 31) / 32;
     long long blocks = (items + 3) / 4;
     const long long cap = (long long)sm_count() * 16;
     if (blocks > cap) blocks = cap;
-    k_hlc<C><<<(unsigned)blocks, 128, 0, s>>>(P);
+    k_hlc<C, S><<<(unsigned)blocks, 128, 0, s>>>(P);
     DFTK_LAUNCHED("k_hlc");
+    if constexpr (S + 1 < HlClass<double, C, 0>::NSPLIT) return launch_hlc<C, S + 1>(P, s);
     return DFTK_OK;
 }
 }  // namespace

@@ -186,43 +186,30 @@ __device__ __forceinline__ void hlc_one(const HlcParams &P, bool valid, int row,
     }
 }
 
-template <int C, int S>
-__device__ __forceinline__ void hlc_split(const HlcParams &P, int split, bool valid, int row, int ket)
-{
-    if (split == S) {
-        hlc_one<C, S>(P, valid, row, ket);
-    } else if constexpr (S + 1 < HlClass<double, C, 0>::NSPLIT) {
-        hlc_split<C, S + 1>(P, split, valid, row, ket);
-    }
-}
-
 // resident 128-thread blocks per SM the class kernels are compiled for
 // (register cap 65536 / (128 x value))
 #ifndef DFTK_HLC_MINB
 #define DFTK_HLC_MINB 1
 #endif
 
-template <int C>
+// One component chunk S of class C over every candidate: one kernel per
+// chunk, so an SM holds a single straight-line body in its instruction cache
+// (measured on B200, (dp|pp) with nine chunks: instruction-fetch stalls of
+// 37 cycles per issue with the chunks interleaved in one kernel).
+template <int C, int S>
 __global__ void __launch_bounds__(128, DFTK_HLC_MINB) k_hlc(const HlcParams P)
 {
     using E0 = HlClass<double, C, 0>;
-    constexpr int NS = E0::NSPLIT;
     constexpr int X = E0::BRA_KIND - 3, Yk = E0::KET_KIND;
     constexpr bool KET_HI = Yk >= 3;
     const dftk_pairs_t &K = KET_HI ? P.hi : P.lo;
     const int *kets = P.kets[Yk];
     const long long ncand = P.total[C];
-    const long long nq = (ncand + 31) >> 5;
-    const long long nwork = nq * NS;
+    const long long nwork = (ncand + 31) >> 5;
     const int lane = threadIdx.x & 31;
     const long long wstride = ((long long)gridDim.x * blockDim.x) >> 5;
-    // split-major work order: the grid sweeps every candidate with chunk 0's
-    // code, then chunk 1's, so the warps resident at one time run the same
-    // straight-line body (measured on B200: with the chunk index fastest,
-    // (dp|pp)'s nine bodies stalled on instruction fetch 37 cycles per issue)
     for (long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; gw < nwork; gw += wstride) {
-        const int split = (int)(gw / nq);
-        const long long cand = (gw % nq) * 32 + lane;
+        const long long cand = gw * 32 + lane;
         bool valid = cand < ncand;
         int row = 0, ket = 0;
         if (valid) {
@@ -235,6 +222,6 @@ __global__ void __launch_bounds__(128, DFTK_HLC_MINB) k_hlc(const HlcParams P)
             valid = __ldg(P.hi.q + row) * __ldg(K.q + ket) * (double)dm >= P.tau;
         }
         if (!__any_sync(DFTK_FULL_MASK, valid)) continue;
-        hlc_split<C, 0>(P, split, valid, row, ket);
+        hlc_one<C, S>(P, valid, row, ket);
     }
 }
