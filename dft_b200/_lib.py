@@ -100,7 +100,7 @@ class Queue(ctypes.Structure):
 # thread-per-quartet d classes: (bra pair kind, ket pair kind), kinds 0 ss,
 # 1 ps, 2 pp, 3 ds, 4 dp, 5 dd (the table of hl_classes.cuh)
 HLC_CLASS_KINDS = [(3, 0), (3, 1), (3, 2), (4, 0), (4, 1), (4, 2), (5, 0), (5, 1), (3, 3), (4, 3), (4, 4), (5, 2),
-                   (5, 3)]
+                   (5, 3), (5, 4), (5, 5)]
 HLC_N_CLASSES = len(HLC_CLASS_KINDS)
 # primitive-pair-count buckets of the class ket lists (DFTK_HLC_BUCKET_BOUNDS)
 HLC_BUCKET_BOUNDS = [1, 4, 9, 16, 36, 1 << 30]

@@ -13,7 +13,8 @@ PKG = os.path.dirname(HERE)
 REPO = os.path.dirname(PKG)
 LIB = os.path.join(PKG, "libdftk.so")
 SOURCES = ["dftk.cu", "jk_noalloc.cu"]
-HEADERS = ["common.cuh", "boys.cuh", "eri_classes.cuh", "jk.cuh", "generic.cuh", "onee.cuh", "grad.cuh", "grid.cuh", "hl.cuh", "hl_classes.cuh", "hlc.cuh"]
+HEADERS = ["common.cuh", "boys.cuh", "eri_classes.cuh", "jk.cuh", "generic.cuh", "onee.cuh", "grad.cuh", "grid.cuh", "hl.cuh",
+           "hl_classes.cuh", "hlc.cuh", "gen_hl.py"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -36,7 +37,26 @@ def needs_build() -> bool:
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
+def generate_hl_classes() -> None:
+    """Write hl_classes.cuh (the generated d classes, ~10 MB, not committed)
+    from gen_hl.py when it is missing or differs from the generator's output."""
+    sys.path.insert(0, HERE)
+    try:
+        import gen_hl
+    finally:
+        sys.path.remove(HERE)
+    text = gen_hl.render()
+    path = os.path.join(HERE, "hl_classes.cuh")
+    if os.path.exists(path):
+        with open(path) as fh:
+            if fh.read() == text:
+                return
+    with open(path, "w") as fh:
+        fh.write(text)
+
+
 def build(verbose: bool = False, force: bool = False, extra=()) -> str:
+    generate_hl_classes()
     if not force and not needs_build():
         return LIB
     cmd = [nvcc(), *NVCC_FLAGS, *extra, "-I", HERE, "-I", os.path.join(REPO, "include"),

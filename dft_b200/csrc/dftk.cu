@@ -1400,7 +1400,7 @@ int dftk_jk_hl(const dftk_shells_t *shells, const dftk_hl_t *hl, const double *D
             (st = launch_hlc<3>(C, s)) || (st = launch_hlc<4>(C, s)) || (st = launch_hlc<5>(C, s)) ||
             (st = launch_hlc<6>(C, s)) || (st = launch_hlc<7>(C, s)) || (st = launch_hlc<8>(C, s)) ||
             (st = launch_hlc<9>(C, s)) || (st = launch_hlc<10>(C, s)) || (st = launch_hlc<11>(C, s)) ||
-            (st = launch_hlc<12>(C, s)))
+            (st = launch_hlc<12>(C, s)) || (st = launch_hlc<13>(C, s)) || (st = launch_hlc<14>(C, s)))
             return st;
     }
     if (total > 0) {

@@ -1,13 +1,12 @@
-"""Generate straight-line McMurchie-Davidson code for the ERI classes with a
-d shell up to total momentum L = 6: (ds|ss), (ds|ps), (ds|pp), (dp|ss),
-(dp|ps), (dp|pp), (dd|ss), (dd|ps), (ds|ds), (dp|ds), (dp|dp), (dd|pp),
-(dd|ds).  (dd|dp), (dd|dd) and every class with an f shell stay with the
-warp-per-quartet kernel (hl.cuh), whose shared scratch holds their larger
-Hermite sets.
+"""Generate straight-line McMurchie-Davidson code for every ERI class with a
+d shell and no f shell: (ds|ss), (ds|ps), (ds|pp), (dp|ss), (dp|ps),
+(dp|pp), (dd|ss), (dd|ps), (ds|ds), (dp|ds), (dp|dp), (dd|pp), (dd|ds),
+(dd|dp), (dd|dd).  Classes with an f shell stay with the warp-per-quartet
+kernel (hl.cuh), whose shared scratch holds their larger Hermite sets.
 
-Writes ``hl_classes.cuh`` next to this file (committed, so a build needs no
-Python).  The scheme is the s/p generator's (gen_eri.py) with the bra
-primitive loop outside: per bra primitive pair i the ket primitives j are
+Writes ``hl_classes.cuh`` next to this file; the build (build.py) runs it, so
+the ~10 MB of straight-line code stays out of the repository.  The scheme
+is the s/p generator's (gen_eri.py) with the bra primitive loop outside: per bra primitive pair i the ket primitives j are
 summed into the Hermite-bra, Cartesian-ket intermediate
 
     W^{cd}_{tuv}(i) = sum_j sum_{tau nu phi} (-1)^{tau+nu+phi} E^{cd}_{tau nu phi}(j) R_{t+tau,u+nu,v+phi}(i, j)
@@ -60,6 +59,8 @@ CLASSES = [
     (2, 1, 2, 1, 1, 18),  # 10 (dp|dp)
     (2, 2, 1, 1, 3, 9),   # 11 (dd|pp)
     (2, 2, 2, 0, 3, 6),   # 12 (dd|ds)
+    (2, 2, 2, 1, 6, 9),   # 13 (dd|dp)
+    (2, 2, 2, 2, 6, 18),  # 14 (dd|dd)
 ]
 FIELD_NAMES = ["Px", "Py", "Pz", "p", "K", "h", "Ax", "Ay", "Az", "Bx", "By", "Bz"]
 
@@ -271,7 +272,7 @@ def render() -> str:
     out = [
         "// GENERATED by gen_hl.py -- do not edit by hand.",
         "// Straight-line McMurchie-Davidson bodies of the ERI classes with a d",
-        "// shell and total momentum <= 6 (but (dd|dp)).",
+        "// shell and no f shell.",
         "#pragma once",
         "",
         "template <typename T, int C, int S> struct HlClass;",

@@ -173,8 +173,8 @@ typedef struct {
     int lmax;                     /* largest shell momentum, 2 (d) or 3 (f): selects the kernels' scratch layout */
     /* Thread-per-quartet classes (generated code): class c = 0 (ds|ss),
      * 1 (ds|ps), 2 (ds|pp), 3 (dp|ss), 4 (dp|ps), 5 (dp|pp), 6 (dd|ss),
-     * 7 (dd|ps), 8 (ds|ds), 9 (dp|ds), 10 (dp|dp), 11 (dd|pp), 12 (dd|ds);
-     * (dd|dp), (dd|dd) and f quartets run in the warp kernel.  Pair kinds: 0 (s,s),
+     * 7 (dd|ps), 8 (ds|ds), 9 (dp|ds), 10 (dp|dp), 11 (dd|pp), 12 (dd|ds),
+     * 13 (dd|dp), 14 (dd|dd); f quartets run in the warp kernel.  Pair kinds: 0 (s,s),
      * 1 (p,s), 2 (p,p) in the lo set, 3 (d,s), 4 (d,p), 5 (d,d) in the hi set.
      * cls_rows[x] lists the hi rows of kind 3 + x ascending (the bras, by
      * descending Schwarz factor).  cls_kets[y] lists the rows of kind y (lo
@@ -183,8 +183,8 @@ typedef struct {
      * ascending within a bucket; bucket b starts at cls_ket_seg[y][b].
      * cls_off[c] are the candidate offsets over (bra position r, bucket b),
      * entry r * DFTK_HLC_NB + b: the quartets of bra r with the Schwarz
-     * prefix of bucket b's kets (for (ds|ds) and (dp|dp) only kets whose hi
-     * row is <= the bra's, so each unique quartet appears once); cls_total[c] = the last
+     * prefix of bucket b's kets (for (ds|ds), (dp|dp) and (dd|dd) only kets
+     * whose hi row is <= the bra's, so each unique quartet appears once); cls_total[c] = the last
      * offset.  Bucketing keeps the 32 lanes of a warp on kets with similar
      * primitive counts.  A class whose cls_off is non-NULL takes every
      * quartet of its two pair kinds: the warp-per-quartet kernel skips them,
@@ -195,8 +195,8 @@ typedef struct {
     long long n_cls_rows[3];
     const int *cls_kets[6];
     long long cls_ket_seg[6][7];
-    const long long *cls_off[13];
-    long long cls_total[13];
+    const long long *cls_off[15];
+    long long cls_total[15];
 } dftk_hl_t;
 
 /* library version (integer, 100 * major + minor) */

@@ -180,8 +180,8 @@ def test_f_shell_eris_and_jk_vs_oracle(oracle_mod):
 
 def test_thread_classes_match_warp_path_and_oracle(oracle_mod):
     """(H2O)_2 with the generally contracted d-polarised basis: the generated
-    thread-per-quartet kernels of the thirteen generated d classes plus the
-    warp kernel for (dd|dp) and (dd|dd) give the warp kernel's J/K alone (1e-12) and the
+    thread-per-quartet kernels of the fifteen generated d classes (every d
+    class, no warp kernel) give the warp kernel's J/K alone (1e-12) and the
     oracle's direct J/K (1e-11 relative), UHF densities with no structure."""
     atoms, centers = geometry.water_cluster((1, 1, 2))
     data = _gc_basis()
@@ -189,12 +189,13 @@ def test_thread_classes_match_warp_path_and_oracle(oracle_mod):
     eng = IntegralEngine(sh, tau_schwarz=0.0)
     warp = IntegralEngine(sh, tau_schwarz=0.0, hl_classes=False)
     assert all(t > 0 for t in eng.hlc_totals)
-    # every (hi|lo) quartet belongs to a class (no f shells), so the warp
-    # kernel's (hi|lo) space is empty; its (hi|hi) space keeps the (d,p) and
-    # (d,d) rows, whose class quartets it skips in-kernel
+    # with no f shells every d quartet belongs to a class: the warp kernel's
+    # spaces are empty, and the class spaces hold exactly its candidates
     lo_classes = [c for c, (bk, kk) in enumerate(_lib.HLC_CLASS_KINDS) if kk < 3]
-    assert eng.hl_totals[0] == 0 and sum(eng.hlc_totals[c] for c in lo_classes) == warp.hl_totals[0]
-    assert 0 < eng.hl_totals[1] < warp.hl_totals[1] and sum(warp.hlc_totals) == 0
+    hi_classes = [c for c, (bk, kk) in enumerate(_lib.HLC_CLASS_KINDS) if kk >= 3]
+    assert eng.hl_totals == [0, 0] and sum(warp.hlc_totals) == 0
+    assert sum(eng.hlc_totals[c] for c in lo_classes) == warp.hl_totals[0]
+    assert sum(eng.hlc_totals[c] for c in hi_classes) == warp.hl_totals[1]
     N = eng.n_ao
     rng = np.random.default_rng(17)
     M1, M2 = rng.normal(size=(N, N)), rng.normal(size=(N, N))

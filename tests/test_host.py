@@ -305,8 +305,9 @@ def test_batch_pack_index_round_trip():
 
 
 def test_generated_d_classes_are_current():
-    """hl_classes.cuh is exactly what gen_hl.py renders, and the class kind
-    table the host uses equals the one the kernels were generated with."""
+    """hl_classes.cuh (written by the build from gen_hl.py) is exactly what
+    gen_hl.py renders, and the class kind table the host uses equals the one
+    the kernels were generated with."""
     import os
     import sys
 
@@ -318,8 +319,10 @@ def test_generated_d_classes_are_current():
         import gen_hl
     finally:
         sys.path.remove(csrc)
-    with open(os.path.join(csrc, "hl_classes.cuh")) as fh:
-        assert fh.read() == gen_hl.render()
+    path = os.path.join(csrc, "hl_classes.cuh")
+    if os.path.exists(path):
+        with open(path) as fh:
+            assert fh.read() == gen_hl.render()
     kinds = [(gen_hl.kind(la, lb), gen_hl.kind(lc, ld)) for la, lb, lc, ld, _, _ in gen_hl.CLASSES]
     assert kinds == _lib.HLC_CLASS_KINDS
 
