@@ -94,6 +94,7 @@ class Queue(ctypes.Structure):
         ("tau_prim", ctypes.c_double),
         ("ket_base", ctypes.c_void_p * N_QCLASS),
         ("mol_active", ctypes.c_void_p),
+        ("bucket_kets", ctypes.c_int),
     ]
 
 

@@ -556,6 +556,7 @@ struct PreparePlan {
     size_t off_ab[DFTK_N_PCLASS], off_np[DFTK_N_PCLASS], off_r64[DFTK_N_PCLASS], off_r32[DFTK_N_PCLASS],
         off_q[DFTK_N_PCLASS], off_qp[DFTK_N_PCLASS], off_c64[DFTK_N_PCLASS], off_c32[DFTK_N_PCLASS],
         off_row[DFTK_N_QCLASS];
+    int bucket_kets = 0;  // the s/p pairs span more than one primitive-count bucket
     size_t bytes = 0;
 };
 
@@ -593,6 +594,22 @@ int prepare_plan(const dftk_shells_t *shells, PreparePlan &pl)
             v.push_back(a);
             v.push_back(b);
         }
+    {
+        // primitive-count buckets of the s/p pairs (as the selection pass forms them)
+        static const long long bounds[DFTK_HLC_NB] = DFTK_HLC_BUCKET_BOUNDS;
+        int first = -1;
+        for (int pc = 0; pc < DFTK_N_PCLASS && !pl.bucket_kets; ++pc)
+            for (size_t k = 0; k < pl.ab[pc].size() / 2; ++k) {
+                const long long n = (long long)np[pl.ab[pc][2 * k]] * np[pl.ab[pc][2 * k + 1]];
+                int b = 0;
+                while (b + 1 < DFTK_HLC_NB && n > bounds[b]) ++b;
+                if (first < 0) first = b;
+                if (b != first) {
+                    pl.bucket_kets = 1;
+                    break;
+                }
+            }
+    }
     size_t at = 0;
     for (int pc = 0; pc < DFTK_N_PCLASS; ++pc) {
         const size_t n = pl.ab[pc].size() / 2, rec = (size_t)pair_fields(pc) * pl.kmax * n;
@@ -1006,6 +1023,7 @@ int dftk_prepare(const dftk_shells_t *shells, double tau_schwarz, double tau_pri
     }
     queue->tau_prim = tau_prim;
     queue->mol_active = nullptr;
+    queue->bucket_kets = pl.bucket_kets;
     DFTK_CUDA(cudaStreamSynchronize(s));  // the host vectors above are sources of the copies
     return DFTK_OK;
 }
@@ -1151,6 +1169,7 @@ int dftk_jk(const dftk_shells_t *shells, const dftk_pairs_t pairs[DFTK_N_PCLASS]
     P.sh = *shells;
     for (int c = 0; c < DFTK_N_QCLASS; ++c) P.ket_base[c] = queue->ket_base[c];
     P.mol_active = queue->mol_active;
+    P.bucket = queue->bucket_kets;
     P.shell_ao = shells->ao;
     for (int k = 0; k < 3; ++k) {
         if (pairs[k].n_pairs > 0 && (!pairs[k].core64 || !pairs[k].core32))
@@ -1618,7 +1637,9 @@ int dftk_grad(const dftk_shells_t *shells, const int *shell_atom, int n_atoms, c
         for (int k = 0; k < 3; ++k) {
             S.ab[k] = pairs[k].ab;
             S.q[k] = pairs[k].q;
+            S.np[k] = pairs[k].nprim;  // the selection groups survivors by the ket's primitive count
         }
+        S.bucket = queue->bucket_kets;
         for (int c = 0; c < DFTK_N_QCLASS; ++c) {
             S.n_rows[c] = P.n_rows[c];
             S.row_off[c] = P.row_off[c];

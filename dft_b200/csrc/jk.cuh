@@ -181,6 +181,7 @@ struct JkParams {
     double tau_lo, tau_hi;  // scan path: quartet processed if tau_lo <= bound < tau_hi
     double tau, tau32;      // select path: FP64 if bound >= tau32, FP32 if tau <= bound < tau32
     int dm_pow2;            // select path: bound Q_ab Q_cd max|D|^2 (gradients) instead of max|D|
+    int bucket;             // select path: group survivors by the ket's primitive-count bucket
     long long *counts;
     // select path: per class one list of (bra row, ket) with capacity total[C];
     // FP64 entries fill it from the front, FP32 entries from the back
@@ -504,11 +505,25 @@ __device__ __forceinline__ void select_classify(const JkParams &P, long long can
 }
 
 // One tile of class C's candidates (the block's SELECT_TILE consecutive
-// candidates starting at tile * SELECT_TILE).
+// candidates starting at tile * SELECT_TILE), with P.bucket set: within the
+// tile the survivors are grouped by the ket pair's primitive-pair-count
+// bucket (select_bucket:
+// nprim <= 1, 4, 9, 16, 36, more), candidate order kept inside a bucket, so
+// the 32 lanes of a class-kernel warp loop over similar primitive counts
+// (generally contracted bases mix 1- and 81-primitive pairs; with one
+// primitive count, as in STO-3G, the order is the candidate order).
+#define SELECT_NB 6
+__device__ __forceinline__ int select_bucket(int nprim)
+{
+    return nprim <= 1 ? 0 : nprim <= 4 ? 1 : nprim <= 9 ? 2 : nprim <= 16 ? 3 : nprim <= 36 ? 4 : 5;
+}
+
 template <int C>
-__device__ __forceinline__ void select_tile(const JkParams &P, long long tile, unsigned *s_cnt64, unsigned *s_cnt32,
+__device__ __forceinline__ void select_tile_bucketed(const JkParams &P, long long tile, unsigned (*s_cnt)[2 * SELECT_NB],
                                             unsigned long long &s_base64, unsigned long long &s_base32)
 {
+    using E0 = EriClass<double, C, 0>;
+    constexpr int Yc = E0::KET_CLASS;
     const long long ncand = P.total[C];
     const long long cap = ncand;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -519,9 +534,10 @@ __device__ __forceinline__ void select_tile(const JkParams &P, long long tile, u
         int r0 = 0;
         if (lane == 0 && wfirst < ncand) r0 = find_row(off, P.n_rows[C], wfirst);
         r0 = __shfl_sync(DFTK_FULL_MASK, r0, 0);
-        unsigned m64[SELECT_PER_WARP], m32[SELECT_PER_WARP];
-        int rows[SELECT_PER_WARP], kets[SELECT_PER_WARP];
-        unsigned n64 = 0, n32 = 0;
+        if (lane < 2 * SELECT_NB) s_cnt[warp][lane] = 0;
+        __syncwarp();
+        int rows[SELECT_PER_WARP], kets[SELECT_PER_WARP], keys[SELECT_PER_WARP];
+        unsigned pos[SELECT_PER_WARP];
 #pragma unroll
         for (int it = 0; it < SELECT_PER_WARP; ++it) {
             const long long cand = wfirst + it * 32 + lane;
@@ -532,56 +548,133 @@ __device__ __forceinline__ void select_tile(const JkParams &P, long long tile, u
                 select_classify<C>(P, cand, rows[it], kets[it], is64, is32, r0);
                 r0 = rows[it];  // later candidates of this lane lie at or beyond this row
             }
-            m64[it] = __ballot_sync(DFTK_FULL_MASK, is64);
-            m32[it] = __ballot_sync(DFTK_FULL_MASK, is32);
-            n64 += __popc(m64[it]);
-            n32 += __popc(m32[it]);
+            // key = bucket x 2 + precision for a survivor (bucket 0 when the
+            // caller passes no primitive counts), -1 for a dropped candidate
+            int key = -1;
+            if (is64 || is32) key = 2 * (P.np[Yc] ? select_bucket(__ldg(P.np[Yc] + kets[it])) : 0) + (is32 ? 1 : 0);
+            const unsigned same = __match_any_sync(DFTK_FULL_MASK, key);
+            pos[it] = key >= 0 ? s_cnt[warp][key] + __popc(same & below) : 0u;
+            __syncwarp();
+            if (key >= 0 && (same & below) == 0) s_cnt[warp][key] += __popc(same);
+            __syncwarp();
+            keys[it] = key;
             r0 = __shfl_sync(DFTK_FULL_MASK, r0, 0);
-        }
-        if (lane == 0) {
-            s_cnt64[warp] = n64;
-            s_cnt32[warp] = n32;
         }
         __syncthreads();
         if (threadIdx.x == 0) {
-            unsigned t64 = 0, t32 = 0;
-            for (int w = 0; w < SELECT_THREADS / 32; ++w) {
-                const unsigned a = s_cnt64[w], b = s_cnt32[w];
-                s_cnt64[w] = t64;
-                s_cnt32[w] = t32;
-                t64 += a;
-                t32 += b;
-            }
-            s_base64 = t64 ? atomicAdd(P.heads + C, (unsigned long long)t64) : 0ull;
-            s_base32 = t32 ? atomicAdd(P.heads + DFTK_N_QCLASS + C, (unsigned long long)t32) : 0ull;
+            // exclusive offsets in (precision, bucket, warp) order
+            unsigned t[2] = {0u, 0u};
+            for (int key = 0; key < 2 * SELECT_NB; ++key)
+                for (int w = 0; w < SELECT_THREADS / 32; ++w) {
+                    const unsigned n = s_cnt[w][key];
+                    s_cnt[w][key] = t[key & 1];
+                    t[key & 1] += n;
+                }
+            s_base64 = t[0] ? atomicAdd(P.heads + C, (unsigned long long)t[0]) : 0ull;
+            s_base32 = t[1] ? atomicAdd(P.heads + DFTK_N_QCLASS + C, (unsigned long long)t[1]) : 0ull;
             if (P.counts) {
-                if (t64) atomicAdd((unsigned long long *)(P.counts + C), (unsigned long long)t64);
-                if (t32) atomicAdd((unsigned long long *)(P.counts + DFTK_N_QCLASS + C), (unsigned long long)t32);
+                if (t[0]) atomicAdd((unsigned long long *)(P.counts + C), (unsigned long long)t[0]);
+                if (t[1]) atomicAdd((unsigned long long *)(P.counts + DFTK_N_QCLASS + C), (unsigned long long)t[1]);
             }
         }
         __syncthreads();
-        unsigned long long p64 = s_base64 + s_cnt64[warp];
-        unsigned long long p32 = s_base32 + s_cnt32[warp];
 #pragma unroll
         for (int it = 0; it < SELECT_PER_WARP; ++it) {
-            if (m64[it] & (1u << lane)) P.list[C][p64 + __popc(m64[it] & below)] = make_int2(rows[it], kets[it]);
-            if (m32[it] & (1u << lane))
-                P.list[C][cap - 1 - (long long)(p32 + __popc(m32[it] & below))] = make_int2(rows[it], kets[it]);
-            p64 += __popc(m64[it]);
-            p32 += __popc(m32[it]);
+            const int key = keys[it];
+            if (key < 0) continue;
+            const unsigned long long p = s_cnt[warp][key] + pos[it];
+            if ((key & 1) == 0) P.list[C][s_base64 + p] = make_int2(rows[it], kets[it]);
+            else P.list[C][cap - 1 - (long long)(s_base32 + p)] = make_int2(rows[it], kets[it]);
         }
         __syncthreads();  // s_base/s_cnt are rewritten by the next tile
     }
 }
 
+// The same in candidate order (P.bucket == 0): per warp and precision one
+// ballot-compacted run.
+template <int C>
+__device__ __forceinline__ void select_tile_plain(const JkParams &P, long long tile, unsigned (*s_cnt)[2 * SELECT_NB],
+                                                  unsigned long long &s_base64, unsigned long long &s_base32)
+{
+    const long long ncand = P.total[C];
+    const long long cap = ncand;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned below = (1u << lane) - 1u;
+    const long long *off = P.row_off[C];
+    const long long wfirst = tile * SELECT_TILE + (long long)warp * 32 * SELECT_PER_WARP;
+    int r0 = 0;
+    if (lane == 0 && wfirst < ncand) r0 = find_row(off, P.n_rows[C], wfirst);
+    r0 = __shfl_sync(DFTK_FULL_MASK, r0, 0);
+    unsigned m64[SELECT_PER_WARP], m32[SELECT_PER_WARP];
+    int rows[SELECT_PER_WARP], kets[SELECT_PER_WARP];
+    unsigned n64 = 0, n32 = 0;
+#pragma unroll
+    for (int it = 0; it < SELECT_PER_WARP; ++it) {
+        const long long cand = wfirst + it * 32 + lane;
+        bool is64 = false, is32 = false;
+        rows[it] = 0;
+        kets[it] = 0;
+        if (cand < ncand) {
+            select_classify<C>(P, cand, rows[it], kets[it], is64, is32, r0);
+            r0 = rows[it];  // later candidates of this lane lie at or beyond this row
+        }
+        m64[it] = __ballot_sync(DFTK_FULL_MASK, is64);
+        m32[it] = __ballot_sync(DFTK_FULL_MASK, is32);
+        n64 += __popc(m64[it]);
+        n32 += __popc(m32[it]);
+        r0 = __shfl_sync(DFTK_FULL_MASK, r0, 0);
+    }
+    if (lane == 0) {
+        s_cnt[warp][0] = n64;
+        s_cnt[warp][1] = n32;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned t64 = 0, t32 = 0;
+        for (int w = 0; w < SELECT_THREADS / 32; ++w) {
+            const unsigned a = s_cnt[w][0], b = s_cnt[w][1];
+            s_cnt[w][0] = t64;
+            s_cnt[w][1] = t32;
+            t64 += a;
+            t32 += b;
+        }
+        s_base64 = t64 ? atomicAdd(P.heads + C, (unsigned long long)t64) : 0ull;
+        s_base32 = t32 ? atomicAdd(P.heads + DFTK_N_QCLASS + C, (unsigned long long)t32) : 0ull;
+        if (P.counts) {
+            if (t64) atomicAdd((unsigned long long *)(P.counts + C), (unsigned long long)t64);
+            if (t32) atomicAdd((unsigned long long *)(P.counts + DFTK_N_QCLASS + C), (unsigned long long)t32);
+        }
+    }
+    __syncthreads();
+    unsigned long long p64 = s_base64 + s_cnt[warp][0];
+    unsigned long long p32 = s_base32 + s_cnt[warp][1];
+#pragma unroll
+    for (int it = 0; it < SELECT_PER_WARP; ++it) {
+        if (m64[it] & (1u << lane)) P.list[C][p64 + __popc(m64[it] & below)] = make_int2(rows[it], kets[it]);
+        if (m32[it] & (1u << lane))
+            P.list[C][cap - 1 - (long long)(p32 + __popc(m32[it] & below))] = make_int2(rows[it], kets[it]);
+        p64 += __popc(m64[it]);
+        p32 += __popc(m32[it]);
+    }
+    __syncthreads();  // s_base/s_cnt are rewritten by the next tile
+}
+
+template <int C>
+__device__ __forceinline__ void select_tile(const JkParams &P, long long tile, unsigned (*s_cnt)[2 * SELECT_NB],
+                                            unsigned long long &s_base64, unsigned long long &s_base32)
+{
+    if (P.bucket) select_tile_bucketed<C>(P, tile, s_cnt, s_base64, s_base32);
+    else select_tile_plain<C>(P, tile, s_cnt, s_base64, s_base32);
+}
+
 template <int C>
 __global__ void __launch_bounds__(SELECT_THREADS) k_select(const JkParams P)
 {
-    __shared__ unsigned s_cnt64[SELECT_THREADS / 32], s_cnt32[SELECT_THREADS / 32];
+    __shared__ unsigned s_cnt[SELECT_THREADS / 32][2 * SELECT_NB];
     __shared__ unsigned long long s_base64, s_base32;
     const long long ntiles = (P.total[C] + SELECT_TILE - 1) / SELECT_TILE;
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
-        select_tile<C>(P, tile, s_cnt64, s_cnt32, s_base64, s_base32);
+        select_tile<C>(P, tile, s_cnt, s_base64, s_base32);
 }
 
 // All classes' selection passes in one launch: block b takes tile b of the
@@ -589,7 +682,7 @@ __global__ void __launch_bounds__(SELECT_THREADS) k_select(const JkParams P)
 // grid-striding over the total.
 __global__ void __launch_bounds__(SELECT_THREADS) k_select_all(const JkParams P)
 {
-    __shared__ unsigned s_cnt64[SELECT_THREADS / 32], s_cnt32[SELECT_THREADS / 32];
+    __shared__ unsigned s_cnt[SELECT_THREADS / 32][2 * SELECT_NB];
     __shared__ unsigned long long s_base64, s_base32;
     long long base[DFTK_N_QCLASS + 1];
     base[0] = 0;
@@ -600,12 +693,12 @@ __global__ void __launch_bounds__(SELECT_THREADS) k_select_all(const JkParams P)
         while (t >= base[c + 1]) ++c;
         const long long tile = t - base[c];
         switch (c) {
-        case 0: select_tile<0>(P, tile, s_cnt64, s_cnt32, s_base64, s_base32); break;
-        case 1: select_tile<1>(P, tile, s_cnt64, s_cnt32, s_base64, s_base32); break;
-        case 2: select_tile<2>(P, tile, s_cnt64, s_cnt32, s_base64, s_base32); break;
-        case 3: select_tile<3>(P, tile, s_cnt64, s_cnt32, s_base64, s_base32); break;
-        case 4: select_tile<4>(P, tile, s_cnt64, s_cnt32, s_base64, s_base32); break;
-        default: select_tile<5>(P, tile, s_cnt64, s_cnt32, s_base64, s_base32); break;
+        case 0: select_tile<0>(P, tile, s_cnt, s_base64, s_base32); break;
+        case 1: select_tile<1>(P, tile, s_cnt, s_base64, s_base32); break;
+        case 2: select_tile<2>(P, tile, s_cnt, s_base64, s_base32); break;
+        case 3: select_tile<3>(P, tile, s_cnt, s_base64, s_base32); break;
+        case 4: select_tile<4>(P, tile, s_cnt, s_base64, s_base32); break;
+        default: select_tile<5>(P, tile, s_cnt, s_base64, s_base32); break;
         }
     }
 }

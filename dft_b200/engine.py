@@ -276,6 +276,11 @@ class IntegralEngine:
             q.total[c] = int(off[-1])
             q.row_off[c] = _lib.ptr(d_off).value
         q.tau_prim = self.tau_prim
+        # group selected quartets by the ket's primitive-count bucket when the
+        # s/p pairs differ in primitive count (general contractions)
+        sp = self._pair_class < 3
+        pb = hlc_bucket(self._seg_nprim[self._pair_a[sp]].astype(np.int64) * self._seg_nprim[self._pair_b[sp]])
+        q.bucket_kets = int(np.unique(pb).size > 1)
         self.c_queue = q
 
     def _generic_set(self, sel: np.ndarray):
@@ -403,6 +408,7 @@ class IntegralEngine:
             q.ket_base[c] = self.c_queue.ket_base[c]
         q.tau_prim = self.c_queue.tau_prim
         q.mol_active = self.c_queue.mol_active
+        q.bucket_kets = self.c_queue.bucket_kets
         q._keep = keep  # device arrays live as long as the queue
         return q
 

@@ -145,6 +145,12 @@ typedef struct {
     /* batches: molecules m with mol_active[m] == 0 are skipped by the
      * selection pass (per-molecule convergence); NULL = all active */
     const unsigned char *mol_active;
+    /* 1: the selection pass groups each tile's surviving quartets by the ket
+     * pair's primitive-pair count (nprim <= 1, 4, 9, 16, 36, more), so a
+     * warp's lanes loop over similar primitive counts (bases whose pairs
+     * differ in primitive count, e.g. general contractions); 0: candidate
+     * order (every pair has the same count, e.g. STO-3G) */
+    int bucket_kets;
 } dftk_queue_t;
 
 /* Shell quartets with a d or f shell (l <= 3).  The reference's eri_kernel takes

@@ -89,6 +89,7 @@ def test_prepare_hl_d_shells_through_the_c_abi():
         _lib.call("dftk_prepare_hl", ctypes.byref(eng.c_shells), 1e-12, eng.tau_prim, _lib.ptr(hstore), hbytes.value,
                   ctypes.byref(hl), stream)
         assert hl.n_rows == eng.c_hl.n_rows and list(hl.total) == list(eng.c_hl.total) and hl.lmax == 2
+        assert queue.bucket_kets == eng.c_queue.bucket_kets
         assert list(hl.cls_total) == list(eng.c_hl.cls_total)
         assert list(hl.n_cls_rows) == list(eng.c_hl.n_cls_rows)
         assert [list(x) for x in hl.cls_ket_seg] == [list(x) for x in eng.c_hl.cls_ket_seg]

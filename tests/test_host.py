@@ -378,3 +378,29 @@ def test_hlc_spaces_enumerate_each_quartet_once():
                     continue
                 want.append((r, k))
         assert sorted(got) == sorted(want) and len(got) == len(set(got)), c
+
+
+def test_bucket_flag_set_only_for_mixed_primitive_counts():
+    """The s/p queue asks the selection pass to group by primitive-count
+    bucket only when the s/p pairs span several buckets: never for STO-3G
+    (3 x 3 primitives in every pair), always for the generally contracted
+    test basis (pairs of 1 to 81 primitive pairs)."""
+    import json
+    import os
+
+    from dft_b200 import basis
+    from dft_b200.engine import hlc_bucket
+
+    def buckets(data, atoms, centers):
+        segs = basis.segments(basis.build_shells(data, atoms, centers))
+        n = np.array([s["exponents"].size for s in segs])
+        l = np.array([s["l"] for s in segs])
+        sp = np.nonzero(l <= 1)[0]
+        i, j = np.tril_indices(sp.size)
+        return np.unique(hlc_bucket(n[sp[i]] * n[sp[j]])).size
+
+    atoms, centers = ["8", "1", "1"], np.array([[0, 0, 0.22], [0, 1.43, -0.89], [0, -1.43, -0.89]])
+    assert buckets(basis.load_basis(), atoms, centers) == 1
+    here = os.path.dirname(os.path.abspath(__file__))
+    with open(os.path.join(here, "golden", "dz_gc_test.json")) as fh:
+        assert buckets(json.load(fh), atoms, centers) > 1
