@@ -611,6 +611,66 @@ def dshell_workload(torch):
     return eng, D, (0.5 * D).contiguous()
 
 
+def dshell_cpu_reference(seed=3, small=5000, large=30000, tau=1e-12):
+    """The reference's CPU path on the d-basis workload: uniform samples of
+    the Schwarz-kept unique quartets of the reference's own (generally
+    contracted) shells at two sizes through the host-compiled reference
+    eri_kernel (oracle/_ref; the restatement when it is not built) with the
+    restated contraction and digestion; the slope between the two timings
+    times the number of kept quartets, plus the intercept, is one build."""
+    from dft_b200 import basis, geometry
+    from oracle import oracle as orc
+
+    with open(os.path.join(REPO, "tests", "golden", "dz_gc_test.json")) as fh:
+        data = json.load(fh)
+    atoms, centers = geometry.water_cluster((2, 2, 4))
+    shells = basis.build_shells(data, atoms, centers)
+    ii, jj = np.tril_indices(len(shells))
+    diag = np.stack([ii, jj, ii, jj], axis=1).astype(np.int32)
+    vals, off = orc.eri_quartets(shells, diag)
+    q = np.sqrt(np.array([np.abs(vals[off[t]:off[t + 1]]).max() for t in range(len(ii))]))
+    # kept unique quartets (pair r >= pair k, q_r q_k >= tau): count by sorting
+    order = np.argsort(-q)
+    qs = q[order]
+    cnt = np.searchsorted(-qs, -np.where(qs > 0, tau / np.where(qs > 0, qs, 1.0), np.inf), side="right")
+    total = int(np.minimum(cnt, np.arange(1, qs.size + 1)).sum())
+    rng = np.random.default_rng(seed)
+    sa = orc.ShellArrays(shells)
+    N = sa.N
+    A = rng.normal(size=(N, N))
+    P = (A + A.T) * 0.01
+    ref = orc.ref_lib()
+
+    def sample(n):
+        out = []
+        while len(out) < n:
+            r = rng.integers(q.size, size=4 * n)
+            k = rng.integers(q.size, size=4 * n)
+            r, k = np.maximum(r, k), np.minimum(r, k)
+            keep = q[r] * q[k] >= tau
+            for x, y in zip(r[keep], k[keep]):
+                out.append((ii[x], jj[x], ii[y], jj[y]))
+        return np.array(out[:n], dtype=np.int32)
+
+    def run(quads):
+        t0 = time.perf_counter()
+        if ref is not None:
+            orc.direct_jk_reference_kernel(shells, quads, P, P / 2, P / 2, ref=ref, sa=sa)
+        else:
+            orc.direct_jk(shells, quads, P, P / 2, P / 2, sa=sa)
+        return time.perf_counter() - t0
+
+    t_small, t_large = run(sample(small)), run(sample(large))
+    slope = max((t_large - t_small) / (large - small), 0.0)
+    fixed = max(t_small - slope * small, 0.0)
+    s_build = slope * total + fixed
+    return {"kind": "reference" if ref is not None else "port", "cores": os.cpu_count(),
+            "kept_unique_quartets": total, "us_per_quartet": slope * 1e6, "s_per_build": s_build,
+            "sample": f"{small} and {large} uniformly drawn Schwarz-kept quartets (tau {tau}) of the reference's "
+                      "generally contracted shells; slope x kept quartets + intercept",
+            "sample_s": t_small + t_large}
+
+
 def dshell_figures(torch):
     """The d/f path on a polarised basis: (H2O)_16 (2x2x4 lattice) with the
     generally contracted, d-polarised test basis (tests/golden/dz_gc_test.json;
@@ -969,6 +1029,10 @@ def run_dftk_arm(args, rank, world, local_rank):
         if not args.no_extras:
             line["c10h22"] = c10h22_figures(torch, cpu=world == 1 and not args.no_cpu_baseline)
             line["d_basis"] = dshell_figures(torch)
+            if world == 1 and not args.no_cpu_baseline:
+                ref = dshell_cpu_reference()
+                ref["gpu_speedup"] = ref["s_per_build"] / (line["d_basis"]["full_build_ms"] / 1e3)
+                line["d_basis"]["cpu_reference"] = ref
             line["grad"] = gradient_figures(torch, eng, atoms, centers, r64)
             line["grad"]["config4"] = config4_gradients(torch)
             line["grid"] = grid_figures(torch, eng, centers, r64, nocc, cpu=world == 1 and not args.no_cpu_baseline)
