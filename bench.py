@@ -972,10 +972,16 @@ def run_dftk_arm(args, rank, world, local_rank):
             from dft_b200.engine import QCLASS_PAIRS
 
             qs = schwarz_by_reference_order(shells)
-            res = cpu_reference_rate(eng.quartet_totals(), shells, qs, seed=7)
+            # median of three timings of the same samples (the host cores are
+            # shared; one timing has varied by a third between runs)
+            runs = sorted((cpu_reference_rate(eng.quartet_totals(), shells, qs, seed=7) for _ in range(3)),
+                          key=lambda r: r["builds_per_s"])
+            res = runs[1]
             cpu = {"value": res["builds_per_s"], "unit": UNIT, "cores": res["cores"], "kind": res["kind"],
-                   "sample": res["sample"], "us_per_quartet": res["us_per_quartet"],
-                   "fixed_ms_per_call": res["fixed_ms"], "sample_s": res["sample_s"]}
+                   "sample": res["sample"] + "; median of 3 timings",
+                   "builds_per_s_3_timings": [r["builds_per_s"] for r in runs],
+                   "us_per_quartet": res["us_per_quartet"],
+                   "fixed_ms_per_call": res["fixed_ms"], "sample_s": sum(r["sample_s"] for r in runs)}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
