@@ -1284,16 +1284,18 @@ template <int LM, typename K> int hl_smem_optin(K kernel, size_t extra_static = 
 // warp work items (32 candidates x ket-component split).
 static_assert(HLC_N_CLASSES == sizeof(((dftk_hl_t *)nullptr)->cls_off) / sizeof(void *),
               "dftk_hl_t holds one candidate space per generated d class");
-template <int C, int S = 0> int launch_hlc(const HlcParams &P, cudaStream_t s)
+// The chunk kernels of class C, dealt round-robin over `ns` streams (their
+// J/K sums are atomics, which commute; small chunk kernels overlap).
+template <int C, int S = 0> int launch_hlc(const HlcParams &P, const cudaStream_t *st, int ns, int &next)
 {
     if (P.total[C] == 0) return DFTK_OK;
     const long long items = (P.total[C] + 31) / 32;
     long long blocks = (items + 3) / 4;
     const long long cap = (long long)sm_count() * 16;
     if (blocks > cap) blocks = cap;
-    k_hlc<C, S><<<(unsigned)blocks, 128, 0, s>>>(P);
+    k_hlc<C, S><<<(unsigned)blocks, 128, 0, st[next++ % ns]>>>(P);
     DFTK_LAUNCHED("k_hlc");
-    if constexpr (S + 1 < HlClass<double, C, 0>::NSPLIT) return launch_hlc<C, S + 1>(P, s);
+    if constexpr (S + 1 < HlClass<double, C, 0>::NSPLIT) return launch_hlc<C, S + 1>(P, st, ns, next);
     return DFTK_OK;
 }
 }  // namespace
@@ -1415,12 +1417,29 @@ int dftk_jk_hl(const dftk_shells_t *shells, const dftk_hl_t *hl, const double *D
         C.uhf = uhf;
         C.tau = tau;
         C.counts = counts;
-        if ((st = launch_hlc<0>(C, s)) || (st = launch_hlc<1>(C, s)) || (st = launch_hlc<2>(C, s)) ||
-            (st = launch_hlc<3>(C, s)) || (st = launch_hlc<4>(C, s)) || (st = launch_hlc<5>(C, s)) ||
-            (st = launch_hlc<6>(C, s)) || (st = launch_hlc<7>(C, s)) || (st = launch_hlc<8>(C, s)) ||
-            (st = launch_hlc<9>(C, s)) || (st = launch_hlc<10>(C, s)) || (st = launch_hlc<11>(C, s)) ||
-            (st = launch_hlc<12>(C, s)) || (st = launch_hlc<13>(C, s)) || (st = launch_hlc<14>(C, s)))
+        // the library's class streams (as dftk_jk forks them), joined below
+        cudaStream_t cls[DFTK_N_QCLASS];
+        int n_aux = 0, dev = 0, next = 0;
+        DFTK_CUDA(cudaGetDevice(&dev));
+        std::unique_lock<std::mutex> fork_lock(g_pool[dev].mutex);
+        if ((st = fork_class_streams(s, cls, n_aux))) return st;
+        cudaStream_t sts[4] = {s, s, s, s};
+        int ns = 1;
+        for (int c = 0; c < DFTK_N_QCLASS && ns < 4; ++c) {
+            bool seen = false;
+            for (int k = 0; k < ns; ++k) seen = seen || sts[k] == cls[c];
+            if (!seen) sts[ns++] = cls[c];
+        }
+        if ((st = launch_hlc<0>(C, sts, ns, next)) || (st = launch_hlc<1>(C, sts, ns, next)) ||
+            (st = launch_hlc<2>(C, sts, ns, next)) || (st = launch_hlc<3>(C, sts, ns, next)) ||
+            (st = launch_hlc<4>(C, sts, ns, next)) || (st = launch_hlc<5>(C, sts, ns, next)) ||
+            (st = launch_hlc<6>(C, sts, ns, next)) || (st = launch_hlc<7>(C, sts, ns, next)) ||
+            (st = launch_hlc<8>(C, sts, ns, next)) || (st = launch_hlc<9>(C, sts, ns, next)) ||
+            (st = launch_hlc<10>(C, sts, ns, next)) || (st = launch_hlc<11>(C, sts, ns, next)) ||
+            (st = launch_hlc<12>(C, sts, ns, next)) || (st = launch_hlc<13>(C, sts, ns, next)) ||
+            (st = launch_hlc<14>(C, sts, ns, next)))
             return st;
+        if ((st = join_class_streams(s, n_aux))) return st;
     }
     if (total > 0) {
         long long blocks = total;
