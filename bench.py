@@ -671,6 +671,36 @@ def dshell_cpu_reference(seed=3, small=5000, large=30000, tau=1e-12):
             "sample_s": t_small + t_large}
 
 
+def dshell_scf(torch):
+    """RHF/DIIS SCF of the d-basis workload ((H2O)_16, generally contracted
+    d-polarised basis, spherical basis as the reference's SCF), FP64 and
+    mixed: wall time (device-synchronised, after one warm-up solve),
+    iterations, Fock builds and their time, energy and the mixed-vs-FP64
+    energy difference."""
+    from dft_b200 import basis, geometry
+    from dft_b200.engine import IntegralEngine
+    from dft_b200.scf import scf_rhf
+
+    with open(os.path.join(REPO, "tests", "golden", "dz_gc_test.json")) as fh:
+        data = json.load(fh)
+    atoms, centers = geometry.water_cluster((2, 2, 4))
+    eng = IntegralEngine(basis.build_shells(data, atoms, centers), tau_schwarz=1e-12)
+    S, T, V = eng.one_electron(atoms, centers)
+    nocc = basis.n_electrons(atoms) // 2
+    enn = geometry.nuclear_repulsion(atoms, centers)
+    out = {"workload": "(H2O)_16 2x2x4 lattice, generally contracted d-polarised test basis, RHF/DIIS"}
+    scf_rhf(eng, T + V, S, nocc, enn)
+    for name, mixed in (("fp64", False), ("mixed", True)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = scf_rhf(eng, T + V, S, nocc, enn, mixed=mixed)
+        torch.cuda.synchronize()
+        out[name] = {"wall_s": time.perf_counter() - t0, "iterations": r.iterations, "converged": bool(r.converged),
+                     "fock_builds": r.fock_builds, "fock_s": r.fock_seconds, "energy": r.energy}
+    out["mixed_minus_fp64_uEh"] = (out["mixed"]["energy"] - out["fp64"]["energy"]) * 1e6
+    return out
+
+
 def dshell_figures(torch):
     """The d/f path on a polarised basis: (H2O)_16 (2x2x4 lattice) with the
     generally contracted, d-polarised test basis (tests/golden/dz_gc_test.json;
@@ -1039,6 +1069,7 @@ def run_dftk_arm(args, rank, world, local_rank):
                 ref = dshell_cpu_reference()
                 ref["gpu_speedup"] = ref["s_per_build"] / (line["d_basis"]["full_build_ms"] / 1e3)
                 line["d_basis"]["cpu_reference"] = ref
+            line["d_basis"]["scf"] = dshell_scf(torch)
             line["grad"] = gradient_figures(torch, eng, atoms, centers, r64)
             line["grad"]["config4"] = config4_gradients(torch)
             line["grid"] = grid_figures(torch, eng, centers, r64, nocc, cpu=world == 1 and not args.no_cpu_baseline)
