@@ -15,7 +15,9 @@
 //   T >= 50: F_0 = sqrt(pi / T) / 2 (erfc(7) < 5e-23) and the upward
 //           recursion F_{m+1} = (2m + 1) F_m / (2T); the exp(-T) < 2e-22 term
 //           it drops changes F_m by < 2e-14 relative for m <= 7.
-// Tables: orders L = 0..12, grid points T_k = 0, 0.1, ..., 50, computed on the
+// Tables (internal linkage: each device module of the library -- dftk.cu and
+// the hlc_part_*.cu units -- holds its own copy, filled by dftk_init):
+// orders L = 0..12, grid points T_k = 0, 0.1, ..., 50, computed on the
 // host in long double from the all-positive series
 // F_m(T) = exp(-T) sum_i (2T)^i / ((2m+1)(2m+3)...(2m+2i+1)).
 // Orders >= 1 in FP64 read a half-step table instead (T_k = k / 20, so
@@ -35,16 +37,16 @@
 #define DFTK_BOYS_W 8          // coefficients per grid point
 #define DFTK_BOYS_TMAX 50.0
 
-__device__ __align__(128) double g_boys64[DFTK_BOYS_NL * DFTK_BOYS_ROWS * DFTK_BOYS_W];
-__device__ double g_bexp64[DFTK_BOYS_ROWS];
+static __device__ __align__(128) double g_boys64[DFTK_BOYS_NL * DFTK_BOYS_ROWS * DFTK_BOYS_W];
+static __device__ double g_bexp64[DFTK_BOYS_ROWS];
 #ifndef DFTK_BOYS_HALFSTEP
 #define DFTK_BOYS_HALFSTEP 1
 #endif
 #define DFTK_BOYS_HROWS 1001   // half-step grid T_k = k / 20, k = 0..1000
 // half-step rows (orders >= 1): F_{L+j}(T_k) / j!, j = 0..6, then exp(-T_k)
-__device__ __align__(128) double g_boys64h[DFTK_BOYS_NL * DFTK_BOYS_HROWS * DFTK_BOYS_W];
-__device__ __align__(128) float g_boys32[DFTK_BOYS_NL * DFTK_BOYS_ROWS * DFTK_BOYS_W];
-__device__ float g_bexp32[DFTK_BOYS_ROWS];
+static __device__ __align__(128) double g_boys64h[DFTK_BOYS_NL * DFTK_BOYS_HROWS * DFTK_BOYS_W];
+static __device__ __align__(128) float g_boys32[DFTK_BOYS_NL * DFTK_BOYS_ROWS * DFTK_BOYS_W];
+static __device__ float g_bexp32[DFTK_BOYS_ROWS];
 
 // 32-byte read-only vector loads (sm_100: ld.global.nc.v4.f64 / .v8.f32);
 // the address must be 32-byte aligned (table rows are)

@@ -20,6 +20,7 @@
 #include "grid.cuh"
 #include "hl.cuh"
 #include "hlc.cuh"
+#include "hlc_parts.h"
 
 namespace {
 
@@ -146,6 +147,14 @@ int ensure_init()
     DFTK_CUDA(cudaMemcpyToSymbol(g_bexp64, g_exp64.data(), sizeof(double) * g_exp64.size()));
     DFTK_CUDA(cudaMemcpyToSymbol(g_bexp32, g_exp32.data(), sizeof(float) * g_exp32.size()));
     DFTK_CUDA(cudaMemcpyToSymbol(g_boys64h, g_tab64h.data(), sizeof(double) * g_tab64h.size()));
+    {
+        const BoysTables t = {g_tab64.data(), g_tab64.size(), g_tab32.data(), g_tab32.size(), g_exp64.data(),
+                              g_exp64.size(), g_exp32.data(), g_exp32.size(), g_tab64h.data(), g_tab64h.size()};
+        int st;
+        if ((st = hlc_part_a_init(t)) || (st = hlc_part_b_init(t)) || (st = hlc_part_c_init(t)) ||
+            (st = hlc_part_d_init(t)))
+            return st;
+    }
     StreamPool &sp = g_pool[dev];
     for (int i = 0; i < 2; ++i) {
         DFTK_CUDA(cudaStreamCreateWithFlags(&sp.aux[i], cudaStreamNonBlocking));
@@ -793,6 +802,8 @@ void class_spaces(const std::vector<int> &l, const std::vector<int> &np, const s
 
 }  // namespace
 
+int dftk_internal_fail_cuda(cudaError_t e, const char *where) { return fail_cuda(e, where); }
+
 extern "C" {
 
 int dftk_prepare_hl_bytes(const dftk_shells_t *shells, size_t *bytes)
@@ -1284,20 +1295,6 @@ template <int LM, typename K> int hl_smem_optin(K kernel, size_t extra_static = 
 // warp work items (32 candidates x ket-component split).
 static_assert(HLC_N_CLASSES == sizeof(((dftk_hl_t *)nullptr)->cls_off) / sizeof(void *),
               "dftk_hl_t holds one candidate space per generated d class");
-// The chunk kernels of class C, dealt round-robin over `ns` streams (their
-// J/K sums are atomics, which commute; small chunk kernels overlap).
-template <int C, int S = 0> int launch_hlc(const HlcParams &P, const cudaStream_t *st, int ns, int &next)
-{
-    if (P.total[C] == 0) return DFTK_OK;
-    const long long items = (P.total[C] + 31) / 32;
-    long long blocks = (items + 3) / 4;
-    const long long cap = (long long)sm_count() * 16;
-    if (blocks > cap) blocks = cap;
-    k_hlc<C, S><<<(unsigned)blocks, 128, 0, st[next++ % ns]>>>(P);
-    DFTK_LAUNCHED("k_hlc");
-    if constexpr (S + 1 < HlClass<double, C, 0>::NSPLIT) return launch_hlc<C, S + 1>(P, st, ns, next);
-    return DFTK_OK;
-}
 }  // namespace
 
 extern "C" {
@@ -1430,14 +1427,9 @@ int dftk_jk_hl(const dftk_shells_t *shells, const dftk_hl_t *hl, const double *D
             for (int k = 0; k < ns; ++k) seen = seen || sts[k] == cls[c];
             if (!seen) sts[ns++] = cls[c];
         }
-        if ((st = launch_hlc<0>(C, sts, ns, next)) || (st = launch_hlc<1>(C, sts, ns, next)) ||
-            (st = launch_hlc<2>(C, sts, ns, next)) || (st = launch_hlc<3>(C, sts, ns, next)) ||
-            (st = launch_hlc<4>(C, sts, ns, next)) || (st = launch_hlc<5>(C, sts, ns, next)) ||
-            (st = launch_hlc<6>(C, sts, ns, next)) || (st = launch_hlc<7>(C, sts, ns, next)) ||
-            (st = launch_hlc<8>(C, sts, ns, next)) || (st = launch_hlc<9>(C, sts, ns, next)) ||
-            (st = launch_hlc<10>(C, sts, ns, next)) || (st = launch_hlc<11>(C, sts, ns, next)) ||
-            (st = launch_hlc<12>(C, sts, ns, next)) || (st = launch_hlc<13>(C, sts, ns, next)) ||
-            (st = launch_hlc<14>(C, sts, ns, next)))
+        // the chunk kernels live in the separately compiled hlc_part_*.cu units
+        if ((st = hlc_part_a_launch(C, sts, ns, next)) || (st = hlc_part_b_launch(C, sts, ns, next)) ||
+            (st = hlc_part_c_launch(C, sts, ns, next)) || (st = hlc_part_d_launch(C, sts, ns, next)))
             return st;
         if ((st = join_class_streams(s, n_aux))) return st;
     }

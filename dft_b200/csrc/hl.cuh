@@ -51,7 +51,7 @@ template <int LM> struct HlScratch {
 
 // Cartesian powers of component k of momentum l, in combinations() order
 // (z power outer, then y, x innermost); packed x | y << 4 | z << 8.
-__constant__ int c_hl_comp[HL_LMAX + 1][HL_NC] = {
+static __constant__ int c_hl_comp[HL_LMAX + 1][HL_NC] = {
     {0x000},
     {0x001, 0x010, 0x100},
     {0x002, 0x011, 0x020, 0x101, 0x110, 0x200},
@@ -60,7 +60,7 @@ __constant__ int c_hl_comp[HL_LMAX + 1][HL_NC] = {
 // 1 / sqrt(prod (2 l_i - 1)!!) per component (1/sqrt(3), 1/sqrt(15))
 #define HL_R3 0.57735026918962576451
 #define HL_R15 0.25819888974716112568
-__constant__ double c_hl_cnorm[HL_LMAX + 1][HL_NC] = {
+static __constant__ double c_hl_cnorm[HL_LMAX + 1][HL_NC] = {
     {1.0},
     {1.0, 1.0, 1.0},
     {HL_R3, 1.0, HL_R3, 1.0, 1.0, HL_R3},
@@ -531,7 +531,7 @@ __global__ void __launch_bounds__(32) k_hl_emit(const dftk_shells_t sh, const df
 // R^{(0)}_{tuv}(alpha, X, Y, Z), t+u+v <= L <= 2 HL_LMAX, for one thread,
 // tet-indexed (hl_tet): the same level-by-level recursion as hl_quartet.
 #define HL_NR1 210  // R^{(n)}_{tuv} with t+u+v+n <= 2 HL_LMAX
-__device__ void hl_R_thread(int L, double alpha, double X, double Y, double Z, double *R0)
+static __device__ void hl_R_thread(int L, double alpha, double X, double Y, double Z, double *R0)
 {
     double F[2 * HL_LMAX + 1];
     boys_runtime(L, alpha * (X * X + Y * Y + Z * Z), F);
@@ -576,7 +576,7 @@ __device__ void hl_R_thread(int L, double alpha, double X, double Y, double Z, d
 // formulas with run-time component loops (overlap_1d and T_raw,
 // shelled.py:104-155; nuclear_kernel's V, shelled.py:420-436), the component
 // normalisation applied per Cartesian function.  One thread per pair.
-__global__ void k_one_electron_hl(const dftk_shells_t sh, int n_atoms, const double *atom_xyz,
+static __global__ void k_one_electron_hl(const dftk_shells_t sh, int n_atoms, const double *atom_xyz,
                                   const double *atom_z, double *S, double *T, double *V)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -677,7 +677,7 @@ __global__ void k_one_electron_hl(const dftk_shells_t sh, int n_atoms, const dou
 
 // J += Y + Y^T, K += Z + Z^T (one molecule): the d-quartet part added to the
 // s/p part dftk_jk wrote.
-__global__ void k_symmetrize_add(int N, const double *Y, const double *Za, const double *Zb, double *J, double *Ka,
+static __global__ void k_symmetrize_add(int N, const double *Y, const double *Za, const double *Zb, double *J, double *Ka,
                                  double *Kb, int uhf)
 {
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < (long long)N * N;

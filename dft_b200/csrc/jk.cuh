@@ -22,7 +22,7 @@ __device__ __forceinline__ void write_core(const dftk_pairs_t &pr, long long slo
 // One thread per (primitive slot k, pair); pair index fastest so the SoA
 // record writes are coalesced.  Replaces the per-pair nuclear_kernel launch
 // and pair_cache dict (shelled.py:1000-1059) for the ERI path.
-__global__ void k_pair_data(const dftk_shells_t sh, const dftk_pairs_t pr, int nfields)
+static __global__ void k_pair_data(const dftk_shells_t sh, const dftk_pairs_t pr, int nfields)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int n = pr.n_pairs;
@@ -112,7 +112,7 @@ __device__ __forceinline__ double diag_max_all(const dftk_pairs_t &pr, int pair,
 // primitive records of the pair are then reordered by descending q_k (both
 // copies) so the ERI loops can stop at the first negligible primitive.
 template <int PC>
-__global__ void k_schwarz(const dftk_pairs_t pr, int nfields)
+static __global__ void k_schwarz(const dftk_pairs_t pr, int nfields)
 {
     const int pair = blockIdx.x * blockDim.x + threadIdx.x;
     if (pair >= pr.n_pairs) return;
@@ -220,7 +220,7 @@ __device__ __forceinline__ int find_row(const long long *off, long long n_rows, 
 // Shell-block maxima of |D| (and |D_a|, |D_b| for UHF): Dsh[dsh + x * ns + y]
 // per molecule (x, y molecule-local shells).  Thread t = (x global, y local),
 // y < max_ns.
-__global__ void k_dsh(const dftk_shells_t sh, int max_ns, const double *D, const double *Da, const double *Db,
+static __global__ void k_dsh(const dftk_shells_t sh, int max_ns, const double *D, const double *Da, const double *Db,
                       int uhf, float *Dsh)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -680,7 +680,7 @@ __global__ void __launch_bounds__(SELECT_THREADS) k_select(const JkParams P)
 // All classes' selection passes in one launch: block b takes tile b of the
 // concatenated tile ranges (tile_base[c] .. tile_base[c + 1] for class c),
 // grid-striding over the total.
-__global__ void __launch_bounds__(SELECT_THREADS) k_select_all(const JkParams P)
+static __global__ void __launch_bounds__(SELECT_THREADS) k_select_all(const JkParams P)
 {
     __shared__ unsigned s_cnt[SELECT_THREADS / 32][2 * SELECT_NB];
     __shared__ unsigned long long s_base64, s_base32;
@@ -864,7 +864,7 @@ __global__ void __launch_bounds__(128, MINB) k_jk_persist(const JkParams P)
 }
 
 // J = Y + Y^T, K = Z + Z^T within each molecule's block (blockIdx.y = molecule)
-__global__ void k_symmetrize(const dftk_shells_t sh, const double *Y, const double *Za, const double *Zb, double *J,
+static __global__ void k_symmetrize(const dftk_shells_t sh, const double *Y, const double *Za, const double *Zb, double *J,
                              double *Ka, double *Kb, int uhf)
 {
     const int m = blockIdx.y;
@@ -961,7 +961,7 @@ __device__ __forceinline__ void emit_any(int C, const EmitParams &P, int row, in
 }
 
 // One thread per quartet; desc flags bit 3 selects the FP32 evaluation.
-__global__ void k_emit(const EmitParams P)
+static __global__ void k_emit(const EmitParams P)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= P.nq) return;
