@@ -531,6 +531,7 @@ __global__ void __launch_bounds__(32) k_hl_emit(const dftk_shells_t sh, const df
 // R^{(0)}_{tuv}(alpha, X, Y, Z), t+u+v <= L <= 2 HL_LMAX, for one thread,
 // tet-indexed (hl_tet): the same level-by-level recursion as hl_quartet.
 #define HL_NR1 210  // R^{(n)}_{tuv} with t+u+v+n <= 2 HL_LMAX
+#ifndef DFTK_HLC_PART  // not compiled into the hlc_part_*.cu units (unused there)
 static __device__ void hl_R_thread(int L, double alpha, double X, double Y, double Z, double *R0)
 {
     double F[2 * HL_LMAX + 1];
@@ -570,12 +571,14 @@ static __device__ void hl_R_thread(int L, double alpha, double X, double Y, doub
 #pragma unroll 1
     for (int k = 0; k < n0; ++k) R0[k] = R[k];
 }
+#endif
 
 // S, T, V of the shell pairs (i, j), j <= i, with a d shell (the s/p pairs
 // are k_one_electron's): the same MD overlap / kinetic / nuclear-attraction
 // formulas with run-time component loops (overlap_1d and T_raw,
 // shelled.py:104-155; nuclear_kernel's V, shelled.py:420-436), the component
 // normalisation applied per Cartesian function.  One thread per pair.
+#ifndef DFTK_HLC_PART  // not compiled into the hlc_part_*.cu units (unused there)
 static __global__ void k_one_electron_hl(const dftk_shells_t sh, int n_atoms, const double *atom_xyz,
                                   const double *atom_z, double *S, double *T, double *V)
 {
@@ -674,9 +677,11 @@ static __global__ void k_one_electron_hl(const dftk_shells_t sh, int n_atoms, co
         V[r] = V[c] = g * v_acc[k];
     }
 }
+#endif
 
 // J += Y + Y^T, K += Z + Z^T (one molecule): the d-quartet part added to the
 // s/p part dftk_jk wrote.
+#ifndef DFTK_HLC_PART  // not compiled into the hlc_part_*.cu units (unused there)
 static __global__ void k_symmetrize_add(int N, const double *Y, const double *Za, const double *Zb, double *J, double *Ka,
                                  double *Kb, int uhf)
 {
@@ -689,3 +694,4 @@ static __global__ void k_symmetrize_add(int N, const double *Y, const double *Za
         if (uhf) Kb[t] += Zb[t] + Zb[ot];
     }
 }
+#endif

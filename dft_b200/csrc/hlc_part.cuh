@@ -3,6 +3,9 @@
 // initialiser HLC_PART_INIT (the including file defines the four macros).
 #pragma once
 
+// leaves out the shared headers' non-template kernels, which only dftk.cu launches
+#define DFTK_HLC_PART 1
+
 #include "dftk.h"
 #include "hlc.cuh"
 #include "hlc_parts.h"

@@ -22,6 +22,7 @@ __device__ __forceinline__ void write_core(const dftk_pairs_t &pr, long long slo
 // One thread per (primitive slot k, pair); pair index fastest so the SoA
 // record writes are coalesced.  Replaces the per-pair nuclear_kernel launch
 // and pair_cache dict (shelled.py:1000-1059) for the ERI path.
+#ifndef DFTK_HLC_PART  // not compiled into the hlc_part_*.cu units (unused there)
 static __global__ void k_pair_data(const dftk_shells_t sh, const dftk_pairs_t pr, int nfields)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -63,6 +64,7 @@ static __global__ void k_pair_data(const dftk_shells_t sh, const dftk_pairs_t pr
     }
     if (pr.core64) write_core(pr, (long long)k * n + pair, f[F_PX], f[F_PY], f[F_PZ], f[F_P], f[F_K], 0.0f);
 }
+#endif
 
 // ------------------------------------------------------------------ helpers
 template <int C, typename T, int S>
@@ -111,6 +113,7 @@ __device__ __forceinline__ double diag_max_all(const dftk_pairs_t &pr, int pair,
 // contracted pair, and per primitive pair q_k = sqrt(max |(ab_k|ab_k)|); the
 // primitive records of the pair are then reordered by descending q_k (both
 // copies) so the ERI loops can stop at the first negligible primitive.
+#ifndef DFTK_HLC_PART  // not compiled into the hlc_part_*.cu units (unused there)
 template <int PC>
 static __global__ void k_schwarz(const dftk_pairs_t pr, int nfields)
 {
@@ -155,6 +158,7 @@ static __global__ void k_schwarz(const dftk_pairs_t pr, int nfields)
                        pr.rec64[3LL * pr.kmax * n + o], pr.rec64[4LL * pr.kmax * n + o], qk[order[k]]);
         }
 }
+#endif
 
 // ------------------------------------------------------------------- J / K
 struct JkParams {
@@ -220,6 +224,7 @@ __device__ __forceinline__ int find_row(const long long *off, long long n_rows, 
 // Shell-block maxima of |D| (and |D_a|, |D_b| for UHF): Dsh[dsh + x * ns + y]
 // per molecule (x, y molecule-local shells).  Thread t = (x global, y local),
 // y < max_ns.
+#ifndef DFTK_HLC_PART  // not compiled into the hlc_part_*.cu units (unused there)
 static __global__ void k_dsh(const dftk_shells_t sh, int max_ns, const double *D, const double *Da, const double *Db,
                       int uhf, float *Dsh)
 {
@@ -242,6 +247,7 @@ static __global__ void k_dsh(const dftk_shells_t sh, int max_ns, const double *D
         }
     Dsh[v.dsh + (long long)(x - v.s0) * v.ns + yl] = (float)m;
 }
+#endif
 
 // Digest one contracted block into the half-accumulators Y (J) and Z (K):
 //   Y_ab += 2/w sum_cd I D_cd,  Y_cd += 2/w sum_ab I D_ab,
@@ -680,6 +686,7 @@ __global__ void __launch_bounds__(SELECT_THREADS) k_select(const JkParams P)
 // All classes' selection passes in one launch: block b takes tile b of the
 // concatenated tile ranges (tile_base[c] .. tile_base[c + 1] for class c),
 // grid-striding over the total.
+#ifndef DFTK_HLC_PART  // not compiled into the hlc_part_*.cu units (unused there)
 static __global__ void __launch_bounds__(SELECT_THREADS) k_select_all(const JkParams P)
 {
     __shared__ unsigned s_cnt[SELECT_THREADS / 32][2 * SELECT_NB];
@@ -702,6 +709,7 @@ static __global__ void __launch_bounds__(SELECT_THREADS) k_select_all(const JkPa
         }
     }
 }
+#endif
 
 // Minimum resident 128-thread blocks per SM requested from the compiler for
 // each class kernel (caps its registers; 1 = no cap).  Measured on B200 for
@@ -864,6 +872,7 @@ __global__ void __launch_bounds__(128, MINB) k_jk_persist(const JkParams P)
 }
 
 // J = Y + Y^T, K = Z + Z^T within each molecule's block (blockIdx.y = molecule)
+#ifndef DFTK_HLC_PART  // not compiled into the hlc_part_*.cu units (unused there)
 static __global__ void k_symmetrize(const dftk_shells_t sh, const double *Y, const double *Za, const double *Zb, double *J,
                              double *Ka, double *Kb, int uhf)
 {
@@ -879,6 +888,7 @@ static __global__ void k_symmetrize(const dftk_shells_t sh, const double *Y, con
         if (uhf) Kb[o] = Zb[o] + Zb[ot];
     }
 }
+#endif
 
 // ------------------------------------------------------------- ERI blocks
 struct EmitParams {
@@ -961,6 +971,7 @@ __device__ __forceinline__ void emit_any(int C, const EmitParams &P, int row, in
 }
 
 // One thread per quartet; desc flags bit 3 selects the FP32 evaluation.
+#ifndef DFTK_HLC_PART  // not compiled into the hlc_part_*.cu units (unused there)
 static __global__ void k_emit(const EmitParams P)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -990,3 +1001,4 @@ static __global__ void k_emit(const EmitParams P)
     if (flags & 8) emit_any<float>(C, P, row, ket, slot, stride, out);
     else emit_any<double>(C, P, row, ket, slot, stride, out);
 }
+#endif
