@@ -1006,17 +1006,23 @@ def run_dftk_arm(args, rank, world, local_rank):
         if world == 1 and not args.no_cpu_baseline:
             from dft_b200.engine import QCLASS_PAIRS
 
-            qs = schwarz_by_reference_order(shells)
-            # median of three timings of the same samples (the host cores are
-            # shared; one timing has varied by a third between runs)
-            runs = sorted((cpu_reference_rate(eng.quartet_totals(), shells, qs, seed=7) for _ in range(3)),
-                          key=lambda r: r["builds_per_s"])
-            res = runs[1]
-            cpu = {"value": res["builds_per_s"], "unit": UNIT, "cores": res["cores"], "kind": res["kind"],
-                   "sample": res["sample"] + "; median of 3 timings",
-                   "builds_per_s_3_timings": [r["builds_per_s"] for r in runs],
-                   "us_per_quartet": res["us_per_quartet"],
-                   "fixed_ms_per_call": res["fixed_ms"], "sample_s": sum(r["sample_s"] for r in runs)}
+            # the reference arm of this script in a child process: the same
+            # code and samples as `--impl reference`, on host cores that this
+            # process's GPU work and thread pools leave alone (timed in-process
+            # after the GPU work, the same samples ran up to a third slower)
+            import subprocess
+
+            child = subprocess.run([sys.executable, os.path.abspath(__file__), "--impl", "reference", "--steps", "3",
+                                    "--warmup", "3"], capture_output=True, text=True, timeout=600,
+                                   env=dict(os.environ, CUDA_VISIBLE_DEVICES=""))
+            ref_lines = [x for x in child.stdout.splitlines() if x.startswith("{")]
+            if child.returncode == 0 and ref_lines:
+                rl = json.loads(ref_lines[-1])
+                cb = rl.get("cpu_baseline", {})
+                cpu = {"value": rl["value"], "unit": UNIT, "cores": cb.get("cores"), "kind": cb.get("kind"),
+                       "sample": cb.get("sample"), "us_per_quartet": cb.get("us_per_quartet"),
+                       "builds_per_s_per_step": rl.get("builds_per_s_per_step"),
+                       "method": "bench.py --impl reference --steps 3 --warmup 3, run as a child process"}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
