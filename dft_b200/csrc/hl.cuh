@@ -1,6 +1,10 @@
 // Shell quartets with a d or f shell (l <= 3): one warp per quartet,
 // McMurchie-Davidson with run-time momenta, the Cartesian block and the
-// Hermite intermediates in shared memory.
+// Hermite intermediates in shared memory.  J/K builds send it the quartets
+// with an f shell (every d class without one has generated thread-per-quartet
+// code, hlc.cuh), or every d/f quartet when the caller gives no class spaces;
+// the ERI-block emission, Schwarz factors and one-electron integrals of d and
+// f shells use it throughout.
 //
 // Per primitive quartet (bra primitive pair i outside, ket pair j inside):
 //   R^{(n)}_{tuv}, t+u+v+n <= L, level by level over the warp's lanes

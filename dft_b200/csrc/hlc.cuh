@@ -1,11 +1,13 @@
-// Thread-per-quartet J/K kernels of the d classes with total momentum <= 5
-// ((ds|ss) .. (dp|ds), hl_classes.cuh, generated by gen_hl.py): candidate
-// spaces indexed through the d path's pair sets (the hi rows of one pair kind
-// as bras; the lo rows of one kind, or the hi rows of one kind, as kets), and
-// the s/p digestion generalised to threads that hold a chunk of bra and of
-// ket components.  One warp takes 32 consecutive candidates of one class (and
-// one component chunk), as the s/p scan kernel does; the quartets of a row
-// are consecutive, so the bra pair is usually warp-uniform.
+// Thread-per-quartet J/K kernels of the fifteen d classes without an f shell
+// ((ds|ss) .. (dd|dd), hl_classes.cuh, written by gen_hl.py at build time):
+// candidate spaces indexed through the d path's pair sets (the hi rows of one
+// pair kind as bras; the lo rows of one kind, or the hi rows of one kind, as
+// kets, grouped by primitive-count bucket), and the s/p digestion generalised
+// to threads that hold a chunk of bra and of ket components.  One warp takes
+// 32 consecutive candidates of one class and component chunk, as the s/p scan
+// kernel does; the quartets of a (row, bucket) segment are consecutive, so
+// the bra pair is usually warp-uniform.  The kernels are instantiated in the
+// hlc_part_*.cu units (hlc_part.cuh), one kernel per chunk.
 //
 // Pair kinds: 0 ss, 1 ps, 2 pp (lo set), 3 ds, 4 dp, 5 dd (hi set); pairs
 // with an f shell have no kind and stay with the warp-per-quartet kernel.
