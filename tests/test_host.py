@@ -404,3 +404,48 @@ def test_bucket_flag_set_only_for_mixed_primitive_counts():
     here = os.path.dirname(os.path.abspath(__file__))
     with open(os.path.join(here, "golden", "dz_gc_test.json")) as fh:
         assert buckets(json.load(fh), atoms, centers) > 1
+
+
+def test_generated_hermite_coefficients_match_recursion():
+    """The E^{ab}_t definitions gen_hl.py emits for the d classes (up to a = b
+    = 2), evaluated here as Python, equal the McMurchie-Davidson recursion
+    E^{a+1,b}_t = h E^{ab}_{t-1} + PA E^{ab}_t + (t+1) E^{ab}_{t+1} (b
+    likewise with PB) computed directly."""
+    import os
+    import re
+    import sys
+
+    csrc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "dft_b200", "csrc")
+    sys.path.insert(0, csrc)
+    try:
+        import gen_hl
+    finally:
+        sys.path.remove(csrc)
+    rng = np.random.default_rng(8)
+    vals = {"bh": rng.uniform(0.1, 2.0)}
+    for x in "xyz":
+        vals[f"bA{x}"], vals[f"bB{x}"] = rng.uniform(-2, 2, size=2)
+    for line in gen_hl.e_defs("b", 2, 2):
+        m = re.match(r"const T (\w+) = (.*);", line)
+        expr = re.sub(r"T\((\d+)\)", r"\1", m.group(2))
+        vals[m.group(1)] = eval(expr, {}, vals)
+
+    def direct(a, b, pa, pb, h):
+        E = {(0, 0): {0: 1.0}}
+        for i in range(1, a + 1):
+            lo = E[(i - 1, 0)]
+            E[(i, 0)] = {t: h * lo.get(t - 1, 0) + pa * lo.get(t, 0) + (t + 1) * lo.get(t + 1, 0) for t in range(i + 1)}
+        for i in range(a + 1):
+            for j in range(1, b + 1):
+                lo = E[(i, j - 1)]
+                E[(i, j)] = {t: h * lo.get(t - 1, 0) + pb * lo.get(t, 0) + (t + 1) * lo.get(t + 1, 0)
+                             for t in range(i + j + 1)}
+        return E
+
+    for axis, x in enumerate("xyz"):
+        E = direct(2, 2, vals[f"bA{x}"], vals[f"bB{x}"], vals["bh"])
+        for a in range(3):
+            for b in range(3):
+                for t, v in gen_hl.e1d("b", a, b, axis).items():
+                    got = 1.0 if v is None else vals[v]  # None: the factor 1 of E^{00}_0
+                    assert abs(got - E[(a, b)][t]) <= 1e-12 * max(1.0, abs(E[(a, b)][t])), (a, b, t)
